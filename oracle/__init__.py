@@ -1,0 +1,251 @@
+"""CPU oracle for the Binius64 prover hot path -- TEST INFRASTRUCTURE ONLY.
+
+ctypes bindings over ``oracle/liboracle.so`` (a C++ restatement of the reference algorithms, see
+``oracle/oracle.h``).  Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+legs may import this module; it is the checker, never the thing measured as the GPU product.
+
+Field elements travel as numpy ``uint64`` arrays of shape ``(n, 2)`` (low word, high word), i.e.
+the reference's 16-byte little-endian u128 encoding.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+
+
+def build(force: bool = False) -> str:
+    """Compile ``liboracle.so`` with the committed Makefile."""
+    if force or not os.path.exists(_LIB_PATH):
+        subprocess.run(["make", "-C", _HERE, "-s"], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.orc_gf_mul.argtypes = [_u64p, _u64p, _u64p]
+        L.orc_gf_mul_portable.argtypes = [_u64p, _u64p, _u64p]
+        L.orc_gf_inv.argtypes = [_u64p, _u64p]
+        L.orc_gf_mul_x.argtypes = [_u64p, _u64p]
+        L.orc_gf_mul_inv_x.argtypes = [_u64p, _u64p]
+        L.orc_gf_mul_vec.argtypes = [_u64p, _u64p, _u64p, ctypes.c_size_t]
+        L.orc_aes_mul.argtypes = [ctypes.c_uint8, ctypes.c_uint8]
+        L.orc_aes_mul.restype = ctypes.c_uint8
+        L.orc_aes_to_ghash_table.argtypes = [_u64p]
+        L.orc_sha256.argtypes = [_u8p, ctypes.c_size_t, _u8p]
+        L.orc_sha256_compress_node.argtypes = [_u8p, _u8p, _u8p]
+        L.orc_domain_twiddles.argtypes = [_u64p, ctypes.c_uint32, _u64p]
+        L.orc_domain_twiddles.restype = ctypes.c_int
+        for name in ("orc_ntt_forward", "orc_ntt_inverse"):
+            f = getattr(L, name)
+            f.argtypes = [_u64p, ctypes.c_uint32, _u64p, ctypes.c_uint32, ctypes.c_uint32,
+                          ctypes.c_uint32]
+            f.restype = ctypes.c_int
+        L.orc_rs_encode_batch.argtypes = [_u64p, ctypes.c_uint32, _u64p, ctypes.c_uint32,
+                                          ctypes.c_uint32, ctypes.c_uint32, _u64p]
+        L.orc_rs_encode_batch.restype = ctypes.c_int
+        L.orc_merkle_commit.argtypes = [_u64p, ctypes.c_uint32, ctypes.c_uint32, _u8p]
+        L.orc_merkle_commit.restype = ctypes.c_int
+        L.orc_eq_ind_partial_eval.argtypes = [_u64p, ctypes.c_uint32, _u64p]
+        L.orc_fri_fold_interleaved.argtypes = [_u64p, ctypes.c_uint32, ctypes.c_uint32, _u64p,
+                                               _u64p]
+        L.orc_fri_fold_interleaved.restype = ctypes.c_int
+        L.orc_fri_fold_codeword.argtypes = [_u64p, ctypes.c_uint32, _u64p, ctypes.c_uint32, _u64p,
+                                            ctypes.c_uint32, _u64p]
+        L.orc_fri_fold_codeword.restype = ctypes.c_int
+        L.orc_calculate_n_test_queries.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
+        L.orc_calculate_n_test_queries.restype = ctypes.c_uint32
+        L.orc_estimate_optimal_arity.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
+        L.orc_estimate_optimal_arity.restype = ctypes.c_uint32
+        L.orc_set_threads.argtypes = [ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _p64(a: np.ndarray):
+    assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_u64p)
+
+
+def _p8(a: np.ndarray):
+    assert a.dtype == np.uint8 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_u8p)
+
+
+def elems(n: int) -> np.ndarray:
+    return np.zeros((n, 2), dtype=np.uint64)
+
+
+def to_int(e) -> int:
+    e = np.asarray(e, dtype=np.uint64).reshape(2)
+    return int(e[0]) | (int(e[1]) << 64)
+
+
+def from_int(v: int) -> np.ndarray:
+    return np.array([v & ((1 << 64) - 1), v >> 64], dtype=np.uint64)
+
+
+def from_ints(vs) -> np.ndarray:
+    return np.stack([from_int(v) for v in vs]) if len(vs) else elems(0)
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+
+
+def gf_mul(a: int, b: int, portable: bool = False) -> int:
+    A, B, O = from_int(a), from_int(b), elems(1)
+    f = lib().orc_gf_mul_portable if portable else lib().orc_gf_mul
+    f(_p64(A), _p64(B), _p64(O))
+    return to_int(O)
+
+
+def gf_mul_vec(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    b = np.ascontiguousarray(b, dtype=np.uint64)
+    out = elems(a.shape[0])
+    lib().orc_gf_mul_vec(_p64(a), _p64(b), _p64(out), a.shape[0])
+    return out
+
+
+def gf_inv(a: int) -> int:
+    A, O = from_int(a), elems(1)
+    lib().orc_gf_inv(_p64(A), _p64(O))
+    return to_int(O)
+
+
+def gf_mul_x(a: int) -> int:
+    A, O = from_int(a), elems(1)
+    lib().orc_gf_mul_x(_p64(A), _p64(O))
+    return to_int(O)
+
+
+def gf_mul_inv_x(a: int) -> int:
+    A, O = from_int(a), elems(1)
+    lib().orc_gf_mul_inv_x(_p64(A), _p64(O))
+    return to_int(O)
+
+
+def aes_mul(a: int, b: int) -> int:
+    return int(lib().orc_aes_mul(a, b))
+
+
+def aes_to_ghash_table() -> list[int]:
+    out = elems(256)
+    lib().orc_aes_to_ghash_table(_p64(out))
+    return [to_int(out[i]) for i in range(256)]
+
+
+def sha256(data: bytes) -> bytes:
+    buf = np.frombuffer(data, dtype=np.uint8).copy() if data else np.zeros(1, dtype=np.uint8)
+    out = np.zeros(32, dtype=np.uint8)
+    lib().orc_sha256(_p8(buf), len(data), _p8(out))
+    return out.tobytes()
+
+
+def compress_node(left: bytes, right: bytes) -> bytes:
+    l = np.frombuffer(left, dtype=np.uint8).copy()
+    r = np.frombuffer(right, dtype=np.uint8).copy()
+    out = np.zeros(32, dtype=np.uint8)
+    lib().orc_sha256_compress_node(_p8(l), _p8(r), _p8(out))
+    return out.tobytes()
+
+
+def domain_twiddles(dim: int, basis=None) -> np.ndarray:
+    """Flat GenericPreExpanded twiddle table (layer l at [2^l - 1, 2^(l+1) - 1))."""
+    out = elems((1 << dim) - 1)
+    bp = None
+    if basis is not None:
+        b = from_ints(list(basis))
+        bp = _p64(b)
+    rc = lib().orc_domain_twiddles(bp, dim, _p64(out))
+    assert rc == 0
+    return out
+
+
+def ntt_forward(twiddles: np.ndarray, log_domain: int, data: np.ndarray, skip_early: int = 0,
+                skip_late: int = 0, inverse: bool = False) -> np.ndarray:
+    d = np.ascontiguousarray(data, dtype=np.uint64).copy()
+    log_d = int(d.shape[0]).bit_length() - 1
+    f = lib().orc_ntt_inverse if inverse else lib().orc_ntt_forward
+    rc = f(_p64(twiddles), log_domain, _p64(d), log_d, skip_early, skip_late)
+    if rc:
+        raise ValueError("ntt precondition violated")
+    return d
+
+
+def rs_encode_batch(twiddles: np.ndarray, log_domain: int, msg: np.ndarray, log_dim: int,
+                    log_inv_rate: int, log_batch: int) -> np.ndarray:
+    msg = np.ascontiguousarray(msg, dtype=np.uint64)
+    assert msg.shape[0] == 1 << (log_dim + log_batch)
+    out = elems(1 << (log_dim + log_batch + log_inv_rate))
+    rc = lib().orc_rs_encode_batch(_p64(twiddles), log_domain, _p64(msg), log_dim, log_inv_rate,
+                                   log_batch, _p64(out))
+    if rc:
+        raise ValueError("rs encode precondition violated")
+    return out
+
+
+def merkle_commit(elems_: np.ndarray, log_leaves: int, log_batch: int) -> np.ndarray:
+    """All tree nodes, (2^(log_leaves+1) - 1, 32) uint8: leaves first, root last."""
+    e = np.ascontiguousarray(elems_, dtype=np.uint64)
+    assert e.shape[0] == 1 << (log_leaves + log_batch)
+    nodes = np.zeros(((1 << (log_leaves + 1)) - 1) * 32, dtype=np.uint8)
+    lib().orc_merkle_commit(_p64(e), log_leaves, log_batch, _p8(nodes))
+    return nodes.reshape(-1, 32)
+
+
+def eq_ind_partial_eval(point: np.ndarray) -> np.ndarray:
+    p = np.ascontiguousarray(point, dtype=np.uint64).reshape(-1, 2)
+    out = elems(1 << p.shape[0])
+    lib().orc_eq_ind_partial_eval(_p64(p) if p.shape[0] else None, p.shape[0], _p64(out))
+    return out
+
+
+def fri_fold_interleaved(codeword: np.ndarray, log_len: int, log_batch: int,
+                         challenges: np.ndarray) -> np.ndarray:
+    cw = np.ascontiguousarray(codeword, dtype=np.uint64)
+    ch = np.ascontiguousarray(challenges, dtype=np.uint64).reshape(-1, 2)
+    assert ch.shape[0] == log_batch
+    out = elems(1 << log_len)
+    lib().orc_fri_fold_interleaved(_p64(cw), log_len, log_batch, _p64(ch) if log_batch else None,
+                                   _p64(out))
+    return out
+
+
+def fri_fold_codeword(twiddles: np.ndarray, log_domain: int, codeword: np.ndarray, log_len: int,
+                      challenges: np.ndarray) -> np.ndarray:
+    cw = np.ascontiguousarray(codeword, dtype=np.uint64)
+    ch = np.ascontiguousarray(challenges, dtype=np.uint64).reshape(-1, 2)
+    n = ch.shape[0]
+    out = elems(1 << (log_len - n))
+    rc = lib().orc_fri_fold_codeword(_p64(twiddles), log_domain, _p64(cw), log_len,
+                                     _p64(ch) if n else None, n, _p64(out))
+    if rc:
+        raise ValueError("fold precondition violated")
+    return out
+
+
+def calculate_n_test_queries(security_bits: int, log_inv_rate: int) -> int:
+    return int(lib().orc_calculate_n_test_queries(security_bits, log_inv_rate))
+
+
+def estimate_optimal_arity(log_block_length: int, digest_size: int, field_size: int) -> int:
+    return int(lib().orc_estimate_optimal_arity(log_block_length, digest_size, field_size))
+
+
+def random_elems(rng: np.random.Generator, n: int) -> np.ndarray:
+    return rng.integers(0, np.iinfo(np.uint64).max, size=(n, 2), dtype=np.uint64, endpoint=True)

@@ -1,0 +1,87 @@
+/*
+ * CPU oracle for the Binius64 prover hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is a plain C++ restatement of the
+ * reference algorithms (IrreducibleOSS/binius64) and exists to check the CUDA
+ * library bit-for-bit.  Only tests/, __graft_entry__.smoke() and bench.py's
+ * cpu_baseline / --impl reference legs may load it.  The product path
+ * (binius64_b200/) never links, imports or calls anything here.
+ *
+ * Parity pins: see tests/test_oracle_pins.py (GHASH KATs from
+ * verifier/field/src/ghash.rs:798-925, the NTT evaluation semantics of
+ * verifier/math/src/ntt/tests_evaluation.rs:244-295, FRI parameter KATs of
+ * verifier/verifier/src/fri/common.rs:225-247, SHA-256 against FIPS 180-4 via
+ * Python's hashlib, transcript chaining of
+ * verifier/transcript/src/fiat_shamir/hasher_challenger.rs:209-280).
+ *
+ * Field elements are 16-byte little-endian u128 values (the reference's
+ * serialization, verifier/field/src/ghash.rs:486-498): two uint64 words, low
+ * word first.
+ */
+#ifndef BINIUS_ORACLE_H
+#define BINIUS_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- GF(2^128), modulus x^128 + x^7 + x^2 + x + 1 (ghash.rs:3, 68-80) ---- */
+void orc_gf_mul(const uint64_t a[2], const uint64_t b[2], uint64_t out[2]);
+void orc_gf_mul_portable(const uint64_t a[2], const uint64_t b[2], uint64_t out[2]);
+void orc_gf_inv(const uint64_t a[2], uint64_t out[2]);
+void orc_gf_mul_x(const uint64_t a[2], uint64_t out[2]);
+void orc_gf_mul_inv_x(const uint64_t a[2], uint64_t out[2]);
+/* Elementwise products of n pairs (used by tests to cross-check the device). */
+void orc_gf_mul_vec(const uint64_t* a, const uint64_t* b, uint64_t* out, size_t n);
+/* AES GF(2^8) (aes_field.rs:26-35) and the GF(2^8) -> GF(2^128) embedding. */
+uint8_t orc_aes_mul(uint8_t a, uint8_t b);
+void orc_aes_to_ghash_table(uint64_t out[512]);
+
+/* ---- SHA-256 (FIPS 180-4) and the Binius node compression (hash/compress.rs:32-57) ---- */
+void orc_sha256(const uint8_t* data, size_t len, uint8_t out[32]);
+void orc_sha256_compress_node(const uint8_t left[32], const uint8_t right[32], uint8_t out[32]);
+
+/* ---- Domain context: GenericPreExpanded (ntt/domain_context.rs:19-46, 99-159) ----
+ * basis: dim elements (NULL = BinarySubspace::with_dim, basis x^i).
+ * Writes the flat twiddle table: layer l occupies [2^l - 1, 2^(l+1) - 1). */
+int orc_domain_twiddles(const uint64_t* basis, uint32_t dim, uint64_t* twiddles_out);
+
+/* ---- Additive NTT, NeighborsLastReference (ntt/reference.rs:20-76) ---- */
+int orc_ntt_forward(const uint64_t* twiddles, uint32_t log_domain, uint64_t* data, uint32_t log_d,
+                    uint32_t skip_early, uint32_t skip_late);
+int orc_ntt_inverse(const uint64_t* twiddles, uint32_t log_domain, uint64_t* data, uint32_t log_d,
+                    uint32_t skip_early, uint32_t skip_late);
+
+/* ---- ReedSolomonCode::encode_batch (reed_solomon.rs:128-201) ---- */
+int orc_rs_encode_batch(const uint64_t* twiddles, uint32_t log_domain, const uint64_t* msg,
+                        uint32_t log_dim, uint32_t log_inv_rate, uint32_t log_batch,
+                        uint64_t* codeword_out);
+
+/* ---- Merkle tree (binary_merkle_tree.rs:65-122), SHA-256 leaves, Binius compression nodes ----
+ * nodes_out: (2^(log_leaves+1) - 1) * 32 bytes, leaves first, root last. */
+int orc_merkle_commit(const uint64_t* elems, uint32_t log_leaves, uint32_t log_batch,
+                      uint8_t* nodes_out);
+
+/* ---- FRI folds (prover/prover/src/fri/fold.rs:260-318; verifier/.../fri/fold.rs:20-130) ---- */
+void orc_eq_ind_partial_eval(const uint64_t* point, uint32_t n, uint64_t* out);
+int orc_fri_fold_interleaved(const uint64_t* codeword, uint32_t log_len, uint32_t log_batch,
+                             const uint64_t* challenges, uint64_t* out);
+int orc_fri_fold_codeword(const uint64_t* twiddles, uint32_t log_domain, const uint64_t* codeword,
+                          uint32_t log_len, const uint64_t* challenges, uint32_t n_challenges,
+                          uint64_t* out);
+
+/* ---- FRI parameters (verifier/verifier/src/fri/common.rs:64-219) ---- */
+uint32_t orc_calculate_n_test_queries(uint32_t security_bits, uint32_t log_inv_rate);
+uint32_t orc_estimate_optimal_arity(uint32_t log_block_length, uint32_t digest_size,
+                                    uint32_t field_size);
+
+/* Number of worker threads the oracle may use (1 = scalar). */
+void orc_set_threads(int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
