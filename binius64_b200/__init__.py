@@ -1,0 +1,336 @@
+"""B200-native (sm_100a) Binius64 prover hot path.
+
+Host-side mirror of the reference's plugin surface for this path, over the C ABI in
+include/binius_gpu.h (libbinius_gpu.so).  Names, argument meaning and error behaviour follow the
+reference:
+
+* ``AdditiveNTT`` -- trait AdditiveNTT / DomainContext (verifier/math/src/ntt/mod.rs:58-179) over a
+  GenericPreExpanded domain (ntt/domain_context.rs:99-159).
+* ``ReedSolomonCode.encode_batch`` -- verifier/math/src/reed_solomon.rs:128-201.
+* ``BinaryMerkleTreeProver`` -- prover/prover/src/merkle_tree/prover.rs:16-119.
+* ``FRIParams`` -- verifier/verifier/src/fri/common.rs:14-219.
+* ``commit_interleaved`` -- prover/prover/src/fri/commit.rs:25-75.
+* ``fold_interleaved`` / ``fold_codeword`` -- prover/prover/src/fri/fold.rs:260-318.
+
+Device buffers are torch tensors (torch is plumbing for device memory and streams only) holding
+field elements as int64 pairs of shape (n, 2): the 16-byte little-endian u128 encoding.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._ffi import ArgumentError, BiniusError, check, lib
+
+__all__ = [
+    "AdditiveNTT", "ReedSolomonCode", "BinaryMerkleTreeProver", "MerkleCommitted", "FRIParams",
+    "CommitOutput", "commit_interleaved", "fold_interleaved", "fold_codeword", "gf_mul_batch",
+    "to_device", "to_host", "ArgumentError", "BiniusError", "version",
+]
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def version() -> str:
+    return lib().binius_version().decode()
+
+
+def _stream(stream=None) -> int:
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def _ptr(t) -> int:
+    return t.data_ptr()
+
+
+def _elems_of(t) -> int:
+    assert t.dtype == _torch().int64 and t.is_contiguous(), "field buffers are contiguous int64"
+    return t.numel() // 2
+
+
+def _log2_exact(n: int, what: str) -> int:
+    if n <= 0 or n & (n - 1):
+        raise ArgumentError(1, f"{what} must be a power of two, got {n}")
+    return n.bit_length() - 1
+
+
+def to_device(arr: np.ndarray, device: str | int = "cuda"):
+    """numpy uint64 (n, 2) -> device int64 (n, 2)."""
+    torch = _torch()
+    a = np.ascontiguousarray(arr, dtype=np.uint64).reshape(-1, 2)
+    return torch.from_numpy(a.view(np.int64)).to(device)
+
+
+def to_host(t) -> np.ndarray:
+    """device int64 (n, 2) -> numpy uint64 (n, 2)."""
+    return t.detach().cpu().contiguous().numpy().view(np.uint64).reshape(-1, 2)
+
+
+def empty_elems(n: int, device="cuda"):
+    return _torch().empty((n, 2), dtype=_torch().int64, device=device)
+
+
+class AdditiveNTT:
+    """Additive NTT over the GenericPreExpanded domain context of a binary subspace.
+
+    ``basis`` is a list of ``log_domain`` field elements as Python ints (None = the standard basis
+    x^i, BinarySubspace::with_dim).
+    """
+
+    def __init__(self, log_domain: int, basis=None, device: int | None = None):
+        torch = _torch()
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        self._handle = ctypes.c_void_p()
+        buf = None
+        if basis is not None:
+            basis = list(basis)
+            if len(basis) != log_domain:
+                raise ArgumentError(1, "basis length must equal log_domain")
+            arr = np.array([[b & (2**64 - 1), b >> 64] for b in basis], dtype=np.uint64)
+            buf = arr.ctypes.data_as(ctypes.c_void_p)
+        check(lib().binius_ntt_create(self.device, buf, log_domain, ctypes.byref(self._handle)))
+        self.basis = basis
+
+    @property
+    def handle(self):
+        return self._handle
+
+    def log_domain_size(self) -> int:
+        return int(lib().binius_ntt_log_domain(self._handle))
+
+    def twiddles(self, copy: bool = True):
+        """The flat twiddle table (layer l at [2^l - 1, 2^(l+1) - 1)) as a device tensor; with
+        copy=False a zero-copy view that is valid while this object is alive."""
+        torch = _torch()
+        n = (1 << self.log_domain_size()) - 1
+        ptr = lib().binius_ntt_twiddles(self._handle)
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (n, 2), "typestr": "<i8", "data": (ptr, False),
+                                        "version": 3, "strides": None}
+
+        view = torch.as_tensor(_View(), device=f"cuda:{self.device}")
+        return view.clone() if copy else view
+
+    def twiddle(self, layer: int, block: int) -> int:
+        t = to_host(self.twiddles(copy=False)[(1 << layer) - 1 + block].reshape(1, 2))[0]
+        return int(t[0]) | (int(t[1]) << 64)
+
+    def forward_transform(self, data, skip_early: int = 0, skip_late: int = 0, stream=None):
+        log_len = _log2_exact(_elems_of(data), "data length")
+        check(lib().binius_ntt_forward(self._handle, _ptr(data), log_len, skip_early, skip_late,
+                                       _stream(stream)))
+
+    def inverse_transform(self, data, skip_early: int = 0, skip_late: int = 0, stream=None):
+        log_len = _log2_exact(_elems_of(data), "data length")
+        check(lib().binius_ntt_inverse(self._handle, _ptr(data), log_len, skip_early, skip_late,
+                                       _stream(stream)))
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            try:
+                lib().binius_ntt_destroy(h)
+            except Exception:
+                pass
+            self._handle = None
+
+
+@dataclass
+class ReedSolomonCode:
+    log_dim: int
+    log_inv_rate: int
+
+    def log_len(self) -> int:
+        return self.log_dim + self.log_inv_rate
+
+    def encode_batch(self, ntt: AdditiveNTT, data, log_batch_size: int, out=None, stream=None):
+        n = _elems_of(data)
+        if n != 1 << (self.log_dim + log_batch_size):
+            raise ArgumentError(1, "data.log_len() must equal log_dim + log_batch_size")
+        if out is None:
+            out = empty_elems(1 << (self.log_len() + log_batch_size), device=data.device)
+        check(lib().binius_rs_encode_batch(ntt.handle, _ptr(data), self.log_dim, self.log_inv_rate,
+                                           log_batch_size, _ptr(out), _stream(stream)))
+        return out
+
+
+@dataclass
+class MerkleCommitted:
+    """BinaryMerkleTree: flat digests (2^(L+1) - 1, 32) on the device, root last."""
+    log_len: int
+    nodes: object  # torch uint8 tensor
+
+    def root(self) -> bytes:
+        return bytes(self.nodes[-1].cpu().numpy().tobytes())
+
+    def layer(self, layer_depth: int):
+        if layer_depth > self.log_len:
+            raise ArgumentError(1, "IncorrectLayerDepth")
+        start = self.nodes.shape[0] + 1 - (1 << (layer_depth + 1))
+        return self.nodes[start:start + (1 << layer_depth)]
+
+    def branch(self, index: int, layer_depth: int, stream=None) -> list[bytes]:
+        n = self.log_len - layer_depth
+        buf = (ctypes.c_uint8 * max(1, 32 * n))()
+        check(lib().binius_merkle_branch(_ptr(self.nodes), self.log_len, index, layer_depth,
+                                         ctypes.addressof(buf), _stream(stream)))
+        raw = bytes(buf)[: 32 * n]
+        return [raw[32 * i: 32 * (i + 1)] for i in range(n)]
+
+
+class BinaryMerkleTreeProver:
+    """SHA-256 leaves + Binius SHA-256 compression nodes (StdDigest / StdCompression)."""
+
+    def commit(self, elements, batch_size: int, stream=None):
+        n = _elems_of(elements)
+        log_batch = _log2_exact(batch_size, "batch_size")
+        if n % batch_size:
+            raise ArgumentError(1, "IncorrectBatchSize")
+        log_len = _log2_exact(n // batch_size, "leaf count")
+        torch = _torch()
+        nodes = torch.empty(((2 << log_len) - 1, 32), dtype=torch.uint8, device=elements.device)
+        check(lib().binius_merkle_commit(_ptr(elements), log_len, log_batch, _ptr(nodes),
+                                         _stream(stream)))
+        committed = MerkleCommitted(log_len, nodes)
+        return committed.root(), committed
+
+
+def n_test_queries(security_bits: int, log_inv_rate: int) -> int:
+    return int(lib().binius_fri_n_test_queries(security_bits, log_inv_rate))
+
+
+def estimate_optimal_arity(log_block_length: int, digest_size: int, field_size: int) -> int:
+    return int(lib().binius_fri_estimate_optimal_arity(log_block_length, digest_size, field_size))
+
+
+def _ceil_log2(n: int) -> int:
+    return 0 if n <= 1 else (n - 1).bit_length()
+
+
+@dataclass
+class FRIParams:
+    rs_code: ReedSolomonCode
+    log_batch_size: int
+    fold_arities: list = field(default_factory=list)
+    n_test_queries: int = 0
+
+    @property
+    def log_terminal_dim(self) -> int:
+        return self.rs_code.log_dim - sum(self.fold_arities)
+
+    @classmethod
+    def choose_with_constant_fold_arity(cls, log_msg_len: int, security_bits: int,
+                                        log_inv_rate: int, arity: int) -> "FRIParams":
+        """verifier/verifier/src/fri/common.rs:64-115."""
+        assert arity > 0
+        log_batch_size = min(log_msg_len, arity)
+        log_dim = log_msg_len - log_batch_size
+        rs = ReedSolomonCode(log_dim, log_inv_rate)
+        nq = n_test_queries(security_bits, log_inv_rate)
+        cap_height = _ceil_log2(nq)
+        log_terminal_len = min(max(cap_height, log_inv_rate), rs.log_len())
+        quotient, remainder = divmod(rs.log_len() - log_terminal_len, arity)
+        arities = [arity] * quotient + ([remainder] if remainder else [])
+        if sum(arities) > rs.log_dim:
+            raise ArgumentError(1, "InvalidFoldAritySequence")
+        return cls(rs, log_batch_size, arities, nq)
+
+    def log_len(self) -> int:
+        return self.rs_code.log_len() + self.log_batch_size
+
+    def log_msg_len(self) -> int:
+        return self.rs_code.log_dim + self.log_batch_size
+
+    def n_fold_rounds(self) -> int:
+        return self.log_msg_len()
+
+    def index_bits(self) -> int:
+        return self.rs_code.log_len()
+
+
+def standard_domain_rs_basis(log_code_len: int, log_batch: int, device=None) -> list[int]:
+    """Basis of the RS code subspace chosen by Verifier::setup (verify.rs:85-97): row `log_batch` of
+    the normalized subspace-polynomial evaluations of the standard domain of dim log_code_len
+    (GenericOnTheFly::subspace)."""
+    big = AdditiveNTT(log_code_len, device=device)
+    n = log_code_len - log_batch
+    base = (1 << (log_code_len - 1 - log_batch)) - 1
+    idx = [base + (1 << k) for k in range(n - 1)]
+    tw = to_host(big.twiddles(copy=False)[idx]) if idx else np.zeros((0, 2), dtype=np.uint64)
+    del big
+    return [1] + [int(t[0]) | (int(t[1]) << 64) for t in tw]
+
+
+@dataclass
+class CommitOutput:
+    commitment: bytes
+    committed: MerkleCommitted
+    codeword: object
+
+
+def commit_interleaved(params: FRIParams, ntt: AdditiveNTT, merkle_prover: BinaryMerkleTreeProver,
+                       message, stream=None) -> CommitOutput:
+    """prover/prover/src/fri/commit.rs:25-75."""
+    if _elems_of(message) != 1 << params.log_msg_len():
+        raise ArgumentError(1, "interleaved message length does not match code parameters")
+    torch = _torch()
+    rs = params.rs_code
+    codeword = empty_elems(1 << params.log_len(), device=message.device)
+    log_leaves = rs.log_len()
+    nodes = torch.empty(((2 << log_leaves) - 1, 32), dtype=torch.uint8, device=message.device)
+    root = (ctypes.c_uint8 * 32)()
+    check(lib().binius_fri_commit_interleaved(ntt.handle, _ptr(message), rs.log_dim,
+                                              rs.log_inv_rate, params.log_batch_size,
+                                              _ptr(codeword), _ptr(nodes), ctypes.addressof(root),
+                                              _stream(stream)))
+    return CommitOutput(bytes(root), MerkleCommitted(log_leaves, nodes), codeword)
+
+
+def _challenges_buf(challenges):
+    arr = np.array([[c & (2**64 - 1), c >> 64] for c in challenges], dtype=np.uint64).reshape(-1, 2)
+    return arr, (arr.ctypes.data_as(ctypes.c_void_p) if len(challenges) else None)
+
+
+def fold_interleaved(codeword, challenges, log_len: int, log_batch_size: int, out=None,
+                     stream=None):
+    """prover/prover/src/fri/fold.rs:260-282."""
+    if len(challenges) != log_batch_size:
+        raise ArgumentError(1, "challenges.len() must equal log_batch_size")
+    if _elems_of(codeword) != 1 << (log_len + log_batch_size):
+        raise ArgumentError(1, "codeword length mismatch")
+    arr, buf = _challenges_buf(challenges)
+    if out is None:
+        out = empty_elems(1 << log_len, device=codeword.device)
+    check(lib().binius_fri_fold_interleaved(_ptr(codeword), log_len, log_batch_size, buf, _ptr(out),
+                                            _stream(stream)))
+    return out
+
+
+def fold_codeword(ntt: AdditiveNTT, codeword, challenges, log_len: int, out=None, stream=None):
+    """prover/prover/src/fri/fold.rs:297-318."""
+    if _elems_of(codeword) != 1 << log_len:
+        raise ArgumentError(1, "codeword length mismatch")
+    arr, buf = _challenges_buf(challenges)
+    if out is None:
+        out = empty_elems(1 << (log_len - len(challenges)), device=codeword.device)
+    check(lib().binius_fri_fold_codeword(ntt.handle, _ptr(codeword), log_len, buf, len(challenges),
+                                         _ptr(out), _stream(stream)))
+    return out
+
+
+def gf_mul_batch(a, b, out=None, stream=None):
+    n = _elems_of(a)
+    if _elems_of(b) != n:
+        raise ArgumentError(1, "operand lengths differ")
+    if out is None:
+        out = empty_elems(n, device=a.device)
+    check(lib().binius_gf_mul_batch(_ptr(a), _ptr(b), _ptr(out), n, _stream(stream)))
+    return out

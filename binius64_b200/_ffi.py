@@ -1,0 +1,102 @@
+"""ctypes binding of libbinius_gpu.so (declarations in include/binius_gpu.h).
+
+The CUDA library is the product path: if it is missing this module raises instead of falling back
+to any CPU implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+LIB_PATH = os.path.join(PKG, "libbinius_gpu.so")
+HEADER_PATHS = [os.path.join(ROOT, "include", "binius_gpu.h")]
+
+BINIUS_OK = 0
+BINIUS_E_ARG = 1
+BINIUS_E_OOM = 2
+BINIUS_E_CUDA = 3
+BINIUS_E_TIMEOUT = 4
+BINIUS_E_UNSUPPORTED = 5
+
+_STATUS_NAMES = {0: "OK", 1: "ArgumentError", 2: "OutOfMemory", 3: "CudaError", 4: "Timeout",
+                 5: "Unsupported"}
+
+
+class BiniusError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class ArgumentError(BiniusError, ValueError):
+    """Mirrors binius_prover::Error::ArgumentError (prover/prover/src/error.rs:9-24)."""
+
+
+_c = ctypes
+_vp = _c.c_void_p
+_u32 = _c.c_uint32
+_u64 = _c.c_uint64
+_int = _c.c_int
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "binius_last_error": (_c.c_char_p, []),
+    "binius_version": (_c.c_char_p, []),
+    "binius_launch_count": (_u64, []),
+    "binius_ntt_create": (_int, [_int, _vp, _u32, _c.POINTER(_vp)]),
+    "binius_ntt_destroy": (_int, [_vp]),
+    "binius_ntt_log_domain": (_u32, [_vp]),
+    "binius_ntt_twiddles": (_vp, [_vp]),
+    "binius_ntt_forward": (_int, [_vp, _vp, _u32, _u32, _u32, _vp]),
+    "binius_ntt_inverse": (_int, [_vp, _vp, _u32, _u32, _u32, _vp]),
+    "binius_rs_encode_batch": (_int, [_vp, _vp, _u32, _u32, _u32, _vp, _vp]),
+    "binius_merkle_commit": (_int, [_vp, _u32, _u32, _vp, _vp]),
+    "binius_merkle_branch": (_int, [_vp, _u32, _u64, _u32, _vp, _vp]),
+    "binius_fri_fold_interleaved": (_int, [_vp, _u32, _u32, _vp, _vp, _vp]),
+    "binius_fri_fold_codeword": (_int, [_vp, _vp, _u32, _vp, _u32, _vp, _vp]),
+    "binius_fri_commit_interleaved": (_int, [_vp, _vp, _u32, _u32, _u32, _vp, _vp, _vp, _vp]),
+    "binius_fri_n_test_queries": (_u32, [_u32, _u32]),
+    "binius_fri_estimate_optimal_arity": (_u32, [_u32, _u32, _u32]),
+    "binius_gf_mul_batch": (_int, [_vp, _vp, _vp, _u64, _vp]),
+}
+
+_lib = None
+
+
+def declared_functions() -> list[str]:
+    """Function names declared in include/*.h (used by the export test)."""
+    names = []
+    for path in HEADER_PATHS:
+        text = open(path).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(binius_[a-z0-9_]+)\s*\(", text):
+            if m.group(1) not in names:
+                names.append(m.group(1))
+    return names
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; "
+                f"g.build()'` (there is no CPU fallback for the GPU prover path)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != BINIUS_OK:
+        msg = lib().binius_last_error().decode(errors="replace")
+        if rc == BINIUS_E_ARG:
+            raise ArgumentError(rc, msg)
+        raise BiniusError(rc, msg)

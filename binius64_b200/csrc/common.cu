@@ -1,0 +1,74 @@
+// Error reporting, version and host field helpers of libbinius_gpu.
+#include <stdio.h>
+
+#include <atomic>
+
+#include "internal.h"
+
+namespace bgpu {
+
+static thread_local std::string g_last_error;
+static std::atomic<uint64_t> g_launches{0};
+
+void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+int set_error(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int clear_error() {
+  g_last_error.clear();
+  return BINIUS_OK;
+}
+
+int cuda_error(cudaError_t e, const char* what) {
+  char buf[512];
+  snprintf(buf, sizeof(buf), "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+  return set_error(e == cudaErrorMemoryAllocation ? BINIUS_E_OOM : BINIUS_E_CUDA, buf);
+}
+
+static inline void clmul64(uint64_t a, uint64_t b, uint64_t& lo, uint64_t& hi) {
+  uint64_t l = 0, h = 0;
+  for (int i = 0; i < 64; i++) {
+    uint64_t m = (uint64_t)0 - ((b >> i) & 1);
+    l ^= (a << i) & m;
+    if (i) h ^= (a >> (64 - i)) & m;
+  }
+  lo = l;
+  hi = h;
+}
+
+hu128 host_gf_mul(hu128 a, hu128 b) {
+  uint64_t a0 = (uint64_t)a, a1 = (uint64_t)(a >> 64), b0 = (uint64_t)b, b1 = (uint64_t)(b >> 64);
+  uint64_t l0, l1, h0, h1, m0, m1, x0, x1;
+  clmul64(a0, b0, l0, l1);
+  clmul64(a1, b1, h0, h1);
+  clmul64(a0, b1, m0, m1);
+  clmul64(a1, b0, x0, x1);
+  uint64_t p0 = l0, p1 = l1 ^ m0 ^ x0, p2 = h0 ^ m1 ^ x1, p3 = h1;
+  uint64_t t = (p3 >> 63) ^ (p3 >> 62) ^ (p3 >> 57);
+  uint64_t lo = p0 ^ p2 ^ (p2 << 1) ^ (p2 << 2) ^ (p2 << 7) ^ t ^ (t << 1) ^ (t << 2) ^ (t << 7);
+  uint64_t hi = p1 ^ p3 ^ ((p3 << 1) | (p2 >> 63)) ^ ((p3 << 2) | (p2 >> 62)) ^
+                ((p3 << 7) | (p2 >> 57));
+  return ((hu128)hi << 64) | lo;
+}
+
+// a^(2^128 - 2) by the chain a^(2^k - 1) = (a^(2^(k-1) - 1))^2 * a.
+hu128 host_gf_inv(hu128 a) {
+  hu128 r = a;
+  for (int k = 2; k <= 127; k++) r = host_gf_mul(host_gf_mul(r, r), a);
+  return host_gf_mul(r, r);
+}
+
+}  // namespace bgpu
+
+extern "C" {
+
+const char* binius_last_error(void) { return bgpu::g_last_error.c_str(); }
+
+const char* binius_version(void) { return "binius64_b200 0.1.0 (sm_100a)"; }
+
+uint64_t binius_launch_count(void) { return bgpu::g_launches.load(std::memory_order_relaxed); }
+
+}  // extern "C"

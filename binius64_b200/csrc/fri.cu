@@ -1,0 +1,244 @@
+// FRI folding, the FRI interleaved commit and FRI parameter selection.
+//
+// fold_interleaved (prover/prover/src/fri/fold.rs:260-282): each output is the inner product of a
+// 2^log_batch chunk with eq_ind(challenges).  The 256-bit carry-less products are XOR-accumulated
+// unreduced and reduced once per output (reduction is linear, so the bits are identical).
+// fold_codeword (prover/prover/src/fri/fold.rs:297-318 -> verifier/verifier/src/fri/fold.rs:20-99):
+// one thread folds one coset of 2^n values in registers through all n rounds: the inverse NTT
+// butterfly with twiddle(log_len - 1 - round, index) then u + (v - u) * r.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+
+#include "gf128.cuh"
+#include "internal.h"
+
+using namespace bgpu;
+
+namespace bgpu {
+int rs_encode_batch(const binius_ntt* ntt, const void* d_msg, uint32_t log_dim,
+                    uint32_t log_inv_rate, uint32_t log_batch, void* d_codeword,
+                    cudaStream_t stream);
+int merkle_commit(const void* d_elems, uint32_t log_leaves, uint32_t log_batch, void* d_nodes,
+                  cudaStream_t stream);
+}  // namespace bgpu
+
+namespace {
+
+constexpr uint32_t kMaxChallenges = 8;
+
+struct Challenges {
+  uint4 r[kMaxChallenges];
+};
+
+unsigned grid_for(uint64_t n, unsigned threads) {
+  uint64_t g = (n + threads - 1) / threads;
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, 148ull * 64));
+}
+
+__global__ void __launch_bounds__(256)
+    fold_interleaved_kernel(const uint4* __restrict__ cw, uint32_t log_len, uint32_t log_batch,
+                            Challenges ch, uint4* __restrict__ out) {
+  __shared__ uint4 tensor[1u << kMaxChallenges];
+  const uint32_t batch = 1u << log_batch;
+  // eq_ind(r)[j] = prod_i (bit_i(j) ? r_i : 1 + r_i)  (multilinear/eq.rs:39-71)
+  for (uint32_t j = threadIdx.x; j < batch; j += blockDim.x) {
+    uint4 acc = gf_one();
+    for (uint32_t i = 0; i < log_batch; i++) {
+      uint4 f = ch.r[i];
+      if (!((j >> i) & 1)) f.x ^= 1u;
+      acc = gf_mul(acc, f);
+    }
+    tensor[j] = acc;
+  }
+  __syncthreads();
+  const uint64_t n = 1ull << log_len;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    u256 acc = {0, 0, 0, 0};
+    const uint4* row = cw + (i << log_batch);
+    for (uint32_t j = 0; j < batch; j++) xor_into(acc, clmul128(__ldg(row + j), tensor[j]));
+    out[i] = reduce256(acc);
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(256)
+    fold_codeword_kernel(const uint4* __restrict__ cw, uint32_t log_len,
+                         const uint4* __restrict__ tw, Challenges ch, uint4* __restrict__ out) {
+  const uint64_t n_chunks = 1ull << (log_len - N);
+  for (uint64_t ci = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; ci < n_chunks;
+       ci += (uint64_t)gridDim.x * blockDim.x) {
+    uint4 v[1 << N];
+#pragma unroll
+    for (int j = 0; j < (1 << N); j++) v[j] = __ldg(cw + (ci << N) + j);
+    uint32_t cur = log_len;
+#pragma unroll
+    for (int kk = 0; kk < N; kk++) {
+      const int size = N - kk;
+      const uint4 r = ch.r[kk];
+      const uint64_t layer_base = (1ull << (cur - 1)) - 1;
+#pragma unroll
+      for (int off = 0; off < (1 << (size - 1)); off++) {
+        uint4 u = v[off << 1], w = v[(off << 1) | 1];
+        const uint64_t index = (ci << (size - 1)) | (uint64_t)off;
+        const uint4 t = __ldg(tw + layer_base + index);
+        gf_add_into(w, u);
+        gf_add_into(u, gf_mul(w, t));
+        gf_add_into(w, u);  // w - u
+        gf_add_into(u, gf_mul(w, r));
+        v[off] = u;
+      }
+      cur--;
+    }
+    out[ci] = v[0];
+  }
+}
+
+__global__ void gf_mul_batch_kernel(const uint4* __restrict__ a, const uint4* __restrict__ b,
+                                    uint4* __restrict__ out, uint64_t n) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = gf_mul(__ldg(a + i), __ldg(b + i));
+}
+
+int load_challenges(const void* h, uint32_t n, Challenges& ch) {
+  if (n > kMaxChallenges) return set_error(BINIUS_E_ARG, "at most 8 folding challenges per call");
+  if (n && !h) return set_error(BINIUS_E_ARG, "challenges is NULL");
+  memset(&ch, 0, sizeof(ch));
+  if (n) memcpy(ch.r, h, 16 * (size_t)n);
+  return BINIUS_OK;
+}
+
+template <int N>
+void launch_fold_codeword(const uint4* cw, uint32_t log_len, const uint4* tw, const Challenges& ch,
+                          uint4* out, cudaStream_t s) {
+  uint64_t n_chunks = 1ull << (log_len - N);
+  fold_codeword_kernel<N><<<grid_for(n_chunks, 256), 256, 0, s>>>(cw, log_len, tw, ch, out);
+}
+
+}  // namespace
+
+extern "C" {
+
+int binius_fri_fold_interleaved(const void* d_codeword, uint32_t log_len, uint32_t log_batch,
+                                const void* h_challenges, void* d_out, void* stream) {
+  BGPU_ARG(d_codeword != nullptr && d_out != nullptr, "codeword / out is NULL");
+  BGPU_ARG(log_len + log_batch <= 40, "codeword too large");
+  Challenges ch;
+  if (int rc = load_challenges(h_challenges, log_batch, ch)) return rc;
+  cudaStream_t s = as_stream(stream);
+  fold_interleaved_kernel<<<grid_for(1ull << log_len, 256), 256, 0, s>>>(
+      static_cast<const uint4*>(d_codeword), log_len, log_batch, ch, static_cast<uint4*>(d_out));
+  BGPU_LAUNCH_CHECK("fold_interleaved_kernel");
+  count_launch();
+  return clear_error();
+}
+
+int binius_fri_fold_codeword(const binius_ntt* ntt, const void* d_codeword, uint32_t log_len,
+                             const void* h_challenges, uint32_t n_challenges, void* d_out,
+                             void* stream) {
+  BGPU_ARG(ntt != nullptr, "ntt is NULL");
+  BGPU_ARG(d_codeword != nullptr && d_out != nullptr, "codeword / out is NULL");
+  BGPU_ARG(n_challenges <= log_len, "more challenges than codeword variables");
+  BGPU_ARG(log_len <= ntt->log_domain, "codeword longer than the NTT domain");
+  Challenges ch;
+  if (int rc = load_challenges(h_challenges, n_challenges, ch)) return rc;
+  cudaStream_t s = as_stream(stream);
+  const uint4* cw = static_cast<const uint4*>(d_codeword);
+  const uint4* tw = static_cast<const uint4*>(ntt->d_twiddles);
+  uint4* out = static_cast<uint4*>(d_out);
+  if (n_challenges == 0) {
+    BGPU_CUDA(cudaMemcpyAsync(d_out, d_codeword, 16ull << log_len, cudaMemcpyDeviceToDevice, s));
+    return clear_error();
+  }
+  // Rounds are applied in steps of at most 4 (one coset of 16 values per thread in registers);
+  // a fold over n challenges equals n successive single-challenge folds of the whole codeword,
+  // so steps chain through a stream-ordered intermediate buffer.
+  void* tmp = nullptr;
+  if (n_challenges > 4) {
+    BGPU_CUDA(cudaMallocAsync(&tmp, 16ull << (log_len - 4), s));
+  }
+  uint32_t done = 0, cur_len = log_len;
+  const uint4* src = cw;
+  while (done < n_challenges) {
+    uint32_t step = std::min<uint32_t>(4, n_challenges - done);
+    Challenges sub;
+    memset(&sub, 0, sizeof(sub));
+    for (uint32_t i = 0; i < step; i++) sub.r[i] = ch.r[done + i];
+    // n <= 8, so there are at most two steps: codeword -> tmp -> out.
+    uint4* dst = (done + step == n_challenges) ? out : static_cast<uint4*>(tmp);
+    switch (step) {
+      case 1: launch_fold_codeword<1>(src, cur_len, tw, sub, dst, s); break;
+      case 2: launch_fold_codeword<2>(src, cur_len, tw, sub, dst, s); break;
+      case 3: launch_fold_codeword<3>(src, cur_len, tw, sub, dst, s); break;
+      default: launch_fold_codeword<4>(src, cur_len, tw, sub, dst, s); break;
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      if (tmp) cudaFreeAsync(tmp, s);
+      return cuda_error(e, "fold_codeword_kernel");
+    }
+    count_launch();
+    src = dst;
+    cur_len -= step;
+    done += step;
+  }
+  if (tmp) BGPU_CUDA(cudaFreeAsync(tmp, s));
+  return clear_error();
+}
+
+int binius_fri_commit_interleaved(const binius_ntt* ntt, const void* d_msg, uint32_t log_dim,
+                                  uint32_t log_inv_rate, uint32_t log_batch, void* d_codeword,
+                                  void* d_nodes, void* h_root, void* stream) {
+  cudaStream_t s = as_stream(stream);
+  if (int rc = bgpu::rs_encode_batch(ntt, d_msg, log_dim, log_inv_rate, log_batch, d_codeword, s))
+    return rc;
+  const uint32_t log_leaves = log_dim + log_inv_rate;
+  if (int rc = bgpu::merkle_commit(d_codeword, log_leaves, log_batch, d_nodes, s)) return rc;
+  if (h_root) {
+    const uint8_t* root = static_cast<const uint8_t*>(d_nodes) + 32 * ((2ull << log_leaves) - 2);
+    BGPU_CUDA(cudaMemcpyAsync(h_root, root, 32, cudaMemcpyDeviceToHost, s));
+    BGPU_CUDA(cudaStreamSynchronize(s));
+  }
+  return clear_error();
+}
+
+// calculate_n_test_queries (verifier/verifier/src/fri/common.rs:182-186).
+uint32_t binius_fri_n_test_queries(uint32_t security_bits, uint32_t log_inv_rate) {
+  double rate = pow(2.0, -(double)log_inv_rate);
+  double per_query_err = 0.5 * (1.0 + rate);
+  return (uint32_t)ceil((double)security_bits / -log2(per_query_err));
+}
+
+// estimate_optimal_arity (verifier/verifier/src/fri/common.rs:191-219).
+uint32_t binius_fri_estimate_optimal_arity(uint32_t log_block_length, uint32_t digest_size,
+                                           uint32_t field_size) {
+  uint32_t best = 1;
+  bool have_old = false;
+  uint64_t old = 0;
+  for (uint32_t arity = 1; arity <= log_block_length; arity++) {
+    uint64_t est =
+        ((uint64_t)(log_block_length / 2) * digest_size + ((uint64_t)1 << arity) * field_size) *
+        (log_block_length - arity) / arity;
+    if (have_old && est > old) break;
+    have_old = true;
+    old = est;
+    best = arity;
+  }
+  return best;
+}
+
+int binius_gf_mul_batch(const void* d_a, const void* d_b, void* d_out, uint64_t n, void* stream) {
+  BGPU_ARG((d_a && d_b && d_out) || n == 0, "NULL operand");
+  if (n == 0) return clear_error();
+  gf_mul_batch_kernel<<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(
+      static_cast<const uint4*>(d_a), static_cast<const uint4*>(d_b), static_cast<uint4*>(d_out),
+      n);
+  BGPU_LAUNCH_CHECK("gf_mul_batch_kernel");
+  count_launch();
+  return clear_error();
+}
+
+}  // extern "C"

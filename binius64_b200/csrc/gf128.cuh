@@ -1,0 +1,109 @@
+// GF(2^128) GHASH-field arithmetic on the sm_100a integer pipes.
+//
+// Field: x^128 + x^7 + x^2 + x + 1, bit i of the little-endian u128 is the coefficient of x^i
+// (BinaryField128bGhash, verifier/field/src/ghash.rs:55-96).  An element lives in a uint4
+// (x = bits 0..31, ..., w = bits 96..127), which is exactly the 16-byte LE serialization, so
+// HBM buffers are read and written with 128-bit vector accesses and no repacking.
+//
+// There is no carry-less multiply instruction on the GPU.  The 32x32 -> 64 carry-less product is
+// built from integer multiplies "with holes" (the bmul technique published in BearSSL's
+// constant-time GHASH, ghash_ctmul.c): split each operand into the four bit classes i = r mod 4;
+// a product of two classes has at most 8 terms at any bit position, which fits in the 4-bit gap
+// before the next position of the same class, so the integer product's bits in the right class
+// are exactly the carry-less sums.  128x128 uses two levels of Karatsuba (9 such products).
+#pragma once
+#include <stdint.h>
+
+namespace bgpu {
+
+struct u256 {
+  uint64_t p0, p1, p2, p3;
+};
+
+__device__ __forceinline__ uint64_t mulw(uint32_t a, uint32_t b) {
+  return (uint64_t)a * (uint64_t)b;
+}
+
+__device__ __forceinline__ uint64_t clmul32(uint32_t x, uint32_t y) {
+  const uint32_t m0 = 0x11111111u, m1 = 0x22222222u, m2 = 0x44444444u, m3 = 0x88888888u;
+  uint32_t x0 = x & m0, x1 = x & m1, x2 = x & m2, x3 = x & m3;
+  uint32_t y0 = y & m0, y1 = y & m1, y2 = y & m2, y3 = y & m3;
+  uint64_t z0 = mulw(x0, y0) ^ mulw(x1, y3) ^ mulw(x2, y2) ^ mulw(x3, y1);
+  uint64_t z1 = mulw(x0, y1) ^ mulw(x1, y0) ^ mulw(x2, y3) ^ mulw(x3, y2);
+  uint64_t z2 = mulw(x0, y2) ^ mulw(x1, y1) ^ mulw(x2, y0) ^ mulw(x3, y3);
+  uint64_t z3 = mulw(x0, y3) ^ mulw(x1, y2) ^ mulw(x2, y1) ^ mulw(x3, y0);
+  return (z0 & 0x1111111111111111ull) | (z1 & 0x2222222222222222ull) |
+         (z2 & 0x4444444444444444ull) | (z3 & 0x8888888888888888ull);
+}
+
+// 64x64 -> 128 carry-less product, one Karatsuba level over clmul32.
+__device__ __forceinline__ void clmul64(uint64_t a, uint64_t b, uint64_t& lo, uint64_t& hi) {
+  uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32);
+  uint32_t b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+  uint64_t l = clmul32(a0, b0);
+  uint64_t h = clmul32(a1, b1);
+  uint64_t m = clmul32(a0 ^ a1, b0 ^ b1) ^ l ^ h;
+  lo = l ^ (m << 32);
+  hi = h ^ (m >> 32);
+}
+
+__device__ __forceinline__ uint64_t lo64(uint4 a) { return ((uint64_t)a.y << 32) | a.x; }
+__device__ __forceinline__ uint64_t hi64(uint4 a) { return ((uint64_t)a.w << 32) | a.z; }
+__device__ __forceinline__ uint4 make_gf(uint64_t lo, uint64_t hi) {
+  return make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
+}
+
+// Unreduced 128x128 -> 256 carry-less product (Karatsuba over clmul64).
+__device__ __forceinline__ u256 clmul128(uint4 a, uint4 b) {
+  uint64_t a0 = lo64(a), a1 = hi64(a), b0 = lo64(b), b1 = hi64(b);
+  uint64_t l0, l1, h0, h1, m0, m1;
+  clmul64(a0, b0, l0, l1);
+  clmul64(a1, b1, h0, h1);
+  clmul64(a0 ^ a1, b0 ^ b1, m0, m1);
+  m0 ^= l0 ^ h0;
+  m1 ^= l1 ^ h1;
+  u256 r;
+  r.p0 = l0;
+  r.p1 = l1 ^ m0;
+  r.p2 = h0 ^ m1;
+  r.p3 = h1;
+  return r;
+}
+
+__device__ __forceinline__ void xor_into(u256& acc, const u256& v) {
+  acc.p0 ^= v.p0;
+  acc.p1 ^= v.p1;
+  acc.p2 ^= v.p2;
+  acc.p3 ^= v.p3;
+}
+
+// Reduction modulo x^128 + x^7 + x^2 + x + 1: the high half H contributes H*(x^7 + x^2 + x + 1);
+// the <= 7 bits pushed past x^127 by that shift are folded a second time.
+__device__ __forceinline__ uint4 reduce256(const u256& p) {
+  uint64_t t = (p.p3 >> 63) ^ (p.p3 >> 62) ^ (p.p3 >> 57);
+  uint64_t lo = p.p0 ^ p.p2 ^ (p.p2 << 1) ^ (p.p2 << 2) ^ (p.p2 << 7) ^ t ^ (t << 1) ^ (t << 2) ^
+                (t << 7);
+  uint64_t hi = p.p1 ^ p.p3 ^ ((p.p3 << 1) | (p.p2 >> 63)) ^ ((p.p3 << 2) | (p.p2 >> 62)) ^
+                ((p.p3 << 7) | (p.p2 >> 57));
+  return make_gf(lo, hi);
+}
+
+__device__ __forceinline__ uint4 gf_mul(uint4 a, uint4 b) { return reduce256(clmul128(a, b)); }
+
+__device__ __forceinline__ uint4 gf_add(uint4 a, uint4 b) {
+  return make_uint4(a.x ^ b.x, a.y ^ b.y, a.z ^ b.z, a.w ^ b.w);
+}
+
+__device__ __forceinline__ void gf_add_into(uint4& a, uint4 b) {
+  a.x ^= b.x;
+  a.y ^= b.y;
+  a.z ^= b.z;
+  a.w ^= b.w;
+}
+
+__device__ __forceinline__ bool gf_is_zero(uint4 a) { return (a.x | a.y | a.z | a.w) == 0u; }
+
+__device__ __forceinline__ uint4 gf_zero() { return make_uint4(0u, 0u, 0u, 0u); }
+__device__ __forceinline__ uint4 gf_one() { return make_uint4(1u, 0u, 0u, 0u); }
+
+}  // namespace bgpu

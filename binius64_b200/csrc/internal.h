@@ -1,0 +1,51 @@
+// Host-side internals shared by the translation units of libbinius_gpu.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/binius_gpu.h"
+
+namespace bgpu {
+
+// Records msg as the calling thread's last error and returns code.
+int set_error(int code, const std::string& msg);
+int clear_error();
+int cuda_error(cudaError_t e, const char* what);
+
+#define BGPU_CUDA(expr)                                    \
+  do {                                                     \
+    cudaError_t _e = (expr);                               \
+    if (_e != cudaSuccess) return ::bgpu::cuda_error(_e, #expr); \
+  } while (0)
+
+#define BGPU_LAUNCH_CHECK(what)                            \
+  do {                                                     \
+    cudaError_t _e = cudaGetLastError();                   \
+    if (_e != cudaSuccess) return ::bgpu::cuda_error(_e, what); \
+  } while (0)
+
+#define BGPU_ARG(cond, msg)                                \
+  do {                                                     \
+    if (!(cond)) return ::bgpu::set_error(BINIUS_E_ARG, msg); \
+  } while (0)
+
+// Cumulative number of kernels this library has launched (all devices, all threads).
+void count_launch(uint64_t n = 1);
+
+static inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Host GF(2^128) arithmetic (portable carry-less multiply); used only for domain set-up, which
+// the reference also performs on the host (Prover::setup, prover/prover/src/prove.rs:95-121).
+typedef unsigned __int128 hu128;
+hu128 host_gf_mul(hu128 a, hu128 b);
+hu128 host_gf_inv(hu128 a);
+
+}  // namespace bgpu
+
+struct binius_ntt {
+  int device;
+  uint32_t log_domain;
+  void* d_twiddles;  // (2^log_domain - 1) elements of 16 bytes
+};

@@ -1,0 +1,231 @@
+// Binary Merkle tree commit with SHA-256 leaves and the Binius SHA-256 node compression.
+//
+// Layout follows BinaryMerkleTree::inner_nodes (prover/prover/src/merkle_tree/binary_merkle_tree.rs
+// :65-122): 2^(L+1) - 1 digests of 32 bytes, the 2^L leaf digests first, then each layer, the root
+// last; node i of layer k+1 compresses nodes 2i and 2i+1 of layer k (parallel_compression.rs:79-91).
+//
+// B200 mapping: one thread hashes one leaf (its 2^log_batch elements are read as 128-bit loads);
+// the CTA's 256 leaf digests stay in shared memory and the next 8 tree layers are compressed there
+// before anything but the layer outputs touches HBM.  Upper layers run in CTAs that fuse 9 layers
+// (512 inputs -> 1).  SHA-256 is pure integer work (funnel-shift rotates, LOP3, IADD3).
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "internal.h"
+#include "sha256.cuh"
+
+using namespace bgpu;
+
+namespace {
+
+constexpr uint32_t kLeafFuse = 8;  // leaves per CTA = 2^8
+constexpr uint32_t kNodeFuse = 9;  // inputs per CTA = 2^9
+
+__host__ __device__ __forceinline__ uint64_t layer_offset(uint32_t L, uint32_t k) {
+  return (1ull << (L + 1)) - (1ull << (L + 1 - k));
+}
+
+__device__ __forceinline__ void store_digest(uint4* nodes, uint64_t i, const uint32_t d[8]) {
+  nodes[2 * i] = make_uint4(d[0], d[1], d[2], d[3]);
+  nodes[2 * i + 1] = make_uint4(d[4], d[5], d[6], d[7]);
+}
+
+__device__ __forceinline__ void load_digest(const uint4* nodes, uint64_t i, uint32_t d[8]) {
+  uint4 a = nodes[2 * i], b = nodes[2 * i + 1];
+  d[0] = a.x; d[1] = a.y; d[2] = a.z; d[3] = a.w;
+  d[4] = b.x; d[5] = b.y; d[6] = b.z; d[7] = b.w;
+}
+
+// Hashes 2^fused leaves per CTA and compresses `fused` layers above them in shared memory.
+__global__ void __launch_bounds__(256) merkle_leaves_kernel(const uint4* __restrict__ elems,
+                                                            uint32_t log_batch,
+                                                            uint4* __restrict__ nodes, uint32_t L,
+                                                            uint32_t fused, NodeIV iv) {
+  __shared__ uint32_t buf[2][256][9];  // padded rows avoid bank conflicts
+  const uint32_t tid = threadIdx.x;
+  const uint64_t leaf = (uint64_t)blockIdx.x * blockDim.x + tid;
+  uint32_t d[8];
+  sha256_elems(elems + (leaf << log_batch), 1u << log_batch, d);
+  store_digest(nodes, leaf, d);
+#pragma unroll
+  for (int i = 0; i < 8; i++) buf[0][tid][i] = d[i];
+  for (uint32_t lvl = 1; lvl <= fused; lvl++) {
+    __syncthreads();
+    const uint32_t n = blockDim.x >> lvl;
+    if (tid < n) {
+      const uint32_t src = (lvl - 1) & 1, dst = lvl & 1;
+      uint32_t l[8], r[8], o[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        l[i] = buf[src][2 * tid][i];
+        r[i] = buf[src][2 * tid + 1][i];
+      }
+      compress_node(iv, l, r, o);
+#pragma unroll
+      for (int i = 0; i < 8; i++) buf[dst][tid][i] = o[i];
+      store_digest(nodes, layer_offset(L, lvl) + (uint64_t)blockIdx.x * n + tid, o);
+    }
+  }
+}
+
+// Compresses `fused` layers starting from layer in_level; each CTA reduces 2^fused inputs.
+__global__ void __launch_bounds__(256) merkle_nodes_kernel(uint4* __restrict__ nodes, uint32_t L,
+                                                           uint32_t in_level, uint32_t fused,
+                                                           NodeIV iv) {
+  __shared__ uint32_t buf[2][256][9];
+  const uint32_t tid = threadIdx.x;
+  const uint64_t in_off = layer_offset(L, in_level);
+  uint32_t l[8], r[8], o[8];
+  {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + tid;
+    load_digest(nodes, in_off + 2 * i, l);
+    load_digest(nodes, in_off + 2 * i + 1, r);
+    compress_node(iv, l, r, o);
+    store_digest(nodes, layer_offset(L, in_level + 1) + i, o);
+#pragma unroll
+    for (int k = 0; k < 8; k++) buf[1][tid][k] = o[k];
+  }
+  for (uint32_t lvl = 2; lvl <= fused; lvl++) {
+    __syncthreads();
+    const uint32_t n = (blockDim.x * 2) >> lvl;
+    if (tid < n) {
+      const uint32_t src = (lvl - 1) & 1, dst = lvl & 1;
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        l[k] = buf[src][2 * tid][k];
+        r[k] = buf[src][2 * tid + 1][k];
+      }
+      compress_node(iv, l, r, o);
+#pragma unroll
+      for (int k = 0; k < 8; k++) buf[dst][tid][k] = o[k];
+      store_digest(nodes, layer_offset(L, in_level + lvl) + (uint64_t)blockIdx.x * n + tid, o);
+    }
+  }
+}
+
+// FIPS 180-4 SHA-256 on the host, used once to derive the node-compression IV.
+void host_sha256(const uint8_t* data, size_t len, uint8_t out[32]) {
+  static const uint32_t K[64] = {
+      0x428a2f98, 0x71374491, 0xb5c0fbcf, 0xe9b5dba5, 0x3956c25b, 0x59f111f1, 0x923f82a4,
+      0xab1c5ed5, 0xd807aa98, 0x12835b01, 0x243185be, 0x550c7dc3, 0x72be5d74, 0x80deb1fe,
+      0x9bdc06a7, 0xc19bf174, 0xe49b69c1, 0xefbe4786, 0x0fc19dc6, 0x240ca1cc, 0x2de92c6f,
+      0x4a7484aa, 0x5cb0a9dc, 0x76f988da, 0x983e5152, 0xa831c66d, 0xb00327c8, 0xbf597fc7,
+      0xc6e00bf3, 0xd5a79147, 0x06ca6351, 0x14292967, 0x27b70a85, 0x2e1b2138, 0x4d2c6dfc,
+      0x53380d13, 0x650a7354, 0x766a0abb, 0x81c2c92e, 0x92722c85, 0xa2bfe8a1, 0xa81a664b,
+      0xc24b8b70, 0xc76c51a3, 0xd192e819, 0xd6990624, 0xf40e3585, 0x106aa070, 0x19a4c116,
+      0x1e376c08, 0x2748774c, 0x34b0bcb5, 0x391c0cb3, 0x4ed8aa4a, 0x5b9cca4f, 0x682e6ff3,
+      0x748f82ee, 0x78a5636f, 0x84c87814, 0x8cc70208, 0x90befffa, 0xa4506ceb, 0xbef9a3f7,
+      0xc67178f2};
+  uint32_t s[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
+                   0x510e527f, 0x9b05688c, 0x1f83d9ab, 0x5be0cd19};
+  auto rotr = [](uint32_t x, int n) { return (x >> n) | (x << (32 - n)); };
+  auto compress = [&](const uint8_t* blk) {
+    uint32_t w[64];
+    for (int t = 0; t < 16; t++)
+      w[t] = ((uint32_t)blk[4 * t] << 24) | ((uint32_t)blk[4 * t + 1] << 16) |
+             ((uint32_t)blk[4 * t + 2] << 8) | blk[4 * t + 3];
+    for (int t = 16; t < 64; t++)
+      w[t] = w[t - 16] + (rotr(w[t - 15], 7) ^ rotr(w[t - 15], 18) ^ (w[t - 15] >> 3)) +
+             w[t - 7] + (rotr(w[t - 2], 17) ^ rotr(w[t - 2], 19) ^ (w[t - 2] >> 10));
+    uint32_t a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5], g = s[6], h = s[7];
+    for (int t = 0; t < 64; t++) {
+      uint32_t t1 = h + (rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25)) + ((e & f) ^ (~e & g)) + K[t] + w[t];
+      uint32_t t2 = (rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
+      h = g; g = f; f = e; e = d + t1; d = c; c = b; b = a; a = t1 + t2;
+    }
+    s[0] += a; s[1] += b; s[2] += c; s[3] += d; s[4] += e; s[5] += f; s[6] += g; s[7] += h;
+  };
+  size_t full = len / 64;
+  for (size_t i = 0; i < full; i++) compress(data + 64 * i);
+  uint8_t tail[128] = {0};
+  size_t rem = len - 64 * full;
+  memcpy(tail, data + 64 * full, rem);
+  tail[rem] = 0x80;
+  size_t tl = rem + 9 <= 64 ? 64 : 128;
+  uint64_t bits = (uint64_t)len * 8;
+  for (int i = 0; i < 8; i++) tail[tl - 1 - i] = (uint8_t)(bits >> (8 * i));
+  compress(tail);
+  if (tl == 128) compress(tail + 64);
+  for (int i = 0; i < 8; i++) {
+    out[4 * i] = (uint8_t)(s[i] >> 24);
+    out[4 * i + 1] = (uint8_t)(s[i] >> 16);
+    out[4 * i + 2] = (uint8_t)(s[i] >> 8);
+    out[4 * i + 3] = (uint8_t)s[i];
+  }
+}
+
+}  // namespace
+
+namespace bgpu {
+
+// Sha256Compression::default (hash/compress.rs:37-44): the digest bytes of
+// "BINIUS SHA-256 COMPRESS" reinterpreted as native little-endian u32 words.
+NodeIV node_iv() {
+  static NodeIV iv;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    const char* tag = "BINIUS SHA-256 COMPRESS";
+    uint8_t d[32];
+    host_sha256(reinterpret_cast<const uint8_t*>(tag), strlen(tag), d);
+    for (int i = 0; i < 8; i++)
+      iv.w[i] = (uint32_t)d[4 * i] | ((uint32_t)d[4 * i + 1] << 8) |
+                ((uint32_t)d[4 * i + 2] << 16) | ((uint32_t)d[4 * i + 3] << 24);
+  });
+  return iv;
+}
+
+int merkle_commit(const void* d_elems, uint32_t log_leaves, uint32_t log_batch, void* d_nodes,
+                  cudaStream_t stream) {
+  BGPU_ARG(d_elems != nullptr && d_nodes != nullptr, "elems / nodes is NULL");
+  BGPU_ARG(log_leaves <= 34, "too many leaves");
+  BGPU_ARG(log_batch <= 20, "leaf too large");
+  const uint32_t L = log_leaves;
+  const NodeIV iv = node_iv();
+  uint4* nodes = static_cast<uint4*>(d_nodes);
+  uint32_t fused = std::min(L, kLeafFuse);
+  uint64_t grid = 1ull << (L - fused);
+  BGPU_ARG(grid <= 0x7fffffffull, "too many leaves");
+  merkle_leaves_kernel<<<(unsigned)grid, 1u << fused, 0, stream>>>(
+      static_cast<const uint4*>(d_elems), log_batch, nodes, L, fused, iv);
+  BGPU_LAUNCH_CHECK("merkle_leaves_kernel");
+  count_launch();
+  uint32_t level = fused;
+  while (level < L) {
+    uint32_t f = std::min(L - level, kNodeFuse);
+    uint64_t g = 1ull << (L - level - f);
+    merkle_nodes_kernel<<<(unsigned)g, 1u << (f - 1), 0, stream>>>(nodes, L, level, f, iv);
+    BGPU_LAUNCH_CHECK("merkle_nodes_kernel");
+    count_launch();
+    level += f;
+  }
+  return clear_error();
+}
+
+}  // namespace bgpu
+
+extern "C" {
+
+int binius_merkle_commit(const void* d_elems, uint32_t log_leaves, uint32_t log_batch,
+                         void* d_nodes, void* stream) {
+  return bgpu::merkle_commit(d_elems, log_leaves, log_batch, d_nodes, as_stream(stream));
+}
+
+int binius_merkle_branch(const void* d_nodes, uint32_t log_leaves, uint64_t index,
+                         uint32_t layer_depth, void* h_branch, void* stream) {
+  BGPU_ARG(d_nodes != nullptr && h_branch != nullptr, "nodes / branch is NULL");
+  BGPU_ARG(log_leaves <= 40, "log_leaves too large");
+  BGPU_ARG(index < (1ull << log_leaves) && layer_depth <= log_leaves, "index out of range");
+  cudaStream_t s = as_stream(stream);
+  const uint8_t* nodes = static_cast<const uint8_t*>(d_nodes);
+  uint8_t* out = static_cast<uint8_t*>(h_branch);
+  for (uint32_t j = 0; j < log_leaves - layer_depth; j++) {
+    uint64_t node = layer_offset(log_leaves, j) | ((index >> j) ^ 1);
+    BGPU_CUDA(cudaMemcpyAsync(out + 32 * j, nodes + 32 * node, 32, cudaMemcpyDeviceToHost, s));
+  }
+  BGPU_CUDA(cudaStreamSynchronize(s));
+  return clear_error();
+}
+
+}  // extern "C"

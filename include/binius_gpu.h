@@ -1,0 +1,137 @@
+/*
+ * binius_gpu.h -- C ABI of the B200 (sm_100a) Binius64 prover hot path.
+ *
+ * Every entry point returns a binius_status; on failure binius_last_error() gives a message
+ * (thread-local).  Field elements are BinaryField128bGhash values in their 16-byte little-endian
+ * u128 encoding (verifier/field/src/ghash.rs:486-498); digests are 32 raw bytes.  Pointers named
+ * d_* are device pointers on the current CUDA device; h_* are host pointers.  `stream` is a
+ * cudaStream_t (NULL = legacy default stream).  Device entry points are asynchronous on `stream`
+ * unless stated otherwise.  No entry point throws or aborts; argument errors map to BINIUS_E_ARG,
+ * mirroring binius_prover::Error::ArgumentError (prover/prover/src/error.rs:9-24).
+ */
+#ifndef BINIUS_GPU_H
+#define BINIUS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum binius_status {
+  BINIUS_OK = 0,
+  BINIUS_E_ARG = 1,     /* invalid argument / precondition (ArgumentError, assert! in the reference) */
+  BINIUS_E_OOM = 2,     /* device allocation refused */
+  BINIUS_E_CUDA = 3,    /* CUDA runtime error */
+  BINIUS_E_TIMEOUT = 4, /* a bounded device-side wait expired */
+  BINIUS_E_UNSUPPORTED = 5
+} binius_status;
+
+/* Last error message of the calling thread ("" if none). */
+const char* binius_last_error(void);
+/* Library version string. */
+const char* binius_version(void);
+/* Cumulative number of CUDA kernels launched by this library in this process (no reference
+ * counterpart: launch accounting for benchmarks and tests). */
+uint64_t binius_launch_count(void);
+
+/* ------------------------------------------------------------------------------------------
+ * AdditiveNTT over a GenericPreExpanded domain context.
+ * Replaces: trait AdditiveNTT (verifier/math/src/ntt/mod.rs:58-113), DomainContext
+ * (ntt/mod.rs:118-179), GenericPreExpanded::generate_from_subspace
+ * (ntt/domain_context.rs:114-133), NeighborsLastMultiThread::forward_transform
+ * (ntt/neighbors_last.rs:461-520).
+ * ------------------------------------------------------------------------------------------ */
+typedef struct binius_ntt binius_ntt;
+
+/* Builds the twiddle table (2^log_domain - 1 elements, layer l at offset 2^l - 1) on `device`.
+ * h_basis: log_domain field elements, or NULL for BinarySubspace::with_dim (basis x^i). */
+int binius_ntt_create(int device, const void* h_basis, uint32_t log_domain, binius_ntt** out);
+int binius_ntt_destroy(binius_ntt* ntt);
+/* log2 of the domain size (DomainContext::log_domain_size). */
+uint32_t binius_ntt_log_domain(const binius_ntt* ntt);
+/* Device pointer of the flat twiddle table (DomainContext::twiddle(layer, block) is entry
+ * 2^layer - 1 + block). */
+const void* binius_ntt_twiddles(const binius_ntt* ntt);
+
+/* In-place forward / inverse transform of 2^log_len elements, layers
+ * [skip_early, log_len - skip_late) (AdditiveNTT::forward_transform / inverse_transform;
+ * preconditions of ntt/reference.rs:85-100). */
+int binius_ntt_forward(const binius_ntt* ntt, void* d_data, uint32_t log_len, uint32_t skip_early,
+                       uint32_t skip_late, void* stream);
+int binius_ntt_inverse(const binius_ntt* ntt, void* d_data, uint32_t log_len, uint32_t skip_early,
+                       uint32_t skip_late, void* stream);
+
+/* ------------------------------------------------------------------------------------------
+ * Reed-Solomon encode.
+ * Replaces: ReedSolomonCode::encode_batch (verifier/math/src/reed_solomon.rs:128-201).
+ * d_msg: 2^(log_dim + log_batch) elements; d_codeword: 2^(log_dim + log_inv_rate + log_batch)
+ * elements (must not alias d_msg).  The code's subspace is the NTT domain's first
+ * log_dim + log_inv_rate basis elements.
+ * ------------------------------------------------------------------------------------------ */
+int binius_rs_encode_batch(const binius_ntt* ntt, const void* d_msg, uint32_t log_dim,
+                           uint32_t log_inv_rate, uint32_t log_batch, void* d_codeword,
+                           void* stream);
+
+/* ------------------------------------------------------------------------------------------
+ * Binary Merkle tree with SHA-256 leaves and the Binius SHA-256 node compression.
+ * Replaces: BinaryMerkleTreeProver::commit / commit_iterated
+ * (prover/prover/src/merkle_tree/prover.rs:93-118), binary_merkle_tree::build_from_iterator
+ * (prover/prover/src/merkle_tree/binary_merkle_tree.rs:65-122), ParallelDigest for Sha256
+ * (prover/prover/src/hash/parallel_digest.rs:145-173), Sha256Compression
+ * (verifier/verifier/src/hash/compress.rs:32-57).
+ * d_elems: 2^(log_leaves + log_batch) elements, leaf i = elements [i*2^log_batch, (i+1)*2^log_batch).
+ * d_nodes: (2^(log_leaves+1) - 1) * 32 bytes, layers flat with the leaf digests first and the root
+ * last (BinaryMerkleTree::inner_nodes).
+ * ------------------------------------------------------------------------------------------ */
+int binius_merkle_commit(const void* d_elems, uint32_t log_leaves, uint32_t log_batch,
+                         void* d_nodes, void* stream);
+/* Copies the Merkle branch of leaf `index` down to layer `layer_depth` (BinaryMerkleTree::branch,
+ * binary_merkle_tree.rs:148-169) into h_branch ((log_leaves - layer_depth) * 32 bytes).
+ * Synchronous. */
+int binius_merkle_branch(const void* d_nodes, uint32_t log_leaves, uint64_t index,
+                         uint32_t layer_depth, void* h_branch, void* stream);
+
+/* ------------------------------------------------------------------------------------------
+ * FRI folding.
+ * binius_fri_fold_interleaved replaces fold_interleaved (prover/prover/src/fri/fold.rs:260-282):
+ *   d_out[i] = <d_codeword[i*2^log_batch ..], eq_ind(h_challenges)>, 2^log_len outputs,
+ *   log_batch <= 8 challenges.
+ * binius_fri_fold_codeword replaces fold_codeword (prover/prover/src/fri/fold.rs:297-318) with
+ *   fold_chunk / fold_pair (verifier/verifier/src/fri/fold.rs:20-99): 2^(log_len - n) outputs,
+ *   n <= 8 challenges; the NTT supplies twiddle(log_len - 1 - k, .) for round k.
+ * h_challenges are host arrays of 16-byte field elements.
+ * ------------------------------------------------------------------------------------------ */
+int binius_fri_fold_interleaved(const void* d_codeword, uint32_t log_len, uint32_t log_batch,
+                                const void* h_challenges, void* d_out, void* stream);
+int binius_fri_fold_codeword(const binius_ntt* ntt, const void* d_codeword, uint32_t log_len,
+                             const void* h_challenges, uint32_t n_challenges, void* d_out,
+                             void* stream);
+
+/* ------------------------------------------------------------------------------------------
+ * FRI commit of an interleaved message: RS encode then Merkle commit with leaves of
+ * 2^log_batch consecutive codeword symbols.
+ * Replaces: fri::commit_interleaved (prover/prover/src/fri/commit.rs:25-75).
+ * Writes the codeword (d_codeword) and tree (d_nodes); if h_root is not NULL the call
+ * synchronizes `stream` and copies the 32-byte root there (CommitOutput::commitment).
+ * ------------------------------------------------------------------------------------------ */
+int binius_fri_commit_interleaved(const binius_ntt* ntt, const void* d_msg, uint32_t log_dim,
+                                  uint32_t log_inv_rate, uint32_t log_batch, void* d_codeword,
+                                  void* d_nodes, void* h_root, void* stream);
+
+/* ------------------------------------------------------------------------------------------
+ * FRI parameters (verifier/verifier/src/fri/common.rs:64-219).
+ * ------------------------------------------------------------------------------------------ */
+uint32_t binius_fri_n_test_queries(uint32_t security_bits, uint32_t log_inv_rate);
+uint32_t binius_fri_estimate_optimal_arity(uint32_t log_block_length, uint32_t digest_size,
+                                           uint32_t field_size);
+
+/* Elementwise GF(2^128) products d_out[i] = d_a[i] * d_b[i] (kernel-level check of the field
+ * multiplier; BinaryField128bGhash::mul, verifier/field/src/ghash.rs:188-194). */
+int binius_gf_mul_batch(const void* d_a, const void* d_b, void* d_out, uint64_t n, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BINIUS_GPU_H */

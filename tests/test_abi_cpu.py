@@ -1,0 +1,77 @@
+"""CPU-only checks of the C ABI: the library loads, exports every declared symbol, and the host-only
+entry points (FRI parameters, argument validation) behave like the reference without a GPU."""
+import ctypes
+
+import pytest
+
+import oracle as orc
+from binius64_b200 import _ffi
+
+
+def test_library_loads_and_exports_all_declared_symbols():
+    L = _ffi.lib()
+    declared = _ffi.declared_functions()
+    assert len(declared) >= 15
+    missing = [n for n in declared if not hasattr(L, n)]
+    assert not missing, f"declared but not exported: {missing}"
+    # every declared function has a ctypes signature in the binding
+    assert set(declared) <= set(_ffi._SIGS), set(declared) - set(_ffi._SIGS)
+
+
+def test_version():
+    assert b"sm_100a" in _ffi.lib().binius_version()
+
+
+@pytest.mark.parametrize("bits,rate", [(96, 1), (96, 2), (128, 1), (64, 3)])
+def test_n_test_queries_matches_oracle(bits, rate):
+    assert _ffi.lib().binius_fri_n_test_queries(bits, rate) == orc.calculate_n_test_queries(bits, rate)
+
+
+def test_fri_param_kats_through_abi():
+    L = _ffi.lib()
+    assert L.binius_fri_n_test_queries(96, 1) == 232
+    assert L.binius_fri_n_test_queries(96, 2) == 142
+    for n in range(22, 35):
+        assert L.binius_fri_estimate_optimal_arity(n, 256, 128) == 4
+    for n in range(22, 28):
+        assert L.binius_fri_estimate_optimal_arity(n, 1024, 128) == 6
+    for n in range(1, 30):
+        assert L.binius_fri_estimate_optimal_arity(n, 32, 16) == orc.estimate_optimal_arity(n, 32, 16)
+
+
+def test_argument_errors_without_gpu():
+    L = _ffi.lib()
+    # NULL handles and impossible shapes are rejected before any CUDA call.
+    assert L.binius_rs_encode_batch(None, None, 4, 1, 0, None, None) == _ffi.BINIUS_E_ARG
+    assert b"NULL" in L.binius_last_error()
+    assert L.binius_ntt_forward(None, None, 4, 0, 0, None) == _ffi.BINIUS_E_ARG
+    assert L.binius_merkle_commit(None, 3, 0, None, None) == _ffi.BINIUS_E_ARG
+    assert L.binius_fri_fold_interleaved(None, 3, 2, None, None, None) == _ffi.BINIUS_E_ARG
+    out = ctypes.c_void_p()
+    assert L.binius_ntt_create(0, None, 0, ctypes.byref(out)) == _ffi.BINIUS_E_ARG
+    assert L.binius_ntt_create(0, None, 33, ctypes.byref(out)) == _ffi.BINIUS_E_ARG
+    assert out.value is None
+    # too many folding challenges for one call
+    assert L.binius_fri_fold_interleaved(ctypes.c_void_p(16), 3, 9, ctypes.c_void_p(16),
+                                         ctypes.c_void_p(16), None) == _ffi.BINIUS_E_ARG
+
+
+def test_check_maps_argument_error():
+    L = _ffi.lib()
+    rc = L.binius_merkle_commit(None, 3, 0, None, None)
+    with pytest.raises(_ffi.ArgumentError):
+        _ffi.check(rc)
+
+
+def test_fri_params_choice_matches_reference_formula():
+    import binius64_b200 as bg
+    # C3: 2^19 B128 witness elements, R = 1 -> log_code_len 20, arity 4 (estimate_optimal_arity with
+    # 32-byte digests and 16-byte elements), batch 2^4, RS dim 2^15, arities [4, 4], 232 queries.
+    arity = bg.estimate_optimal_arity(20, 32, 16)
+    assert arity == 4
+    p = bg.FRIParams.choose_with_constant_fold_arity(19, 96, 1, arity)
+    assert p.log_batch_size == 4
+    assert p.rs_code.log_dim == 15
+    assert p.fold_arities == [4, 4]
+    assert p.n_test_queries == 232
+    assert p.log_terminal_dim == 7
