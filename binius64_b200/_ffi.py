@@ -57,6 +57,7 @@ _SIGS = {
     "binius_merkle_branch": (_int, [_vp, _u32, _u64, _u32, _vp, _vp]),
     "binius_fri_fold_interleaved": (_int, [_vp, _u32, _u32, _vp, _vp, _vp]),
     "binius_fri_fold_codeword": (_int, [_vp, _vp, _u32, _vp, _u32, _vp, _vp]),
+    "binius_fri_fold_codeword_noalloc": (_int, [_vp, _vp, _u32, _vp, _u32, _vp, _vp]),
     "binius_fri_commit_interleaved": (_int, [_vp, _vp, _u32, _u32, _u32, _vp, _vp, _vp, _vp]),
     "binius_fri_n_test_queries": (_u32, [_u32, _u32]),
     "binius_fri_estimate_optimal_arity": (_u32, [_u32, _u32, _u32]),

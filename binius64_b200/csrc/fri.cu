@@ -10,6 +10,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "gf128.cuh"
 #include "internal.h"
@@ -118,6 +119,37 @@ void launch_fold_codeword(const uint4* cw, uint32_t log_len, const uint4* tw, co
   fold_codeword_kernel<N><<<grid_for(n_chunks, 256), 256, 0, s>>>(cw, log_len, tw, ch, out);
 }
 
+// ---- Scratch for binius_fri_fold_codeword_noalloc ----
+// A fold over more than 4 challenges passes the codeword after its first 4 rounds through an
+// intermediate buffer.  The allocation-free entry point keeps that buffer in this file-scope device
+// array instead of allocating: 2^18 elements = 4 MiB, reserved on every GPU that loads this
+// library until the process exits.
+constexpr uint64_t kNoAllocScratchElems = 1ull << 18;
+static __device__ __align__(256) uint4 g_fold_scratch[kNoAllocScratchElems];
+
+constexpr int kMaxDevices = 64;
+struct ScratchSlot {
+  std::once_flag once;
+  void* ptr = nullptr;
+  cudaError_t err = cudaSuccess;
+};
+static ScratchSlot g_scratch_slots[kMaxDevices];
+
+// Device address of g_fold_scratch on the current device.  Host code cannot use the symbol's name
+// as a device pointer, so the address is looked up once per device (the device being current).
+int noalloc_scratch(void** out) {
+  int dev = -1;
+  BGPU_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return set_error(BINIUS_E_ARG, "device ordinal out of range");
+  ScratchSlot& slot = g_scratch_slots[dev];
+  std::call_once(slot.once, [&slot] {
+    slot.err = cudaGetSymbolAddress(&slot.ptr, g_fold_scratch);
+  });
+  if (slot.err != cudaSuccess) return cuda_error(slot.err, "cudaGetSymbolAddress(g_fold_scratch)");
+  *out = slot.ptr;
+  return BINIUS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -186,6 +218,65 @@ int binius_fri_fold_codeword(const binius_ntt* ntt, const void* d_codeword, uint
     done += step;
   }
   if (tmp) BGPU_CUDA(cudaFreeAsync(tmp, s));
+  return clear_error();
+}
+
+// Same result as binius_fri_fold_codeword, for callers that may not allocate device memory.  For
+// n_challenges > 4 the intermediate codeword lives in g_fold_scratch (at most 2^18 elements, so
+// log_len - 4 <= 18); larger folds are rejected with BINIUS_E_ARG.  The first call on a device looks
+// up the scratch address (cudaGetSymbolAddress); make that first call before any stream capture.
+// Every call on a device shares the one scratch array: calls whose kernels overlap on the GPU (for
+// example on two streams) race on it.  No cudaMalloc, cudaFree or other allocating call is made.
+int binius_fri_fold_codeword_noalloc(const binius_ntt* ntt, const void* d_codeword,
+                                     uint32_t log_len, const void* h_challenges,
+                                     uint32_t n_challenges, void* d_out, void* stream) {
+  BGPU_ARG(ntt != nullptr, "ntt is NULL");
+  BGPU_ARG(d_codeword != nullptr && d_out != nullptr, "codeword / out is NULL");
+  BGPU_ARG(n_challenges <= log_len, "more challenges than codeword variables");
+  BGPU_ARG(log_len <= ntt->log_domain, "codeword longer than the NTT domain");
+  Challenges ch;
+  if (int rc = load_challenges(h_challenges, n_challenges, ch)) return rc;
+  uint4* scratch = nullptr;
+  if (n_challenges > 4) {
+    if (log_len - 4 > 18)
+      return set_error(BINIUS_E_ARG,
+                       "binius_fri_fold_codeword_noalloc: a fold of more than 4 challenges needs "
+                       "2^(log_len-4) scratch elements and the static scratch holds 2^18 (4 MiB); "
+                       "use binius_fri_fold_codeword for log_len > 22");
+    void* p = nullptr;
+    if (int rc = noalloc_scratch(&p)) return rc;
+    scratch = static_cast<uint4*>(p);
+  }
+  cudaStream_t s = as_stream(stream);
+  const uint4* cw = static_cast<const uint4*>(d_codeword);
+  const uint4* tw = static_cast<const uint4*>(ntt->d_twiddles);
+  uint4* out = static_cast<uint4*>(d_out);
+  if (n_challenges == 0) {
+    BGPU_CUDA(cudaMemcpyAsync(d_out, d_codeword, 16ull << log_len, cudaMemcpyDeviceToDevice, s));
+    return clear_error();
+  }
+  uint32_t done = 0, cur_len = log_len;
+  const uint4* src = cw;
+  while (done < n_challenges) {
+    uint32_t step = std::min<uint32_t>(4, n_challenges - done);
+    Challenges sub;
+    memset(&sub, 0, sizeof(sub));
+    for (uint32_t i = 0; i < step; i++) sub.r[i] = ch.r[done + i];
+    // n <= 8: codeword -> scratch -> out.  The scratch is fully written by the first step before
+    // the second reads it (same stream), so it needs no clearing.
+    uint4* dst = (done + step == n_challenges) ? out : scratch;
+    switch (step) {
+      case 1: launch_fold_codeword<1>(src, cur_len, tw, sub, dst, s); break;
+      case 2: launch_fold_codeword<2>(src, cur_len, tw, sub, dst, s); break;
+      case 3: launch_fold_codeword<3>(src, cur_len, tw, sub, dst, s); break;
+      default: launch_fold_codeword<4>(src, cur_len, tw, sub, dst, s); break;
+    }
+    BGPU_LAUNCH_CHECK("fold_codeword_kernel");
+    count_launch();
+    src = dst;
+    cur_len -= step;
+    done += step;
+  }
   return clear_error();
 }
 

@@ -109,6 +109,19 @@ int binius_fri_fold_codeword(const binius_ntt* ntt, const void* d_codeword, uint
                              const void* h_challenges, uint32_t n_challenges, void* d_out,
                              void* stream);
 
+/* Allocation-free form of binius_fri_fold_codeword, with no counterpart in the reference.  For
+ * callers that may not allocate device memory themselves or let a library do it behind them: a
+ * serving loop that admits requests by the free HBM it has budgeted, or a host that owns all device
+ * memory in its own arena.  Same arguments and bit-identical output.  A fold over more than 4
+ * challenges stages the codeword through a static 4 MiB device array (2^18 elements), so it accepts
+ * log_len <= 22 in that case and returns BINIUS_E_ARG beyond; that array is reserved on every GPU
+ * that loads the library until exit.  The first call on a device looks up the array's address; make
+ * it before any stream capture.  All calls on a device share the array, so calls that overlap on
+ * the GPU race.  Makes no cudaMalloc/cudaFree or other allocating call. */
+int binius_fri_fold_codeword_noalloc(const binius_ntt* ntt, const void* d_codeword,
+                                     uint32_t log_len, const void* h_challenges,
+                                     uint32_t n_challenges, void* d_out, void* stream);
+
 /* ------------------------------------------------------------------------------------------
  * FRI commit of an interleaved message: RS encode then Merkle commit with leaves of
  * 2^log_batch consecutive codeword symbols.
