@@ -71,6 +71,21 @@ def lib():
         L.orc_estimate_optimal_arity.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
         L.orc_estimate_optimal_arity.restype = ctypes.c_uint32
         L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_transcript_new.restype = ctypes.c_void_p
+        L.orc_transcript_free.argtypes = [ctypes.c_void_p]
+        L.orc_transcript_observe.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_size_t]
+        L.orc_transcript_sample.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_size_t]
+        L.orc_eval_1b_mle.argtypes = [_u64p, ctypes.c_uint32, _u64p, _u64p]
+        _u32p = ctypes.POINTER(ctypes.c_uint32)
+        L.orc_pcs_prove.argtypes = [_u64p, _u64p, ctypes.c_uint32, ctypes.c_uint32,
+                                    ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32,
+                                    _u64p, _u8p, ctypes.c_size_t,
+                                    ctypes.POINTER(ctypes.c_size_t)]
+        L.orc_pcs_prove.restype = ctypes.c_int
+        L.orc_pcs_verify.argtypes = [_u64p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                     _u32p, ctypes.c_uint32, ctypes.c_uint32, _u64p, _u64p, _u8p,
+                                     ctypes.c_size_t]
+        L.orc_pcs_verify.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -249,3 +264,62 @@ def estimate_optimal_arity(log_block_length: int, digest_size: int, field_size: 
 
 def random_elems(rng: np.random.Generator, n: int) -> np.ndarray:
     return rng.integers(0, np.iinfo(np.uint64).max, size=(n, 2), dtype=np.uint64, endpoint=True)
+
+
+class Transcript:
+    """HasherChallenger<Sha256> state machine (observe / sample only)."""
+
+    def __init__(self):
+        self._h = lib().orc_transcript_new()
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_transcript_free(self._h)
+            self._h = None
+
+    def observe(self, data: bytes) -> None:
+        buf = np.frombuffer(data, dtype=np.uint8).copy() if data else np.zeros(1, dtype=np.uint8)
+        lib().orc_transcript_observe(self._h, _p8(buf), len(data))
+
+    def sample(self, n: int) -> bytes:
+        out = np.zeros(max(n, 1), dtype=np.uint8)
+        lib().orc_transcript_sample(self._h, _p8(out), n)
+        return out.tobytes()[:n]
+
+
+def eval_1b_mle(witness: np.ndarray, point: np.ndarray) -> np.ndarray:
+    w = np.ascontiguousarray(witness, dtype=np.uint64)
+    pt = np.ascontiguousarray(point, dtype=np.uint64)
+    out = elems(1)
+    lib().orc_eval_1b_mle(_p64(w), w.shape[0].bit_length() - 1, _p64(pt), _p64(out))
+    return out[0]
+
+
+def _u32arr(vals):
+    a = np.array(list(vals) or [0], dtype=np.uint32)
+    return a, a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+
+
+def pcs_prove(twiddles, witness, log_batch, log_inv_rate, arities, n_queries, eval_point) -> bytes:
+    w = np.ascontiguousarray(witness, dtype=np.uint64)
+    log_msg = w.shape[0].bit_length() - 1
+    pt = np.ascontiguousarray(eval_point, dtype=np.uint64)
+    ar, arp = _u32arr(arities)
+    cap = 1 << 26
+    out = np.zeros(cap, dtype=np.uint8)
+    n = ctypes.c_size_t(0)
+    rc = lib().orc_pcs_prove(_p64(twiddles), _p64(w), log_msg, log_batch, log_inv_rate, arp,
+                             len(arities), n_queries, _p64(pt), _p8(out), cap, ctypes.byref(n))
+    assert rc == 0, "proof buffer too small"
+    return out[: n.value].tobytes()
+
+
+def pcs_verify(twiddles, log_msg, log_batch, log_inv_rate, arities, n_queries, eval_point, claim,
+               proof: bytes) -> int:
+    pt = np.ascontiguousarray(eval_point, dtype=np.uint64)
+    ar, arp = _u32arr(arities)
+    cl = np.ascontiguousarray(claim, dtype=np.uint64).reshape(2)
+    pr = np.frombuffer(proof, dtype=np.uint8).copy()
+    return int(lib().orc_pcs_verify(_p64(twiddles), log_msg, log_batch, log_inv_rate, arp,
+                                    len(arities), n_queries, _p64(pt), _p64(cl), _p8(pr),
+                                    len(proof)))

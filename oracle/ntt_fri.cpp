@@ -46,7 +46,7 @@ static void expand_twiddles(const std::vector<std::vector<u128>>& evals, u128* o
   }
 }
 
-static inline u128 twiddle(const u128* tw, uint32_t layer, size_t block) {
+u128 twiddle(const u128* tw, uint32_t layer, size_t block) {
   return tw[((size_t)1 << layer) - 1 + block];
 }
 
@@ -101,7 +101,7 @@ void ntt_inverse(const u128* tw, u128* data, uint32_t log_d, uint32_t skip_early
   }
 }
 
-static inline size_t reverse_bits(size_t x, uint32_t bits) {
+size_t reverse_bits(size_t x, uint32_t bits) {
   size_t r = 0;
   for (uint32_t i = 0; i < bits; i++) r |= ((x >> i) & 1) << (bits - 1 - i);
   return r;
@@ -145,6 +145,71 @@ void eq_ind_partial_eval(const u128* point, uint32_t n, u128* out) {
   }
 }
 
+
+// fold_interleaved (prover/prover/src/fri/fold.rs:260-282) -> fold_interleaved_chunk
+// (verifier/verifier/src/fri/fold.rs:124-130): out[i] = <codeword[i*2^b .. (i+1)*2^b], eq(r)>.
+void fold_interleaved(const u128* cw, uint32_t log_len, uint32_t log_batch, const u128* ch,
+                      u128* o) {
+  size_t batch = (size_t)1 << log_batch;
+  std::vector<u128> tensor(batch);
+  eq_ind_partial_eval(ch, log_batch, tensor.data());
+  parallel_for((size_t)1 << log_len, [&](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; i++) {
+      u128 acc = 0;
+      for (size_t j = 0; j < batch; j++) acc ^= gf_mul(cw[i * batch + j], tensor[j]);
+      o[i] = acc;
+    }
+  });
+}
+
+// fold_chunk / fold_pair (verifier/verifier/src/fri/fold.rs:20-99): n rounds of the inverse
+// butterfly with twiddle(log_len-1, index) followed by the line extrapolation u + (v - u) r.
+u128 fold_chunk(const u128* tw, uint32_t log_len, size_t chunk_index, u128* vals, const u128* r,
+                uint32_t n) {
+  uint32_t cur_log_len = log_len, log_size = n;
+  for (uint32_t k = 0; k < n; k++) {
+    for (size_t off = 0; off < ((size_t)1 << (log_size - 1)); off++) {
+      u128 u = vals[off << 1], v = vals[(off << 1) | 1];
+      size_t index = (chunk_index << (log_size - 1)) | off;
+      u128 t = twiddle(tw, cur_log_len - 1, index);
+      v ^= u;
+      u ^= gf_mul(v, t);
+      vals[off] = u ^ gf_mul(v ^ u, r[k]);
+    }
+    cur_log_len--;
+    log_size--;
+  }
+  return vals[0];
+}
+
+// fold_codeword (prover/prover/src/fri/fold.rs:297-318): fold_chunk over every coset of 2^n.
+void fold_codeword(const u128* tw, const u128* cw, uint32_t log_len, const u128* r, uint32_t n,
+                   u128* o) {
+  size_t chunk = (size_t)1 << n;
+  size_t n_chunks = ((size_t)1 << log_len) / chunk;
+  parallel_for(n_chunks, [&](size_t lo, size_t hi) {
+    std::vector<u128> vals(chunk);
+    for (size_t ci = lo; ci < hi; ci++) {
+      memcpy(vals.data(), cw + ci * chunk, chunk * sizeof(u128));
+      o[ci] = fold_chunk(tw, log_len, ci, vals.data(), r, n);
+    }
+  });
+}
+
+// ReedSolomonCode::encode_batch (reed_solomon.rs:128-201): bit-reverse the whole message index
+// (log_dim + log_batch bits), repeat it 2^log_inv_rate times, then forward-transform with
+// skip_early = log_inv_rate and skip_late = log_batch.
+void rs_encode(const u128* tw, const u128* m, uint32_t log_dim, uint32_t log_inv_rate,
+               uint32_t log_batch, u128* out) {
+  uint32_t log_msg = log_dim + log_batch;
+  uint32_t log_out = log_msg + log_inv_rate;
+  size_t n_msg = (size_t)1 << log_msg;
+  for (size_t i = 0; i < n_msg; i++) out[reverse_bits(i, log_msg)] = m[i];
+  for (size_t r = 1; r < ((size_t)1 << log_inv_rate); r++)
+    memcpy(out + r * n_msg, out, n_msg * sizeof(u128));
+  ntt_forward(tw, out, log_out, log_inv_rate, log_batch);
+}
+
 }  // namespace orc
 
 using namespace orc;
@@ -174,22 +239,12 @@ int orc_ntt_inverse(const uint64_t* twiddles, uint32_t log_domain, uint64_t* dat
   return 0;
 }
 
-// ReedSolomonCode::encode_batch (reed_solomon.rs:128-201): bit-reverse the whole message index
-// (log_dim + log_batch bits), repeat it 2^log_inv_rate times, then forward-transform with
-// skip_early = log_inv_rate and skip_late = log_batch.
 int orc_rs_encode_batch(const uint64_t* twiddles, uint32_t log_domain, const uint64_t* msg,
                         uint32_t log_dim, uint32_t log_inv_rate, uint32_t log_batch,
                         uint64_t* codeword_out) {
-  uint32_t log_msg = log_dim + log_batch;
-  uint32_t log_out = log_msg + log_inv_rate;
   if (log_dim + log_inv_rate > log_domain) return 1;
-  const u128* m = (const u128*)msg;
-  u128* out = (u128*)codeword_out;
-  size_t n_msg = (size_t)1 << log_msg;
-  for (size_t i = 0; i < n_msg; i++) out[reverse_bits(i, log_msg)] = m[i];
-  for (size_t r = 1; r < ((size_t)1 << log_inv_rate); r++)
-    memcpy(out + r * n_msg, out, n_msg * sizeof(u128));
-  ntt_forward((const u128*)twiddles, out, log_out, log_inv_rate, log_batch);
+  rs_encode((const u128*)twiddles, (const u128*)msg, log_dim, log_inv_rate, log_batch,
+            (u128*)codeword_out);
   return 0;
 }
 
@@ -203,58 +258,18 @@ void orc_eq_ind_partial_eval(const uint64_t* point, uint32_t n, uint64_t* out) {
   eq_ind_partial_eval((const u128*)point, n, (u128*)out);
 }
 
-// fold_interleaved (prover/prover/src/fri/fold.rs:260-282) -> fold_interleaved_chunk
-// (verifier/verifier/src/fri/fold.rs:124-130): out[i] = <codeword[i*2^b .. (i+1)*2^b], eq(r)>.
 int orc_fri_fold_interleaved(const uint64_t* codeword, uint32_t log_len, uint32_t log_batch,
                              const uint64_t* challenges, uint64_t* out) {
-  size_t batch = (size_t)1 << log_batch;
-  std::vector<u128> tensor(batch);
-  eq_ind_partial_eval((const u128*)challenges, log_batch, tensor.data());
-  const u128* cw = (const u128*)codeword;
-  u128* o = (u128*)out;
-  parallel_for((size_t)1 << log_len, [&](size_t lo, size_t hi) {
-    for (size_t i = lo; i < hi; i++) {
-      u128 acc = 0;
-      for (size_t j = 0; j < batch; j++) acc ^= gf_mul(cw[i * batch + j], tensor[j]);
-      o[i] = acc;
-    }
-  });
+  fold_interleaved((const u128*)codeword, log_len, log_batch, (const u128*)challenges, (u128*)out);
   return 0;
 }
 
-// fold_codeword (prover/prover/src/fri/fold.rs:297-318) -> fold_chunk / fold_pair
-// (verifier/verifier/src/fri/fold.rs:20-99): per coset of 2^n values, n rounds of the inverse
-// butterfly with twiddle(log_len-1, index) followed by the line extrapolation u + (v - u) r.
 int orc_fri_fold_codeword(const uint64_t* twiddles, uint32_t log_domain, const uint64_t* codeword,
                           uint32_t log_len, const uint64_t* challenges, uint32_t n_challenges,
                           uint64_t* out) {
   if (n_challenges > log_len || log_len > log_domain) return 1;
-  const u128* tw = (const u128*)twiddles;
-  const u128* cw = (const u128*)codeword;
-  const u128* r = (const u128*)challenges;
-  u128* o = (u128*)out;
-  size_t chunk = (size_t)1 << n_challenges;
-  size_t n_chunks = ((size_t)1 << log_len) / chunk;
-  parallel_for(n_chunks, [&](size_t lo, size_t hi) {
-    std::vector<u128> vals(chunk);
-    for (size_t ci = lo; ci < hi; ci++) {
-      memcpy(vals.data(), cw + ci * chunk, chunk * sizeof(u128));
-      uint32_t cur_log_len = log_len, log_size = n_challenges;
-      for (uint32_t k = 0; k < n_challenges; k++) {
-        for (size_t off = 0; off < ((size_t)1 << (log_size - 1)); off++) {
-          u128 u = vals[off << 1], v = vals[(off << 1) | 1];
-          size_t index = (ci << (log_size - 1)) | off;
-          u128 t = twiddle(tw, cur_log_len - 1, index);
-          v ^= u;
-          u ^= gf_mul(v, t);
-          vals[off] = u ^ gf_mul(v ^ u, r[k]);
-        }
-        cur_log_len--;
-        log_size--;
-      }
-      o[ci] = vals[0];
-    }
-  });
+  fold_codeword((const u128*)twiddles, (const u128*)codeword, log_len, (const u128*)challenges,
+                n_challenges, (u128*)out);
   return 0;
 }
 

@@ -78,6 +78,28 @@ uint32_t orc_calculate_n_test_queries(uint32_t security_bits, uint32_t log_inv_r
 uint32_t orc_estimate_optimal_arity(uint32_t log_block_length, uint32_t digest_size,
                                     uint32_t field_size);
 
+/* ---- Fiat-Shamir transcript (HasherChallenger<Sha256>), for known-answer tests ---- */
+void* orc_transcript_new(void);
+void orc_transcript_free(void* t);
+void orc_transcript_observe(void* t, const uint8_t* p, size_t n);
+void orc_transcript_sample(void* t, uint8_t* out, size_t n);
+
+/* ---- 1-bit multilinear PCS (ring switching + BaseFold + FRI) ----
+ * witness: 2^log_msg packed B128 elements (the B1 multilinear of log_msg + 7 variables);
+ * eval_point: log_msg + 7 elements; twiddles: the RS code domain's table. */
+void orc_eval_1b_mle(const uint64_t* witness, uint32_t log_msg, const uint64_t* point,
+                     uint64_t* out);
+int orc_pcs_prove(const uint64_t* twiddles, const uint64_t* witness, uint32_t log_msg,
+                  uint32_t log_batch, uint32_t log_inv_rate, const uint32_t* arities,
+                  uint32_t n_arities, uint32_t n_queries, const uint64_t* eval_point,
+                  uint8_t* proof_out, size_t proof_cap, size_t* proof_len);
+/* 0 = accepted; otherwise the failed check (1 evaluation claim, 2 tape, 3 terminal root,
+ * 4 terminal degree, 5 layer root, 6 query path, 7 query fold, 8 final consistency, 9 trailing). */
+int orc_pcs_verify(const uint64_t* twiddles, uint32_t log_msg, uint32_t log_batch,
+                   uint32_t log_inv_rate, const uint32_t* arities, uint32_t n_arities,
+                   uint32_t n_queries, const uint64_t* eval_point, const uint64_t* claim,
+                   const uint8_t* proof, size_t proof_len);
+
 /* Number of worker threads the oracle may use (1 = scalar). */
 void orc_set_threads(int n);
 

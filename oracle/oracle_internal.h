@@ -30,6 +30,34 @@ void sha256(const uint8_t* data, size_t len, uint8_t out[32]);
 void sha256_compress(uint32_t state[8], const uint8_t block[64]);
 void compress_node(const uint8_t left[32], const uint8_t right[32], uint8_t out[32]);
 
+// Incremental SHA-256 (FIPS 180-4): the streaming hasher behind the Fiat-Shamir challenger.
+struct Sha256Ctx {
+  uint32_t h[8];
+  uint8_t buf[64];
+  size_t buflen;
+  uint64_t total;
+  Sha256Ctx() { reset(); }
+  void reset();
+  void update(const uint8_t* data, size_t len);
+  void finalize(uint8_t out[32]);  // does not reset
+};
+
+// NTT / RS / Merkle / FRI building blocks (ntt_fri.cpp).
+u128 twiddle(const u128* tw, uint32_t layer, size_t block);
+size_t reverse_bits(size_t x, uint32_t bits);
+void ntt_forward(const u128* tw, u128* data, uint32_t log_d, uint32_t skip_early,
+                 uint32_t skip_late);
+void rs_encode(const u128* tw, const u128* msg, uint32_t log_dim, uint32_t log_inv_rate,
+               uint32_t log_batch, u128* out);
+void merkle_commit(const u128* elems, uint32_t log_leaves, uint32_t log_batch, uint8_t* nodes);
+void eq_ind_partial_eval(const u128* point, uint32_t n, u128* out);
+void fold_interleaved(const u128* cw, uint32_t log_len, uint32_t log_batch, const u128* ch,
+                      u128* out);
+u128 fold_chunk(const u128* tw, uint32_t log_len, size_t chunk_index, u128* vals, const u128* r,
+                uint32_t n);
+void fold_codeword(const u128* tw, const u128* cw, uint32_t log_len, const u128* r, uint32_t n,
+                   u128* out);
+
 // Runs f(i) for i in [0, n), split into contiguous ranges over the configured thread count.
 void parallel_for(size_t n, const std::function<void(size_t, size_t)>& range_fn);
 int num_threads();

@@ -1,0 +1,618 @@
+// CPU oracle (test infrastructure only): the Fiat-Shamir transcript and the FRI-Binius 1-bit
+// multilinear polynomial commitment scheme (ring switching + BaseFold + FRI), prover and verifier.
+//
+// Restates:
+//   transcript   verifier/transcript/src/fiat_shamir/hasher_challenger.rs:14-200,
+//                verifier/transcript/src/transcript.rs:204-407, fiat_shamir/sampling.rs:34-50
+//   PCS prover   prover/prover/src/pcs.rs:107-169, ring_switch.rs:130-265,
+//                protocols/basefold.rs:69-166, protocols/sumcheck/bivariate_product.rs:43-95,
+//                protocols/sumcheck/round_evals.rs:58-142, fri/fold.rs:117-244, fri/query.rs:51-134,
+//                merkle_tree/prover.rs:67-81, merkle_tree/binary_merkle_tree.rs:142-169
+//   PCS verifier verifier/verifier/src/pcs.rs:19-97, protocols/basefold.rs:16-67,
+//                fri/fold.rs:132-278, fri/verify.rs:40-320, merkle_tree/scheme.rs:85-180
+#include <string.h>
+
+#include <vector>
+
+#include "oracle.h"
+#include "oracle_internal.h"
+
+namespace orc {
+
+// ---------------------------------------------------------------- transcript
+
+struct Transcript {
+  Sha256Ctx ctx;
+  bool sampling = true;
+  uint8_t buffer[32];
+  uint32_t index = 0;
+  std::vector<uint8_t> tape;
+  size_t pos = 0;
+  bool overrun = false;
+
+  // HasherChallenger::default: the sampler starts on SHA-256("") with the hasher holding it.
+  Transcript() {
+    uint8_t d0[32];
+    sha256(nullptr, 0, d0);
+    ctx.update(d0, 32);
+    memcpy(buffer, d0, 32);
+  }
+
+  void to_observer() {
+    if (sampling) {
+      uint8_t le[8];
+      for (int i = 0; i < 8; i++) le[i] = (uint8_t)((uint64_t)index >> (8 * i));
+      ctx.update(le, 8);
+      sampling = false;
+    }
+  }
+  void observe(const uint8_t* p, size_t n) {
+    if (n == 0) return;  // an empty write never reaches the observer
+    to_observer();
+    ctx.update(p, n);
+  }
+  void sample_bytes(uint8_t* out, size_t n) {
+    if (!sampling) {
+      sampling = true;
+      index = 32;
+    }
+    for (size_t i = 0; i < n; i++) {
+      if (index == 32) {
+        uint8_t d[32];
+        ctx.finalize(d);
+        ctx.reset();
+        ctx.update(d, 32);
+        memcpy(buffer, d, 32);
+        index = 0;
+      }
+      out[i] = buffer[index++];
+    }
+  }
+  u128 sample() {
+    uint8_t b[16];
+    sample_bytes(b, 16);
+    u128 v = 0;
+    for (int i = 15; i >= 0; i--) v = (v << 8) | b[i];
+    return v;
+  }
+  uint32_t sample_bits(uint32_t bits) {
+    uint8_t b[4];
+    sample_bytes(b, 4);
+    uint32_t v = (uint32_t)b[0] | ((uint32_t)b[1] << 8) | ((uint32_t)b[2] << 16) |
+                 ((uint32_t)b[3] << 24);
+    if (bits > 32) bits = 32;
+    uint32_t mask = bits == 32 ? 0xffffffffu : ((1u << bits) - 1);
+    return v & mask;
+  }
+  // prover
+  void message(const uint8_t* p, size_t n) {
+    tape.insert(tape.end(), p, p + n);
+    observe(p, n);
+  }
+  void message_elems(const u128* e, size_t n) { message((const uint8_t*)e, 16 * n); }
+  void decommit(const uint8_t* p, size_t n) { tape.insert(tape.end(), p, p + n); }
+  void decommit_elems(const u128* e, size_t n) { decommit((const uint8_t*)e, 16 * n); }
+  // verifier
+  bool read_decommit(uint8_t* p, size_t n) {
+    if (pos + n > tape.size()) {
+      overrun = true;
+      memset(p, 0, n);
+      return false;
+    }
+    memcpy(p, tape.data() + pos, n);
+    pos += n;
+    return true;
+  }
+  bool read_message(uint8_t* p, size_t n) {
+    bool ok = read_decommit(p, n);
+    observe(p, n);
+    return ok;
+  }
+};
+
+// ---------------------------------------------------------------- Merkle helpers
+
+struct Tree {
+  uint32_t log_leaves = 0;
+  std::vector<uint8_t> nodes;
+  const uint8_t* root() const { return nodes.data() + nodes.size() - 32; }
+  // BinaryMerkleTree::layer (binary_merkle_tree.rs:142-150)
+  const uint8_t* layer(uint32_t depth) const {
+    size_t total = nodes.size() / 32;
+    return nodes.data() + 32 * (total + 1 - ((size_t)1 << (depth + 1)));
+  }
+  // BinaryMerkleTree::branch (binary_merkle_tree.rs:152-169)
+  void branch(size_t index, uint32_t depth, std::vector<uint8_t>& out) const {
+    uint32_t L = log_leaves;
+    for (uint32_t j = 0; j < L - depth; j++) {
+      size_t node = ((((size_t)1 << j) - 1) << (L + 1 - j)) | ((index >> j) ^ 1);
+      out.insert(out.end(), nodes.data() + 32 * node, nodes.data() + 32 * node + 32);
+    }
+  }
+};
+
+static Tree build_tree(const u128* elems, uint32_t log_leaves, uint32_t log_batch) {
+  Tree t;
+  t.log_leaves = log_leaves;
+  t.nodes.resize(32 * (((size_t)2 << log_leaves) - 1));
+  merkle_commit(elems, log_leaves, log_batch, t.nodes.data());
+  return t;
+}
+
+static uint32_t ceil_log2(uint32_t n) {
+  uint32_t r = 0;
+  while (((uint64_t)1 << r) < n) r++;
+  return r;
+}
+
+static uint32_t log2_exact(size_t n) {
+  uint32_t r = 0;
+  while (((size_t)1 << r) < n) r++;
+  return r;
+}
+
+// ---------------------------------------------------------------- FRI parameters
+
+struct FriParams {
+  uint32_t log_msg;       // log2 of the interleaved message length (the multilinear's n_vars)
+  uint32_t log_batch;
+  uint32_t log_inv_rate;
+  std::vector<uint32_t> arities;
+  uint32_t n_queries;
+  uint32_t log_dim() const { return log_msg - log_batch; }
+  uint32_t rs_log_len() const { return log_dim() + log_inv_rate; }
+  uint32_t log_len() const { return rs_log_len() + log_batch; }
+  uint32_t n_final_challenges() const {
+    uint32_t s = 0;
+    for (auto a : arities) s += a;
+    return log_dim() - s;
+  }
+  // vcs_optimal_layers_depths_iter (verifier/verifier/src/fri/common.rs:154-168)
+  std::vector<uint32_t> optimal_depths() const {
+    std::vector<uint32_t> d;
+    uint32_t cap = ceil_log2(n_queries);
+    uint32_t log_n_cosets = log_len();
+    std::vector<uint32_t> steps{log_batch};
+    steps.insert(steps.end(), arities.begin(), arities.end());
+    for (auto a : steps) {
+      log_n_cosets -= a;
+      d.push_back(cap < log_n_cosets ? cap : log_n_cosets);
+    }
+    return d;
+  }
+};
+
+// ---------------------------------------------------------------- FRI fold prover
+
+struct FriFolder {
+  const FriParams& p;
+  const u128* tw;
+  const u128* codeword;
+  const Tree& codeword_tree;
+  std::vector<std::vector<u128>> round_words;
+  std::vector<Tree> round_trees;
+  uint32_t curr_round = 0;
+  int64_t next_commit_round;
+  std::vector<u128> unprocessed;
+
+  FriFolder(const FriParams& p_, const u128* tw_, const u128* cw, const Tree& tree)
+      : p(p_), tw(tw_), codeword(cw), codeword_tree(tree), next_commit_round(p_.log_batch) {}
+
+  // FRIFoldProver::execute_fold_round (prover/prover/src/fri/fold.rs:117-175)
+  bool execute_fold_round(uint8_t root[32]) {
+    if (next_commit_round < 0 || (int64_t)curr_round != next_commit_round) return false;
+    std::vector<u128> folded;
+    if (round_words.empty()) {
+      folded.resize((size_t)1 << p.rs_log_len());
+      fold_interleaved(codeword, p.rs_log_len(), p.log_batch, unprocessed.data(), folded.data());
+    } else {
+      const auto& prev = round_words.back();
+      uint32_t log_prev = log2_exact(prev.size());
+      folded.resize(prev.size() >> unprocessed.size());
+      fold_codeword(tw, prev.data(), log_prev, unprocessed.data(), (uint32_t)unprocessed.size(),
+                    folded.data());
+    }
+    unprocessed.clear();
+    bool has_next = round_words.size() < p.arities.size();
+    uint32_t next_arity = has_next ? p.arities[round_words.size()] : 0;
+    uint32_t log_coset = has_next ? next_arity : p.n_final_challenges();
+    uint32_t log_leaves = log2_exact(folded.size()) - log_coset;
+    Tree t = build_tree(folded.data(), log_leaves, log_coset);
+    memcpy(root, t.root(), 32);
+    next_commit_round = has_next ? next_commit_round + next_arity : -1;
+    round_words.push_back(std::move(folded));
+    round_trees.push_back(std::move(t));
+    return true;
+  }
+
+  void receive_challenge(u128 c) {
+    unprocessed.push_back(c);
+    curr_round++;
+  }
+
+  // prove_coset_opening (prover/prover/src/fri/query.rs:112-134)
+  static void coset_opening(Transcript& t, const u128* word, const Tree& tree, size_t coset_index,
+                            uint32_t log_coset, uint32_t depth) {
+    t.decommit_elems(word + (coset_index << log_coset), (size_t)1 << log_coset);
+    std::vector<uint8_t> br;
+    tree.branch(coset_index, depth, br);
+    t.decommit(br.data(), br.size());
+  }
+
+  // FRIFoldProver::finish_proof (fri/fold.rs:221-244) and FRIQueryProver (fri/query.rs:51-110)
+  void finish_proof(Transcript& t) {
+    if (round_words.empty())
+      t.decommit_elems(codeword, (size_t)1 << p.log_len());
+    else
+      t.decommit_elems(round_words.back().data(), round_words.back().size());
+    auto depths = p.optimal_depths();
+    std::vector<const Tree*> trees{&codeword_tree};
+    for (size_t i = 0; i + 1 < round_trees.size(); i++) trees.push_back(&round_trees[i]);
+    for (size_t i = 0; i < trees.size() && i < depths.size(); i++)
+      t.decommit(trees[i]->layer(depths[i]), 32 * ((size_t)1 << depths[i]));
+    for (uint32_t q = 0; q < p.n_queries; q++) {
+      size_t index = t.sample_bits(p.rs_log_len());
+      coset_opening(t, codeword, codeword_tree, index, p.log_batch, depths[0]);
+      for (size_t i = 0; i < round_words.size() && i < p.arities.size() && i + 1 < depths.size();
+           i++) {
+        index >>= p.arities[i];
+        coset_opening(t, round_words[i].data(), round_trees[i], index, p.arities[i], depths[i + 1]);
+      }
+    }
+  }
+};
+
+// ---------------------------------------------------------------- ring switching helpers
+
+// fold_1b_rows_for_b128 (ring_switch.rs:197-265): out[k] = sum_i bit_k(mat[i]) * vec[i].
+static void fold_1b_rows(const u128* mat, const u128* vec, size_t n, u128 out[128]) {
+  for (int k = 0; k < 128; k++) out[k] = 0;
+  for (size_t i = 0; i < n; i++) {
+    u128 m = mat[i];
+    for (int k = 0; k < 128; k++)
+      if ((m >> k) & 1) out[k] ^= vec[i];
+  }
+}
+
+// fold_b128_elems_inplace (ring_switch.rs:130-171): x -> sum_k bit_k(x) * vec[k].
+static u128 fold_elem(u128 x, const u128 vec[128]) {
+  u128 acc = 0;
+  for (int k = 0; k < 128; k++)
+    if ((x >> k) & 1) acc ^= vec[k];
+  return acc;
+}
+
+// TensorAlgebra<B1, B128>::transpose: the 128 x 128 bit matrix with row k = s[k].
+static void transpose128(const u128 in[128], u128 out[128]) {
+  for (int j = 0; j < 128; j++) {
+    u128 v = 0;
+    for (int k = 0; k < 128; k++) v |= (u128)((in[k] >> j) & 1) << k;
+    out[j] = v;
+  }
+}
+
+static u128 inner(const u128* a, const u128* b, size_t n) {
+  u128 acc = 0;
+  for (size_t i = 0; i < n; i++) acc ^= gf_mul(a[i], b[i]);
+  return acc;
+}
+
+// ---------------------------------------------------------------- PCS prover
+
+void pcs_prove(const FriParams& p, const u128* tw, const u128* codeword, const Tree& tree,
+               const u128* witness, const u128* eval_point, Transcript& t) {
+  const uint32_t n = p.log_msg;
+  const size_t N = (size_t)1 << n;
+  std::vector<u128> suffix_tensor(N);
+  eq_ind_partial_eval(eval_point + 7, n, suffix_tensor.data());
+  u128 s_hat_v[128];
+  fold_1b_rows(witness, suffix_tensor.data(), N, s_hat_v);
+  t.message_elems(s_hat_v, 128);
+  u128 s_hat_u[128];
+  transpose128(s_hat_v, s_hat_u);
+  u128 r_dp[7];
+  for (int i = 0; i < 7; i++) r_dp[i] = t.sample();
+  u128 eq_r[128];
+  eq_ind_partial_eval(r_dp, 7, eq_r);
+  u128 sum = inner(s_hat_u, eq_r, 128);
+  std::vector<u128> a(witness, witness + N), b(N);
+  for (size_t i = 0; i < N; i++) b[i] = fold_elem(suffix_tensor[i], eq_r);
+
+  // BaseFoldProver::prove: bivariate product sumcheck interleaved with FRI folding.
+  FriFolder fri(p, tw, codeword, tree);
+  for (uint32_t round = 0; round < n; round++) {
+    size_t half = a.size() / 2;
+    u128 y1 = 0, yinf = 0;
+    for (size_t i = 0; i < half; i++) {
+      y1 ^= gf_mul(a[half + i], b[half + i]);
+      yinf ^= gf_mul(a[i] ^ a[half + i], b[i] ^ b[half + i]);
+    }
+    u128 c0 = sum ^ y1, c2 = yinf, c1 = y1 ^ c0 ^ c2;
+    uint8_t root[32];
+    bool committed = fri.execute_fold_round(root);
+    u128 coeffs[2] = {c0, c1};
+    t.message_elems(coeffs, 2);
+    if (committed) t.message(root, 32);
+    u128 r = t.sample();
+    for (size_t i = 0; i < half; i++) {
+      a[i] ^= gf_mul(r, a[half + i] ^ a[i]);
+      b[i] ^= gf_mul(r, b[half + i] ^ b[i]);
+    }
+    a.resize(half);
+    b.resize(half);
+    sum = c0 ^ gf_mul(c1, r) ^ gf_mul(c2, gf_mul(r, r));
+    fri.receive_challenge(r);
+  }
+  uint8_t root[32];
+  if (fri.execute_fold_round(root)) t.message(root, 32);
+  fri.finish_proof(t);
+}
+
+// ---------------------------------------------------------------- PCS verifier
+
+enum VerifyError {
+  V_OK = 0,
+  V_EVAL_CLAIM = 1,
+  V_TAPE = 2,
+  V_TERMINAL_ROOT = 3,
+  V_TERMINAL_DEGREE = 4,
+  V_LAYER_ROOT = 5,
+  V_QUERY_PATH = 6,
+  V_QUERY_FOLD = 7,
+  V_FINAL = 8,
+  V_TRAILING = 9,
+};
+
+static void leaf_digest(const u128* vals, size_t n, uint8_t out[32]) {
+  sha256((const uint8_t*)vals, 16 * n, out);
+}
+
+static void fold_digests(std::vector<uint8_t> d, uint8_t root[32]) {
+  size_t len = d.size() / 32;
+  while (len > 1) {
+    for (size_t i = 0; i < len / 2; i++) {
+      uint8_t o[32];
+      compress_node(&d[64 * i], &d[64 * i + 32], o);
+      memcpy(&d[32 * i], o, 32);
+    }
+    len /= 2;
+  }
+  memcpy(root, d.data(), 32);
+}
+
+// BinaryMerkleTreeScheme::verify_opening (merkle_tree/scheme.rs:122-158)
+static bool verify_opening(Transcript& t, size_t index, const u128* vals, size_t n_vals,
+                           uint32_t layer_depth, uint32_t tree_depth, const uint8_t* layer) {
+  uint8_t d[32];
+  leaf_digest(vals, n_vals, d);
+  for (uint32_t j = 0; j < tree_depth - layer_depth; j++) {
+    uint8_t sib[32], o[32];
+    if (!t.read_decommit(sib, 32)) return false;
+    if ((index & 1) == 0)
+      compress_node(d, sib, o);
+    else
+      compress_node(sib, d, o);
+    memcpy(d, o, 32);
+    index >>= 1;
+  }
+  return memcmp(d, layer + 32 * index, 32) == 0;
+}
+
+int pcs_verify(const FriParams& p, const u128* tw, const u128* eval_point, u128 claim,
+               const uint8_t codeword_root[32], Transcript& t) {
+  const uint32_t n = p.log_msg;
+  u128 s_hat_v[128];
+  if (!t.read_message((uint8_t*)s_hat_v, 16 * 128)) return V_TAPE;
+  u128 eq_lo[128];
+  eq_ind_partial_eval(eval_point, 7, eq_lo);
+  if (inner(s_hat_v, eq_lo, 128) != claim) return V_EVAL_CLAIM;
+  u128 s_hat_u[128];
+  transpose128(s_hat_v, s_hat_u);
+  u128 batching[7];
+  for (int i = 0; i < 7; i++) batching[i] = t.sample();
+  u128 eq_b[128];
+  eq_ind_partial_eval(batching, 7, eq_b);
+  u128 sum = inner(s_hat_u, eq_b, 128);
+
+  // calculate_fri_commit_rounds (verifier/verifier/src/fri/fold.rs:257-278) with n + 1 rounds.
+  std::vector<bool> commit_rounds(n + 1, false);
+  {
+    uint32_t idx = 0;
+    std::vector<uint32_t> steps{p.log_batch};
+    steps.insert(steps.end(), p.arities.begin(), p.arities.end());
+    for (auto a : steps) {
+      idx += a;
+      if (idx < n + 1)
+        commit_rounds[idx] = true;
+      else
+        break;
+    }
+  }
+  std::vector<std::vector<uint8_t>> round_roots;
+  std::vector<u128> challenges;
+  for (uint32_t round = 0; round < n; round++) {
+    u128 c[2];
+    if (!t.read_message((uint8_t*)c, 32)) return V_TAPE;
+    if (commit_rounds[round]) {
+      std::vector<uint8_t> r(32);
+      if (!t.read_message(r.data(), 32)) return V_TAPE;
+      round_roots.push_back(r);
+    }
+    // RoundProof::recover: c2 = sum - c0 - (c0 + c1)
+    u128 c2 = sum ^ c[0] ^ c[0] ^ c[1];
+    u128 r = t.sample();
+    challenges.push_back(r);
+    sum = c[0] ^ gf_mul(c[1], r) ^ gf_mul(c2, gf_mul(r, r));
+  }
+  if (commit_rounds[n]) {
+    std::vector<uint8_t> r(32);
+    if (!t.read_message(r.data(), 32)) return V_TAPE;
+    round_roots.push_back(r);
+  }
+  if (round_roots.size() != 1 + p.arities.size()) return V_TAPE;
+
+  // FRIQueryVerifier::verify (verifier/verifier/src/fri/verify.rs:86-200)
+  const uint32_t n_final = p.n_final_challenges();
+  std::vector<u128> terminal((size_t)1 << (n_final + p.log_inv_rate));
+  if (!t.read_decommit((uint8_t*)terminal.data(), 16 * terminal.size())) return V_TAPE;
+  {
+    std::vector<uint8_t> digests;
+    size_t coset = (size_t)1 << n_final;
+    for (size_t i = 0; i < terminal.size() / coset; i++) {
+      uint8_t d[32];
+      leaf_digest(terminal.data() + i * coset, coset, d);
+      digests.insert(digests.end(), d, d + 32);
+    }
+    uint8_t root[32];
+    fold_digests(digests, root);
+    if (memcmp(root, round_roots.back().data(), 32) != 0) return V_TERMINAL_ROOT;
+  }
+  const u128* fold_ch = challenges.data() + p.log_batch;
+  const size_t n_fold_ch = challenges.size() - p.log_batch;
+  u128 final_value = 0;
+  {
+    size_t coset = (size_t)1 << n_final;
+    std::vector<u128> scratch(coset);
+    for (size_t i = 0; i < terminal.size() / coset; i++) {
+      memcpy(scratch.data(), terminal.data() + i * coset, 16 * coset);
+      u128 v = fold_chunk(tw, n_final + p.log_inv_rate, i, scratch.data(),
+                          fold_ch + (n_fold_ch - n_final), n_final);
+      if (i == 0)
+        final_value = v;
+      else if (v != final_value)
+        return V_TERMINAL_DEGREE;
+    }
+  }
+  auto depths = p.optimal_depths();
+  std::vector<std::vector<uint8_t>> layers;
+  for (auto d : depths) {
+    std::vector<uint8_t> l(32 * ((size_t)1 << d));
+    if (!t.read_decommit(l.data(), l.size())) return V_TAPE;
+    layers.push_back(l);
+  }
+  for (size_t i = 0; i < layers.size(); i++) {
+    const uint8_t* commitment = i == 0 ? codeword_root : round_roots[i - 1].data();
+    uint8_t root[32];
+    fold_digests(layers[i], root);
+    if (memcmp(root, commitment, 32) != 0) return V_LAYER_ROOT;
+  }
+  std::vector<u128> interleave_tensor((size_t)1 << p.log_batch);
+  eq_ind_partial_eval(challenges.data(), p.log_batch, interleave_tensor.data());
+  for (uint32_t q = 0; q < p.n_queries; q++) {
+    size_t index = t.sample_bits(p.rs_log_len());
+    std::vector<u128> vals((size_t)1 << p.log_batch);
+    if (!t.read_decommit((uint8_t*)vals.data(), 16 * vals.size())) return V_TAPE;
+    if (!verify_opening(t, index, vals.data(), vals.size(), depths[0], p.rs_log_len(),
+                        layers[0].data()))
+      return V_QUERY_PATH;
+    u128 next = inner(vals.data(), interleave_tensor.data(), vals.size());
+    uint32_t fold_round = 0, log_n_cosets = p.rs_log_len();
+    for (size_t i = 0; i < p.arities.size() && i + 1 < layers.size(); i++) {
+      uint32_t arity = p.arities[i];
+      size_t coset_index = index >> arity;
+      log_n_cosets -= arity;
+      std::vector<u128> cv((size_t)1 << arity);
+      if (!t.read_decommit((uint8_t*)cv.data(), 16 * cv.size())) return V_TAPE;
+      if (!verify_opening(t, coset_index, cv.data(), cv.size(), depths[i + 1], log_n_cosets,
+                          layers[i + 1].data()))
+        return V_QUERY_PATH;
+      if (next != cv[index % ((size_t)1 << arity)]) return V_QUERY_FOLD;
+      next = fold_chunk(tw, p.rs_log_len() - fold_round, coset_index, cv.data(),
+                        fold_ch + fold_round, arity);
+      index = coset_index;
+      fold_round += arity;
+    }
+    if (next != terminal[index]) return V_QUERY_FOLD;
+  }
+
+  // Final consistency (pcs.rs verify): sumcheck value == fri value * rs_eq(z, reversed r, eq_b),
+  // with rs_eq evaluated as <rs_eq_ind(batching, z), eq(reversed challenges)>.
+  std::vector<u128> rev(challenges.rbegin(), challenges.rend());
+  const size_t N = (size_t)1 << n;
+  std::vector<u128> z_tensor(N), q_tensor(N);
+  eq_ind_partial_eval(eval_point + 7, n, z_tensor.data());
+  eq_ind_partial_eval(rev.data(), n, q_tensor.data());
+  u128 rs_eq = 0;
+  for (size_t i = 0; i < N; i++) rs_eq ^= gf_mul(fold_elem(z_tensor[i], eq_b), q_tensor[i]);
+  if (sum != gf_mul(final_value, rs_eq)) return V_FINAL;
+  return V_OK;
+}
+
+static FriParams make_params(uint32_t log_msg, uint32_t log_batch, uint32_t log_inv_rate,
+                             const uint32_t* arities, uint32_t n_arities, uint32_t n_queries) {
+  FriParams p;
+  p.log_msg = log_msg;
+  p.log_batch = log_batch;
+  p.log_inv_rate = log_inv_rate;
+  p.arities.assign(arities, arities + n_arities);
+  p.n_queries = n_queries;
+  return p;
+}
+
+}  // namespace orc
+
+using namespace orc;
+
+extern "C" {
+
+void* orc_transcript_new(void) { return new Transcript(); }
+void orc_transcript_free(void* t) { delete static_cast<Transcript*>(t); }
+void orc_transcript_observe(void* t, const uint8_t* p, size_t n) {
+  static_cast<Transcript*>(t)->observe(p, n);
+}
+void orc_transcript_sample(void* t, uint8_t* out, size_t n) {
+  static_cast<Transcript*>(t)->sample_bytes(out, n);
+}
+
+// Multilinear evaluation of the B1 polynomial whose bit (i << 7) | k is bit k of witness[i].
+void orc_eval_1b_mle(const uint64_t* witness, uint32_t log_msg, const uint64_t* point,
+                     uint64_t* out) {
+  const u128* w = (const u128*)witness;
+  const u128* pt = (const u128*)point;
+  size_t N = (size_t)1 << log_msg;
+  std::vector<u128> hi(N);
+  eq_ind_partial_eval(pt + 7, log_msg, hi.data());
+  u128 lo[128];
+  eq_ind_partial_eval(pt, 7, lo);
+  u128 acc = 0;
+  for (size_t i = 0; i < N; i++) acc ^= gf_mul(fold_elem(w[i], lo), hi[i]);
+  store(out, acc);
+}
+
+// Commits the witness (RS encode + Merkle), writes the root as the first transcript message and
+// proves the evaluation at eval_point (log_msg + 7 coordinates).  twiddles: the RS code's domain.
+int orc_pcs_prove(const uint64_t* twiddles, const uint64_t* witness, uint32_t log_msg,
+                  uint32_t log_batch, uint32_t log_inv_rate, const uint32_t* arities,
+                  uint32_t n_arities, uint32_t n_queries, const uint64_t* eval_point,
+                  uint8_t* proof_out, size_t proof_cap, size_t* proof_len) {
+  FriParams p = make_params(log_msg, log_batch, log_inv_rate, arities, n_arities, n_queries);
+  const u128* tw = (const u128*)twiddles;
+  std::vector<u128> codeword((size_t)1 << p.log_len());
+  rs_encode(tw, (const u128*)witness, p.log_dim(), log_inv_rate, log_batch, codeword.data());
+  Tree tree = build_tree(codeword.data(), p.rs_log_len(), log_batch);
+  Transcript t;
+  t.message(tree.root(), 32);
+  pcs_prove(p, tw, codeword.data(), tree, (const u128*)witness, (const u128*)eval_point, t);
+  *proof_len = t.tape.size();
+  if (t.tape.size() > proof_cap) return 1;
+  memcpy(proof_out, t.tape.data(), t.tape.size());
+  return 0;
+}
+
+int orc_pcs_verify(const uint64_t* twiddles, uint32_t log_msg, uint32_t log_batch,
+                   uint32_t log_inv_rate, const uint32_t* arities, uint32_t n_arities,
+                   uint32_t n_queries, const uint64_t* eval_point, const uint64_t* claim,
+                   const uint8_t* proof, size_t proof_len) {
+  FriParams p = make_params(log_msg, log_batch, log_inv_rate, arities, n_arities, n_queries);
+  Transcript t;
+  t.tape.assign(proof, proof + proof_len);
+  uint8_t root[32];
+  if (!t.read_message(root, 32)) return V_TAPE;
+  int rc = pcs_verify(p, (const u128*)twiddles, (const u128*)eval_point, load(claim), root, t);
+  if (rc) return rc;
+  if (t.overrun) return V_TAPE;
+  if (t.pos != t.tape.size()) return V_TRAILING;
+  return V_OK;
+}
+
+}  // extern "C"

@@ -95,6 +95,47 @@ void sha256(const uint8_t* data, size_t len, uint8_t out[32]) {
   }
 }
 
+void Sha256Ctx::reset() {
+  memcpy(h, H0, sizeof(h));
+  buflen = 0;
+  total = 0;
+}
+
+void Sha256Ctx::update(const uint8_t* data, size_t len) {
+  total += len;
+  while (len > 0) {
+    size_t take = 64 - buflen < len ? 64 - buflen : len;
+    memcpy(buf + buflen, data, take);
+    buflen += take;
+    data += take;
+    len -= take;
+    if (buflen == 64) {
+      sha256_compress(h, buf);
+      buflen = 0;
+    }
+  }
+}
+
+void Sha256Ctx::finalize(uint8_t out[32]) {
+  uint32_t s[8];
+  memcpy(s, h, sizeof(s));
+  uint8_t tail[128];
+  memset(tail, 0, sizeof(tail));
+  memcpy(tail, buf, buflen);
+  tail[buflen] = 0x80;
+  size_t tail_len = (buflen + 9 <= 64) ? 64 : 128;
+  uint64_t bits = total * 8;
+  for (int i = 0; i < 8; i++) tail[tail_len - 1 - i] = (uint8_t)(bits >> (8 * i));
+  sha256_compress(s, tail);
+  if (tail_len == 128) sha256_compress(s, tail + 64);
+  for (int i = 0; i < 8; i++) {
+    out[4 * i] = (uint8_t)(s[i] >> 24);
+    out[4 * i + 1] = (uint8_t)(s[i] >> 16);
+    out[4 * i + 2] = (uint8_t)(s[i] >> 8);
+    out[4 * i + 3] = (uint8_t)s[i];
+  }
+}
+
 // The compression IV: the digest bytes of "BINIUS SHA-256 COMPRESS" read as native
 // (little-endian) u32 words, as `bytes_of_mut(&mut initial_state).copy_from_slice(...)` does.
 static void node_iv(uint32_t iv[8]) {
