@@ -64,7 +64,14 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--log-len", type=int, default=None,
+                    help="per-column codeword log length (default 20; smaller cases for profiling)")
+    args = ap.parse_args()
+    if args.log_len is not None:
+        global LOG_LEN
+        assert 13 <= args.log_len <= 24
+        LOG_LEN = args.log_len
+    return args
 
 
 def dist_env():

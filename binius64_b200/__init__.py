@@ -334,3 +334,111 @@ def gf_mul_batch(a, b, out=None, stream=None):
         out = empty_elems(n, device=a.device)
     check(lib().binius_gf_mul_batch(_ptr(a), _ptr(b), _ptr(out), n, _stream(stream)))
     return out
+
+
+class ProverTranscript:
+    """ProverTranscript<HasherChallenger<Sha256>> (verifier/transcript/src/transcript.rs:204-407)."""
+
+    def __init__(self):
+        self._h = ctypes.c_void_p()
+        check(lib().binius_transcript_create(ctypes.byref(self._h)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def message(self, data: bytes) -> None:
+        check(lib().binius_transcript_message(self._h, data, len(data)))
+
+    def decommitment(self, data: bytes) -> None:
+        check(lib().binius_transcript_decommitment(self._h, data, len(data)))
+
+    def observe(self, data: bytes) -> None:
+        check(lib().binius_transcript_observe(self._h, data, len(data)))
+
+    def sample_bytes(self, n: int) -> bytes:
+        buf = (ctypes.c_uint8 * max(n, 1))()
+        check(lib().binius_transcript_sample(self._h, ctypes.addressof(buf), n))
+        return bytes(buf)[:n]
+
+    def sample(self) -> int:
+        """CanSample<B128>: 16 bytes as a little-endian u128."""
+        return int.from_bytes(self.sample_bytes(16), "little")
+
+    def sample_bits(self, bits: int) -> int:
+        return int(lib().binius_transcript_sample_bits(self._h, bits))
+
+    def finalize(self) -> bytes:
+        n = int(lib().binius_transcript_len(self._h))
+        buf = (ctypes.c_uint8 * max(n, 1))()
+        out = ctypes.c_size_t(0)
+        check(lib().binius_transcript_finalize(self._h, ctypes.addressof(buf), n, ctypes.byref(out)))
+        return bytes(buf)[: out.value]
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().binius_transcript_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
+class PcsCommitted:
+    """Device-resident codeword + Merkle tree of a PCS commitment."""
+
+    def __init__(self, handle, root: bytes):
+        self.handle = handle
+        self.root = root
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                lib().binius_pcs_committed_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+
+class OneBitPCSProver:
+    """OneBitPCSProver (prover/prover/src/pcs.rs:30-169) with SHA-256 Merkle trees."""
+
+    def __init__(self, ntt: AdditiveNTT, fri_params: FRIParams):
+        self.ntt = ntt
+        self.fri_params = fri_params
+        self._h = ctypes.c_void_p()
+        ar = (ctypes.c_uint32 * max(1, len(fri_params.fold_arities)))(*fri_params.fold_arities)
+        check(lib().binius_pcs_create(ntt.handle, fri_params.log_msg_len(),
+                                      fri_params.log_batch_size, fri_params.rs_code.log_inv_rate,
+                                      ar, len(fri_params.fold_arities), fri_params.n_test_queries,
+                                      ctypes.byref(self._h)))
+
+    def commit(self, packed_multilin, stream=None) -> PcsCommitted:
+        if _elems_of(packed_multilin) != 1 << self.fri_params.log_msg_len():
+            raise ArgumentError(1, "packed multilinear length does not match the FRI parameters")
+        out = ctypes.c_void_p()
+        root = (ctypes.c_uint8 * 32)()
+        check(lib().binius_pcs_commit(self._h, _ptr(packed_multilin), ctypes.byref(out),
+                                      ctypes.addressof(root), _stream(stream)))
+        return PcsCommitted(out, bytes(root))
+
+    def prove(self, committed: PcsCommitted, packed_multilin, evaluation_point,
+              transcript: ProverTranscript, stream=None) -> None:
+        n = self.fri_params.log_msg_len() + 7
+        if len(evaluation_point) != n:
+            raise ArgumentError(1, f"evaluation point must have {n} coordinates")
+        pt = np.array([[c & (2**64 - 1), c >> 64] for c in evaluation_point], dtype=np.uint64)
+        check(lib().binius_pcs_prove(self._h, committed.handle, _ptr(packed_multilin),
+                                     pt.ctypes.data_as(ctypes.c_void_p), transcript.handle,
+                                     _stream(stream)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().binius_pcs_destroy(h)
+            except Exception:
+                pass
+            self._h = None

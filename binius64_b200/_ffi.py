@@ -59,6 +59,21 @@ _SIGS = {
     "binius_fri_fold_codeword": (_int, [_vp, _vp, _u32, _vp, _u32, _vp, _vp]),
     "binius_fri_fold_codeword_noalloc": (_int, [_vp, _vp, _u32, _vp, _u32, _vp, _vp]),
     "binius_fri_commit_interleaved": (_int, [_vp, _vp, _u32, _u32, _u32, _vp, _vp, _vp, _vp]),
+    "binius_transcript_create": (_int, [_c.POINTER(_vp)]),
+    "binius_transcript_destroy": (_int, [_vp]),
+    "binius_transcript_message": (_int, [_vp, _vp, _c.c_size_t]),
+    "binius_transcript_decommitment": (_int, [_vp, _vp, _c.c_size_t]),
+    "binius_transcript_observe": (_int, [_vp, _vp, _c.c_size_t]),
+    "binius_transcript_sample": (_int, [_vp, _vp, _c.c_size_t]),
+    "binius_transcript_sample_bits": (_u32, [_vp, _u32]),
+    "binius_transcript_len": (_c.c_size_t, [_vp]),
+    "binius_transcript_finalize": (_int, [_vp, _vp, _c.c_size_t, _c.POINTER(_c.c_size_t)]),
+    "binius_pcs_create": (_int, [_vp, _u32, _u32, _u32, _vp, _u32, _u32, _c.POINTER(_vp)]),
+    "binius_pcs_destroy": (_int, [_vp]),
+    "binius_pcs_commit": (_int, [_vp, _vp, _c.POINTER(_vp), _vp, _vp]),
+    "binius_pcs_committed_destroy": (_int, [_vp]),
+    "binius_pcs_committed_codeword": (_vp, [_vp]),
+    "binius_pcs_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "binius_fri_n_test_queries": (_u32, [_u32, _u32]),
     "binius_fri_estimate_optimal_arity": (_u32, [_u32, _u32, _u32]),
     "binius_gf_mul_batch": (_int, [_vp, _vp, _vp, _u64, _vp]),

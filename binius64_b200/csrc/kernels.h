@@ -1,0 +1,47 @@
+// Host-side launch helpers shared by the protocol drivers (all asynchronous on `s`).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/binius_gpu.h"
+
+namespace bgpu {
+
+// Up to 32 field elements passed to a kernel by value.
+struct Point32 {
+  uint4 r[32];
+};
+
+// One contiguous copy of a gather: `bytes` (a multiple of 16, 16-byte aligned) from src to
+// dst + dst_off.
+struct GatherSegment {
+  const uint8_t* src;
+  uint64_t dst_off;
+  uint32_t bytes;
+  uint32_t pad;
+};
+
+// eq_ind_partial_eval of a host point with n <= 32 coordinates into d_out (2^n elements).
+int eq_tensor(const uint4* h_point, uint32_t n, uint4* d_out, cudaStream_t s);
+// d_out512 (128 elements) = fold_1b_rows_for_b128(mat, vec) over n rows.
+int fold_1b_rows(const uint4* d_mat, const uint4* d_vec, uint64_t n, uint32_t* d_out512,
+                 cudaStream_t s);
+// d_out[i] = sum_k bit_k(d_in[i]) * d_vec128[k]  (d_out may equal d_in).
+int fold_b128_elems(const uint4* d_in, uint4* d_out, uint64_t n, const uint4* d_vec128,
+                    cudaStream_t s);
+// d_out8 = (y_1, y_inf) of the bivariate product round on (a, b) of length 2*half.
+int bivariate_eval(const uint4* d_a, const uint4* d_b, uint64_t half, uint32_t* d_out8,
+                   cudaStream_t s);
+// Fold (a, b) of length size by r, then (y_1, y_inf) of the next round.
+int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[16],
+                        uint32_t* d_out8, cudaStream_t s);
+int gather_segments(const GatherSegment* d_segs, uint32_t n, uint8_t* d_dst, cudaStream_t s);
+
+// From the other translation units.
+int rs_encode_batch(const binius_ntt* ntt, const void* d_msg, uint32_t log_dim,
+                    uint32_t log_inv_rate, uint32_t log_batch, void* d_codeword,
+                    cudaStream_t stream);
+int merkle_commit(const void* d_elems, uint32_t log_leaves, uint32_t log_batch, void* d_nodes,
+                  cudaStream_t stream);
+
+}  // namespace bgpu

@@ -1,0 +1,404 @@
+// FRI-Binius 1-bit multilinear polynomial commitment: commit and the evaluation proof.
+//
+// Host driver of OneBitPCSProver (prover/prover/src/pcs.rs:58-169): the protocol's sequential
+// Fiat-Shamir steps run on the host (transcript.h) while every data-parallel step runs on the GPU
+// over device-resident buffers: RS encode + Merkle commit, the eq tensor of the evaluation point's
+// suffix, the ring-switch row fold, the ring-switch equality indicator, the BaseFold rounds
+// (bivariate product sumcheck, protocols/basefold.rs:130-166) interleaved with FRI folds and
+// Merkle commits of the folded codewords (fri/fold.rs:117-175), and the FRI query openings
+// (fri/fold.rs:221-244, fri/query.rs:51-134) gathered into one buffer by a single kernel.
+#include <string.h>
+
+#include <vector>
+
+#include "internal.h"
+#include "kernels.h"
+#include "transcript.h"
+
+using namespace bgpu;
+
+struct binius_pcs {
+  const binius_ntt* ntt;
+  uint32_t log_msg, log_batch, log_inv_rate, n_queries;
+  std::vector<uint32_t> arities;
+  uint32_t log_dim() const { return log_msg - log_batch; }
+  uint32_t rs_log_len() const { return log_dim() + log_inv_rate; }
+  uint32_t log_len() const { return rs_log_len() + log_batch; }
+  uint32_t n_final() const {
+    uint32_t s = 0;
+    for (auto a : arities) s += a;
+    return log_dim() - s;
+  }
+  // vcs_optimal_layers_depths_iter (verifier/verifier/src/fri/common.rs:154-168)
+  std::vector<uint32_t> optimal_depths() const {
+    uint32_t cap = 0;
+    while ((1ull << cap) < n_queries) cap++;
+    std::vector<uint32_t> d;
+    uint32_t log_n_cosets = log_len();
+    std::vector<uint32_t> steps{log_batch};
+    steps.insert(steps.end(), arities.begin(), arities.end());
+    for (auto a : steps) {
+      log_n_cosets -= a;
+      d.push_back(cap < log_n_cosets ? cap : log_n_cosets);
+    }
+    return d;
+  }
+};
+
+struct binius_pcs_committed {
+  int device;
+  uint32_t log_len;      // codeword log length (rs_log_len + log_batch)
+  uint32_t log_leaves;   // rs_log_len
+  void* d_codeword;
+  void* d_nodes;
+  uint8_t root[32];
+};
+
+namespace {
+
+typedef unsigned __int128 u128h;
+
+u128h to_u128(const uint8_t b[16]) {
+  u128h v;
+  memcpy(&v, b, 16);
+  return v;
+}
+void from_u128(u128h v, uint8_t b[16]) { memcpy(b, &v, 16); }
+
+uint64_t layer_off(uint32_t L, uint32_t j) { return (1ull << (L + 1)) - (1ull << (L + 1 - j)); }
+
+// Device-side FRIFoldProver state.
+struct DevFri {
+  const binius_pcs& P;
+  const binius_pcs_committed& C;
+  cudaStream_t s;
+  std::vector<uint4*> words;
+  std::vector<uint32_t> word_log_len;
+  std::vector<uint8_t*> trees;
+  std::vector<uint32_t> tree_log_leaves;
+  uint32_t curr_round = 0;
+  int64_t next_commit;
+  std::vector<uint8_t> unprocessed;  // 16 bytes per challenge
+
+  DevFri(const binius_pcs& p, const binius_pcs_committed& c, cudaStream_t st)
+      : P(p), C(c), s(st), next_commit(p.log_batch) {}
+  ~DevFri() {
+    for (auto w : words) cudaFreeAsync(w, s);
+    for (auto t : trees) cudaFreeAsync(t, s);
+  }
+
+  // FRIFoldProver::execute_fold_round (prover/prover/src/fri/fold.rs:117-175)
+  int execute(bool* committed, uint8_t root[32]) {
+    *committed = false;
+    if (next_commit < 0 || (int64_t)curr_round != next_commit) return BINIUS_OK;
+    const uint32_t n = (uint32_t)(unprocessed.size() / 16);
+    uint4* out = nullptr;
+    uint32_t log_out;
+    if (words.empty()) {
+      log_out = P.rs_log_len();
+      BGPU_CUDA(cudaMallocAsync(&out, 16ull << log_out, s));
+      words.push_back(out);
+      word_log_len.push_back(log_out);
+      if (int rc = binius_fri_fold_interleaved(C.d_codeword, log_out, P.log_batch,
+                                               unprocessed.data(), out, s))
+        return rc;
+    } else {
+      const uint32_t log_prev = word_log_len.back();
+      log_out = log_prev - n;
+      const uint4* prev = words.back();
+      BGPU_CUDA(cudaMallocAsync(&out, 16ull << log_out, s));
+      words.push_back(out);
+      word_log_len.push_back(log_out);
+      if (int rc = binius_fri_fold_codeword(P.ntt, prev, log_prev, unprocessed.data(), n, out, s))
+        return rc;
+    }
+    unprocessed.clear();
+    const size_t idx = words.size() - 1;  // number of rounds committed before this one
+    const bool has_next = idx < P.arities.size();
+    const uint32_t next_arity = has_next ? P.arities[idx] : 0;
+    const uint32_t log_coset = has_next ? next_arity : P.n_final();
+    const uint32_t log_leaves = log_out - log_coset;
+    uint8_t* nodes = nullptr;
+    BGPU_CUDA(cudaMallocAsync(&nodes, 32ull * ((2ull << log_leaves) - 1), s));
+    trees.push_back(nodes);
+    tree_log_leaves.push_back(log_leaves);
+    if (int rc = merkle_commit(out, log_leaves, log_coset, nodes, s)) return rc;
+    BGPU_CUDA(cudaMemcpyAsync(root, nodes + 32 * ((2ull << log_leaves) - 2), 32,
+                              cudaMemcpyDeviceToHost, s));
+    BGPU_CUDA(cudaStreamSynchronize(s));
+    next_commit = has_next ? next_commit + next_arity : -1;
+    *committed = true;
+    return BINIUS_OK;
+  }
+
+  void receive(const uint8_t r[16]) {
+    unprocessed.insert(unprocessed.end(), r, r + 16);
+    curr_round++;
+  }
+
+  void add_branch(std::vector<GatherSegment>& segs, uint64_t& off, const uint8_t* nodes,
+                  uint32_t L, uint64_t index, uint32_t depth) {
+    for (uint32_t j = 0; j < L - depth; j++) {
+      const uint64_t node = layer_off(L, j) | ((index >> j) ^ 1);
+      segs.push_back({nodes + 32 * node, off, 32, 0});
+      off += 32;
+    }
+  }
+
+  // FRIFoldProver::finish_proof (fri/fold.rs:221-244) with FRIQueryProver (fri/query.rs:51-110)
+  int finish(Transcript& t) {
+    {
+      const void* term = words.empty() ? C.d_codeword : words.back();
+      const uint32_t log_term = words.empty() ? C.log_len : word_log_len.back();
+      std::vector<uint8_t> h(16ull << log_term);
+      BGPU_CUDA(cudaMemcpyAsync(h.data(), term, h.size(), cudaMemcpyDeviceToHost, s));
+      BGPU_CUDA(cudaStreamSynchronize(s));
+      t.decommitment(h.data(), h.size());
+    }
+    const auto depths = P.optimal_depths();
+    {
+      std::vector<const uint8_t*> tr{static_cast<const uint8_t*>(C.d_nodes)};
+      std::vector<uint32_t> tl{C.log_leaves};
+      for (size_t i = 0; i + 1 < trees.size(); i++) {
+        tr.push_back(trees[i]);
+        tl.push_back(tree_log_leaves[i]);
+      }
+      for (size_t i = 0; i < tr.size() && i < depths.size(); i++) {
+        const uint32_t d = depths[i], L = tl[i];
+        std::vector<uint8_t> h(32ull << d);
+        const uint8_t* src = tr[i] + 32 * ((2ull << L) - 1 + 1 - (2ull << d));
+        BGPU_CUDA(cudaMemcpyAsync(h.data(), src, h.size(), cudaMemcpyDeviceToHost, s));
+        BGPU_CUDA(cudaStreamSynchronize(s));
+        t.decommitment(h.data(), h.size());
+      }
+    }
+    std::vector<GatherSegment> segs;
+    uint64_t off = 0;
+    const uint8_t* cw = static_cast<const uint8_t*>(C.d_codeword);
+    for (uint32_t q = 0; q < P.n_queries; q++) {
+      uint64_t index = t.sample_bits(P.rs_log_len());
+      segs.push_back({cw + (index << P.log_batch) * 16, off, 16u << P.log_batch, 0});
+      off += 16u << P.log_batch;
+      add_branch(segs, off, static_cast<const uint8_t*>(C.d_nodes), C.log_leaves, index,
+                 depths[0]);
+      for (size_t i = 0; i < words.size() && i < P.arities.size() && i + 1 < depths.size(); i++) {
+        const uint32_t a = P.arities[i];
+        index >>= a;
+        const uint8_t* w = reinterpret_cast<const uint8_t*>(words[i]);
+        segs.push_back({w + (index << a) * 16, off, 16u << a, 0});
+        off += 16u << a;
+        add_branch(segs, off, trees[i], tree_log_leaves[i], index, depths[i + 1]);
+      }
+    }
+    if (off == 0) return BINIUS_OK;
+    GatherSegment* d_segs = nullptr;
+    uint8_t* d_dst = nullptr;
+    BGPU_CUDA(cudaMallocAsync(&d_segs, segs.size() * sizeof(GatherSegment), s));
+    BGPU_CUDA(cudaMallocAsync(&d_dst, off, s));
+    std::vector<uint8_t> h(off);
+    int rc = BINIUS_OK;
+    do {
+      cudaError_t e = cudaMemcpyAsync(d_segs, segs.data(), segs.size() * sizeof(GatherSegment),
+                                      cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) { rc = cuda_error(e, "upload query segments"); break; }
+      if ((rc = gather_segments(d_segs, (uint32_t)segs.size(), d_dst, s))) break;
+      e = cudaMemcpyAsync(h.data(), d_dst, off, cudaMemcpyDeviceToHost, s);
+      if (e != cudaSuccess) { rc = cuda_error(e, "download query openings"); break; }
+      e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) { rc = cuda_error(e, "query gather"); break; }
+    } while (0);
+    cudaFreeAsync(d_segs, s);
+    cudaFreeAsync(d_dst, s);
+    if (rc) return rc;
+    t.decommitment(h.data(), h.size());
+    return BINIUS_OK;
+  }
+};
+
+// TensorAlgebra<B1, B128>::transpose of the 128 x 128 bit matrix whose row k is s[k].
+void transpose128(const u128h in[128], u128h out[128]) {
+  for (int j = 0; j < 128; j++) {
+    u128h v = 0;
+    for (int k = 0; k < 128; k++) v |= (u128h)((in[k] >> j) & 1) << k;
+    out[j] = v;
+  }
+}
+
+int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const void* d_witness,
+                   const uint8_t* h_point, Transcript& t, cudaStream_t s) {
+  const uint32_t n = P->log_msg;
+  const uint64_t N = 1ull << n;
+  uint4 *a = nullptr, *b = nullptr, *eq_r = nullptr;
+  uint32_t* d_small = nullptr;  // 128 elements (ring switch) then 2 (round sums)
+  BGPU_CUDA(cudaMallocAsync(&a, 16 * N, s));
+  BGPU_CUDA(cudaMallocAsync(&b, 16 * N, s));
+  BGPU_CUDA(cudaMallocAsync(&eq_r, 16 * 128, s));
+  BGPU_CUDA(cudaMallocAsync(&d_small, 16 * 128, s));
+  int rc = BINIUS_OK;
+  {
+    DevFri fri(*P, *C, s);
+    do {
+      // suffix tensor of the evaluation point (coordinates 7..) into b
+      if ((rc = eq_tensor(reinterpret_cast<const uint4*>(h_point + 16 * 7), n, b, s))) break;
+      // s_hat_v = fold_1b_rows_for_b128(witness, suffix_tensor)
+      if ((rc = fold_1b_rows(static_cast<const uint4*>(d_witness), b, N, d_small, s))) break;
+      uint8_t s_hat_v[128 * 16];
+      cudaError_t e = cudaMemcpyAsync(s_hat_v, d_small, sizeof(s_hat_v), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) { rc = cuda_error(e, "ring switch fold"); break; }
+      t.message(s_hat_v, sizeof(s_hat_v));
+      u128h v[128], u[128];
+      for (int k = 0; k < 128; k++) v[k] = to_u128(s_hat_v + 16 * k);
+      transpose128(v, u);
+      uint8_t r_dp[7 * 16];
+      for (int i = 0; i < 7; i++) t.sample_elem(r_dp + 16 * i);
+      if ((rc = eq_tensor(reinterpret_cast<const uint4*>(r_dp), 7, eq_r, s))) break;
+      uint8_t h_eq[128 * 16];
+      e = cudaMemcpyAsync(h_eq, eq_r, sizeof(h_eq), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) { rc = cuda_error(e, "eq(r'')"); break; }
+      u128h sum = 0;
+      for (int j = 0; j < 128; j++) sum ^= host_gf_mul(u[j], to_u128(h_eq + 16 * j));
+      // rs_eq_ind = fold_b128_elems_inplace(suffix_tensor, eq(r'')) in place in b
+      if ((rc = fold_b128_elems(b, b, N, eq_r, s))) break;
+      e = cudaMemcpyAsync(a, d_witness, 16 * N, cudaMemcpyDeviceToDevice, s);
+      if (e != cudaSuccess) { rc = cuda_error(e, "copy witness"); break; }
+
+      // BaseFold rounds
+      uint8_t r_prev[16];
+      for (uint32_t round = 0; round < n && rc == BINIUS_OK; round++) {
+        const uint64_t size = N >> round;
+        if (round == 0)
+          rc = bivariate_eval(a, b, size / 2, d_small, s);
+        else
+          rc = bivariate_fold_eval(a, b, size * 2, r_prev, d_small, s);
+        if (rc) break;
+        uint8_t ys[32];
+        e = cudaMemcpyAsync(ys, d_small, 32, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { rc = cuda_error(e, "round sums"); break; }
+        const u128h y1 = to_u128(ys), yinf = to_u128(ys + 16);
+        const u128h c0 = sum ^ y1, c2 = yinf, c1 = y1 ^ c0 ^ c2;
+        bool committed = false;
+        uint8_t root[32];
+        if ((rc = fri.execute(&committed, root))) break;
+        uint8_t coeffs[32];
+        from_u128(c0, coeffs);
+        from_u128(c1, coeffs + 16);
+        t.message(coeffs, 32);
+        if (committed) t.message(root, 32);
+        t.sample_elem(r_prev);
+        const u128h r = to_u128(r_prev);
+        sum = c0 ^ host_gf_mul(c1, r) ^ host_gf_mul(c2, host_gf_mul(r, r));
+        fri.receive(r_prev);
+      }
+      if (rc) break;
+      bool committed = false;
+      uint8_t root[32];
+      if ((rc = fri.execute(&committed, root))) break;
+      if (committed) t.message(root, 32);
+      rc = fri.finish(t);
+    } while (0);
+  }
+  cudaFreeAsync(a, s);
+  cudaFreeAsync(b, s);
+  cudaFreeAsync(eq_r, s);
+  cudaFreeAsync(d_small, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (rc == BINIUS_OK && e != cudaSuccess) rc = cuda_error(e, "pcs prove");
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int binius_pcs_create(const binius_ntt* ntt, uint32_t log_msg, uint32_t log_batch,
+                      uint32_t log_inv_rate, const uint32_t* arities, uint32_t n_arities,
+                      uint32_t n_queries, binius_pcs** out) {
+  BGPU_ARG(out != nullptr && ntt != nullptr, "NULL argument");
+  *out = nullptr;
+  BGPU_ARG(log_batch <= log_msg && log_batch <= 8, "log_batch must be <= log_msg and <= 8");
+  BGPU_ARG(log_msg <= 32, "log_msg too large");
+  BGPU_ARG(n_arities == 0 || arities != nullptr, "arities is NULL");
+  BGPU_ARG(n_queries >= 1, "n_queries must be positive");
+  uint32_t sum = 0;
+  for (uint32_t i = 0; i < n_arities; i++) {
+    BGPU_ARG(arities[i] >= 1 && arities[i] <= 8, "fold arities must be in [1, 8]");
+    sum += arities[i];
+  }
+  BGPU_ARG(sum <= log_msg - log_batch, "InvalidFoldAritySequence: arities exceed log_dim");
+  BGPU_ARG(log_msg - log_batch + log_inv_rate <= ntt->log_domain,
+           "NTT domain smaller than the RS code");
+  binius_pcs* p = new binius_pcs();
+  p->ntt = ntt;
+  p->log_msg = log_msg;
+  p->log_batch = log_batch;
+  p->log_inv_rate = log_inv_rate;
+  p->n_queries = n_queries;
+  p->arities.assign(arities, arities + n_arities);
+  *out = p;
+  return clear_error();
+}
+
+int binius_pcs_destroy(binius_pcs* pcs) {
+  delete pcs;
+  return BINIUS_OK;
+}
+
+int binius_pcs_commit(const binius_pcs* P, const void* d_witness, binius_pcs_committed** out,
+                      void* h_root, void* stream) {
+  BGPU_ARG(P != nullptr && d_witness != nullptr && out != nullptr, "NULL argument");
+  *out = nullptr;
+  cudaStream_t s = as_stream(stream);
+  binius_pcs_committed* c = new binius_pcs_committed();
+  BGPU_CUDA(cudaGetDevice(&c->device));
+  c->log_len = P->log_len();
+  c->log_leaves = P->rs_log_len();
+  c->d_codeword = nullptr;
+  c->d_nodes = nullptr;
+  int rc = BINIUS_OK;
+  do {
+    cudaError_t e = cudaMalloc(&c->d_codeword, 16ull << c->log_len);
+    if (e != cudaSuccess) { rc = cuda_error(e, "cudaMalloc(codeword)"); break; }
+    e = cudaMalloc(&c->d_nodes, 32ull * ((2ull << c->log_leaves) - 1));
+    if (e != cudaSuccess) { rc = cuda_error(e, "cudaMalloc(tree)"); break; }
+    if ((rc = binius_fri_commit_interleaved(P->ntt, d_witness, P->log_dim(), P->log_inv_rate,
+                                            P->log_batch, c->d_codeword, c->d_nodes, c->root,
+                                            stream)))
+      break;
+  } while (0);
+  if (rc) {
+    if (c->d_codeword) cudaFree(c->d_codeword);
+    if (c->d_nodes) cudaFree(c->d_nodes);
+    delete c;
+    return rc;
+  }
+  (void)s;
+  if (h_root) memcpy(h_root, c->root, 32);
+  *out = c;
+  return clear_error();
+}
+
+int binius_pcs_committed_destroy(binius_pcs_committed* c) {
+  if (!c) return BINIUS_OK;
+  cudaFree(c->d_codeword);
+  cudaFree(c->d_nodes);
+  delete c;
+  return BINIUS_OK;
+}
+
+const void* binius_pcs_committed_codeword(const binius_pcs_committed* c) {
+  return c ? c->d_codeword : nullptr;
+}
+
+int binius_pcs_prove(const binius_pcs* P, const binius_pcs_committed* C, const void* d_witness,
+                     const void* h_eval_point, binius_transcript* transcript, void* stream) {
+  BGPU_ARG(P && C && d_witness && h_eval_point && transcript, "NULL argument");
+  BGPU_ARG(C->log_len == P->log_len(), "commitment does not match the PCS parameters");
+  int rc = pcs_prove_impl(P, C, d_witness, static_cast<const uint8_t*>(h_eval_point),
+                          transcript->t, as_stream(stream));
+  return rc ? rc : clear_error();
+}
+
+}  // extern "C"

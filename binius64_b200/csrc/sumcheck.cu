@@ -1,0 +1,306 @@
+// Multilinear / sumcheck kernels of the PCS opening and the reductions.
+//
+// * eq tensor (eq_ind_partial_eval, verifier/math/src/multilinear/eq.rs:39-71): coordinate i
+//   selects index bit i; built as lo[i & mask] * hi[i >> k] from two small tensors (one multiply
+//   per output; the product order does not change the field value).
+// * ring-switch row fold (fold_1b_rows_for_b128, prover/prover/src/ring_switch.rs:197-265):
+//   out[k] = sum_i bit_k(mat[i]) * vec[i] for the 128 bit columns k.  A CTA of 128 threads gives
+//   one column to each thread, streams rows through shared memory and XOR-accumulates the masked
+//   vector entries; CTA partials meet in global memory through atomicXor (addition in GF(2^128)).
+// * element fold (fold_b128_elems_inplace, ring_switch.rs:130-171): x -> sum_k bit_k(x) * vec[k]
+//   through 16 byte-indexed tables of 256 subset sums held in shared memory.
+// * bivariate product round (BivariateProductSumcheckProver::execute / fold,
+//   prover/prover/src/protocols/sumcheck/bivariate_product.rs:43-95): y_1 = sum a_hi*b_hi,
+//   y_inf = sum (a_lo + a_hi)(b_lo + b_hi), the top variable is folded by
+//   fold_highest_var_inplace (multilinear/fold.rs:14-29).  The fold by the previous challenge and
+//   the next round's evaluation run in one pass; products accumulate unreduced (256-bit) and are
+//   reduced once per thread.
+#include <string.h>
+
+#include <algorithm>
+
+#include "gf128.cuh"
+#include "internal.h"
+#include "kernels.h"
+
+using namespace bgpu;
+
+namespace {
+
+constexpr int kThreads = 256;
+
+unsigned grid_for(uint64_t n, unsigned threads, unsigned max_blocks = 148 * 8) {
+  uint64_t g = (n + threads - 1) / threads;
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, max_blocks));
+}
+
+__device__ __forceinline__ void atomic_xor_gf(uint32_t* dst, uint4 v) {
+  if (v.x) atomicXor(dst + 0, v.x);
+  if (v.y) atomicXor(dst + 1, v.y);
+  if (v.z) atomicXor(dst + 2, v.z);
+  if (v.w) atomicXor(dst + 3, v.w);
+}
+
+__device__ __forceinline__ uint4 shfl_xor_gf(uint4 v, int lane_mask) {
+  v.x = __shfl_xor_sync(0xffffffffu, v.x, lane_mask);
+  v.y = __shfl_xor_sync(0xffffffffu, v.y, lane_mask);
+  v.z = __shfl_xor_sync(0xffffffffu, v.z, lane_mask);
+  v.w = __shfl_xor_sync(0xffffffffu, v.w, lane_mask);
+  return v;
+}
+
+// XOR-reduces `nv` field values across the CTA and adds the totals into dst[0..nv).
+template <int NV>
+__device__ __forceinline__ void block_xor_reduce(uint4 (&v)[NV], uint32_t* dst) {
+  __shared__ uint4 red[NV][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; q++) {
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) gf_add_into(v[q], shfl_xor_gf(v[q], m));
+    if (lane == 0) red[q][warp] = v[q];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nwarps = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; q++) {
+      uint4 x = lane < nwarps ? red[q][lane] : gf_zero();
+#pragma unroll
+      for (int m = 16; m >= 1; m >>= 1) gf_add_into(x, shfl_xor_gf(x, m));
+      if (lane == 0) atomic_xor_gf(dst + 4 * q, x);
+    }
+  }
+}
+
+__global__ void eq_small_kernel(uint4* __restrict__ out, Point32 p, uint32_t off, uint32_t n) {
+  const uint64_t total = 1ull << n;
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < total;
+       j += (uint64_t)gridDim.x * blockDim.x) {
+    uint4 acc = gf_one();
+    for (uint32_t i = 0; i < n; i++) {
+      uint4 f = p.r[off + i];
+      if (!((j >> i) & 1)) f.x ^= 1u;
+      acc = gf_mul(acc, f);
+    }
+    out[j] = acc;
+  }
+}
+
+__global__ void eq_expand_kernel(uint4* __restrict__ out, const uint4* __restrict__ lo,
+                                 const uint4* __restrict__ hi, uint32_t k, uint64_t total) {
+  const uint64_t mask = (1ull << k) - 1;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = gf_mul(__ldg(lo + (i & mask)), __ldg(hi + (i >> k)));
+}
+
+constexpr int kRowTile = 256;
+
+__global__ void __launch_bounds__(128)
+    fold_rows_kernel(const uint4* __restrict__ mat, const uint4* __restrict__ vec, uint64_t n,
+                     uint32_t* __restrict__ out) {
+  __shared__ uint32_t s_mat[kRowTile][4];
+  __shared__ uint4 s_vec[kRowTile];
+  const uint32_t k = threadIdx.x;  // bit column
+  const uint32_t word = k >> 5, bit = k & 31;
+  uint4 acc = gf_zero();
+  for (uint64_t base = (uint64_t)blockIdx.x * kRowTile; base < n;
+       base += (uint64_t)gridDim.x * kRowTile) {
+    const uint32_t rows = (uint32_t)((n - base) < (uint64_t)kRowTile ? (n - base) : (uint64_t)kRowTile);
+    __syncthreads();
+    for (uint32_t r = threadIdx.x; r < rows; r += blockDim.x) {
+      uint4 m = __ldg(mat + base + r);
+      s_mat[r][0] = m.x;
+      s_mat[r][1] = m.y;
+      s_mat[r][2] = m.z;
+      s_mat[r][3] = m.w;
+      s_vec[r] = __ldg(vec + base + r);
+    }
+    __syncthreads();
+    for (uint32_t r = 0; r < rows; r++) {
+      const uint32_t msk = 0u - ((s_mat[r][word] >> bit) & 1u);
+      const uint4 v = s_vec[r];
+      acc.x ^= v.x & msk;
+      acc.y ^= v.y & msk;
+      acc.z ^= v.z & msk;
+      acc.w ^= v.w & msk;
+    }
+  }
+  atomic_xor_gf(out + 4 * k, acc);
+}
+
+// tables[p][b] = sum over the set bits j of b of vec[8p + j].
+__global__ void build_fold_tables_kernel(const uint4* __restrict__ vec, uint4* __restrict__ tables) {
+  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= 16 * 256) return;
+  const uint32_t p = idx >> 8, b = idx & 255;
+  uint4 acc = gf_zero();
+  for (uint32_t j = 0; j < 8; j++)
+    if ((b >> j) & 1) gf_add_into(acc, vec[8 * p + j]);
+  tables[idx] = acc;
+}
+
+__device__ __forceinline__ uint32_t byte_of(uint4 v, uint32_t p) {
+  const uint32_t w = p < 4 ? v.x : p < 8 ? v.y : p < 12 ? v.z : v.w;
+  return (w >> (8 * (p & 3))) & 255u;
+}
+
+__global__ void __launch_bounds__(kThreads)
+    fold_elems_kernel(const uint4* __restrict__ in, uint4* __restrict__ out, uint64_t n,
+                      const uint4* __restrict__ tables) {
+  extern __shared__ uint4 s_tab[];  // 16 x 256
+  for (uint32_t i = threadIdx.x; i < 16 * 256; i += blockDim.x) s_tab[i] = tables[i];
+  __syncthreads();
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint4 x = in[i];
+    uint4 acc = gf_zero();
+#pragma unroll
+    for (uint32_t p = 0; p < 16; p++) gf_add_into(acc, s_tab[(p << 8) | byte_of(x, p)]);
+    out[i] = acc;
+  }
+}
+
+// Round evaluation on (a, b) of length 2*half, no fold.
+__global__ void __launch_bounds__(kThreads)
+    bivariate_eval_kernel(const uint4* __restrict__ a, const uint4* __restrict__ b, uint64_t half,
+                          uint32_t* __restrict__ out) {
+  u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < half;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint4 a0 = a[i], a1 = a[half + i], b0 = b[i], b1 = b[half + i];
+    xor_into(s1, clmul128(a1, b1));
+    xor_into(sinf, clmul128(gf_add(a0, a1), gf_add(b0, b1)));
+  }
+  uint4 v[2] = {reduce256(s1), reduce256(sinf)};
+  block_xor_reduce<2>(v, out);
+}
+
+// Folds (a, b) of length `size` by r in place (a[i] = a[i] + r (a[i + size/2] - a[i])) and
+// evaluates the next round on the folded length-size/2 arrays.  Thread j owns folded positions j
+// and j + size/4, so no two threads touch the same element.
+__global__ void __launch_bounds__(kThreads)
+    bivariate_fold_eval_kernel(uint4* __restrict__ a, uint4* __restrict__ b, uint64_t size, uint4 r,
+                               uint32_t* __restrict__ out) {
+  const uint64_t h = size >> 1, q = size >> 2;
+  u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < q;
+       j += (uint64_t)gridDim.x * blockDim.x) {
+    uint4 a_lo = a[j], a_hi = a[h + j], a_lo2 = a[q + j], a_hi2 = a[h + q + j];
+    uint4 b_lo = b[j], b_hi = b[h + j], b_lo2 = b[q + j], b_hi2 = b[h + q + j];
+    uint4 fa0 = gf_add(a_lo, gf_mul(r, gf_add(a_hi, a_lo)));
+    uint4 fa1 = gf_add(a_lo2, gf_mul(r, gf_add(a_hi2, a_lo2)));
+    uint4 fb0 = gf_add(b_lo, gf_mul(r, gf_add(b_hi, b_lo)));
+    uint4 fb1 = gf_add(b_lo2, gf_mul(r, gf_add(b_hi2, b_lo2)));
+    a[j] = fa0;
+    a[q + j] = fa1;
+    b[j] = fb0;
+    b[q + j] = fb1;
+    xor_into(s1, clmul128(fa1, fb1));
+    xor_into(sinf, clmul128(gf_add(fa0, fa1), gf_add(fb0, fb1)));
+  }
+  uint4 v[2] = {reduce256(s1), reduce256(sinf)};
+  block_xor_reduce<2>(v, out);
+}
+
+__global__ void gather_segments_kernel(const GatherSegment* __restrict__ segs, uint32_t n,
+                                       uint8_t* __restrict__ dst) {
+  for (uint32_t s = blockIdx.x; s < n; s += gridDim.x) {
+    const GatherSegment g = segs[s];
+    const uint4* src = reinterpret_cast<const uint4*>(g.src);
+    uint4* d = reinterpret_cast<uint4*>(dst + g.dst_off);
+    for (uint32_t i = threadIdx.x; i < g.bytes / 16; i += blockDim.x) d[i] = src[i];
+  }
+}
+
+}  // namespace
+
+namespace bgpu {
+
+int eq_tensor(const uint4* h_point, uint32_t n, uint4* d_out, cudaStream_t s) {
+  if (n > 32) return set_error(BINIUS_E_ARG, "eq tensor: at most 32 coordinates");
+  Point32 p;
+  memset(&p, 0, sizeof(p));
+  if (n) memcpy(p.r, h_point, 16 * (size_t)n);
+  if (n <= 12) {
+    eq_small_kernel<<<grid_for(1ull << n, kThreads), kThreads, 0, s>>>(d_out, p, 0, n);
+    BGPU_LAUNCH_CHECK("eq_small_kernel");
+    count_launch();
+    return BINIUS_OK;
+  }
+  const uint32_t k = n / 2;
+  uint4* tmp = nullptr;
+  const uint64_t nlo = 1ull << k, nhi = 1ull << (n - k);
+  BGPU_CUDA(cudaMallocAsync(&tmp, 16 * (nlo + nhi), s));
+  eq_small_kernel<<<grid_for(nlo, kThreads), kThreads, 0, s>>>(tmp, p, 0, k);
+  eq_small_kernel<<<grid_for(nhi, kThreads), kThreads, 0, s>>>(tmp + nlo, p, k, n - k);
+  eq_expand_kernel<<<grid_for(1ull << n, kThreads, 148 * 16), kThreads, 0, s>>>(d_out, tmp, tmp + nlo,
+                                                                              k, 1ull << n);
+  cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(tmp, s);
+  if (e != cudaSuccess) return cuda_error(e, "eq tensor kernels");
+  count_launch(3);
+  return BINIUS_OK;
+}
+
+int fold_1b_rows(const uint4* d_mat, const uint4* d_vec, uint64_t n, uint32_t* d_out512,
+                 cudaStream_t s) {
+  BGPU_CUDA(cudaMemsetAsync(d_out512, 0, 128 * 16, s));
+  unsigned blocks = (unsigned)std::max<uint64_t>(
+      1, std::min<uint64_t>((n + kRowTile - 1) / kRowTile, 148 * 4));
+  fold_rows_kernel<<<blocks, 128, 0, s>>>(d_mat, d_vec, n, d_out512);
+  BGPU_LAUNCH_CHECK("fold_rows_kernel");
+  count_launch();
+  return BINIUS_OK;
+}
+
+int fold_b128_elems(const uint4* d_in, uint4* d_out, uint64_t n, const uint4* d_vec128,
+                    cudaStream_t s) {
+  uint4* tables = nullptr;
+  BGPU_CUDA(cudaMallocAsync(&tables, 16 * 16 * 256, s));
+  build_fold_tables_kernel<<<16, 256, 0, s>>>(d_vec128, tables);
+  const size_t smem = 16 * 256 * sizeof(uint4);
+  cudaError_t e =
+      cudaFuncSetAttribute(fold_elems_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) {
+    fold_elems_kernel<<<grid_for(n, kThreads, 148 * 2), kThreads, smem, s>>>(d_in, d_out, n, tables);
+    e = cudaGetLastError();
+  }
+  cudaFreeAsync(tables, s);
+  if (e != cudaSuccess) return cuda_error(e, "fold_elems_kernel");
+  count_launch(2);
+  return BINIUS_OK;
+}
+
+int bivariate_eval(const uint4* d_a, const uint4* d_b, uint64_t half, uint32_t* d_out8,
+                   cudaStream_t s) {
+  BGPU_CUDA(cudaMemsetAsync(d_out8, 0, 32, s));
+  bivariate_eval_kernel<<<grid_for(half, kThreads), kThreads, 0, s>>>(d_a, d_b, half, d_out8);
+  BGPU_LAUNCH_CHECK("bivariate_eval_kernel");
+  count_launch();
+  return BINIUS_OK;
+}
+
+int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[16],
+                        uint32_t* d_out8, cudaStream_t s) {
+  if (size < 4) return set_error(BINIUS_E_ARG, "bivariate_fold_eval needs size >= 4");
+  uint4 rv;
+  memcpy(&rv, r, 16);
+  BGPU_CUDA(cudaMemsetAsync(d_out8, 0, 32, s));
+  bivariate_fold_eval_kernel<<<grid_for(size / 4, kThreads), kThreads, 0, s>>>(d_a, d_b, size, rv,
+                                                                            d_out8);
+  BGPU_LAUNCH_CHECK("bivariate_fold_eval_kernel");
+  count_launch();
+  return BINIUS_OK;
+}
+
+int gather_segments(const GatherSegment* d_segs, uint32_t n, uint8_t* d_dst, cudaStream_t s) {
+  if (n == 0) return BINIUS_OK;
+  gather_segments_kernel<<<std::min<uint32_t>(n, 148 * 16), 64, 0, s>>>(d_segs, n, d_dst);
+  BGPU_LAUNCH_CHECK("gather_segments_kernel");
+  count_launch();
+  return BINIUS_OK;
+}
+
+}  // namespace bgpu

@@ -134,6 +134,58 @@ int binius_fri_commit_interleaved(const binius_ntt* ntt, const void* d_msg, uint
                                   void* d_nodes, void* h_root, void* stream);
 
 /* ------------------------------------------------------------------------------------------
+ * Fiat-Shamir transcript: ProverTranscript<HasherChallenger<Sha256>>.
+ * Replaces: ProverTranscript (verifier/transcript/src/transcript.rs:204-327), HasherChallenger
+ * (verifier/transcript/src/fiat_shamir/hasher_challenger.rs:14-200), sample_bits_reader
+ * (fiat_shamir/sampling.rs:34-50).  Host-side state; the proof is the tape of message() and
+ * decommitment() bytes (ProverTranscript::finalize).
+ * ------------------------------------------------------------------------------------------ */
+typedef struct binius_transcript binius_transcript;
+
+int binius_transcript_create(binius_transcript** out);
+int binius_transcript_destroy(binius_transcript* t);
+/* message(): written to the proof and observed by the challenger. */
+int binius_transcript_message(binius_transcript* t, const void* h_bytes, size_t n);
+/* decommitment(): written to the proof only. */
+int binius_transcript_decommitment(binius_transcript* t, const void* h_bytes, size_t n);
+/* observe(): observed only (switches the challenger to observing even when n == 0). */
+int binius_transcript_observe(binius_transcript* t, const void* h_bytes, size_t n);
+/* n sampled bytes; a B128 challenge is 16 bytes read as a little-endian u128. */
+int binius_transcript_sample(binius_transcript* t, void* h_out, size_t n);
+uint32_t binius_transcript_sample_bits(binius_transcript* t, uint32_t bits);
+size_t binius_transcript_len(const binius_transcript* t);
+int binius_transcript_finalize(const binius_transcript* t, void* h_out, size_t cap, size_t* len);
+
+/* ------------------------------------------------------------------------------------------
+ * 1-bit multilinear PCS (ring switching + BaseFold + FRI).
+ * Replaces: OneBitPCSProver::{new, commit, prove} (prover/prover/src/pcs.rs:58-169) with
+ * ring_switch::{fold_1b_rows_for_b128, fold_b128_elems_inplace} (ring_switch.rs:130-265),
+ * BaseFoldProver (protocols/basefold.rs:33-166), FRIFoldProver / FRIQueryProver
+ * (fri/fold.rs:30-244, fri/query.rs:18-134).
+ * FRI parameters as FRIParams::new (verifier/verifier/src/fri/common.rs:35-57): the message is
+ * 2^log_msg packed B128 elements (the B1 multilinear has log_msg + 7 variables).  The NTT must be
+ * the RS code's domain (dimension >= log_msg - log_batch + log_inv_rate).
+ * ------------------------------------------------------------------------------------------ */
+typedef struct binius_pcs binius_pcs;
+typedef struct binius_pcs_committed binius_pcs_committed;
+
+int binius_pcs_create(const binius_ntt* ntt, uint32_t log_msg, uint32_t log_batch,
+                      uint32_t log_inv_rate, const uint32_t* arities, uint32_t n_arities,
+                      uint32_t n_queries, binius_pcs** out);
+int binius_pcs_destroy(binius_pcs* pcs);
+/* RS encode + Merkle commit of d_witness (2^log_msg elements); the codeword and tree stay on the
+ * device in *out; h_root receives the 32-byte commitment.  Synchronous. */
+int binius_pcs_commit(const binius_pcs* pcs, const void* d_witness, binius_pcs_committed** out,
+                      void* h_root, void* stream);
+int binius_pcs_committed_destroy(binius_pcs_committed* committed);
+const void* binius_pcs_committed_codeword(const binius_pcs_committed* committed);
+/* Proves the evaluation of the committed B1 multilinear at h_eval_point (log_msg + 7 field
+ * elements), appending the proof to `transcript`.  Synchronous. */
+int binius_pcs_prove(const binius_pcs* pcs, const binius_pcs_committed* committed,
+                     const void* d_witness, const void* h_eval_point,
+                     binius_transcript* transcript, void* stream);
+
+/* ------------------------------------------------------------------------------------------
  * FRI parameters (verifier/verifier/src/fri/common.rs:64-219).
  * ------------------------------------------------------------------------------------------ */
 uint32_t binius_fri_n_test_queries(uint32_t security_bits, uint32_t log_inv_rate);

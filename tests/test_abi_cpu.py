@@ -75,3 +75,48 @@ def test_fri_params_choice_matches_reference_formula():
     assert p.fold_arities == [4, 4]
     assert p.n_test_queries == 232
     assert p.log_terminal_dim == 7
+
+
+def test_library_transcript_known_answers():
+    """The library's host transcript against hasher_challenger.rs:209-280's chaining structure."""
+    import hashlib
+
+    import numpy as np
+
+    import binius64_b200 as bg
+    d0 = hashlib.sha256(b"").digest()
+    t = bg.ProverTranscript()
+    assert t.sample_bytes(8) == d0[:8]
+    assert t.sample_bytes(24) == d0[8:]
+    t.observe(bytes([0x48, 0x55]))
+    assert t.sample_bytes(2) == hashlib.sha256(d0 + bytes([32] + [0] * 7) + bytes([0x48, 0x55])).digest()[:2]
+
+    rng = np.random.default_rng(0)
+    obs = rng.integers(0, 256, 1019, dtype=np.uint8).tobytes()
+    t = bg.ProverTranscript()
+    t.message(obs[:300])
+    t.decommitment(b"not observed")
+    t.message(obs[300:])
+    first = hashlib.sha256(d0 + bytes(8) + obs).digest()
+    assert t.sample_bytes(7) == first[:7]
+    assert t.finalize() == obs[:300] + b"not observed" + obs[300:]
+    # sample_bits: u32 LE of the next 4 bytes, masked
+    v = t.sample_bits(5)
+    assert v == int.from_bytes(first[7:11], "little") & 31
+
+
+def test_library_transcript_matches_oracle_transcript():
+    import numpy as np
+
+    import binius64_b200 as bg
+    import oracle as orc
+    rng = np.random.default_rng(5)
+    a, b = bg.ProverTranscript(), orc.Transcript()
+    for step in range(40):
+        if rng.integers(0, 2):
+            data = rng.integers(0, 256, int(rng.integers(1, 200)), dtype=np.uint8).tobytes()
+            a.message(data)
+            b.observe(data)
+        else:
+            n = int(rng.integers(1, 80))
+            assert a.sample_bytes(n) == b.sample(n), step
