@@ -86,6 +86,16 @@ def lib():
                                      _u32p, ctypes.c_uint32, ctypes.c_uint32, _u64p, _u64p, _u8p,
                                      ctypes.c_size_t]
         L.orc_pcs_verify.restype = ctypes.c_int
+        L.orc_shifted_word.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32]
+        L.orc_shifted_word.restype = ctypes.c_uint64
+        L.orc_and_univariate_round.argtypes = [_u64p, _u64p, _u64p, ctypes.c_uint32, _u64p, _u64p]
+        L.orc_and_fold_words.argtypes = [_u64p, ctypes.c_size_t, _u64p, _u64p]
+        L.orc_and_reduction_prove.argtypes = [_u64p, _u64p, _u64p, ctypes.c_uint32, _u8p,
+                                              ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t),
+                                              _u64p, _u64p]
+        L.orc_and_reduction_prove.restype = ctypes.c_int
+        L.orc_and_reduction_verify.argtypes = [ctypes.c_uint32, _u8p, ctypes.c_size_t, _u64p, _u64p]
+        L.orc_and_reduction_verify.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -323,3 +333,55 @@ def pcs_verify(twiddles, log_msg, log_batch, log_inv_rate, arities, n_queries, e
     return int(lib().orc_pcs_verify(_p64(twiddles), log_msg, log_batch, log_inv_rate, arp,
                                     len(arities), n_queries, _p64(pt), _p64(cl), _p8(pr),
                                     len(proof)))
+
+
+def shifted_word(w: int, variant: int, amount: int) -> int:
+    return int(lib().orc_shifted_word(w, variant, amount))
+
+
+def and_univariate_round(a, b, c, big) -> np.ndarray:
+    a, b, c = (np.ascontiguousarray(x, dtype=np.uint64) for x in (a, b, c))
+    log_n = a.shape[0].bit_length() - 1
+    big = np.ascontiguousarray(big, dtype=np.uint64).reshape(-1, 2)
+    out = elems(64)
+    lib().orc_and_univariate_round(_p64(a), _p64(b), _p64(c), log_n,
+                                   _p64(big) if big.shape[0] else None, _p64(out))
+    return out
+
+
+def and_fold_words(w, z) -> np.ndarray:
+    w = np.ascontiguousarray(w, dtype=np.uint64)
+    zz = np.ascontiguousarray(z, dtype=np.uint64).reshape(2)
+    out = elems(w.shape[0])
+    lib().orc_and_fold_words(_p64(w), w.shape[0], _p64(zz), _p64(out))
+    return out
+
+
+def and_reduction_prove(a, b, c):
+    """Returns (proof bytes, (a_eval, b_eval, c_eval, z), eval_point) on a fresh transcript."""
+    a, b, c = (np.ascontiguousarray(x, dtype=np.uint64) for x in (a, b, c))
+    log_n = a.shape[0].bit_length() - 1
+    cap = 1 << 20
+    out = np.zeros(cap, dtype=np.uint8)
+    n = ctypes.c_size_t(0)
+    meta = elems(4)
+    point = elems(log_n)
+    rc = lib().orc_and_reduction_prove(_p64(a), _p64(b), _p64(c), log_n, _p8(out), cap,
+                                       ctypes.byref(n), _p64(meta), _p64(point))
+    assert rc == 0
+    return out[: n.value].tobytes(), meta, point
+
+
+def and_reduction_verify(log_n: int, proof: bytes):
+    pr = np.frombuffer(proof, dtype=np.uint8).copy()
+    meta = elems(4)
+    point = elems(log_n)
+    rc = lib().orc_and_reduction_verify(log_n, _p8(pr), len(proof), _p64(meta), _p64(point))
+    return rc, meta, point
+
+
+def mle_eval(values: np.ndarray, point: np.ndarray) -> np.ndarray:
+    """Multilinear evaluation sum_i values[i] eq(point)[i] (point[j] <-> index bit j)."""
+    eq = eq_ind_partial_eval(point)
+    prods = gf_mul_vec(np.ascontiguousarray(values, dtype=np.uint64), eq)
+    return np.bitwise_xor.reduce(prods, axis=0)

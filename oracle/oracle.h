@@ -100,6 +100,17 @@ int orc_pcs_verify(const uint64_t* twiddles, uint32_t log_msg, uint32_t log_batc
                    uint32_t n_queries, const uint64_t* eval_point, const uint64_t* claim,
                    const uint8_t* proof, size_t proof_len);
 
+/* ---- Operands and the AND reduction (prover/prover/src/and_reduction/*, prove.rs:329-372) ---- */
+uint64_t orc_shifted_word(uint64_t w, uint32_t variant, uint32_t amount);
+void orc_and_univariate_round(const uint64_t* a, const uint64_t* b, const uint64_t* c,
+                              uint32_t log_n, const uint64_t* big, uint64_t* msg_out);
+void orc_and_fold_words(const uint64_t* w, size_t n, const uint64_t* z, uint64_t* out);
+int orc_and_reduction_prove(const uint64_t* a, const uint64_t* b, const uint64_t* c,
+                            uint32_t log_n, uint8_t* proof_out, size_t cap, size_t* len,
+                            uint64_t* out_meta, uint64_t* out_point);
+int orc_and_reduction_verify(uint32_t log_n, const uint8_t* proof, size_t len, uint64_t* out_meta,
+                             uint64_t* out_point);
+
 /* Number of worker threads the oracle may use (1 = scalar). */
 void orc_set_threads(int n);
 
