@@ -442,3 +442,55 @@ class OneBitPCSProver:
             except Exception:
                 pass
             self._h = None
+
+
+class DeviceConstraintSystem:
+    """A constraint system parsed from the reference's v2 wire format and uploaded to the device
+    (ConstraintSystem::deserialize + validate_and_prepare)."""
+
+    def __init__(self, cs_bytes: bytes, device: int | None = None):
+        torch = _torch()
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        self._h = ctypes.c_void_p()
+        check(lib().binius_cs_from_bytes(self.device, cs_bytes, len(cs_bytes), ctypes.byref(self._h)))
+        info = (ctypes.c_uint32 * 12)()
+        check(lib().binius_cs_info(self._h, ctypes.addressof(info)))
+        (self.n_const, self.n_inout, self.n_witness, self.n_internal, self.offset_inout,
+         self.offset_witness, self.committed_total_len, self.n_scratch, self.n_and, self.n_mul,
+         self.n_and_real, self.n_mul_real) = list(info)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def eval_operands(self, witness_words, which: int = 0, stream=None):
+        torch = _torch()
+        k, n = (3, self.n_and) if which == 0 else (4, self.n_mul)
+        out = torch.empty(k * n, dtype=torch.int64, device=witness_words.device)
+        check(lib().binius_eval_operands(self._h, witness_words.data_ptr(), which, out.data_ptr(),
+                                         _stream(stream)))
+        return out.view(k, n)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().binius_cs_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
+def and_reduction_prove(cs: DeviceConstraintSystem, witness_words, transcript: ProverTranscript,
+                        stream=None):
+    """prove_bitand_reduction: returns ((a_eval, b_eval, c_eval, z), eval_point) as ints."""
+    log_n = cs.n_and.bit_length() - 1
+    meta = (ctypes.c_uint8 * 64)()
+    point = (ctypes.c_uint8 * (16 * log_n))()
+    check(lib().binius_and_reduction_prove(cs.handle, witness_words.data_ptr(), transcript.handle,
+                                           ctypes.addressof(meta), ctypes.addressof(point),
+                                           _stream(stream)))
+    mb, pb = bytes(meta), bytes(point)
+    m = [int.from_bytes(mb[16 * i:16 * i + 16], "little") for i in range(4)]
+    p = [int.from_bytes(pb[16 * i:16 * i + 16], "little") for i in range(log_n)]
+    return m, p

@@ -74,6 +74,11 @@ _SIGS = {
     "binius_pcs_committed_destroy": (_int, [_vp]),
     "binius_pcs_committed_codeword": (_vp, [_vp]),
     "binius_pcs_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "binius_cs_from_bytes": (_int, [_int, _c.c_char_p, _c.c_size_t, _c.POINTER(_vp)]),
+    "binius_cs_destroy": (_int, [_vp]),
+    "binius_cs_info": (_int, [_vp, _vp]),
+    "binius_eval_operands": (_int, [_vp, _vp, _int, _vp, _vp]),
+    "binius_and_reduction_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "binius_fri_n_test_queries": (_u32, [_u32, _u32]),
     "binius_fri_estimate_optimal_arity": (_u32, [_u32, _u32, _u32]),
     "binius_gf_mul_batch": (_int, [_vp, _vp, _vp, _u64, _vp]),

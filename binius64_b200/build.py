@@ -14,6 +14,7 @@ LIB = os.path.join(PKG, "libbinius_gpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
+         "-Xcompiler", "-mpclmul", "-Xcompiler", "-msse4.1",
          "-I", os.path.join(ROOT, "include")]
 
 

@@ -1,0 +1,590 @@
+// AND reduction: the oblong zerocheck of (A & B) ^ C = 0 over the 64-bit rows of every AND
+// constraint, with a univariate skip round over the 64 bit positions.
+//
+// Follows prove_bitand_reduction (prover/prover/src/prove.rs:329-372) and OblongZerocheckProver
+// (prover/prover/src/and_reduction/prover.rs:74-276):
+//  1. log_n - 3 big-field challenges are sampled; eq_big is their eq tensor.
+//  2. Univariate round (and_reduction/sumcheck_round_messages.rs:62-136): each word's 64 bits are
+//     the values on the subspace {0, .., 63} of GF(2^8) (AES field, basis 1, 2, .., 32) of a
+//     polynomial of degree < 64; its values at the points 64 .. 127 come from byte-indexed tables of
+//     Lagrange sums (ntt_lookup.rs:91-164).  Per group of 8 constraints the GF(2^8) values
+//     (A*B + C) * eq_small[j] are summed (eq_small is the eq tensor of the fixed challenges 2, 4, 16,
+//     config.rs:33-37), embedded into GF(2^128) and weighted by eq_big.  The 64 sums are the message.
+//  3. The words are folded at the univariate challenge z (fold_lookup.rs:18-92): word -> sum of the
+//     Lagrange basis at z over the set bits, through 8 byte tables.
+//  4. A quadratic MLE-check (protocols/sumcheck/quadratic_mle.rs:21-196 with gruen32.rs) on
+//     (a, b, c) with composition a*b - c over the point [2, 4, 16] ++ big (embedded), claim = the
+//     message extended by zeros on the base domain and evaluated at z.
+//
+// B200 mapping: the univariate round keeps its 128 KiB of GF(2^8) tables in shared memory laid out
+// [byte index][byte value][4-point group] so the 16 threads of a constraint group hit 16 distinct
+// banks; GF(2^8) products use log/exp tables; the embedding into GF(2^128) is done once per group
+// and bit (8 multiplies per group instead of 64).  The MLE-check rounds fuse the fold by the previous
+// challenge, the truncation of the eq tensor and the next round's evaluation in one pass.
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+#include "cs.h"
+#include "gf128.cuh"
+#include "internal.h"
+#include "kernels.h"
+#include "transcript.h"
+
+using namespace bgpu;
+
+namespace {
+
+typedef unsigned __int128 u128h;
+
+// ------------------------------------------------------------------ host constants
+
+uint8_t aes_mul_h(uint8_t a, uint8_t b) {
+  uint8_t r = 0;
+  for (int i = 0; i < 8; i++) {
+    if (b & 1) r ^= a;
+    uint8_t hi = a & 0x80;
+    a = (uint8_t)(a << 1);
+    if (hi) a ^= 0x1b;
+    b >>= 1;
+  }
+  return r;
+}
+
+uint8_t aes_inv_h(uint8_t a) {
+  uint8_t r = 1;
+  for (int i = 0; i < 254; i++) r = aes_mul_h(r, a);
+  return a ? r : 0;
+}
+
+struct AndConstants {
+  uint32_t ntt[8][256][16];  // [byte index][byte value][point group] -> 4 GF(2^8) values
+  uint8_t mul_eq[8][256];    // x * eq_small[j]
+  uint8_t log[256];
+  uint8_t exp[512];
+  u128h phi[256];            // the GF(2^8) -> GF(2^128) embedding
+};
+
+// The embedding is fixed by the image of the AES generator x (byte 0x02), the entry for 0x02 of
+// `From<AESTowerField8b> for BinaryField128bGhash` (verifier/field/src/ghash.rs:520-530); the other
+// entries follow by linearity.
+const u128h kAesXInGhash = ((u128h)0x0dcb364640a222feull << 64) | (u128h)0x6b8330483c2e9849ull;
+
+const AndConstants& and_constants() {
+  static AndConstants C;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    // Lagrange basis over {0..63} evaluated at 64 + k: M[k][t]
+    uint8_t denom = 1;
+    for (int u = 1; u < 64; u++) denom = aes_mul_h(denom, (uint8_t)u);
+    const uint8_t dinv = aes_inv_h(denom);
+    static uint8_t M[64][64];
+    for (int k = 0; k < 64; k++)
+      for (int t = 0; t < 64; t++) {
+        uint8_t num = 1;
+        for (int s = 0; s < 64; s++)
+          if (s != t) num = aes_mul_h(num, (uint8_t)((64 + k) ^ s));
+        M[k][t] = aes_mul_h(num, dinv);
+      }
+    for (int bi = 0; bi < 8; bi++)
+      for (int bv = 0; bv < 256; bv++)
+        for (int kq = 0; kq < 16; kq++) {
+          uint32_t packed = 0;
+          for (int l = 0; l < 4; l++) {
+            uint8_t acc = 0;
+            for (int j = 0; j < 8; j++)
+              if ((bv >> j) & 1) acc ^= M[4 * kq + l][8 * bi + j];
+            packed |= (uint32_t)acc << (8 * l);
+          }
+          C.ntt[bi][bv][kq] = packed;
+        }
+    // eq_small = eq tensor of (2, 4, 16) in GF(2^8)
+    const uint8_t r[3] = {0x2, 0x4, 0x10};
+    uint8_t eq[8] = {1};
+    uint32_t len = 1;
+    for (int i = 0; i < 3; i++) {
+      for (uint32_t j = 0; j < len; j++) {
+        uint8_t prod = aes_mul_h(eq[j], r[i]);
+        eq[j] ^= prod;
+        eq[len + j] = prod;
+      }
+      len <<= 1;
+    }
+    for (int j = 0; j < 8; j++)
+      for (int x = 0; x < 256; x++) C.mul_eq[j][x] = aes_mul_h((uint8_t)x, eq[j]);
+    uint8_t e = 1;
+    for (int i = 0; i < 255; i++) {
+      C.exp[i] = e;
+      C.exp[i + 255] = e;
+      C.log[e] = (uint8_t)i;
+      e = aes_mul_h(e, 3);
+    }
+    C.exp[510] = C.exp[0];
+    C.exp[511] = C.exp[1];
+    C.log[0] = 0;
+    u128h pw[8];
+    pw[0] = 1;
+    for (int i = 1; i < 8; i++) pw[i] = host_gf_mul(pw[i - 1], kAesXInGhash);
+    for (int b = 0; b < 256; b++) {
+      u128h acc = 0;
+      for (int i = 0; i < 8; i++)
+        if ((b >> i) & 1) acc ^= pw[i];
+      C.phi[b] = acc;
+    }
+  });
+  return C;
+}
+
+// Lagrange basis of {phi(t) : t < 2^dim} at x (univariate_lagrange.rs:22-66).
+void lagrange_b128(uint32_t dim, u128h x, u128h* out) {
+  const AndConstants& C = and_constants();
+  const uint32_t n = 1u << dim;
+  u128h denom = 1;
+  for (uint32_t u = 1; u < n; u++) denom = host_gf_mul(denom, C.phi[u]);
+  const u128h dinv = host_gf_inv(denom);
+  std::vector<u128h> diff(n), suffix(n + 1);
+  for (uint32_t s = 0; s < n; s++) diff[s] = x ^ C.phi[s];
+  suffix[n] = 1;
+  for (int s = (int)n - 1; s >= 0; s--) suffix[s] = host_gf_mul(suffix[s + 1], diff[s]);
+  u128h prefix = 1;
+  for (uint32_t t = 0; t < n; t++) {
+    out[t] = host_gf_mul(host_gf_mul(prefix, suffix[t + 1]), dinv);
+    prefix = host_gf_mul(prefix, diff[t]);
+  }
+}
+
+// ------------------------------------------------------------------ device tables
+
+struct DevAndTables {
+  uint32_t* ntt = nullptr;  // 8 * 256 * 16
+  uint8_t* mul_eq = nullptr;
+  uint8_t* log = nullptr;
+  uint8_t* exp = nullptr;
+};
+
+struct PhiPowers {
+  uint4 p[8];
+};
+
+constexpr int kUniThreads = 512;
+constexpr int kSlots = kUniThreads / 16;
+constexpr size_t kUniSmem = sizeof(uint32_t) * 8 * 256 * 16 + 8 * 256 + 256 + 512 +
+                            sizeof(uint4) * kSlots * 8;
+
+__device__ __forceinline__ uint8_t gf8_mul(const uint8_t* s_log, const uint8_t* s_exp, uint32_t a,
+                                           uint32_t b) {
+  return (a && b) ? s_exp[s_log[a] + s_log[b]] : 0;
+}
+
+__device__ __forceinline__ uint32_t word_ntt(const uint32_t* sT, uint64_t w, uint32_t kq) {
+  uint32_t acc = 0;
+#pragma unroll
+  for (int bi = 0; bi < 8; bi++) acc ^= sT[((bi << 8) | (uint32_t)((w >> (8 * bi)) & 255)) * 16 + kq];
+  return acc;
+}
+
+__global__ void __launch_bounds__(kUniThreads, 1)
+    univariate_round_kernel(const uint64_t* __restrict__ wa, const uint64_t* __restrict__ wb,
+                            const uint64_t* __restrict__ wc, const uint4* __restrict__ eq_big,
+                            uint64_t n_chunks, DevAndTables tab, PhiPowers phi,
+                            uint32_t* __restrict__ out) {
+  extern __shared__ uint4 smem4[];
+  uint32_t* sT = reinterpret_cast<uint32_t*>(smem4);
+  uint8_t* s_mul = reinterpret_cast<uint8_t*>(sT + 8 * 256 * 16);
+  uint8_t* s_log = s_mul + 8 * 256;
+  uint8_t* s_exp = s_log + 256;
+  uint4* s_P = reinterpret_cast<uint4*>(s_exp + 512);  // [kSlots][8], 16-byte aligned
+  for (uint32_t i = threadIdx.x; i < 8 * 256 * 16; i += blockDim.x) sT[i] = tab.ntt[i];
+  for (uint32_t i = threadIdx.x; i < 8 * 256; i += blockDim.x) s_mul[i] = tab.mul_eq[i];
+  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) s_log[i] = tab.log[i];
+  for (uint32_t i = threadIdx.x; i < 512; i += blockDim.x) s_exp[i] = tab.exp[i];
+  const uint32_t kq = threadIdx.x & 15, slot = threadIdx.x >> 4;
+  uint4 acc[4] = {gf_zero(), gf_zero(), gf_zero(), gf_zero()};
+  const uint64_t stride = (uint64_t)gridDim.x * kSlots;
+  const uint64_t iters = (n_chunks + stride - 1) / stride;
+  for (uint64_t it = 0; it < iters; it++) {
+    const uint64_t chunk = it * stride + (uint64_t)blockIdx.x * kSlots + slot;
+    const bool valid = chunk < n_chunks;
+    __syncthreads();
+    if (valid && kq < 8) s_P[slot * 8 + kq] = gf_mul(eq_big[chunk], phi.p[kq]);
+    __syncthreads();
+    if (valid) {
+      uint32_t v4 = 0;
+#pragma unroll 1
+      for (int j = 0; j < 8; j++) {
+        const uint64_t i = chunk * 8 + j;
+        const uint32_t A = word_ntt(sT, __ldg(wa + i), kq);
+        const uint32_t B = word_ntt(sT, __ldg(wb + i), kq);
+        const uint32_t Cv = word_ntt(sT, __ldg(wc + i), kq);
+        const uint8_t* mj = s_mul + (j << 8);
+#pragma unroll
+        for (int l = 0; l < 4; l++) {
+          const uint32_t x = gf8_mul(s_log, s_exp, (A >> (8 * l)) & 255, (B >> (8 * l)) & 255) ^
+                             ((Cv >> (8 * l)) & 255);
+          v4 ^= (uint32_t)mj[x] << (8 * l);
+        }
+      }
+#pragma unroll
+      for (int l = 0; l < 4; l++) {
+        const uint32_t v = (v4 >> (8 * l)) & 255;
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+          const uint32_t m = 0u - ((v >> b) & 1u);
+          const uint4 P = s_P[slot * 8 + b];
+          acc[l].x ^= P.x & m;
+          acc[l].y ^= P.y & m;
+          acc[l].z ^= P.z & m;
+          acc[l].w ^= P.w & m;
+        }
+      }
+    }
+  }
+  // reduce over the slots: reuse the table area as [64 points][kSlots] accumulators
+  __syncthreads();
+  uint4* red = smem4;
+#pragma unroll
+  for (int l = 0; l < 4; l++) red[(4 * kq + l) * kSlots + slot] = acc[l];
+  __syncthreads();
+  if (threadIdx.x < 64) {
+    uint4 s = gf_zero();
+    for (int q = 0; q < kSlots; q++) gf_add_into(s, red[threadIdx.x * kSlots + q]);
+    uint32_t* dst = out + 4 * threadIdx.x;
+    if (s.x) atomicXor(dst + 0, s.x);
+    if (s.y) atomicXor(dst + 1, s.y);
+    if (s.z) atomicXor(dst + 2, s.z);
+    if (s.w) atomicXor(dst + 3, s.w);
+  }
+}
+
+struct Lag64 {
+  uint4 l[64];
+};
+
+// out[i] = sum over set bits t of words[i] of lag[t], through 8 byte tables of subset sums.
+__global__ void __launch_bounds__(256)
+    fold_words_kernel(const uint64_t* __restrict__ words, uint64_t n, Lag64 lag,
+                      uint4* __restrict__ out) {
+  __shared__ uint4 tab[8][256];
+  for (uint32_t i = threadIdx.x; i < 8 * 256; i += blockDim.x) {
+    const uint32_t bi = i >> 8, bv = i & 255;
+    uint4 acc = gf_zero();
+    for (int j = 0; j < 8; j++)
+      if ((bv >> j) & 1) gf_add_into(acc, lag.l[8 * bi + j]);
+    tab[bi][bv] = acc;
+  }
+  __syncthreads();
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t w = __ldg(words + i);
+    uint4 acc = gf_zero();
+#pragma unroll
+    for (int bi = 0; bi < 8; bi++) gf_add_into(acc, tab[bi][(w >> (8 * bi)) & 255]);
+    out[i] = acc;
+  }
+}
+
+__device__ __forceinline__ uint4 shfl_gf(uint4 v, int m) {
+  v.x = __shfl_xor_sync(0xffffffffu, v.x, m);
+  v.y = __shfl_xor_sync(0xffffffffu, v.y, m);
+  v.z = __shfl_xor_sync(0xffffffffu, v.z, m);
+  v.w = __shfl_xor_sync(0xffffffffu, v.w, m);
+  return v;
+}
+
+__device__ __forceinline__ void reduce2_atomic(uint4 v0, uint4 v1, uint32_t* dst) {
+  __shared__ uint4 red[2][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int m = 16; m >= 1; m >>= 1) {
+    gf_add_into(v0, shfl_gf(v0, m));
+    gf_add_into(v1, shfl_gf(v1, m));
+  }
+  if (lane == 0) {
+    red[0][warp] = v0;
+    red[1][warp] = v1;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    uint4 a = lane < nw ? red[0][lane] : gf_zero();
+    uint4 b = lane < nw ? red[1][lane] : gf_zero();
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) {
+      gf_add_into(a, shfl_gf(a, m));
+      gf_add_into(b, shfl_gf(b, m));
+    }
+    if (lane == 0) {
+      const uint32_t v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+      for (int q = 0; q < 8; q++)
+        if (v[q]) atomicXor(dst + q, v[q]);
+    }
+  }
+}
+
+// Round evaluation without a fold: columns of length 2*half, eq of length half.
+__global__ void __launch_bounds__(256)
+    and_mle_eval_kernel(const uint4* __restrict__ fa, const uint4* __restrict__ fb,
+                        const uint4* __restrict__ fc, const uint4* __restrict__ eq, uint64_t half,
+                        uint32_t* __restrict__ out) {
+  u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < half;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint4 a0 = fa[i], a1 = fa[half + i], b0 = fb[i], b1 = fb[half + i], c1 = fc[half + i];
+    const uint4 e = eq[i];
+    xor_into(s1, clmul128(e, gf_add(gf_mul(a1, b1), c1)));
+    xor_into(sinf, clmul128(e, gf_mul(gf_add(a0, a1), gf_add(b0, b1))));
+  }
+  reduce2_atomic(reduce256(s1), reduce256(sinf), out);
+}
+
+// Fold the three columns (length size) by r, truncate eq (length size/2 -> size/4) and evaluate
+// the next round.  Thread j owns folded positions j, j + size/4 and eq position j.
+__global__ void __launch_bounds__(256)
+    and_mle_fold_eval_kernel(uint4* __restrict__ fa, uint4* __restrict__ fb, uint4* __restrict__ fc,
+                             uint4* __restrict__ eq, uint64_t size, uint4 r,
+                             uint32_t* __restrict__ out) {
+  const uint64_t h = size >> 1, q = size >> 2;
+  u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < q;
+       j += (uint64_t)gridDim.x * blockDim.x) {
+    uint4 f[3][2];
+    uint4* cols[3] = {fa, fb, fc};
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      uint4* col = cols[c];
+      const uint4 lo0 = col[j], hi0 = col[h + j], lo1 = col[q + j], hi1 = col[h + q + j];
+      f[c][0] = gf_add(lo0, gf_mul(r, gf_add(hi0, lo0)));
+      f[c][1] = gf_add(lo1, gf_mul(r, gf_add(hi1, lo1)));
+      col[j] = f[c][0];
+      col[q + j] = f[c][1];
+    }
+    const uint4 e = gf_add(eq[j], eq[q + j]);
+    eq[j] = e;
+    xor_into(s1, clmul128(e, gf_add(gf_mul(f[0][1], f[1][1]), f[2][1])));
+    xor_into(sinf, clmul128(e, gf_mul(gf_add(f[0][0], f[0][1]), gf_add(f[1][0], f[1][1]))));
+  }
+  reduce2_atomic(reduce256(s1), reduce256(sinf), out);
+}
+
+// Final fold of length-2 columns by r: out[c] = lo + r (hi - lo).
+__global__ void and_fold_final_kernel(const uint4* __restrict__ fa, const uint4* __restrict__ fb,
+                                      const uint4* __restrict__ fc, uint4 r, uint4* __restrict__ out) {
+  const int c = threadIdx.x;
+  if (c >= 3) return;
+  const uint4* col = c == 0 ? fa : (c == 1 ? fb : fc);
+  out[c] = gf_add(col[0], gf_mul(r, gf_add(col[1], col[0])));
+}
+
+struct DevTablesHolder {
+  DevAndTables t;
+  int device = -1;
+};
+
+int device_tables(DevAndTables& out) {
+  static std::mutex m;
+  static DevTablesHolder holders[64];
+  int dev = 0;
+  BGPU_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return set_error(BINIUS_E_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> g(m);
+  DevTablesHolder& h = holders[dev];
+  if (h.device != dev) {
+    const AndConstants& C = and_constants();
+    BGPU_CUDA(cudaMalloc(&h.t.ntt, sizeof(C.ntt)));
+    BGPU_CUDA(cudaMemcpy(h.t.ntt, C.ntt, sizeof(C.ntt), cudaMemcpyHostToDevice));
+    BGPU_CUDA(cudaMalloc(&h.t.mul_eq, sizeof(C.mul_eq) + 256 + 512));
+    h.t.log = h.t.mul_eq + sizeof(C.mul_eq);
+    h.t.exp = h.t.log + 256;
+    BGPU_CUDA(cudaMemcpy(h.t.mul_eq, C.mul_eq, sizeof(C.mul_eq), cudaMemcpyHostToDevice));
+    BGPU_CUDA(cudaMemcpy(h.t.log, C.log, 256, cudaMemcpyHostToDevice));
+    BGPU_CUDA(cudaMemcpy(h.t.exp, C.exp, 512, cudaMemcpyHostToDevice));
+    BGPU_CUDA(cudaFuncSetAttribute(univariate_round_kernel,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUniSmem));
+    h.device = dev;
+  }
+  out = h.t;
+  return BINIUS_OK;
+}
+
+uint4 to_uint4(u128h v) {
+  uint4 r;
+  memcpy(&r, &v, 16);
+  return r;
+}
+u128h from_bytes16(const uint8_t* b) {
+  u128h v;
+  memcpy(&v, b, 16);
+  return v;
+}
+
+unsigned grid_for(uint64_t n, unsigned threads, unsigned cap = 148 * 8) {
+  uint64_t g = (n + threads - 1) / threads;
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, cap));
+}
+
+}  // namespace
+
+namespace bgpu {
+
+struct AndResult {
+  u128h a_eval, b_eval, c_eval, z;
+  std::vector<u128h> eval_point;
+};
+
+// d_witness: committed_total_len words; writes the AND reduction's transcript messages.
+int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcript& t,
+                        AndResult& res, cudaStream_t s) {
+  const uint64_t N = cs->and_ops.n_constraints;
+  uint32_t log_n = 0;
+  while ((1ull << log_n) < N) log_n++;
+  if (log_n < 3) return set_error(BINIUS_E_ARG, "AND reduction needs at least 8 constraints");
+  const uint64_t n_chunks = N >> 3;
+  DevAndTables tab;
+  if (int rc = device_tables(tab)) return rc;
+  const AndConstants& C = and_constants();
+
+  uint64_t* words = nullptr;
+  uint4 *eq_big = nullptr, *fcols = nullptr, *eq = nullptr;
+  uint32_t* d_acc = nullptr;
+  BGPU_CUDA(cudaMallocAsync(&words, 8 * 3 * N, s));
+  BGPU_CUDA(cudaMallocAsync(&eq_big, 16 * n_chunks, s));
+  BGPU_CUDA(cudaMallocAsync(&fcols, 16 * 3 * N, s));
+  BGPU_CUDA(cudaMallocAsync(&eq, 16 * (N / 2), s));
+  BGPU_CUDA(cudaMallocAsync(&d_acc, 64 * 16, s));
+  int rc = BINIUS_OK;
+  do {
+    if ((rc = eval_operands(cs->and_ops, d_witness, words, s))) break;
+    // big-field zerocheck challenges
+    std::vector<uint8_t> big(16 * (log_n - 3));
+    for (uint32_t i = 0; i < log_n - 3; i++) t.sample_elem(big.data() + 16 * i);
+    if ((rc = eq_tensor(reinterpret_cast<const uint4*>(big.data()), log_n - 3, eq_big, s))) break;
+    // univariate round
+    PhiPowers pw;
+    for (int i = 0; i < 8; i++) pw.p[i] = to_uint4(C.phi[1u << i]);
+    cudaError_t e = cudaMemsetAsync(d_acc, 0, 64 * 16, s);
+    if (e != cudaSuccess) { rc = cuda_error(e, "memset"); break; }
+    univariate_round_kernel<<<148, kUniThreads, kUniSmem, s>>>(words, words + N, words + 2 * N,
+                                                              eq_big, n_chunks, tab, pw, d_acc);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) { rc = cuda_error(e, "univariate_round_kernel"); break; }
+    count_launch();
+    uint8_t msg[64 * 16];
+    e = cudaMemcpyAsync(msg, d_acc, sizeof(msg), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { rc = cuda_error(e, "univariate message"); break; }
+    t.message(msg, sizeof(msg));
+    uint8_t zb[16];
+    t.sample_elem(zb);
+    const u128h z = from_bytes16(zb);
+    res.z = z;
+    // fold the words at z
+    u128h lag[128];
+    lagrange_b128(6, z, lag);
+    Lag64 l64;
+    for (int i = 0; i < 64; i++) l64.l[i] = to_uint4(lag[i]);
+    fold_words_kernel<<<grid_for(3 * N, 256), 256, 0, s>>>(words, 3 * N, l64, fcols);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) { rc = cuda_error(e, "fold_words_kernel"); break; }
+    count_launch();
+    // claim: the message (zero on the base domain) evaluated at z over the 128-point domain
+    lagrange_b128(7, z, lag);
+    u128h sum = 0;
+    for (int k = 0; k < 64; k++) sum ^= host_gf_mul(from_bytes16(msg + 16 * k), lag[64 + k]);
+    // MLE-check over the point [phi(2), phi(4), phi(16)] ++ big
+    std::vector<u128h> point{C.phi[2], C.phi[4], C.phi[16]};
+    for (uint32_t i = 0; i < log_n - 3; i++) point.push_back(from_bytes16(big.data() + 16 * i));
+    std::vector<uint4> pt4(point.size());
+    for (size_t i = 0; i < point.size(); i++) pt4[i] = to_uint4(point[i]);
+    if ((rc = eq_tensor(pt4.data(), log_n - 1, eq, s))) break;
+    uint4* fa = fcols;
+    uint4* fb = fcols + N;
+    uint4* fc = fcols + 2 * N;
+    std::vector<u128h> challenges;
+    uint8_t rb[16];
+    for (uint32_t n_rem = log_n; n_rem > 0; n_rem--) {
+      e = cudaMemsetAsync(d_acc, 0, 32, s);
+      if (e != cudaSuccess) { rc = cuda_error(e, "memset"); break; }
+      const uint64_t size = 1ull << n_rem;
+      if (n_rem == log_n) {
+        and_mle_eval_kernel<<<grid_for(size / 2, 256), 256, 0, s>>>(fa, fb, fc, eq, size / 2,
+                                                                    d_acc);
+      } else {
+        uint4 r4;
+        memcpy(&r4, rb, 16);
+        and_mle_fold_eval_kernel<<<grid_for(size / 2, 256), 256, 0, s>>>(fa, fb, fc, eq,
+                                                                         size * 2, r4, d_acc);
+      }
+      e = cudaGetLastError();
+      if (e != cudaSuccess) { rc = cuda_error(e, "AND MLE-check round"); break; }
+      count_launch();
+      uint8_t ys[32];
+      e = cudaMemcpyAsync(ys, d_acc, 32, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) { rc = cuda_error(e, "round sums"); break; }
+      const u128h y1 = from_bytes16(ys), yinf = from_bytes16(ys + 16);
+      const u128h alpha = point[n_rem - 1];
+      // RoundEvals2::interpolate_eq (round_evals.rs:80-86)
+      const u128h y0 = host_gf_mul(sum ^ host_gf_mul(y1, alpha), host_gf_inv(1 ^ alpha));
+      const u128h c0 = y0, c2 = yinf, c1 = y1 ^ c0 ^ c2;
+      uint8_t rp[32];  // mlecheck::RoundProof::truncate drops c0
+      memcpy(rp, &c1, 16);
+      memcpy(rp + 16, &c2, 16);
+      t.message(rp, 32);
+      t.sample_elem(rb);
+      const u128h r = from_bytes16(rb);
+      challenges.push_back(r);
+      sum = c0 ^ host_gf_mul(c1, r) ^ host_gf_mul(c2, host_gf_mul(r, r));
+    }
+    if (rc) break;
+    uint4 r4;
+    memcpy(&r4, rb, 16);
+    uint4* d_ev = reinterpret_cast<uint4*>(d_acc);
+    and_fold_final_kernel<<<1, 32, 0, s>>>(fa, fb, fc, r4, d_ev);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) { rc = cuda_error(e, "and_fold_final_kernel"); break; }
+    count_launch();
+    uint8_t ev[48];
+    e = cudaMemcpyAsync(ev, d_ev, 48, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { rc = cuda_error(e, "final evals"); break; }
+    t.message(ev, 48);
+    res.a_eval = from_bytes16(ev);
+    res.b_eval = from_bytes16(ev + 16);
+    res.c_eval = from_bytes16(ev + 32);
+    res.eval_point.assign(challenges.rbegin(), challenges.rend());
+  } while (0);
+  cudaFreeAsync(words, s);
+  cudaFreeAsync(eq_big, s);
+  cudaFreeAsync(fcols, s);
+  cudaFreeAsync(eq, s);
+  cudaFreeAsync(d_acc, s);
+  return rc;
+}
+
+}  // namespace bgpu
+
+extern "C" {
+
+int binius_and_reduction_prove(const binius_cs* cs, const void* d_witness,
+                               binius_transcript* transcript, void* h_out_meta,
+                               void* h_out_point, void* stream) {
+  BGPU_ARG(cs && d_witness && transcript, "NULL argument");
+  AndResult res;
+  int rc = and_reduction_prove(cs, static_cast<const uint64_t*>(d_witness), transcript->t, res,
+                               as_stream(stream));
+  if (rc) return rc;
+  if (h_out_meta) {
+    uint8_t* m = static_cast<uint8_t*>(h_out_meta);
+    memcpy(m, &res.a_eval, 16);
+    memcpy(m + 16, &res.b_eval, 16);
+    memcpy(m + 32, &res.c_eval, 16);
+    memcpy(m + 48, &res.z, 16);
+  }
+  if (h_out_point)
+    memcpy(h_out_point, res.eval_point.data(), 16 * res.eval_point.size());
+  return clear_error();
+}
+
+}  // extern "C"

@@ -3,6 +3,10 @@
 
 #include <atomic>
 
+#if defined(__PCLMUL__) && defined(__SSE4_1__)
+#include <immintrin.h>
+#endif
+
 #include "internal.h"
 
 namespace bgpu {
@@ -42,10 +46,26 @@ static inline void clmul64(uint64_t a, uint64_t b, uint64_t& lo, uint64_t& hi) {
 hu128 host_gf_mul(hu128 a, hu128 b) {
   uint64_t a0 = (uint64_t)a, a1 = (uint64_t)(a >> 64), b0 = (uint64_t)b, b1 = (uint64_t)(b >> 64);
   uint64_t l0, l1, h0, h1, m0, m1, x0, x1;
+#if defined(__PCLMUL__) && defined(__SSE4_1__)
+  // PCLMULQDQ for the host side of the protocol (scalar interpolation and challenges).
+  __m128i va = _mm_set_epi64x((long long)a1, (long long)a0);
+  __m128i vb = _mm_set_epi64x((long long)b1, (long long)b0);
+  __m128i l = _mm_clmulepi64_si128(va, vb, 0x00), h = _mm_clmulepi64_si128(va, vb, 0x11);
+  __m128i m = _mm_clmulepi64_si128(va, vb, 0x01), x = _mm_clmulepi64_si128(va, vb, 0x10);
+  l0 = (uint64_t)_mm_cvtsi128_si64(l);
+  l1 = (uint64_t)_mm_extract_epi64(l, 1);
+  h0 = (uint64_t)_mm_cvtsi128_si64(h);
+  h1 = (uint64_t)_mm_extract_epi64(h, 1);
+  m0 = (uint64_t)_mm_cvtsi128_si64(m);
+  m1 = (uint64_t)_mm_extract_epi64(m, 1);
+  x0 = (uint64_t)_mm_cvtsi128_si64(x);
+  x1 = (uint64_t)_mm_extract_epi64(x, 1);
+#else
   clmul64(a0, b0, l0, l1);
   clmul64(a1, b1, h0, h1);
   clmul64(a0, b1, m0, m1);
   clmul64(a1, b0, x0, x1);
+#endif
   uint64_t p0 = l0, p1 = l1 ^ m0 ^ x0, p2 = h0 ^ m1 ^ x1, p3 = h1;
   uint64_t t = (p3 >> 63) ^ (p3 >> 62) ^ (p3 >> 57);
   uint64_t lo = p0 ^ p2 ^ (p2 << 1) ^ (p2 << 2) ^ (p2 << 7) ^ t ^ (t << 1) ^ (t << 2) ^ (t << 7);

@@ -1,0 +1,249 @@
+// Constraint systems on the device: the reference's v2 wire format, validate_and_prepare's padding
+// and operand evaluation.
+//
+// ConstraintSystem::deserialize (verifier/core/src/constraint_system.rs:615-650): u32 version (2),
+// the ValueVecLayout as eight u32 (usize fields), constants (u32 count + u64 words), AND
+// constraints (u32 count, then per constraint the operands a, b, c) and MUL constraints (a, b, hi,
+// lo); an operand is a u32 count of (u32 value index, u8 shift variant, u32 amount) terms.
+// validate (:466-530) and validate_and_prepare (:558-584: pad AND to a power of two >= 8 and MUL to
+// a power of two >= 1 with empty constraints).
+//
+// Operands live on the device in CSR form: group g = constraint * k + slot with offsets[g] into a
+// term array of (value index, variant << 8 | amount).  eval_operand (verifier/core/src/verify.rs:
+// 14-35) runs one thread per group: a gather of the witness words, the shift, and an XOR.
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "cs.h"
+#include "internal.h"
+
+using namespace bgpu;
+
+namespace {
+
+struct Reader {
+  const uint8_t* p;
+  size_t len, pos = 0;
+  bool ok = true;
+  uint32_t u32() {
+    if (pos + 4 > len) {
+      ok = false;
+      return 0;
+    }
+    uint32_t v;
+    memcpy(&v, p + pos, 4);
+    pos += 4;
+    return v;
+  }
+  uint64_t u64() {
+    if (pos + 8 > len) {
+      ok = false;
+      return 0;
+    }
+    uint64_t v;
+    memcpy(&v, p + pos, 8);
+    pos += 8;
+    return v;
+  }
+  uint8_t u8() {
+    if (pos + 1 > len) {
+      ok = false;
+      return 0;
+    }
+    return p[pos++];
+  }
+};
+
+__device__ __forceinline__ uint64_t shifted_word(uint64_t w, uint32_t variant, uint32_t n) {
+  const uint32_t lo = (uint32_t)w, hi = (uint32_t)(w >> 32), n5 = n & 31;
+  switch (variant) {
+    case 0: return w << n;                                              // Sll
+    case 1: return w >> n;                                              // Slr
+    case 2: return (uint64_t)((int64_t)w >> n);                         // Sar
+    case 3: return n ? ((w >> n) | (w << (64 - n))) : w;                // Rotr
+    case 4: return ((uint64_t)(hi << n5) << 32) | (uint32_t)(lo << n5);  // Sll32
+    case 5: return ((uint64_t)(hi >> n5) << 32) | (uint32_t)(lo >> n5);  // Srl32
+    case 6:
+      return ((uint64_t)(uint32_t)((int32_t)hi >> n5) << 32) | (uint32_t)((int32_t)lo >> n5);
+    default:
+      return ((uint64_t)__funnelshift_r(hi, hi, n5) << 32) | __funnelshift_r(lo, lo, n5);
+  }
+}
+
+__global__ void eval_operands_kernel(const uint32_t* __restrict__ offsets,
+                                     const uint2* __restrict__ terms,
+                                     const uint64_t* __restrict__ witness, uint64_t n_constraints,
+                                     uint32_t k, uint64_t* __restrict__ out) {
+  const uint64_t groups = n_constraints * k;
+  for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < groups;
+       g += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t lo = __ldg(offsets + g), hi = __ldg(offsets + g + 1);
+    uint64_t acc = 0;
+    for (uint32_t t = lo; t < hi; t++) {
+      const uint2 term = __ldg(terms + t);
+      acc ^= shifted_word(__ldg(witness + term.x), term.y >> 8, term.y & 255);
+    }
+    const uint64_t c = g / k, slot = g - c * k;
+    out[slot * n_constraints + c] = acc;
+  }
+}
+
+int parse_operands(Reader& r, uint32_t n, uint32_t k, uint32_t total_len, HostOperands& ops) {
+  ops.k = k;
+  ops.offsets.assign(1, 0);
+  ops.terms.clear();
+  for (uint32_t i = 0; i < n && r.ok; i++) {
+    for (uint32_t s = 0; s < k && r.ok; s++) {
+      uint32_t cnt = r.u32();
+      if (!r.ok || cnt > (1u << 24)) return set_error(BINIUS_E_ARG, "malformed operand length");
+      for (uint32_t t = 0; t < cnt && r.ok; t++) {
+        uint32_t vi = r.u32();
+        uint32_t variant = r.u8();
+        uint32_t amount = r.u32();
+        if (!r.ok) break;
+        if (variant > 7) return set_error(BINIUS_E_ARG, "unknown ShiftVariant");
+        if (amount >= 64) return set_error(BINIUS_E_ARG, "ShiftedValueIndex::amount >= 64");
+        if (amount == 0 && variant != 0)
+          return set_error(BINIUS_E_ARG, "non-canonical shift (amount 0 with a non-Sll variant)");
+        if (vi >= total_len) return set_error(BINIUS_E_ARG, "value index out of range");
+        ops.terms.push_back(make_uint2(vi, (variant << 8) | amount));
+      }
+      ops.offsets.push_back((uint32_t)ops.terms.size());
+    }
+  }
+  if (!r.ok) return set_error(BINIUS_E_ARG, "constraint system bytes truncated");
+  return BINIUS_OK;
+}
+
+void pad_operands(HostOperands& ops, uint32_t n_target) {
+  const uint32_t n = (uint32_t)((ops.offsets.size() - 1) / ops.k);
+  for (uint32_t i = n; i < n_target; i++)
+    for (uint32_t s = 0; s < ops.k; s++) ops.offsets.push_back((uint32_t)ops.terms.size());
+}
+
+uint32_t next_pow2_at_least(uint32_t n, uint32_t min) {
+  uint32_t v = n < min ? min : n;
+  uint32_t p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+int upload(const HostOperands& h, DevOperands& d) {
+  d.k = h.k;
+  d.n_constraints = (uint32_t)((h.offsets.size() - 1) / h.k);
+  d.n_terms = h.terms.size();
+  BGPU_CUDA(cudaMalloc(&d.offsets, 4 * h.offsets.size()));
+  BGPU_CUDA(cudaMemcpy(d.offsets, h.offsets.data(), 4 * h.offsets.size(), cudaMemcpyHostToDevice));
+  BGPU_CUDA(cudaMalloc(&d.terms, 8 * (h.terms.empty() ? 1 : h.terms.size())));
+  if (!h.terms.empty())
+    BGPU_CUDA(cudaMemcpy(d.terms, h.terms.data(), 8 * h.terms.size(), cudaMemcpyHostToDevice));
+  return BINIUS_OK;
+}
+
+bool is_pow2(uint32_t v) { return v && !(v & (v - 1)); }
+
+}  // namespace
+
+namespace bgpu {
+
+int eval_operands(const DevOperands& ops, const uint64_t* d_witness, uint64_t* d_out,
+                  cudaStream_t s) {
+  const uint64_t groups = (uint64_t)ops.n_constraints * ops.k;
+  if (groups == 0) return BINIUS_OK;
+  unsigned blocks = (unsigned)std::min<uint64_t>((groups + 255) / 256, 148 * 16);
+  eval_operands_kernel<<<blocks, 256, 0, s>>>(ops.offsets, ops.terms, d_witness,
+                                              ops.n_constraints, ops.k, d_out);
+  BGPU_LAUNCH_CHECK("eval_operands_kernel");
+  count_launch();
+  return BINIUS_OK;
+}
+
+}  // namespace bgpu
+
+extern "C" {
+
+int binius_cs_from_bytes(int device, const void* h_bytes, size_t len, binius_cs** out) {
+  BGPU_ARG(out != nullptr && (h_bytes != nullptr || len == 0), "NULL argument");
+  *out = nullptr;
+  Reader r{static_cast<const uint8_t*>(h_bytes), len};
+  uint32_t version = r.u32();
+  BGPU_ARG(r.ok && version == 2, "ConstraintSystem::version must be 2");
+  binius_cs* cs = new binius_cs();
+  cs->device = device;
+  uint32_t* fields[8] = {&cs->n_const,      &cs->n_inout,         &cs->n_witness,
+                         &cs->n_internal,   &cs->offset_inout,    &cs->offset_witness,
+                         &cs->committed_total_len, &cs->n_scratch};
+  for (auto f : fields) *f = r.u32();
+  uint32_t n_constants = r.u32();
+  int rc = BINIUS_OK;
+  do {
+    if (!r.ok) { rc = set_error(BINIUS_E_ARG, "constraint system bytes truncated"); break; }
+    // ValueVecLayout::validate (constraint_system.rs:686-703)
+    if (!is_pow2(cs->committed_total_len)) {
+      rc = set_error(BINIUS_E_ARG, "ValueVecLenNotPowerOfTwo");
+      break;
+    }
+    if (!is_pow2(cs->offset_witness)) { rc = set_error(BINIUS_E_ARG, "PublicInputPowerOfTwo"); break; }
+    if (cs->offset_witness < 2) { rc = set_error(BINIUS_E_ARG, "PublicInputTooShort"); break; }
+    if (n_constants != cs->n_const || n_constants > (1u << 24)) {
+      rc = set_error(BINIUS_E_ARG, "ConstraintSystem::constants length != n_const");
+      break;
+    }
+    for (uint32_t i = 0; i < n_constants; i++) cs->constants.push_back(r.u64());
+    uint32_t n_and = r.u32();
+    if ((rc = parse_operands(r, n_and, 3, cs->committed_total_len, cs->h_and))) break;
+    uint32_t n_mul = r.u32();
+    if ((rc = parse_operands(r, n_mul, 4, cs->committed_total_len, cs->h_mul))) break;
+    cs->n_and_real = n_and;
+    cs->n_mul_real = n_mul;
+    pad_operands(cs->h_and, next_pow2_at_least(n_and, 8));
+    pad_operands(cs->h_mul, next_pow2_at_least(n_mul, 1));
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    rc = upload(cs->h_and, cs->and_ops);
+    if (!rc) rc = upload(cs->h_mul, cs->mul_ops);
+    cudaSetDevice(prev);
+  } while (0);
+  if (rc) {
+    binius_cs_destroy(cs);
+    return rc;
+  }
+  *out = cs;
+  return clear_error();
+}
+
+int binius_cs_destroy(binius_cs* cs) {
+  if (!cs) return BINIUS_OK;
+  cudaFree(cs->and_ops.offsets);
+  cudaFree(cs->and_ops.terms);
+  cudaFree(cs->mul_ops.offsets);
+  cudaFree(cs->mul_ops.terms);
+  delete cs;
+  return BINIUS_OK;
+}
+
+int binius_cs_info(const binius_cs* cs, uint32_t* h_out12) {
+  BGPU_ARG(cs && h_out12, "NULL argument");
+  uint32_t v[12] = {cs->n_const,      cs->n_inout,         cs->n_witness,     cs->n_internal,
+                    cs->offset_inout, cs->offset_witness,  cs->committed_total_len, cs->n_scratch,
+                    cs->and_ops.n_constraints, cs->mul_ops.n_constraints, cs->n_and_real,
+                    cs->n_mul_real};
+  memcpy(h_out12, v, sizeof(v));
+  return clear_error();
+}
+
+int binius_eval_operands(const binius_cs* cs, const void* d_witness, int which, void* d_out,
+                         void* stream) {
+  BGPU_ARG(cs && d_witness && d_out, "NULL argument");
+  BGPU_ARG(which == 0 || which == 1, "which must be 0 (AND) or 1 (MUL)");
+  return eval_operands(which == 0 ? cs->and_ops : cs->mul_ops,
+                       static_cast<const uint64_t*>(d_witness), static_cast<uint64_t*>(d_out),
+                       as_stream(stream))
+             ? BINIUS_E_CUDA
+             : clear_error();
+}
+
+}  // extern "C"

@@ -1,0 +1,40 @@
+// Constraint-system handle shared by the reduction drivers.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "../../include/binius_gpu.h"
+
+namespace bgpu {
+
+struct HostOperands {
+  uint32_t k = 0;
+  std::vector<uint32_t> offsets;  // n_constraints * k + 1
+  std::vector<uint2> terms;       // (value index, variant << 8 | amount)
+};
+
+struct DevOperands {
+  uint32_t k = 0;
+  uint32_t n_constraints = 0;
+  uint64_t n_terms = 0;
+  uint32_t* offsets = nullptr;
+  uint2* terms = nullptr;
+};
+
+// d_out[slot * n_constraints + i] = eval_operand of constraint i's operand `slot`.
+int eval_operands(const DevOperands& ops, const uint64_t* d_witness, uint64_t* d_out,
+                  cudaStream_t s);
+
+}  // namespace bgpu
+
+struct binius_cs {
+  int device = 0;
+  uint32_t n_const = 0, n_inout = 0, n_witness = 0, n_internal = 0;
+  uint32_t offset_inout = 0, offset_witness = 0, committed_total_len = 0, n_scratch = 0;
+  uint32_t n_and_real = 0, n_mul_real = 0;
+  std::vector<uint64_t> constants;
+  bgpu::HostOperands h_and, h_mul;  // padded (validate_and_prepare)
+  bgpu::DevOperands and_ops, mul_ops;
+};

@@ -186,6 +186,41 @@ int binius_pcs_prove(const binius_pcs* pcs, const binius_pcs_committed* committe
                      binius_transcript* transcript, void* stream);
 
 /* ------------------------------------------------------------------------------------------
+ * Constraint systems.
+ * Replaces: ConstraintSystem::deserialize (verifier/core/src/constraint_system.rs:615-650) with
+ * ValueVecLayout::validate / validate_and_prepare (:466-584); eval_operand
+ * (verifier/core/src/verify.rs:14-35) used by build_bitand_witness / build_intmul_witness
+ * (prover/prover/src/prove.rs:407-465).
+ * The CS is parsed from the reference's v2 wire format, padded (AND to a power of two >= 8, MUL
+ * to a power of two >= 1) and uploaded to `device` in CSR form.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct binius_cs binius_cs;
+
+int binius_cs_from_bytes(int device, const void* h_bytes, size_t len, binius_cs** out);
+int binius_cs_destroy(binius_cs* cs);
+/* h_out12: n_const, n_inout, n_witness, n_internal, offset_inout, offset_witness,
+ * committed_total_len, n_scratch, padded AND count, padded MUL count, AND count, MUL count. */
+int binius_cs_info(const binius_cs* cs, uint32_t* h_out12);
+/* which = 0: AND operands a, b, c -> d_out[3 * n_and] (slot-major); which = 1: MUL operands a, b,
+ * hi, lo -> d_out[4 * n_mul].  d_witness: committed_total_len u64 words. */
+int binius_eval_operands(const binius_cs* cs, const void* d_witness, int which, void* d_out,
+                         void* stream);
+
+/* ------------------------------------------------------------------------------------------
+ * AND reduction.
+ * Replaces: build_bitand_witness + prove_bitand_reduction (prover/prover/src/prove.rs:329-431),
+ * OblongZerocheckProver (prover/prover/src/and_reduction/prover.rs:74-276) with the univariate
+ * round (sumcheck_round_messages.rs:62-136), FoldLookup (fold_lookup.rs:18-92) and the quadratic
+ * MLE-check (protocols/sumcheck/quadratic_mle.rs, prove.rs:89-121).
+ * Samples its challenges from and writes its messages to `transcript`.  h_out_meta receives
+ * a_eval, b_eval, c_eval and the univariate challenge z (4 x 16 bytes); h_out_point the output
+ * evaluation point (log2(padded AND count) x 16 bytes).  Synchronous.
+ * ------------------------------------------------------------------------------------------ */
+int binius_and_reduction_prove(const binius_cs* cs, const void* d_witness,
+                               binius_transcript* transcript, void* h_out_meta,
+                               void* h_out_point, void* stream);
+
+/* ------------------------------------------------------------------------------------------
  * FRI parameters (verifier/verifier/src/fri/common.rs:64-219).
  * ------------------------------------------------------------------------------------------ */
 uint32_t binius_fri_n_test_queries(uint32_t security_bits, uint32_t log_inv_rate);
