@@ -385,3 +385,98 @@ def mle_eval(values: np.ndarray, point: np.ndarray) -> np.ndarray:
     eq = eq_ind_partial_eval(point)
     prods = gf_mul_vec(np.ascontiguousarray(values, dtype=np.uint64), eq)
     return np.bitwise_xor.reduce(prods, axis=0)
+
+
+# ---- shift reduction ----
+
+_u32pp = ctypes.POINTER(ctypes.POINTER(ctypes.c_uint32))
+
+
+def _csr_args(csr):
+    """(keep-alive arrays, u32 pointer triple, u8 variants, n_constraints) for an OperandCSR."""
+    arrs = [np.ascontiguousarray(x, dtype=np.uint32)
+            for x in (csr.offsets, csr.value_index, csr.amount)]
+    arrs = [a if a.size else np.zeros(1, np.uint32) for a in arrs]
+    ptrs = (ctypes.POINTER(ctypes.c_uint32) * 3)(
+        *[a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)) for a in arrs])
+    var = np.ascontiguousarray(csr.variant, dtype=np.uint8)
+    if not var.size:
+        var = np.zeros(1, np.uint8)
+    n = (len(csr.offsets) - 1) // csr.k
+    return (arrs, var), ctypes.cast(ptrs, _u32pp), _p8(var), n
+
+
+def _op_data(d):
+    evals, rz, rx = (np.ascontiguousarray(x, dtype=np.uint64).reshape(-1, 2) for x in d)
+    if rx.size == 0:
+        rx = elems(1)
+    return (evals, rz, rx)
+
+
+def _shift_lib():
+    L = lib()
+    if not getattr(L, "_shift_ready", False):
+        common = [_u64p, ctypes.c_uint32, ctypes.c_uint32, _u32pp, _u8p, ctypes.c_uint32, _u32pp,
+                  _u8p, ctypes.c_uint32, _u64p, _u64p, _u64p, _u64p, _u64p, _u64p]
+        L.orc_shift_prove.argtypes = common + [_u8p, ctypes.c_size_t,
+                                               ctypes.POINTER(ctypes.c_size_t), _u64p, _u64p]
+        L.orc_shift_verify.argtypes = common + [_u8p, ctypes.c_size_t, _u64p, _u64p]
+        L.orc_oblong_eval.argtypes = [_u64p, ctypes.c_uint32, _u64p, _u64p, _u64p]
+        L._shift_ready = True
+    return L
+
+
+def shift_prove(words, log_public, and_csr, mul_csr, and_data, mul_data):
+    """Shift reduction on a fresh transcript.
+
+    and_data / mul_data = (evals, r_zhat', r_x') with AND evals (a, b, c) and MUL evals
+    (a, b, lo, hi).  Returns (proof bytes, point r_j ++ r_y, (witness_eval, initial_sum, claim)).
+    """
+    L = _shift_lib()
+    words = np.ascontiguousarray(words, dtype=np.uint64)
+    log_words = words.shape[0].bit_length() - 1
+    ka, pa, va, na = _csr_args(and_csr)
+    km, pm, vm, nm = _csr_args(mul_csr)
+    ad, md = _op_data(and_data), _op_data(mul_data)
+    cap = 64 * (log_words + 16) + 4096
+    out = np.zeros(cap, dtype=np.uint8)
+    n = ctypes.c_size_t(0)
+    point = elems(6 + log_words)
+    out3 = elems(3)
+    rc = L.orc_shift_prove(_p64(words), log_words, log_public, pa, va, na, pm, vm, nm,
+                           *[_p64(x) for x in ad], *[_p64(x) for x in md], _p8(out), cap,
+                           ctypes.byref(n), _p64(point), _p64(out3))
+    assert rc == 0
+    return out[: n.value].tobytes(), point, out3
+
+
+def shift_verify(public_words, log_words, log_public, and_csr, mul_csr, and_data, mul_data,
+                 proof: bytes):
+    """Restated shift verifier; returns (rc, witness_eval, point) with rc 0 = accepted."""
+    L = _shift_lib()
+    pub = np.ascontiguousarray(public_words, dtype=np.uint64)
+    ka, pa, va, na = _csr_args(and_csr)
+    km, pm, vm, nm = _csr_args(mul_csr)
+    ad, md = _op_data(and_data), _op_data(mul_data)
+    pr = np.frombuffer(proof, dtype=np.uint8).copy()
+    ev = elems(1)
+    point = elems(6 + log_words)
+    rc = L.orc_shift_verify(_p64(pub), log_words, log_public, pa, va, na, pm, vm, nm,
+                            *[_p64(x) for x in ad], *[_p64(x) for x in md], _p8(pr), len(proof),
+                            _p64(ev), _p64(point))
+    return rc, ev[0], point
+
+
+def oblong_eval(values, z, r_x) -> np.ndarray:
+    """sum_c eq(r_x)[c] sum_j bit_j(values[c]) L_j(z) over the {phi(t) : t < 64} domain."""
+    L = _shift_lib()
+    v = np.ascontiguousarray(values, dtype=np.uint64)
+    rx = np.ascontiguousarray(r_x, dtype=np.uint64).reshape(-1, 2)
+    log_n = rx.shape[0]
+    assert v.shape[0] == 1 << log_n
+    if rx.size == 0:
+        rx = elems(1)
+    zz = np.ascontiguousarray(z, dtype=np.uint64).reshape(2)
+    out = elems(1)
+    L.orc_oblong_eval(_p64(v), log_n, _p64(zz), _p64(rx), _p64(out))
+    return out[0]

@@ -100,7 +100,7 @@ int orc_pcs_verify(const uint64_t* twiddles, uint32_t log_msg, uint32_t log_batc
                    uint32_t n_queries, const uint64_t* eval_point, const uint64_t* claim,
                    const uint8_t* proof, size_t proof_len);
 
-/* ---- Operands and the AND reduction (prover/prover/src/and_reduction/*, prove.rs:329-372) ---- */
+/* ---- Operands and the AND reduction (prover/prover/src/and_reduction/, prove.rs:329-372) ---- */
 uint64_t orc_shifted_word(uint64_t w, uint32_t variant, uint32_t amount);
 void orc_and_univariate_round(const uint64_t* a, const uint64_t* b, const uint64_t* c,
                               uint32_t log_n, const uint64_t* big, uint64_t* msg_out);
@@ -110,6 +110,24 @@ int orc_and_reduction_prove(const uint64_t* a, const uint64_t* b, const uint64_t
                             uint64_t* out_meta, uint64_t* out_point);
 int orc_and_reduction_verify(uint32_t log_n, const uint8_t* proof, size_t len, uint64_t* out_meta,
                              uint64_t* out_point);
+
+/* ---- Shift reduction (prover/prover/src/protocols/shift/, verifier/verifier/src/protocols/shift/verify.rs) ----
+ * csr = {offsets, value indices, amounts} (u32 arrays), var = shift variants (u8). */
+int orc_shift_prove(const uint64_t* words, uint32_t log_words, uint32_t log_public,
+                    const uint32_t* const* and_csr, const uint8_t* and_var, uint32_t n_and,
+                    const uint32_t* const* mul_csr, const uint8_t* mul_var, uint32_t n_mul,
+                    const uint64_t* and_evals, const uint64_t* and_rz, const uint64_t* and_rx,
+                    const uint64_t* mul_evals, const uint64_t* mul_rz, const uint64_t* mul_rx,
+                    uint8_t* proof, size_t cap, size_t* len, uint64_t* out_point,
+                    uint64_t* out3);
+int orc_shift_verify(const uint64_t* public_words, uint32_t log_words, uint32_t log_public,
+                     const uint32_t* const* and_csr, const uint8_t* and_var, uint32_t n_and,
+                     const uint32_t* const* mul_csr, const uint8_t* mul_var, uint32_t n_mul,
+                     const uint64_t* and_evals, const uint64_t* and_rz, const uint64_t* and_rx,
+                     const uint64_t* mul_evals, const uint64_t* mul_rz, const uint64_t* mul_rx,
+                     const uint8_t* proof, size_t len, uint64_t* out_eval, uint64_t* out_point);
+void orc_oblong_eval(const uint64_t* v, uint32_t log_n, const uint64_t* z, const uint64_t* r_x,
+                     uint64_t* out);
 
 /* Number of worker threads the oracle may use (1 = scalar). */
 void orc_set_threads(int n);
