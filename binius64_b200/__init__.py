@@ -494,3 +494,29 @@ def and_reduction_prove(cs: DeviceConstraintSystem, witness_words, transcript: P
     m = [int.from_bytes(mb[16 * i:16 * i + 16], "little") for i in range(4)]
     p = [int.from_bytes(pb[16 * i:16 * i + 16], "little") for i in range(log_n)]
     return m, p
+
+
+def _elem_bytes(vals) -> bytes:
+    return b"".join(int(v).to_bytes(16, "little") for v in vals)
+
+
+def shift_reduction_prove(cs: DeviceConstraintSystem, witness_words, transcript: ProverTranscript,
+                          bitand_data, intmul_data, stream=None):
+    """shift::prove.  bitand_data = ((a, b, c) evals, r_zhat', r_x'), intmul_data = ((a, b, lo, hi)
+    evals, r_zhat', r_x'), all as ints.  Returns (r_j ++ r_y, witness_eval) as ints."""
+    (ae, az, ax), (me, mz, mx) = bitand_data, intmul_data
+    if len(ae) != 3 or len(me) != 4:
+        raise ArgumentError(1, "operator data: 3 AND and 4 MUL evaluations")
+    if len(ax) != cs.n_and.bit_length() - 1 or len(mx) != cs.n_mul.bit_length() - 1:
+        raise ArgumentError(1, "operator data: r_x' length != log2(padded constraint count)")
+    band = _elem_bytes([*ae, az, *ax])
+    bmul = _elem_bytes([*me, mz, *mx])
+    n_point = 6 + cs.committed_total_len.bit_length() - 1
+    point = (ctypes.c_uint8 * (16 * n_point))()
+    ev = (ctypes.c_uint8 * 16)()
+    check(lib().binius_shift_reduction_prove(cs.handle, witness_words.data_ptr(), transcript.handle,
+                                             band, bmul, ctypes.addressof(point),
+                                             ctypes.addressof(ev), _stream(stream)))
+    pb = bytes(point)
+    return ([int.from_bytes(pb[16 * i:16 * i + 16], "little") for i in range(n_point)],
+            int.from_bytes(bytes(ev), "little"))

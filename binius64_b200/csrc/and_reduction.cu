@@ -31,6 +31,7 @@
 #include "gf128.cuh"
 #include "internal.h"
 #include "kernels.h"
+#include "reductions.h"
 #include "transcript.h"
 
 using namespace bgpu;
@@ -428,10 +429,19 @@ unsigned grid_for(uint64_t n, unsigned threads, unsigned cap = 148 * 8) {
 
 namespace bgpu {
 
-struct AndResult {
-  u128h a_eval, b_eval, c_eval, z;
-  std::vector<u128h> eval_point;
-};
+void lagrange_phi(uint32_t dim, hu128 x, hu128* out) { lagrange_b128(dim, x, out); }
+hu128 phi_elem(uint32_t b) { return and_constants().phi[b & 255]; }
+
+int fold_words64(const uint64_t* d_words, uint64_t n, const hu128* vec64, uint4* d_out,
+                 cudaStream_t s) {
+  if (n == 0) return BINIUS_OK;
+  Lag64 l64;
+  for (int i = 0; i < 64; i++) l64.l[i] = to_uint4(vec64[i]);
+  fold_words_kernel<<<grid_for(n, 256), 256, 0, s>>>(d_words, n, l64, d_out);
+  BGPU_LAUNCH_CHECK("fold_words_kernel");
+  count_launch();
+  return BINIUS_OK;
+}
 
 // d_witness: committed_total_len words; writes the AND reduction's transcript messages.
 int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcript& t,

@@ -144,6 +144,45 @@ int upload(const HostOperands& h, DevOperands& d) {
 
 bool is_pow2(uint32_t v) { return v && !(v & (v - 1)); }
 
+// Counting sort of all operand terms by shift key (see ShiftTerms).
+int build_shift_terms(const HostOperands& and_h, const HostOperands& mul_h, ShiftTerms& d) {
+  static const uint8_t and_class[3] = {0, 1, 2};
+  static const uint8_t mul_class[4] = {3, 4, 6, 5};  // CSR slots (a, b, hi, lo)
+  std::vector<uint32_t> count(kShiftKeys + 1, 0);
+  auto key_of = [](uint32_t packed, uint32_t cls) {
+    return (uint32_t)(((packed >> 8) * 64 + (packed & 255)) * 8 + cls);
+  };
+  auto visit = [&](const HostOperands& h, const uint8_t* cls, auto&& fn) {
+    const uint32_t groups = (uint32_t)(h.offsets.size() - 1);
+    for (uint32_t g = 0; g < groups; g++)
+      for (uint32_t t = h.offsets[g]; t < h.offsets[g + 1]; t++)
+        fn(h.terms[t], g / h.k, key_of(h.terms[t].y, cls[g % h.k]));
+  };
+  visit(and_h, and_class, [&](uint2, uint32_t, uint32_t k) { count[k + 1]++; });
+  visit(mul_h, mul_class, [&](uint2, uint32_t, uint32_t k) { count[k + 1]++; });
+  for (uint32_t k = 0; k < kShiftKeys; k++) count[k + 1] += count[k];
+  const uint64_t n = count[kShiftKeys];
+  std::vector<uint32_t> vi(n ? n : 1), cc(n ? n : 1);
+  std::vector<uint16_t> key(n ? n : 1);
+  auto place = [&](uint2 term, uint32_t c, uint32_t k) {
+    const uint32_t pos = count[k]++;
+    vi[pos] = term.x;
+    cc[pos] = c;
+    key[pos] = (uint16_t)k;
+  };
+  visit(and_h, and_class, place);
+  visit(mul_h, mul_class, place);
+  d.n = n;
+  const size_t m = n ? n : 1;
+  BGPU_CUDA(cudaMalloc(&d.vi, 4 * m));
+  BGPU_CUDA(cudaMalloc(&d.c, 4 * m));
+  BGPU_CUDA(cudaMalloc(&d.key, 2 * m));
+  BGPU_CUDA(cudaMemcpy(d.vi, vi.data(), 4 * m, cudaMemcpyHostToDevice));
+  BGPU_CUDA(cudaMemcpy(d.c, cc.data(), 4 * m, cudaMemcpyHostToDevice));
+  BGPU_CUDA(cudaMemcpy(d.key, key.data(), 2 * m, cudaMemcpyHostToDevice));
+  return BINIUS_OK;
+}
+
 }  // namespace
 
 namespace bgpu {
@@ -205,6 +244,7 @@ int binius_cs_from_bytes(int device, const void* h_bytes, size_t len, binius_cs*
     cudaSetDevice(device);
     rc = upload(cs->h_and, cs->and_ops);
     if (!rc) rc = upload(cs->h_mul, cs->mul_ops);
+    if (!rc) rc = build_shift_terms(cs->h_and, cs->h_mul, cs->shift_terms);
     cudaSetDevice(prev);
   } while (0);
   if (rc) {
@@ -221,6 +261,9 @@ int binius_cs_destroy(binius_cs* cs) {
   cudaFree(cs->and_ops.terms);
   cudaFree(cs->mul_ops.offsets);
   cudaFree(cs->mul_ops.terms);
+  cudaFree(cs->shift_terms.vi);
+  cudaFree(cs->shift_terms.c);
+  cudaFree(cs->shift_terms.key);
   delete cs;
   return BINIUS_OK;
 }

@@ -23,6 +23,20 @@ struct DevOperands {
   uint2* terms = nullptr;
 };
 
+// Operand terms of both operations in the order the shift reduction consumes them: sorted by
+// key = (variant * 64 + amount) * 8 + class, class 0..2 the AND operands (a, b, c) and 3..6 the
+// MUL operands in KeyCollection order (a, b, lo, hi).  One entry per term; the reference's
+// KeyCollection (prover/prover/src/protocols/shift/key_collection.rs:246-312) groups the same
+// terms by word and id, and every quantity the reduction takes from it is a sum over terms.
+struct ShiftTerms {
+  uint64_t n = 0;
+  uint32_t* vi = nullptr;   // value index
+  uint32_t* c = nullptr;    // constraint index within its operation
+  uint16_t* key = nullptr;
+};
+constexpr uint32_t kShiftKeys = 512 * 8;
+constexpr uint32_t kShiftClasses = 7;
+
 // d_out[slot * n_constraints + i] = eval_operand of constraint i's operand `slot`.
 int eval_operands(const DevOperands& ops, const uint64_t* d_witness, uint64_t* d_out,
                   cudaStream_t s);
@@ -37,4 +51,5 @@ struct binius_cs {
   std::vector<uint64_t> constants;
   bgpu::HostOperands h_and, h_mul;  // padded (validate_and_prepare)
   bgpu::DevOperands and_ops, mul_ops;
+  bgpu::ShiftTerms shift_terms;
 };

@@ -1,0 +1,47 @@
+// CTA-wide XOR (GF(2^128) addition) reductions with atomicXor accumulation into global memory.
+#pragma once
+#include "gf128.cuh"
+
+namespace bgpu {
+
+__device__ __forceinline__ void atomic_xor_gf(uint32_t* dst, uint4 v) {
+  if (v.x) atomicXor(dst + 0, v.x);
+  if (v.y) atomicXor(dst + 1, v.y);
+  if (v.z) atomicXor(dst + 2, v.z);
+  if (v.w) atomicXor(dst + 3, v.w);
+}
+
+__device__ __forceinline__ uint4 shfl_xor_gf(uint4 v, int lane_mask) {
+  v.x = __shfl_xor_sync(0xffffffffu, v.x, lane_mask);
+  v.y = __shfl_xor_sync(0xffffffffu, v.y, lane_mask);
+  v.z = __shfl_xor_sync(0xffffffffu, v.z, lane_mask);
+  v.w = __shfl_xor_sync(0xffffffffu, v.w, lane_mask);
+  return v;
+}
+
+// XOR-reduces `NV` field values across the CTA and adds the totals into dst[0..NV) (4 words
+// each).  Every thread of the CTA must call it.
+template <int NV>
+__device__ __forceinline__ void block_xor_reduce(uint4 (&v)[NV], uint32_t* dst) {
+  __shared__ uint4 red[NV][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; q++) {
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) gf_add_into(v[q], shfl_xor_gf(v[q], m));
+    if (lane == 0) red[q][warp] = v[q];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nwarps = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; q++) {
+      uint4 x = lane < nwarps ? red[q][lane] : gf_zero();
+#pragma unroll
+      for (int m = 16; m >= 1; m >>= 1) gf_add_into(x, shfl_xor_gf(x, m));
+      if (lane == 0) atomic_xor_gf(dst + 4 * q, x);
+    }
+  }
+}
+
+}  // namespace bgpu

@@ -4,6 +4,7 @@
 #include <stdint.h>
 
 #include "../../include/binius_gpu.h"
+#include "internal.h"
 
 namespace bgpu {
 
@@ -36,6 +37,15 @@ int bivariate_eval(const uint4* d_a, const uint4* d_b, uint64_t half, uint32_t* 
 int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[16],
                         uint32_t* d_out8, cudaStream_t s);
 int gather_segments(const GatherSegment* d_segs, uint32_t n, uint8_t* d_dst, cudaStream_t s);
+
+// Lagrange basis of the subspace {phi(t) : t < 2^dim} at x, phi the AES-to-GHASH embedding
+// (BinarySubspace::<AESTowerField8b>::with_dim(dim).isomorphic(), lagrange_evals).
+void lagrange_phi(uint32_t dim, hu128 x, hu128* out);
+hu128 phi_elem(uint32_t b);
+// d_out[i] = sum over set bits t of d_words[i] of vec64[t] (fold_words, prover/prover/src/
+// fold_word.rs:77-96).
+int fold_words64(const uint64_t* d_words, uint64_t n, const hu128* vec64, uint4* d_out,
+                 cudaStream_t s);
 
 // From the other translation units.
 int rs_encode_batch(const binius_ntt* ntt, const void* d_msg, uint32_t log_dim,

@@ -1,0 +1,45 @@
+// The constraint reductions of Prover::prove (prover/prover/src/prove.rs:124-303) as host drivers
+// over device data; each writes its messages into the host transcript.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "cs.h"
+#include "internal.h"
+#include "transcript.h"
+
+namespace bgpu {
+
+// AndCheckOutput (prover/prover/src/and_reduction/prover.rs): the three operand evaluations at
+// (z, eval_point).
+struct AndResult {
+  hu128 a_eval, b_eval, c_eval, z;
+  std::vector<hu128> eval_point;
+};
+
+// d_witness: committed_total_len words; writes the AND reduction's transcript messages.
+int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcript& t,
+                        AndResult& res, cudaStream_t s);
+
+// OperatorData (prover/prover/src/protocols/shift/prove.rs:20-33): operand evaluations at the
+// oblong point (r_zhat', r_x').  AND: (a, b, c); MUL: (a, b, lo, hi).
+struct ShiftOperatorData {
+  std::vector<hu128> evals;
+  hu128 r_zhat = 0;
+  std::vector<hu128> r_x;
+};
+
+// SumcheckOutput of shift::prove: point r_j ++ r_y and the witness evaluation there.
+struct ShiftResult {
+  std::vector<hu128> point;
+  hu128 witness_eval = 0;
+};
+
+int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcript& t,
+                          const ShiftOperatorData& bitand_data,
+                          const ShiftOperatorData& intmul_data, ShiftResult& res,
+                          cudaStream_t s);
+
+}  // namespace bgpu

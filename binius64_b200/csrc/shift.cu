@@ -1,0 +1,557 @@
+// Shift reduction (prover/prover/src/protocols/shift/prove.rs:103-153) on the device.
+//
+// Phase 1 (phase_1.rs:43-276): the g parts g_v[s*64 + j] = sum over operand terms with shift
+// (v, s) of lambda^(operand+1) * eq(r_x')[constraint] * bit_j(word), and the h parts
+// (monster.rs:34-104) built from the Lagrange basis of {phi(t) : t < 64} at r_zhat'.  The eight
+// (g_v, h_v) pairs live interleaved as one array of 8 * 4096 elements, index (s*64 + j)*8 + v, so
+// the eight bivariate provers' top-variable folds are the top-variable fold of that one array and
+// their summed round sums are its round sums.
+//
+// g is accumulated from the key-sorted term table (ShiftTerms): terms arrive grouped by
+// key = (v*64 + s)*8 + operand class, a CTA stages 256 of them in shared memory (eq value of the
+// constraint and the witness word), and each 64-thread group owns the 64 bit positions j of its
+// slice, XOR-adding eq into the position's accumulator when bit j of the word is set.  A group
+// sees keys in increasing order and flushes its accumulators with atomicXor when the key changes;
+// the lambda powers are applied once per (key, j) afterwards.
+//
+// Phase 2 (phase_2.rs:56-160): r_j_witness = fold_words(words, eq(r_j)), the monster multilinear
+// (monster.rs:138-219) M[w] = sum over terms of word w of lambda^(operand+1) eq(r_x')[c]
+// h_op[v] eq(r_s)[s] (one multiply per term into a per-key scalar table, atomicXor into M), then
+// the batched sumcheck of the bivariate product (r_j_witness, M) with the in/out MLE-check
+// (protocols/inout_check.rs:19-211, sumcheck/mle_to_sumcheck.rs:28-77, sumcheck/batch.rs:41-103).
+// Round polynomials and challenges pass through the host transcript between launches.
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "cs.h"
+#include "gf128.cuh"
+#include "gf_reduce.cuh"
+#include "internal.h"
+#include "kernels.h"
+#include "reductions.h"
+#include "transcript.h"
+
+using namespace bgpu;
+
+namespace {
+
+constexpr uint32_t kLen = 4096;           // 2^(2 * LOG_WORD_SIZE_BITS)
+constexpr uint32_t kFlat = 8 * kLen;      // eight shift variants
+constexpr uint32_t kNoKey = 0xffffffffu;
+constexpr int kTile = 256;
+
+struct Lag64 {
+  uint4 l[64];
+};
+
+struct ClassPowers {
+  uint4 p[8];  // lambda power of each operand class (class 7 unused)
+};
+
+unsigned grid_for(uint64_t n, unsigned threads, unsigned cap = 148 * 8) {
+  uint64_t g = (n + threads - 1) / threads;
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, cap));
+}
+
+__device__ __forceinline__ const uint4* eq_of_class(uint32_t key, const uint4* eq_and,
+                                                    const uint4* eq_mul) {
+  return (key & 7) < 3 ? eq_and : eq_mul;
+}
+
+// g_raw[key * 64 + j] += sum over terms with that key of eq[c] * bit_j(word).
+__global__ void __launch_bounds__(kTile)
+    shift_g_kernel(const uint32_t* __restrict__ vi, const uint32_t* __restrict__ cidx,
+                   const uint16_t* __restrict__ keys, uint64_t n,
+                   const uint64_t* __restrict__ words, const uint4* __restrict__ eq_and,
+                   const uint4* __restrict__ eq_mul, uint32_t* __restrict__ g_raw) {
+  __shared__ uint4 s_eq[kTile];
+  __shared__ uint64_t s_w[kTile];
+  __shared__ uint32_t s_key[kTile];
+  const uint32_t j = threadIdx.x & 63, grp = threadIdx.x >> 6;
+  uint32_t cur = kNoKey;
+  uint4 acc = gf_zero();
+  const uint64_t n_tiles = (n + kTile - 1) / kTile;
+  for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const uint64_t t = tile * kTile + threadIdx.x;
+    __syncthreads();
+    if (t < n) {
+      const uint32_t k = keys[t];
+      s_key[threadIdx.x] = k;
+      s_eq[threadIdx.x] = __ldg(eq_of_class(k, eq_and, eq_mul) + cidx[t]);
+      s_w[threadIdx.x] = __ldg(words + vi[t]);
+    } else {
+      s_key[threadIdx.x] = kNoKey;
+      s_eq[threadIdx.x] = gf_zero();
+      s_w[threadIdx.x] = 0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int q = 0; q < 64; q++) {
+      const int e = grp * 64 + q;
+      const uint32_t k = s_key[e];
+      if (k != cur) {
+        if (cur != kNoKey) atomic_xor_gf(g_raw + 4 * ((uint64_t)cur * 64 + j), acc);
+        cur = k;
+        acc = gf_zero();
+      }
+      const uint32_t m = 0u - (uint32_t)((s_w[e] >> j) & 1);
+      const uint4 x = s_eq[e];
+      acc.x ^= x.x & m;
+      acc.y ^= x.y & m;
+      acc.z ^= x.z & m;
+      acc.w ^= x.w & m;
+    }
+  }
+  if (cur != kNoKey) atomic_xor_gf(g_raw + 4 * ((uint64_t)cur * 64 + j), acc);
+}
+
+// g[(s*64 + j)*8 + v] = sum over classes of lambda_class * g_raw[((v*64 + s)*8 + class)*64 + j].
+__global__ void shift_g_combine_kernel(const uint4* __restrict__ g_raw, ClassPowers pw,
+                                       uint4* __restrict__ g) {
+  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= kFlat) return;
+  const uint32_t v = idx & 7, s = (idx >> 3) >> 6, j = (idx >> 3) & 63;
+  const uint32_t id = v * 64 + s;
+  u256 acc = {0, 0, 0, 0};
+#pragma unroll
+  for (uint32_t cls = 0; cls < kShiftClasses; cls++) {
+    const uint4 x = g_raw[(id * 8 + cls) * 64 + j];
+    if (!gf_is_zero(x)) xor_into(acc, clmul128(x, pw.p[cls]));
+  }
+  g[idx] = reduce256(acc);
+}
+
+// build_h_parts (monster.rs:34-104) from l_tilde, interleaved layout.
+__global__ void shift_h_kernel(Lag64 L, uint4* __restrict__ h) {
+  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= kFlat) return;
+  const uint32_t v = idx & 7, s = (idx >> 3) >> 6, j = (idx >> 3) & 63;
+  uint4 val = gf_zero();
+  if (v < 4) {
+    switch (v) {
+      case 0:  // sll
+        if (j + s < 64) val = L.l[s + j];
+        break;
+      case 1:  // srl
+        if (j >= s) val = L.l[j - s];
+        break;
+      case 2:  // sra
+        if (j >= s) val = L.l[j - s];
+        if (j == 63)
+          for (uint32_t t = 64 - s; t < 64; t++) gf_add_into(val, L.l[t]);
+        break;
+      default:  // rotr
+        val = j < s ? L.l[64 - s + j] : L.l[j - s];
+        break;
+    }
+  } else {
+    const uint32_t s32 = s & 31, base = j & 32, jj = j & 31;
+    switch (v) {
+      case 4:  // sll32
+        if (jj + s32 < 32) val = L.l[base + s32 + jj];
+        break;
+      case 5:  // srl32
+        if (jj >= s32) val = L.l[base + jj - s32];
+        break;
+      case 6:  // sra32
+        if (jj >= s32) val = L.l[base + jj - s32];
+        if (jj == 31)
+          for (uint32_t t = 32 - s32; t < 32; t++) gf_add_into(val, L.l[base + t]);
+        break;
+      default:  // rotr32
+        val = jj < s32 ? L.l[base + 32 - s32 + jj] : L.l[base + jj - s32];
+        break;
+    }
+  }
+  h[idx] = val;
+}
+
+// out[v] = <h_v, eq(r_j ++ r_s)> for the 8 variants (evaluate_h_op).  One CTA of 256 threads.
+__global__ void __launch_bounds__(256)
+    shift_h_ops_kernel(const uint4* __restrict__ h, const uint4* __restrict__ eq,
+                       uint4* __restrict__ out) {
+  __shared__ uint4 part[256];
+  const uint32_t v = threadIdx.x & 7;
+  u256 acc = {0, 0, 0, 0};
+  for (uint32_t i = threadIdx.x >> 3; i < kLen; i += 32) xor_into(acc, clmul128(h[i * 8 + v], eq[i]));
+  part[threadIdx.x] = reduce256(acc);
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    uint4 x = gf_zero();
+    for (uint32_t q = 0; q < 32; q++) gf_add_into(x, part[q * 8 + threadIdx.x]);
+    out[threadIdx.x] = x;
+  }
+}
+
+// T[key] = lambda_class * h_op(kind)[v] * eq(r_s)[s] (the monster scalars, monster.rs:168-190).
+__global__ void shift_scalars_kernel(ClassPowers pw, Lag64 eq_rs, const uint4* __restrict__ h_ops,
+                                     uint4* __restrict__ T) {
+  const uint32_t key = blockIdx.x * blockDim.x + threadIdx.x;
+  if (key >= kShiftKeys) return;
+  const uint32_t cls = key & 7, id = key >> 3, v = id >> 6, s = id & 63;
+  if (cls >= kShiftClasses) {
+    T[key] = gf_zero();
+    return;
+  }
+  const uint4 hop = h_ops[(cls < 3 ? 0 : 8) + v];
+  T[key] = gf_mul(gf_mul(pw.p[cls], hop), eq_rs.l[s]);
+}
+
+// M[vi] += T[key] * eq[c] for every term.
+__global__ void __launch_bounds__(256)
+    shift_monster_kernel(const uint32_t* __restrict__ vi, const uint32_t* __restrict__ cidx,
+                         const uint16_t* __restrict__ keys, uint64_t n,
+                         const uint4* __restrict__ eq_and, const uint4* __restrict__ eq_mul,
+                         const uint4* __restrict__ T, uint32_t* __restrict__ M) {
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t k = keys[t];
+    const uint4 e = __ldg(eq_of_class(k, eq_and, eq_mul) + cidx[t]);
+    atomic_xor_gf(M + 4 * (uint64_t)vi[t], gf_mul(__ldg(T + k), e));
+  }
+}
+
+// out[0] += <x[off0 ..], eq>, out[1] += <x[off1 ..], eq> over len elements.
+__global__ void __launch_bounds__(256)
+    dot2_kernel(const uint4* __restrict__ x, uint64_t off0, uint64_t off1,
+                const uint4* __restrict__ eq, uint64_t len, uint32_t* __restrict__ out) {
+  u256 a0 = {0, 0, 0, 0}, a1 = {0, 0, 0, 0};
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < len;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint4 e = eq[i];
+    xor_into(a0, clmul128(x[off0 + i], e));
+    xor_into(a1, clmul128(x[off1 + i], e));
+  }
+  uint4 v[2] = {reduce256(a0), reduce256(a1)};
+  block_xor_reduce<2>(v, out);
+}
+
+// ------------------------------------------------------------------ host helpers
+
+uint4 u4(hu128 v) {
+  uint4 r;
+  memcpy(&r, &v, 16);
+  return r;
+}
+hu128 h128(const void* p) {
+  hu128 v;
+  memcpy(&v, p, 16);
+  return v;
+}
+hu128 sample(Transcript& t) {
+  uint8_t b[16];
+  t.sample_elem(b);
+  return h128(b);
+}
+void eq_host(const hu128* point, uint32_t n, hu128* out) {
+  out[0] = 1;
+  for (uint32_t i = 0; i < n; i++) {
+    const size_t half = (size_t)1 << i;
+    for (size_t k = 0; k < half; k++) {
+      const hu128 hi = host_gf_mul(out[k], point[i]);
+      out[half + k] = hi;
+      out[k] ^= hi;
+    }
+  }
+}
+std::vector<uint4> to_u4(const std::vector<hu128>& v) {
+  std::vector<uint4> r(v.size());
+  for (size_t i = 0; i < v.size(); i++) r[i] = u4(v[i]);
+  return r;
+}
+uint32_t log2_ceil(uint64_t n) {
+  uint32_t r = 0;
+  while ((1ull << r) < n) r++;
+  return r;
+}
+
+// Device buffers of one shift reduction (freed on every exit path).
+struct ShiftBuffers {
+  cudaStream_t s;
+  std::vector<void*> ptrs;
+  explicit ShiftBuffers(cudaStream_t st) : s(st) {}
+  ~ShiftBuffers() {
+    for (void* p : ptrs) cudaFreeAsync(p, s);
+  }
+  template <class T>
+  int alloc(T** p, size_t bytes) {
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(p), bytes ? bytes : 16, s);
+    if (e != cudaSuccess) return cuda_error(e, "shift reduction buffers");
+    ptrs.push_back(*p);
+    return BINIUS_OK;
+  }
+};
+
+#define SHIFT_TRY(expr)                 \
+  do {                                  \
+    if (int _rc = (expr)) return _rc;   \
+  } while (0)
+
+int launched(const char* what, uint64_t n = 1) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, what);
+  count_launch(n);
+  return BINIUS_OK;
+}
+
+int d2h_sync(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  BGPU_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+  BGPU_CUDA(cudaStreamSynchronize(s));
+  return BINIUS_OK;
+}
+
+}  // namespace
+
+namespace bgpu {
+
+int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcript& t,
+                          const ShiftOperatorData& band, const ShiftOperatorData& bmul,
+                          ShiftResult& res, cudaStream_t s) {
+  const uint64_t n_words = cs->committed_total_len;
+  const uint32_t log_words = log2_ceil(n_words);
+  const uint32_t log_public = log2_ceil(cs->offset_witness);
+  const uint32_t log_and = log2_ceil(cs->and_ops.n_constraints);
+  const uint32_t log_mul = log2_ceil(cs->mul_ops.n_constraints);
+  if (band.evals.size() != 3 || bmul.evals.size() != 4)
+    return set_error(BINIUS_E_ARG, "operator data: 3 AND and 4 MUL evaluations");
+  if (band.r_x.size() != log_and || bmul.r_x.size() != log_mul)
+    return set_error(BINIUS_E_ARG, "operator data: r_x' length != log2(constraints)");
+  if (log_public < 1 || log_public > log_words)
+    return set_error(BINIUS_E_ARG, "public segment must hold 2..committed words");
+  const ShiftTerms& terms = cs->shift_terms;
+
+  ShiftBuffers B(s);
+  uint4 *eq_and, *eq_mul, *g, *h, *h_keep, *eq_rjs, *h_ops, *T, *W, *M, *eq_pub;
+  uint32_t *g_raw, *acc;
+  SHIFT_TRY(B.alloc(&eq_and, 16ull << log_and));
+  SHIFT_TRY(B.alloc(&eq_mul, 16ull << log_mul));
+  SHIFT_TRY(B.alloc(&g_raw, 16ull * kShiftKeys * 64));
+  SHIFT_TRY(B.alloc(&g, 16ull * kFlat));
+  SHIFT_TRY(B.alloc(&h, 16ull * kFlat));
+  SHIFT_TRY(B.alloc(&h_keep, 16ull * kFlat * 2));
+  SHIFT_TRY(B.alloc(&eq_rjs, 16ull * kLen));
+  SHIFT_TRY(B.alloc(&h_ops, 16ull * 16));
+  SHIFT_TRY(B.alloc(&T, 16ull * kShiftKeys));
+  SHIFT_TRY(B.alloc(&W, 16ull * n_words));
+  SHIFT_TRY(B.alloc(&M, 16ull * n_words));
+  SHIFT_TRY(B.alloc(&eq_pub, 16ull << (log_public > 0 ? log_public - 1 : 0)));
+  SHIFT_TRY(B.alloc(&acc, 64));
+
+  // lambdas and their powers per operand class
+  const hu128 lam_and = sample(t), lam_mul = sample(t);
+  ClassPowers pw;
+  memset(&pw, 0, sizeof(pw));
+  {
+    hu128 p = lam_and;
+    for (int i = 0; i < 3; i++, p = host_gf_mul(p, lam_and)) pw.p[i] = u4(p);
+    p = lam_mul;
+    for (int i = 0; i < 4; i++, p = host_gf_mul(p, lam_mul)) pw.p[3 + i] = u4(p);
+  }
+  SHIFT_TRY(eq_tensor(to_u4(band.r_x).data(), log_and, eq_and, s));
+  SHIFT_TRY(eq_tensor(to_u4(bmul.r_x).data(), log_mul, eq_mul, s));
+
+  // ---- phase 1: g and h parts
+  BGPU_CUDA(cudaMemsetAsync(g_raw, 0, 16ull * kShiftKeys * 64, s));
+  if (terms.n) {
+    shift_g_kernel<<<grid_for(terms.n, kTile, 148 * 8), kTile, 0, s>>>(
+        terms.vi, terms.c, terms.key, terms.n, d_witness, eq_and, eq_mul, g_raw);
+    SHIFT_TRY(launched("shift_g_kernel"));
+  }
+  shift_g_combine_kernel<<<kFlat / 256, 256, 0, s>>>(reinterpret_cast<const uint4*>(g_raw), pw, g);
+  SHIFT_TRY(launched("shift_g_combine_kernel"));
+  const bool same_z = band.r_zhat == bmul.r_zhat;
+  for (int kind = 0; kind < (same_z ? 1 : 2); kind++) {
+    hu128 lt[64];
+    lagrange_phi(6, kind == 0 ? band.r_zhat : bmul.r_zhat, lt);
+    Lag64 L;
+    for (int i = 0; i < 64; i++) L.l[i] = u4(lt[i]);
+    shift_h_kernel<<<kFlat / 256, 256, 0, s>>>(L, h_keep + kind * kFlat);
+    SHIFT_TRY(launched("shift_h_kernel"));
+  }
+  BGPU_CUDA(cudaMemcpyAsync(h, h_keep, 16ull * kFlat, cudaMemcpyDeviceToDevice, s));
+
+  // the provers' claims: sum_v <g_v, h_v> (phase_1.rs:96-101)
+  BGPU_CUDA(cudaMemsetAsync(acc + 8, 0, 32, s));
+  dot2_kernel<<<grid_for(kFlat, 256, 148), 256, 0, s>>>(g, 0, 0, h, kFlat, acc + 8);
+  SHIFT_TRY(launched("dot2_kernel"));
+  std::vector<hu128> ch1;
+  hu128 sum = 0;
+  uint8_t rb[16] = {0};
+  hu128 gamma = 0;
+  for (int round = 0; round < 12; round++) {
+    const uint64_t size = (uint64_t)kFlat >> round;  // before this round's fold
+    if (round == 0) {
+      SHIFT_TRY(bivariate_eval(g, h, size / 2, acc, s));
+    } else {
+      SHIFT_TRY(bivariate_fold_eval(g, h, size * 2, rb, acc, s));
+    }
+    uint8_t host[64 + 2 * 16 * 16];
+    const bool last = round == 11;
+    BGPU_CUDA(cudaMemcpyAsync(host, acc, round == 0 ? 64 : 32, cudaMemcpyDeviceToHost, s));
+    if (last) {
+      BGPU_CUDA(cudaMemcpyAsync(host + 64, g, 256, cudaMemcpyDeviceToHost, s));
+      BGPU_CUDA(cudaMemcpyAsync(host + 64 + 256, h, 256, cudaMemcpyDeviceToHost, s));
+    }
+    BGPU_CUDA(cudaStreamSynchronize(s));
+    if (round == 0) sum = h128(host + 32);
+    const hu128 y1 = h128(host), yinf = h128(host + 16);
+    const hu128 c0 = sum ^ y1, c2 = yinf, c1 = y1 ^ c0 ^ c2;
+    uint8_t rp[32];
+    memcpy(rp, &c0, 16);
+    memcpy(rp + 16, &c1, 16);
+    t.message(rp, 32);
+    t.sample_elem(rb);
+    const hu128 r = h128(rb);
+    ch1.push_back(r);
+    sum = c0 ^ host_gf_mul(c1, r) ^ host_gf_mul(c2, host_gf_mul(r, r));
+    if (last) {
+      // fold the remaining 16-element arrays by r; gamma = sum_v g_v(r) h_v(r)
+      for (int v = 0; v < 8; v++) {
+        const hu128 g0 = h128(host + 64 + 16 * v), g1 = h128(host + 64 + 16 * (8 + v));
+        const hu128 h0 = h128(host + 320 + 16 * v), h1 = h128(host + 320 + 16 * (8 + v));
+        gamma ^= host_gf_mul(g0 ^ host_gf_mul(r, g1 ^ g0), h0 ^ host_gf_mul(r, h1 ^ h0));
+      }
+    }
+  }
+  std::vector<hu128> rev(ch1.rbegin(), ch1.rend());
+  std::vector<hu128> r_j(rev.begin(), rev.begin() + 6), r_s(rev.begin() + 6, rev.end());
+
+  // ---- phase 2: fold the words at r_j, build the monster multilinear
+  hu128 eq_rj[64], eq_rs[64];
+  eq_host(r_j.data(), 6, eq_rj);
+  eq_host(r_s.data(), 6, eq_rs);
+  SHIFT_TRY(fold_words64(d_witness, n_words, eq_rj, W, s));
+  SHIFT_TRY(eq_tensor(to_u4(rev).data(), 12, eq_rjs, s));
+  for (int kind = 0; kind < 2; kind++) {
+    const uint4* hk = h_keep + ((same_z || kind == 0) ? 0 : kFlat);
+    shift_h_ops_kernel<<<1, 256, 0, s>>>(hk, eq_rjs, h_ops + 8 * kind);
+    SHIFT_TRY(launched("shift_h_ops_kernel"));
+  }
+  Lag64 ers;
+  for (int i = 0; i < 64; i++) ers.l[i] = u4(eq_rs[i]);
+  shift_scalars_kernel<<<kShiftKeys / 256, 256, 0, s>>>(pw, ers, h_ops, T);
+  SHIFT_TRY(launched("shift_scalars_kernel"));
+  BGPU_CUDA(cudaMemsetAsync(M, 0, 16ull * n_words, s));
+  if (terms.n) {
+    shift_monster_kernel<<<grid_for(terms.n, 256, 148 * 16), 256, 0, s>>>(
+        terms.vi, terms.c, terms.key, terms.n, eq_and, eq_mul, T, reinterpret_cast<uint32_t*>(M));
+    SHIFT_TRY(launched("shift_monster_kernel"));
+  }
+
+  // in/out check point and the public evaluation (InOutCheckProver::new)
+  const uint32_t p = log_public;
+  std::vector<hu128> z(p);
+  for (auto& v : z) v = sample(t);
+  auto dot2 = [&](uint64_t off0, uint64_t off1, uint64_t len) -> int {
+    BGPU_CUDA(cudaMemsetAsync(acc + 8, 0, 32, s));
+    dot2_kernel<<<grid_for(len, 256, 148 * 2), 256, 0, s>>>(W, off0, off1, eq_pub, len, acc + 8);
+    SHIFT_TRY(launched("dot2_kernel"));
+    return BINIUS_OK;
+  };
+  auto read2 = [&](hu128& o0, hu128& o1) -> int {
+    uint8_t b[32];
+    SHIFT_TRY(d2h_sync(b, acc + 8, 32, s));
+    o0 = h128(b);
+    o1 = h128(b + 16);
+    return BINIUS_OK;
+  };
+  uint32_t gn = p;  // Gruen32::n_vars_remaining
+  SHIFT_TRY(eq_tensor(to_u4(z).data(), gn - 1, eq_pub, s));
+  hu128 lo, hi;
+  SHIFT_TRY(dot2(0, 1ull << (gn - 1), 1ull << (gn - 1)));
+  SHIFT_TRY(read2(lo, hi));
+  hu128 inout_eval = lo ^ host_gf_mul(hi ^ lo, z[gn - 1]);
+
+  const hu128 beta = sample(t);
+  hu128 shift_sum = gamma, eq_prefix = 1;
+  std::vector<hu128> ch2;
+  for (uint32_t n_rem = log_words; n_rem > 0; n_rem--) {
+    const uint64_t half = 1ull << (n_rem - 1);
+    if (n_rem == log_words) {
+      SHIFT_TRY(bivariate_eval(W, M, half, acc, s));
+    } else {
+      SHIFT_TRY(bivariate_fold_eval(W, M, half * 4, rb, acc, s));
+    }
+    const bool early = p < n_rem;
+    if (early) {
+      SHIFT_TRY(dot2(half, half + (1ull << (gn - 1)), 1ull << (gn - 1)));
+    } else {
+      SHIFT_TRY(eq_tensor(to_u4(z).data(), n_rem - 1, eq_pub, s));
+      SHIFT_TRY(dot2(half, half, half));
+    }
+    uint8_t host[64 + 32];
+    BGPU_CUDA(cudaMemcpyAsync(host, acc, 64, cudaMemcpyDeviceToHost, s));
+    if (n_rem == 1) BGPU_CUDA(cudaMemcpyAsync(host + 64, W, 32, cudaMemcpyDeviceToHost, s));
+    BGPU_CUDA(cudaStreamSynchronize(s));
+    const hu128 y1 = h128(host), yinf = h128(host + 16);
+    const hu128 s0 = shift_sum ^ y1, s2 = yinf, s1 = y1 ^ s0 ^ s2;
+    hu128 iy0, iy1;
+    lo = h128(host + 32);
+    hi = h128(host + 48);
+    if (early) {
+      iy1 = lo ^ host_gf_mul(hi ^ lo, z[gn - 1]);
+      iy0 = inout_eval;
+    } else {
+      iy1 = lo;
+      const hu128 alpha = z[gn - 1];
+      iy0 = host_gf_mul(inout_eval ^ host_gf_mul(iy1, alpha), host_gf_inv(1 ^ alpha));
+    }
+    const hu128 q0 = iy0, q1 = iy1 ^ iy0;
+    const hu128 alpha_dec = n_rem <= p ? z[n_rem - 1] : 0;
+    const hu128 one_a = 1 ^ alpha_dec;
+    const hu128 d0 = host_gf_mul(host_gf_mul(q0, one_a), eq_prefix);
+    const hu128 d1 = host_gf_mul(host_gf_mul(q1, one_a) ^ q0, eq_prefix);
+    const hu128 b0 = s0 ^ host_gf_mul(beta, d0), b1 = s1 ^ host_gf_mul(beta, d1);
+    uint8_t rp[32];
+    memcpy(rp, &b0, 16);
+    memcpy(rp + 16, &b1, 16);
+    t.message(rp, 32);
+    t.sample_elem(rb);
+    const hu128 r = h128(rb);
+    ch2.push_back(r);
+    shift_sum = s0 ^ host_gf_mul(s1, r) ^ host_gf_mul(s2, host_gf_mul(r, r));
+    inout_eval = q0 ^ host_gf_mul(q1, r);
+    if (n_rem <= p) gn--;
+    eq_prefix = host_gf_mul(eq_prefix, 1 ^ r ^ alpha_dec);
+    if (n_rem == 1) {
+      const hu128 w0 = h128(host + 64), w1 = h128(host + 80);
+      res.witness_eval = w0 ^ host_gf_mul(r, w1 ^ w0);
+    }
+  }
+  t.message(&res.witness_eval, 16);
+  res.point = r_j;
+  res.point.insert(res.point.end(), ch2.rbegin(), ch2.rend());
+  return BINIUS_OK;
+}
+
+}  // namespace bgpu
+
+extern "C" {
+
+int binius_shift_reduction_prove(const binius_cs* cs, const void* d_witness,
+                                 binius_transcript* transcript, const void* h_and_data,
+                                 const void* h_mul_data, void* h_out_point, void* h_out_eval,
+                                 void* stream) {
+  BGPU_ARG(cs && d_witness && transcript && h_and_data && h_mul_data, "NULL argument");
+  const uint32_t log_and = log2_ceil(cs->and_ops.n_constraints);
+  const uint32_t log_mul = log2_ceil(cs->mul_ops.n_constraints);
+  auto parse = [](const uint8_t* b, uint32_t n_evals, uint32_t log_n, ShiftOperatorData& d) {
+    for (uint32_t i = 0; i < n_evals; i++) d.evals.push_back(h128(b + 16 * i));
+    d.r_zhat = h128(b + 16 * n_evals);
+    for (uint32_t i = 0; i < log_n; i++) d.r_x.push_back(h128(b + 16 * (n_evals + 1 + i)));
+  };
+  ShiftOperatorData band, bmul;
+  parse(static_cast<const uint8_t*>(h_and_data), 3, log_and, band);
+  parse(static_cast<const uint8_t*>(h_mul_data), 4, log_mul, bmul);
+  ShiftResult res;
+  int rc = shift_reduction_prove(cs, static_cast<const uint64_t*>(d_witness), transcript->t, band,
+                                 bmul, res, as_stream(stream));
+  if (rc) return rc;
+  if (h_out_point) memcpy(h_out_point, res.point.data(), 16 * res.point.size());
+  if (h_out_eval) memcpy(h_out_eval, &res.witness_eval, 16);
+  return clear_error();
+}
+
+}  // extern "C"

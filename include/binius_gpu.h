@@ -221,6 +221,23 @@ int binius_and_reduction_prove(const binius_cs* cs, const void* d_witness,
                                void* h_out_point, void* stream);
 
 /* ------------------------------------------------------------------------------------------
+ * Shift reduction.
+ * Replaces: shift::prove (prover/prover/src/protocols/shift/prove.rs:103-153) with
+ * build_key_collection (key_collection.rs:246-312), prove_phase_1 (phase_1.rs:43-139),
+ * build_h_parts / build_monster_multilinear (monster.rs:34-219) and prove_phase_2
+ * (phase_2.rs:56-160) over InOutCheckProver (protocols/inout_check.rs:19-211).
+ * h_and_data: AND OperatorData as 16-byte elements a_eval, b_eval, c_eval, r_zhat', then r_x'
+ * (log2(padded AND count) elements).  h_mul_data: a_eval, b_eval, lo_eval, hi_eval, r_zhat', then
+ * r_x' (log2(padded MUL count) elements).  The public segment is the first offset_witness words.
+ * h_out_point receives r_j ++ r_y (6 + log2(committed_total_len) elements), h_out_eval the witness
+ * evaluation there.  Samples from and writes to `transcript`.  Synchronous.
+ * ------------------------------------------------------------------------------------------ */
+int binius_shift_reduction_prove(const binius_cs* cs, const void* d_witness,
+                                 binius_transcript* transcript, const void* h_and_data,
+                                 const void* h_mul_data, void* h_out_point, void* h_out_eval,
+                                 void* stream);
+
+/* ------------------------------------------------------------------------------------------
  * FRI parameters (verifier/verifier/src/fri/common.rs:64-219).
  * ------------------------------------------------------------------------------------------ */
 uint32_t binius_fri_n_test_queries(uint32_t security_bits, uint32_t log_inv_rate);
