@@ -480,3 +480,43 @@ def oblong_eval(values, z, r_x) -> np.ndarray:
     out = elems(1)
     L.orc_oblong_eval(_p64(v), log_n, _p64(zz), _p64(rx), _p64(out))
     return out[0]
+
+
+# ---- integer multiplication reduction ----
+
+def _intmul_lib():
+    L = lib()
+    if not getattr(L, "_intmul_ready", False):
+        L.orc_intmul_prove.argtypes = [_u64p, _u64p, _u64p, _u64p, ctypes.c_uint32, _u8p,
+                                       ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), _u64p,
+                                       _u64p]
+        L.orc_intmul_verify.argtypes = [ctypes.c_uint32, _u8p, ctypes.c_size_t, _u64p, _u64p]
+        L._intmul_ready = True
+    return L
+
+
+def intmul_prove(a, b, lo, hi):
+    """IntMul reduction on a fresh transcript; returns (proof, eval_point, evals (4, 64, 2)) with
+    evals the bit-column evaluations of a, b, lo, hi."""
+    L = _intmul_lib()
+    cols = [np.ascontiguousarray(x, dtype=np.uint64) for x in (a, b, lo, hi)]
+    log_n = cols[0].shape[0].bit_length() - 1
+    cap = 1 << 22
+    out = np.zeros(cap, dtype=np.uint8)
+    n = ctypes.c_size_t(0)
+    point = elems(max(log_n, 1))
+    evals = elems(256)
+    rc = L.orc_intmul_prove(*[_p64(c) for c in cols], log_n, _p8(out), cap, ctypes.byref(n),
+                            _p64(point), _p64(evals))
+    assert rc == 0
+    return out[: n.value].tobytes(), point[:log_n], evals.reshape(4, 64, 2)
+
+
+def intmul_verify(log_n: int, proof: bytes):
+    """Restated IntMul verifier; returns (rc, eval_point, evals) with rc 0 = accepted."""
+    L = _intmul_lib()
+    pr = np.frombuffer(proof, dtype=np.uint8).copy()
+    point = elems(max(log_n, 1))
+    evals = elems(256)
+    rc = L.orc_intmul_verify(log_n, _p8(pr), len(proof), _p64(point), _p64(evals))
+    return rc, point[:log_n], evals.reshape(4, 64, 2)

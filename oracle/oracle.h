@@ -129,6 +129,14 @@ int orc_shift_verify(const uint64_t* public_words, uint32_t log_words, uint32_t 
 void orc_oblong_eval(const uint64_t* v, uint32_t log_n, const uint64_t* z, const uint64_t* r_x,
                      uint64_t* out);
 
+/* ---- Integer multiplication reduction (prover/prover/src/protocols/intmul/) ----
+ * out_point: log_n elements; out_evals: 4 x 64 elements (bit-column evaluations of a, b, lo, hi). */
+int orc_intmul_prove(const uint64_t* a, const uint64_t* b, const uint64_t* lo, const uint64_t* hi,
+                     uint32_t log_n, uint8_t* proof, size_t cap, size_t* len,
+                     uint64_t* out_point, uint64_t* out_evals);
+int orc_intmul_verify(uint32_t log_n, const uint8_t* proof, size_t len, uint64_t* out_point,
+                      uint64_t* out_evals);
+
 /* Number of worker threads the oracle may use (1 = scalar). */
 void orc_set_threads(int n);
 
