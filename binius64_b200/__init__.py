@@ -520,3 +520,19 @@ def shift_reduction_prove(cs: DeviceConstraintSystem, witness_words, transcript:
     pb = bytes(point)
     return ([int.from_bytes(pb[16 * i:16 * i + 16], "little") for i in range(n_point)],
             int.from_bytes(bytes(ev), "little"))
+
+
+def intmul_reduction_prove(cs: DeviceConstraintSystem, witness_words, transcript: ProverTranscript,
+                           stream=None):
+    """prove_intmul_reduction: returns (eval_point, [a, b, c_lo, c_hi] bit-column evaluations)
+    as ints (64 per column)."""
+    log_n = cs.n_mul.bit_length() - 1
+    point = (ctypes.c_uint8 * max(16, 16 * log_n))()
+    evals = (ctypes.c_uint8 * (16 * 256))()
+    check(lib().binius_intmul_reduction_prove(cs.handle, witness_words.data_ptr(),
+                                              transcript.handle, ctypes.addressof(point),
+                                              ctypes.addressof(evals), _stream(stream)))
+    pb, eb = bytes(point), bytes(evals)
+    p = [int.from_bytes(pb[16 * i:16 * i + 16], "little") for i in range(log_n)]
+    e = [int.from_bytes(eb[16 * i:16 * i + 16], "little") for i in range(256)]
+    return p, [e[64 * k:64 * (k + 1)] for k in range(4)]

@@ -80,6 +80,7 @@ _SIGS = {
     "binius_eval_operands": (_int, [_vp, _vp, _int, _vp, _vp]),
     "binius_and_reduction_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "binius_shift_reduction_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "binius_intmul_reduction_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "binius_fri_n_test_queries": (_u32, [_u32, _u32]),
     "binius_fri_estimate_optimal_arity": (_u32, [_u32, _u32, _u32]),
     "binius_gf_mul_batch": (_int, [_vp, _vp, _vp, _u64, _vp]),

@@ -23,6 +23,16 @@ struct AndResult {
 int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcript& t,
                         AndResult& res, cudaStream_t s);
 
+// IntMulOutput (verifier/verifier/src/protocols/intmul/common.rs:6-13): bit-column evaluations
+// of a, b, c_lo and c_hi at eval_point.
+struct IntMulResult {
+  std::vector<hu128> eval_point;
+  std::vector<hu128> a_evals, b_evals, c_lo_evals, c_hi_evals;
+};
+
+int intmul_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcript& t,
+                           IntMulResult& res, cudaStream_t s);
+
 // OperatorData (prover/prover/src/protocols/shift/prove.rs:20-33): operand evaluations at the
 // oblong point (r_zhat', r_x').  AND: (a, b, c); MUL: (a, b, lo, hi).
 struct ShiftOperatorData {

@@ -221,6 +221,19 @@ int binius_and_reduction_prove(const binius_cs* cs, const void* d_witness,
                                void* h_out_point, void* stream);
 
 /* ------------------------------------------------------------------------------------------
+ * Integer multiplication reduction.
+ * Replaces: build_intmul_witness + prove_intmul_reduction (prover/prover/src/prove.rs:374-391,
+ * 432-470), intmul Witness (protocols/intmul/witness.rs:47-270) and IntMulProver::prove
+ * (protocols/intmul/prove.rs:93-509).
+ * Samples from and writes to `transcript`.  h_out_point receives the output point
+ * (log2(padded MUL count) x 16 bytes), h_out_evals the 64 bit-column evaluations of a, b, c_lo and
+ * c_hi in that order (4 x 64 x 16 bytes).  Synchronous.
+ * ------------------------------------------------------------------------------------------ */
+int binius_intmul_reduction_prove(const binius_cs* cs, const void* d_witness,
+                                  binius_transcript* transcript, void* h_out_point,
+                                  void* h_out_evals, void* stream);
+
+/* ------------------------------------------------------------------------------------------
  * Shift reduction.
  * Replaces: shift::prove (prover/prover/src/protocols/shift/prove.rs:103-153) with
  * build_key_collection (key_collection.rs:246-312), prove_phase_1 (phase_1.rs:43-139),
