@@ -520,3 +520,58 @@ def intmul_verify(log_n: int, proof: bytes):
     evals = elems(256)
     rc = L.orc_intmul_verify(log_n, _p8(pr), len(proof), _p64(point), _p64(evals))
     return rc, point[:log_n], evals.reshape(4, 64, 2)
+
+
+# ---- whole prove / verify ----
+
+def _prove_lib():
+    L = lib()
+    if not getattr(L, "_prove_ready", False):
+        csr = [_u32pp, _u8p, ctypes.c_uint32]
+        L.orc_prove_params.argtypes = [ctypes.c_uint32, ctypes.c_uint32,
+                                       ctypes.POINTER(ctypes.c_uint32),
+                                       ctypes.POINTER(ctypes.c_uint32)]
+        L.orc_prove.argtypes = ([_u64p, ctypes.c_uint32, ctypes.c_uint32] + csr + csr +
+                                [ctypes.c_uint32, _u8p, ctypes.c_size_t,
+                                 ctypes.POINTER(ctypes.c_size_t)])
+        L.orc_verify.argtypes = ([_u64p, ctypes.c_uint32, ctypes.c_uint32] + csr + csr +
+                                 [ctypes.c_uint32, _u8p, ctypes.c_size_t])
+        L._prove_ready = True
+    return L
+
+
+def prove_params(log_words: int, log_inv_rate: int = 1):
+    """(log_witness_elems, log_batch, n_queries, arities) chosen by Verifier::setup."""
+    L = _prove_lib()
+    o4 = (ctypes.c_uint32 * 4)()
+    ar = (ctypes.c_uint32 * 8)()
+    L.orc_prove_params(log_words, log_inv_rate, o4, ar)
+    return o4[0], o4[1], o4[2], list(ar)[: o4[3]]
+
+
+def prove(words, log_public: int, and_csr, mul_csr, log_inv_rate: int = 1) -> bytes:
+    """Prover::prove on a fresh transcript over the prepared (padded) CSR constraint system."""
+    L = _prove_lib()
+    w = np.ascontiguousarray(words, dtype=np.uint64)
+    log_words = w.shape[0].bit_length() - 1
+    ka, pa, va, na = _csr_args(and_csr)
+    km, pm, vm, nm = _csr_args(mul_csr)
+    cap = 1 << 24
+    out = np.zeros(cap, dtype=np.uint8)
+    n = ctypes.c_size_t(0)
+    rc = L.orc_prove(_p64(w), log_words, log_public, pa, va, na, pm, vm, nm, log_inv_rate,
+                     _p8(out), cap, ctypes.byref(n))
+    assert rc == 0
+    return out[: n.value].tobytes()
+
+
+def verify(public_words, log_words: int, log_public: int, and_csr, mul_csr, proof: bytes,
+           log_inv_rate: int = 1) -> int:
+    """Restated Verifier::verify; 0 = accepted."""
+    L = _prove_lib()
+    pub = np.ascontiguousarray(public_words, dtype=np.uint64)
+    ka, pa, va, na = _csr_args(and_csr)
+    km, pm, vm, nm = _csr_args(mul_csr)
+    pr = np.frombuffer(proof, dtype=np.uint8).copy()
+    return L.orc_verify(_p64(pub), log_words, log_public, pa, va, na, pm, vm, nm, log_inv_rate,
+                        _p8(pr), len(proof))

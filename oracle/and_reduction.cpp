@@ -24,6 +24,7 @@
 
 #include "oracle.h"
 #include "oracle_internal.h"
+#include "protocols.h"
 #include "transcript.h"
 
 namespace orc {
@@ -118,10 +119,6 @@ static void eq_aes(const uint8_t* r, uint32_t n, uint8_t* out) {
 
 // ---------------------------------------------------------------- AND reduction prover
 
-struct AndOutput {
-  u128 a_eval, b_eval, c_eval, z;
-  std::vector<u128> eval_point;
-};
 
 static const uint8_t kSmallChallenges[3] = {0x2, 0x4, 0x10};  // config.rs:33-37
 

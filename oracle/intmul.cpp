@@ -19,6 +19,7 @@
 
 #include "oracle.h"
 #include "oracle_internal.h"
+#include "protocols.h"
 #include "transcript.h"
 
 namespace orc {
@@ -295,10 +296,10 @@ std::unique_ptr<SumcheckProver> decorated(MleCheckProver* p) {
 }
 
 // BinaryTree layers, root first: layers[k] holds 2^k multilinears of n values.
-typedef std::vector<std::vector<Vec>> Tree;
+typedef std::vector<std::vector<Vec>> Layers;
 
-Tree build_layers(std::vector<Vec> leaves) {
-  Tree t;
+Layers build_layers(std::vector<Vec> leaves) {
+  Layers t;
   t.push_back(std::move(leaves));
   while (t.back().size() > 1) {
     const auto& cur = t.back();
@@ -314,7 +315,7 @@ Tree build_layers(std::vector<Vec> leaves) {
   return t;
 }
 
-Tree constant_base(u128 base, const uint64_t* e, size_t n) {
+Layers constant_base(u128 base, const uint64_t* e, size_t n) {
   std::vector<Vec> leaves;
   u128 b = base;
   for (int i = 0; i < 64; i++, b = gf_square(b)) {
@@ -325,7 +326,7 @@ Tree constant_base(u128 base, const uint64_t* e, size_t n) {
   return build_layers(std::move(leaves));
 }
 
-Tree variable_base(Vec bases, const uint64_t* e, size_t n) {
+Layers variable_base(Vec bases, const uint64_t* e, size_t n) {
   std::vector<Vec> leaves;
   for (int i = 0; i < 64; i++) {
     Vec l(n);
@@ -346,20 +347,16 @@ std::vector<Vec> concat_layers(std::initializer_list<const std::vector<Vec>*> ls
 
 }  // namespace
 
-struct IntMulResult {
-  Vec eval_point;
-  Vec a_evals, b_evals, c_lo_evals, c_hi_evals;
-};
 
 IntMulResult intmul_prove(const uint64_t* a, const uint64_t* b, const uint64_t* lo,
                           const uint64_t* hi, uint32_t n_vars, Transcript& t) {
   const size_t n = (size_t)1 << n_vars;
   const u128 g = kGen;
   const u128 g_hi = sq_n(g, 64);
-  Tree ta = constant_base(g, a, n);
-  Tree tlo = constant_base(g, lo, n);
-  Tree thi = constant_base(g_hi, hi, n);
-  Tree tb = variable_base(ta[0][0], b, n);
+  Layers ta = constant_base(g, a, n);
+  Layers tlo = constant_base(g, lo, n);
+  Layers thi = constant_base(g_hi, hi, n);
+  Layers tb = variable_base(ta[0][0], b, n);
   Vec c_root(n);
   for (size_t x = 0; x < n; x++) c_root[x] = gf_mul(tlo[0][0][x], thi[0][0][x]);
 

@@ -137,6 +137,20 @@ int orc_intmul_prove(const uint64_t* a, const uint64_t* b, const uint64_t* lo, c
 int orc_intmul_verify(uint32_t log_n, const uint8_t* proof, size_t len, uint64_t* out_point,
                       uint64_t* out_evals);
 
+/* ---- Prover::prove / Verifier::verify (prover/prover/src/prove.rs:124-303,
+ * verifier/verifier/src/verify.rs:61-282) over a CSR constraint system (as for the shift
+ * reduction) and 2^log_words witness words. */
+void orc_prove_params(uint32_t log_words, uint32_t log_inv_rate, uint32_t* out4,
+                      uint32_t* out_arities);
+int orc_prove(const uint64_t* words, uint32_t log_words, uint32_t log_public,
+              const uint32_t* const* and_csr, const uint8_t* and_var, uint32_t n_and,
+              const uint32_t* const* mul_csr, const uint8_t* mul_var, uint32_t n_mul,
+              uint32_t log_inv_rate, uint8_t* proof, size_t cap, size_t* len);
+int orc_verify(const uint64_t* public_words, uint32_t log_words, uint32_t log_public,
+               const uint32_t* const* and_csr, const uint8_t* and_var, uint32_t n_and,
+               const uint32_t* const* mul_csr, const uint8_t* mul_var, uint32_t n_mul,
+               uint32_t log_inv_rate, const uint8_t* proof, size_t len);
+
 /* Number of worker threads the oracle may use (1 = scalar). */
 void orc_set_threads(int n);
 

@@ -16,81 +16,10 @@
 
 #include "oracle.h"
 #include "oracle_internal.h"
+#include "protocols.h"
 #include "transcript.h"
 
 namespace orc {
-
-// ---------------------------------------------------------------- Merkle helpers
-
-struct Tree {
-  uint32_t log_leaves = 0;
-  std::vector<uint8_t> nodes;
-  const uint8_t* root() const { return nodes.data() + nodes.size() - 32; }
-  // BinaryMerkleTree::layer (binary_merkle_tree.rs:142-150)
-  const uint8_t* layer(uint32_t depth) const {
-    size_t total = nodes.size() / 32;
-    return nodes.data() + 32 * (total + 1 - ((size_t)1 << (depth + 1)));
-  }
-  // BinaryMerkleTree::branch (binary_merkle_tree.rs:152-169)
-  void branch(size_t index, uint32_t depth, std::vector<uint8_t>& out) const {
-    uint32_t L = log_leaves;
-    for (uint32_t j = 0; j < L - depth; j++) {
-      size_t node = ((((size_t)1 << j) - 1) << (L + 1 - j)) | ((index >> j) ^ 1);
-      out.insert(out.end(), nodes.data() + 32 * node, nodes.data() + 32 * node + 32);
-    }
-  }
-};
-
-static Tree build_tree(const u128* elems, uint32_t log_leaves, uint32_t log_batch) {
-  Tree t;
-  t.log_leaves = log_leaves;
-  t.nodes.resize(32 * (((size_t)2 << log_leaves) - 1));
-  merkle_commit(elems, log_leaves, log_batch, t.nodes.data());
-  return t;
-}
-
-static uint32_t ceil_log2(uint32_t n) {
-  uint32_t r = 0;
-  while (((uint64_t)1 << r) < n) r++;
-  return r;
-}
-
-static uint32_t log2_exact(size_t n) {
-  uint32_t r = 0;
-  while (((size_t)1 << r) < n) r++;
-  return r;
-}
-
-// ---------------------------------------------------------------- FRI parameters
-
-struct FriParams {
-  uint32_t log_msg;       // log2 of the interleaved message length (the multilinear's n_vars)
-  uint32_t log_batch;
-  uint32_t log_inv_rate;
-  std::vector<uint32_t> arities;
-  uint32_t n_queries;
-  uint32_t log_dim() const { return log_msg - log_batch; }
-  uint32_t rs_log_len() const { return log_dim() + log_inv_rate; }
-  uint32_t log_len() const { return rs_log_len() + log_batch; }
-  uint32_t n_final_challenges() const {
-    uint32_t s = 0;
-    for (auto a : arities) s += a;
-    return log_dim() - s;
-  }
-  // vcs_optimal_layers_depths_iter (verifier/verifier/src/fri/common.rs:154-168)
-  std::vector<uint32_t> optimal_depths() const {
-    std::vector<uint32_t> d;
-    uint32_t cap = ceil_log2(n_queries);
-    uint32_t log_n_cosets = log_len();
-    std::vector<uint32_t> steps{log_batch};
-    steps.insert(steps.end(), arities.begin(), arities.end());
-    for (auto a : steps) {
-      log_n_cosets -= a;
-      d.push_back(cap < log_n_cosets ? cap : log_n_cosets);
-    }
-    return d;
-  }
-};
 
 // ---------------------------------------------------------------- FRI fold prover
 

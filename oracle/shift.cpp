@@ -18,6 +18,7 @@
 
 #include "oracle.h"
 #include "oracle_internal.h"
+#include "protocols.h"
 #include "transcript.h"
 
 namespace orc {
@@ -84,24 +85,6 @@ void build_h_parts(u128 r_zhat, std::vector<u128>& h) {
   }
 }
 
-struct Ops {
-  uint32_t k;                 // operands per constraint
-  uint32_t n;                 // constraints (padded)
-  const uint32_t* off;        // n * k + 1
-  const uint32_t* vi;
-  const uint8_t* var;
-  const uint32_t* amt;
-  const uint32_t* slot_to_operand;  // CSR slot -> KeyCollection operand index
-};
-
-struct OpData {
-  std::vector<u128> evals;
-  u128 r_zhat;
-  std::vector<u128> r_x;
-  std::vector<u128> eq;       // eq(r_x)
-  std::vector<u128> lpow;     // lambda^(i+1)
-};
-
 u128 inner(const u128* a, const u128* b, size_t n) {
   u128 acc = 0;
   for (size_t i = 0; i < n; i++) acc ^= gf_mul(a[i], b[i]);
@@ -126,12 +109,8 @@ void fold_top(std::vector<u128>& a, size_t off, size_t len, u128 r, std::vector<
 
 }  // namespace
 
-struct ShiftResult {
-  std::vector<u128> challenges;  // r_j ++ r_y
-  u128 witness_eval;
-  u128 initial_sum;              // sum_v <g_v, h_v>
-  u128 claim;                    // sum over operators of lambda^(i+1) evals[i]
-};
+
+void l_tilde64(u128 z, u128 out[64]) { l_tilde(z, out); }
 
 ShiftResult shift_prove(const uint64_t* words, uint32_t log_words, uint32_t log_public,
                         const Ops& and_ops, const Ops& mul_ops, OpData& band, OpData& bmul,
