@@ -536,3 +536,37 @@ def intmul_reduction_prove(cs: DeviceConstraintSystem, witness_words, transcript
     p = [int.from_bytes(pb[16 * i:16 * i + 16], "little") for i in range(log_n)]
     e = [int.from_bytes(eb[16 * i:16 * i + 16], "little") for i in range(256)]
     return p, [e[64 * k:64 * (k + 1)] for k in range(4)]
+
+
+class Prover:
+    """Prover::setup + Prover::prove (prover/prover/src/prove.rs:95-303) over a device constraint
+    system, with the parameters Verifier::setup chooses (verifier/verifier/src/verify.rs:61-108)."""
+
+    def __init__(self, cs: DeviceConstraintSystem, log_inv_rate: int = 1):
+        self.cs = cs  # the native prover keeps a reference
+        self._h = ctypes.c_void_p()
+        check(lib().binius_prover_setup(cs.handle, log_inv_rate, ctypes.byref(self._h)))
+        info = (ctypes.c_uint32 * 12)()
+        check(lib().binius_prover_info(self._h, ctypes.addressof(info)))
+        v = list(info)
+        self.log_witness_elems, self.log_batch, self.log_inv_rate, self.n_queries = v[:4]
+        self.fold_arities = v[5:5 + v[4]]
+
+    def prove(self, witness_words, transcript: ProverTranscript | None = None,
+              stream=None) -> ProverTranscript:
+        """witness_words: device int64 tensor of committed_total_len words."""
+        if witness_words.numel() != self.cs.committed_total_len:
+            raise ArgumentError(1, "witness length != committed_total_len")
+        t = transcript if transcript is not None else ProverTranscript()
+        check(lib().binius_prover_prove(self._h, witness_words.data_ptr(), t.handle,
+                                        _stream(stream)))
+        return t
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().binius_prover_destroy(h)
+            except Exception:
+                pass
+            self._h = None

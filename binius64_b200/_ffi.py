@@ -81,6 +81,10 @@ _SIGS = {
     "binius_and_reduction_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "binius_shift_reduction_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "binius_intmul_reduction_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "binius_prover_setup": (_int, [_vp, _u32, _vp]),
+    "binius_prover_destroy": (_int, [_vp]),
+    "binius_prover_info": (_int, [_vp, _vp]),
+    "binius_prover_prove": (_int, [_vp, _vp, _vp, _vp]),
     "binius_fri_n_test_queries": (_u32, [_u32, _u32]),
     "binius_fri_estimate_optimal_arity": (_u32, [_u32, _u32, _u32]),
     "binius_gf_mul_batch": (_int, [_vp, _vp, _vp, _u64, _vp]),

@@ -1,0 +1,155 @@
+// The top-level prove entry on the device: Verifier::setup's parameter choice
+// (verifier/verifier/src/verify.rs:61-108), Prover::setup (prover/prover/src/prove.rs:95-121) and
+// Prover::prove (prove.rs:124-303).
+//
+// The witness stays on the device for the whole proof: its committed words are the packed
+// multilinear of the PCS (pack_witness reads word pairs as little-endian 128-bit elements, which
+// is their memory layout), the operand columns of the reductions are evaluated from it, and the
+// shift reduction and the PCS opening read it in place.  The NTT is the standard-basis domain of
+// dim log_code_len; the Reed-Solomon code of the FRI parameters uses its first
+// log_dim + log_inv_rate layers.
+#include <string.h>
+
+#include <vector>
+
+#include "cs.h"
+#include "internal.h"
+#include "kernels.h"
+#include "reductions.h"
+#include "transcript.h"
+
+using namespace bgpu;
+
+struct binius_prover {
+  const binius_cs* cs = nullptr;
+  binius_ntt* ntt = nullptr;
+  binius_pcs* pcs = nullptr;
+  uint32_t log_inv_rate = 0, log_witness_elems = 0, log_batch = 0, n_queries = 0;
+  std::vector<uint32_t> arities;
+};
+
+namespace {
+
+constexpr uint32_t kSecurityBits = 96;  // verifier/verifier/src/verify.rs:39
+constexpr uint32_t kDigestSize = 32;    // SHA-256
+constexpr uint32_t kFieldSize = 16;     // B128
+
+uint32_t log2_ceil(uint64_t n) {
+  uint32_t r = 0;
+  while ((1ull << r) < n) r++;
+  return r;
+}
+
+hu128 h128(const void* p) {
+  hu128 v;
+  memcpy(&v, p, 16);
+  return v;
+}
+
+// make_final_claim (prove.rs:230-243): sum_i evals[i] l_tilde[i].
+hu128 final_claim(const std::vector<hu128>& evals, const hu128* L) {
+  hu128 acc = 0;
+  for (int i = 0; i < 64; i++) acc ^= host_gf_mul(evals[i], L[i]);
+  return acc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int binius_prover_setup(const binius_cs* cs, uint32_t log_inv_rate, binius_prover** out) {
+  BGPU_ARG(cs && out, "NULL argument");
+  *out = nullptr;
+  BGPU_ARG(log_inv_rate >= 1 && log_inv_rate <= 4, "log_inv_rate must be in [1, 4]");
+  binius_prover* P = new binius_prover();
+  P->cs = cs;
+  P->log_inv_rate = log_inv_rate;
+  uint32_t log_words = log2_ceil(cs->committed_total_len);
+  if (log_words < 1) log_words = 1;
+  P->log_witness_elems = log_words - 1;
+  const uint32_t log_code_len = P->log_witness_elems + log_inv_rate;
+  // FRIParams::choose_with_constant_fold_arity (verifier/verifier/src/fri/common.rs:64-115)
+  const uint32_t arity = binius_fri_estimate_optimal_arity(log_code_len, kDigestSize, kFieldSize);
+  P->log_batch = P->log_witness_elems < arity ? P->log_witness_elems : arity;
+  P->n_queries = binius_fri_n_test_queries(kSecurityBits, log_inv_rate);
+  const uint32_t rs_log_len = P->log_witness_elems - P->log_batch + log_inv_rate;
+  uint32_t term = log2_ceil(P->n_queries);
+  if (term < log_inv_rate) term = log_inv_rate;
+  if (term > rs_log_len) term = rs_log_len;
+  P->arities.assign((rs_log_len - term) / arity, arity);
+  if ((rs_log_len - term) % arity) P->arities.push_back((rs_log_len - term) % arity);
+  int rc = binius_ntt_create(cs->device, nullptr, log_code_len, &P->ntt);
+  if (!rc)
+    rc = binius_pcs_create(P->ntt, P->log_witness_elems, P->log_batch, log_inv_rate,
+                           P->arities.data(), (uint32_t)P->arities.size(), P->n_queries, &P->pcs);
+  if (rc) {
+    binius_prover_destroy(P);
+    return rc;
+  }
+  *out = P;
+  return clear_error();
+}
+
+int binius_prover_destroy(binius_prover* P) {
+  if (!P) return BINIUS_OK;
+  binius_pcs_destroy(P->pcs);
+  binius_ntt_destroy(P->ntt);
+  delete P;
+  return BINIUS_OK;
+}
+
+int binius_prover_info(const binius_prover* P, uint32_t* h_out12) {
+  BGPU_ARG(P && h_out12, "NULL argument");
+  memset(h_out12, 0, 12 * sizeof(uint32_t));
+  h_out12[0] = P->log_witness_elems;
+  h_out12[1] = P->log_batch;
+  h_out12[2] = P->log_inv_rate;
+  h_out12[3] = P->n_queries;
+  h_out12[4] = (uint32_t)P->arities.size();
+  for (size_t i = 0; i < P->arities.size() && i < 7; i++) h_out12[5 + i] = P->arities[i];
+  return clear_error();
+}
+
+int binius_prover_prove(const binius_prover* P, const void* d_witness,
+                        binius_transcript* transcript, void* stream) {
+  BGPU_ARG(P && d_witness && transcript, "NULL argument");
+  const binius_cs* cs = P->cs;
+  cudaStream_t s = as_stream(stream);
+  const uint64_t* words = static_cast<const uint64_t*>(d_witness);
+  Transcript& t = transcript->t;
+
+  // [phase] Witness Commit
+  binius_pcs_committed* committed = nullptr;
+  uint8_t root[32];
+  int rc = binius_pcs_commit(P->pcs, d_witness, &committed, root, stream);
+  if (rc) return rc;
+  t.message(root, 32);
+  do {
+    // [phase] IntMul Reduction
+    IntMulResult im;
+    if ((rc = intmul_reduction_prove(cs, words, t, im, s))) break;
+    // [phase] BitAnd Reduction
+    AndResult ao;
+    if ((rc = and_reduction_prove(cs, words, t, ao, s))) break;
+    // OperatorData of both operations at the AND reduction's r_zhat'
+    ShiftOperatorData band, bmul;
+    band.evals = {ao.a_eval, ao.b_eval, ao.c_eval};
+    band.r_zhat = ao.z;
+    band.r_x = ao.eval_point;
+    hu128 L[64];
+    lagrange_phi(6, ao.z, L);
+    bmul.evals = {final_claim(im.a_evals, L), final_claim(im.b_evals, L),
+                  final_claim(im.c_lo_evals, L), final_claim(im.c_hi_evals, L)};
+    bmul.r_zhat = ao.z;
+    bmul.r_x = im.eval_point;
+    // [phase] Shift Reduction
+    ShiftResult sh;
+    if ((rc = shift_reduction_prove(cs, words, t, band, bmul, sh, s))) break;
+    // [phase] PCS Opening at r_j ++ r_y
+    rc = binius_pcs_prove(P->pcs, committed, d_witness, sh.point.data(), transcript, stream);
+  } while (0);
+  binius_pcs_committed_destroy(committed);
+  return rc ? rc : clear_error();
+}
+
+}  // extern "C"

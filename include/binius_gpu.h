@@ -221,6 +221,27 @@ int binius_and_reduction_prove(const binius_cs* cs, const void* d_witness,
                                void* h_out_point, void* stream);
 
 /* ------------------------------------------------------------------------------------------
+ * The prove entry.
+ * Replaces: Verifier::setup's parameter choice (verifier/verifier/src/verify.rs:61-108: 96-bit
+ * security, FRI arity from estimate_optimal_arity(log_code_len, 32, 16),
+ * FRIParams::choose_with_constant_fold_arity), Prover::setup (prover/prover/src/prove.rs:95-121)
+ * and Prover::prove (prove.rs:124-303): commit, IntMul, AND and shift reductions and the PCS
+ * opening on one transcript.
+ * binius_prover_setup keeps a reference to `cs`, which must outlive the prover.
+ * binius_prover_prove: d_witness holds the committed_total_len witness words (the ValueVec's
+ * combined witness) on the CS's device; the proof is appended to `transcript`.  Synchronous.
+ * binius_prover_info h_out12: log_witness_elems, log_batch, log_inv_rate, n_queries, n_arities,
+ * then up to 7 fold arities.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct binius_prover binius_prover;
+
+int binius_prover_setup(const binius_cs* cs, uint32_t log_inv_rate, binius_prover** out);
+int binius_prover_destroy(binius_prover* prover);
+int binius_prover_info(const binius_prover* prover, uint32_t* h_out12);
+int binius_prover_prove(const binius_prover* prover, const void* d_witness,
+                        binius_transcript* transcript, void* stream);
+
+/* ------------------------------------------------------------------------------------------
  * Integer multiplication reduction.
  * Replaces: build_intmul_witness + prove_intmul_reduction (prover/prover/src/prove.rs:374-391,
  * 432-470), intmul Witness (protocols/intmul/witness.rs:47-270) and IntMulProver::prove

@@ -1,0 +1,73 @@
+"""The GPU prove entry against the oracle's Prover::prove: byte-identical proofs, accepted by the
+restated Verifier::verify."""
+import numpy as np
+import pytest
+
+import oracle as orc
+from binius64_b200 import constraint_system as csm
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover - CPU containers
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import binius64_b200 as bg  # noqa: E402
+
+
+def _prove_both(log_words, n_and, n_mul, seed, log_public=1, log_inv_rate=1):
+    sc = csm.synthetic_circuit(log_words, n_and, n_mul, seed=seed, log_public=log_public)
+    prep = sc.cs.prepared()
+    orc.set_threads(8)
+    try:
+        ref = orc.prove(sc.witness, log_public, prep.and_csr, prep.mul_csr, log_inv_rate)
+    finally:
+        orc.set_threads(1)
+    dcs = bg.DeviceConstraintSystem(sc.cs.serialize())
+    prover = bg.Prover(dcs, log_inv_rate)
+    w = torch.from_numpy(sc.witness.view(np.int64)).cuda()
+    got = prover.prove(w).finalize()
+    return sc, prep, ref, got, prover
+
+
+def _assert_same(ref, got):
+    assert len(got) == len(ref)
+    if got != ref:
+        first = next(i for i in range(len(ref)) if got[i] != ref[i])
+        pytest.fail(f"proof bytes differ first at offset {first} of {len(ref)}")
+
+
+@pytest.mark.parametrize("log_words,n_and,n_mul,log_public,log_inv_rate", [
+    (4, 3, 1, 1, 1),
+    (8, 60, 1, 1, 1),
+    (10, 300, 5, 3, 1),
+    (12, 1500, 17, 2, 2),
+    (16, 60000, 1, 1, 1),
+    (17, 100000, 300, 4, 1),
+])
+def test_prove_matches_oracle(log_words, n_and, n_mul, log_public, log_inv_rate):
+    sc, prep, ref, got, prover = _prove_both(log_words, n_and, n_mul, log_words, log_public,
+                                             log_inv_rate)
+    _assert_same(ref, got)
+    assert orc.verify(sc.witness[: 1 << log_public], log_words, log_public, prep.and_csr,
+                      prep.mul_csr, got, log_inv_rate) == 0
+
+
+def test_prove_2_20_words():
+    """The 2^20-word shape: about 2^20 AND constraints, one MUL, FRI arities [4, 4]."""
+    sc, prep, ref, got, prover = _prove_both(20, (1 << 20) - (1 << 16), 1, 20)
+    assert (prover.log_witness_elems, prover.log_batch, prover.fold_arities) == (19, 4, [4, 4])
+    _assert_same(ref, got)
+    assert orc.verify(sc.witness[:2], 20, 1, prep.and_csr, prep.mul_csr, got) == 0
+
+
+def test_prover_is_reusable_and_deterministic():
+    sc = csm.synthetic_circuit(10, 200, 2, seed=7)
+    dcs = bg.DeviceConstraintSystem(sc.cs.serialize())
+    prover = bg.Prover(dcs)
+    w = torch.from_numpy(sc.witness.view(np.int64)).cuda()
+    a = prover.prove(w).finalize()
+    b = prover.prove(w).finalize()
+    assert a == b
+    with pytest.raises(bg.ArgumentError):
+        prover.prove(w[:-1])
