@@ -1,18 +1,23 @@
 #!/usr/bin/env python
-"""Benchmark of the kernel-level FRI commit pipeline on B200.
+"""Benchmark of the Binius64 prove entry on B200.
 
-Workload (one "step"): the FRI commit path of the Binius64 prover at kernel level on seeded
-uniform GF(2^128) input -- RS encode (additive NTT, R = 1) of 16 interleaved columns whose per-column
-codeword length is 2^20, the SHA-256 Merkle commit of the 2^24-element codeword (leaves of 16
-symbols), then 3 FRI folds, each followed by the Merkle commit of the folded codeword with coset
-leaves of 16 symbols: fold_interleaved (4 challenges) -> 2^20, fold_codeword (4) -> 2^16,
-fold_codeword (4) -> 2^12.  Mirrors fri::commit_interleaved + FRIFoldProver::execute_fold_round
-(prover/prover/src/fri/{commit,fold}.rs).
+Default workload (one "step" = one whole proof): Prover::prove of a synthetic constraint system
+with 2^20 committed witness words, 2^20 - 2^16 AND constraints (padded to 2^20) and one MUL
+constraint, log_inv_rate 1 -- the shape of the reference's sha512 64 KiB example (2^20 words,
+2^20 ANDs, 1 intmul), whose constraint system cannot be built here (it comes from the Rust
+frontend).  Operands are XORs of 1-3 shifted witness words over all eight shift variants, the
+witness is seeded random and satisfies every constraint.  Proof parameters come from
+Verifier::setup: 2^19 packed elements, 16 interleaved columns, fold arities [4, 4], 232 queries.
 
-value: device time per step (CUDA events, message resident in HBM).  e2e: the same step through the
-public API with the message copied from pinned host memory and the roots plus the final folded
-codeword copied back, inside the timed region.  Inputs (128 MiB message, 256 MiB codeword) exceed the
-126 MB L2, so no explicit flush is needed between steps.
+value: milliseconds per proof with the witness resident in HBM (CUDA events around each proof on
+the proving stream; a 256 MiB buffer is written between proofs to flush L2).  e2e: the same proof
+through the public API with the witness copied from pinned host memory inside the timed region;
+the proof bytes (assembled on the host) are the result.  roofline: the dominant kernel of the
+proof (the bivariate product sumcheck fold + round, shift phase 2 and BaseFold) timed live on
+2^20-element operands.
+
+--workload commit: the kernel-level FRI commit pipeline (RS encode of 16 interleaved columns of
+codeword length 2^20, SHA-256 Merkle commit, 3 FRI folds with commits) with the NTT pass roofline.
 
 --impl reference times the CPU restatement of the reference (oracle/, all host threads) on the
 same workload; the Rust reference cannot be built in this image (no cargo).
@@ -34,24 +39,46 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-LOG_LEN = 20          # per-column codeword length 2^20
+SEED = 20241203
 LOG_INV_RATE = 1
+
+# prove workload
+LOG_WORDS = 20
+
+# commit workload
+LOG_LEN = 20          # per-column codeword length 2^20
 LOG_BATCH = 4         # 16 interleaved columns
 FOLD_ARITY = 4
 N_FOLDS = 3
-SEED = 20241203
 
-METRIC = "FRI commit ms: RS encode + SHA-256 Merkle + 3 FRI folds with commits"
+PROVE_METRIC = "prove ms @2^20 words"
+COMMIT_METRIC = "FRI commit ms: RS encode + SHA-256 Merkle + 3 FRI folds with commits"
 
 
-def workload_config():
+def n_and_for(log_words):
+    return (1 << log_words) - (1 << (log_words - 4))
+
+
+def prove_config(log_words):
+    return {
+        "workload": f"Prover::prove, synthetic AND/MUL constraint system with 2^{log_words} "
+                    f"committed words, {n_and_for(log_words)} AND constraints (padded to "
+                    f"2^{log_words}), 1 MUL, log_inv_rate {LOG_INV_RATE}",
+        "log_words": log_words, "n_and": n_and_for(log_words), "n_mul": 1,
+        "log_inv_rate": LOG_INV_RATE, "security_bits": 96,
+        "stand_in_for": "sha512 example circuit, 64 KiB message (2^20 words, 2^20 ANDs, 1 MUL)",
+        "l2": "256 MiB buffer written between timed proofs (L2 flush)",
+        "seed": SEED,
+    }
+
+
+def commit_config():
     log_dim = LOG_LEN - LOG_INV_RATE
     return {
         "workload": f"kernel-level FRI commit, log_len={LOG_LEN} per column, R={LOG_INV_RATE}, "
                     f"{1 << LOG_BATCH} interleaved columns, {N_FOLDS} folds (arity {FOLD_ARITY})",
         "log_len": LOG_LEN, "log_inv_rate": LOG_INV_RATE, "batch_columns": 1 << LOG_BATCH,
         "message_elems": 1 << (log_dim + LOG_BATCH), "codeword_elems": 1 << (LOG_LEN + LOG_BATCH),
-        "field": "GF(2^128) GHASH", "hash": "SHA-256 leaves + Binius SHA-256 compression",
         "l2": "inputs larger than L2 (128 MiB message, 256 MiB codeword); no flush",
         "seed": SEED,
     }
@@ -63,14 +90,21 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="prove", choices=["prove", "commit"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--log-words", type=int, default=None,
+                    help="prove workload: log2 committed words (default 20)")
     ap.add_argument("--log-len", type=int, default=None,
-                    help="per-column codeword log length (default 20; smaller cases for profiling)")
+                    help="commit workload: per-column codeword log length (default 20)")
     args = ap.parse_args()
+    global LOG_WORDS, LOG_LEN
+    if args.log_words is not None:
+        assert 8 <= args.log_words <= 22
+        LOG_WORDS = args.log_words
     if args.log_len is not None:
-        global LOG_LEN
         assert 13 <= args.log_len <= 24
         LOG_LEN = args.log_len
+    args.warmup = max(3, args.warmup)
     return args
 
 
@@ -82,69 +116,10 @@ def dist_env():
 
 
 def fold_challenges(rng, n):
-    v = rng.integers(0, np.iinfo(np.uint64).max, size=(n, 2), dtype=np.uint64, endpoint=True)
-    return v
+    return rng.integers(0, np.iinfo(np.uint64).max, size=(n, 2), dtype=np.uint64, endpoint=True)
 
 
-def elem_ints(arr):
-    return [int(a[0]) | (int(a[1]) << 64) for a in arr]
-
-
-# ----------------------------------------------------------------------------- GPU pipeline
-
-class GpuPipeline:
-    """Preallocated buffers; one step = encode + commit + 3 x (fold + commit) via the C ABI."""
-
-    def __init__(self, torch, device):
-        import binius64_b200 as bg
-        from binius64_b200._ffi import check, lib
-        self.torch, self.bg, self.L, self.check = torch, bg, lib(), check
-        self.device = device
-        log_dim = LOG_LEN - LOG_INV_RATE
-        self.log_dim = log_dim
-        basis = bg.standard_domain_rs_basis(LOG_LEN + LOG_BATCH, LOG_BATCH, device=device)
-        self.ntt = bg.AdditiveNTT(LOG_LEN, basis=basis, device=device)
-        gen = torch.Generator(device=f"cuda:{device}").manual_seed(SEED)
-        d = f"cuda:{device}"
-        self.msg = torch.randint(-2**63, 2**63 - 1, (1 << (log_dim + LOG_BATCH), 2),
-                                 dtype=torch.int64, device=d, generator=gen)
-        self.codeword = torch.empty((1 << (LOG_LEN + LOG_BATCH), 2), dtype=torch.int64, device=d)
-        self.nodes = [torch.empty(((2 << LOG_LEN) - 1, 32), dtype=torch.uint8, device=d)]
-        self.folded = []
-        cur = LOG_LEN
-        for i in range(N_FOLDS):
-            out_len = cur if i == 0 else cur - FOLD_ARITY
-            self.folded.append(torch.empty((1 << out_len, 2), dtype=torch.int64, device=d))
-            leaves = out_len - FOLD_ARITY
-            self.nodes.append(torch.empty(((2 << leaves) - 1, 32), dtype=torch.uint8, device=d))
-            cur = out_len
-        rng = np.random.default_rng(SEED)
-        self.ch = [fold_challenges(rng, LOG_BATCH)] + [fold_challenges(rng, FOLD_ARITY)
-                                                        for _ in range(N_FOLDS - 1)]
-        self.ch_ptrs = [c.ctypes.data_as(ctypes.c_void_p) for c in self.ch]
-
-    def step(self, stream):
-        L, chk = self.L, self.check
-        s = stream.cuda_stream
-        chk(L.binius_fri_commit_interleaved(self.ntt.handle, self.msg.data_ptr(), self.log_dim,
-                                            LOG_INV_RATE, LOG_BATCH, self.codeword.data_ptr(),
-                                            self.nodes[0].data_ptr(), None, s))
-        chk(L.binius_fri_fold_interleaved(self.codeword.data_ptr(), LOG_LEN, LOG_BATCH,
-                                          self.ch_ptrs[0], self.folded[0].data_ptr(), s))
-        chk(L.binius_merkle_commit(self.folded[0].data_ptr(), LOG_LEN - FOLD_ARITY, FOLD_ARITY,
-                                   self.nodes[1].data_ptr(), s))
-        cur = LOG_LEN
-        for i in range(1, N_FOLDS):
-            chk(L.binius_fri_fold_codeword(self.ntt.handle, self.folded[i - 1].data_ptr(), cur,
-                                           self.ch_ptrs[i], FOLD_ARITY, self.folded[i].data_ptr(),
-                                           s))
-            cur -= FOLD_ARITY
-            chk(L.binius_merkle_commit(self.folded[i].data_ptr(), cur - FOLD_ARITY, FOLD_ARITY,
-                                       self.nodes[i + 1].data_ptr(), s))
-
-    def roots(self):
-        return [bytes(n[-1].cpu().numpy().tobytes()) for n in self.nodes]
-
+# ----------------------------------------------------------------------------- clocks / peaks
 
 def sample_clocks_start(device):
     try:
@@ -203,11 +178,10 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """dram bytes per ntt_pass_kernel launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "ntt_pass_kernel_log20_b4.md")
+def profiled_traffic(name):
+    """dram bytes per launch from a committed ncu summary under profiles/, if present."""
     try:
-        for line in open(path):
+        for line in open(os.path.join(ROOT, "profiles", name)):
             if line.startswith("traffic_bytes_per_launch:"):
                 return int(line.split(":")[1].strip())
     except (OSError, ValueError):
@@ -215,8 +189,243 @@ def profiled_traffic():
     return None
 
 
-def run_cpu_pipeline(threads):
-    """The same step on the CPU oracle (reference restatement); returns seconds."""
+def pct(xs, q):
+    xs = sorted(xs)
+    k = min(len(xs) - 1, max(0, int(round(q / 100.0 * (len(xs) - 1)))))
+    return xs[k]
+
+
+# ----------------------------------------------------------------------------- prove workload
+
+def make_circuit(log_words):
+    from binius64_b200 import constraint_system as csm
+    return csm.synthetic_circuit(log_words, n_and_for(log_words), 1, seed=SEED + log_words)
+
+
+def cpu_prove_ms(circ, threads, reps=1):
+    """Whole proofs on the oracle (C++ restatement of the reference); returns ms per proof."""
+    import oracle as orc
+    prep = circ.cs.prepared()
+    orc.set_threads(threads)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        orc.prove(circ.witness, 1, prep.and_csr, prep.mul_csr, LOG_INV_RATE)
+        times.append(time.perf_counter() - t0)
+    orc.set_threads(1)
+    return 1000.0 * statistics.mean(times)
+
+
+def bivariate_roofline(torch, bg, lib, device, stream, reps=20):
+    """Live timing of binius_sumcheck_bivariate_fold_execute on 2^20-element operands (the first
+    folded round of shift phase 2): algorithmic bytes = read a, b (2 x 16 MiB) + write the folded
+    halves (2 x 8 MiB)."""
+    log_len = 20
+    n = 1 << log_len
+    gen = torch.Generator(device=f"cuda:{device}").manual_seed(SEED)
+    a0 = torch.randint(-2**63, 2**63 - 1, (n, 2), dtype=torch.int64, device=f"cuda:{device}",
+                       generator=gen)
+    b0 = torch.randint(-2**63, 2**63 - 1, (n, 2), dtype=torch.int64, device=f"cuda:{device}",
+                       generator=gen)
+    a, b = a0.clone(), b0.clone()
+    out = torch.zeros((2, 2), dtype=torch.int64, device=f"cuda:{device}")
+    r = (ctypes.c_uint8 * 16)(*range(1, 17))
+    s = stream.cuda_stream
+    for _ in range(3):
+        a.copy_(a0)
+        b.copy_(b0)
+        lib.binius_sumcheck_bivariate_fold_execute(a.data_ptr(), b.data_ptr(), log_len, r,
+                                                   out.data_ptr(), s)
+    torch.cuda.synchronize()
+    tot = 0.0
+    for _ in range(reps):
+        a.copy_(a0)
+        b.copy_(b0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        lib.binius_sumcheck_bivariate_fold_execute(a.data_ptr(), b.data_ptr(), log_len, r,
+                                                   out.data_ptr(), s)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        tot += e0.elapsed_time(e1)
+    launch_ms = tot / reps
+    bytes_per_launch = 2 * 16 * n + 2 * 16 * (n // 2)
+    mults = n + n // 2  # n folds (both operands) + n/4 pairs x 2 products
+    return launch_ms, bytes_per_launch, mults
+
+
+def run_prove(args, rank, world, local):
+    import torch
+    import binius64_b200 as bg
+    from binius64_b200._ffi import lib
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    stream = torch.cuda.current_stream()
+    circ = make_circuit(LOG_WORDS)
+    dcs = bg.DeviceConstraintSystem(circ.cs.serialize(), device=local)
+    prover = bg.Prover(dcs, LOG_INV_RATE)
+    w = torch.from_numpy(circ.witness.view(np.int64)).to(f"cuda:{local}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    proof = None
+    for _ in range(args.warmup):
+        proof = prover.prove(w).finalize()
+    torch.cuda.synchronize()
+
+    # --- device-resident witness: CUDA events around each proof
+    launches0 = lib().binius_launch_count()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clk = sample_clocks_start(local)
+    per, phases = [], []
+    t_wall0 = time.perf_counter()
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        prover.prove(w)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        per.append(e0.elapsed_time(e1))
+        phases.append(prover.phase_ms())
+    wall = time.perf_counter() - t_wall0
+    clocks = sample_clocks_stop(clk)
+    launches = (lib().binius_launch_count() - launches0) / args.steps
+    total_ms = sum(per)
+    if pg:
+        pg.barrier()
+        t = torch.tensor([total_ms], device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms = total_ms / (args.steps * world)  # whole-job ms per proof (replicas)
+
+    # --- end to end: pinned host witness -> device, prove, proof bytes on the host
+    host_w = torch.from_numpy(circ.witness.view(np.int64)).pin_memory()
+    e2e = []
+    proof_len = 0
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        w.copy_(host_w, non_blocking=True)
+        pb = prover.prove(w).finalize()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e.append(e0.elapsed_time(e1))
+        proof_len = len(pb)
+        assert pb == proof, "proof changed between runs"
+    e2e_ms = statistics.mean(e2e)
+
+    line = None
+    if rank == 0:
+        launch_ms, bpl, mults = bivariate_roofline(torch, bg, lib(), local, stream)
+        achieved = bpl / (launch_ms * 1e-3) / 1e9
+        peak, peak_kind = measured_peak_hbm()
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            cpu_ms = cpu_prove_ms(circ, threads, reps=2)
+            cpu = {"value": cpu_ms, "unit": "ms", "cores": threads, "kind": "port",
+                   "sample": f"2 whole proofs of the same 2^{LOG_WORDS}-word circuit on the "
+                             "oracle (C++ restatement of the reference prover, PCLMULQDQ, "
+                             "std::thread over all host cores); the Rust reference needs cargo"}
+        ph = {k: statistics.median(p[k] for p in phases) for k in phases[0]}
+        line = {
+            "metric": PROVE_METRIC, "value": ms, "unit": "ms", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "GF(2^128) GHASH / u64 words", "data": "synthetic (seeded witness and "
+            "constraint system of the reference's 2^20-word shape)",
+            "config": prove_config(LOG_WORDS),
+            "latency_ms": {"p50": pct(per, 50), "p99": pct(per, 99), "min": min(per),
+                           "max": max(per), "wall_per_proof": 1000.0 * wall / args.steps},
+            "phase_ms_host": ph,
+            "proof_bytes": proof_len,
+            "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(host_w.numel() * 8),
+                    "d2h_bytes_per_step": proof_len},
+            "gpu_launches": int(round(launches)),
+            "roofline": {"bound": "hbm", "kernel": "bivariate_fold_eval_kernel",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": profiled_traffic("bivariate_fold_eval_kernel_log20.md"),
+                         "launch_ms": launch_ms, "algorithmic_bytes_per_launch": bpl,
+                         "gf_mults_per_launch": mults,
+                         "gf_mults_per_s": mults / (launch_ms * 1e-3),
+                         "note": "GF(2^128) multiply-bound (integer pipes); HBM fraction "
+                                 "reported against the measured copy bandwidth"},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if line:
+        print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- commit workload
+
+class GpuPipeline:
+    """Preallocated buffers; one step = encode + commit + 3 x (fold + commit) via the C ABI."""
+
+    def __init__(self, torch, device):
+        import binius64_b200 as bg
+        from binius64_b200._ffi import check, lib
+        self.torch, self.bg, self.L, self.check = torch, bg, lib(), check
+        self.device = device
+        log_dim = LOG_LEN - LOG_INV_RATE
+        self.log_dim = log_dim
+        basis = bg.standard_domain_rs_basis(LOG_LEN + LOG_BATCH, LOG_BATCH, device=device)
+        self.ntt = bg.AdditiveNTT(LOG_LEN, basis=basis, device=device)
+        gen = torch.Generator(device=f"cuda:{device}").manual_seed(SEED)
+        d = f"cuda:{device}"
+        self.msg = torch.randint(-2**63, 2**63 - 1, (1 << (log_dim + LOG_BATCH), 2),
+                                 dtype=torch.int64, device=d, generator=gen)
+        self.codeword = torch.empty((1 << (LOG_LEN + LOG_BATCH), 2), dtype=torch.int64, device=d)
+        self.nodes = [torch.empty(((2 << LOG_LEN) - 1, 32), dtype=torch.uint8, device=d)]
+        self.folded = []
+        cur = LOG_LEN
+        for i in range(N_FOLDS):
+            out_len = cur if i == 0 else cur - FOLD_ARITY
+            self.folded.append(torch.empty((1 << out_len, 2), dtype=torch.int64, device=d))
+            leaves = out_len - FOLD_ARITY
+            self.nodes.append(torch.empty(((2 << leaves) - 1, 32), dtype=torch.uint8, device=d))
+            cur = out_len
+        rng = np.random.default_rng(SEED)
+        self.ch = [fold_challenges(rng, LOG_BATCH)] + [fold_challenges(rng, FOLD_ARITY)
+                                                        for _ in range(N_FOLDS - 1)]
+        self.ch_ptrs = [c.ctypes.data_as(ctypes.c_void_p) for c in self.ch]
+
+    def step(self, stream):
+        L, chk = self.L, self.check
+        s = stream.cuda_stream
+        chk(L.binius_fri_commit_interleaved(self.ntt.handle, self.msg.data_ptr(), self.log_dim,
+                                            LOG_INV_RATE, LOG_BATCH, self.codeword.data_ptr(),
+                                            self.nodes[0].data_ptr(), None, s))
+        chk(L.binius_fri_fold_interleaved(self.codeword.data_ptr(), LOG_LEN, LOG_BATCH,
+                                          self.ch_ptrs[0], self.folded[0].data_ptr(), s))
+        chk(L.binius_merkle_commit(self.folded[0].data_ptr(), LOG_LEN - FOLD_ARITY, FOLD_ARITY,
+                                   self.nodes[1].data_ptr(), s))
+        cur = LOG_LEN
+        for i in range(1, N_FOLDS):
+            chk(L.binius_fri_fold_codeword(self.ntt.handle, self.folded[i - 1].data_ptr(), cur,
+                                           self.ch_ptrs[i], FOLD_ARITY, self.folded[i].data_ptr(),
+                                           s))
+            cur -= FOLD_ARITY
+            chk(L.binius_merkle_commit(self.folded[i].data_ptr(), cur - FOLD_ARITY, FOLD_ARITY,
+                                       self.nodes[i + 1].data_ptr(), s))
+
+
+def run_cpu_commit(threads):
+    """The commit step on the CPU oracle (reference restatement); returns seconds."""
     import oracle as orc
     orc.set_threads(threads)
     log_dim = LOG_LEN - LOG_INV_RATE
@@ -235,41 +444,12 @@ def run_cpu_pipeline(threads):
         f = orc.fri_fold_codeword(tw, LOG_LEN, f, cur, ch[i])
         cur -= FOLD_ARITY
         orc.merkle_commit(f, cur - FOLD_ARITY, FOLD_ARITY)
+    orc.set_threads(1)
     return time.perf_counter() - t0
 
 
-def reference_arm(args, rank):
-    if rank != 0:
-        return
-    threads = os.cpu_count() or 1
-    times = []
-    for i in range(args.warmup + args.steps):
-        t = run_cpu_pipeline(threads)
-        if i >= args.warmup:
-            times.append(t)
-    ms = 1000.0 * statistics.mean(times)
-    line = {
-        "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "GF(2^128) (u128)", "data": "synthetic",
-        "config": workload_config(),
-        "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "port",
-                         "sample": "the full step, every step (oracle/ C++ restatement of the "
-                                   "reference; the Rust reference needs cargo, absent here)"},
-        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
-
-
-def main():
-    args = parse_args()
-    rank, world, local = dist_env()
-    if args.impl == "reference":
-        reference_arm(args, rank)
-        return
-
+def run_commit(args, rank, world, local):
     import torch
-    import binius64_b200 as bg
     from binius64_b200._ffi import lib
 
     torch.cuda.set_device(local)
@@ -281,12 +461,9 @@ def main():
         pg = dist
     stream = torch.cuda.current_stream()
     pipe = GpuPipeline(torch, local)
-
-    for _ in range(max(3, args.warmup)):
+    for _ in range(args.warmup):
         pipe.step(stream)
     torch.cuda.synchronize()
-
-    # --- device-timed region
     launches0 = lib().binius_launch_count()
     if pg:
         pg.barrier()
@@ -299,16 +476,15 @@ def main():
     ev1.record(stream)
     torch.cuda.synchronize()
     clocks = sample_clocks_stop(clk)
-    if pg:
-        pg.barrier()
-    launches = lib().binius_launch_count() - launches0
+    launches = (lib().binius_launch_count() - launches0) / args.steps
     ms = ev0.elapsed_time(ev1) / args.steps
     if pg:
+        pg.barrier()
         t = torch.tensor([ms], device=f"cuda:{local}")
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = float(t.item()) / world
 
-    # --- dominant kernel: the NTT pass (3 launches of ntt_pass_kernel over the codeword)
+    # dominant kernel: the NTT pass (ntt_pass_kernel launches over the codeword)
     reps = max(3, args.steps)
     for _ in range(2):
         pipe.ntt.forward_transform(pipe.codeword, LOG_INV_RATE, LOG_BATCH)
@@ -322,12 +498,11 @@ def main():
     n_layers = LOG_LEN - LOG_INV_RATE
     n_passes = (n_layers + 7) // 8
     launch_ms = e0.elapsed_time(e1) / (reps * n_passes)
-    bytes_per_launch = 32 * (1 << (LOG_LEN + LOG_BATCH))  # read + write of every element
+    bytes_per_launch = 32 * (1 << (LOG_LEN + LOG_BATCH))
     achieved = bytes_per_launch / (launch_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak_hbm()
     mults_per_launch = (n_layers / n_passes) * (1 << (LOG_LEN + LOG_BATCH - 1))
 
-    # --- end to end: pinned host message in, roots + final folded codeword out
     host_msg = torch.empty_like(pipe.msg, device="cpu").pin_memory()
     host_msg.copy_(pipe.msg.cpu())
     host_out = torch.empty_like(pipe.folded[-1], device="cpu").pin_memory()
@@ -349,23 +524,22 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        cpu_s = run_cpu_pipeline(threads)
-        cpu = {"value": cpu_s * 1000.0, "unit": "ms", "cores": threads, "kind": "port",
-               "sample": "one full step of the same workload on the oracle (C++ restatement of "
-                         "the reference, PCLMULQDQ, std::thread over all host cores)"}
-
+        cpu = {"value": run_cpu_commit(threads) * 1000.0, "unit": "ms", "cores": threads,
+               "kind": "port", "sample": "one full step of the same workload on the oracle"}
     if rank == 0:
         line = {
-            "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
-            "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "GF(2^128) (u128)",
-            "data": "synthetic (seeded uniform field elements)", "config": workload_config(),
+            "metric": COMMIT_METRIC, "value": ms, "unit": "ms", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "GF(2^128) GHASH", "data": "synthetic (seeded uniform field elements)",
+            "config": commit_config(),
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "gpu_launches": int(launches),
+            "gpu_launches": int(round(launches)),
             "roofline": {"bound": "hbm", "kernel": "ntt_pass_kernel", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": peak_kind, "traffic": profiled_traffic(),
+                         "peak_kind": peak_kind,
+                         "traffic": profiled_traffic("ntt_pass_kernel_log20_b4.md"),
                          "launch_ms": launch_ms, "algorithmic_bytes_per_launch": bytes_per_launch,
                          "gf_mults_per_launch": mults_per_launch,
                          "gf_mults_per_s": mults_per_launch / (launch_ms * 1e-3)},
@@ -376,6 +550,57 @@ def main():
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+# ----------------------------------------------------------------------------- reference arm
+
+def reference_arm(args, rank):
+    """The reference's CPU path on the same workload: the oracle (C++ restatement, all host
+    threads); rank 0 only."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    if args.workload == "prove":
+        circ = make_circuit(LOG_WORDS)
+        times = []
+        for i in range(args.warmup + args.steps):
+            t = cpu_prove_ms(circ, threads)
+            if i >= args.warmup:
+                times.append(t)
+        metric, config = PROVE_METRIC, prove_config(LOG_WORDS)
+        sample = f"each step one whole proof of the 2^{LOG_WORDS}-word circuit"
+    else:
+        times = []
+        for i in range(args.warmup + args.steps):
+            t = 1000.0 * run_cpu_commit(threads)
+            if i >= args.warmup:
+                times.append(t)
+        metric, config = COMMIT_METRIC, commit_config()
+        sample = "each step the full commit workload"
+    ms = statistics.mean(times)
+    line = {
+        "impl": "reference", "metric": metric, "value": ms, "unit": "ms", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "GF(2^128) GHASH / u64 words",
+        "data": "synthetic", "config": config,
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "port",
+                         "sample": sample + " on the oracle (C++ restatement of the reference; "
+                                   "the Rust reference needs cargo, absent here)"},
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+    if args.workload == "prove":
+        run_prove(args, rank, world, local)
+    else:
+        run_commit(args, rank, world, local)
 
 
 if __name__ == "__main__":

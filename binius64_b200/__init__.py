@@ -562,6 +562,12 @@ class Prover:
                                         _stream(stream)))
         return t
 
+    def phase_ms(self) -> dict:
+        """Host wall-clock milliseconds of the last prove's phases."""
+        out = (ctypes.c_double * 5)()
+        check(lib().binius_prover_phase_ms(self._h, out))
+        return dict(zip(("commit", "intmul", "bitand", "shift", "pcs"), list(out)))
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:

@@ -85,9 +85,12 @@ _SIGS = {
     "binius_prover_destroy": (_int, [_vp]),
     "binius_prover_info": (_int, [_vp, _vp]),
     "binius_prover_prove": (_int, [_vp, _vp, _vp, _vp]),
+    "binius_prover_phase_ms": (_int, [_vp, _vp]),
     "binius_fri_n_test_queries": (_u32, [_u32, _u32]),
     "binius_fri_estimate_optimal_arity": (_u32, [_u32, _u32, _u32]),
     "binius_gf_mul_batch": (_int, [_vp, _vp, _vp, _u64, _vp]),
+    "binius_sumcheck_bivariate_execute": (_int, [_vp, _vp, _u32, _vp, _vp]),
+    "binius_sumcheck_bivariate_fold_execute": (_int, [_vp, _vp, _u32, _vp, _vp, _vp]),
 }
 
 _lib = None

@@ -2,6 +2,8 @@
 #include <stdio.h>
 
 #include <atomic>
+#include <mutex>
+#include <vector>
 
 #if defined(__PCLMUL__) && defined(__SSE4_1__)
 #include <immintrin.h>
@@ -79,6 +81,24 @@ hu128 host_gf_inv(hu128 a) {
   hu128 r = a;
   for (int k = 2; k <= 127; k++) r = host_gf_mul(host_gf_mul(r, r), a);
   return host_gf_mul(r, r);
+}
+
+// The stream-ordered allocator of `device` keeps freed blocks cached (release threshold = max)
+// instead of returning them to the driver at every synchronisation: a proof synchronises once per
+// sumcheck round and reallocates its scratch per phase.  The attribute belongs to this process's
+// default pool; it changes no setting of the GPU.
+int configure_device_pool(int device) {
+  static std::mutex mu;
+  static std::vector<int> done;
+  std::lock_guard<std::mutex> lock(mu);
+  for (int d : done)
+    if (d == device) return BINIUS_OK;
+  cudaMemPool_t pool;
+  BGPU_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+  uint64_t threshold = ~0ull;
+  BGPU_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+  done.push_back(device);
+  return BINIUS_OK;
 }
 
 }  // namespace bgpu

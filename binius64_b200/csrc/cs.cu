@@ -209,6 +209,7 @@ int binius_cs_from_bytes(int device, const void* h_bytes, size_t len, binius_cs*
   Reader r{static_cast<const uint8_t*>(h_bytes), len};
   uint32_t version = r.u32();
   BGPU_ARG(r.ok && version == 2, "ConstraintSystem::version must be 2");
+  if (int rc = configure_device_pool(device)) return rc;
   binius_cs* cs = new binius_cs();
   cs->device = device;
   uint32_t* fields[8] = {&cs->n_const,      &cs->n_inout,         &cs->n_witness,

@@ -31,6 +31,9 @@ int cuda_error(cudaError_t e, const char* what);
     if (!(cond)) return ::bgpu::set_error(BINIUS_E_ARG, msg); \
   } while (0)
 
+// Keeps the default memory pool of `device` from releasing cached blocks (see common.cu).
+int configure_device_pool(int device);
+
 // Cumulative number of kernels this library has launched (all devices, all threads).
 void count_launch(uint64_t n = 1);
 

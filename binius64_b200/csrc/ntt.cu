@@ -229,6 +229,7 @@ int binius_ntt_create(int device, const void* h_basis, uint32_t log_domain, bini
   BGPU_ARG(out != nullptr, "out is NULL");
   *out = nullptr;
   BGPU_ARG(log_domain >= 1 && log_domain <= 32, "log_domain must be in [1, 32]");
+  if (int rc = configure_device_pool(device)) return rc;
   const uint32_t l = log_domain;
   std::vector<hu128> basis(l);
   for (uint32_t i = 0; i < l; i++) {

@@ -10,6 +10,7 @@
 // log_dim + log_inv_rate layers.
 #include <string.h>
 
+#include <chrono>
 #include <vector>
 
 #include "cs.h"
@@ -26,6 +27,8 @@ struct binius_prover {
   binius_pcs* pcs = nullptr;
   uint32_t log_inv_rate = 0, log_witness_elems = 0, log_batch = 0, n_queries = 0;
   std::vector<uint32_t> arities;
+  // host wall-clock milliseconds of the last prove's phases: commit, IntMul, AND, shift, PCS
+  mutable double phase_ms[5] = {0, 0, 0, 0, 0};
 };
 
 namespace {
@@ -110,6 +113,12 @@ int binius_prover_info(const binius_prover* P, uint32_t* h_out12) {
   return clear_error();
 }
 
+int binius_prover_phase_ms(const binius_prover* P, double* h_out5) {
+  BGPU_ARG(P && h_out5, "NULL argument");
+  memcpy(h_out5, P->phase_ms, sizeof(P->phase_ms));
+  return clear_error();
+}
+
 int binius_prover_prove(const binius_prover* P, const void* d_witness,
                         binius_transcript* transcript, void* stream) {
   BGPU_ARG(P && d_witness && transcript, "NULL argument");
@@ -118,19 +127,29 @@ int binius_prover_prove(const binius_prover* P, const void* d_witness,
   const uint64_t* words = static_cast<const uint64_t*>(d_witness);
   Transcript& t = transcript->t;
 
+  typedef std::chrono::steady_clock Clock;
+  auto t0 = Clock::now();
+  auto lap = [&](int phase) {
+    const auto now = Clock::now();
+    P->phase_ms[phase] = std::chrono::duration<double, std::milli>(now - t0).count();
+    t0 = now;
+  };
   // [phase] Witness Commit
   binius_pcs_committed* committed = nullptr;
   uint8_t root[32];
   int rc = binius_pcs_commit(P->pcs, d_witness, &committed, root, stream);
   if (rc) return rc;
   t.message(root, 32);
+  lap(0);
   do {
     // [phase] IntMul Reduction
     IntMulResult im;
     if ((rc = intmul_reduction_prove(cs, words, t, im, s))) break;
+    lap(1);
     // [phase] BitAnd Reduction
     AndResult ao;
     if ((rc = and_reduction_prove(cs, words, t, ao, s))) break;
+    lap(2);
     // OperatorData of both operations at the AND reduction's r_zhat'
     ShiftOperatorData band, bmul;
     band.evals = {ao.a_eval, ao.b_eval, ao.c_eval};
@@ -145,8 +164,10 @@ int binius_prover_prove(const binius_prover* P, const void* d_witness,
     // [phase] Shift Reduction
     ShiftResult sh;
     if ((rc = shift_reduction_prove(cs, words, t, band, bmul, sh, s))) break;
+    lap(3);
     // [phase] PCS Opening at r_j ++ r_y
     rc = binius_pcs_prove(P->pcs, committed, d_witness, sh.point.data(), transcript, stream);
+    lap(4);
   } while (0);
   binius_pcs_committed_destroy(committed);
   return rc ? rc : clear_error();

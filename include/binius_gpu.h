@@ -240,6 +240,10 @@ int binius_prover_destroy(binius_prover* prover);
 int binius_prover_info(const binius_prover* prover, uint32_t* h_out12);
 int binius_prover_prove(const binius_prover* prover, const void* d_witness,
                         binius_transcript* transcript, void* stream);
+/* Host wall-clock milliseconds of the last prove's phases (the spans of prove.rs:164-300):
+ * witness commit, IntMul, BitAnd, shift reduction, PCS opening.  No counterpart in the reference
+ * beyond its tracing spans. */
+int binius_prover_phase_ms(const binius_prover* prover, double* h_out5);
 
 /* ------------------------------------------------------------------------------------------
  * Integer multiplication reduction.
@@ -277,6 +281,20 @@ int binius_shift_reduction_prove(const binius_cs* cs, const void* d_witness,
 uint32_t binius_fri_n_test_queries(uint32_t security_bits, uint32_t log_inv_rate);
 uint32_t binius_fri_estimate_optimal_arity(uint32_t log_block_length, uint32_t digest_size,
                                            uint32_t field_size);
+
+/* ------------------------------------------------------------------------------------------
+ * Bivariate product sumcheck rounds (BivariateProductSumcheckProver::execute / fold,
+ * prover/prover/src/protocols/sumcheck/bivariate_product.rs:43-95; fold_highest_var_inplace,
+ * verifier/math/src/multilinear/fold.rs:14-29).  d_a, d_b: 2^log_len elements each.
+ * execute: d_out2 = (y_1, y_inf) = (sum a_hi b_hi, sum (a_lo + a_hi)(b_lo + b_hi)).
+ * fold_execute: folds the top variable of both by h_r in place (a[i] += r (a[i + half] - a[i]))
+ * and writes the next round's (y_1, y_inf) on the 2^(log_len-1) folded values.  d_out2 stays on
+ * the device; both are asynchronous on `stream`.
+ * ------------------------------------------------------------------------------------------ */
+int binius_sumcheck_bivariate_execute(const void* d_a, const void* d_b, uint32_t log_len,
+                                      void* d_out2, void* stream);
+int binius_sumcheck_bivariate_fold_execute(void* d_a, void* d_b, uint32_t log_len,
+                                           const void* h_r, void* d_out2, void* stream);
 
 /* Elementwise GF(2^128) products d_out[i] = d_a[i] * d_b[i] (kernel-level check of the field
  * multiplier; BinaryField128bGhash::mul, verifier/field/src/ghash.rs:188-194). */
