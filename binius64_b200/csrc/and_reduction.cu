@@ -142,9 +142,17 @@ const AndConstants& and_constants() {
 void lagrange_b128(uint32_t dim, u128h x, u128h* out) {
   const AndConstants& C = and_constants();
   const uint32_t n = 1u << dim;
-  u128h denom = 1;
-  for (uint32_t u = 1; u < n; u++) denom = host_gf_mul(denom, C.phi[u]);
-  const u128h dinv = host_gf_inv(denom);
+  // 1 / prod_{u != 0} phi(u): a constant per dimension, computed once
+  static const std::vector<u128h> dinvs = [&C] {
+    std::vector<u128h> v(9);
+    for (uint32_t d = 0; d <= 8; d++) {
+      u128h denom = 1;
+      for (uint32_t u = 1; u < (1u << d); u++) denom = host_gf_mul(denom, C.phi[u & 255]);
+      v[d] = host_gf_inv(denom);
+    }
+    return v;
+  }();
+  const u128h dinv = dinvs[dim];
   std::vector<u128h> diff(n), suffix(n + 1);
   for (uint32_t s = 0; s < n; s++) diff[s] = x ^ C.phi[s];
   suffix[n] = 1;

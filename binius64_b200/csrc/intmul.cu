@@ -225,18 +225,51 @@ hu128 sq_n(hu128 x, int n) {
   for (int i = 0; i < n; i++) x = host_gf_mul(x, x);
   return x;
 }
+// 1 / (g^(2^i) - 1) for i < 128 (normalize_a_c_exponent_evals, common.rs:107-138), computed once.
+const hu128* conj_inv_table() {
+  static const std::vector<hu128> table = [] {
+    std::vector<hu128> t(128);
+    hu128 c = ((hu128)0x494ef99794d5244fULL << 64) | (hu128)0x9152df59d87a9186ULL;
+    for (int i = 0; i < 128; i++, c = host_gf_mul(c, c)) t[i] = host_gf_inv(c ^ 1);
+    return t;
+  }();
+  return table.data();
+}
+
+// normalize_a_c_exponent_evals: the 192 leaf evaluations (a, c_lo, c_hi) -> bit evaluations.
+void normalize_leaves(const std::vector<hu128>& biv, IntMulResult& res) {
+  const hu128* inv = conj_inv_table();
+  res.a_evals.clear();
+  res.c_lo_evals.clear();
+  res.c_hi_evals.clear();
+  for (int i = 0; i < 64; i++) {
+    res.a_evals.push_back(host_gf_mul(biv[i] ^ 1, inv[i]));
+    res.c_lo_evals.push_back(host_gf_mul(biv[64 + i] ^ 1, inv[i]));
+    res.c_hi_evals.push_back(host_gf_mul(biv[128 + i] ^ 1, inv[64 + i]));
+  }
+}
+
 hu128 eval_poly(const Poly& c, hu128 x) {
   hu128 acc = 0;
   for (size_t i = c.size(); i-- > 0;) acc = host_gf_mul(acc, x) ^ c[i];
   return acc;
 }
+// (1 + alpha)^-1 (invert_or_zero), memoised per thread: the claims of one prover share alpha.
+hu128 inv_one_plus(hu128 alpha) {
+  thread_local hu128 last_alpha = 0, last_inv = 1;
+  if (alpha != last_alpha) {
+    last_alpha = alpha;
+    last_inv = host_gf_inv(1 ^ alpha);
+  }
+  return last_inv;
+}
 // RoundEvals2 / RoundEvals1 ::interpolate_eq (round_evals.rs:23-27, 80-87).
 Poly interp2(hu128 sum, hu128 y1, hu128 yinf, hu128 alpha) {
-  const hu128 y0 = host_gf_mul(sum ^ host_gf_mul(y1, alpha), host_gf_inv(1 ^ alpha));
+  const hu128 y0 = host_gf_mul(sum ^ host_gf_mul(y1, alpha), inv_one_plus(alpha));
   return {y0, y1 ^ y0 ^ yinf, yinf};
 }
 Poly interp1(hu128 sum, hu128 y1, hu128 alpha) {
-  const hu128 y0 = host_gf_mul(sum ^ host_gf_mul(y1, alpha), host_gf_inv(1 ^ alpha));
+  const hu128 y0 = host_gf_mul(sum ^ host_gf_mul(y1, alpha), inv_one_plus(alpha));
   return {y0, y1 ^ y0};
 }
 // round_coeffs_by_eq (round_evals.rs:145-156) times `scale`.
@@ -291,6 +324,12 @@ class IntMulDevice {
 
   int run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* d_lo, const uint64_t* d_hi,
           uint32_t n_vars, IntMulResult& res);
+
+ private:
+  // One statement (n_vars = 0): every sumcheck has zero rounds, so the transcript carries the
+  // tree values themselves; they are read back from the device in one copy.
+  int run_single(uint4* acl, uint4* btree, uint4* bcols, uint4* lo0, const uint64_t* d_a,
+                 const uint64_t* d_b, const uint64_t* d_lo, IntMulResult& res);
 
  private:
   template <class T>
@@ -394,6 +433,56 @@ int IntMulDevice::layer(uint4* set, uint32_t pairs, std::vector<hu128>& point,
   return BINIUS_OK;
 }
 
+int IntMulDevice::run_single(uint4* acl, uint4* btree, uint4* bcols, uint4* lo0,
+                             const uint64_t* d_a, const uint64_t* d_b, const uint64_t* d_lo,
+                             IntMulResult& res) {
+  constexpr int kAcl = 3 * 127 + 2, kB = 127;
+  bit_columns_kernel<<<1, kT, 0, s_>>>(d_b, 1, 0, 64, bcols, 1);
+  bit_columns_kernel<<<1, kT, 0, s_>>>(d_a, 1, 0, 1, acl + 3 * 127, 1);
+  bit_columns_kernel<<<1, kT, 0, s_>>>(d_b, 1, 0, 1, acl + 3 * 127 + 1, 1);
+  bit_columns_kernel<<<1, kT, 0, s_>>>(d_lo, 1, 0, 1, lo0, 1);
+  if (int rc = check("bit_columns_kernel", 4)) return rc;
+  // c_root = c_lo_root * c_hi_root (acl nodes 1 and 2), through the dot kernel with eq = [1]
+  if (int rc = eq_single({}, 0, eq_)) return rc;
+  BGPU_CUDA(cudaMemsetAsync(acc_, 0, 16, s_));
+  dot_kernel<<<1, kT, 0, s_>>>(acl + 1, acl + 2, eq_, 1, acc_);
+  if (int rc = check("dot_kernel")) return rc;
+  std::vector<hu128> hacl(kAcl), hb(kB), hcols(64);
+  hu128 c_root = 0, lo_bit = 0;
+  BGPU_CUDA(cudaMemcpyAsync(hacl.data(), acl, 16 * kAcl, cudaMemcpyDeviceToHost, s_));
+  BGPU_CUDA(cudaMemcpyAsync(hb.data(), btree, 16 * kB, cudaMemcpyDeviceToHost, s_));
+  BGPU_CUDA(cudaMemcpyAsync(hcols.data(), bcols, 16 * 64, cudaMemcpyDeviceToHost, s_));
+  BGPU_CUDA(cudaMemcpyAsync(&c_root, acc_, 16, cudaMemcpyDeviceToHost, s_));
+  BGPU_CUDA(cudaMemcpyAsync(&lo_bit, lo0, 16, cudaMemcpyDeviceToHost, s_));
+  BGPU_CUDA(cudaStreamSynchronize(s_));
+  auto acl_layer = [&](int k) { return hacl.begin() + 3 * ((1 << k) - 1); };
+  auto b_layer = [&](int k) { return hb.begin() + ((1 << k) - 1); };
+  write_elems(t_, {hb[0], c_root});
+  for (int d = 0; d < 6; d++) {  // phase 1
+    sample(t_);
+    write_elems(t_, std::vector<hu128>(b_layer(d + 1), b_layer(d + 1) + (2 << d)));
+  }
+  sample(t_);  // phase 3
+  std::vector<hu128> sel = hcols;
+  sel.push_back(hacl[0]);
+  write_elems(t_, sel);
+  write_elems(t_, {hacl[1], hacl[2]});
+  for (int d = 0; d < 5; d++) {  // phase 4
+    sample(t_);
+    write_elems(t_, std::vector<hu128>(acl_layer(d + 1), acl_layer(d + 1) + (6 << d)));
+  }
+  write_elems(t_, {lo_bit});  // phase 5
+  sample(t_);
+  std::vector<hu128> biv(acl_layer(6), acl_layer(6) + 194);
+  write_elems(t_, biv);
+  write_elems(t_, {lo_bit});
+  write_elems(t_, hcols);
+  res = IntMulResult();
+  normalize_leaves(biv, res);
+  res.b_evals = hcols;
+  return BINIUS_OK;
+}
+
 int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* d_lo,
                       const uint64_t* d_hi, uint32_t n_vars, IntMulResult& res) {
   n_ = n_vars;
@@ -438,6 +527,8 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
     tree_layer_kernel<<<blocks_for((1u << k) * N), kT, 0, s_>>>(b_layer(k + 1), b_layer(k), 1u << k, N, N);
     if (int rc = check("tree_layer_kernel")) return rc;
   }
+
+  if (n_ == 0) return run_single(acl, btree, bcols, lo0, d_a, d_b, d_lo, res);
 
   // ---- root evaluations at the initial point
   std::vector<hu128> point0(n_);
@@ -611,18 +702,8 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
     write_elems(t_, lo_ev);
     write_elems(t_, b_ev);
     // normalize_a_c_exponent_evals (common.rs:107-138)
-    std::vector<hu128> conj(128);
-    hu128 c = g;
-    for (int i = 0; i < 128; i++, c = host_gf_mul(c, c)) conj[i] = c;
     res.eval_point.assign(ch.rbegin(), ch.rend());
-    res.a_evals.clear();
-    res.c_lo_evals.clear();
-    res.c_hi_evals.clear();
-    for (int i = 0; i < 64; i++) {
-      res.a_evals.push_back(host_gf_mul(biv[i] ^ 1, host_gf_inv(conj[i] ^ 1)));
-      res.c_lo_evals.push_back(host_gf_mul(biv[64 + i] ^ 1, host_gf_inv(conj[i] ^ 1)));
-      res.c_hi_evals.push_back(host_gf_mul(biv[128 + i] ^ 1, host_gf_inv(conj[64 + i] ^ 1)));
-    }
+    normalize_leaves(biv, res);
     res.b_evals = b_ev;
   }
   return BINIUS_OK;

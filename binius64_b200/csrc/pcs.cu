@@ -51,6 +51,7 @@ struct binius_pcs_committed {
   uint32_t log_leaves;   // rs_log_len
   void* d_codeword;
   void* d_nodes;
+  cudaStream_t stream;   // the commit stream: allocation and release are ordered on it
   uint8_t root[32];
 };
 
@@ -357,33 +358,35 @@ int binius_pcs_commit(const binius_pcs* P, const void* d_witness, binius_pcs_com
   c->log_leaves = P->rs_log_len();
   c->d_codeword = nullptr;
   c->d_nodes = nullptr;
+  c->stream = s;
   int rc = BINIUS_OK;
   do {
-    cudaError_t e = cudaMalloc(&c->d_codeword, 16ull << c->log_len);
-    if (e != cudaSuccess) { rc = cuda_error(e, "cudaMalloc(codeword)"); break; }
-    e = cudaMalloc(&c->d_nodes, 32ull * ((2ull << c->log_leaves) - 1));
-    if (e != cudaSuccess) { rc = cuda_error(e, "cudaMalloc(tree)"); break; }
+    // stream-ordered allocations from the (cached) device pool: no device-wide synchronisation
+    cudaError_t e = cudaMallocAsync(&c->d_codeword, 16ull << c->log_len, s);
+    if (e != cudaSuccess) { rc = cuda_error(e, "cudaMallocAsync(codeword)"); break; }
+    e = cudaMallocAsync(&c->d_nodes, 32ull * ((2ull << c->log_leaves) - 1), s);
+    if (e != cudaSuccess) { rc = cuda_error(e, "cudaMallocAsync(tree)"); break; }
     if ((rc = binius_fri_commit_interleaved(P->ntt, d_witness, P->log_dim(), P->log_inv_rate,
                                             P->log_batch, c->d_codeword, c->d_nodes, c->root,
                                             stream)))
       break;
   } while (0);
   if (rc) {
-    if (c->d_codeword) cudaFree(c->d_codeword);
-    if (c->d_nodes) cudaFree(c->d_nodes);
+    if (c->d_codeword) cudaFreeAsync(c->d_codeword, s);
+    if (c->d_nodes) cudaFreeAsync(c->d_nodes, s);
     delete c;
     return rc;
   }
-  (void)s;
   if (h_root) memcpy(h_root, c->root, 32);
   *out = c;
   return clear_error();
 }
 
+// Releases the buffers in order on the commit stream, which must still exist.
 int binius_pcs_committed_destroy(binius_pcs_committed* c) {
   if (!c) return BINIUS_OK;
-  cudaFree(c->d_codeword);
-  cudaFree(c->d_nodes);
+  cudaFreeAsync(c->d_codeword, c->stream);
+  cudaFreeAsync(c->d_nodes, c->stream);
   delete c;
   return BINIUS_OK;
 }

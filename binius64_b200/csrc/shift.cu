@@ -168,26 +168,31 @@ __global__ void shift_h_kernel(Lag64 L, uint4* __restrict__ h) {
   h[idx] = val;
 }
 
-// out[v] = <h_v, eq(r_j ++ r_s)> for the 8 variants (evaluate_h_op).  One CTA of 256 threads.
+// out[v] += <h_v, eq(r_j ++ r_s)> for the 8 variants (evaluate_h_op); out zeroed by the caller.
+// Each of kHopsBlocks CTAs takes a 4096 / kHopsBlocks slice of the index; a thread owns one
+// variant and every 32nd index of the slice.
+constexpr int kHopsBlocks = 64;
 __global__ void __launch_bounds__(256)
     shift_h_ops_kernel(const uint4* __restrict__ h, const uint4* __restrict__ eq,
-                       uint4* __restrict__ out) {
+                       uint32_t* __restrict__ out) {
   __shared__ uint4 part[256];
   const uint32_t v = threadIdx.x & 7;
+  constexpr uint32_t kSlice = kLen / kHopsBlocks;
   u256 acc = {0, 0, 0, 0};
-  for (uint32_t i = threadIdx.x >> 3; i < kLen; i += 32) xor_into(acc, clmul128(h[i * 8 + v], eq[i]));
+  for (uint32_t i = blockIdx.x * kSlice + (threadIdx.x >> 3); i < (blockIdx.x + 1) * kSlice; i += 32)
+    xor_into(acc, clmul128(h[i * 8 + v], eq[i]));
   part[threadIdx.x] = reduce256(acc);
   __syncthreads();
   if (threadIdx.x < 8) {
     uint4 x = gf_zero();
     for (uint32_t q = 0; q < 32; q++) gf_add_into(x, part[q * 8 + threadIdx.x]);
-    out[threadIdx.x] = x;
+    atomic_xor_gf(out + 4 * threadIdx.x, x);
   }
 }
 
 // T[key] = lambda_class * h_op(kind)[v] * eq(r_s)[s] (the monster scalars, monster.rs:168-190).
 __global__ void shift_scalars_kernel(ClassPowers pw, Lag64 eq_rs, const uint4* __restrict__ h_ops,
-                                     uint4* __restrict__ T) {
+                                     uint32_t mul_offset, uint4* __restrict__ T) {
   const uint32_t key = blockIdx.x * blockDim.x + threadIdx.x;
   if (key >= kShiftKeys) return;
   const uint32_t cls = key & 7, id = key >> 3, v = id >> 6, s = id & 63;
@@ -195,7 +200,7 @@ __global__ void shift_scalars_kernel(ClassPowers pw, Lag64 eq_rs, const uint4* _
     T[key] = gf_zero();
     return;
   }
-  const uint4 hop = h_ops[(cls < 3 ? 0 : 8) + v];
+  const uint4 hop = h_ops[(cls < 3 ? 0 : mul_offset) + v];
   T[key] = gf_mul(gf_mul(pw.p[cls], hop), eq_rs.l[s]);
 }
 
@@ -424,14 +429,15 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
   eq_host(r_s.data(), 6, eq_rs);
   SHIFT_TRY(fold_words64(d_witness, n_words, eq_rj, W, s));
   SHIFT_TRY(eq_tensor(to_u4(rev).data(), 12, eq_rjs, s));
-  for (int kind = 0; kind < 2; kind++) {
-    const uint4* hk = h_keep + ((same_z || kind == 0) ? 0 : kFlat);
-    shift_h_ops_kernel<<<1, 256, 0, s>>>(hk, eq_rjs, h_ops + 8 * kind);
+  BGPU_CUDA(cudaMemsetAsync(h_ops, 0, 16 * 16, s));
+  for (int kind = 0; kind < (same_z ? 1 : 2); kind++) {
+    shift_h_ops_kernel<<<kHopsBlocks, 256, 0, s>>>(h_keep + kind * kFlat, eq_rjs,
+                                                   reinterpret_cast<uint32_t*>(h_ops + 8 * kind));
     SHIFT_TRY(launched("shift_h_ops_kernel"));
   }
   Lag64 ers;
   for (int i = 0; i < 64; i++) ers.l[i] = u4(eq_rs[i]);
-  shift_scalars_kernel<<<kShiftKeys / 256, 256, 0, s>>>(pw, ers, h_ops, T);
+  shift_scalars_kernel<<<kShiftKeys / 256, 256, 0, s>>>(pw, ers, h_ops, same_z ? 0 : 8, T);
   SHIFT_TRY(launched("shift_scalars_kernel"));
   BGPU_CUDA(cudaMemsetAsync(M, 0, 16ull * n_words, s));
   if (terms.n) {

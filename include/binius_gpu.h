@@ -174,7 +174,9 @@ int binius_pcs_create(const binius_ntt* ntt, uint32_t log_msg, uint32_t log_batc
                       uint32_t n_queries, binius_pcs** out);
 int binius_pcs_destroy(binius_pcs* pcs);
 /* RS encode + Merkle commit of d_witness (2^log_msg elements); the codeword and tree stay on the
- * device in *out; h_root receives the 32-byte commitment.  Synchronous. */
+ * device in *out; h_root receives the 32-byte commitment.  Synchronous.  The buffers come from
+ * the device's stream-ordered pool on `stream` and are released on it by
+ * binius_pcs_committed_destroy, so the stream must outlive the committed object. */
 int binius_pcs_commit(const binius_pcs* pcs, const void* d_witness, binius_pcs_committed** out,
                       void* h_root, void* stream);
 int binius_pcs_committed_destroy(binius_pcs_committed* committed);
