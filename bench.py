@@ -90,7 +90,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="prove", choices=["prove", "commit"])
+    ap.add_argument("--workload", default="prove", choices=["prove", "commit", "batch", "serve"])
+    ap.add_argument("--requests", type=int, default=256, help="batch / serve: proofs submitted")
+    ap.add_argument("--workers", type=int, default=16, help="batch / serve: proving threads")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--log-words", type=int, default=None,
                     help="prove workload: log2 committed words (default 20)")
@@ -254,6 +256,130 @@ def bivariate_roofline(torch, bg, lib, device, stream, reps=20):
     return launch_ms, bytes_per_launch, mults
 
 
+
+# ----------------------------------------------------------------------------- batch / serve
+
+BATCH_LOG_MIN, BATCH_LOG_MAX, BATCH_DISTINCT = 12, 20, 12
+
+
+def batch_statements(torch, bg, device, n_distinct=BATCH_DISTINCT):
+    """Distinct synthetic statements with log2(words) uniform in [12, 20] (log-uniform sizes),
+    AND chains over shifted operands plus 2^(log_words - 10) MUL constraints each."""
+    from binius64_b200 import constraint_system as csm
+    rng = np.random.default_rng(SEED + 7)
+    sizes = sorted(int(x) for x in rng.integers(BATCH_LOG_MIN, BATCH_LOG_MAX + 1, size=n_distinct))
+    out = []
+    for i, lw in enumerate(sizes):
+        n_mul = max(1, 1 << (lw - 10))
+        sc = csm.synthetic_circuit(lw, n_and_for(lw) - 2 * n_mul, n_mul, seed=SEED + 100 + i)
+        prover = bg.Prover(bg.DeviceConstraintSystem(sc.cs.serialize(), device=device),
+                           LOG_INV_RATE)
+        w = torch.from_numpy(sc.witness.view(np.int64)).to(f"cuda:{device}")
+        out.append((lw, prover, w))
+    return sizes, out
+
+
+def one_at_a_time(torch, stmts, order):
+    """The requests proved back to back on one stream; returns (seconds, proofs by statement)."""
+    proofs = {}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in order:
+        pb = stmts[i][1].prove(stmts[i][2]).finalize()
+        proofs.setdefault(i, pb)
+    torch.cuda.synchronize()
+    return time.perf_counter() - t0, proofs
+
+
+def run_queue(bg, stmts, order, workers, arrivals=None):
+    """Submits the requests (all at once, or at the given arrival offsets in seconds) to a
+    ProveQueue; returns (seconds, latencies ms, prove ms, proofs in request order)."""
+    q = bg.ProveQueue(n_workers=workers)
+    tickets = []
+    t0 = time.perf_counter()
+    for k, i in enumerate(order):
+        if arrivals is not None:
+            delay = t0 + arrivals[k] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+        tickets.append(q.submit(stmts[i][1], stmts[i][2]))
+    lat, prove, proofs = [], [], []
+    for t in tickets:
+        pb, tm = q.wait(t)
+        lat.append(tm["latency_ms"])
+        prove.append(tm["prove_ms"])
+        proofs.append(pb)
+    secs = time.perf_counter() - t0
+    q.close()
+    return secs, lat, prove, proofs
+
+
+def batch_summary(torch, bg, device, n_requests, workers):
+    sizes, stmts = batch_statements(torch, bg, device)
+    rng = np.random.default_rng(SEED + 11)
+    order = [int(x) for x in rng.integers(0, len(stmts), size=n_requests)]
+    for i in set(order):  # warm-up of every shape
+        stmts[i][1].prove(stmts[i][2])
+    t_seq, lone = one_at_a_time(torch, stmts, order)
+    t_q, lat, prove, proofs = run_queue(bg, stmts, order, workers)
+    identical = all(proofs[k] == lone[i] for k, i in enumerate(order))
+    return {
+        "requests": n_requests, "workers": workers, "distinct_statements": len(stmts),
+        "log_words": sizes, "proofs_per_s": n_requests / t_q,
+        "one_at_a_time_proofs_per_s": n_requests / t_seq,
+        "speedup_vs_one_at_a_time": t_seq / t_q,
+        "latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99)},
+        "prove_ms_in_mix": {"p50": pct(prove, 50), "p99": pct(prove, 99)},
+        "bit_identical_to_lone_proofs": identical,
+    }, (sizes, stmts, order, t_seq, lone)
+
+
+def run_batch_workload(args, rank, world, local, serve=False):
+    import torch
+    import binius64_b200 as bg
+    from binius64_b200._ffi import lib
+
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return
+    clk = sample_clocks_start(local)
+    launches0 = lib().binius_launch_count()
+    summ, (sizes, stmts, order, t_seq, lone) = batch_summary(torch, bg, local, args.requests,
+                                                             args.workers)
+    line = {
+        "metric": "batched proofs/s" if not serve else "served proofs/s (Poisson arrivals)",
+        "unit": "proofs/s", "n_gpus": 1, "steps": args.requests, "warmup": len(set(order)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "GF(2^128) GHASH / u64 words",
+        "data": "synthetic statements, log2(words) uniform in [12, 20], seeded",
+        "config": {"workload": "independent proofs of a seeded mix of synthetic AND/MUL "
+                               "constraint systems (2^12..2^20 words) through ProveQueue",
+                   "requests": args.requests, "workers": args.workers, "log_words": sizes},
+    }
+    if not serve:
+        line.update({"value": summ["proofs_per_s"], "ms_per_step": 1000.0 / summ["proofs_per_s"],
+                     "batch": summ})
+    else:
+        rate = 0.7 * summ["proofs_per_s"]
+        rng = np.random.default_rng(SEED + 13)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=args.requests)).tolist()
+        t_q, lat, prove, proofs = run_queue(bg, stmts, order, args.workers, arrivals)
+        identical = all(proofs[k] == lone[i] for k, i in enumerate(order))
+        line.update({"value": args.requests / t_q, "ms_per_step": 1000.0 * t_q / args.requests,
+                     "serve": {"arrival_rate_per_s": rate, "proofs_per_s": args.requests / t_q,
+                               "latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99),
+                                              "max": max(lat)},
+                               "prove_ms_in_mix": {"p50": pct(prove, 50), "p99": pct(prove, 99)},
+                               "one_at_a_time_proofs_per_s": args.requests / t_seq,
+                               "bit_identical_to_lone_proofs": identical},
+                     "batch": summ})
+    line["gpu_launches"] = int(round((lib().binius_launch_count() - launches0) / args.requests))
+    line["e2e"] = {"value": line["value"], "unit": "proofs/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}
+    line["clocks"] = sample_clocks_stop(clk)
+    print(json.dumps(line), flush=True)
+
+
 def run_prove(args, rank, world, local):
     import torch
     import binius64_b200 as bg
@@ -337,6 +463,9 @@ def run_prove(args, rank, world, local):
                    "sample": f"2 whole proofs of the same 2^{LOG_WORDS}-word circuit on the "
                              "oracle (C++ restatement of the reference prover, PCLMULQDQ, "
                              "std::thread over all host cores); the Rust reference needs cargo"}
+        batched = None
+        if world == 1:
+            batched, _ = batch_summary(torch, bg, local, 128, 16)
         ph = {k: statistics.median(p[k] for p in phases) for k in phases[0]}
         line = {
             "metric": PROVE_METRIC, "value": ms, "unit": "ms", "n_gpus": world,
@@ -348,6 +477,7 @@ def run_prove(args, rank, world, local):
             "latency_ms": {"p50": pct(per, 50), "p99": pct(per, 99), "min": min(per),
                            "max": max(per), "wall_per_proof": 1000.0 * wall / args.steps},
             "phase_ms_host": ph,
+            "batched": batched,
             "proof_bytes": proof_len,
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(host_w.numel() * 8),
                     "d2h_bytes_per_step": proof_len},
@@ -599,6 +729,8 @@ def main():
         return
     if args.workload == "prove":
         run_prove(args, rank, world, local)
+    elif args.workload in ("batch", "serve"):
+        run_batch_workload(args, rank, world, local, serve=args.workload == "serve")
     else:
         run_commit(args, rank, world, local)
 

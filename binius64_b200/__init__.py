@@ -576,3 +576,69 @@ class Prover:
             except Exception:
                 pass
             self._h = None
+
+
+class ProveQueue:
+    """Batched / served proving over binius_queue_* (see include/binius_gpu.h): n_workers proving
+    threads with their own streams, FIFO admission under an HBM budget."""
+
+    def __init__(self, n_workers: int = 8, hbm_budget_bytes: int = 0, device: int | None = None):
+        torch = _torch()
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        self._h = ctypes.c_void_p()
+        check(lib().binius_queue_create(self.device, n_workers, hbm_budget_bytes,
+                                        ctypes.byref(self._h)))
+        self._keep = {}
+
+    def submit(self, prover: Prover, witness) -> int:
+        """witness: a device int64 tensor or a host numpy uint64 array of committed_total_len
+        words; it is kept alive until wait() returns."""
+        t = ctypes.c_uint64(0)
+        if isinstance(witness, np.ndarray):
+            w = np.ascontiguousarray(witness, dtype=np.uint64)
+            if w.shape[0] != prover.cs.committed_total_len:
+                raise ArgumentError(1, "witness length != committed_total_len")
+            check(lib().binius_queue_submit(self._h, prover._h, w.ctypes.data_as(ctypes.c_void_p),
+                                            0, ctypes.byref(t)))
+        else:
+            w = witness
+            if w.numel() != prover.cs.committed_total_len:
+                raise ArgumentError(1, "witness length != committed_total_len")
+            check(lib().binius_queue_submit(self._h, prover._h, w.data_ptr(), 1, ctypes.byref(t)))
+        self._keep[t.value] = (w, prover)
+        return t.value
+
+    def done(self, ticket: int) -> bool:
+        d = ctypes.c_int(0)
+        check(lib().binius_queue_poll(self._h, ticket, ctypes.byref(d)))
+        return bool(d.value)
+
+    def wait(self, ticket: int):
+        """Returns (proof bytes, {"queued_ms", "prove_ms", "latency_ms"})."""
+        n = ctypes.c_size_t(0)
+        times = (ctypes.c_double * 3)()
+        cap = 1 << 21
+        while True:
+            buf = (ctypes.c_uint8 * cap)()
+            rc = lib().binius_queue_wait(self._h, ticket, buf, cap, ctypes.byref(n), times)
+            if rc == 1 and n.value > cap:  # buffer too small: the result is kept
+                cap = n.value
+                continue
+            break
+        self._keep.pop(ticket, None)
+        check(rc)
+        return bytes(buf)[: n.value], {"queued_ms": times[0], "prove_ms": times[1],
+                                       "latency_ms": times[2]}
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().binius_queue_destroy(h)
+            self._h = None
+        self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -86,6 +86,13 @@ _SIGS = {
     "binius_prover_info": (_int, [_vp, _vp]),
     "binius_prover_prove": (_int, [_vp, _vp, _vp, _vp]),
     "binius_prover_phase_ms": (_int, [_vp, _vp]),
+    "binius_prover_committed_words": (_u64, [_vp]),
+    "binius_prover_workspace_bytes": (_u64, [_vp]),
+    "binius_queue_create": (_int, [_int, _u32, _u64, _vp]),
+    "binius_queue_destroy": (_int, [_vp]),
+    "binius_queue_submit": (_int, [_vp, _vp, _vp, _int, _vp]),
+    "binius_queue_poll": (_int, [_vp, _u64, _vp]),
+    "binius_queue_wait": (_int, [_vp, _u64, _vp, _c.c_size_t, _vp, _vp]),
     "binius_fri_n_test_queries": (_u32, [_u32, _u32]),
     "binius_fri_estimate_optimal_arity": (_u32, [_u32, _u32, _u32]),
     "binius_gf_mul_batch": (_int, [_vp, _vp, _vp, _u64, _vp]),

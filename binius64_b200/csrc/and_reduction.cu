@@ -490,7 +490,7 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
     count_launch();
     uint8_t msg[64 * 16];
     e = cudaMemcpyAsync(msg, d_acc, sizeof(msg), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = stream_wait(s);
     if (e != cudaSuccess) { rc = cuda_error(e, "univariate message"); break; }
     t.message(msg, sizeof(msg));
     uint8_t zb[16];
@@ -539,7 +539,7 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
       count_launch();
       uint8_t ys[32];
       e = cudaMemcpyAsync(ys, d_acc, 32, cudaMemcpyDeviceToHost, s);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e == cudaSuccess) e = stream_wait(s);
       if (e != cudaSuccess) { rc = cuda_error(e, "round sums"); break; }
       const u128h y1 = from_bytes16(ys), yinf = from_bytes16(ys + 16);
       const u128h alpha = point[n_rem - 1];
@@ -565,7 +565,7 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
     count_launch();
     uint8_t ev[48];
     e = cudaMemcpyAsync(ev, d_ev, 48, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = stream_wait(s);
     if (e != cudaSuccess) { rc = cuda_error(e, "final evals"); break; }
     t.message(ev, 48);
     res.a_eval = from_bytes16(ev);

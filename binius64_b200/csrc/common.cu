@@ -83,6 +83,43 @@ hu128 host_gf_inv(hu128 a) {
   return host_gf_mul(r, r);
 }
 
+// Raises the dynamic shared memory limit of `func` on the current device to `bytes`, once per
+// (device, kernel).  Setting a per-launch value instead races between threads that launch the
+// same kernel with different sizes.
+int ensure_smem_limit(const void* func, size_t bytes) {
+  static std::mutex mu;
+  static std::vector<std::pair<int, const void*>> done;
+  int dev = 0;
+  BGPU_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  for (auto& d : done)
+    if (d.first == dev && d.second == func) return BINIUS_OK;
+  BGPU_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  done.emplace_back(dev, func);
+  return BINIUS_OK;
+}
+
+// Waits for the work queued on `s`.  Threads that set blocking waits (the proving workers of a
+// queue, many of which wait at once) sleep on a blocking-sync event instead of spinning in
+// cudaStreamSynchronize, leaving the host cores to the threads that have work.
+namespace {
+thread_local bool t_blocking_wait = false;
+thread_local cudaEvent_t t_wait_event = nullptr;
+}  // namespace
+
+void set_blocking_waits(bool on) { t_blocking_wait = on; }
+
+cudaError_t stream_wait(cudaStream_t s) {
+  if (!t_blocking_wait) return cudaStreamSynchronize(s);
+  if (!t_wait_event) {
+    cudaError_t e = cudaEventCreateWithFlags(&t_wait_event,
+                                             cudaEventBlockingSync | cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+  }
+  cudaError_t e = cudaEventRecord(t_wait_event, s);
+  return e == cudaSuccess ? cudaEventSynchronize(t_wait_event) : e;
+}
+
 // The stream-ordered allocator of `device` keeps freed blocks cached (release threshold = max)
 // instead of returning them to the driver at every synchronisation: a proof synchronises once per
 // sumcheck round and reallocates its scratch per phase.  The attribute belongs to this process's

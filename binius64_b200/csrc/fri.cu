@@ -291,7 +291,7 @@ int binius_fri_commit_interleaved(const binius_ntt* ntt, const void* d_msg, uint
   if (h_root) {
     const uint8_t* root = static_cast<const uint8_t*>(d_nodes) + 32 * ((2ull << log_leaves) - 2);
     BGPU_CUDA(cudaMemcpyAsync(h_root, root, 32, cudaMemcpyDeviceToHost, s));
-    BGPU_CUDA(cudaStreamSynchronize(s));
+    BGPU_CUDA(stream_wait(s));
   }
   return clear_error();
 }

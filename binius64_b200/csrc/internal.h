@@ -31,6 +31,14 @@ int cuda_error(cudaError_t e, const char* what);
     if (!(cond)) return ::bgpu::set_error(BINIUS_E_ARG, msg); \
   } while (0)
 
+// Waits for the work queued on s: cudaStreamSynchronize, or a blocking-sync event wait on threads
+// that called set_blocking_waits(true).
+cudaError_t stream_wait(cudaStream_t s);
+void set_blocking_waits(bool on);
+
+// Sets the dynamic shared memory limit of a kernel once per device (see common.cu).
+int ensure_smem_limit(const void* func, size_t bytes);
+
 // Keeps the default memory pool of `device` from releasing cached blocks (see common.cu).
 int configure_device_pool(int device);
 

@@ -347,7 +347,7 @@ class IntMulDevice {
   }
   int sync_read(void* dst, const void* src, size_t bytes) {
     BGPU_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s_));
-    BGPU_CUDA(cudaStreamSynchronize(s_));
+    BGPU_CUDA(stream_wait(s_));
     return BINIUS_OK;
   }
   // values [0] of `count` multilinears with stride `stride`
@@ -355,7 +355,7 @@ class IntMulDevice {
     out.resize(count);
     BGPU_CUDA(cudaMemcpy2DAsync(out.data(), 16, set, 16 * stride, 16, count,
                                 cudaMemcpyDeviceToHost, s_));
-    BGPU_CUDA(cudaStreamSynchronize(s_));
+    BGPU_CUDA(stream_wait(s_));
     return BINIUS_OK;
   }
   int eq_single(const std::vector<hu128>& point, uint32_t m, uint4* out) {
@@ -454,7 +454,7 @@ int IntMulDevice::run_single(uint4* acl, uint4* btree, uint4* bcols, uint4* lo0,
   BGPU_CUDA(cudaMemcpyAsync(hcols.data(), bcols, 16 * 64, cudaMemcpyDeviceToHost, s_));
   BGPU_CUDA(cudaMemcpyAsync(&c_root, acc_, 16, cudaMemcpyDeviceToHost, s_));
   BGPU_CUDA(cudaMemcpyAsync(&lo_bit, lo0, 16, cudaMemcpyDeviceToHost, s_));
-  BGPU_CUDA(cudaStreamSynchronize(s_));
+  BGPU_CUDA(stream_wait(s_));
   auto acl_layer = [&](int k) { return hacl.begin() + 3 * ((1 << k) - 1); };
   auto b_layer = [&](int k) { return hb.begin() + ((1 << k) - 1); };
   write_elems(t_, {hb[0], c_root});

@@ -174,7 +174,7 @@ int binius_merkle_branch(const void* d_nodes, uint32_t log_leaves, uint64_t inde
     uint64_t node = layer_offset(log_leaves, j) | ((index >> j) ^ 1);
     BGPU_CUDA(cudaMemcpyAsync(out + 32 * j, nodes + 32 * node, 32, cudaMemcpyDeviceToHost, s));
   }
-  BGPU_CUDA(cudaStreamSynchronize(s));
+  BGPU_CUDA(stream_wait(s));
   return clear_error();
 }
 

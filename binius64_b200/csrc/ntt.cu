@@ -152,7 +152,11 @@ int launch_pass(const NttPass& p, uint4* data, const uint4* src, const uint4* tw
                 cudaStream_t stream) {
   size_t smem = ((size_t(1) << (p.k + p.c)) + (size_t(1) << p.k) - 1) * sizeof(uint4);
   auto kern = ntt_pass_kernel<INVERSE, RS>;
-  BGPU_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // the largest tile of any pass: 2^kTileBits elements plus 2^kMaxPassLayers - 1 twiddles
+  constexpr size_t kMaxSmem = ((size_t(1) << kTileBits) + (size_t(1) << kMaxPassLayers) - 1) *
+                              sizeof(uint4);
+  if (smem > kMaxSmem) return set_error(BINIUS_E_ARG, "ntt: pass tile exceeds the planned maximum");
+  if (int rc = ensure_smem_limit(reinterpret_cast<const void*>(kern), kMaxSmem)) return rc;
   uint64_t n_tiles = 1ull << (p.log_d - p.k - p.c);
   if (n_tiles > 0x7fffffffull) return set_error(BINIUS_E_ARG, "ntt: buffer too large");
   kern<<<(unsigned)n_tiles, kNttThreads, smem, stream>>>(data, src, tw, p);

@@ -126,7 +126,7 @@ struct DevFri {
     if (int rc = merkle_commit(out, log_leaves, log_coset, nodes, s)) return rc;
     BGPU_CUDA(cudaMemcpyAsync(root, nodes + 32 * ((2ull << log_leaves) - 2), 32,
                               cudaMemcpyDeviceToHost, s));
-    BGPU_CUDA(cudaStreamSynchronize(s));
+    BGPU_CUDA(stream_wait(s));
     next_commit = has_next ? next_commit + next_arity : -1;
     *committed = true;
     return BINIUS_OK;
@@ -153,7 +153,7 @@ struct DevFri {
       const uint32_t log_term = words.empty() ? C.log_len : word_log_len.back();
       std::vector<uint8_t> h(16ull << log_term);
       BGPU_CUDA(cudaMemcpyAsync(h.data(), term, h.size(), cudaMemcpyDeviceToHost, s));
-      BGPU_CUDA(cudaStreamSynchronize(s));
+      BGPU_CUDA(stream_wait(s));
       t.decommitment(h.data(), h.size());
     }
     const auto depths = P.optimal_depths();
@@ -169,7 +169,7 @@ struct DevFri {
         std::vector<uint8_t> h(32ull << d);
         const uint8_t* src = tr[i] + 32 * ((2ull << L) - 1 + 1 - (2ull << d));
         BGPU_CUDA(cudaMemcpyAsync(h.data(), src, h.size(), cudaMemcpyDeviceToHost, s));
-        BGPU_CUDA(cudaStreamSynchronize(s));
+        BGPU_CUDA(stream_wait(s));
         t.decommitment(h.data(), h.size());
       }
     }
@@ -205,7 +205,7 @@ struct DevFri {
       if ((rc = gather_segments(d_segs, (uint32_t)segs.size(), d_dst, s))) break;
       e = cudaMemcpyAsync(h.data(), d_dst, off, cudaMemcpyDeviceToHost, s);
       if (e != cudaSuccess) { rc = cuda_error(e, "download query openings"); break; }
-      e = cudaStreamSynchronize(s);
+      e = stream_wait(s);
       if (e != cudaSuccess) { rc = cuda_error(e, "query gather"); break; }
     } while (0);
     cudaFreeAsync(d_segs, s);
@@ -245,7 +245,7 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
       if ((rc = fold_1b_rows(static_cast<const uint4*>(d_witness), b, N, d_small, s))) break;
       uint8_t s_hat_v[128 * 16];
       cudaError_t e = cudaMemcpyAsync(s_hat_v, d_small, sizeof(s_hat_v), cudaMemcpyDeviceToHost, s);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e == cudaSuccess) e = stream_wait(s);
       if (e != cudaSuccess) { rc = cuda_error(e, "ring switch fold"); break; }
       t.message(s_hat_v, sizeof(s_hat_v));
       u128h v[128], u[128];
@@ -256,7 +256,7 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
       if ((rc = eq_tensor(reinterpret_cast<const uint4*>(r_dp), 7, eq_r, s))) break;
       uint8_t h_eq[128 * 16];
       e = cudaMemcpyAsync(h_eq, eq_r, sizeof(h_eq), cudaMemcpyDeviceToHost, s);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e == cudaSuccess) e = stream_wait(s);
       if (e != cudaSuccess) { rc = cuda_error(e, "eq(r'')"); break; }
       u128h sum = 0;
       for (int j = 0; j < 128; j++) sum ^= host_gf_mul(u[j], to_u128(h_eq + 16 * j));
@@ -276,7 +276,7 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
         if (rc) break;
         uint8_t ys[32];
         e = cudaMemcpyAsync(ys, d_small, 32, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess) e = stream_wait(s);
         if (e != cudaSuccess) { rc = cuda_error(e, "round sums"); break; }
         const u128h y1 = to_u128(ys), yinf = to_u128(ys + 16);
         const u128h c0 = sum ^ y1, c2 = yinf, c1 = y1 ^ c0 ^ c2;
@@ -305,7 +305,7 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
   cudaFreeAsync(b, s);
   cudaFreeAsync(eq_r, s);
   cudaFreeAsync(d_small, s);
-  cudaError_t e = cudaStreamSynchronize(s);
+  cudaError_t e = stream_wait(s);
   if (rc == BINIUS_OK && e != cudaSuccess) rc = cuda_error(e, "pcs prove");
   return rc;
 }

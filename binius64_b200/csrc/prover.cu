@@ -27,11 +27,13 @@ struct binius_prover {
   binius_pcs* pcs = nullptr;
   uint32_t log_inv_rate = 0, log_witness_elems = 0, log_batch = 0, n_queries = 0;
   std::vector<uint32_t> arities;
-  // host wall-clock milliseconds of the last prove's phases: commit, IntMul, AND, shift, PCS
-  mutable double phase_ms[5] = {0, 0, 0, 0, 0};
 };
 
 namespace {
+
+// Host wall-clock milliseconds of the calling thread's last prove: commit, IntMul, AND, shift,
+// PCS (per thread, so that concurrent proofs on one prover do not share it).
+thread_local double t_phase_ms[5] = {0, 0, 0, 0, 0};
 
 constexpr uint32_t kSecurityBits = 96;  // verifier/verifier/src/verify.rs:39
 constexpr uint32_t kDigestSize = 32;    // SHA-256
@@ -113,9 +115,24 @@ int binius_prover_info(const binius_prover* P, uint32_t* h_out12) {
   return clear_error();
 }
 
+uint64_t binius_prover_committed_words(const binius_prover* P) {
+  return P ? P->cs->committed_total_len : 0;
+}
+
+uint64_t binius_prover_workspace_bytes(const binius_prover* P) {
+  if (!P) return 0;
+  const binius_cs* cs = P->cs;
+  const uint64_t words = cs->committed_total_len, n_and = cs->and_ops.n_constraints;
+  const uint64_t n_mul = cs->mul_ops.n_constraints;
+  const uint64_t code = 16ull << (P->log_witness_elems + P->log_inv_rate);
+  // codeword + tree, AND columns / folds / eq, shift W / M / g parts, PCS fold buffers, IntMul
+  // trees; an upper bound of the stream-ordered allocations one proof holds at once
+  return 2 * code + 96 * n_and + 80 * words + 12288 * n_mul + (8ull << 20);
+}
+
 int binius_prover_phase_ms(const binius_prover* P, double* h_out5) {
   BGPU_ARG(P && h_out5, "NULL argument");
-  memcpy(h_out5, P->phase_ms, sizeof(P->phase_ms));
+  memcpy(h_out5, t_phase_ms, sizeof(t_phase_ms));
   return clear_error();
 }
 
@@ -131,7 +148,7 @@ int binius_prover_prove(const binius_prover* P, const void* d_witness,
   auto t0 = Clock::now();
   auto lap = [&](int phase) {
     const auto now = Clock::now();
-    P->phase_ms[phase] = std::chrono::duration<double, std::milli>(now - t0).count();
+    t_phase_ms[phase] = std::chrono::duration<double, std::milli>(now - t0).count();
     t0 = now;
   };
   // [phase] Witness Commit

@@ -1,0 +1,236 @@
+// Served / batched proving: a request queue over the prove entry.
+//
+// A queue owns `n_workers` host threads on one device, each with its own non-blocking CUDA
+// stream.  Requests (a prover, i.e. a constraint system with its parameters, and a witness) are
+// admitted in FIFO order while the sum of the admitted requests' workspace estimates
+// (binius_prover_workspace_bytes, plus the witness copy for host witnesses) stays within the
+// queue's HBM budget; an admitted request runs binius_prover_prove on its worker's stream with a
+// fresh transcript.  A proof is a chain of Fiat-Shamir rounds that synchronise with the host, so
+// requests proving at the same time fill each other's round trips with kernels, and the device
+// keeps every witness, codeword and tree resident until that request's proof is emitted.  Each
+// proof is exactly the proof of a lone call: no state is shared between requests.
+//
+// The reference has no serving layer (its CLI proves one statement per process,
+// prover/examples/src/cli.rs:455-509); this is the batching / serving wrapper around
+// Prover::prove (prover/prover/src/prove.rs:124-303).
+#include <string.h>
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "internal.h"
+#include "transcript.h"
+
+using namespace bgpu;
+
+namespace {
+
+typedef std::chrono::steady_clock Clock;
+
+struct Request {
+  uint64_t ticket = 0;
+  const binius_prover* prover = nullptr;
+  const void* witness = nullptr;
+  bool on_device = false;
+  uint64_t n_words = 0;
+  uint64_t bytes = 0;  // admission estimate
+  Clock::time_point submitted, started, finished;
+  bool done = false;
+  int status = BINIUS_OK;
+  std::string error;
+  std::vector<uint8_t> proof;
+};
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+}  // namespace
+
+struct binius_queue {
+  int device = 0;
+  uint64_t budget = 0, in_use = 0;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<std::shared_ptr<Request>> pending;
+  std::unordered_map<uint64_t, std::shared_ptr<Request>> requests;
+  std::vector<std::thread> workers;
+  bool stop = false;
+  uint64_t next_ticket = 1;
+  uint64_t completed = 0;
+
+  void worker_loop();
+};
+
+void binius_queue::worker_loop() {
+  cudaSetDevice(device);
+  set_blocking_waits(true);
+  cudaStream_t s = nullptr;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return;
+  for (;;) {
+    std::shared_ptr<Request> r;
+    {
+      std::unique_lock<std::mutex> lock(mu);
+      // FIFO admission: the head request waits until its workspace fits in the budget (a lone
+      // request is always admitted, so an oversized one cannot stall the queue forever)
+      cv_work.wait(lock, [&] {
+        return stop || (!pending.empty() &&
+                        (in_use == 0 || in_use + pending.front()->bytes <= budget));
+      });
+      if (pending.empty()) {
+        if (stop) break;
+        continue;
+      }
+      r = pending.front();
+      pending.pop_front();
+      in_use += r->bytes;
+      r->started = Clock::now();
+    }
+    int rc = BINIUS_OK;
+    std::string err;
+    std::vector<uint8_t> proof;
+    const void* d_w = r->witness;
+    void* owned = nullptr;
+    if (!r->on_device) {
+      cudaError_t e = cudaMallocAsync(&owned, 8 * r->n_words, s);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(owned, r->witness, 8 * r->n_words, cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) rc = cuda_error(e, "queue witness upload");
+      d_w = owned;
+    }
+    if (!rc) {
+      binius_transcript tr;
+      rc = binius_prover_prove(r->prover, d_w, &tr, s);
+      if (!rc) proof = tr.t.tape();
+    }
+    if (rc) err = binius_last_error();
+    if (owned) cudaFreeAsync(owned, s);
+    stream_wait(s);
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      in_use -= r->bytes;
+      r->finished = Clock::now();
+      r->status = rc;
+      r->error = err;
+      r->proof.swap(proof);
+      r->done = true;
+      completed++;
+    }
+    cv_done.notify_all();
+    cv_work.notify_all();
+  }
+  cudaStreamDestroy(s);
+}
+
+extern "C" {
+
+int binius_queue_create(int device, uint32_t n_workers, uint64_t hbm_budget_bytes,
+                        binius_queue** out) {
+  BGPU_ARG(out != nullptr, "NULL argument");
+  *out = nullptr;
+  BGPU_ARG(n_workers >= 1 && n_workers <= 256, "n_workers must be in [1, 256]");
+  BGPU_CUDA(cudaSetDevice(device));
+  if (int rc = configure_device_pool(device)) return rc;
+  binius_queue* q = new binius_queue();
+  q->device = device;
+  if (hbm_budget_bytes == 0) {
+    size_t free_b = 0, total_b = 0;
+    cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
+    if (e != cudaSuccess) {
+      delete q;
+      return cuda_error(e, "cudaMemGetInfo");
+    }
+    hbm_budget_bytes = (uint64_t)(0.9 * (double)free_b);
+  }
+  q->budget = hbm_budget_bytes;
+  for (uint32_t i = 0; i < n_workers; i++) q->workers.emplace_back([q] { q->worker_loop(); });
+  *out = q;
+  return clear_error();
+}
+
+int binius_queue_destroy(binius_queue* q) {
+  if (!q) return BINIUS_OK;
+  {
+    // requests not yet admitted are cancelled; admitted ones run to completion
+    std::lock_guard<std::mutex> lock(q->mu);
+    for (auto& r : q->pending) {
+      r->status = BINIUS_E_ARG;
+      r->error = "queue destroyed before the request was admitted";
+      r->done = true;
+    }
+    q->pending.clear();
+    q->stop = true;
+  }
+  q->cv_work.notify_all();
+  q->cv_done.notify_all();
+  for (auto& w : q->workers) w.join();
+  delete q;
+  return BINIUS_OK;
+}
+
+int binius_queue_submit(binius_queue* q, const binius_prover* prover, const void* witness,
+                        int witness_on_device, uint64_t* ticket) {
+  BGPU_ARG(q && prover && witness && ticket, "NULL argument");
+  auto r = std::make_shared<Request>();
+  r->prover = prover;
+  r->witness = witness;
+  r->on_device = witness_on_device != 0;
+  r->n_words = binius_prover_committed_words(prover);
+  r->bytes = binius_prover_workspace_bytes(prover) + (r->on_device ? 0 : 8 * r->n_words);
+  {
+    std::lock_guard<std::mutex> lock(q->mu);
+    BGPU_ARG(!q->stop, "queue is shutting down");
+    r->ticket = q->next_ticket++;
+    r->submitted = Clock::now();
+    q->pending.push_back(r);
+    q->requests[r->ticket] = r;
+    *ticket = r->ticket;
+  }
+  q->cv_work.notify_all();
+  return clear_error();
+}
+
+int binius_queue_poll(binius_queue* q, uint64_t ticket, int* done) {
+  BGPU_ARG(q && done, "NULL argument");
+  std::lock_guard<std::mutex> lock(q->mu);
+  auto it = q->requests.find(ticket);
+  BGPU_ARG(it != q->requests.end(), "unknown ticket");
+  *done = it->second->done ? 1 : 0;
+  return clear_error();
+}
+
+int binius_queue_wait(binius_queue* q, uint64_t ticket, void* h_proof, size_t cap, size_t* len,
+                      double* h_times3) {
+  BGPU_ARG(q && len, "NULL argument");
+  std::unique_lock<std::mutex> lock(q->mu);
+  auto it = q->requests.find(ticket);
+  BGPU_ARG(it != q->requests.end(), "unknown ticket");
+  std::shared_ptr<Request> r = it->second;
+  q->cv_done.wait(lock, [&] { return r->done; });
+  it = q->requests.find(ticket);  // the map may have rehashed while waiting
+  if (h_times3) {
+    h_times3[0] = ms_between(r->submitted, r->started);  // queued
+    h_times3[1] = ms_between(r->started, r->finished);   // proving
+    h_times3[2] = ms_between(r->submitted, r->finished); // total latency
+  }
+  *len = r->proof.size();
+  if (r->status) {
+    const int st = r->status;
+    const std::string msg = r->error;
+    q->requests.erase(it);
+    return set_error(st, msg);
+  }
+  BGPU_ARG(h_proof != nullptr && cap >= r->proof.size(), "proof buffer too small (len set)");
+  memcpy(h_proof, r->proof.data(), r->proof.size());
+  q->requests.erase(it);
+  return clear_error();
+}
+
+}  // extern "C"

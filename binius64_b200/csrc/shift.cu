@@ -303,7 +303,7 @@ int launched(const char* what, uint64_t n = 1) {
 
 int d2h_sync(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   BGPU_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
-  BGPU_CUDA(cudaStreamSynchronize(s));
+  BGPU_CUDA(stream_wait(s));
   return BINIUS_OK;
 }
 
@@ -399,7 +399,7 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
       BGPU_CUDA(cudaMemcpyAsync(host + 64, g, 256, cudaMemcpyDeviceToHost, s));
       BGPU_CUDA(cudaMemcpyAsync(host + 64 + 256, h, 256, cudaMemcpyDeviceToHost, s));
     }
-    BGPU_CUDA(cudaStreamSynchronize(s));
+    BGPU_CUDA(stream_wait(s));
     if (round == 0) sum = h128(host + 32);
     const hu128 y1 = h128(host), yinf = h128(host + 16);
     const hu128 c0 = sum ^ y1, c2 = yinf, c1 = y1 ^ c0 ^ c2;
@@ -490,7 +490,7 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
     uint8_t host[64 + 32];
     BGPU_CUDA(cudaMemcpyAsync(host, acc, 64, cudaMemcpyDeviceToHost, s));
     if (n_rem == 1) BGPU_CUDA(cudaMemcpyAsync(host + 64, W, 32, cudaMemcpyDeviceToHost, s));
-    BGPU_CUDA(cudaStreamSynchronize(s));
+    BGPU_CUDA(stream_wait(s));
     const hu128 y1 = h128(host), yinf = h128(host + 16);
     const hu128 s0 = shift_sum ^ y1, s2 = yinf, s1 = y1 ^ s0 ^ s2;
     hu128 iy0, iy1;

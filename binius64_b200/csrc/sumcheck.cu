@@ -223,8 +223,9 @@ int fold_b128_elems(const uint4* d_in, uint4* d_out, uint64_t n, const uint4* d_
   BGPU_CUDA(cudaMallocAsync(&tables, 16 * 16 * 256, s));
   build_fold_tables_kernel<<<16, 256, 0, s>>>(d_vec128, tables);
   const size_t smem = 16 * 256 * sizeof(uint4);
-  cudaError_t e =
-      cudaFuncSetAttribute(fold_elems_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = ensure_smem_limit(reinterpret_cast<const void*>(fold_elems_kernel), smem)
+                      ? cudaErrorInvalidValue
+                      : cudaSuccess;
   if (e == cudaSuccess) {
     fold_elems_kernel<<<grid_for(n, kThreads, 148 * 2), kThreads, smem, s>>>(d_in, d_out, n, tables);
     e = cudaGetLastError();

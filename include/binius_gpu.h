@@ -242,10 +242,39 @@ int binius_prover_destroy(binius_prover* prover);
 int binius_prover_info(const binius_prover* prover, uint32_t* h_out12);
 int binius_prover_prove(const binius_prover* prover, const void* d_witness,
                         binius_transcript* transcript, void* stream);
-/* Host wall-clock milliseconds of the last prove's phases (the spans of prove.rs:164-300):
+/* committed_total_len of the prover's constraint system (the witness length in words). */
+uint64_t binius_prover_committed_words(const binius_prover* prover);
+/* Upper-bound estimate of the device memory one proof allocates while it runs (admission of
+ * concurrent proofs); no reference counterpart. */
+uint64_t binius_prover_workspace_bytes(const binius_prover* prover);
+/* Host wall-clock milliseconds of the calling thread's last prove's phases (the spans of prove.rs:164-300):
  * witness commit, IntMul, BitAnd, shift reduction, PCS opening.  No counterpart in the reference
  * beyond its tracing spans. */
 int binius_prover_phase_ms(const binius_prover* prover, double* h_out5);
+
+/* ------------------------------------------------------------------------------------------
+ * Batched / served proving (no reference counterpart: the reference proves one statement per
+ * call of Prover::prove, prover/prover/src/prove.rs:124-303, and per process in its CLI,
+ * prover/examples/src/cli.rs:455-509).
+ * A queue runs n_workers proving threads on `device`, each with its own CUDA stream, and admits
+ * requests in FIFO order while the workspace estimates of the running requests fit in
+ * hbm_budget_bytes (0 = 90% of the free device memory at creation).  submit: `witness` holds the
+ * prover's committed_total_len words, on the device (witness_on_device = 1) or on the host; it
+ * must stay valid until wait returns.  wait blocks until the request is done, copies its proof
+ * (the finalized transcript of a fresh ProverTranscript) into h_proof and releases the ticket;
+ * with a too-small buffer it sets *len, returns BINIUS_E_ARG and keeps the result.  h_times3
+ * (optional): queued, proving and total milliseconds.  destroy finishes the admitted requests.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct binius_queue binius_queue;
+
+int binius_queue_create(int device, uint32_t n_workers, uint64_t hbm_budget_bytes,
+                        binius_queue** out);
+int binius_queue_destroy(binius_queue* queue);
+int binius_queue_submit(binius_queue* queue, const binius_prover* prover, const void* witness,
+                        int witness_on_device, uint64_t* ticket);
+int binius_queue_poll(binius_queue* queue, uint64_t ticket, int* done);
+int binius_queue_wait(binius_queue* queue, uint64_t ticket, void* h_proof, size_t cap,
+                      size_t* len, double* h_times3);
 
 /* ------------------------------------------------------------------------------------------
  * Integer multiplication reduction.
