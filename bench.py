@@ -94,6 +94,8 @@ def parse_args():
     ap.add_argument("--requests", type=int, default=256, help="batch / serve: proofs submitted")
     ap.add_argument("--workers", type=int, default=16, help="batch / serve: proving threads")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="prove workload: skip the batched-queue summary (profiling runs)")
     ap.add_argument("--log-words", type=int, default=None,
                     help="prove workload: log2 committed words (default 20)")
     ap.add_argument("--log-len", type=int, default=None,
@@ -464,7 +466,7 @@ def run_prove(args, rank, world, local):
                              "oracle (C++ restatement of the reference prover, PCLMULQDQ, "
                              "std::thread over all host cores); the Rust reference needs cargo"}
         batched = None
-        if world == 1:
+        if world == 1 and not args.no_batch:
             batched, _ = batch_summary(torch, bg, local, 128, 16)
         ph = {k: statistics.median(p[k] for p in phases) for k in phases[0]}
         line = {
