@@ -614,9 +614,9 @@ class ProveQueue:
         return bool(d.value)
 
     def wait(self, ticket: int):
-        """Returns (proof bytes, {"queued_ms", "prove_ms", "latency_ms"})."""
+        """Returns (proof bytes, {"queued_ms", "prove_ms", "latency_ms", "phase_ms"})."""
         n = ctypes.c_size_t(0)
-        times = (ctypes.c_double * 3)()
+        times = (ctypes.c_double * 8)()
         cap = 1 << 21
         while True:
             buf = (ctypes.c_uint8 * cap)()
@@ -628,7 +628,9 @@ class ProveQueue:
         self._keep.pop(ticket, None)
         check(rc)
         return bytes(buf)[: n.value], {"queued_ms": times[0], "prove_ms": times[1],
-                                       "latency_ms": times[2]}
+                                       "latency_ms": times[2],
+                                       "phase_ms": dict(zip(("commit", "intmul", "bitand", "shift",
+                                                             "pcs"), list(times)[3:]))}
 
     def close(self):
         h = getattr(self, "_h", None)

@@ -349,13 +349,16 @@ __global__ void __launch_bounds__(256)
 }
 
 // Fold the three columns (length size) by r, truncate eq (length size/2 -> size/4) and evaluate
-// the next round.  Thread j owns folded positions j, j + size/4 and eq position j.
-__global__ void __launch_bounds__(256)
+// the next round.  Thread j owns folded positions j, j + size/4 and eq position j.  With TAB the
+// six products by r go through r's byte table (gf_mul_table).
+template <bool TAB>
+__global__ void __launch_bounds__(256, 2)
     and_mle_fold_eval_kernel(uint4* __restrict__ fa, uint4* __restrict__ fb, uint4* __restrict__ fc,
                              uint4* __restrict__ eq, uint64_t size, uint4 r,
-                             uint32_t* __restrict__ out) {
+                             const uint4* __restrict__ tab, uint32_t* __restrict__ out) {
   const uint64_t h = size >> 1, q = size >> 2;
   u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
+  auto mul_r = [&](uint4 x) { return TAB ? gf_mul_table(tab, x) : gf_mul(r, x); };
   for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < q;
        j += (uint64_t)gridDim.x * blockDim.x) {
     uint4 f[3][2];
@@ -364,8 +367,8 @@ __global__ void __launch_bounds__(256)
     for (int c = 0; c < 3; c++) {
       uint4* col = cols[c];
       const uint4 lo0 = col[j], hi0 = col[h + j], lo1 = col[q + j], hi1 = col[h + q + j];
-      f[c][0] = gf_add(lo0, gf_mul(r, gf_add(hi0, lo0)));
-      f[c][1] = gf_add(lo1, gf_mul(r, gf_add(hi1, lo1)));
+      f[c][0] = gf_add(lo0, mul_r(gf_add(hi0, lo0)));
+      f[c][1] = gf_add(lo1, mul_r(gf_add(hi1, lo1)));
       col[j] = f[c][0];
       col[q + j] = f[c][1];
     }
@@ -375,15 +378,6 @@ __global__ void __launch_bounds__(256)
     xor_into(sinf, clmul128(e, gf_mul(gf_add(f[0][0], f[0][1]), gf_add(f[1][0], f[1][1]))));
   }
   reduce2_atomic(reduce256(s1), reduce256(sinf), out);
-}
-
-// Final fold of length-2 columns by r: out[c] = lo + r (hi - lo).
-__global__ void and_fold_final_kernel(const uint4* __restrict__ fa, const uint4* __restrict__ fb,
-                                      const uint4* __restrict__ fc, uint4 r, uint4* __restrict__ out) {
-  const int c = threadIdx.x;
-  if (c >= 3) return;
-  const uint4* col = c == 0 ? fa : (c == 1 ? fb : fc);
-  out[c] = gf_add(col[0], gf_mul(r, gf_add(col[1], col[0])));
 }
 
 struct DevTablesHolder {
@@ -470,7 +464,10 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
   BGPU_CUDA(cudaMallocAsync(&eq_big, 16 * n_chunks, s));
   BGPU_CUDA(cudaMallocAsync(&fcols, 16 * 3 * N, s));
   BGPU_CUDA(cudaMallocAsync(&eq, 16 * (N / 2), s));
-  BGPU_CUDA(cudaMallocAsync(&d_acc, 64 * 16, s));
+  // 64 univariate slots, then one (y_1, y_inf) slot pair per MLE-check round, zeroed once
+  BGPU_CUDA(cudaMallocAsync(&d_acc, 16 * (64 + 2 * (log_n + 1)), s));
+  uint4* mul_tab = nullptr;
+  BGPU_CUDA(cudaMallocAsync(&mul_tab, 16 * kMulTableEntries, s));
   int rc = BINIUS_OK;
   do {
     if ((rc = eval_operands(cs->and_ops, d_witness, words, s))) break;
@@ -481,7 +478,7 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
     // univariate round
     PhiPowers pw;
     for (int i = 0; i < 8; i++) pw.p[i] = to_uint4(C.phi[1u << i]);
-    cudaError_t e = cudaMemsetAsync(d_acc, 0, 64 * 16, s);
+    cudaError_t e = cudaMemsetAsync(d_acc, 0, 16 * (64 + 2 * (log_n + 1)), s);
     if (e != cudaSuccess) { rc = cuda_error(e, "memset"); break; }
     univariate_round_kernel<<<148, kUniThreads, kUniSmem, s>>>(words, words + N, words + 2 * N,
                                                               eq_big, n_chunks, tab, pw, d_acc);
@@ -489,9 +486,7 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
     if (e != cudaSuccess) { rc = cuda_error(e, "univariate_round_kernel"); break; }
     count_launch();
     uint8_t msg[64 * 16];
-    e = cudaMemcpyAsync(msg, d_acc, sizeof(msg), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = stream_wait(s);
-    if (e != cudaSuccess) { rc = cuda_error(e, "univariate message"); break; }
+    if ((rc = read_sync(msg, d_acc, sizeof(msg), s))) break;
     t.message(msg, sizeof(msg));
     uint8_t zb[16];
     t.sample_elem(zb);
@@ -521,26 +516,37 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
     uint4* fc = fcols + 2 * N;
     std::vector<u128h> challenges;
     uint8_t rb[16];
+    uint8_t last[96];  // (lo, hi) of a, b, c before the final fold
     for (uint32_t n_rem = log_n; n_rem > 0; n_rem--) {
-      e = cudaMemsetAsync(d_acc, 0, 32, s);
-      if (e != cudaSuccess) { rc = cuda_error(e, "memset"); break; }
+      uint32_t* acc = d_acc + 4 * (64 + 2 * (log_n - n_rem));
       const uint64_t size = 1ull << n_rem;
       if (n_rem == log_n) {
         and_mle_eval_kernel<<<grid_for(size / 2, 256), 256, 0, s>>>(fa, fb, fc, eq, size / 2,
-                                                                    d_acc);
+                                                                    acc);
       } else {
         uint4 r4;
         memcpy(&r4, rb, 16);
-        and_mle_fold_eval_kernel<<<grid_for(size / 2, 256), 256, 0, s>>>(fa, fb, fc, eq,
-                                                                         size * 2, r4, d_acc);
+        if (size * 2 >= kMulTableMinSize) {
+          if ((rc = build_mul_table(rb, mul_tab, s))) break;
+          and_mle_fold_eval_kernel<true><<<grid_for(size / 2, 256), 256, 0, s>>>(
+              fa, fb, fc, eq, size * 2, r4, mul_tab, acc);
+        } else {
+          and_mle_fold_eval_kernel<false><<<grid_for(size / 2, 256), 256, 0, s>>>(
+              fa, fb, fc, eq, size * 2, r4, nullptr, acc);
+        }
       }
       e = cudaGetLastError();
       if (e != cudaSuccess) { rc = cuda_error(e, "AND MLE-check round"); break; }
       count_launch();
       uint8_t ys[32];
-      e = cudaMemcpyAsync(ys, d_acc, 32, cudaMemcpyDeviceToHost, s);
-      if (e == cudaSuccess) e = stream_wait(s);
-      if (e != cudaSuccess) { rc = cuda_error(e, "round sums"); break; }
+      StagedReads rd(s);
+      if ((rc = rd.add(ys, acc, 32))) break;
+      if (n_rem == 1) {  // the last round: the length-2 columns are read with its sums
+        for (int c = 0; c < 3; c++)
+          if ((rc = rd.add(last + 32 * c, fcols + (uint64_t)c * N, 32))) break;
+        if (rc) break;
+      }
+      if ((rc = rd.wait())) break;
       const u128h y1 = from_bytes16(ys), yinf = from_bytes16(ys + 16);
       const u128h alpha = point[n_rem - 1];
       // RoundEvals2::interpolate_eq (round_evals.rs:80-86)
@@ -556,17 +562,14 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
       sum = c0 ^ host_gf_mul(c1, r) ^ host_gf_mul(c2, host_gf_mul(r, r));
     }
     if (rc) break;
-    uint4 r4;
-    memcpy(&r4, rb, 16);
-    uint4* d_ev = reinterpret_cast<uint4*>(d_acc);
-    and_fold_final_kernel<<<1, 32, 0, s>>>(fa, fb, fc, r4, d_ev);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) { rc = cuda_error(e, "and_fold_final_kernel"); break; }
-    count_launch();
+    // final fold of the length-2 columns by the last challenge: lo + r (hi - lo)
     uint8_t ev[48];
-    e = cudaMemcpyAsync(ev, d_ev, 48, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = stream_wait(s);
-    if (e != cudaSuccess) { rc = cuda_error(e, "final evals"); break; }
+    const u128h r_last = from_bytes16(rb);
+    for (int c = 0; c < 3; c++) {
+      const u128h lo = from_bytes16(last + 32 * c), hi = from_bytes16(last + 32 * c + 16);
+      const u128h v = lo ^ host_gf_mul(r_last, hi ^ lo);
+      memcpy(ev + 16 * c, &v, 16);
+    }
     t.message(ev, 48);
     res.a_eval = from_bytes16(ev);
     res.b_eval = from_bytes16(ev + 16);
@@ -578,6 +581,7 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
   cudaFreeAsync(fcols, s);
   cudaFreeAsync(eq, s);
   cudaFreeAsync(d_acc, s);
+  cudaFreeAsync(mul_tab, s);
   return rc;
 }
 

@@ -1,8 +1,11 @@
 // Error reporting, version and host field helpers of libbinius_gpu.
 #include <stdio.h>
+#include <string.h>
 
 #include <atomic>
+#include <chrono>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #if defined(__PCLMUL__) && defined(__SSE4_1__)
@@ -99,12 +102,92 @@ int ensure_smem_limit(const void* func, size_t bytes) {
   return BINIUS_OK;
 }
 
-// Waits for the work queued on `s`.  Threads that set blocking waits (the proving workers of a
-// queue, many of which wait at once) sleep on a blocking-sync event instead of spinning in
-// cudaStreamSynchronize, leaving the host cores to the threads that have work.
+// ---- staged device-to-host reads
+
+namespace {
+struct PinnedStage {
+  uint8_t* buf = nullptr;
+  ~PinnedStage() {
+    if (buf) cudaFreeHost(buf);
+  }
+};
+thread_local PinnedStage t_stage;
+// The stage is allocated once per thread and never resized: cudaFreeHost and cudaHostAlloc
+// synchronise with the device, which would stall every concurrent proof.  Reads that do not fit
+// go straight to pageable memory.
+constexpr size_t kStageBytes = 4u << 20;
+}  // namespace
+
+StagedReads::StagedReads(cudaStream_t s) : s_(s) {}
+
+int StagedReads::reserve(size_t bytes, uint8_t** at) {
+  *at = nullptr;
+  const size_t need = used_ + ((bytes + 15) & ~size_t(15));
+  if (need > kStageBytes) return BINIUS_OK;  // the caller copies directly
+  if (!t_stage.buf)
+    BGPU_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&t_stage.buf), kStageBytes,
+                            cudaHostAllocDefault));
+  *at = t_stage.buf + used_;
+  used_ = need;
+  return BINIUS_OK;
+}
+
+int StagedReads::add(void* dst, const void* src, size_t bytes) {
+  uint8_t* at = nullptr;
+  if (int rc = reserve(bytes, &at)) return rc;
+  if (!at) {  // larger than the stage: a pageable copy, complete when the call returns
+    BGPU_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s_));
+    return BINIUS_OK;
+  }
+  BGPU_CUDA(cudaMemcpyAsync(at, src, bytes, cudaMemcpyDeviceToHost, s_));
+  pending_.push_back({dst, at, bytes, 0, 0, 0});
+  return BINIUS_OK;
+}
+
+int StagedReads::add2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width,
+                       size_t height) {
+  uint8_t* at = nullptr;
+  if (int rc = reserve(width * height, &at)) return rc;
+  if (!at) {
+    BGPU_CUDA(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height, cudaMemcpyDeviceToHost,
+                                s_));
+    return BINIUS_OK;
+  }
+  BGPU_CUDA(cudaMemcpy2DAsync(at, width, src, spitch, width, height, cudaMemcpyDeviceToHost, s_));
+  pending_.push_back({dst, at, width, dpitch, width, height});
+  return BINIUS_OK;
+}
+
+int StagedReads::wait() {
+  BGPU_CUDA(stream_wait(s_));
+  for (const auto& p : pending_) {
+    if (p.height == 0) {
+      memcpy(p.dst, p.stage, p.bytes);
+    } else {
+      for (size_t r = 0; r < p.height; r++)
+        memcpy(static_cast<uint8_t*>(p.dst) + r * p.dpitch, p.stage + r * p.width, p.width);
+    }
+  }
+  pending_.clear();
+  used_ = 0;
+  return BINIUS_OK;
+}
+
+int read_sync(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  StagedReads r(s);
+  if (int rc = r.add(dst, src, bytes)) return rc;
+  return r.wait();
+}
+
+// Waits for the work queued on `s`.  Threads that enable shared waits (the proving workers of a
+// queue, many of which wait at once) poll an event and yield the core between polls for a short
+// while -- most round trips of a proof end within it -- and then sleep on the event (blocking
+// sync): polling without end from many threads contends for the driver, and sleeping at once
+// would add the driver's wake-up latency to each of a proof's ~100 round trips.
 namespace {
 thread_local bool t_blocking_wait = false;
 thread_local cudaEvent_t t_wait_event = nullptr;
+constexpr double kPollMicros = 100.0;
 }  // namespace
 
 void set_blocking_waits(bool on) { t_blocking_wait = on; }
@@ -117,7 +200,16 @@ cudaError_t stream_wait(cudaStream_t s) {
     if (e != cudaSuccess) return e;
   }
   cudaError_t e = cudaEventRecord(t_wait_event, s);
-  return e == cudaSuccess ? cudaEventSynchronize(t_wait_event) : e;
+  if (e != cudaSuccess) return e;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    e = cudaEventQuery(t_wait_event);
+    if (e != cudaErrorNotReady) return e;
+    if (std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count() >
+        kPollMicros)
+      return cudaEventSynchronize(t_wait_event);
+    std::this_thread::yield();
+  }
 }
 
 // The stream-ordered allocator of `device` keeps freed blocks cached (release threshold = max)

@@ -290,8 +290,7 @@ int binius_fri_commit_interleaved(const binius_ntt* ntt, const void* d_msg, uint
   if (int rc = bgpu::merkle_commit(d_codeword, log_leaves, log_batch, d_nodes, s)) return rc;
   if (h_root) {
     const uint8_t* root = static_cast<const uint8_t*>(d_nodes) + 32 * ((2ull << log_leaves) - 2);
-    BGPU_CUDA(cudaMemcpyAsync(h_root, root, 32, cudaMemcpyDeviceToHost, s));
-    BGPU_CUDA(stream_wait(s));
+    if (int rc = bgpu::read_sync(h_root, root, 32, s)) return rc;
   }
   return clear_error();
 }

@@ -106,4 +106,27 @@ __device__ __forceinline__ bool gf_is_zero(uint4 a) { return (a.x | a.y | a.z | 
 __device__ __forceinline__ uint4 gf_zero() { return make_uint4(0u, 0u, 0u, 0u); }
 __device__ __forceinline__ uint4 gf_one() { return make_uint4(1u, 0u, 0u, 0u); }
 
+// Multiplication by a fixed element r through a byte table (the fold challenge of a sumcheck
+// round multiplies every element by the same r): tab[j * 256 + v] = r * (v x^(8j)), so
+// r * x = XOR over the 16 bytes x_j of x of tab[j * 256 + x_j] -- 16 cached loads and XORs, no
+// reduction.  The 64 KiB table is read through the read-only data cache.
+constexpr int kMulTableEntries = 16 * 256;
+
+__device__ __forceinline__ uint4 gf_mul_x(uint4 a) {
+  const uint32_t carry = a.w >> 31;
+  uint4 r = make_uint4(a.x << 1, (a.y << 1) | (a.x >> 31), (a.z << 1) | (a.y >> 31),
+                       (a.w << 1) | (a.z >> 31));
+  r.x ^= carry * 0x87u;  // x^128 = x^7 + x^2 + x + 1
+  return r;
+}
+
+__device__ __forceinline__ uint4 gf_mul_table(const uint4* __restrict__ tab, uint4 x) {
+  uint4 acc = gf_zero();
+  const uint32_t w[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+  for (int j = 0; j < 16; j++)
+    gf_add_into(acc, __ldg(tab + j * 256 + ((w[j >> 2] >> (8 * (j & 3))) & 255u)));
+  return acc;
+}
+
 }  // namespace bgpu

@@ -4,6 +4,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/binius_gpu.h"
 
@@ -31,10 +32,36 @@ int cuda_error(cudaError_t e, const char* what);
     if (!(cond)) return ::bgpu::set_error(BINIUS_E_ARG, msg); \
   } while (0)
 
-// Waits for the work queued on s: cudaStreamSynchronize, or a blocking-sync event wait on threads
-// that called set_blocking_waits(true).
+// Waits for the work queued on s: cudaStreamSynchronize, or (threads that called
+// set_blocking_waits(true)) an event poll that yields the core, then a blocking-sync wait.
 cudaError_t stream_wait(cudaStream_t s);
 void set_blocking_waits(bool on);
+
+// Device-to-host reads through a per-thread pinned staging buffer: add() queues copies on the
+// stream, wait() synchronises once and scatters them to their destinations.  Small reads from
+// pinned memory are truly asynchronous, unlike copies into pageable memory.
+class StagedReads {
+ public:
+  explicit StagedReads(cudaStream_t s);
+  int add(void* dst, const void* src, size_t bytes);
+  int add2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width,
+            size_t height);
+  int wait();
+
+ private:
+  struct Pending {
+    void* dst;
+    uint8_t* stage;
+    size_t bytes, dpitch, width, height;
+  };
+  int reserve(size_t bytes, uint8_t** at);
+  cudaStream_t s_;
+  size_t used_ = 0;
+  std::vector<Pending> pending_;
+};
+
+// One staged read: copy, synchronise, return.
+int read_sync(void* dst, const void* src, size_t bytes, cudaStream_t s);
 
 // Sets the dynamic shared memory limit of a kernel once per device (see common.cu).
 int ensure_smem_limit(const void* func, size_t bytes);

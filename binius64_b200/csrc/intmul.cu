@@ -96,19 +96,42 @@ __global__ void bit_columns_kernel(const uint64_t* __restrict__ e, uint64_t n, u
 
 // ---------------------------------------------------------------- sumcheck kernels
 
-// Pair p of `set` (multilinears 2p, 2p + 1 of length 2 * half): out[2p] += sum eq[i] a1 b1,
-// out[2p + 1] += sum eq[i] (a0 + a1)(b0 + b1).  Grid: (chunks, pairs).
+__device__ __forceinline__ uint4 fold1(uint4 lo, uint4 hi, uint4 r) {
+  return gf_add(lo, gf_mul(r, gf_add(hi, lo)));
+}
+
+// One round of the bivariate products on pair p of `set` (multilinears 2p and 2p + 1, current
+// length L): out[8p..] += (sum eq[i] a1 b1, sum eq[i] (a0 + a1)(b0 + b1)) over i < L/2.  With
+// `fold`, both multilinears first shrink from 2L to L by r in place (fold_highest_var_inplace);
+// thread i owns positions i and i + L/2, so the fold and the round need one pass.  Grid: (chunks,
+// pairs).
 __global__ void __launch_bounds__(kT)
-    biv_round_kernel(const uint4* __restrict__ set, uint64_t half, uint64_t stride,
-                     const uint4* __restrict__ eq, uint32_t* __restrict__ out) {
+    biv_round_kernel(uint4* __restrict__ set, uint64_t L, uint64_t stride,
+                     const uint4* __restrict__ eq, int fold, uint4 r, uint32_t* __restrict__ out) {
   const uint32_t p = blockIdx.y;
-  const uint4* a = set + 2 * p * stride;
-  const uint4* b = a + stride;
+  uint4* a = set + 2 * p * stride;
+  uint4* b = a + stride;
+  const uint64_t h = L >> 1;
   u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < half;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < h;
        i += (uint64_t)gridDim.x * blockDim.x) {
+    uint4 a0, a1, b0, b1;
+    if (fold) {
+      a0 = fold1(a[i], a[L + i], r);
+      a1 = fold1(a[h + i], a[L + h + i], r);
+      b0 = fold1(b[i], b[L + i], r);
+      b1 = fold1(b[h + i], b[L + h + i], r);
+      a[i] = a0;
+      a[h + i] = a1;
+      b[i] = b0;
+      b[h + i] = b1;
+    } else {
+      a0 = a[i];
+      a1 = a[h + i];
+      b0 = b[i];
+      b1 = b[h + i];
+    }
     const uint4 e = eq[i];
-    const uint4 a0 = a[i], a1 = a[half + i], b0 = b[i], b1 = b[half + i];
     xor_into(s1, clmul128(e, gf_mul(a1, b1)));
     xor_into(sinf, clmul128(e, gf_mul(gf_add(a0, a1), gf_add(b0, b1))));
   }
@@ -116,34 +139,56 @@ __global__ void __launch_bounds__(kT)
   block_xor_reduce<2>(v, out + 8 * p);
 }
 
-// Column k of `set`: out[k] += sum eq[i] col_k[half + i].  Grid: (chunks, columns).
+// Column k of `set` (current length L): out[4k..] += sum eq[i] col_k[L/2 + i], with the same
+// optional fused fold.  Grid: (chunks, columns).
 __global__ void __launch_bounds__(kT)
-    lin_round_kernel(const uint4* __restrict__ set, uint64_t half, uint64_t stride,
-                     const uint4* __restrict__ eq, uint32_t* __restrict__ out) {
+    lin_round_kernel(uint4* __restrict__ set, uint64_t L, uint64_t stride,
+                     const uint4* __restrict__ eq, int fold, uint4 r, uint32_t* __restrict__ out) {
   const uint32_t k = blockIdx.y;
-  const uint4* c = set + k * stride + half;
+  uint4* c = set + k * stride;
+  const uint64_t h = L >> 1;
   u256 s1 = {0, 0, 0, 0};
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < half;
-       i += (uint64_t)gridDim.x * blockDim.x)
-    xor_into(s1, clmul128(eq[i], c[i]));
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < h;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint4 c1;
+    if (fold) {
+      c[i] = fold1(c[i], c[L + i], r);
+      c1 = fold1(c[h + i], c[L + h + i], r);
+      c[h + i] = c1;
+    } else {
+      c1 = c[h + i];
+    }
+    xor_into(s1, clmul128(eq[i], c1));
+  }
   uint4 v[1] = {reduce256(s1)};
   block_xor_reduce<1>(v, out + 4 * k);
 }
 
-// Selector claim k (its own eq_k): out[2k] += sum eq_k[i] (s1 (sel1 + 1) + 1),
-// out[2k + 1] += sum eq_k[i] (s0 + s1)(sel0 + sel1).  Grid: (chunks, claims).
+// Selector claim k with its own eq_k: out[8k..] += (sum eq_k[i] (s1 (sel1 + 1) + 1),
+// sum eq_k[i] (s0 + s1)(sel0 + sel1)); `sel` (shared by all claims) is folded beforehand, the
+// column s_k is folded here when `fold` is set.  Grid: (chunks, claims).
 __global__ void __launch_bounds__(kT)
-    selector_round_kernel(const uint4* __restrict__ sel, const uint4* __restrict__ cols,
-                          uint64_t half, uint64_t stride, const uint4* __restrict__ eqs,
-                          uint64_t eq_stride, uint32_t* __restrict__ out) {
+    selector_round_kernel(const uint4* __restrict__ sel, uint4* __restrict__ cols, uint64_t L,
+                          uint64_t stride, const uint4* __restrict__ eqs, uint64_t eq_stride,
+                          int fold, uint4 r, uint32_t* __restrict__ out) {
   const uint32_t k = blockIdx.y;
-  const uint4* s = cols + k * stride;
+  uint4* s = cols + k * stride;
   const uint4* eq = eqs + k * eq_stride;
+  const uint64_t h = L >> 1;
   u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < half;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < h;
        i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint4 e = eq[i];
-    const uint4 sel0 = sel[i], sel1 = sel[half + i], c0 = s[i], c1 = s[half + i];
+    uint4 c0, c1;
+    if (fold) {
+      c0 = fold1(s[i], s[L + i], r);
+      c1 = fold1(s[h + i], s[L + h + i], r);
+      s[i] = c0;
+      s[h + i] = c1;
+    } else {
+      c0 = s[i];
+      c1 = s[h + i];
+    }
+    const uint4 e = eq[i], sel0 = sel[i], sel1 = sel[h + i];
     xor_into(s1, clmul128(e, gf_add(gf_mul(c1, gf_add(sel1, gf_one())), gf_one())));
     xor_into(sinf, clmul128(e, gf_mul(gf_add(c0, c1), gf_add(sel0, sel1))));
   }
@@ -159,36 +204,27 @@ __global__ void fold_set_kernel(uint4* __restrict__ set, uint32_t count, uint64_
        t += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t k = t / half, i = t - k * half;
     uint4* m = set + k * stride;
-    const uint4 lo = m[i], hi = m[half + i];
-    m[i] = gf_add(lo, gf_mul(r, gf_add(hi, lo)));
+    m[i] = fold1(m[i], m[half + i], r);
   }
 }
 
-// eq over one coordinate fewer: eq_k[i] += eq_k[i + half] (eq_ind_truncate_low_inplace).
-__global__ void eq_truncate_kernel(uint4* __restrict__ eqs, uint32_t count, uint64_t half,
-                                   uint64_t stride) {
-  const uint64_t total = (uint64_t)count * half;
+// The eq tensors of `count` points over their first m' coordinates for every m' <= m (the Gruen
+// eq factor of each round, gruen32.rs; in place of eq_ind_truncate_low_inplace per round):
+// out[k * stride + (2^m' - 1) + i] = prod_{j < m'} (bit_j(i) ? p_kj : 1 + p_kj).
+__global__ void eq_levels_kernel(const uint4* __restrict__ points, uint32_t count, uint32_t m,
+                                 uint4* __restrict__ out, uint64_t stride) {
+  const uint64_t per = (2ull << m) - 1, total = (uint64_t)count * per;
   for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total;
        t += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t k = t / half, i = t - k * half;
-    gf_add_into(eqs[k * stride + i], eqs[k * stride + half + i]);
-  }
-}
-
-// count eq tensors over m coordinates each: out[k * stride + i] = prod_j (bit_j(i) ? p : 1 + p)
-// with p = points[k * m + j].
-__global__ void eq_many_kernel(const uint4* __restrict__ points, uint32_t count, uint32_t m,
-                               uint4* __restrict__ out, uint64_t stride) {
-  const uint64_t len = 1ull << m, total = (uint64_t)count * len;
-  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total;
-       t += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t k = t / len, i = t - k * len;
+    const uint64_t k = t / per, rr = t - k * per;
+    const uint32_t lvl = 63 - __clzll(rr + 1);
+    const uint64_t i = rr + 1 - (1ull << lvl);
     uint4 acc = gf_one();
-    for (uint32_t j = 0; j < m; j++) {
+    for (uint32_t j = 0; j < lvl; j++) {
       const uint4 p = points[k * m + j];
       acc = gf_mul(acc, ((i >> j) & 1) ? p : gf_add(p, gf_one()));
     }
-    out[k * stride + i] = acc;
+    out[k * stride + rr] = acc;
   }
 }
 
@@ -345,18 +381,13 @@ class IntMulDevice {
     count_launch(launches);
     return BINIUS_OK;
   }
-  int sync_read(void* dst, const void* src, size_t bytes) {
-    BGPU_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s_));
-    BGPU_CUDA(stream_wait(s_));
-    return BINIUS_OK;
-  }
+  int sync_read(void* dst, const void* src, size_t bytes) { return read_sync(dst, src, bytes, s_); }
   // values [0] of `count` multilinears with stride `stride`
   int read_first(const uint4* set, uint32_t count, uint64_t stride, std::vector<hu128>& out) {
     out.resize(count);
-    BGPU_CUDA(cudaMemcpy2DAsync(out.data(), 16, set, 16 * stride, 16, count,
-                                cudaMemcpyDeviceToHost, s_));
-    BGPU_CUDA(stream_wait(s_));
-    return BINIUS_OK;
+    StagedReads rd(s_);
+    if (int rc = rd.add2d(out.data(), 16, set, 16 * stride, 16, count)) return rc;
+    return rd.wait();
   }
   int eq_single(const std::vector<hu128>& point, uint32_t m, uint4* out) {
     std::vector<uint4> p(m);
@@ -368,20 +399,43 @@ class IntMulDevice {
     fold_set_kernel<<<blocks_for((uint64_t)count * half), kT, 0, s_>>>(set, count, half, N_, u4(r));
     return check("fold_set_kernel");
   }
-  int truncate(uint4* eqs, uint32_t count, uint64_t half) {
-    if (half == 0) return BINIUS_OK;
-    eq_truncate_kernel<<<blocks_for((uint64_t)count * half), kT, 0, s_>>>(eqs, count, half, N_);
-    return check("eq_truncate_kernel");
-  }
-  int biv_round(const uint4* set, uint32_t pairs, uint64_t half, const uint4* eq, uint32_t* out) {
-    dim3 grid(blocks_for(half, 148 * 2), pairs);
-    biv_round_kernel<<<grid, kT, 0, s_>>>(set, half, N_, eq, out);
+  // Fused round launches on multilinears of current length L (fold from 2L first when `fold`).
+  int biv_round(uint4* set, uint32_t pairs, uint64_t L, const uint4* eq, bool fold, hu128 r,
+                uint32_t* out) {
+    dim3 grid(blocks_for(L / 2, 148 * 2), pairs);
+    biv_round_kernel<<<grid, kT, 0, s_>>>(set, L, N_, eq, fold ? 1 : 0, u4(r), out);
     return check("biv_round_kernel");
   }
-  int lin_round(const uint4* set, uint32_t cols, uint64_t half, const uint4* eq, uint32_t* out) {
-    dim3 grid(blocks_for(half, 148 * 2), cols);
-    lin_round_kernel<<<grid, kT, 0, s_>>>(set, half, N_, eq, out);
+  int lin_round(uint4* set, uint32_t cols, uint64_t L, const uint4* eq, bool fold, hu128 r,
+                uint32_t* out) {
+    dim3 grid(blocks_for(L / 2, 148 * 2), cols);
+    lin_round_kernel<<<grid, kT, 0, s_>>>(set, L, N_, eq, fold ? 1 : 0, u4(r), out);
     return check("lin_round_kernel");
+  }
+  // eq levels of the given points over their first m' <= m coordinates (stride N_ per point).
+  int eq_levels(const std::vector<const std::vector<hu128>*>& points, uint32_t m, uint4* out) {
+    const uint32_t count = (uint32_t)points.size();
+    uint4* d_pts = nullptr;
+    if (m > 0) {
+      std::vector<uint4> h;
+      for (auto* pt : points)
+        for (uint32_t j = 0; j < m; j++) h.push_back(u4((*pt)[j]));
+      if (int rc = alloc(&d_pts, h.size())) return rc;
+      BGPU_CUDA(cudaMemcpyAsync(d_pts, h.data(), 16 * h.size(), cudaMemcpyHostToDevice, s_));
+    }
+    eq_levels_kernel<<<blocks_for((uint64_t)count << (m + 1)), kT, 0, s_>>>(d_pts, count, m, out, N_);
+    return check("eq_levels_kernel");
+  }
+  static const uint4* level(const uint4* eqs, uint32_t lvl) { return eqs + ((1ull << lvl) - 1); }
+  // queue the read of entries 0 and 1 of `count` multilinears (the last round's pre-fold pairs)
+  int copy_pairs(StagedReads& rd, const uint4* set, uint32_t count, hu128* dst) {
+    return rd.add2d(dst, 32, set, 16 * N_, 32, count);
+  }
+  static std::vector<hu128> fold_pairs(const std::vector<hu128>& pairs, hu128 r) {
+    std::vector<hu128> out(pairs.size() / 2);
+    for (size_t m = 0; m < out.size(); m++)
+      out[m] = pairs[2 * m] ^ host_gf_mul(r, pairs[2 * m + 1] ^ pairs[2 * m]);
+    return out;
   }
   // One GKR layer: decorated BivariateProductMultiMlecheckProver over `pairs` pairs of `set`,
   // batched alone and its evaluations written (prove.rs:207-243, 297-330).
@@ -401,34 +455,44 @@ int IntMulDevice::layer(uint4* set, uint32_t pairs, std::vector<hu128>& point,
                         std::vector<hu128>& claims) {
   const uint32_t n = (uint32_t)point.size();
   const hu128 beta = sample(t_);
-  GruenState g{point, n};
-  if (n > 0)
-    if (int rc = eq_single(point, n - 1, eq_)) return rc;
-  std::vector<hu128> sums = claims, ch;
-  std::vector<uint8_t> host(32ull * pairs);
-  for (uint32_t round = 0; round < n; round++) {
-    const uint64_t half = 1ull << (g.n_rem - 1);
-    BGPU_CUDA(cudaMemsetAsync(acc_, 0, 32ull * pairs, s_));
-    if (int rc = biv_round(set, pairs, half, eq_, acc_)) return rc;
-    if (int rc = sync_read(host.data(), acc_, 32ull * pairs)) return rc;
-    const hu128 alpha = g.alpha();
-    std::vector<Poly> primes, all;
-    for (uint32_t p = 0; p < pairs; p++) {
-      primes.push_back(interp2(sums[p], h128(&host[32 * p]), h128(&host[32 * p + 16]), alpha));
-      all.push_back(by_eq(primes.back(), alpha, g.prefix));
-    }
-    write_batched(t_, all, beta);
-    const hu128 r = sample(t_);
-    ch.push_back(r);
-    for (uint32_t p = 0; p < pairs; p++) sums[p] = eval_poly(primes[p], r);
-    g.fold(r);
-    if (int rc = fold(set, 2 * pairs, half, r)) return rc;
-    if (int rc = truncate(eq_, 1, half / 2)) return rc;
-  }
   std::vector<hu128> evals;
-  if (int rc = read_first(set, 2 * pairs, N_, evals)) return rc;
+  if (n == 0) {
+    if (int rc = read_first(set, 2 * pairs, N_, evals)) return rc;
+  } else {
+    GruenState g{point, n};
+    if (int rc = eq_levels({&point}, n - 1, eq_)) return rc;
+    uint32_t* acc = nullptr;
+    if (int rc = alloc(&acc, 2ull * pairs * n)) return rc;
+    BGPU_CUDA(cudaMemsetAsync(acc, 0, 32ull * pairs * n, s_));
+    std::vector<hu128> sums = claims, ch, last(4 * pairs);
+    std::vector<uint8_t> host(32ull * pairs);
+    hu128 r = 0;
+    for (uint32_t t = 0; t < n; t++) {
+      uint32_t* out = acc + 8ull * pairs * t;
+      if (int rc = biv_round(set, pairs, 1ull << (n - t), level(eq_, n - t - 1), t > 0, r, out))
+        return rc;
+      StagedReads rd(s_);
+      if (int rc = rd.add(host.data(), out, host.size())) return rc;
+      if (t + 1 == n)
+        if (int rc = copy_pairs(rd, set, 2 * pairs, last.data())) return rc;
+      if (int rc = rd.wait()) return rc;
+      const hu128 alpha = g.alpha();
+      std::vector<Poly> primes, all;
+      for (uint32_t p = 0; p < pairs; p++) {
+        primes.push_back(interp2(sums[p], h128(&host[32 * p]), h128(&host[32 * p + 16]), alpha));
+        all.push_back(by_eq(primes.back(), alpha, g.prefix));
+      }
+      write_batched(t_, all, beta);
+      r = sample(t_);
+      ch.push_back(r);
+      for (uint32_t p = 0; p < pairs; p++) sums[p] = eval_poly(primes[p], r);
+      g.fold(r);
+    }
+    evals = fold_pairs(last, r);
+    point.assign(ch.rbegin(), ch.rend());
+  }
   write_elems(t_, evals);
-  point.assign(ch.rbegin(), ch.rend());
+  if (n == 0) point.clear();
   claims = evals;
   return BINIUS_OK;
 }
@@ -449,12 +513,13 @@ int IntMulDevice::run_single(uint4* acl, uint4* btree, uint4* bcols, uint4* lo0,
   if (int rc = check("dot_kernel")) return rc;
   std::vector<hu128> hacl(kAcl), hb(kB), hcols(64);
   hu128 c_root = 0, lo_bit = 0;
-  BGPU_CUDA(cudaMemcpyAsync(hacl.data(), acl, 16 * kAcl, cudaMemcpyDeviceToHost, s_));
-  BGPU_CUDA(cudaMemcpyAsync(hb.data(), btree, 16 * kB, cudaMemcpyDeviceToHost, s_));
-  BGPU_CUDA(cudaMemcpyAsync(hcols.data(), bcols, 16 * 64, cudaMemcpyDeviceToHost, s_));
-  BGPU_CUDA(cudaMemcpyAsync(&c_root, acc_, 16, cudaMemcpyDeviceToHost, s_));
-  BGPU_CUDA(cudaMemcpyAsync(&lo_bit, lo0, 16, cudaMemcpyDeviceToHost, s_));
-  BGPU_CUDA(stream_wait(s_));
+  StagedReads rd(s_);
+  if (int rc = rd.add(hacl.data(), acl, 16 * kAcl)) return rc;
+  if (int rc = rd.add(hb.data(), btree, 16 * kB)) return rc;
+  if (int rc = rd.add(hcols.data(), bcols, 16 * 64)) return rc;
+  if (int rc = rd.add(&c_root, acc_, 16)) return rc;
+  if (int rc = rd.add(&lo_bit, lo0, 16)) return rc;
+  if (int rc = rd.wait()) return rc;
   auto acl_layer = [&](int k) { return hacl.begin() + 3 * ((1 << k) - 1); };
   auto b_layer = [&](int k) { return hb.begin() + ((1 << k) - 1); };
   write_elems(t_, {hb[0], c_root});
@@ -562,17 +627,10 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
   {
     bit_columns_kernel<<<blocks_for(64 * N), kT, 0, s_>>>(d_b, N, 0, 64, bcols, N);
     if (int rc = check("bit_columns_kernel")) return rc;
-    if (n_ > 0) {
-      std::vector<uint4> pts;
-      for (int i = 0; i < 64; i++)
-        for (uint32_t j = 0; j + 1 < n_; j++) pts.push_back(u4(tw_points[i][j]));
-      uint4* d_pts = nullptr;
-      if (int rc = alloc(&d_pts, pts.size())) return rc;
-      BGPU_CUDA(cudaMemcpyAsync(d_pts, pts.data(), 16 * pts.size(), cudaMemcpyHostToDevice, s_));
-      eq_many_kernel<<<blocks_for(64ull << (n_ - 1)), kT, 0, s_>>>(d_pts, 64, n_ - 1, sel_eqs, N);
-      if (int rc = check("eq_many_kernel")) return rc;
-      if (int rc = eq_single(point0, n_ - 1, eq_)) return rc;
-    }
+    std::vector<const std::vector<hu128>*> tw_ptrs;
+    for (int i = 0; i < 64; i++) tw_ptrs.push_back(&tw_points[i]);
+    if (int rc = eq_levels(tw_ptrs, n_ - 1, sel_eqs)) return rc;
+    if (int rc = eq_levels({&point0}, n_ - 1, eq_)) return rc;
     std::vector<GruenState> gs;
     for (int i = 0; i < 64; i++) gs.push_back(GruenState{tw_points[i], n_});
     GruenState gc{point0, n_};
@@ -580,16 +638,30 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
     uint4* croot = acl_layer(0) + N;
     hu128 c_sum = c_eval;
     const hu128 beta = sample(t_);
-    std::vector<uint8_t> host(16 * (128 + 2));
-    std::vector<hu128> ch;
-    for (uint32_t round = 0; round < n_; round++) {
-      const uint64_t half = 1ull << (n_ - round - 1);
-      BGPU_CUDA(cudaMemsetAsync(acc, 0, 16 * 130, s_));
-      dim3 grid(blocks_for(half, 148 * 2), 64);
-      selector_round_kernel<<<grid, kT, 0, s_>>>(sel, bcols, half, N, sel_eqs, N, acc);
+    uint32_t* acc3 = nullptr;
+    if (int rc = alloc(&acc3, 130ull * n_)) return rc;
+    BGPU_CUDA(cudaMemsetAsync(acc3, 0, 16ull * 130 * n_, s_));
+    std::vector<uint8_t> host(16 * 130);
+    std::vector<hu128> ch, last_cols(128), last_roots(6);
+    hu128 r = 0;
+    for (uint32_t t = 0; t < n_; t++) {
+      const uint64_t L = 1ull << (n_ - t);
+      uint32_t* out = acc3 + 4ull * 130 * t;
+      if (t > 0)
+        if (int rc = fold(sel, 1, L, r)) return rc;  // a_root, shared by the 64 claims
+      dim3 grid(blocks_for(L / 2, 148 * 2), 64);
+      selector_round_kernel<<<grid, kT, 0, s_>>>(sel, bcols, L, N, level(sel_eqs, n_ - t - 1), N,
+                                                 t > 0 ? 1 : 0, u4(r), out);
       if (int rc = check("selector_round_kernel")) return rc;
-      if (int rc = biv_round(croot, 1, half, eq_, acc + 4 * 128)) return rc;
-      if (int rc = sync_read(host.data(), acc, host.size())) return rc;
+      if (int rc = biv_round(croot, 1, L, level(eq_, n_ - t - 1), t > 0, r, out + 4 * 128))
+        return rc;
+      StagedReads rd(s_);
+      if (int rc = rd.add(host.data(), out, host.size())) return rc;
+      if (t + 1 == n_) {
+        if (int rc = copy_pairs(rd, bcols, 64, last_cols.data())) return rc;
+        if (int rc = copy_pairs(rd, sel, 3, last_roots.data())) return rc;
+      }
+      if (int rc = rd.wait()) return rc;
       std::vector<Poly> primes, all;
       for (int i = 0; i < 64; i++) {
         const hu128 a = gs[i].alpha();
@@ -599,7 +671,7 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
       primes.push_back(interp2(c_sum, h128(&host[2048]), h128(&host[2048 + 16]), gc.alpha()));
       all.push_back(by_eq(primes.back(), gc.alpha(), gc.prefix));
       write_batched(t_, all, beta);
-      const hu128 r = sample(t_);
+      r = sample(t_);
       ch.push_back(r);
       for (int i = 0; i < 64; i++) {
         sel_sums[i] = eval_poly(primes[i], r);
@@ -607,14 +679,8 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
       }
       c_sum = eval_poly(primes[64], r);
       gc.fold(r);
-      if (int rc = fold(sel, 3, half, r)) return rc;  // a_root, c_lo_root, c_hi_root
-      if (int rc = fold(bcols, 64, half, r)) return rc;
-      if (int rc = truncate(sel_eqs, 64, half / 2)) return rc;
-      if (int rc = truncate(eq_, 1, half / 2)) return rc;
     }
-    std::vector<hu128> colv, roots;
-    if (int rc = read_first(bcols, 64, N, colv)) return rc;
-    if (int rc = read_first(sel, 3, N, roots)) return rc;
+    const std::vector<hu128> colv = fold_pairs(last_cols, r), roots = fold_pairs(last_roots, r);
     std::vector<hu128> sel_evals = colv;
     sel_evals.push_back(roots[0]);
     write_elems(t_, sel_evals);
@@ -648,26 +714,36 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
     if (int rc = sync_read(cb, acc, 16)) return rc;
     const hu128 c_lo_0_eval = h128(cb);
     t_.message(cb, 16);
-    if (n_ > 0) {
-      if (int rc = eq_single(pt, n_ - 1, eq_)) return rc;
-      if (int rc = eq_single(p3, n_ - 1, eq2_)) return rc;
-    }
+    if (int rc = eq_levels({&pt}, n_ - 1, eq_)) return rc;
+    if (int rc = eq_levels({&p3}, n_ - 1, eq2_)) return rc;
     GruenState gb{pt, n_}, gl{pt, n_}, gr{p3, n_};
     std::vector<hu128> biv_sums = evals;
     biv_sums.push_back(c_lo_0_eval);
     hu128 lo_sum = c_lo_0_eval;
     std::vector<hu128> b_sums = b_exp_evals;
     const hu128 beta = sample(t_);
-    const size_t nbytes = 16 * (2 * 97 + 1 + 64);
-    std::vector<uint8_t> host(nbytes);
-    std::vector<hu128> ch;
-    for (uint32_t round = 0; round < n_; round++) {
-      const uint64_t half = 1ull << (n_ - round - 1);
-      BGPU_CUDA(cudaMemsetAsync(acc, 0, nbytes, s_));
-      if (int rc = biv_round(leaves, 97, half, eq_, acc)) return rc;
-      if (int rc = lin_round(lo0, 1, half, eq_, acc + 4 * 194)) return rc;
-      if (int rc = lin_round(bcols, 64, half, eq2_, acc + 4 * 195)) return rc;
-      if (int rc = sync_read(host.data(), acc, nbytes)) return rc;
+    constexpr size_t kSlots = 2 * 97 + 1 + 64;
+    uint32_t* acc5 = nullptr;
+    if (int rc = alloc(&acc5, kSlots * n_)) return rc;
+    BGPU_CUDA(cudaMemsetAsync(acc5, 0, 16 * kSlots * n_, s_));
+    std::vector<uint8_t> host(16 * kSlots);
+    std::vector<hu128> ch, last_leaves(2 * 194), last_lo(2), last_b(2 * 64);
+    hu128 r = 0;
+    for (uint32_t t = 0; t < n_; t++) {
+      const uint64_t L = 1ull << (n_ - t);
+      uint32_t* out = acc5 + 4 * kSlots * t;
+      const bool f = t > 0;
+      if (int rc = biv_round(leaves, 97, L, level(eq_, n_ - t - 1), f, r, out)) return rc;
+      if (int rc = lin_round(lo0, 1, L, level(eq_, n_ - t - 1), f, r, out + 4 * 194)) return rc;
+      if (int rc = lin_round(bcols, 64, L, level(eq2_, n_ - t - 1), f, r, out + 4 * 195)) return rc;
+      StagedReads rd(s_);
+      if (int rc = rd.add(host.data(), out, host.size())) return rc;
+      if (t + 1 == n_) {
+        if (int rc = copy_pairs(rd, leaves, 194, last_leaves.data())) return rc;
+        if (int rc = copy_pairs(rd, lo0, 1, last_lo.data())) return rc;
+        if (int rc = copy_pairs(rd, bcols, 64, last_b.data())) return rc;
+      }
+      if (int rc = rd.wait()) return rc;
       std::vector<Poly> primes, all;
       for (int p = 0; p < 97; p++) {
         primes.push_back(interp2(biv_sums[p], h128(&host[32 * p]), h128(&host[32 * p + 16]), gb.alpha()));
@@ -680,7 +756,7 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
         all.push_back(by_eq(primes.back(), gr.alpha(), gr.prefix));
       }
       write_batched(t_, all, beta);
-      const hu128 r = sample(t_);
+      r = sample(t_);
       ch.push_back(r);
       for (int p = 0; p < 97; p++) biv_sums[p] = eval_poly(primes[p], r);
       lo_sum = eval_poly(primes[97], r);
@@ -688,16 +764,9 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
       gb.fold(r);
       gl.fold(r);
       gr.fold(r);
-      if (int rc = fold(leaves, 194, half, r)) return rc;
-      if (int rc = fold(lo0, 1, half, r)) return rc;
-      if (int rc = fold(bcols, 64, half, r)) return rc;
-      if (int rc = truncate(eq_, 1, half / 2)) return rc;
-      if (int rc = truncate(eq2_, 1, half / 2)) return rc;
     }
-    std::vector<hu128> biv, lo_ev, b_ev;
-    if (int rc = read_first(leaves, 194, N, biv)) return rc;
-    if (int rc = read_first(lo0, 1, N, lo_ev)) return rc;
-    if (int rc = read_first(bcols, 64, N, b_ev)) return rc;
+    const std::vector<hu128> biv = fold_pairs(last_leaves, r), lo_ev = fold_pairs(last_lo, r),
+                             b_ev = fold_pairs(last_b, r);
     write_elems(t_, biv);
     write_elems(t_, lo_ev);
     write_elems(t_, b_ev);

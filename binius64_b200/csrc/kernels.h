@@ -37,6 +37,10 @@ int bivariate_eval(const uint4* d_a, const uint4* d_b, uint64_t half, uint32_t* 
 int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[16],
                         uint32_t* d_out8, cudaStream_t s);
 int gather_segments(const GatherSegment* d_segs, uint32_t n, uint8_t* d_dst, cudaStream_t s);
+// d_tab (16 * 256 elements) = the byte table of multiplication by r (gf_mul_table).
+int build_mul_table(const uint8_t r[16], uint4* d_tab, cudaStream_t s);
+// Folds of at least this many elements multiply by the fold challenge through its byte table.
+constexpr uint64_t kMulTableMinSize = 1ull << 15;
 
 // Lagrange basis of the subspace {phi(t) : t < 2^dim} at x, phi the AES-to-GHASH embedding
 // (BinarySubspace::<AESTowerField8b>::with_dim(dim).isomorphic(), lagrange_evals).

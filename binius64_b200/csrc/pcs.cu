@@ -89,7 +89,8 @@ struct DevFri {
   }
 
   // FRIFoldProver::execute_fold_round (prover/prover/src/fri/fold.rs:117-175)
-  int execute(bool* committed, uint8_t root[32]) {
+  // The new tree's root is queued on `rd` (read with the round's sums); the caller waits.
+  int execute(bool* committed, uint8_t root[32], StagedReads& rd) {
     *committed = false;
     if (next_commit < 0 || (int64_t)curr_round != next_commit) return BINIUS_OK;
     const uint32_t n = (uint32_t)(unprocessed.size() / 16);
@@ -124,9 +125,7 @@ struct DevFri {
     trees.push_back(nodes);
     tree_log_leaves.push_back(log_leaves);
     if (int rc = merkle_commit(out, log_leaves, log_coset, nodes, s)) return rc;
-    BGPU_CUDA(cudaMemcpyAsync(root, nodes + 32 * ((2ull << log_leaves) - 2), 32,
-                              cudaMemcpyDeviceToHost, s));
-    BGPU_CUDA(stream_wait(s));
+    if (int rc = rd.add(root, nodes + 32 * ((2ull << log_leaves) - 2), 32)) return rc;
     next_commit = has_next ? next_commit + next_arity : -1;
     *committed = true;
     return BINIUS_OK;
@@ -146,15 +145,26 @@ struct DevFri {
     }
   }
 
-  // FRIFoldProver::finish_proof (fri/fold.rs:221-244) with FRIQueryProver (fri/query.rs:51-110)
+  // FRIFoldProver::finish_proof (fri/fold.rs:221-244) with FRIQueryProver (fri/query.rs:51-110).
+  // The terminal codeword and the optimal Merkle layers are decommitments (tape only, unseen by
+  // the challenger), so the query indices can be sampled first and every opened byte -- terminal
+  // codeword, layers, then per query the coset values and branches -- gathered in one pass and
+  // read back once, then appended in the reference's order.
   int finish(Transcript& t) {
+    std::vector<GatherSegment> segs;
+    uint64_t off = 0;
+    auto add_bulk = [&](const uint8_t* src, uint64_t bytes) {
+      for (uint64_t done = 0; done < bytes;) {  // segments of at most 1 MiB
+        const uint64_t n = bytes - done < (1ull << 20) ? bytes - done : (1ull << 20);
+        segs.push_back({src + done, off, (uint32_t)n, 0});
+        off += n;
+        done += n;
+      }
+    };
     {
-      const void* term = words.empty() ? C.d_codeword : words.back();
+      const uint8_t* term = static_cast<const uint8_t*>(words.empty() ? C.d_codeword : words.back());
       const uint32_t log_term = words.empty() ? C.log_len : word_log_len.back();
-      std::vector<uint8_t> h(16ull << log_term);
-      BGPU_CUDA(cudaMemcpyAsync(h.data(), term, h.size(), cudaMemcpyDeviceToHost, s));
-      BGPU_CUDA(stream_wait(s));
-      t.decommitment(h.data(), h.size());
+      add_bulk(term, 16ull << log_term);
     }
     const auto depths = P.optimal_depths();
     {
@@ -166,15 +176,9 @@ struct DevFri {
       }
       for (size_t i = 0; i < tr.size() && i < depths.size(); i++) {
         const uint32_t d = depths[i], L = tl[i];
-        std::vector<uint8_t> h(32ull << d);
-        const uint8_t* src = tr[i] + 32 * ((2ull << L) - 1 + 1 - (2ull << d));
-        BGPU_CUDA(cudaMemcpyAsync(h.data(), src, h.size(), cudaMemcpyDeviceToHost, s));
-        BGPU_CUDA(stream_wait(s));
-        t.decommitment(h.data(), h.size());
+        add_bulk(tr[i] + 32 * ((2ull << L) - 1 + 1 - (2ull << d)), 32ull << d);
       }
     }
-    std::vector<GatherSegment> segs;
-    uint64_t off = 0;
     const uint8_t* cw = static_cast<const uint8_t*>(C.d_codeword);
     for (uint32_t q = 0; q < P.n_queries; q++) {
       uint64_t index = t.sample_bits(P.rs_log_len());
@@ -203,10 +207,7 @@ struct DevFri {
                                       cudaMemcpyHostToDevice, s);
       if (e != cudaSuccess) { rc = cuda_error(e, "upload query segments"); break; }
       if ((rc = gather_segments(d_segs, (uint32_t)segs.size(), d_dst, s))) break;
-      e = cudaMemcpyAsync(h.data(), d_dst, off, cudaMemcpyDeviceToHost, s);
-      if (e != cudaSuccess) { rc = cuda_error(e, "download query openings"); break; }
-      e = stream_wait(s);
-      if (e != cudaSuccess) { rc = cuda_error(e, "query gather"); break; }
+      rc = read_sync(h.data(), d_dst, off, s);
     } while (0);
     cudaFreeAsync(d_segs, s);
     cudaFreeAsync(d_dst, s);
@@ -244,22 +245,28 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
       // s_hat_v = fold_1b_rows_for_b128(witness, suffix_tensor)
       if ((rc = fold_1b_rows(static_cast<const uint4*>(d_witness), b, N, d_small, s))) break;
       uint8_t s_hat_v[128 * 16];
-      cudaError_t e = cudaMemcpyAsync(s_hat_v, d_small, sizeof(s_hat_v), cudaMemcpyDeviceToHost, s);
-      if (e == cudaSuccess) e = stream_wait(s);
-      if (e != cudaSuccess) { rc = cuda_error(e, "ring switch fold"); break; }
+      if ((rc = read_sync(s_hat_v, d_small, sizeof(s_hat_v), s))) break;
       t.message(s_hat_v, sizeof(s_hat_v));
       u128h v[128], u[128];
       for (int k = 0; k < 128; k++) v[k] = to_u128(s_hat_v + 16 * k);
       transpose128(v, u);
       uint8_t r_dp[7 * 16];
       for (int i = 0; i < 7; i++) t.sample_elem(r_dp + 16 * i);
-      if ((rc = eq_tensor(reinterpret_cast<const uint4*>(r_dp), 7, eq_r, s))) break;
-      uint8_t h_eq[128 * 16];
-      e = cudaMemcpyAsync(h_eq, eq_r, sizeof(h_eq), cudaMemcpyDeviceToHost, s);
-      if (e == cudaSuccess) e = stream_wait(s);
-      if (e != cudaSuccess) { rc = cuda_error(e, "eq(r'')"); break; }
+      // eq(r'') (128 entries) on the host; the device copy feeds the element fold
+      u128h h_eq[128];
+      h_eq[0] = 1;
+      for (int i = 0; i < 7; i++) {
+        const u128h ri = to_u128(r_dp + 16 * i);
+        for (int k = 0; k < (1 << i); k++) {
+          const u128h hi = host_gf_mul(h_eq[k], ri);
+          h_eq[(1 << i) + k] = hi;
+          h_eq[k] ^= hi;
+        }
+      }
+      cudaError_t e = cudaMemcpyAsync(eq_r, h_eq, sizeof(h_eq), cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) { rc = cuda_error(e, "eq(r'') upload"); break; }
       u128h sum = 0;
-      for (int j = 0; j < 128; j++) sum ^= host_gf_mul(u[j], to_u128(h_eq + 16 * j));
+      for (int j = 0; j < 128; j++) sum ^= host_gf_mul(u[j], h_eq[j]);
       // rs_eq_ind = fold_b128_elems_inplace(suffix_tensor, eq(r'')) in place in b
       if ((rc = fold_b128_elems(b, b, N, eq_r, s))) break;
       e = cudaMemcpyAsync(a, d_witness, 16 * N, cudaMemcpyDeviceToDevice, s);
@@ -275,14 +282,14 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
           rc = bivariate_fold_eval(a, b, size * 2, r_prev, d_small, s);
         if (rc) break;
         uint8_t ys[32];
-        e = cudaMemcpyAsync(ys, d_small, 32, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = stream_wait(s);
-        if (e != cudaSuccess) { rc = cuda_error(e, "round sums"); break; }
-        const u128h y1 = to_u128(ys), yinf = to_u128(ys + 16);
-        const u128h c0 = sum ^ y1, c2 = yinf, c1 = y1 ^ c0 ^ c2;
         bool committed = false;
         uint8_t root[32];
-        if ((rc = fri.execute(&committed, root))) break;
+        StagedReads rd(s);
+        if ((rc = rd.add(ys, d_small, 32))) break;
+        if ((rc = fri.execute(&committed, root, rd))) break;
+        if ((rc = rd.wait())) break;
+        const u128h y1 = to_u128(ys), yinf = to_u128(ys + 16);
+        const u128h c0 = sum ^ y1, c2 = yinf, c1 = y1 ^ c0 ^ c2;
         uint8_t coeffs[32];
         from_u128(c0, coeffs);
         from_u128(c1, coeffs + 16);
@@ -296,7 +303,9 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
       if (rc) break;
       bool committed = false;
       uint8_t root[32];
-      if ((rc = fri.execute(&committed, root))) break;
+      StagedReads rd(s);
+      if ((rc = fri.execute(&committed, root, rd))) break;
+      if ((rc = rd.wait())) break;
       if (committed) t.message(root, 32);
       rc = fri.finish(t);
     } while (0);

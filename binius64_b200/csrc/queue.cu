@@ -43,6 +43,7 @@ struct Request {
   uint64_t bytes = 0;  // admission estimate
   Clock::time_point submitted, started, finished;
   bool done = false;
+  double phase_ms[5] = {0, 0, 0, 0, 0};
   int status = BINIUS_OK;
   std::string error;
   std::vector<uint8_t> proof;
@@ -105,10 +106,12 @@ void binius_queue::worker_loop() {
       if (e != cudaSuccess) rc = cuda_error(e, "queue witness upload");
       d_w = owned;
     }
+    double phases[5] = {0, 0, 0, 0, 0};
     if (!rc) {
       binius_transcript tr;
       rc = binius_prover_prove(r->prover, d_w, &tr, s);
       if (!rc) proof = tr.t.tape();
+      binius_prover_phase_ms(r->prover, phases);
     }
     if (rc) err = binius_last_error();
     if (owned) cudaFreeAsync(owned, s);
@@ -120,6 +123,7 @@ void binius_queue::worker_loop() {
       r->status = rc;
       r->error = err;
       r->proof.swap(proof);
+      memcpy(r->phase_ms, phases, sizeof(phases));
       r->done = true;
       completed++;
     }
@@ -150,6 +154,18 @@ int binius_queue_create(int device, uint32_t n_workers, uint64_t hbm_budget_byte
     hbm_budget_bytes = (uint64_t)(0.9 * (double)free_b);
   }
   q->budget = hbm_budget_bytes;
+  // Reserve pool capacity up front (allocate and release one block; the pool keeps it cached):
+  // proofs running side by side then carve their scratch from cached memory instead of growing
+  // the pool, which maps memory under the pool's lock while every other proof waits.
+  {
+    const uint64_t reserve = hbm_budget_bytes / 2 < (8ull << 30) ? hbm_budget_bytes / 2 : (8ull << 30);
+    void* p = nullptr;
+    if (reserve && cudaMallocAsync(&p, reserve, 0) == cudaSuccess) {
+      cudaFreeAsync(p, 0);
+      cudaStreamSynchronize(0);
+    }
+    cudaGetLastError();
+  }
   for (uint32_t i = 0; i < n_workers; i++) q->workers.emplace_back([q] { q->worker_loop(); });
   *out = q;
   return clear_error();
@@ -207,7 +223,7 @@ int binius_queue_poll(binius_queue* q, uint64_t ticket, int* done) {
 }
 
 int binius_queue_wait(binius_queue* q, uint64_t ticket, void* h_proof, size_t cap, size_t* len,
-                      double* h_times3) {
+                      double* h_times8) {
   BGPU_ARG(q && len, "NULL argument");
   std::unique_lock<std::mutex> lock(q->mu);
   auto it = q->requests.find(ticket);
@@ -215,10 +231,11 @@ int binius_queue_wait(binius_queue* q, uint64_t ticket, void* h_proof, size_t ca
   std::shared_ptr<Request> r = it->second;
   q->cv_done.wait(lock, [&] { return r->done; });
   it = q->requests.find(ticket);  // the map may have rehashed while waiting
-  if (h_times3) {
-    h_times3[0] = ms_between(r->submitted, r->started);  // queued
-    h_times3[1] = ms_between(r->started, r->finished);   // proving
-    h_times3[2] = ms_between(r->submitted, r->finished); // total latency
+  if (h_times8) {
+    h_times8[0] = ms_between(r->submitted, r->started);  // queued
+    h_times8[1] = ms_between(r->started, r->finished);   // proving
+    h_times8[2] = ms_between(r->submitted, r->finished); // total latency
+    memcpy(h_times8 + 3, r->phase_ms, sizeof(r->phase_ms));
   }
   *len = r->proof.size();
   if (r->status) {

@@ -301,11 +301,6 @@ int launched(const char* what, uint64_t n = 1) {
   return BINIUS_OK;
 }
 
-int d2h_sync(void* dst, const void* src, size_t bytes, cudaStream_t s) {
-  BGPU_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
-  BGPU_CUDA(stream_wait(s));
-  return BINIUS_OK;
-}
 
 }  // namespace
 
@@ -394,12 +389,13 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
     }
     uint8_t host[64 + 2 * 16 * 16];
     const bool last = round == 11;
-    BGPU_CUDA(cudaMemcpyAsync(host, acc, round == 0 ? 64 : 32, cudaMemcpyDeviceToHost, s));
+    StagedReads rd(s);
+    SHIFT_TRY(rd.add(host, acc, round == 0 ? 64 : 32));
     if (last) {
-      BGPU_CUDA(cudaMemcpyAsync(host + 64, g, 256, cudaMemcpyDeviceToHost, s));
-      BGPU_CUDA(cudaMemcpyAsync(host + 64 + 256, h, 256, cudaMemcpyDeviceToHost, s));
+      SHIFT_TRY(rd.add(host + 64, g, 256));
+      SHIFT_TRY(rd.add(host + 64 + 256, h, 256));
     }
-    BGPU_CUDA(stream_wait(s));
+    SHIFT_TRY(rd.wait());
     if (round == 0) sum = h128(host + 32);
     const hu128 y1 = h128(host), yinf = h128(host + 16);
     const hu128 c0 = sum ^ y1, c2 = yinf, c1 = y1 ^ c0 ^ c2;
@@ -458,7 +454,7 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
   };
   auto read2 = [&](hu128& o0, hu128& o1) -> int {
     uint8_t b[32];
-    SHIFT_TRY(d2h_sync(b, acc + 8, 32, s));
+    SHIFT_TRY(read_sync(b, acc + 8, 32, s));
     o0 = h128(b);
     o1 = h128(b + 16);
     return BINIUS_OK;
@@ -488,9 +484,10 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
       SHIFT_TRY(dot2(half, half, half));
     }
     uint8_t host[64 + 32];
-    BGPU_CUDA(cudaMemcpyAsync(host, acc, 64, cudaMemcpyDeviceToHost, s));
-    if (n_rem == 1) BGPU_CUDA(cudaMemcpyAsync(host + 64, W, 32, cudaMemcpyDeviceToHost, s));
-    BGPU_CUDA(stream_wait(s));
+    StagedReads rd(s);
+    SHIFT_TRY(rd.add(host, acc, 64));
+    if (n_rem == 1) SHIFT_TRY(rd.add(host + 64, W, 32));
+    SHIFT_TRY(rd.wait());
     const hu128 y1 = h128(host), yinf = h128(host + 16);
     const hu128 s0 = shift_sum ^ y1, s2 = yinf, s1 = y1 ^ s0 ^ s2;
     hu128 iy0, iy1;

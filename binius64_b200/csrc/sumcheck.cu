@@ -141,20 +141,23 @@ __global__ void __launch_bounds__(kThreads)
 
 // Folds (a, b) of length `size` by r in place (a[i] = a[i] + r (a[i + size/2] - a[i])) and
 // evaluates the next round on the folded length-size/2 arrays.  Thread j owns folded positions j
-// and j + size/4, so no two threads touch the same element.
+// and j + size/4, so no two threads touch the same element.  With TAB the four products by r go
+// through the byte table of r (gf_mul_table).
+template <bool TAB>
 __global__ void __launch_bounds__(kThreads)
     bivariate_fold_eval_kernel(uint4* __restrict__ a, uint4* __restrict__ b, uint64_t size, uint4 r,
-                               uint32_t* __restrict__ out) {
+                               const uint4* __restrict__ tab, uint32_t* __restrict__ out) {
   const uint64_t h = size >> 1, q = size >> 2;
   u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
+  auto mul_r = [&](uint4 x) { return TAB ? gf_mul_table(tab, x) : gf_mul(r, x); };
   for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < q;
        j += (uint64_t)gridDim.x * blockDim.x) {
     uint4 a_lo = a[j], a_hi = a[h + j], a_lo2 = a[q + j], a_hi2 = a[h + q + j];
     uint4 b_lo = b[j], b_hi = b[h + j], b_lo2 = b[q + j], b_hi2 = b[h + q + j];
-    uint4 fa0 = gf_add(a_lo, gf_mul(r, gf_add(a_hi, a_lo)));
-    uint4 fa1 = gf_add(a_lo2, gf_mul(r, gf_add(a_hi2, a_lo2)));
-    uint4 fb0 = gf_add(b_lo, gf_mul(r, gf_add(b_hi, b_lo)));
-    uint4 fb1 = gf_add(b_lo2, gf_mul(r, gf_add(b_hi2, b_lo2)));
+    uint4 fa0 = gf_add(a_lo, mul_r(gf_add(a_hi, a_lo)));
+    uint4 fa1 = gf_add(a_lo2, mul_r(gf_add(a_hi2, a_lo2)));
+    uint4 fb0 = gf_add(b_lo, mul_r(gf_add(b_hi, b_lo)));
+    uint4 fb1 = gf_add(b_lo2, mul_r(gf_add(b_hi2, b_lo2)));
     a[j] = fa0;
     a[q + j] = fa1;
     b[j] = fb0;
@@ -164,6 +167,23 @@ __global__ void __launch_bounds__(kThreads)
   }
   uint4 v[2] = {reduce256(s1), reduce256(sinf)};
   block_xor_reduce<2>(v, out);
+}
+
+// tab[j * 256 + v] = r * (v x^(8j)): the byte table of gf_mul_table, one entry per thread from
+// r x^(8j) by repeated multiplication by x.
+__global__ void build_mul_table_kernel(uint4 r, uint4* __restrict__ tab) {
+  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (uint32_t)kMulTableEntries) return;
+  const uint32_t j = idx >> 8, v = idx & 255u;
+  uint4 base = r;
+  for (uint32_t k = 0; k < 8 * j; k++) base = gf_mul_x(base);
+  uint4 acc = gf_zero();
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    if ((v >> k) & 1u) gf_add_into(acc, base);
+    base = gf_mul_x(base);
+  }
+  tab[idx] = acc;
 }
 
 __global__ void gather_segments_kernel(const GatherSegment* __restrict__ segs, uint32_t n,
@@ -245,14 +265,37 @@ int bivariate_eval(const uint4* d_a, const uint4* d_b, uint64_t half, uint32_t* 
   return BINIUS_OK;
 }
 
+int build_mul_table(const uint8_t r[16], uint4* d_tab, cudaStream_t s) {
+  uint4 rv;
+  memcpy(&rv, r, 16);
+  build_mul_table_kernel<<<kMulTableEntries / 256, 256, 0, s>>>(rv, d_tab);
+  BGPU_LAUNCH_CHECK("build_mul_table_kernel");
+  count_launch();
+  return BINIUS_OK;
+}
+
 int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[16],
                         uint32_t* d_out8, cudaStream_t s) {
   if (size < 4) return set_error(BINIUS_E_ARG, "bivariate_fold_eval needs size >= 4");
   uint4 rv;
   memcpy(&rv, r, 16);
   BGPU_CUDA(cudaMemsetAsync(d_out8, 0, 32, s));
-  bivariate_fold_eval_kernel<<<grid_for(size / 4, kThreads), kThreads, 0, s>>>(d_a, d_b, size, rv,
-                                                                            d_out8);
+  const unsigned grid = grid_for(size / 4, kThreads);
+  if (size >= kMulTableMinSize) {
+    // large rounds: the four products by r per thread go through r's byte table
+    uint4* tab = nullptr;
+    BGPU_CUDA(cudaMallocAsync(&tab, 16 * kMulTableEntries, s));
+    int rc = build_mul_table(r, tab, s);
+    if (!rc) {
+      bivariate_fold_eval_kernel<true><<<grid, kThreads, 0, s>>>(d_a, d_b, size, rv, tab, d_out8);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) rc = cuda_error(e, "bivariate_fold_eval_kernel");
+      else count_launch();
+    }
+    cudaFreeAsync(tab, s);
+    return rc;
+  }
+  bivariate_fold_eval_kernel<false><<<grid, kThreads, 0, s>>>(d_a, d_b, size, rv, nullptr, d_out8);
   BGPU_LAUNCH_CHECK("bivariate_fold_eval_kernel");
   count_launch();
   return BINIUS_OK;

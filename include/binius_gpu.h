@@ -262,8 +262,10 @@ int binius_prover_phase_ms(const binius_prover* prover, double* h_out5);
  * prover's committed_total_len words, on the device (witness_on_device = 1) or on the host; it
  * must stay valid until wait returns.  wait blocks until the request is done, copies its proof
  * (the finalized transcript of a fresh ProverTranscript) into h_proof and releases the ticket;
- * with a too-small buffer it sets *len, returns BINIUS_E_ARG and keeps the result.  h_times3
- * (optional): queued, proving and total milliseconds.  destroy finishes the admitted requests.
+ * with a too-small buffer it sets *len, returns BINIUS_E_ARG and keeps the result.  h_times8
+ * (optional): queued, proving and total milliseconds, then the proof's phase milliseconds
+ * (commit, IntMul, AND, shift, PCS).  destroy cancels requests not yet admitted and finishes the
+ * admitted ones.
  * ------------------------------------------------------------------------------------------ */
 typedef struct binius_queue binius_queue;
 
@@ -274,7 +276,7 @@ int binius_queue_submit(binius_queue* queue, const binius_prover* prover, const 
                         int witness_on_device, uint64_t* ticket);
 int binius_queue_poll(binius_queue* queue, uint64_t ticket, int* done);
 int binius_queue_wait(binius_queue* queue, uint64_t ticket, void* h_proof, size_t cap,
-                      size_t* len, double* h_times3);
+                      size_t* len, double* h_times8);
 
 /* ------------------------------------------------------------------------------------------
  * Integer multiplication reduction.
