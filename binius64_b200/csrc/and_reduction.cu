@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "cs.h"
+#include "dev_transcript.cuh"
 #include "gf128.cuh"
 #include "internal.h"
 #include "kernels.h"
@@ -348,17 +349,21 @@ __global__ void __launch_bounds__(256)
   reduce2_atomic(reduce256(s1), reduce256(sinf), out);
 }
 
-// Fold the three columns (length size) by r, truncate eq (length size/2 -> size/4) and evaluate
-// the next round.  Thread j owns folded positions j, j + size/4 and eq position j.  With TAB the
-// six products by r go through r's byte table (gf_mul_table).
+// Fold the three columns (length size) by the previous round's challenge *r_ptr, truncate eq
+// (length size/2 -> size/4) and evaluate the next round.  Thread j owns folded positions j,
+// j + size/4 and eq position j.  With TAB the six products by r go through r's byte table
+// (gf_mul_table), which the previous round's finish kernel built.
 template <bool TAB>
 __global__ void __launch_bounds__(256, 2)
     and_mle_fold_eval_kernel(uint4* __restrict__ fa, uint4* __restrict__ fb, uint4* __restrict__ fc,
-                             uint4* __restrict__ eq, uint64_t size, uint4 r,
+                             uint4* __restrict__ eq, uint64_t size, const uint4* __restrict__ r_ptr,
                              const uint4* __restrict__ tab, uint32_t* __restrict__ out) {
   const uint64_t h = size >> 1, q = size >> 2;
   u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
-  auto mul_r = [&](uint4 x) { return TAB ? gf_mul_table(tab, x) : gf_mul(r, x); };
+  uint4 s1r = gf_zero(), sinfr = gf_zero();  // small rounds: reduced sums
+  const uint4 r = TAB ? gf_zero() : *r_ptr;
+  // small rounds (no table) run on few threads once: out-of-line multiplies keep the code compact
+  auto mul_r = [&](uint4 x) { return TAB ? gf_mul_table(tab, x) : gf_mul_nl(r, x); };
   for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < q;
        j += (uint64_t)gridDim.x * blockDim.x) {
     uint4 f[3][2];
@@ -374,10 +379,56 @@ __global__ void __launch_bounds__(256, 2)
     }
     const uint4 e = gf_add(eq[j], eq[q + j]);
     eq[j] = e;
-    xor_into(s1, clmul128(e, gf_add(gf_mul(f[0][1], f[1][1]), f[2][1])));
-    xor_into(sinf, clmul128(e, gf_mul(gf_add(f[0][0], f[0][1]), gf_add(f[1][0], f[1][1]))));
+    if constexpr (TAB) {
+      xor_into(s1, clmul128(e, gf_add(gf_mul(f[0][1], f[1][1]), f[2][1])));
+      xor_into(sinf, clmul128(e, gf_mul(gf_add(f[0][0], f[0][1]), gf_add(f[1][0], f[1][1]))));
+    } else {
+      gf_add_into(s1r, gf_mul_nl(e, gf_add(gf_mul_nl(f[0][1], f[1][1]), f[2][1])));
+      gf_add_into(sinfr, gf_mul_nl(e, gf_mul_nl(gf_add(f[0][0], f[0][1]),
+                                                gf_add(f[1][0], f[1][1]))));
+    }
   }
-  reduce2_atomic(reduce256(s1), reduce256(sinf), out);
+  if constexpr (TAB)
+    reduce2_atomic(reduce256(s1), reduce256(sinf), out);
+  else
+    reduce2_atomic(s1r, sinfr, out);
+}
+
+// Per-round constants of the MLE-check: the eq coordinate alpha the round binds and
+// 1 / (1 + alpha), both known before the loop starts.
+struct AndRoundConst {
+  uint4 alpha, inv_one_plus_alpha;
+};
+
+// The Fiat-Shamir step of one MLE-check round, on the device: the round's sums (y_1, y_inf) ->
+// the round polynomial by RoundEvals2::interpolate_eq (prover/prover/src/protocols/sumcheck/
+// round_evals.rs:80-86) -> the truncated proof (c_1, c_2) (mlecheck::RoundProof::truncate) ->
+// the challenge r -> the next claim c_0 + c_1 r + c_2 r^2.  Thread 0 runs the chain; with a
+// table pointer the whole block then builds r's byte table for the next fold.
+__global__ void __launch_bounds__(256)
+    and_round_finish_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
+                            const uint4* __restrict__ ys, const AndRoundConst* __restrict__ rc,
+                            uint4* __restrict__ claim, uint4* __restrict__ r_out,
+                            uint4* __restrict__ tab) {
+  __shared__ uint4 r_sh;
+  if (threadIdx.x == 0) {
+    DevTr st;
+    st.load(ts);
+    const uint4 y1 = ys[0], yinf = ys[1];
+    const uint4 y0 = gf_mul_1t(gf_add(*claim, gf_mul_1t(y1, rc->alpha)), rc->inv_one_plus_alpha);
+    const uint4 c0 = y0, c2 = yinf, c1 = gf_add(gf_add(y1, c0), c2);
+    const uint4 msg[2] = {c1, c2};
+    st.message_elems(tape, msg, 2);
+    const uint4 r = st.sample_elem();
+    *r_out = r;
+    *claim = gf_add(c0, gf_mul_1t(r, gf_add(c1, gf_mul_1t(c2, r))));
+    st.store(ts);
+    r_sh = r;
+  }
+  if (tab) {
+    __syncthreads();
+    dt_build_mul_table(r_sh, tab);
+  }
 }
 
 struct DevTablesHolder {
@@ -468,6 +519,9 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
   BGPU_CUDA(cudaMallocAsync(&d_acc, 16 * (64 + 2 * (log_n + 1)), s));
   uint4* mul_tab = nullptr;
   BGPU_CUDA(cudaMallocAsync(&mul_tab, 16 * kMulTableEntries, s));
+  // round constants (2 per round), the claim slot pair, the challenges
+  uint4* dev = nullptr;
+  BGPU_CUDA(cudaMallocAsync(&dev, 16 * (2 * (log_n + 1) + log_n), s));
   int rc = BINIUS_OK;
   do {
     if ((rc = eval_operands(cs->and_ops, d_witness, words, s))) break;
@@ -514,57 +568,61 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
     uint4* fa = fcols;
     uint4* fb = fcols + N;
     uint4* fc = fcols + 2 * N;
-    std::vector<u128h> challenges;
-    uint8_t rb[16];
-    uint8_t last[96];  // (lo, hi) of a, b, c before the final fold
+    // The round loop runs on the device transcript: per round one evaluation kernel and one
+    // finish kernel, no host round trip.  dev holds the claim, the round constants (rounds in
+    // order log_n .. 1) and the challenges.
+    std::vector<AndRoundConst> consts(log_n + 1);
     for (uint32_t n_rem = log_n; n_rem > 0; n_rem--) {
-      uint32_t* acc = d_acc + 4 * (64 + 2 * (log_n - n_rem));
+      const u128h alpha = point[n_rem - 1];
+      consts[log_n - n_rem] = {to_uint4(alpha), to_uint4(host_gf_inv(1 ^ alpha))};
+    }
+    consts[log_n].alpha = to_uint4(sum);  // the initial claim rides in the spare slot
+    AndRoundConst* d_consts = reinterpret_cast<AndRoundConst*>(dev);
+    uint4* d_claim = dev + 2 * log_n;
+    uint4* d_chal = dev + 2 * (log_n + 1);
+    e = cudaMemcpyAsync(d_consts, consts.data(), sizeof(AndRoundConst) * (log_n + 1),
+                        cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) { rc = cuda_error(e, "round constants"); break; }
+    DeviceTranscript dt;
+    if ((rc = dt.begin(t, s))) break;
+    for (uint32_t n_rem = log_n; n_rem > 0; n_rem--) {
+      const uint32_t k = log_n - n_rem;
+      uint32_t* acc = d_acc + 4 * (64 + 2 * k);
       const uint64_t size = 1ull << n_rem;
       if (n_rem == log_n) {
         and_mle_eval_kernel<<<grid_for(size / 2, 256), 256, 0, s>>>(fa, fb, fc, eq, size / 2,
                                                                     acc);
+      } else if (size * 2 >= kMulTableMinSize) {
+        and_mle_fold_eval_kernel<true><<<grid_for(size / 2, 256), 256, 0, s>>>(
+            fa, fb, fc, eq, size * 2, d_chal + k - 1, mul_tab, acc);
       } else {
-        uint4 r4;
-        memcpy(&r4, rb, 16);
-        if (size * 2 >= kMulTableMinSize) {
-          if ((rc = build_mul_table(rb, mul_tab, s))) break;
-          and_mle_fold_eval_kernel<true><<<grid_for(size / 2, 256), 256, 0, s>>>(
-              fa, fb, fc, eq, size * 2, r4, mul_tab, acc);
-        } else {
-          and_mle_fold_eval_kernel<false><<<grid_for(size / 2, 256), 256, 0, s>>>(
-              fa, fb, fc, eq, size * 2, r4, nullptr, acc);
-        }
+        and_mle_fold_eval_kernel<false><<<grid_for(size / 2, 256), 256, 0, s>>>(
+            fa, fb, fc, eq, size * 2, d_chal + k - 1, nullptr, acc);
       }
       e = cudaGetLastError();
       if (e != cudaSuccess) { rc = cuda_error(e, "AND MLE-check round"); break; }
-      count_launch();
-      uint8_t ys[32];
-      StagedReads rd(s);
-      if ((rc = rd.add(ys, acc, 32))) break;
-      if (n_rem == 1) {  // the last round: the length-2 columns are read with its sums
-        for (int c = 0; c < 3; c++)
-          if ((rc = rd.add(last + 32 * c, fcols + (uint64_t)c * N, 32))) break;
-        if (rc) break;
-      }
-      if ((rc = rd.wait())) break;
-      const u128h y1 = from_bytes16(ys), yinf = from_bytes16(ys + 16);
-      const u128h alpha = point[n_rem - 1];
-      // RoundEvals2::interpolate_eq (round_evals.rs:80-86)
-      const u128h y0 = host_gf_mul(sum ^ host_gf_mul(y1, alpha), host_gf_inv(1 ^ alpha));
-      const u128h c0 = y0, c2 = yinf, c1 = y1 ^ c0 ^ c2;
-      uint8_t rp[32];  // mlecheck::RoundProof::truncate drops c0
-      memcpy(rp, &c1, 16);
-      memcpy(rp + 16, &c2, 16);
-      t.message(rp, 32);
-      t.sample_elem(rb);
-      const u128h r = from_bytes16(rb);
-      challenges.push_back(r);
-      sum = c0 ^ host_gf_mul(c1, r) ^ host_gf_mul(c2, host_gf_mul(r, r));
+      // the next round folds by this round's challenge through a table when it is large
+      const bool next_tab = n_rem > 1 && size >= kMulTableMinSize;
+      and_round_finish_kernel<<<1, 256, 0, s>>>(dt.state(), dt.tape(),
+                                                reinterpret_cast<const uint4*>(acc),
+                                                d_consts + k, d_claim, d_chal + k,
+                                                next_tab ? mul_tab : nullptr);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) { rc = cuda_error(e, "and_round_finish_kernel"); break; }
+      count_launch(2);
     }
     if (rc) break;
+    // one read: the transcript, the challenges and the length-2 columns before the final fold
+    std::vector<u128h> challenges(log_n);
+    uint8_t last[96];  // (lo, hi) of a, b, c
+    StagedReads rd(s);
+    if ((rc = dt.read(rd, 32 * log_n))) break;
+    if ((rc = rd.add(challenges.data(), d_chal, 16 * log_n))) break;
+    for (int c = 0; c < 3 && !rc; c++) rc = rd.add(last + 32 * c, fcols + (uint64_t)c * N, 32);
+    if (rc || (rc = rd.wait()) || (rc = dt.finish(t))) break;
     // final fold of the length-2 columns by the last challenge: lo + r (hi - lo)
     uint8_t ev[48];
-    const u128h r_last = from_bytes16(rb);
+    const u128h r_last = challenges[log_n - 1];
     for (int c = 0; c < 3; c++) {
       const u128h lo = from_bytes16(last + 32 * c), hi = from_bytes16(last + 32 * c + 16);
       const u128h v = lo ^ host_gf_mul(r_last, hi ^ lo);
@@ -582,6 +640,7 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
   cudaFreeAsync(eq, s);
   cudaFreeAsync(d_acc, s);
   cudaFreeAsync(mul_tab, s);
+  cudaFreeAsync(dev, s);
   return rc;
 }
 

@@ -1,0 +1,323 @@
+// The Fiat-Shamir transcript on the device, for stretches of the protocol that run without the
+// host: the sumcheck round loops, whose every round is a kernel's sums -> round polynomial ->
+// proof message -> challenge -> the next kernel's fold.  Run on the host, each round costs a
+// device-to-host round trip; run here, a loop is a chain of launches the host enqueues at once.
+//
+// The state is the host Transcript's own (TranscriptState): the same HasherChallenger rules
+// (verifier/transcript/src/fiat_shamir/hasher_challenger.rs:14-200) over the same SHA-256 stream,
+// so a stretch may start and end anywhere in the protocol and the proof bytes do not change.  A
+// device stretch is advanced by ONE thread (the steps are a strict chain); message bytes go to a
+// device tape that the host appends to the proof when the stretch ends.
+#pragma once
+#include <stdint.h>
+
+#include <vector>
+
+#include "gf128.cuh"
+#include "internal.h"
+#include "sha256.cuh"
+#include "transcript.h"
+
+namespace bgpu {
+
+// Code run once by a single thread is fetched cold: straight-line code costs an instruction-cache
+// miss every few instructions, which for fully unrolled SHA-256 rounds and inlined GF(2^128)
+// multiplies comes to tens of microseconds per launch.  The scalar protocol steps therefore call
+// one out-of-line copy of each: the multiply (gf_mul_nl) and a compression whose 64 rounds run
+// as 4 passes of a 16-round body.
+__device__ __forceinline__ uint4 gf_mul_1t(uint4 a, uint4 b) { return gf_mul_nl(a, b); }
+
+static __device__ __noinline__ void sha256_compress_1t(uint32_t* st, const uint32_t* blk) {
+  uint32_t w[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) w[i] = blk[i];
+  uint32_t a = st[0], b = st[1], c = st[2], d = st[3], e = st[4], f = st[5], g = st[6], h = st[7];
+#pragma unroll 1
+  for (int t0 = 0; t0 < 64; t0 += 16) {
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      if (t0) {  // message schedule, w[j] = W[t - 16] becomes W[t]
+        const uint32_t w15 = w[(j + 1) & 15], w2 = w[(j + 14) & 15];
+        const uint32_t s0 = rotr32(w15, 7) ^ rotr32(w15, 18) ^ (w15 >> 3);
+        const uint32_t s1 = rotr32(w2, 17) ^ rotr32(w2, 19) ^ (w2 >> 10);
+        w[j] += s0 + w[(j + 9) & 15] + s1;
+      }
+      const uint32_t S1 = rotr32(e, 6) ^ rotr32(e, 11) ^ rotr32(e, 25);
+      const uint32_t ch = (e & f) ^ (~e & g);
+      const uint32_t t1 = h + S1 + ch + kSha256K[t0 + j] + w[j];
+      const uint32_t S0 = rotr32(a, 2) ^ rotr32(a, 13) ^ rotr32(a, 22);
+      const uint32_t mj = (a & b) ^ (a & c) ^ (b & c);
+      h = g;
+      g = f;
+      f = e;
+      e = d + t1;
+      d = c;
+      c = b;
+      b = a;
+      a = t1 + S0 + mj;
+    }
+  }
+  st[0] += a;
+  st[1] += b;
+  st[2] += c;
+  st[3] += d;
+  st[4] += e;
+  st[5] += f;
+  st[6] += g;
+  st[7] += h;
+}
+
+// The challenger held in registers by the thread that advances it.  The partial SHA-256 block
+// is kept as 16 big-endian words, zero past `len`, so absorbing a word is a shift/OR into the word
+// at a run-time position -- written as unrolled selects, which keeps every array in registers.
+// The stream is absorbed in 4-byte pieces (every message of the protocol is a whole number of
+// words); a piece may start at any byte offset.
+struct DevTr {
+  uint32_t h[8], w[16], len;  // chaining value, partial block, bytes in it
+  uint64_t total;             // bytes absorbed since the last reset
+  uint32_t sampling, index;   // mode and bytes of buf consumed
+  uint32_t buf[8];            // sample buffer, little-endian words
+  uint32_t tape_len, tape_cap, error;
+
+  __device__ __forceinline__ void load(const TranscriptState* g) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) h[i] = g->h[i];
+#pragma unroll
+    for (int i = 0; i < 16; i++) w[i] = g->w[i];
+    len = g->block_len & 63u;
+    total = g->total;
+    sampling = g->sampling;
+    index = g->index;
+#pragma unroll
+    for (int i = 0; i < 8; i++) buf[i] = g->buf[i];
+    tape_len = g->tape_len;
+    tape_cap = g->tape_cap;
+    error = g->error;
+  }
+
+  __device__ __forceinline__ void store(TranscriptState* g) const {
+#pragma unroll
+    for (int i = 0; i < 8; i++) g->h[i] = h[i];
+#pragma unroll
+    for (int i = 0; i < 16; i++) g->w[i] = w[i];
+    g->block_len = len;
+    g->total = total;
+    g->sampling = sampling;
+    g->index = index;
+#pragma unroll
+    for (int i = 0; i < 8; i++) g->buf[i] = buf[i];
+    g->tape_len = tape_len;
+    g->tape_cap = tape_cap;
+    g->error = error;
+  }
+
+  __device__ __forceinline__ void or_word(uint32_t k, uint32_t v) {
+#pragma unroll
+    for (uint32_t i = 0; i < 16; i++)
+      if (i == k) w[i] |= v;
+  }
+
+  __device__ __forceinline__ void compress_block() {
+    sha256_compress_1t(h, w);
+#pragma unroll
+    for (int i = 0; i < 16; i++) w[i] = 0;
+    len = 0;
+  }
+
+  // Absorbs 4 stream bytes given as a little-endian word (first byte lowest).
+  __device__ __forceinline__ void absorb_word(uint32_t le) {
+    const uint32_t be = bswap32(le);
+    const uint32_t off = len & 3u;
+    total += 4;
+    if (off == 0) {
+      or_word(len >> 2, be);
+      len += 4;
+      if (len == 64) compress_block();
+    } else {
+      or_word(len >> 2, be >> (8 * off));
+      len += 4 - off;
+      if (len == 64) compress_block();
+      or_word(len >> 2, be << (8 * (4 - off)));
+      len += off;
+    }
+  }
+
+  // Digest of the stream (FIPS 180-4 padding) as 8 big-endian words; the stream is unchanged.
+  __device__ __forceinline__ void digest(uint32_t d[8]) const {
+    uint32_t st[8], m[16];
+#pragma unroll
+    for (int i = 0; i < 8; i++) st[i] = h[i];
+#pragma unroll
+    for (int i = 0; i < 16; i++) m[i] = w[i];
+    const uint32_t pad = 0x80u << (24 - 8 * (len & 3u));
+#pragma unroll
+    for (uint32_t i = 0; i < 16; i++)
+      if (i == (len >> 2)) m[i] |= pad;
+    const uint64_t bits = total * 8;
+    if (len + 9 > 64) {
+      sha256_compress_1t(st, m);
+#pragma unroll
+      for (int i = 0; i < 16; i++) m[i] = 0;
+    }
+    m[14] = (uint32_t)(bits >> 32);
+    m[15] = (uint32_t)bits;
+    sha256_compress_1t(st, m);
+#pragma unroll
+    for (int i = 0; i < 8; i++) d[i] = st[i];
+  }
+
+  __device__ __forceinline__ void to_observer() {
+    if (sampling) {
+      const uint32_t idx = index;
+      absorb_word(idx);
+      absorb_word(0u);
+      sampling = 0;
+    }
+  }
+
+  // Appends n whole words (little-endian) to the tape; sets error instead when they do not fit.
+  __device__ __forceinline__ void tape_words(uint8_t* tape, const uint32_t* v, uint32_t n) {
+    if (tape_len + 4 * n > tape_cap) {
+      error = 1;
+      return;
+    }
+    if ((tape_len & 3u) == 0) {
+      uint32_t* t32 = reinterpret_cast<uint32_t*>(tape + tape_len);
+      for (uint32_t i = 0; i < n; i++) t32[i] = v[i];
+    } else {
+      for (uint32_t i = 0; i < 4 * n; i++) tape[tape_len + i] = (uint8_t)(v[i >> 2] >> (8 * (i & 3)));
+    }
+    tape_len += 4 * n;
+  }
+
+  // message(): n words to the tape and the challenger.
+  __device__ __forceinline__ void message_words(uint8_t* tape, const uint32_t* v, uint32_t n) {
+    tape_words(tape, v, n);
+    if (n) {
+      to_observer();
+      for (uint32_t i = 0; i < n; i++) absorb_word(v[i]);
+    }
+  }
+  __device__ __forceinline__ void message_elems(uint8_t* tape, const uint4* e, uint32_t n) {
+    message_words(tape, reinterpret_cast<const uint32_t*>(e), 4 * n);
+  }
+  __device__ __forceinline__ void observe_words(const uint32_t* v, uint32_t n) {
+    to_observer();
+    for (uint32_t i = 0; i < n; i++) absorb_word(v[i]);
+  }
+
+  // Refills the sample buffer from the digest of the stream, which restarts as that digest.
+  __device__ __forceinline__ void refill() {
+    uint32_t d[8];
+    digest(d);
+    const uint32_t iv[8] = {0x6a09e667u, 0xbb67ae85u, 0x3c6ef372u, 0xa54ff53au,
+                            0x510e527fu, 0x9b05688cu, 0x1f83d9abu, 0x5be0cd19u};
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      h[i] = iv[i];
+      w[i] = d[i];
+      w[8 + i] = 0;
+      buf[i] = bswap32(d[i]);
+    }
+    len = 32;
+    total = 32;
+    index = 0;
+  }
+
+  __device__ __forceinline__ uint32_t buf_byte(uint32_t i) const {
+    uint32_t v = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < 8; k++)
+      if (k == (i >> 2)) v = buf[k];
+    return (v >> (8 * (i & 3u))) & 255u;
+  }
+
+  __device__ __forceinline__ void begin_sampling() {
+    if (!sampling) {
+      sampling = 1;
+      index = 32;
+    }
+  }
+
+  // n bytes as little-endian words out[(n + 3) / 4].
+  __device__ __forceinline__ void sample_words(uint32_t* out, uint32_t n) {
+    begin_sampling();
+    for (uint32_t i = 0; i < (n + 3) / 4; i++) out[i] = 0;
+    for (uint32_t i = 0; i < n; i++) {
+      if (index == 32) refill();
+      out[i >> 2] |= buf_byte(index) << (8 * (i & 3u));
+      index++;
+    }
+  }
+
+  // A field element: 16 bytes read as a little-endian u128 (transcript.rs:398-407).  The common
+  // case (a word-aligned read within the buffer) is four register selects.
+  __device__ __forceinline__ uint4 sample_elem() {
+    begin_sampling();
+    if (index == 32) refill();
+    if ((index & 3u) == 0 && index + 16 <= 32) {
+      uint32_t o[4] = {0, 0, 0, 0};
+#pragma unroll
+      for (uint32_t k = 0; k < 8; k++)
+#pragma unroll
+        for (uint32_t j = 0; j < 4; j++)
+          if (k == (index >> 2) + j) o[j] = buf[k];
+      index += 16;
+      return make_uint4(o[0], o[1], o[2], o[3]);
+    }
+    uint32_t o[4];
+    sample_words(o, 16);
+    return make_uint4(o[0], o[1], o[2], o[3]);
+  }
+
+  // sample_bits_reader (fiat_shamir/sampling.rs:34-50): a little-endian u32, masked.
+  __device__ __forceinline__ uint32_t sample_bits(uint32_t bits) {
+    uint32_t v;
+    sample_words(&v, 4);
+    return bits >= 32 ? v : v & ((1u << bits) - 1);
+  }
+};
+
+// r's byte table for gf_mul_table, built by the calling block (any size) from r.
+__device__ __forceinline__ void dt_build_mul_table(uint4 r, uint4* __restrict__ tab) {
+  for (uint32_t v = threadIdx.x; v < 256; v += blockDim.x) {
+    uint4 base = r;
+    for (uint32_t j = 0; j < 16; j++) {
+      uint4 acc = gf_zero();
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        if ((v >> k) & 1u) gf_add_into(acc, base);
+        base = gf_mul_x(base);
+      }
+      tab[j * 256 + v] = acc;
+    }
+  }
+}
+
+// Host side of one device stretch.  begin() hands the host transcript's state to the device;
+// kernels advance state() and write to tape(); read() queues the copy-back of the state and of
+// the `tape_bytes` the stretch is known to write, and finish() (after the reads were waited on)
+// hands the state back to the host transcript with those bytes appended.
+class DeviceTranscript {
+ public:
+  static constexpr uint32_t kTapeCap = 1u << 16;
+
+  ~DeviceTranscript();
+  int begin(const Transcript& t, cudaStream_t s);
+  TranscriptState* state() const { return reinterpret_cast<TranscriptState*>(mem_); }
+  uint8_t* tape() const { return mem_ + kStateBytes; }
+  // message() of n_bytes (a multiple of 4, 4-byte aligned) that are in device memory.
+  int message_device(const void* d_bytes, uint32_t n_bytes, cudaStream_t s);
+  int read(StagedReads& rd, uint32_t tape_bytes);
+  int finish(Transcript& t);
+
+ private:
+  static constexpr size_t kStateBytes = 256;
+  cudaStream_t s_ = nullptr;
+  uint8_t* mem_ = nullptr;
+  uint32_t expect_ = 0;
+  TranscriptState host_state_;
+  std::vector<uint8_t> host_tape_;
+};
+
+}  // namespace bgpu

@@ -14,6 +14,7 @@
 
 #include "gf128.cuh"
 #include "internal.h"
+#include "kernels.h"
 
 using namespace bgpu;
 
@@ -38,16 +39,18 @@ unsigned grid_for(uint64_t n, unsigned threads) {
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, 148ull * 64));
 }
 
+// Challenges come from ch, or from device memory at dch when that is set (challenges sampled by
+// the device transcript).
 __global__ void __launch_bounds__(256)
     fold_interleaved_kernel(const uint4* __restrict__ cw, uint32_t log_len, uint32_t log_batch,
-                            Challenges ch, uint4* __restrict__ out) {
+                            Challenges ch, const uint4* __restrict__ dch, uint4* __restrict__ out) {
   __shared__ uint4 tensor[1u << kMaxChallenges];
   const uint32_t batch = 1u << log_batch;
   // eq_ind(r)[j] = prod_i (bit_i(j) ? r_i : 1 + r_i)  (multilinear/eq.rs:39-71)
   for (uint32_t j = threadIdx.x; j < batch; j += blockDim.x) {
     uint4 acc = gf_one();
     for (uint32_t i = 0; i < log_batch; i++) {
-      uint4 f = ch.r[i];
+      uint4 f = dch ? dch[i] : ch.r[i];
       if (!((j >> i) & 1)) f.x ^= 1u;
       acc = gf_mul(acc, f);
     }
@@ -67,8 +70,12 @@ __global__ void __launch_bounds__(256)
 template <int N>
 __global__ void __launch_bounds__(256)
     fold_codeword_kernel(const uint4* __restrict__ cw, uint32_t log_len,
-                         const uint4* __restrict__ tw, Challenges ch, uint4* __restrict__ out) {
+                         const uint4* __restrict__ tw, Challenges ch, const uint4* __restrict__ dch,
+                         uint4* __restrict__ out) {
   const uint64_t n_chunks = 1ull << (log_len - N);
+  uint4 rr[N];
+#pragma unroll
+  for (int kk = 0; kk < N; kk++) rr[kk] = dch ? dch[kk] : ch.r[kk];
   for (uint64_t ci = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; ci < n_chunks;
        ci += (uint64_t)gridDim.x * blockDim.x) {
     uint4 v[1 << N];
@@ -78,7 +85,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int kk = 0; kk < N; kk++) {
       const int size = N - kk;
-      const uint4 r = ch.r[kk];
+      const uint4 r = rr[kk];
       const uint64_t layer_base = (1ull << (cur - 1)) - 1;
 #pragma unroll
       for (int off = 0; off < (1 << (size - 1)); off++) {
@@ -114,9 +121,9 @@ int load_challenges(const void* h, uint32_t n, Challenges& ch) {
 
 template <int N>
 void launch_fold_codeword(const uint4* cw, uint32_t log_len, const uint4* tw, const Challenges& ch,
-                          uint4* out, cudaStream_t s) {
+                          const uint4* dch, uint4* out, cudaStream_t s) {
   uint64_t n_chunks = 1ull << (log_len - N);
-  fold_codeword_kernel<N><<<grid_for(n_chunks, 256), 256, 0, s>>>(cw, log_len, tw, ch, out);
+  fold_codeword_kernel<N><<<grid_for(n_chunks, 256), 256, 0, s>>>(cw, log_len, tw, ch, dch, out);
 }
 
 // ---- Scratch for binius_fri_fold_codeword_noalloc ----
@@ -150,40 +157,16 @@ int noalloc_scratch(void** out) {
   return BINIUS_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-int binius_fri_fold_interleaved(const void* d_codeword, uint32_t log_len, uint32_t log_batch,
-                                const void* h_challenges, void* d_out, void* stream) {
-  BGPU_ARG(d_codeword != nullptr && d_out != nullptr, "codeword / out is NULL");
-  BGPU_ARG(log_len + log_batch <= 40, "codeword too large");
-  Challenges ch;
-  if (int rc = load_challenges(h_challenges, log_batch, ch)) return rc;
-  cudaStream_t s = as_stream(stream);
-  fold_interleaved_kernel<<<grid_for(1ull << log_len, 256), 256, 0, s>>>(
-      static_cast<const uint4*>(d_codeword), log_len, log_batch, ch, static_cast<uint4*>(d_out));
-  BGPU_LAUNCH_CHECK("fold_interleaved_kernel");
-  count_launch();
-  return clear_error();
-}
-
-int binius_fri_fold_codeword(const binius_ntt* ntt, const void* d_codeword, uint32_t log_len,
-                             const void* h_challenges, uint32_t n_challenges, void* d_out,
-                             void* stream) {
-  BGPU_ARG(ntt != nullptr, "ntt is NULL");
-  BGPU_ARG(d_codeword != nullptr && d_out != nullptr, "codeword / out is NULL");
-  BGPU_ARG(n_challenges <= log_len, "more challenges than codeword variables");
-  BGPU_ARG(log_len <= ntt->log_domain, "codeword longer than the NTT domain");
-  Challenges ch;
-  if (int rc = load_challenges(h_challenges, n_challenges, ch)) return rc;
-  cudaStream_t s = as_stream(stream);
+// The fold behind binius_fri_fold_codeword; challenges from ch, or from device memory at dch.
+int fold_codeword_impl(const binius_ntt* ntt, const void* d_codeword, uint32_t log_len,
+                       const Challenges& ch, const uint4* dch, uint32_t n_challenges, void* d_out,
+                       cudaStream_t s) {
   const uint4* cw = static_cast<const uint4*>(d_codeword);
   const uint4* tw = static_cast<const uint4*>(ntt->d_twiddles);
   uint4* out = static_cast<uint4*>(d_out);
   if (n_challenges == 0) {
     BGPU_CUDA(cudaMemcpyAsync(d_out, d_codeword, 16ull << log_len, cudaMemcpyDeviceToDevice, s));
-    return clear_error();
+    return BINIUS_OK;
   }
   // Rounds are applied in steps of at most 4 (one coset of 16 values per thread in registers);
   // a fold over n challenges equals n successive single-challenge folds of the whole codeword,
@@ -199,13 +182,14 @@ int binius_fri_fold_codeword(const binius_ntt* ntt, const void* d_codeword, uint
     Challenges sub;
     memset(&sub, 0, sizeof(sub));
     for (uint32_t i = 0; i < step; i++) sub.r[i] = ch.r[done + i];
+    const uint4* dsub = dch ? dch + done : nullptr;
     // n <= 8, so there are at most two steps: codeword -> tmp -> out.
     uint4* dst = (done + step == n_challenges) ? out : static_cast<uint4*>(tmp);
     switch (step) {
-      case 1: launch_fold_codeword<1>(src, cur_len, tw, sub, dst, s); break;
-      case 2: launch_fold_codeword<2>(src, cur_len, tw, sub, dst, s); break;
-      case 3: launch_fold_codeword<3>(src, cur_len, tw, sub, dst, s); break;
-      default: launch_fold_codeword<4>(src, cur_len, tw, sub, dst, s); break;
+      case 1: launch_fold_codeword<1>(src, cur_len, tw, sub, dsub, dst, s); break;
+      case 2: launch_fold_codeword<2>(src, cur_len, tw, sub, dsub, dst, s); break;
+      case 3: launch_fold_codeword<3>(src, cur_len, tw, sub, dsub, dst, s); break;
+      default: launch_fold_codeword<4>(src, cur_len, tw, sub, dsub, dst, s); break;
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
@@ -218,6 +202,66 @@ int binius_fri_fold_codeword(const binius_ntt* ntt, const void* d_codeword, uint
     done += step;
   }
   if (tmp) BGPU_CUDA(cudaFreeAsync(tmp, s));
+  return BINIUS_OK;
+}
+
+}  // namespace
+
+namespace bgpu {
+
+int fri_fold_interleaved_dev(const void* d_codeword, uint32_t log_len, uint32_t log_batch,
+                             const uint4* d_challenges, void* d_out, cudaStream_t s) {
+  if (log_batch > kMaxChallenges) return set_error(BINIUS_E_ARG, "at most 8 folding challenges");
+  Challenges none;
+  memset(&none, 0, sizeof(none));
+  fold_interleaved_kernel<<<grid_for(1ull << log_len, 256), 256, 0, s>>>(
+      static_cast<const uint4*>(d_codeword), log_len, log_batch, none, d_challenges,
+      static_cast<uint4*>(d_out));
+  BGPU_LAUNCH_CHECK("fold_interleaved_kernel");
+  count_launch();
+  return BINIUS_OK;
+}
+
+int fri_fold_codeword_dev(const binius_ntt* ntt, const void* d_codeword, uint32_t log_len,
+                          const uint4* d_challenges, uint32_t n_challenges, void* d_out,
+                          cudaStream_t s) {
+  if (n_challenges > kMaxChallenges) return set_error(BINIUS_E_ARG, "at most 8 folding challenges");
+  Challenges none;
+  memset(&none, 0, sizeof(none));
+  return fold_codeword_impl(ntt, d_codeword, log_len, none, d_challenges, n_challenges, d_out, s);
+}
+
+}  // namespace bgpu
+
+extern "C" {
+
+int binius_fri_fold_interleaved(const void* d_codeword, uint32_t log_len, uint32_t log_batch,
+                                const void* h_challenges, void* d_out, void* stream) {
+  BGPU_ARG(d_codeword != nullptr && d_out != nullptr, "codeword / out is NULL");
+  BGPU_ARG(log_len + log_batch <= 40, "codeword too large");
+  Challenges ch;
+  if (int rc = load_challenges(h_challenges, log_batch, ch)) return rc;
+  cudaStream_t s = as_stream(stream);
+  fold_interleaved_kernel<<<grid_for(1ull << log_len, 256), 256, 0, s>>>(
+      static_cast<const uint4*>(d_codeword), log_len, log_batch, ch, nullptr,
+      static_cast<uint4*>(d_out));
+  BGPU_LAUNCH_CHECK("fold_interleaved_kernel");
+  count_launch();
+  return clear_error();
+}
+
+int binius_fri_fold_codeword(const binius_ntt* ntt, const void* d_codeword, uint32_t log_len,
+                             const void* h_challenges, uint32_t n_challenges, void* d_out,
+                             void* stream) {
+  BGPU_ARG(ntt != nullptr, "ntt is NULL");
+  BGPU_ARG(d_codeword != nullptr && d_out != nullptr, "codeword / out is NULL");
+  BGPU_ARG(n_challenges <= log_len, "more challenges than codeword variables");
+  BGPU_ARG(log_len <= ntt->log_domain, "codeword longer than the NTT domain");
+  Challenges ch;
+  if (int rc = load_challenges(h_challenges, n_challenges, ch)) return rc;
+  if (int rc = fold_codeword_impl(ntt, d_codeword, log_len, ch, nullptr, n_challenges, d_out,
+                                  as_stream(stream)))
+    return rc;
   return clear_error();
 }
 
@@ -266,10 +310,10 @@ int binius_fri_fold_codeword_noalloc(const binius_ntt* ntt, const void* d_codewo
     // the second reads it (same stream), so it needs no clearing.
     uint4* dst = (done + step == n_challenges) ? out : scratch;
     switch (step) {
-      case 1: launch_fold_codeword<1>(src, cur_len, tw, sub, dst, s); break;
-      case 2: launch_fold_codeword<2>(src, cur_len, tw, sub, dst, s); break;
-      case 3: launch_fold_codeword<3>(src, cur_len, tw, sub, dst, s); break;
-      default: launch_fold_codeword<4>(src, cur_len, tw, sub, dst, s); break;
+      case 1: launch_fold_codeword<1>(src, cur_len, tw, sub, nullptr, dst, s); break;
+      case 2: launch_fold_codeword<2>(src, cur_len, tw, sub, nullptr, dst, s); break;
+      case 3: launch_fold_codeword<3>(src, cur_len, tw, sub, nullptr, dst, s); break;
+      default: launch_fold_codeword<4>(src, cur_len, tw, sub, nullptr, dst, s); break;
     }
     BGPU_LAUNCH_CHECK("fold_codeword_kernel");
     count_launch();

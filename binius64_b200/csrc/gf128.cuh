@@ -90,6 +90,11 @@ __device__ __forceinline__ uint4 reduce256(const u256& p) {
 
 __device__ __forceinline__ uint4 gf_mul(uint4 a, uint4 b) { return reduce256(clmul128(a, b)); }
 
+// An out-of-line multiply for code that runs once per launch on few threads (small sumcheck
+// rounds, scalar protocol steps): one copy of the multiply stays in the instruction cache, where
+// inlined copies would each be fetched cold.
+static __device__ __noinline__ uint4 gf_mul_nl(uint4 a, uint4 b) { return reduce256(clmul128(a, b)); }
+
 __device__ __forceinline__ uint4 gf_add(uint4 a, uint4 b) {
   return make_uint4(a.x ^ b.x, a.y ^ b.y, a.z ^ b.z, a.w ^ b.w);
 }

@@ -54,6 +54,20 @@ class HostSha256 {
     }
   }
 
+  // Raw state, for handing the stream to the device transcript and back.
+  void save(uint32_t h[8], uint8_t blk[64], uint32_t& blk_len, uint64_t& total) const {
+    memcpy(h, h_, sizeof(h_));
+    memcpy(blk, buf_, 64);
+    blk_len = (uint32_t)buflen_;
+    total = total_;
+  }
+  void load(const uint32_t h[8], const uint8_t blk[64], uint32_t blk_len, uint64_t total) {
+    memcpy(h_, h, sizeof(h_));
+    memcpy(buf_, blk, 64);
+    buflen_ = blk_len & 63;
+    total_ = total;
+  }
+
   static void oneshot(const uint8_t* data, size_t len, uint8_t out[32]) {
     HostSha256 h;
     h.update(data, len);

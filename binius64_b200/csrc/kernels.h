@@ -36,6 +36,18 @@ int bivariate_eval(const uint4* d_a, const uint4* d_b, uint64_t half, uint32_t* 
 // Fold (a, b) of length size by r, then (y_1, y_inf) of the next round.
 int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[16],
                         uint32_t* d_out8, cudaStream_t s);
+// As bivariate_fold_eval with the challenge in device memory (d_r) and no clearing of d_out8:
+// folds of at least kMulTableMinSize elements read r's byte table d_tab, built beforehand.
+int bivariate_fold_eval_dev(uint4* d_a, uint4* d_b, uint64_t size, const uint4* d_r,
+                            const uint4* d_tab, uint32_t* d_out8, cudaStream_t s);
+class DeviceTranscript;
+// The device Fiat-Shamir step of a plain bivariate product round: reads (y_1, y_inf) at d_ys
+// and the claim (d_claim_init if set, else d_claim), writes the message (c_0, c_1) and then the
+// 32 bytes at d_commitment if set, samples r into d_r_out, updates d_claim and, with d_tab,
+// builds r's byte table.
+int bivariate_round_finish(const DeviceTranscript& dt, const uint4* d_ys, const uint4* d_claim_init,
+                           uint4* d_claim, const uint8_t* d_commitment, uint4* d_r_out,
+                           uint4* d_tab, cudaStream_t s);
 int gather_segments(const GatherSegment* d_segs, uint32_t n, uint8_t* d_dst, cudaStream_t s);
 // d_tab (16 * 256 elements) = the byte table of multiplication by r (gf_mul_table).
 int build_mul_table(const uint8_t r[16], uint4* d_tab, cudaStream_t s);
@@ -50,6 +62,14 @@ hu128 phi_elem(uint32_t b);
 // fold_word.rs:77-96).
 int fold_words64(const uint64_t* d_words, uint64_t n, const hu128* vec64, uint4* d_out,
                  cudaStream_t s);
+
+// FRI folds whose challenges are in device memory (sampled by the device transcript); the same
+// results as binius_fri_fold_interleaved / binius_fri_fold_codeword.
+int fri_fold_interleaved_dev(const void* d_codeword, uint32_t log_len, uint32_t log_batch,
+                             const uint4* d_challenges, void* d_out, cudaStream_t s);
+int fri_fold_codeword_dev(const binius_ntt* ntt, const void* d_codeword, uint32_t log_len,
+                          const uint4* d_challenges, uint32_t n_challenges, void* d_out,
+                          cudaStream_t s);
 
 // From the other translation units.
 int rs_encode_batch(const binius_ntt* ntt, const void* d_msg, uint32_t log_dim,

@@ -11,6 +11,7 @@
 
 #include <vector>
 
+#include "dev_transcript.cuh"
 #include "internal.h"
 #include "kernels.h"
 #include "transcript.h"
@@ -79,21 +80,24 @@ struct DevFri {
   std::vector<uint32_t> tree_log_leaves;
   uint32_t curr_round = 0;
   int64_t next_commit;
-  std::vector<uint8_t> unprocessed;  // 16 bytes per challenge
+  const uint4* d_chal;         // the device transcript's challenges, one per round
+  uint32_t n_unprocessed = 0;  // challenges received since the last commit
 
-  DevFri(const binius_pcs& p, const binius_pcs_committed& c, cudaStream_t st)
-      : P(p), C(c), s(st), next_commit(p.log_batch) {}
+  DevFri(const binius_pcs& p, const binius_pcs_committed& c, cudaStream_t st, const uint4* chal)
+      : P(p), C(c), s(st), next_commit(p.log_batch), d_chal(chal) {}
   ~DevFri() {
     for (auto w : words) cudaFreeAsync(w, s);
     for (auto t : trees) cudaFreeAsync(t, s);
   }
 
-  // FRIFoldProver::execute_fold_round (prover/prover/src/fri/fold.rs:117-175)
-  // The new tree's root is queued on `rd` (read with the round's sums); the caller waits.
-  int execute(bool* committed, uint8_t root[32], StagedReads& rd) {
+  // FRIFoldProver::execute_fold_round (prover/prover/src/fri/fold.rs:117-175): on a commit round,
+  // folds by the challenges received since the last commit (device memory) and commits the new
+  // codeword; *d_root is then the device address of the new tree's root.
+  int execute(bool* committed, const uint8_t** d_root) {
     *committed = false;
     if (next_commit < 0 || (int64_t)curr_round != next_commit) return BINIUS_OK;
-    const uint32_t n = (uint32_t)(unprocessed.size() / 16);
+    const uint32_t n = n_unprocessed;
+    const uint4* ch = d_chal + (curr_round - n);
     uint4* out = nullptr;
     uint32_t log_out;
     if (words.empty()) {
@@ -101,8 +105,7 @@ struct DevFri {
       BGPU_CUDA(cudaMallocAsync(&out, 16ull << log_out, s));
       words.push_back(out);
       word_log_len.push_back(log_out);
-      if (int rc = binius_fri_fold_interleaved(C.d_codeword, log_out, P.log_batch,
-                                               unprocessed.data(), out, s))
+      if (int rc = fri_fold_interleaved_dev(C.d_codeword, log_out, P.log_batch, ch, out, s))
         return rc;
     } else {
       const uint32_t log_prev = word_log_len.back();
@@ -111,10 +114,9 @@ struct DevFri {
       BGPU_CUDA(cudaMallocAsync(&out, 16ull << log_out, s));
       words.push_back(out);
       word_log_len.push_back(log_out);
-      if (int rc = binius_fri_fold_codeword(P.ntt, prev, log_prev, unprocessed.data(), n, out, s))
-        return rc;
+      if (int rc = fri_fold_codeword_dev(P.ntt, prev, log_prev, ch, n, out, s)) return rc;
     }
-    unprocessed.clear();
+    n_unprocessed = 0;
     const size_t idx = words.size() - 1;  // number of rounds committed before this one
     const bool has_next = idx < P.arities.size();
     const uint32_t next_arity = has_next ? P.arities[idx] : 0;
@@ -125,14 +127,14 @@ struct DevFri {
     trees.push_back(nodes);
     tree_log_leaves.push_back(log_leaves);
     if (int rc = merkle_commit(out, log_leaves, log_coset, nodes, s)) return rc;
-    if (int rc = rd.add(root, nodes + 32 * ((2ull << log_leaves) - 2), 32)) return rc;
+    *d_root = nodes + 32 * ((2ull << log_leaves) - 2);
     next_commit = has_next ? next_commit + next_arity : -1;
     *committed = true;
     return BINIUS_OK;
   }
 
-  void receive(const uint8_t r[16]) {
-    unprocessed.insert(unprocessed.end(), r, r + 16);
+  void receive() {
+    n_unprocessed++;
     curr_round++;
   }
 
@@ -230,15 +232,22 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
                    const uint8_t* h_point, Transcript& t, cudaStream_t s) {
   const uint32_t n = P->log_msg;
   const uint64_t N = 1ull << n;
-  uint4 *a = nullptr, *b = nullptr, *eq_r = nullptr;
-  uint32_t* d_small = nullptr;  // 128 elements (ring switch) then 2 (round sums)
+  uint4 *a = nullptr, *b = nullptr, *eq_r = nullptr, *dev = nullptr;
+  uint32_t* d_small = nullptr;  // 128 elements (ring switch)
   BGPU_CUDA(cudaMallocAsync(&a, 16 * N, s));
   BGPU_CUDA(cudaMallocAsync(&b, 16 * N, s));
   BGPU_CUDA(cudaMallocAsync(&eq_r, 16 * 128, s));
   BGPU_CUDA(cudaMallocAsync(&d_small, 16 * 128, s));
+  // BaseFold round state: sums (2 per round), the claim pair, challenges, r's byte table
+  const uint64_t n_dev = 2ull * n + 2 + n + kMulTableEntries;
+  BGPU_CUDA(cudaMallocAsync(&dev, 16 * n_dev, s));
+  uint4* slots = dev;
+  uint4* claim = dev + 2 * n;  // [0] running claim, [1] initial claim
+  uint4* chal = claim + 2;
+  uint4* tab = chal + n;
   int rc = BINIUS_OK;
   {
-    DevFri fri(*P, *C, s);
+    DevFri fri(*P, *C, s, chal);
     do {
       // suffix tensor of the evaluation point (coordinates 7..) into b
       if ((rc = eq_tensor(reinterpret_cast<const uint4*>(h_point + 16 * 7), n, b, s))) break;
@@ -267,46 +276,50 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
       if (e != cudaSuccess) { rc = cuda_error(e, "eq(r'') upload"); break; }
       u128h sum = 0;
       for (int j = 0; j < 128; j++) sum ^= host_gf_mul(u[j], h_eq[j]);
+      e = cudaMemcpyAsync(claim + 1, &sum, 16, cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) { rc = cuda_error(e, "claim upload"); break; }
+      e = cudaMemsetAsync(slots, 0, 32ull * n, s);
+      if (e != cudaSuccess) { rc = cuda_error(e, "round sums"); break; }
       // rs_eq_ind = fold_b128_elems_inplace(suffix_tensor, eq(r'')) in place in b
       if ((rc = fold_b128_elems(b, b, N, eq_r, s))) break;
       e = cudaMemcpyAsync(a, d_witness, 16 * N, cudaMemcpyDeviceToDevice, s);
       if (e != cudaSuccess) { rc = cuda_error(e, "copy witness"); break; }
 
-      // BaseFold rounds
-      uint8_t r_prev[16];
+      // BaseFold rounds on the device transcript: the round's sums, the FRI fold and commit on a
+      // commit round, then the finish kernel (message, root, challenge, next table)
+      DeviceTranscript dt;
+      if ((rc = dt.begin(t, s))) break;
+      uint32_t tape_bytes = 0;
       for (uint32_t round = 0; round < n && rc == BINIUS_OK; round++) {
         const uint64_t size = N >> round;
+        uint32_t* ys = reinterpret_cast<uint32_t*>(slots + 2 * round);
         if (round == 0)
-          rc = bivariate_eval(a, b, size / 2, d_small, s);
+          rc = bivariate_eval(a, b, size / 2, ys, s);
         else
-          rc = bivariate_fold_eval(a, b, size * 2, r_prev, d_small, s);
+          rc = bivariate_fold_eval_dev(a, b, size * 2, chal + round - 1,
+                                       size * 2 >= kMulTableMinSize ? tab : nullptr, ys, s);
         if (rc) break;
-        uint8_t ys[32];
         bool committed = false;
-        uint8_t root[32];
-        StagedReads rd(s);
-        if ((rc = rd.add(ys, d_small, 32))) break;
-        if ((rc = fri.execute(&committed, root, rd))) break;
-        if ((rc = rd.wait())) break;
-        const u128h y1 = to_u128(ys), yinf = to_u128(ys + 16);
-        const u128h c0 = sum ^ y1, c2 = yinf, c1 = y1 ^ c0 ^ c2;
-        uint8_t coeffs[32];
-        from_u128(c0, coeffs);
-        from_u128(c1, coeffs + 16);
-        t.message(coeffs, 32);
-        if (committed) t.message(root, 32);
-        t.sample_elem(r_prev);
-        const u128h r = to_u128(r_prev);
-        sum = c0 ^ host_gf_mul(c1, r) ^ host_gf_mul(c2, host_gf_mul(r, r));
-        fri.receive(r_prev);
+        const uint8_t* d_root = nullptr;
+        if ((rc = fri.execute(&committed, &d_root))) break;
+        const bool next_tab = round + 1 < n && size >= kMulTableMinSize;
+        if ((rc = bivariate_round_finish(dt, slots + 2 * round, round == 0 ? claim + 1 : nullptr,
+                                         claim, committed ? d_root : nullptr, chal + round,
+                                         next_tab ? tab : nullptr, s)))
+          break;
+        tape_bytes += committed ? 64 : 32;
+        fri.receive();
       }
       if (rc) break;
       bool committed = false;
-      uint8_t root[32];
+      const uint8_t* d_root = nullptr;
+      if ((rc = fri.execute(&committed, &d_root))) break;
+      if (committed) {
+        if ((rc = dt.message_device(d_root, 32, s))) break;
+        tape_bytes += 32;
+      }
       StagedReads rd(s);
-      if ((rc = fri.execute(&committed, root, rd))) break;
-      if ((rc = rd.wait())) break;
-      if (committed) t.message(root, 32);
+      if ((rc = dt.read(rd, tape_bytes)) || (rc = rd.wait()) || (rc = dt.finish(t))) break;
       rc = fri.finish(t);
     } while (0);
   }
@@ -314,6 +327,7 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
   cudaFreeAsync(b, s);
   cudaFreeAsync(eq_r, s);
   cudaFreeAsync(d_small, s);
+  cudaFreeAsync(dev, s);
   cudaError_t e = stream_wait(s);
   if (rc == BINIUS_OK && e != cudaSuccess) rc = cuda_error(e, "pcs prove");
   return rc;

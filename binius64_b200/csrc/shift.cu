@@ -19,13 +19,16 @@
 // h_op[v] eq(r_s)[s] (one multiply per term into a per-key scalar table, atomicXor into M), then
 // the batched sumcheck of the bivariate product (r_j_witness, M) with the in/out MLE-check
 // (protocols/inout_check.rs:19-211, sumcheck/mle_to_sumcheck.rs:28-77, sumcheck/batch.rs:41-103).
-// Round polynomials and challenges pass through the host transcript between launches.
+// Both round loops run on the device transcript (dev_transcript.cuh): each round is an
+// evaluation kernel and a finish kernel that forms the round polynomial, writes the message and
+// samples the challenge; the host waits once per phase.
 #include <string.h>
 
 #include <algorithm>
 #include <vector>
 
 #include "cs.h"
+#include "dev_transcript.cuh"
 #include "gf128.cuh"
 #include "gf_reduce.cuh"
 #include "internal.h"
@@ -233,6 +236,69 @@ __global__ void __launch_bounds__(256)
   block_xor_reduce<2>(v, out);
 }
 
+// Per-round constants of the phase-2 batch, known before the loop: the in/out check's current
+// eq coordinate zc = z[gn - 1] and 1 / (1 + zc) (used when the round is past the public
+// segment's extra variables), the coordinate alpha_dec the Gruen eq prefix absorbs (0 while the
+// round is early), and whether the round is early (p < n_rem).
+struct ShiftRoundConst {
+  uint4 zc, inv_one_plus_zc, alpha_dec;
+  uint32_t early, pad[3];
+};
+
+// The Fiat-Shamir step of one phase-2 round on the device.  ys = (y_1, y_inf) of the bivariate
+// product (r_j_witness, M) and (lo, hi) of the in/out check's dot products; st3 = (shift claim,
+// in/out claim, Gruen eq prefix).  The batch message is the shift round's (s_0, s_1) plus beta
+// times the in/out check's Gruen-scaled (d_0, d_1) (MleToSumCheckDecorator + batch_prove); then r
+// is sampled and the three running values advance.  When init_lohi is set (the first round) the
+// in/out claim is first set to lo + (hi - lo) z0 from it.
+__global__ void __launch_bounds__(256)
+    shift_round_finish_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
+                              const uint4* __restrict__ ys, const ShiftRoundConst* __restrict__ rc,
+                              const uint4* __restrict__ init_lohi, uint4 z0, uint4 beta,
+                              uint4* __restrict__ st3, uint4* __restrict__ r_out,
+                              uint4* __restrict__ tab) {
+  __shared__ uint4 r_sh;
+  if (threadIdx.x == 0) {
+    DevTr st;
+    st.load(ts);
+    const ShiftRoundConst c = *rc;
+    uint4 inout = st3[1];
+    if (init_lohi)
+      inout = gf_add(init_lohi[0], gf_mul_1t(gf_add(init_lohi[1], init_lohi[0]), z0));
+    const uint4 y1 = ys[0], yinf = ys[1], lo = ys[2], hi = ys[3];
+    const uint4 s0 = gf_add(st3[0], y1), s2 = yinf, s1 = gf_add(gf_add(y1, s0), s2);
+    uint4 iy0, iy1;
+    if (c.early) {
+      iy1 = gf_add(lo, gf_mul_1t(gf_add(hi, lo), c.zc));
+      iy0 = inout;
+    } else {
+      iy1 = lo;
+      iy0 = gf_mul_1t(gf_add(inout, gf_mul_1t(iy1, c.zc)), c.inv_one_plus_zc);
+    }
+    const uint4 q0 = iy0, q1 = gf_add(iy1, iy0);
+    uint4 one_a = c.alpha_dec;
+    one_a.x ^= 1u;
+    const uint4 eqp = st3[2];
+    const uint4 d0 = gf_mul_1t(gf_mul_1t(q0, one_a), eqp);
+    const uint4 d1 = gf_mul_1t(gf_add(gf_mul_1t(q1, one_a), q0), eqp);
+    const uint4 msg[2] = {gf_add(s0, gf_mul_1t(beta, d0)), gf_add(s1, gf_mul_1t(beta, d1))};
+    st.message_elems(tape, msg, 2);
+    const uint4 r = st.sample_elem();
+    *r_out = r;
+    st3[0] = gf_add(s0, gf_mul_1t(r, gf_add(s1, gf_mul_1t(s2, r))));
+    st3[1] = gf_add(q0, gf_mul_1t(q1, r));
+    uint4 f = gf_add(r, c.alpha_dec);
+    f.x ^= 1u;
+    st3[2] = gf_mul_1t(eqp, f);
+    st.store(ts);
+    r_sh = r;
+  }
+  if (tab) {
+    __syncthreads();
+    dt_build_mul_table(r_sh, tab);
+  }
+}
+
 // ------------------------------------------------------------------ host helpers
 
 uint4 u4(hu128 v) {
@@ -372,48 +438,59 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
   }
   BGPU_CUDA(cudaMemcpyAsync(h, h_keep, 16ull * kFlat, cudaMemcpyDeviceToDevice, s));
 
+  // device round state: phase-1 sum slots (12 x 2), phase-2 slots (log_words x 4); dstate = the
+  // phase-1 claim, the phase-2 running values (shift claim, in/out claim, eq prefix) and the
+  // in/out check's first (lo, hi); challenges (12 + log_words); the last challenge's byte table
+  uint4 *slots, *dstate, *chal, *tab;
+  ShiftRoundConst* rconst;
+  const uint64_t n_slots = 2 * 12 + 4 * (uint64_t)log_words;
+  SHIFT_TRY(B.alloc(&slots, 16 * n_slots));
+  SHIFT_TRY(B.alloc(&dstate, 16 * 6));
+  SHIFT_TRY(B.alloc(&chal, 16 * (12 + (uint64_t)log_words)));
+  SHIFT_TRY(B.alloc(&tab, 16 * kMulTableEntries));
+  SHIFT_TRY(B.alloc(&rconst, sizeof(ShiftRoundConst) * log_words));
+  BGPU_CUDA(cudaMemsetAsync(slots, 0, 16 * n_slots, s));
+  uint4* slots2 = slots + 24;
+
   // the provers' claims: sum_v <g_v, h_v> (phase_1.rs:96-101)
   BGPU_CUDA(cudaMemsetAsync(acc + 8, 0, 32, s));
   dot2_kernel<<<grid_for(kFlat, 256, 148), 256, 0, s>>>(g, 0, 0, h, kFlat, acc + 8);
   SHIFT_TRY(launched("dot2_kernel"));
-  std::vector<hu128> ch1;
-  hu128 sum = 0;
-  uint8_t rb[16] = {0};
-  hu128 gamma = 0;
+  DeviceTranscript dt;
+  SHIFT_TRY(dt.begin(t, s));
   for (int round = 0; round < 12; round++) {
     const uint64_t size = (uint64_t)kFlat >> round;  // before this round's fold
+    uint32_t* ys = reinterpret_cast<uint32_t*>(slots + 2 * round);
     if (round == 0) {
-      SHIFT_TRY(bivariate_eval(g, h, size / 2, acc, s));
+      SHIFT_TRY(bivariate_eval(g, h, size / 2, ys, s));
     } else {
-      SHIFT_TRY(bivariate_fold_eval(g, h, size * 2, rb, acc, s));
+      SHIFT_TRY(bivariate_fold_eval_dev(g, h, size * 2, chal + round - 1,
+                                        size * 2 >= kMulTableMinSize ? tab : nullptr, ys, s));
     }
-    uint8_t host[64 + 2 * 16 * 16];
-    const bool last = round == 11;
+    // the next round folds arrays of `size` elements
+    const bool next_tab = round < 11 && size >= kMulTableMinSize;
+    SHIFT_TRY(bivariate_round_finish(dt, slots + 2 * round,
+                                     round == 0 ? reinterpret_cast<const uint4*>(acc + 8) : nullptr,
+                                     dstate, nullptr, chal + round, next_tab ? tab : nullptr, s));
+  }
+  // one read: transcript, challenges and the remaining 16-element g and h
+  std::vector<hu128> ch1(12);
+  hu128 gamma = 0;
+  {
+    uint8_t host[2 * 256];
     StagedReads rd(s);
-    SHIFT_TRY(rd.add(host, acc, round == 0 ? 64 : 32));
-    if (last) {
-      SHIFT_TRY(rd.add(host + 64, g, 256));
-      SHIFT_TRY(rd.add(host + 64 + 256, h, 256));
-    }
+    SHIFT_TRY(dt.read(rd, 12 * 32));
+    SHIFT_TRY(rd.add(ch1.data(), chal, 16 * 12));
+    SHIFT_TRY(rd.add(host, g, 256));
+    SHIFT_TRY(rd.add(host + 256, h, 256));
     SHIFT_TRY(rd.wait());
-    if (round == 0) sum = h128(host + 32);
-    const hu128 y1 = h128(host), yinf = h128(host + 16);
-    const hu128 c0 = sum ^ y1, c2 = yinf, c1 = y1 ^ c0 ^ c2;
-    uint8_t rp[32];
-    memcpy(rp, &c0, 16);
-    memcpy(rp + 16, &c1, 16);
-    t.message(rp, 32);
-    t.sample_elem(rb);
-    const hu128 r = h128(rb);
-    ch1.push_back(r);
-    sum = c0 ^ host_gf_mul(c1, r) ^ host_gf_mul(c2, host_gf_mul(r, r));
-    if (last) {
-      // fold the remaining 16-element arrays by r; gamma = sum_v g_v(r) h_v(r)
-      for (int v = 0; v < 8; v++) {
-        const hu128 g0 = h128(host + 64 + 16 * v), g1 = h128(host + 64 + 16 * (8 + v));
-        const hu128 h0 = h128(host + 320 + 16 * v), h1 = h128(host + 320 + 16 * (8 + v));
-        gamma ^= host_gf_mul(g0 ^ host_gf_mul(r, g1 ^ g0), h0 ^ host_gf_mul(r, h1 ^ h0));
-      }
+    SHIFT_TRY(dt.finish(t));
+    // fold the remaining 16-element arrays by the last r; gamma = sum_v g_v(r) h_v(r)
+    const hu128 r = ch1[11];
+    for (int v = 0; v < 8; v++) {
+      const hu128 g0 = h128(host + 16 * v), g1 = h128(host + 16 * (8 + v));
+      const hu128 h0 = h128(host + 256 + 16 * v), h1 = h128(host + 256 + 16 * (8 + v));
+      gamma ^= host_gf_mul(g0 ^ host_gf_mul(r, g1 ^ g0), h0 ^ host_gf_mul(r, h1 ^ h0));
     }
   }
   std::vector<hu128> rev(ch1.rbegin(), ch1.rend());
@@ -442,90 +519,86 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
     SHIFT_TRY(launched("shift_monster_kernel"));
   }
 
-  // in/out check point and the public evaluation (InOutCheckProver::new)
+  // in/out check point (InOutCheckProver::new) and the batching coefficient; the public
+  // evaluation is taken on the device by the first round's finish kernel
   const uint32_t p = log_public;
   std::vector<hu128> z(p);
   for (auto& v : z) v = sample(t);
-  auto dot2 = [&](uint64_t off0, uint64_t off1, uint64_t len) -> int {
-    BGPU_CUDA(cudaMemsetAsync(acc + 8, 0, 32, s));
-    dot2_kernel<<<grid_for(len, 256, 148 * 2), 256, 0, s>>>(W, off0, off1, eq_pub, len, acc + 8);
+  const hu128 beta = sample(t);
+  auto dot2 = [&](uint64_t off0, uint64_t off1, uint64_t len, uint4* out) -> int {
+    dot2_kernel<<<grid_for(len, 256, 148 * 2), 256, 0, s>>>(W, off0, off1, eq_pub, len,
+                                                            reinterpret_cast<uint32_t*>(out));
     SHIFT_TRY(launched("dot2_kernel"));
-    return BINIUS_OK;
-  };
-  auto read2 = [&](hu128& o0, hu128& o1) -> int {
-    uint8_t b[32];
-    SHIFT_TRY(read_sync(b, acc + 8, 32, s));
-    o0 = h128(b);
-    o1 = h128(b + 16);
     return BINIUS_OK;
   };
   uint32_t gn = p;  // Gruen32::n_vars_remaining
   SHIFT_TRY(eq_tensor(to_u4(z).data(), gn - 1, eq_pub, s));
-  hu128 lo, hi;
-  SHIFT_TRY(dot2(0, 1ull << (gn - 1), 1ull << (gn - 1)));
-  SHIFT_TRY(read2(lo, hi));
-  hu128 inout_eval = lo ^ host_gf_mul(hi ^ lo, z[gn - 1]);
-
-  const hu128 beta = sample(t);
-  hu128 shift_sum = gamma, eq_prefix = 1;
-  std::vector<hu128> ch2;
-  for (uint32_t n_rem = log_words; n_rem > 0; n_rem--) {
-    const uint64_t half = 1ull << (n_rem - 1);
-    if (n_rem == log_words) {
-      SHIFT_TRY(bivariate_eval(W, M, half, acc, s));
-    } else {
-      SHIFT_TRY(bivariate_fold_eval(W, M, half * 4, rb, acc, s));
-    }
-    const bool early = p < n_rem;
-    if (early) {
-      SHIFT_TRY(dot2(half, half + (1ull << (gn - 1)), 1ull << (gn - 1)));
-    } else {
-      SHIFT_TRY(eq_tensor(to_u4(z).data(), n_rem - 1, eq_pub, s));
-      SHIFT_TRY(dot2(half, half, half));
-    }
-    uint8_t host[64 + 32];
-    StagedReads rd(s);
-    SHIFT_TRY(rd.add(host, acc, 64));
-    if (n_rem == 1) SHIFT_TRY(rd.add(host + 64, W, 32));
-    SHIFT_TRY(rd.wait());
-    const hu128 y1 = h128(host), yinf = h128(host + 16);
-    const hu128 s0 = shift_sum ^ y1, s2 = yinf, s1 = y1 ^ s0 ^ s2;
-    hu128 iy0, iy1;
-    lo = h128(host + 32);
-    hi = h128(host + 48);
-    if (early) {
-      iy1 = lo ^ host_gf_mul(hi ^ lo, z[gn - 1]);
-      iy0 = inout_eval;
-    } else {
-      iy1 = lo;
-      const hu128 alpha = z[gn - 1];
-      iy0 = host_gf_mul(inout_eval ^ host_gf_mul(iy1, alpha), host_gf_inv(1 ^ alpha));
-    }
-    const hu128 q0 = iy0, q1 = iy1 ^ iy0;
-    const hu128 alpha_dec = n_rem <= p ? z[n_rem - 1] : 0;
-    const hu128 one_a = 1 ^ alpha_dec;
-    const hu128 d0 = host_gf_mul(host_gf_mul(q0, one_a), eq_prefix);
-    const hu128 d1 = host_gf_mul(host_gf_mul(q1, one_a) ^ q0, eq_prefix);
-    const hu128 b0 = s0 ^ host_gf_mul(beta, d0), b1 = s1 ^ host_gf_mul(beta, d1);
-    uint8_t rp[32];
-    memcpy(rp, &b0, 16);
-    memcpy(rp + 16, &b1, 16);
-    t.message(rp, 32);
-    t.sample_elem(rb);
-    const hu128 r = h128(rb);
-    ch2.push_back(r);
-    shift_sum = s0 ^ host_gf_mul(s1, r) ^ host_gf_mul(s2, host_gf_mul(r, r));
-    inout_eval = q0 ^ host_gf_mul(q1, r);
-    if (n_rem <= p) gn--;
-    eq_prefix = host_gf_mul(eq_prefix, 1 ^ r ^ alpha_dec);
-    if (n_rem == 1) {
-      const hu128 w0 = h128(host + 64), w1 = h128(host + 80);
-      res.witness_eval = w0 ^ host_gf_mul(r, w1 ^ w0);
+  uint4* run = dstate + 1;
+  uint4* init_lohi = dstate + 4;
+  BGPU_CUDA(cudaMemsetAsync(init_lohi, 0, 32, s));
+  SHIFT_TRY(dot2(0, 1ull << (gn - 1), 1ull << (gn - 1), init_lohi));
+  const uint4 z0 = u4(z[gn - 1]);
+  std::vector<ShiftRoundConst> consts(log_words);
+  {
+    uint32_t g2 = p;
+    for (uint32_t n_rem = log_words; n_rem > 0; n_rem--) {
+      ShiftRoundConst& c = consts[log_words - n_rem];
+      memset(&c, 0, sizeof(c));
+      const hu128 zc = z[g2 - 1];
+      c.zc = u4(zc);
+      c.early = p < n_rem;
+      if (!c.early) c.inv_one_plus_zc = u4(host_gf_inv(1 ^ zc));
+      c.alpha_dec = u4(n_rem <= p ? z[n_rem - 1] : 0);
+      if (n_rem <= p) g2--;
     }
   }
+  BGPU_CUDA(cudaMemcpyAsync(rconst, consts.data(), sizeof(ShiftRoundConst) * log_words,
+                            cudaMemcpyHostToDevice, s));
+  {
+    // the in/out claim is set by the first round from init_lohi
+    const uint4 init3[3] = {u4(gamma), u4(0), u4(1)};
+    BGPU_CUDA(cudaMemcpyAsync(run, init3, sizeof(init3), cudaMemcpyHostToDevice, s));
+  }
+  SHIFT_TRY(dt.begin(t, s));
+  for (uint32_t n_rem = log_words; n_rem > 0; n_rem--) {
+    const uint32_t k = log_words - n_rem;
+    const uint64_t half = 1ull << (n_rem - 1);
+    uint4* ys = slots2 + 4 * k;
+    if (n_rem == log_words) {
+      SHIFT_TRY(bivariate_eval(W, M, half, reinterpret_cast<uint32_t*>(ys), s));
+    } else {
+      SHIFT_TRY(bivariate_fold_eval_dev(W, M, half * 4, chal + 12 + k - 1,
+                                        half * 4 >= kMulTableMinSize ? tab : nullptr,
+                                        reinterpret_cast<uint32_t*>(ys), s));
+    }
+    if (p < n_rem) {
+      SHIFT_TRY(dot2(half, half + (1ull << (gn - 1)), 1ull << (gn - 1), ys + 2));
+    } else {
+      SHIFT_TRY(eq_tensor(to_u4(z).data(), n_rem - 1, eq_pub, s));
+      SHIFT_TRY(dot2(half, half, half, ys + 2));
+    }
+    if (n_rem <= p) gn--;
+    const bool next_tab = n_rem > 1 && half * 2 >= kMulTableMinSize;
+    shift_round_finish_kernel<<<1, 256, 0, s>>>(
+        dt.state(), dt.tape(), ys, rconst + k, n_rem == log_words ? init_lohi : nullptr, z0,
+        u4(beta), run, chal + 12 + k, next_tab ? tab : nullptr);
+    SHIFT_TRY(launched("shift_round_finish_kernel"));
+  }
+  {
+    std::vector<hu128> ch2(log_words);
+    uint8_t w01[32];
+    StagedReads rd(s);
+    SHIFT_TRY(dt.read(rd, 32 * log_words));
+    SHIFT_TRY(rd.add(ch2.data(), chal + 12, 16ull * log_words));
+    SHIFT_TRY(rd.add(w01, W, 32));
+    SHIFT_TRY(rd.wait());
+    SHIFT_TRY(dt.finish(t));
+    const hu128 r = ch2[log_words - 1], w0 = h128(w01), w1 = h128(w01 + 16);
+    res.witness_eval = w0 ^ host_gf_mul(r, w1 ^ w0);
+    res.point = r_j;
+    res.point.insert(res.point.end(), ch2.rbegin(), ch2.rend());
+  }
   t.message(&res.witness_eval, 16);
-  res.point = r_j;
-  res.point.insert(res.point.end(), ch2.rbegin(), ch2.rend());
   return BINIUS_OK;
 }
 

@@ -19,6 +19,7 @@
 
 #include <algorithm>
 
+#include "dev_transcript.cuh"
 #include "gf128.cuh"
 #include "gf_reduce.cuh"
 #include "internal.h"
@@ -29,6 +30,8 @@ using namespace bgpu;
 namespace {
 
 constexpr int kThreads = 256;
+
+uint4 gf_zero_host() { return make_uint4(0u, 0u, 0u, 0u); }
 
 unsigned grid_for(uint64_t n, unsigned threads, unsigned max_blocks = 148 * 8) {
   uint64_t g = (n + threads - 1) / threads;
@@ -142,14 +145,19 @@ __global__ void __launch_bounds__(kThreads)
 // Folds (a, b) of length `size` by r in place (a[i] = a[i] + r (a[i + size/2] - a[i])) and
 // evaluates the next round on the folded length-size/2 arrays.  Thread j owns folded positions j
 // and j + size/4, so no two threads touch the same element.  With TAB the four products by r go
-// through the byte table of r (gf_mul_table).
+// through the byte table of r (gf_mul_table); otherwise r is r_arg, or *r_ptr when that is set
+// (a challenge the device transcript sampled).
 template <bool TAB>
 __global__ void __launch_bounds__(kThreads)
-    bivariate_fold_eval_kernel(uint4* __restrict__ a, uint4* __restrict__ b, uint64_t size, uint4 r,
+    bivariate_fold_eval_kernel(uint4* __restrict__ a, uint4* __restrict__ b, uint64_t size,
+                               uint4 r_arg, const uint4* __restrict__ r_ptr,
                                const uint4* __restrict__ tab, uint32_t* __restrict__ out) {
   const uint64_t h = size >> 1, q = size >> 2;
   u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
-  auto mul_r = [&](uint4 x) { return TAB ? gf_mul_table(tab, x) : gf_mul(r, x); };
+  uint4 s1r = gf_zero(), sinfr = gf_zero();  // small rounds: reduced sums
+  const uint4 r = TAB || !r_ptr ? r_arg : *r_ptr;
+  // small rounds (no table) run on few threads once: out-of-line multiplies keep the code compact
+  auto mul_r = [&](uint4 x) { return TAB ? gf_mul_table(tab, x) : gf_mul_nl(r, x); };
   for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < q;
        j += (uint64_t)gridDim.x * blockDim.x) {
     uint4 a_lo = a[j], a_hi = a[h + j], a_lo2 = a[q + j], a_hi2 = a[h + q + j];
@@ -162,11 +170,54 @@ __global__ void __launch_bounds__(kThreads)
     a[q + j] = fa1;
     b[j] = fb0;
     b[q + j] = fb1;
-    xor_into(s1, clmul128(fa1, fb1));
-    xor_into(sinf, clmul128(gf_add(fa0, fa1), gf_add(fb0, fb1)));
+    if constexpr (TAB) {
+      xor_into(s1, clmul128(fa1, fb1));
+      xor_into(sinf, clmul128(gf_add(fa0, fa1), gf_add(fb0, fb1)));
+    } else {
+      gf_add_into(s1r, gf_mul_nl(fa1, fb1));
+      gf_add_into(sinfr, gf_mul_nl(gf_add(fa0, fa1), gf_add(fb0, fb1)));
+    }
   }
-  uint4 v[2] = {reduce256(s1), reduce256(sinf)};
+  uint4 v[2] = {TAB ? reduce256(s1) : s1r, TAB ? reduce256(sinf) : sinfr};
   block_xor_reduce<2>(v, out);
+}
+
+// The Fiat-Shamir step of a plain bivariate product round (BivariateProductSumcheckProver,
+// bivariate_product.rs:43-95, through the prover's round-proof truncation) on the device: the
+// sums (y_1, y_inf) and the claim give c_0 = claim + y_1, c_2 = y_inf, c_1 = y_1 + c_0 + c_2; the
+// message is (c_0, c_1), then optionally a 32-byte commitment (a Merkle root the device just
+// built), then the challenge r is sampled and the claim becomes c_0 + c_1 r + c_2 r^2.  The claim
+// is read from claim_init when that is set (the first round).  With a table pointer the block
+// then builds r's byte table for the next fold.
+__global__ void __launch_bounds__(256)
+    bivariate_round_finish_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
+                                  const uint4* __restrict__ ys, const uint4* __restrict__ claim_init,
+                                  uint4* __restrict__ claim, const uint8_t* __restrict__ commitment,
+                                  uint4* __restrict__ r_out, uint4* __restrict__ tab) {
+  __shared__ uint4 r_sh;
+  if (threadIdx.x == 0) {
+    DevTr st;
+    st.load(ts);
+    const uint4 y1 = ys[0], yinf = ys[1];
+    const uint4 c0 = gf_add(claim_init ? *claim_init : *claim, y1), c2 = yinf;
+    const uint4 c1 = gf_add(gf_add(y1, c0), c2);
+    const uint4 msg[2] = {c0, c1};
+    st.message_elems(tape, msg, 2);
+    if (commitment) {
+      uint32_t root[8];
+      for (int i = 0; i < 8; i++) root[i] = reinterpret_cast<const uint32_t*>(commitment)[i];
+      st.message_words(tape, root, 8);
+    }
+    const uint4 r = st.sample_elem();
+    *r_out = r;
+    *claim = gf_add(c0, gf_mul_1t(r, gf_add(c1, gf_mul_1t(c2, r))));
+    st.store(ts);
+    r_sh = r;
+  }
+  if (tab) {
+    __syncthreads();
+    dt_build_mul_table(r_sh, tab);
+  }
 }
 
 // tab[j * 256 + v] = r * (v x^(8j)): the byte table of gf_mul_table, one entry per thread from
@@ -287,7 +338,8 @@ int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[1
     BGPU_CUDA(cudaMallocAsync(&tab, 16 * kMulTableEntries, s));
     int rc = build_mul_table(r, tab, s);
     if (!rc) {
-      bivariate_fold_eval_kernel<true><<<grid, kThreads, 0, s>>>(d_a, d_b, size, rv, tab, d_out8);
+      bivariate_fold_eval_kernel<true><<<grid, kThreads, 0, s>>>(d_a, d_b, size, rv, nullptr, tab,
+                                                                 d_out8);
       cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) rc = cuda_error(e, "bivariate_fold_eval_kernel");
       else count_launch();
@@ -295,8 +347,36 @@ int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[1
     cudaFreeAsync(tab, s);
     return rc;
   }
-  bivariate_fold_eval_kernel<false><<<grid, kThreads, 0, s>>>(d_a, d_b, size, rv, nullptr, d_out8);
+  bivariate_fold_eval_kernel<false><<<grid, kThreads, 0, s>>>(d_a, d_b, size, rv, nullptr, nullptr,
+                                                              d_out8);
   BGPU_LAUNCH_CHECK("bivariate_fold_eval_kernel");
+  count_launch();
+  return BINIUS_OK;
+}
+
+int bivariate_fold_eval_dev(uint4* d_a, uint4* d_b, uint64_t size, const uint4* d_r,
+                            const uint4* d_tab, uint32_t* d_out8, cudaStream_t s) {
+  if (size < 4) return set_error(BINIUS_E_ARG, "bivariate_fold_eval needs size >= 4");
+  const unsigned grid = grid_for(size / 4, kThreads);
+  if (size >= kMulTableMinSize) {
+    if (!d_tab) return set_error(BINIUS_E_ARG, "a large fold needs the challenge's table");
+    bivariate_fold_eval_kernel<true><<<grid, kThreads, 0, s>>>(d_a, d_b, size, gf_zero_host(),
+                                                               nullptr, d_tab, d_out8);
+  } else {
+    bivariate_fold_eval_kernel<false><<<grid, kThreads, 0, s>>>(d_a, d_b, size, gf_zero_host(),
+                                                                d_r, nullptr, d_out8);
+  }
+  BGPU_LAUNCH_CHECK("bivariate_fold_eval_kernel");
+  count_launch();
+  return BINIUS_OK;
+}
+
+int bivariate_round_finish(const DeviceTranscript& dt, const uint4* d_ys, const uint4* d_claim_init,
+                           uint4* d_claim, const uint8_t* d_commitment, uint4* d_r_out,
+                           uint4* d_tab, cudaStream_t s) {
+  bivariate_round_finish_kernel<<<1, 256, 0, s>>>(dt.state(), dt.tape(), d_ys, d_claim_init,
+                                                  d_claim, d_commitment, d_r_out, d_tab);
+  BGPU_LAUNCH_CHECK("bivariate_round_finish_kernel");
   count_launch();
   return BINIUS_OK;
 }

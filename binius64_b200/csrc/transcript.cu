@@ -1,8 +1,74 @@
-// C ABI of the host-side Fiat-Shamir transcript (transcript.h).
+// C ABI of the host-side Fiat-Shamir transcript (transcript.h), and the host side of device
+// transcript stretches (dev_transcript.cuh).
+#include "dev_transcript.cuh"
 #include "internal.h"
 #include "transcript.h"
 
 using namespace bgpu;
+
+namespace {
+
+__global__ void transcript_load_kernel(TranscriptState st, TranscriptState* dst) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *dst = st;
+}
+
+__global__ void transcript_message_kernel(TranscriptState* ts, uint8_t* tape,
+                                          const uint32_t* __restrict__ words, uint32_t n) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  DevTr st;
+  st.load(ts);
+  st.message_words(tape, words, n);
+  st.store(ts);
+}
+
+}  // namespace
+
+namespace bgpu {
+
+DeviceTranscript::~DeviceTranscript() {
+  if (mem_) cudaFreeAsync(mem_, s_);
+}
+
+int DeviceTranscript::begin(const Transcript& t, cudaStream_t s) {
+  s_ = s;
+  if (!mem_) BGPU_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&mem_), kStateBytes + kTapeCap, s));
+  TranscriptState st;
+  t.save(st);
+  st.tape_cap = kTapeCap;
+  transcript_load_kernel<<<1, 32, 0, s>>>(st, state());
+  BGPU_LAUNCH_CHECK("transcript_load_kernel");
+  count_launch();
+  return BINIUS_OK;
+}
+
+int DeviceTranscript::message_device(const void* d_bytes, uint32_t n_bytes, cudaStream_t s) {
+  if (n_bytes % 4 || reinterpret_cast<uintptr_t>(d_bytes) % 4)
+    return set_error(BINIUS_E_ARG, "device message: whole aligned words only");
+  transcript_message_kernel<<<1, 32, 0, s>>>(state(), tape(),
+                                             static_cast<const uint32_t*>(d_bytes), n_bytes / 4);
+  BGPU_LAUNCH_CHECK("transcript_message_kernel");
+  count_launch();
+  return BINIUS_OK;
+}
+
+int DeviceTranscript::read(StagedReads& rd, uint32_t tape_bytes) {
+  if (tape_bytes > kTapeCap) return set_error(BINIUS_E_ARG, "device transcript tape too small");
+  expect_ = tape_bytes;
+  host_tape_.resize(tape_bytes);
+  if (int rc = rd.add(&host_state_, state(), sizeof(TranscriptState))) return rc;
+  if (tape_bytes)
+    if (int rc = rd.add(host_tape_.data(), tape(), tape_bytes)) return rc;
+  return BINIUS_OK;
+}
+
+int DeviceTranscript::finish(Transcript& t) {
+  if (host_state_.error || host_state_.tape_len != expect_)
+    return set_error(BINIUS_E_CUDA, "device transcript wrote an unexpected number of bytes");
+  t.load(host_state_, host_tape_.data());
+  return BINIUS_OK;
+}
+
+}  // namespace bgpu
 
 extern "C" {
 

@@ -18,6 +18,23 @@
 
 namespace bgpu {
 
+// The challenger's whole state as plain data in the word form the device transcript
+// (dev_transcript.cuh) works in: the SHA-256 stream (chaining value, the partial block as
+// big-endian words zero past block_len, length), the sampling mode, the sample buffer as
+// little-endian words and its read index, plus the device tape's fill level.
+struct TranscriptState {
+  uint32_t h[8];
+  uint32_t w[16];
+  uint64_t total;
+  uint32_t block_len;
+  uint32_t sampling;
+  uint32_t index;
+  uint32_t tape_len;  // bytes the device appended to its tape
+  uint32_t tape_cap;
+  uint32_t error;     // set when the device tape overflowed
+  uint32_t buf[8];
+};
+
 class Transcript {
  public:
   Transcript() {
@@ -74,6 +91,26 @@ class Transcript {
     return v & ((1u << bits) - 1);
   }
   const std::vector<uint8_t>& tape() const { return tape_; }
+
+  void save(TranscriptState& st) const {
+    memset(&st, 0, sizeof(st));
+    uint8_t blk[64];
+    hasher_.save(st.h, blk, st.block_len, st.total);
+    for (uint32_t i = 0; i < st.block_len; i++) st.w[i >> 2] |= (uint32_t)blk[i] << (24 - 8 * (i & 3));
+    st.sampling = sampling_ ? 1u : 0u;
+    st.index = index_;
+    for (int i = 0; i < 32; i++) st.buf[i >> 2] |= (uint32_t)buffer_[i] << (8 * (i & 3));
+  }
+  // Takes over a state the device advanced and appends the tape bytes it wrote.
+  void load(const TranscriptState& st, const uint8_t* tape) {
+    uint8_t blk[64];
+    for (int i = 0; i < 64; i++) blk[i] = (uint8_t)(st.w[i >> 2] >> (24 - 8 * (i & 3)));
+    hasher_.load(st.h, blk, st.block_len, st.total);
+    sampling_ = st.sampling != 0;
+    index_ = st.index;
+    for (int i = 0; i < 32; i++) buffer_[i] = (uint8_t)(st.buf[i >> 2] >> (8 * (i & 3)));
+    tape_.insert(tape_.end(), tape, tape + st.tape_len);
+  }
 
  private:
   void to_observer() {
