@@ -30,6 +30,7 @@
 #include "cs.h"
 #include "dev_transcript.cuh"
 #include "gf128.cuh"
+#include "gf_reduce.cuh"
 #include "internal.h"
 #include "kernels.h"
 #include "reductions.h"
@@ -403,7 +404,7 @@ struct AndRoundConst {
 // The Fiat-Shamir step of one MLE-check round, on the device: the round's sums (y_1, y_inf) ->
 // the round polynomial by RoundEvals2::interpolate_eq (prover/prover/src/protocols/sumcheck/
 // round_evals.rs:80-86) -> the truncated proof (c_1, c_2) (mlecheck::RoundProof::truncate) ->
-// the challenge r -> the next claim c_0 + c_1 r + c_2 r^2.  Thread 0 runs the chain; with a
+// the challenge r -> the next claim c_0 + c_1 r + c_2 r^2.  Warp 0 runs the chain; with a
 // table pointer the whole block then builds r's byte table for the next fold.
 __global__ void __launch_bounds__(256)
     and_round_finish_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
@@ -411,23 +412,84 @@ __global__ void __launch_bounds__(256)
                             uint4* __restrict__ claim, uint4* __restrict__ r_out,
                             uint4* __restrict__ tab) {
   __shared__ uint4 r_sh;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
     DevTr st;
     st.load(ts);
     const uint4 y1 = ys[0], yinf = ys[1];
-    const uint4 y0 = gf_mul_1t(gf_add(*claim, gf_mul_1t(y1, rc->alpha)), rc->inv_one_plus_alpha);
+    const uint4 y0 =
+        gf_mul_warp(gf_add(*claim, gf_mul_warp(y1, rc->alpha)), rc->inv_one_plus_alpha);
     const uint4 c0 = y0, c2 = yinf, c1 = gf_add(gf_add(y1, c0), c2);
     const uint4 msg[2] = {c1, c2};
     st.message_elems(tape, msg, 2);
     const uint4 r = st.sample_elem();
     *r_out = r;
-    *claim = gf_add(c0, gf_mul_1t(r, gf_add(c1, gf_mul_1t(c2, r))));
+    *claim = gf_add(c0, gf_mul_warp(r, gf_add(c1, gf_mul_warp(c2, r))));
     st.store(ts);
     r_sh = r;
   }
   if (tab) {
     __syncthreads();
     dt_build_mul_table(r_sh, tab);
+  }
+}
+
+// The small last rounds of the MLE-check in one CTA (see bivariate_tail_kernel): per round fold
+// the three columns (length len -> len/2) by the previous challenge, truncate eq (len/2 -> len/4),
+// evaluate (y_1, y_inf) and let warp 0 run and_round_finish_kernel's Fiat-Shamir step with
+// the round's constants rc[k].
+constexpr int kAndTailThreads = 512;
+__global__ void __launch_bounds__(kAndTailThreads)
+    and_tail_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
+                    uint4* __restrict__ fa, uint4* __restrict__ fb, uint4* __restrict__ fc,
+                    uint4* __restrict__ eq, uint64_t len, uint32_t n_rounds,
+                    const uint4* __restrict__ r_first, const AndRoundConst* __restrict__ rc,
+                    uint4* __restrict__ claim, uint4* __restrict__ chal) {
+  __shared__ uint4 r_sh;
+  DevTr st;
+  uint4 cl = gf_zero();
+  if (threadIdx.x < 32) {
+    st.load(ts);
+    cl = *claim;
+    r_sh = *r_first;
+  }
+  __syncthreads();
+  for (uint32_t k = 0; k < n_rounds; k++) {
+    const uint4 r = r_sh;
+    const uint64_t h = len >> 1, q = len >> 2;
+    for (uint64_t j = threadIdx.x; j < h; j += blockDim.x) {
+      const uint4 a0 = fa[j], b0 = fb[j], c0 = fc[j];
+      fa[j] = gf_add(a0, gf_mul(r, gf_add(fa[h + j], a0)));
+      fb[j] = gf_add(b0, gf_mul(r, gf_add(fb[h + j], b0)));
+      fc[j] = gf_add(c0, gf_mul(r, gf_add(fc[h + j], c0)));
+    }
+    for (uint64_t j = threadIdx.x; j < q; j += blockDim.x) eq[j] = gf_add(eq[j], eq[q + j]);
+    len = h;
+    __syncthreads();
+    uint4 v[2] = {gf_zero(), gf_zero()};
+    for (uint64_t j = threadIdx.x; j < q; j += blockDim.x) {
+      const uint4 e = eq[j];
+      const uint4 a0 = fa[j], a1 = fa[q + j], b0 = fb[j], b1 = fb[q + j], c1 = fc[q + j];
+      gf_add_into(v[0], gf_mul(e, gf_add(gf_mul(a1, b1), c1)));
+      gf_add_into(v[1], gf_mul(e, gf_mul(gf_add(a0, a1), gf_add(b0, b1))));
+    }
+    block_xor_sum<2>(v);
+    if (threadIdx.x < 32) {
+      const AndRoundConst c = rc[k];
+      const uint4 y1 = v[0], yinf = v[1];
+      const uint4 y0 = gf_mul_warp(gf_add(cl, gf_mul_warp(y1, c.alpha)), c.inv_one_plus_alpha);
+      const uint4 c0 = y0, c2 = yinf, c1 = gf_add(gf_add(y1, c0), c2);
+      const uint4 msg[2] = {c1, c2};
+      st.message_elems(tape, msg, 2);
+      const uint4 rr = st.sample_elem();
+      chal[k] = rr;
+      cl = gf_add(c0, gf_mul_warp(rr, gf_add(c1, gf_mul_warp(c2, rr))));
+      r_sh = rr;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    st.store(ts);
+    *claim = cl;
   }
 }
 
@@ -585,7 +647,14 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
     if (e != cudaSuccess) { rc = cuda_error(e, "round constants"); break; }
     DeviceTranscript dt;
     if ((rc = dt.begin(t, s))) break;
-    for (uint32_t n_rem = log_n; n_rem > 0; n_rem--) {
+    // rounds whose fold starts from at most kTailMaxLen elements run in the single-CTA tail
+    uint32_t tail_n = 0;  // n_rem of the first tail round (0: no tail)
+    for (uint32_t n_rem = log_n - 1; n_rem > 0; n_rem--)
+      if ((2ull << n_rem) <= kTailMaxLen) {
+        tail_n = n_rem;
+        break;
+      }
+    for (uint32_t n_rem = log_n; n_rem > tail_n; n_rem--) {
       const uint32_t k = log_n - n_rem;
       uint32_t* acc = d_acc + 4 * (64 + 2 * k);
       const uint64_t size = 1ull << n_rem;
@@ -612,6 +681,15 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
       count_launch(2);
     }
     if (rc) break;
+    if (tail_n) {
+      const uint32_t k0 = log_n - tail_n;
+      and_tail_kernel<<<1, kAndTailThreads, 0, s>>>(dt.state(), dt.tape(), fa, fb, fc, eq,
+                                                     2ull << tail_n, tail_n, d_chal + k0 - 1,
+                                                     d_consts + k0, d_claim, d_chal + k0);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) { rc = cuda_error(e, "and_tail_kernel"); break; }
+      count_launch();
+    }
     // one read: the transcript, the challenges and the length-2 columns before the final fold
     std::vector<u128h> challenges(log_n);
     uint8_t last[96];  // (lo, hi) of a, b, c

@@ -6,8 +6,9 @@
 // The state is the host Transcript's own (TranscriptState): the same HasherChallenger rules
 // (verifier/transcript/src/fiat_shamir/hasher_challenger.rs:14-200) over the same SHA-256 stream,
 // so a stretch may start and end anywhere in the protocol and the proof bytes do not change.  A
-// device stretch is advanced by ONE thread (the steps are a strict chain); message bytes go to a
-// device tape that the host appends to the proof when the stretch ends.
+// device stretch is advanced by one warp whose lanes hold the same state (the steps are a strict
+// chain; the lanes share the multiplies, see gf_mul_warp); message bytes go to a device tape that
+// the host appends to the proof when the stretch ends.
 #pragma once
 #include <stdint.h>
 
@@ -23,49 +24,42 @@ namespace bgpu {
 // Code run once by a single thread is fetched cold: straight-line code costs an instruction-cache
 // miss every few instructions, which for fully unrolled SHA-256 rounds and inlined GF(2^128)
 // multiplies comes to tens of microseconds per launch.  The scalar protocol steps therefore call
-// one out-of-line copy of each: the multiply (gf_mul_nl) and a compression whose 64 rounds run
-// as 4 passes of a 16-round body.
+// one out-of-line copy of each: the multiply (gf_mul_nl) and the compression
+// (sha256_compress_compact).
 __device__ __forceinline__ uint4 gf_mul_1t(uint4 a, uint4 b) { return gf_mul_nl(a, b); }
 
-static __device__ __noinline__ void sha256_compress_1t(uint32_t* st, const uint32_t* blk) {
-  uint32_t w[16];
+// A product on the critical path of a Fiat-Shamir step, computed by a whole warp: every lane
+// passes the same a and b; lane l < 16 forms the 32x32 carry-less product of word l/4 of a and
+// word l%4 of b, the 16 products are XOR-combined into the eight words of the 256-bit product by
+// shuffle reductions, and every lane returns the reduced product.  One multiply's latency is
+// then one clmul32 plus the shuffles instead of nine dependent clmul32 on one thread; one
+// out-of-line copy keeps the launch's cold instruction fetch small.
+static __device__ __noinline__ uint4 gf_mul_warp(uint4 a, uint4 b) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t i = (lane >> 2) & 3, j = lane & 3;
+  const uint32_t ai = i == 0 ? a.x : i == 1 ? a.y : i == 2 ? a.z : a.w;
+  const uint32_t bj = j == 0 ? b.x : j == 1 ? b.y : j == 2 ? b.z : b.w;
+  const uint64_t p = lane < 16 ? clmul32(ai, bj) : 0ull;
+  const uint32_t lo = (uint32_t)p, hi = (uint32_t)(p >> 32), k = i + j;
+  uint32_t w[8];
 #pragma unroll
-  for (int i = 0; i < 16; i++) w[i] = blk[i];
-  uint32_t a = st[0], b = st[1], c = st[2], d = st[3], e = st[4], f = st[5], g = st[6], h = st[7];
-#pragma unroll 1
-  for (int t0 = 0; t0 < 64; t0 += 16) {
+  for (uint32_t q = 0; q < 8; q++) {
+    uint32_t v = (k == q ? lo : 0u) ^ (k + 1 == q ? hi : 0u);
 #pragma unroll
-    for (int j = 0; j < 16; j++) {
-      if (t0) {  // message schedule, w[j] = W[t - 16] becomes W[t]
-        const uint32_t w15 = w[(j + 1) & 15], w2 = w[(j + 14) & 15];
-        const uint32_t s0 = rotr32(w15, 7) ^ rotr32(w15, 18) ^ (w15 >> 3);
-        const uint32_t s1 = rotr32(w2, 17) ^ rotr32(w2, 19) ^ (w2 >> 10);
-        w[j] += s0 + w[(j + 9) & 15] + s1;
-      }
-      const uint32_t S1 = rotr32(e, 6) ^ rotr32(e, 11) ^ rotr32(e, 25);
-      const uint32_t ch = (e & f) ^ (~e & g);
-      const uint32_t t1 = h + S1 + ch + kSha256K[t0 + j] + w[j];
-      const uint32_t S0 = rotr32(a, 2) ^ rotr32(a, 13) ^ rotr32(a, 22);
-      const uint32_t mj = (a & b) ^ (a & c) ^ (b & c);
-      h = g;
-      g = f;
-      f = e;
-      e = d + t1;
-      d = c;
-      c = b;
-      b = a;
-      a = t1 + S0 + mj;
-    }
+    for (int m = 16; m >= 1; m >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, m);
+    w[q] = v;
   }
-  st[0] += a;
-  st[1] += b;
-  st[2] += c;
-  st[3] += d;
-  st[4] += e;
-  st[5] += f;
-  st[6] += g;
-  st[7] += h;
+  u256 r;
+  r.p0 = ((uint64_t)w[1] << 32) | w[0];
+  r.p1 = ((uint64_t)w[3] << 32) | w[2];
+  r.p2 = ((uint64_t)w[5] << 32) | w[4];
+  r.p3 = ((uint64_t)w[7] << 32) | w[6];
+  return reduce256(r);
 }
+__device__ __forceinline__ void sha256_compress_1t(uint32_t* st, const uint32_t* blk) {
+  sha256_compress_compact(st, blk);
+}
+
 
 // The challenger held in registers by the thread that advances it.  The partial SHA-256 block
 // is kept as 16 big-endian words, zero past `len`, so absorbing a word is a shift/OR into the word
@@ -181,11 +175,13 @@ struct DevTr {
       error = 1;
       return;
     }
-    if ((tape_len & 3u) == 0) {
+    if (threadIdx.x & 31) {  // a warp advancing the transcript together writes from lane 0
+    } else if ((tape_len & 3u) == 0) {
       uint32_t* t32 = reinterpret_cast<uint32_t*>(tape + tape_len);
       for (uint32_t i = 0; i < n; i++) t32[i] = v[i];
     } else {
-      for (uint32_t i = 0; i < 4 * n; i++) tape[tape_len + i] = (uint8_t)(v[i >> 2] >> (8 * (i & 3)));
+      for (uint32_t i = 0; i < 4 * n; i++)
+        tape[tape_len + i] = (uint8_t)(v[i >> 2] >> (8 * (i & 3)));
     }
     tape_len += 4 * n;
   }

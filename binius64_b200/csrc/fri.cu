@@ -104,6 +104,45 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// The same fold with compact code for launches of less than one wave: a kernel whose threads
+// each run it once fetches its instructions cold, so the unrolled variant's ~30 inlined
+// multiplies cost more in instruction fetch than in arithmetic.  Here the rounds and butterflies
+// are loops and the multiply is one out-of-line copy (gf_mul_nl).
+template <int N>
+__global__ void __launch_bounds__(256)
+    fold_codeword_compact_kernel(const uint4* __restrict__ cw, uint32_t log_len,
+                                 const uint4* __restrict__ tw, Challenges ch,
+                                 const uint4* __restrict__ dch, uint4* __restrict__ out) {
+  constexpr uint32_t n = N;
+  const uint64_t n_chunks = 1ull << (log_len - n);
+  for (uint64_t ci = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; ci < n_chunks;
+       ci += (uint64_t)gridDim.x * blockDim.x) {
+    uint4 v[1 << N];
+#pragma unroll 1
+    for (uint32_t j = 0; j < (1u << n); j++) v[j] = __ldg(cw + (ci << n) + j);
+    uint32_t cur = log_len;
+#pragma unroll 1
+    for (uint32_t kk = 0; kk < n; kk++) {
+      const uint32_t size = n - kk;
+      const uint4 r = dch ? dch[kk] : ch.r[kk];
+      const uint64_t layer_base = (1ull << (cur - 1)) - 1;
+#pragma unroll 1
+      for (uint32_t off = 0; off < (1u << (size - 1)); off++) {
+        uint4 u = v[off << 1], w = v[(off << 1) | 1];
+        const uint64_t index = (ci << (size - 1)) | (uint64_t)off;
+        const uint4 t = __ldg(tw + layer_base + index);
+        gf_add_into(w, u);
+        gf_add_into(u, gf_mul_nl(w, t));
+        gf_add_into(w, u);
+        gf_add_into(u, gf_mul_nl(w, r));
+        v[off] = u;
+      }
+      cur--;
+    }
+    out[ci] = v[0];
+  }
+}
+
 __global__ void gf_mul_batch_kernel(const uint4* __restrict__ a, const uint4* __restrict__ b,
                                     uint4* __restrict__ out, uint64_t n) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
@@ -119,11 +158,19 @@ int load_challenges(const void* h, uint32_t n, Challenges& ch) {
   return BINIUS_OK;
 }
 
+// Launches of fewer chunks than this (under one wave of 256-thread blocks on 148 SMs) take the
+// compact kernel.
+constexpr uint64_t kCompactFoldChunks = 148ull * 256;
+
 template <int N>
 void launch_fold_codeword(const uint4* cw, uint32_t log_len, const uint4* tw, const Challenges& ch,
                           const uint4* dch, uint4* out, cudaStream_t s) {
   uint64_t n_chunks = 1ull << (log_len - N);
-  fold_codeword_kernel<N><<<grid_for(n_chunks, 256), 256, 0, s>>>(cw, log_len, tw, ch, dch, out);
+  if (n_chunks < kCompactFoldChunks)
+    fold_codeword_compact_kernel<N><<<grid_for(n_chunks, 256), 256, 0, s>>>(cw, log_len, tw, ch,
+                                                                            dch, out);
+  else
+    fold_codeword_kernel<N><<<grid_for(n_chunks, 256), 256, 0, s>>>(cw, log_len, tw, ch, dch, out);
 }
 
 // ---- Scratch for binius_fri_fold_codeword_noalloc ----

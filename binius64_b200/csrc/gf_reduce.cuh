@@ -44,4 +44,30 @@ __device__ __forceinline__ void block_xor_reduce(uint4 (&v)[NV], uint32_t* dst) 
   }
 }
 
+// XOR-reduces NV field values across the CTA; the lanes of warp 0 get the totals in v.  Every
+// thread must call it; it ends with the CTA synchronised, so it may be called again in a loop.
+template <int NV>
+__device__ __forceinline__ void block_xor_sum(uint4 (&v)[NV]) {
+  __shared__ uint4 red[NV][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; q++) {
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) gf_add_into(v[q], shfl_xor_gf(v[q], m));
+    if (lane == 0) red[q][warp] = v[q];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nwarps = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; q++) {
+      uint4 x = lane < nwarps ? red[q][lane] : gf_zero();
+#pragma unroll
+      for (int m = 16; m >= 1; m >>= 1) gf_add_into(x, shfl_xor_gf(x, m));
+      v[q] = x;
+    }
+  }
+  __syncthreads();
+}
+
 }  // namespace bgpu

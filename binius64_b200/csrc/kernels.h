@@ -48,6 +48,16 @@ class DeviceTranscript;
 int bivariate_round_finish(const DeviceTranscript& dt, const uint4* d_ys, const uint4* d_claim_init,
                            uint4* d_claim, const uint8_t* d_commitment, uint4* d_r_out,
                            uint4* d_tab, cudaStream_t s);
+// The last n_rounds rounds of a plain bivariate product sumcheck in one launch (one CTA): each
+// round folds (a, b) -- of length len before the first fold -- by the previous challenge
+// (d_r_first for the first round, when set) and runs the Fiat-Shamir step of
+// bivariate_round_finish; challenges go to d_chal[0 .. n_rounds), the claim stays in d_claim.
+int bivariate_tail(const DeviceTranscript& dt, uint4* d_a, uint4* d_b, uint64_t len,
+                   uint32_t n_rounds, const uint4* d_r_first, uint4* d_claim, uint4* d_chal,
+                   cudaStream_t s);
+// Sumcheck rounds whose arrays have at most this many elements before the fold run in the
+// single-CTA tail kernels.
+constexpr uint64_t kTailMaxLen = 1ull << 11;
 int gather_segments(const GatherSegment* d_segs, uint32_t n, uint8_t* d_dst, cudaStream_t s);
 // d_tab (16 * 256 elements) = the byte table of multiplication by r (gf_mul_table).
 int build_mul_table(const uint8_t r[16], uint4* d_tab, cudaStream_t s);

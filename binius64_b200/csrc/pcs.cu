@@ -9,6 +9,7 @@
 // (fri/fold.rs:221-244, fri/query.rs:51-134) gathered into one buffer by a single kernel.
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "dev_transcript.cuh"
@@ -290,7 +291,19 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
       DeviceTranscript dt;
       if ((rc = dt.begin(t, s))) break;
       uint32_t tape_bytes = 0;
-      for (uint32_t round = 0; round < n && rc == BINIUS_OK; round++) {
+      // the rounds after the last FRI commit inside the loop whose fold starts from at most
+      // kTailMaxLen elements run in the single-CTA tail
+      uint32_t tail0 = 1;
+      {
+        uint32_t c = P->log_batch;
+        if (c < n) tail0 = std::max(tail0, c + 1);
+        for (uint32_t a_i : P->arities) {
+          c += a_i;
+          if (c < n) tail0 = std::max(tail0, c + 1);
+        }
+        while (tail0 < n && (N >> (tail0 - 1)) > kTailMaxLen) tail0++;
+      }
+      for (uint32_t round = 0; round < tail0 && round < n && rc == BINIUS_OK; round++) {
         const uint64_t size = N >> round;
         uint32_t* ys = reinterpret_cast<uint32_t*>(slots + 2 * round);
         if (round == 0)
@@ -311,6 +324,13 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
         fri.receive();
       }
       if (rc) break;
+      if (tail0 < n) {
+        if ((rc = bivariate_tail(dt, a, b, N >> (tail0 - 1), n - tail0, chal + tail0 - 1, claim,
+                                 chal + tail0, s)))
+          break;
+        for (uint32_t round = tail0; round < n; round++) fri.receive();
+        tape_bytes += 32 * (n - tail0);
+      }
       bool committed = false;
       const uint8_t* d_root = nullptr;
       if ((rc = fri.execute(&committed, &d_root))) break;

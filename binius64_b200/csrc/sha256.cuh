@@ -71,6 +71,49 @@ __device__ __forceinline__ void sha256_compress(uint32_t s[8], uint32_t w[16]) {
   s[7] += h;
 }
 
+// The same compression as one out-of-line copy whose 64 rounds run as 4 passes of a 16-round
+// body, for code that runs on few threads once per launch (small trees, the device transcript):
+// there the fully unrolled form costs more in cold instruction fetch than in arithmetic.
+static __device__ __noinline__ void sha256_compress_compact(uint32_t* st, const uint32_t* blk) {
+  uint32_t w[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) w[i] = blk[i];
+  uint32_t a = st[0], b = st[1], c = st[2], d = st[3], e = st[4], f = st[5], g = st[6], h = st[7];
+#pragma unroll 1
+  for (int t0 = 0; t0 < 64; t0 += 16) {
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      if (t0) {  // message schedule, w[j] = W[t - 16] becomes W[t]
+        const uint32_t w15 = w[(j + 1) & 15], w2 = w[(j + 14) & 15];
+        const uint32_t s0 = rotr32(w15, 7) ^ rotr32(w15, 18) ^ (w15 >> 3);
+        const uint32_t s1 = rotr32(w2, 17) ^ rotr32(w2, 19) ^ (w2 >> 10);
+        w[j] += s0 + w[(j + 9) & 15] + s1;
+      }
+      const uint32_t S1 = rotr32(e, 6) ^ rotr32(e, 11) ^ rotr32(e, 25);
+      const uint32_t ch = (e & f) ^ (~e & g);
+      const uint32_t t1 = h + S1 + ch + kSha256K[t0 + j] + w[j];
+      const uint32_t S0 = rotr32(a, 2) ^ rotr32(a, 13) ^ rotr32(a, 22);
+      const uint32_t mj = (a & b) ^ (a & c) ^ (b & c);
+      h = g;
+      g = f;
+      f = e;
+      e = d + t1;
+      d = c;
+      c = b;
+      b = a;
+      a = t1 + S0 + mj;
+    }
+  }
+  st[0] += a;
+  st[1] += b;
+  st[2] += c;
+  st[3] += d;
+  st[4] += e;
+  st[5] += f;
+  st[6] += g;
+  st[7] += h;
+}
+
 __device__ __forceinline__ void sha256_init(uint32_t s[8]) {
   s[0] = 0x6a09e667u;
   s[1] = 0xbb67ae85u;
@@ -84,6 +127,7 @@ __device__ __forceinline__ void sha256_init(uint32_t s[8]) {
 
 // SHA-256 of n_elems consecutive 16-byte elements.  out receives the digest as the 8 words that,
 // stored little-endian, give the standard digest bytes.
+template <bool COMPACT = false>
 __device__ __forceinline__ void sha256_elems(const uint4* __restrict__ p, uint32_t n_elems,
                                              uint32_t out[8]) {
   uint32_t s[8];
@@ -99,7 +143,7 @@ __device__ __forceinline__ void sha256_elems(const uint4* __restrict__ p, uint32
       w[4 * q + 2] = bswap32(v.z);
       w[4 * q + 3] = bswap32(v.w);
     }
-    sha256_compress(s, w);
+    if constexpr (COMPACT) sha256_compress_compact(s, w); else sha256_compress(s, w);
   }
   // Final block: the 0, 1, 2 or 3 trailing elements (at most 48 bytes), 0x80, zeros and the
   // 64-bit big-endian bit length always fit in one block.
@@ -122,13 +166,14 @@ __device__ __forceinline__ void sha256_elems(const uint4* __restrict__ p, uint32
   uint64_t bits = (uint64_t)n_elems * 128u;
   w[14] = (uint32_t)(bits >> 32);
   w[15] = (uint32_t)bits;
-  sha256_compress(s, w);
+  if constexpr (COMPACT) sha256_compress_compact(s, w); else sha256_compress(s, w);
 #pragma unroll
   for (int i = 0; i < 8; i++) out[i] = bswap32(s[i]);
 }
 
 // Binius node compression of two 32-byte digests given as little-endian-loaded words; the result
 // words, stored little-endian, are the node digest bytes.
+template <bool COMPACT = false>
 __device__ __forceinline__ void compress_node(const NodeIV& iv, const uint32_t left[8],
                                               const uint32_t right[8], uint32_t out[8]) {
   uint32_t s[8];
@@ -140,7 +185,7 @@ __device__ __forceinline__ void compress_node(const NodeIV& iv, const uint32_t l
     w[i] = bswap32(left[i]);
     w[8 + i] = bswap32(right[i]);
   }
-  sha256_compress(s, w);
+  if constexpr (COMPACT) sha256_compress_compact(s, w); else sha256_compress(s, w);
 #pragma unroll
   for (int i = 0; i < 8; i++) out[i] = s[i];
 }

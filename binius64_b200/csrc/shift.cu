@@ -258,44 +258,133 @@ __global__ void __launch_bounds__(256)
                               uint4* __restrict__ st3, uint4* __restrict__ r_out,
                               uint4* __restrict__ tab) {
   __shared__ uint4 r_sh;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
     DevTr st;
     st.load(ts);
     const ShiftRoundConst c = *rc;
     uint4 inout = st3[1];
     if (init_lohi)
-      inout = gf_add(init_lohi[0], gf_mul_1t(gf_add(init_lohi[1], init_lohi[0]), z0));
+      inout = gf_add(init_lohi[0], gf_mul_warp(gf_add(init_lohi[1], init_lohi[0]), z0));
     const uint4 y1 = ys[0], yinf = ys[1], lo = ys[2], hi = ys[3];
     const uint4 s0 = gf_add(st3[0], y1), s2 = yinf, s1 = gf_add(gf_add(y1, s0), s2);
     uint4 iy0, iy1;
     if (c.early) {
-      iy1 = gf_add(lo, gf_mul_1t(gf_add(hi, lo), c.zc));
+      iy1 = gf_add(lo, gf_mul_warp(gf_add(hi, lo), c.zc));
       iy0 = inout;
     } else {
       iy1 = lo;
-      iy0 = gf_mul_1t(gf_add(inout, gf_mul_1t(iy1, c.zc)), c.inv_one_plus_zc);
+      iy0 = gf_mul_warp(gf_add(inout, gf_mul_warp(iy1, c.zc)), c.inv_one_plus_zc);
     }
     const uint4 q0 = iy0, q1 = gf_add(iy1, iy0);
     uint4 one_a = c.alpha_dec;
     one_a.x ^= 1u;
     const uint4 eqp = st3[2];
-    const uint4 d0 = gf_mul_1t(gf_mul_1t(q0, one_a), eqp);
-    const uint4 d1 = gf_mul_1t(gf_add(gf_mul_1t(q1, one_a), q0), eqp);
-    const uint4 msg[2] = {gf_add(s0, gf_mul_1t(beta, d0)), gf_add(s1, gf_mul_1t(beta, d1))};
+    const uint4 d0 = gf_mul_warp(gf_mul_warp(q0, one_a), eqp);
+    const uint4 d1 = gf_mul_warp(gf_add(gf_mul_warp(q1, one_a), q0), eqp);
+    const uint4 msg[2] = {gf_add(s0, gf_mul_warp(beta, d0)), gf_add(s1, gf_mul_warp(beta, d1))};
     st.message_elems(tape, msg, 2);
     const uint4 r = st.sample_elem();
     *r_out = r;
-    st3[0] = gf_add(s0, gf_mul_1t(r, gf_add(s1, gf_mul_1t(s2, r))));
-    st3[1] = gf_add(q0, gf_mul_1t(q1, r));
+    st3[0] = gf_add(s0, gf_mul_warp(r, gf_add(s1, gf_mul_warp(s2, r))));
+    st3[1] = gf_add(q0, gf_mul_warp(q1, r));
     uint4 f = gf_add(r, c.alpha_dec);
     f.x ^= 1u;
-    st3[2] = gf_mul_1t(eqp, f);
+    st3[2] = gf_mul_warp(eqp, f);
     st.store(ts);
     r_sh = r;
   }
   if (tab) {
     __syncthreads();
     dt_build_mul_table(r_sh, tab);
+  }
+}
+
+// The small last rounds of phase 2 in one CTA (see bivariate_tail_kernel).  Round n_rem folds
+// (W, M) from 2^(n_rem+1) to 2^n_rem elements by the previous challenge, evaluates the product
+// round, takes the in/out check's two dot products with eq_pub and lets warp 0 run
+// shift_round_finish_kernel's Fiat-Shamir step.  eq_pub holds eq(z[0 .. m)) with m = p - 1 while
+// rounds are early (p < n_rem), then m = n_rem - 1: summing the two halves of eq(z[0 .. m))
+// gives eq(z[0 .. m - 1)), so later rounds shrink it in place.  On entry eq_pub is right for
+// the first round.
+constexpr int kShiftTailThreads = 512;
+__global__ void __launch_bounds__(kShiftTailThreads)
+    shift_tail_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
+                      uint4* __restrict__ W, uint4* __restrict__ M, uint4* __restrict__ eq_pub,
+                      uint32_t n_rem0, uint32_t p, const uint4* __restrict__ r_first,
+                      const ShiftRoundConst* __restrict__ rc, uint4 beta, uint4* __restrict__ run,
+                      uint4* __restrict__ chal) {
+  __shared__ uint4 r_sh;
+  DevTr st;
+  uint4 sum = gf_zero(), inout = gf_zero(), eqp = gf_zero();
+  if (threadIdx.x < 32) {
+    st.load(ts);
+    sum = run[0];
+    inout = run[1];
+    eqp = run[2];
+    r_sh = *r_first;
+  }
+  __syncthreads();
+  for (uint32_t k = 0, n_rem = n_rem0; n_rem > 0; k++, n_rem--) {
+    const uint4 r = r_sh;
+    const uint64_t h = 1ull << n_rem, half = h >> 1;
+    for (uint64_t j = threadIdx.x; j < h; j += blockDim.x) {
+      const uint4 w0 = W[j], m0 = M[j];
+      W[j] = gf_add(w0, gf_mul(r, gf_add(W[h + j], w0)));
+      M[j] = gf_add(m0, gf_mul(r, gf_add(M[h + j], m0)));
+    }
+    const bool early = p < n_rem;
+    if (k > 0 && n_rem < p)
+      for (uint64_t i = threadIdx.x; i < half; i += blockDim.x)
+        eq_pub[i] = gf_add(eq_pub[i], eq_pub[half + i]);
+    __syncthreads();
+    uint4 v[4] = {gf_zero(), gf_zero(), gf_zero(), gf_zero()};
+    for (uint64_t j = threadIdx.x; j < half; j += blockDim.x) {
+      const uint4 w0 = W[j], w1 = W[half + j], m0 = M[j], m1 = M[half + j];
+      gf_add_into(v[0], gf_mul(w1, m1));
+      gf_add_into(v[1], gf_mul(gf_add(w0, w1), gf_add(m0, m1)));
+    }
+    const uint64_t E = early ? 1ull << (p - 1) : half;
+    for (uint64_t i = threadIdx.x; i < E; i += blockDim.x) {
+      const uint4 e = eq_pub[i];
+      gf_add_into(v[2], gf_mul(W[half + i], e));
+      if (early) gf_add_into(v[3], gf_mul(W[half + E + i], e));
+    }
+    block_xor_sum<4>(v);
+    if (threadIdx.x < 32) {
+      const ShiftRoundConst c = rc[k];
+      const uint4 y1 = v[0], yinf = v[1], lo = v[2], hi = early ? v[3] : v[2];
+      const uint4 s0 = gf_add(sum, y1), s2 = yinf, s1 = gf_add(gf_add(y1, s0), s2);
+      uint4 iy0, iy1;
+      if (c.early) {
+        iy1 = gf_add(lo, gf_mul_warp(gf_add(hi, lo), c.zc));
+        iy0 = inout;
+      } else {
+        iy1 = lo;
+        iy0 = gf_mul_warp(gf_add(inout, gf_mul_warp(iy1, c.zc)), c.inv_one_plus_zc);
+      }
+      const uint4 q0 = iy0, q1 = gf_add(iy1, iy0);
+      uint4 one_a = c.alpha_dec;
+      one_a.x ^= 1u;
+      const uint4 d0 = gf_mul_warp(gf_mul_warp(q0, one_a), eqp);
+      const uint4 d1 = gf_mul_warp(gf_add(gf_mul_warp(q1, one_a), q0), eqp);
+      const uint4 msg[2] = {gf_add(s0, gf_mul_warp(beta, d0)), gf_add(s1, gf_mul_warp(beta, d1))};
+      st.message_elems(tape, msg, 2);
+      const uint4 rr = st.sample_elem();
+      chal[k] = rr;
+      sum = gf_add(s0, gf_mul_warp(rr, gf_add(s1, gf_mul_warp(s2, rr))));
+      inout = gf_add(q0, gf_mul_warp(q1, rr));
+      uint4 f = gf_add(rr, c.alpha_dec);
+      f.x ^= 1u;
+      eqp = gf_mul_warp(eqp, f);
+      r_sh = rr;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    st.store(ts);
+    run[0] = sum;
+    run[1] = inout;
+    run[2] = eqp;
   }
 }
 
@@ -458,7 +547,10 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
   SHIFT_TRY(launched("dot2_kernel"));
   DeviceTranscript dt;
   SHIFT_TRY(dt.begin(t, s));
-  for (int round = 0; round < 12; round++) {
+  // rounds whose fold starts from at most kTailMaxLen elements run in the single-CTA tail
+  int tail0 = 1;
+  while (((uint64_t)kFlat >> (tail0 - 1)) > kTailMaxLen) tail0++;
+  for (int round = 0; round < tail0; round++) {
     const uint64_t size = (uint64_t)kFlat >> round;  // before this round's fold
     uint32_t* ys = reinterpret_cast<uint32_t*>(slots + 2 * round);
     if (round == 0) {
@@ -473,6 +565,8 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
                                      round == 0 ? reinterpret_cast<const uint4*>(acc + 8) : nullptr,
                                      dstate, nullptr, chal + round, next_tab ? tab : nullptr, s));
   }
+  SHIFT_TRY(bivariate_tail(dt, g, h, (uint64_t)kFlat >> (tail0 - 1), 12 - tail0, chal + tail0 - 1,
+                           dstate, chal + tail0, s));
   // one read: transcript, challenges and the remaining 16-element g and h
   std::vector<hu128> ch1(12);
   hu128 gamma = 0;
@@ -560,7 +654,14 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
     BGPU_CUDA(cudaMemcpyAsync(run, init3, sizeof(init3), cudaMemcpyHostToDevice, s));
   }
   SHIFT_TRY(dt.begin(t, s));
-  for (uint32_t n_rem = log_words; n_rem > 0; n_rem--) {
+  // rounds whose fold starts from at most kTailMaxLen elements run in the single-CTA tail
+  uint32_t tail_n = 0;  // n_rem of the first tail round (0: no tail)
+  for (uint32_t n_rem = log_words - 1; n_rem > 0; n_rem--)
+    if ((2ull << n_rem) <= kTailMaxLen) {
+      tail_n = n_rem;
+      break;
+    }
+  for (uint32_t n_rem = log_words; n_rem > tail_n; n_rem--) {
     const uint32_t k = log_words - n_rem;
     const uint64_t half = 1ull << (n_rem - 1);
     uint4* ys = slots2 + 4 * k;
@@ -583,6 +684,14 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
         dt.state(), dt.tape(), ys, rconst + k, n_rem == log_words ? init_lohi : nullptr, z0,
         u4(beta), run, chal + 12 + k, next_tab ? tab : nullptr);
     SHIFT_TRY(launched("shift_round_finish_kernel"));
+  }
+  if (tail_n) {
+    const uint32_t k0 = log_words - tail_n;
+    if (tail_n <= p) SHIFT_TRY(eq_tensor(to_u4(z).data(), tail_n - 1, eq_pub, s));
+    shift_tail_kernel<<<1, kShiftTailThreads, 0, s>>>(dt.state(), dt.tape(), W, M, eq_pub, tail_n,
+                                                      p, chal + 12 + k0 - 1, rconst + k0, u4(beta),
+                                                      run, chal + 12 + k0);
+    SHIFT_TRY(launched("shift_tail_kernel"));
   }
   {
     std::vector<hu128> ch2(log_words);

@@ -30,6 +30,7 @@ using namespace bgpu;
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kTailThreads = 512;
 
 uint4 gf_zero_host() { return make_uint4(0u, 0u, 0u, 0u); }
 
@@ -38,17 +39,21 @@ unsigned grid_for(uint64_t n, unsigned threads, unsigned max_blocks = 148 * 8) {
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, max_blocks));
 }
 
+// out[j] = prod_i (bit_i(j) ? r_i : 1 + r_i).  The n factors are multiplied as a balanced tree
+// (depth ceil(log2 n) instead of a chain of n dependent multiplies), out of line: these tensors are
+// small and on the protocol's critical path, so latency and code size matter, not throughput.
 __global__ void eq_small_kernel(uint4* __restrict__ out, Point32 p, uint32_t off, uint32_t n) {
   const uint64_t total = 1ull << n;
   for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < total;
        j += (uint64_t)gridDim.x * blockDim.x) {
-    uint4 acc = gf_one();
+    uint4 f[32];
     for (uint32_t i = 0; i < n; i++) {
-      uint4 f = p.r[off + i];
-      if (!((j >> i) & 1)) f.x ^= 1u;
-      acc = gf_mul(acc, f);
+      f[i] = p.r[off + i];
+      if (!((j >> i) & 1)) f[i].x ^= 1u;
     }
-    out[j] = acc;
+    for (uint32_t step = 1; step < n; step <<= 1)
+      for (uint32_t i = 0; i + step < n; i += 2 * step) f[i] = gf_mul_nl(f[i], f[i + step]);
+    out[j] = n ? f[0] : gf_one();
   }
 }
 
@@ -195,7 +200,7 @@ __global__ void __launch_bounds__(256)
                                   uint4* __restrict__ claim, const uint8_t* __restrict__ commitment,
                                   uint4* __restrict__ r_out, uint4* __restrict__ tab) {
   __shared__ uint4 r_sh;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
     DevTr st;
     st.load(ts);
     const uint4 y1 = ys[0], yinf = ys[1];
@@ -210,13 +215,71 @@ __global__ void __launch_bounds__(256)
     }
     const uint4 r = st.sample_elem();
     *r_out = r;
-    *claim = gf_add(c0, gf_mul_1t(r, gf_add(c1, gf_mul_1t(c2, r))));
+    *claim = gf_add(c0, gf_mul_warp(r, gf_add(c1, gf_mul_warp(c2, r))));
     st.store(ts);
     r_sh = r;
   }
   if (tab) {
     __syncthreads();
     dt_build_mul_table(r_sh, tab);
+  }
+}
+
+// The small last rounds of a plain bivariate product sumcheck in one CTA: per round, fold (a, b)
+// by the previous challenge (r_first for the first round when set), evaluate (y_1, y_inf) on the
+// folded arrays, and let warp 0 run the Fiat-Shamir step of bivariate_round_finish_kernel with
+// the transcript held in its registers.  The rounds of a sumcheck below a few thousand elements
+// are latency chains; run as one launch, the loop body stays in the instruction cache and no
+// launch gap separates the rounds.  len is the arrays' length before the first fold.
+__global__ void __launch_bounds__(kTailThreads)
+    bivariate_tail_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
+                          uint4* __restrict__ a, uint4* __restrict__ b, uint64_t len,
+                          uint32_t n_rounds, const uint4* __restrict__ r_first,
+                          uint4* __restrict__ claim, uint4* __restrict__ chal) {
+  __shared__ uint4 r_sh;
+  DevTr st;
+  uint4 cl = gf_zero();
+  if (threadIdx.x < 32) {
+    st.load(ts);
+    cl = *claim;
+    if (r_first) r_sh = *r_first;
+  }
+  __syncthreads();
+  for (uint32_t k = 0; k < n_rounds; k++) {
+    if (k > 0 || r_first) {
+      const uint4 r = r_sh;
+      const uint64_t h = len >> 1;
+      for (uint64_t j = threadIdx.x; j < h; j += blockDim.x) {
+        const uint4 a0 = a[j], b0 = b[j];
+        a[j] = gf_add(a0, gf_mul(r, gf_add(a[h + j], a0)));
+        b[j] = gf_add(b0, gf_mul(r, gf_add(b[h + j], b0)));
+      }
+      len = h;
+      __syncthreads();
+    }
+    const uint64_t h = len >> 1;
+    uint4 v[2] = {gf_zero(), gf_zero()};
+    for (uint64_t j = threadIdx.x; j < h; j += blockDim.x) {
+      const uint4 a0 = a[j], a1 = a[h + j], b0 = b[j], b1 = b[h + j];
+      gf_add_into(v[0], gf_mul(a1, b1));
+      gf_add_into(v[1], gf_mul(gf_add(a0, a1), gf_add(b0, b1)));
+    }
+    block_xor_sum<2>(v);
+    if (threadIdx.x < 32) {
+      const uint4 y1 = v[0], yinf = v[1];
+      const uint4 c0 = gf_add(cl, y1), c2 = yinf, c1 = gf_add(gf_add(y1, c0), c2);
+      const uint4 msg[2] = {c0, c1};
+      st.message_elems(tape, msg, 2);
+      const uint4 r = st.sample_elem();
+      chal[k] = r;
+      cl = gf_add(c0, gf_mul_warp(r, gf_add(c1, gf_mul_warp(c2, r))));
+      r_sh = r;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    st.store(ts);
+    *claim = cl;
   }
 }
 
@@ -377,6 +440,19 @@ int bivariate_round_finish(const DeviceTranscript& dt, const uint4* d_ys, const 
   bivariate_round_finish_kernel<<<1, 256, 0, s>>>(dt.state(), dt.tape(), d_ys, d_claim_init,
                                                   d_claim, d_commitment, d_r_out, d_tab);
   BGPU_LAUNCH_CHECK("bivariate_round_finish_kernel");
+  count_launch();
+  return BINIUS_OK;
+}
+
+int bivariate_tail(const DeviceTranscript& dt, uint4* d_a, uint4* d_b, uint64_t len,
+                   uint32_t n_rounds, const uint4* d_r_first, uint4* d_claim, uint4* d_chal,
+                   cudaStream_t s) {
+  if (n_rounds == 0) return BINIUS_OK;
+  if ((len >> (n_rounds - (d_r_first ? 0 : 1))) < 2)
+    return set_error(BINIUS_E_ARG, "bivariate tail: more rounds than variables");
+  bivariate_tail_kernel<<<1, kTailThreads, 0, s>>>(dt.state(), dt.tape(), d_a, d_b, len, n_rounds,
+                                                   d_r_first, d_claim, d_chal);
+  BGPU_LAUNCH_CHECK("bivariate_tail_kernel");
   count_launch();
   return BINIUS_OK;
 }

@@ -96,7 +96,8 @@ class Transcript {
     memset(&st, 0, sizeof(st));
     uint8_t blk[64];
     hasher_.save(st.h, blk, st.block_len, st.total);
-    for (uint32_t i = 0; i < st.block_len; i++) st.w[i >> 2] |= (uint32_t)blk[i] << (24 - 8 * (i & 3));
+    for (uint32_t i = 0; i < st.block_len; i++)
+      st.w[i >> 2] |= (uint32_t)blk[i] << (24 - 8 * (i & 3));
     st.sampling = sampling_ ? 1u : 0u;
     st.index = index_;
     for (int i = 0; i < 32; i++) st.buf[i >> 2] |= (uint32_t)buffer_[i] << (8 * (i & 3));
