@@ -63,7 +63,29 @@ __device__ __forceinline__ const uint4* eq_of_class(uint32_t key, const uint4* e
   return (key & 7) < 3 ? eq_and : eq_mul;
 }
 
+// 8x8 bit-matrix transpose (byte i of x is row i): byte k of the result holds bit k of every
+// input byte, bit i from byte i (Hacker's Delight 7-3).
+__device__ __forceinline__ uint64_t transpose8x8(uint64_t x) {
+  uint64_t t = (x ^ (x >> 7)) & 0x00AA00AA00AA00AAull;
+  x ^= t ^ (t << 7);
+  t = (x ^ (x >> 14)) & 0x0000CCCC0000CCCCull;
+  x ^= t ^ (t << 14);
+  t = (x ^ (x >> 28)) & 0x00000000F0F0F0F0ull;
+  x ^= t ^ (t << 28);
+  return x;
+}
+
 // g_raw[key * 64 + j] += sum over terms with that key of eq[c] * bit_j(word).
+//
+// A tile of 256 key-sorted terms is staged in shared memory as 32 chunks of 8.  For each chunk the
+// CTA first builds (a) its 64 bit-column bytes, byte j holding bit j of the chunk's 8 words (one
+// 8x8 bit transpose per thread), and (b) two 16-entry tables of XOR combinations of the chunk's
+// eq values (terms 0-3 and 4-7), a method-of-four-Russians split of the 0/1 x GF(2^128) product.
+// Then each 64-thread group walks its 8 chunks with thread j owning bit position j: a chunk whose
+// 8 terms share one key costs one byte load and two table lookups; a chunk that straddles a key
+// boundary falls back to per-term masked XORs.  A group flushes its accumulators with atomicXor
+// when the key changes.
+constexpr uint32_t kChunk = 8, kChunks = kTile / kChunk;
 __global__ void __launch_bounds__(kTile)
     shift_g_kernel(const uint32_t* __restrict__ vi, const uint32_t* __restrict__ cidx,
                    const uint16_t* __restrict__ keys, uint64_t n,
@@ -72,39 +94,91 @@ __global__ void __launch_bounds__(kTile)
   __shared__ uint4 s_eq[kTile];
   __shared__ uint64_t s_w[kTile];
   __shared__ uint32_t s_key[kTile];
-  const uint32_t j = threadIdx.x & 63, grp = threadIdx.x >> 6;
+  __shared__ uint8_t s_col[kChunks][64];
+  __shared__ uint4 s_tab[kChunks][2][16];
+  const uint32_t tid = threadIdx.x, j = tid & 63, grp = tid >> 6;
   uint32_t cur = kNoKey;
   uint4 acc = gf_zero();
-  const uint64_t n_tiles = (n + kTile - 1) / kTile;
-  for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-    const uint64_t t = tile * kTile + threadIdx.x;
-    __syncthreads();
-    if (t < n) {
-      const uint32_t k = keys[t];
-      s_key[threadIdx.x] = k;
-      s_eq[threadIdx.x] = __ldg(eq_of_class(k, eq_and, eq_mul) + cidx[t]);
-      s_w[threadIdx.x] = __ldg(words + vi[t]);
+  auto switch_key = [&](uint32_t k) {
+    if (k != cur) {
+      if (cur != kNoKey) atomic_xor_gf(g_raw + 4 * ((uint64_t)cur * 64 + j), acc);
+      cur = k;
+      acc = gf_zero();
+    }
+  };
+  // each CTA takes a contiguous range of tiles: the terms are sorted by key, so a group's key
+  // (and its flush of 64 accumulators) changes only at key boundaries
+  const uint64_t n_tiles_all = (n + kTile - 1) / kTile;
+  const uint64_t per = (n_tiles_all + gridDim.x - 1) / gridDim.x;
+  const uint64_t tile0 = (uint64_t)blockIdx.x * per;
+  const uint64_t n_tiles = tile0 + per < n_tiles_all ? tile0 + per : n_tiles_all;
+  // the gathers of a tile (eq value and word of each term) are issued one tile ahead, so their
+  // latency overlaps the previous tile's work
+  uint32_t nk = kNoKey;
+  uint4 ne = gf_zero();
+  uint64_t nw = 0;
+  auto fetch = [&](uint64_t tile) {
+    const uint64_t t = tile * kTile + tid;
+    if (tile < n_tiles && t < n) {
+      nk = keys[t];
+      ne = __ldg(eq_of_class(nk, eq_and, eq_mul) + cidx[t]);
+      nw = __ldg(words + vi[t]);
     } else {
-      s_key[threadIdx.x] = kNoKey;
-      s_eq[threadIdx.x] = gf_zero();
-      s_w[threadIdx.x] = 0;
+      nk = kNoKey;
+      ne = gf_zero();
+      nw = 0;
+    }
+  };
+  fetch(tile0);
+  for (uint64_t tile = tile0; tile < n_tiles; tile++) {
+    __syncthreads();
+    s_key[tid] = nk;
+    s_eq[tid] = ne;
+    s_w[tid] = nw;
+    fetch(tile + 1);
+    __syncthreads();
+    {  // bit columns: thread (chunk c, byte block b)
+      const uint32_t c = tid >> 3, b = tid & 7;
+      uint64_t x = 0;
+#pragma unroll
+      for (uint32_t i = 0; i < 8; i++) x |= ((s_w[c * 8 + i] >> (8 * b)) & 0xffull) << (8 * i);
+      x = transpose8x8(x);
+#pragma unroll
+      for (uint32_t k = 0; k < 8; k++) s_col[c][8 * b + k] = (uint8_t)(x >> (8 * k));
+    }
+#pragma unroll
+    for (uint32_t q = 0; q < 4; q++) {  // tables: 1024 entries, 4 per thread
+      const uint32_t idx = tid * 4 + q, c = idx >> 5, h = (idx >> 4) & 1, nib = idx & 15;
+      uint4 v = gf_zero();
+#pragma unroll
+      for (uint32_t i = 0; i < 4; i++)
+        if ((nib >> i) & 1) gf_add_into(v, s_eq[c * 8 + 4 * h + i]);
+      s_tab[c][h][nib] = v;
     }
     __syncthreads();
-#pragma unroll 4
-    for (int q = 0; q < 64; q++) {
-      const int e = grp * 64 + q;
-      const uint32_t k = s_key[e];
-      if (k != cur) {
-        if (cur != kNoKey) atomic_xor_gf(g_raw + 4 * ((uint64_t)cur * 64 + j), acc);
-        cur = k;
-        acc = gf_zero();
+#pragma unroll 2
+    for (uint32_t cc = 0; cc < kChunks / 4; cc++) {
+      const uint32_t c = grp * (kChunks / 4) + cc, e0 = c * 8;
+      const uint32_t k0 = s_key[e0], k7 = s_key[e0 + 7];
+      if (k0 == k7) {
+        switch_key(k0);
+        if (k0 != kNoKey) {
+          const uint32_t byte = s_col[c][j];
+          gf_add_into(acc, s_tab[c][0][byte & 15]);
+          gf_add_into(acc, s_tab[c][1][byte >> 4]);
+        }
+      } else {
+        for (uint32_t i = 0; i < 8; i++) {
+          const uint32_t e = e0 + i;
+          switch_key(s_key[e]);
+          const uint32_t m = 0u - (uint32_t)((s_w[e] >> j) & 1);
+          const uint4 x = s_eq[e];
+          acc.x ^= x.x & m;
+          acc.y ^= x.y & m;
+          acc.z ^= x.z & m;
+          acc.w ^= x.w & m;
+        }
       }
-      const uint32_t m = 0u - (uint32_t)((s_w[e] >> j) & 1);
-      const uint4 x = s_eq[e];
-      acc.x ^= x.x & m;
-      acc.y ^= x.y & m;
-      acc.z ^= x.z & m;
-      acc.w ^= x.w & m;
     }
   }
   if (cur != kNoKey) atomic_xor_gf(g_raw + 4 * ((uint64_t)cur * 64 + j), acc);
