@@ -23,7 +23,6 @@ namespace {
 
 constexpr uint32_t kLeafFuse = 8;  // leaves per CTA = 2^8
 constexpr uint32_t kNodeFuse = 9;  // inputs per CTA = 2^9
-constexpr uint64_t kCompactLeaves = 148ull * 256;  // one wave of 256-leaf CTAs
 
 __host__ __device__ __forceinline__ uint64_t layer_offset(uint32_t L, uint32_t k) {
   return (1ull << (L + 1)) - (1ull << (L + 1 - k));
@@ -41,8 +40,6 @@ __device__ __forceinline__ void load_digest(const uint4* nodes, uint64_t i, uint
 }
 
 // Hashes 2^fused leaves per CTA and compresses `fused` layers above them in shared memory.
-// COMPACT (trees of less than one wave of leaves) uses the out-of-line compression.
-template <bool COMPACT>
 __global__ void __launch_bounds__(256) merkle_leaves_kernel(const uint4* __restrict__ elems,
                                                             uint32_t log_batch,
                                                             uint4* __restrict__ nodes, uint32_t L,
@@ -51,7 +48,7 @@ __global__ void __launch_bounds__(256) merkle_leaves_kernel(const uint4* __restr
   const uint32_t tid = threadIdx.x;
   const uint64_t leaf = (uint64_t)blockIdx.x * blockDim.x + tid;
   uint32_t d[8];
-  sha256_elems<COMPACT>(elems + (leaf << log_batch), 1u << log_batch, d);
+  sha256_elems(elems + (leaf << log_batch), 1u << log_batch, d);
   store_digest(nodes, leaf, d);
 #pragma unroll
   for (int i = 0; i < 8; i++) buf[0][tid][i] = d[i];
@@ -66,7 +63,7 @@ __global__ void __launch_bounds__(256) merkle_leaves_kernel(const uint4* __restr
         l[i] = buf[src][2 * tid][i];
         r[i] = buf[src][2 * tid + 1][i];
       }
-      compress_node<COMPACT>(iv, l, r, o);
+      compress_node(iv, l, r, o);
 #pragma unroll
       for (int i = 0; i < 8; i++) buf[dst][tid][i] = o[i];
       store_digest(nodes, layer_offset(L, lvl) + (uint64_t)blockIdx.x * n + tid, o);
@@ -75,7 +72,6 @@ __global__ void __launch_bounds__(256) merkle_leaves_kernel(const uint4* __restr
 }
 
 // Compresses `fused` layers starting from layer in_level; each CTA reduces 2^fused inputs.
-template <bool COMPACT>
 __global__ void __launch_bounds__(256) merkle_nodes_kernel(uint4* __restrict__ nodes, uint32_t L,
                                                            uint32_t in_level, uint32_t fused,
                                                            NodeIV iv) {
@@ -87,7 +83,7 @@ __global__ void __launch_bounds__(256) merkle_nodes_kernel(uint4* __restrict__ n
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + tid;
     load_digest(nodes, in_off + 2 * i, l);
     load_digest(nodes, in_off + 2 * i + 1, r);
-    compress_node<COMPACT>(iv, l, r, o);
+    compress_node(iv, l, r, o);
     store_digest(nodes, layer_offset(L, in_level + 1) + i, o);
 #pragma unroll
     for (int k = 0; k < 8; k++) buf[1][tid][k] = o[k];
@@ -102,7 +98,7 @@ __global__ void __launch_bounds__(256) merkle_nodes_kernel(uint4* __restrict__ n
         l[k] = buf[src][2 * tid][k];
         r[k] = buf[src][2 * tid + 1][k];
       }
-      compress_node<COMPACT>(iv, l, r, o);
+      compress_node(iv, l, r, o);
 #pragma unroll
       for (int k = 0; k < 8; k++) buf[dst][tid][k] = o[k];
       store_digest(nodes, layer_offset(L, in_level + lvl) + (uint64_t)blockIdx.x * n + tid, o);
@@ -141,24 +137,15 @@ int merkle_commit(const void* d_elems, uint32_t log_leaves, uint32_t log_batch, 
   uint32_t fused = std::min(L, kLeafFuse);
   uint64_t grid = 1ull << (L - fused);
   BGPU_ARG(grid <= 0x7fffffffull, "too many leaves");
-  // trees of less than one wave of leaves are hashed by compact code (see sha256.cuh)
-  const bool compact = (1ull << L) < kCompactLeaves;
-  if (compact)
-    merkle_leaves_kernel<true><<<(unsigned)grid, 1u << fused, 0, stream>>>(
-        static_cast<const uint4*>(d_elems), log_batch, nodes, L, fused, iv);
-  else
-    merkle_leaves_kernel<false><<<(unsigned)grid, 1u << fused, 0, stream>>>(
-        static_cast<const uint4*>(d_elems), log_batch, nodes, L, fused, iv);
+  merkle_leaves_kernel<<<(unsigned)grid, 1u << fused, 0, stream>>>(
+      static_cast<const uint4*>(d_elems), log_batch, nodes, L, fused, iv);
   BGPU_LAUNCH_CHECK("merkle_leaves_kernel");
   count_launch();
   uint32_t level = fused;
   while (level < L) {
     uint32_t f = std::min(L - level, kNodeFuse);
     uint64_t g = 1ull << (L - level - f);
-    if (compact || g < 148)
-      merkle_nodes_kernel<true><<<(unsigned)g, 1u << (f - 1), 0, stream>>>(nodes, L, level, f, iv);
-    else
-      merkle_nodes_kernel<false><<<(unsigned)g, 1u << (f - 1), 0, stream>>>(nodes, L, level, f, iv);
+    merkle_nodes_kernel<<<(unsigned)g, 1u << (f - 1), 0, stream>>>(nodes, L, level, f, iv);
     BGPU_LAUNCH_CHECK("merkle_nodes_kernel");
     count_launch();
     level += f;

@@ -72,8 +72,8 @@ __device__ __forceinline__ void sha256_compress(uint32_t s[8], uint32_t w[16]) {
 }
 
 // The same compression as one out-of-line copy whose 64 rounds run as 4 passes of a 16-round
-// body, for code that runs on few threads once per launch (small trees, the device transcript):
-// there the fully unrolled form costs more in cold instruction fetch than in arithmetic.
+// body, for the device transcript's single-warp steps: there the fully unrolled form costs more
+// in cold instruction fetch than in arithmetic.
 static __device__ __noinline__ void sha256_compress_compact(uint32_t* st, const uint32_t* blk) {
   uint32_t w[16];
 #pragma unroll
@@ -127,7 +127,6 @@ __device__ __forceinline__ void sha256_init(uint32_t s[8]) {
 
 // SHA-256 of n_elems consecutive 16-byte elements.  out receives the digest as the 8 words that,
 // stored little-endian, give the standard digest bytes.
-template <bool COMPACT = false>
 __device__ __forceinline__ void sha256_elems(const uint4* __restrict__ p, uint32_t n_elems,
                                              uint32_t out[8]) {
   uint32_t s[8];
@@ -143,7 +142,7 @@ __device__ __forceinline__ void sha256_elems(const uint4* __restrict__ p, uint32
       w[4 * q + 2] = bswap32(v.z);
       w[4 * q + 3] = bswap32(v.w);
     }
-    if constexpr (COMPACT) sha256_compress_compact(s, w); else sha256_compress(s, w);
+    sha256_compress(s, w);
   }
   // Final block: the 0, 1, 2 or 3 trailing elements (at most 48 bytes), 0x80, zeros and the
   // 64-bit big-endian bit length always fit in one block.
@@ -166,14 +165,13 @@ __device__ __forceinline__ void sha256_elems(const uint4* __restrict__ p, uint32
   uint64_t bits = (uint64_t)n_elems * 128u;
   w[14] = (uint32_t)(bits >> 32);
   w[15] = (uint32_t)bits;
-  if constexpr (COMPACT) sha256_compress_compact(s, w); else sha256_compress(s, w);
+  sha256_compress(s, w);
 #pragma unroll
   for (int i = 0; i < 8; i++) out[i] = bswap32(s[i]);
 }
 
 // Binius node compression of two 32-byte digests given as little-endian-loaded words; the result
 // words, stored little-endian, are the node digest bytes.
-template <bool COMPACT = false>
 __device__ __forceinline__ void compress_node(const NodeIV& iv, const uint32_t left[8],
                                               const uint32_t right[8], uint32_t out[8]) {
   uint32_t s[8];
@@ -185,7 +183,7 @@ __device__ __forceinline__ void compress_node(const NodeIV& iv, const uint32_t l
     w[i] = bswap32(left[i]);
     w[8 + i] = bswap32(right[i]);
   }
-  if constexpr (COMPACT) sha256_compress_compact(s, w); else sha256_compress(s, w);
+  sha256_compress(s, w);
 #pragma unroll
   for (int i = 0; i < 8; i++) out[i] = s[i];
 }
