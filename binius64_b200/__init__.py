@@ -578,6 +578,96 @@ class Prover:
             self._h = None
 
 
+# ---------------------------------------------------------------------------------------- formats
+
+STD_CHALLENGER = "HasherChallenger<Sha256>"  # ChallengerWithName::NAME (verifier/verifier/src/config.rs:19-21)
+
+
+def _size_out():
+    return ctypes.c_size_t(0)
+
+
+class ValuesData:
+    """ValuesData (verifier/core/src/constraint_system.rs:889-990): a run of 64-bit words in the
+    version-1 wire format (u32 version, u32 count, u64 words)."""
+
+    SERIALIZATION_VERSION = 1
+
+    def __init__(self, words):
+        self.words = np.ascontiguousarray(np.asarray(words, dtype=np.uint64))
+
+    def serialize(self) -> bytes:
+        n = _size_out()
+        buf = ctypes.create_string_buffer(8 + 8 * len(self.words))
+        check(lib().binius_values_data_encode(self.words.ctypes.data, len(self.words), buf,
+                                              len(buf), ctypes.byref(n)))
+        return buf.raw[:n.value]
+
+    @classmethod
+    def deserialize(cls, data: bytes) -> "ValuesData":
+        n = _size_out()
+        cap = max(0, (len(data) - 8) // 8)
+        out = np.zeros(max(cap, 1), dtype=np.uint64)
+        check(lib().binius_values_data_decode(data, len(data), out.ctypes.data, cap,
+                                              ctypes.byref(n)))
+        return cls(out[:n.value].copy())
+
+    def __len__(self):
+        return len(self.words)
+
+
+class Proof:
+    """Proof (verifier/core/src/constraint_system.rs:993-1100): the transcript bytes and the
+    challenger type, in the version-1 wire format."""
+
+    SERIALIZATION_VERSION = 1
+
+    def __init__(self, data: bytes, challenger_type: str = STD_CHALLENGER):
+        self.data = bytes(data)
+        self.challenger_type = challenger_type
+
+    def serialize(self) -> bytes:
+        n = _size_out()
+        ch = self.challenger_type.encode()
+        buf = ctypes.create_string_buffer(12 + len(ch) + len(self.data))
+        check(lib().binius_proof_encode(self.data, len(self.data), ch, buf, len(buf),
+                                        ctypes.byref(n)))
+        return buf.raw[:n.value]
+
+    @classmethod
+    def deserialize(cls, data: bytes) -> "Proof":
+        n = _size_out()
+        out = ctypes.create_string_buffer(max(len(data), 1))
+        ch = ctypes.create_string_buffer(max(len(data), 1) + 1)
+        check(lib().binius_proof_decode(data, len(data), out, len(out), ctypes.byref(n), ch,
+                                        len(ch)))
+        return cls(out.raw[:n.value], ch.value.decode())
+
+
+def value_vec_from_data(cs: DeviceConstraintSystem, public, non_public) -> np.ndarray:
+    """ValueVec::new_from_data (verifier/core/src/constraint_system.rs:803-823): the committed words
+    public ++ non_public (their total must be committed_total_len), then n_scratch zero words."""
+    pub = np.ascontiguousarray(np.asarray(public, dtype=np.uint64))
+    npub = np.ascontiguousarray(np.asarray(non_public, dtype=np.uint64))
+    out = np.zeros(cs.committed_total_len + cs.n_scratch, dtype=np.uint64)
+    check(lib().binius_value_vec_from_data(cs.handle, pub.ctypes.data, len(pub), npub.ctypes.data,
+                                           len(npub), out.ctypes.data))
+    return out
+
+
+def load_prove(cs_bytes: bytes, public_bytes: bytes, non_public_bytes: bytes,
+               log_inv_rate: int = 1, device: int | None = None) -> bytes:
+    """The reference prover binary's flow (prover/examples/src/bin/prover.rs:46-99) on the GPU:
+    ConstraintSystem v2 + public / non-public ValuesData v1 in, Proof v1 bytes out."""
+    torch = _torch()
+    cs = DeviceConstraintSystem(cs_bytes, device=device)
+    words = value_vec_from_data(cs, ValuesData.deserialize(public_bytes).words,
+                                ValuesData.deserialize(non_public_bytes).words)
+    w = torch.from_numpy(words[:cs.committed_total_len].view(np.int64)).to(f"cuda:{cs.device}")
+    transcript = Prover(cs, log_inv_rate).prove(w)
+    return Proof(transcript.finalize(), STD_CHALLENGER).serialize()
+
+
 class ProveQueue:
     """Batched / served proving over binius_queue_* (see include/binius_gpu.h): n_workers proving
     threads with their own streams, FIFO admission under an HBM budget."""

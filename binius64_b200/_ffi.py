@@ -77,6 +77,15 @@ _SIGS = {
     "binius_cs_from_bytes": (_int, [_int, _c.c_char_p, _c.c_size_t, _c.POINTER(_vp)]),
     "binius_cs_destroy": (_int, [_vp]),
     "binius_cs_info": (_int, [_vp, _vp]),
+    "binius_values_data_encode": (_int, [_vp, _c.c_size_t, _vp, _c.c_size_t,
+                                         _c.POINTER(_c.c_size_t)]),
+    "binius_values_data_decode": (_int, [_vp, _c.c_size_t, _vp, _c.c_size_t,
+                                         _c.POINTER(_c.c_size_t)]),
+    "binius_proof_encode": (_int, [_vp, _c.c_size_t, _c.c_char_p, _vp, _c.c_size_t,
+                                   _c.POINTER(_c.c_size_t)]),
+    "binius_proof_decode": (_int, [_vp, _c.c_size_t, _vp, _c.c_size_t, _c.POINTER(_c.c_size_t),
+                                   _c.c_char_p, _c.c_size_t]),
+    "binius_value_vec_from_data": (_int, [_vp, _vp, _c.c_size_t, _vp, _c.c_size_t, _vp]),
     "binius_eval_operands": (_int, [_vp, _vp, _int, _vp, _vp]),
     "binius_and_reduction_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "binius_shift_reduction_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

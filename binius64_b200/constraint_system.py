@@ -191,6 +191,43 @@ class ConstraintSystem:
             operand(c.a), operand(c.b), operand(c.hi), operand(c.lo)
         return bytes(out)
 
+    @classmethod
+    def deserialize(cls, data: bytes) -> "ConstraintSystem":
+        """ConstraintSystem::deserialize (constraint_system.rs:617-650): version 2, the layout, the
+        constants (their count must equal n_const), then the AND and MUL constraint lists."""
+        pos = 0
+
+        def take(n):
+            nonlocal pos
+            if pos + n > len(data):
+                raise ValueError("NotEnoughBytes")
+            b = data[pos:pos + n]
+            pos += n
+            return b
+
+        u32 = lambda: struct.unpack("<I", take(4))[0]  # noqa: E731
+        if u32() != cls.SERIALIZATION_VERSION:
+            raise ValueError("InvalidConstruction: ConstraintSystem::version")
+        layout = ValueVecLayout(*[u32() for _ in range(8)])
+        constants = [struct.unpack("<Q", take(8))[0] for _ in range(u32())]
+        if len(constants) != layout.n_const:
+            raise ValueError("InvalidConstruction: ConstraintSystem::constants")
+
+        def operand():
+            out = []
+            for _ in range(u32()):
+                vi = u32()
+                variant = take(1)[0]
+                amount = u32()
+                if variant > ROTR32:
+                    raise ValueError("UnknownEnumVariant: ShiftVariant")
+                out.append(ShiftedValueIndex(vi, variant, amount))
+            return out
+
+        ands = [AndConstraint(operand(), operand(), operand()) for _ in range(u32())]
+        muls = [MulConstraint(operand(), operand(), operand(), operand()) for _ in range(u32())]
+        return cls(layout, constants, ands, muls)
+
     def prepared(self) -> "ConstraintSystem":
         """validate_and_prepare: pad the constraint lists to powers of two (>= 8 AND, >= 1 MUL)."""
         n_and = max(MIN_AND_CONSTRAINTS, self.n_and())

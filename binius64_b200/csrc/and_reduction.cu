@@ -573,17 +573,17 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
   uint64_t* words = nullptr;
   uint4 *eq_big = nullptr, *fcols = nullptr, *eq = nullptr;
   uint32_t* d_acc = nullptr;
-  BGPU_CUDA(cudaMallocAsync(&words, 8 * 3 * N, s));
-  BGPU_CUDA(cudaMallocAsync(&eq_big, 16 * n_chunks, s));
-  BGPU_CUDA(cudaMallocAsync(&fcols, 16 * 3 * N, s));
-  BGPU_CUDA(cudaMallocAsync(&eq, 16 * (N / 2), s));
+  BGPU_CUDA(dev_alloc(&words, 8 * 3 * N, s));
+  BGPU_CUDA(dev_alloc(&eq_big, 16 * n_chunks, s));
+  BGPU_CUDA(dev_alloc(&fcols, 16 * 3 * N, s));
+  BGPU_CUDA(dev_alloc(&eq, 16 * (N / 2), s));
   // 64 univariate slots, then one (y_1, y_inf) slot pair per MLE-check round, zeroed once
-  BGPU_CUDA(cudaMallocAsync(&d_acc, 16 * (64 + 2 * (log_n + 1)), s));
+  BGPU_CUDA(dev_alloc(&d_acc, 16 * (64 + 2 * (log_n + 1)), s));
   uint4* mul_tab = nullptr;
-  BGPU_CUDA(cudaMallocAsync(&mul_tab, 16 * kMulTableEntries, s));
+  BGPU_CUDA(dev_alloc(&mul_tab, 16 * kMulTableEntries, s));
   // round constants (2 per round), the claim slot pair, the challenges
   uint4* dev = nullptr;
-  BGPU_CUDA(cudaMallocAsync(&dev, 16 * (2 * (log_n + 1) + log_n), s));
+  BGPU_CUDA(dev_alloc(&dev, 16 * (2 * (log_n + 1) + log_n), s));
   int rc = BINIUS_OK;
   do {
     if ((rc = eval_operands(cs->and_ops, d_witness, words, s))) break;
@@ -712,13 +712,13 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
     res.c_eval = from_bytes16(ev + 32);
     res.eval_point.assign(challenges.rbegin(), challenges.rend());
   } while (0);
-  cudaFreeAsync(words, s);
-  cudaFreeAsync(eq_big, s);
-  cudaFreeAsync(fcols, s);
-  cudaFreeAsync(eq, s);
-  cudaFreeAsync(d_acc, s);
-  cudaFreeAsync(mul_tab, s);
-  cudaFreeAsync(dev, s);
+  dev_free(words, s);
+  dev_free(eq_big, s);
+  dev_free(fcols, s);
+  dev_free(eq, s);
+  dev_free(d_acc, s);
+  dev_free(mul_tab, s);
+  dev_free(dev, s);
   return rc;
 }
 

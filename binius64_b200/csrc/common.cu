@@ -173,6 +173,91 @@ int StagedReads::wait() {
   return BINIUS_OK;
 }
 
+namespace {
+
+struct ArenaChunk {
+  uint8_t* base;
+  size_t size, used;
+};
+
+struct Arena {
+  cudaStream_t s = nullptr;
+  bool active = false, keep = false;
+  std::vector<ArenaChunk> chunks;
+  bool owns(const void* p) const {
+    const uint8_t* b = static_cast<const uint8_t*>(p);
+    for (const auto& c : chunks)
+      if (b >= c.base && b < c.base + c.size) return true;
+    return false;
+  }
+  void release() {
+    for (const auto& c : chunks) cudaFreeAsync(c.base, s);
+    chunks.clear();
+  }
+};
+
+thread_local Arena t_arena;
+constexpr size_t kArenaChunk = 64ull << 20;
+
+}  // namespace
+
+cudaError_t dev_alloc_raw(void** p, size_t bytes, cudaStream_t s) {
+  Arena& a = t_arena;
+  if (!a.active || a.s != s) return cudaMallocAsync(p, bytes ? bytes : 16, s);
+  const size_t need = (bytes + 255) & ~size_t(255);
+  for (auto& c : a.chunks)  // first fit among the scope's few chunks
+    if (c.used + need <= c.size) {
+      *p = c.base + c.used;
+      c.used += need;
+      return cudaSuccess;
+    }
+  void* base = nullptr;
+  const size_t size = need > kArenaChunk ? need : kArenaChunk;
+  cudaError_t e = cudaMallocAsync(&base, size, s);
+  if (e != cudaSuccess) return e;
+  a.chunks.push_back({static_cast<uint8_t*>(base), size, need});
+  *p = base;
+  return cudaSuccess;
+}
+
+cudaError_t dev_free(void* p, cudaStream_t s) {
+  if (!p) return cudaSuccess;
+  const Arena& a = t_arena;
+  if (a.active && a.s == s && a.owns(p)) return cudaSuccess;  // released with the scope
+  return cudaFreeAsync(p, s);
+}
+
+ArenaScope::ArenaScope(cudaStream_t s, bool keep) {
+  Arena& a = t_arena;
+  if (a.active) return;  // nested: the outer scope serves the allocations
+  if (a.s != s) {        // kept chunks of another stream go back to the pool first
+    a.release();
+    a.s = s;
+  }
+  a.active = true;
+  a.keep = keep;
+  owner_ = true;
+}
+
+ArenaScope::~ArenaScope() {
+  if (!owner_) return;
+  Arena& a = t_arena;
+  a.active = false;
+  if (a.keep) {
+    for (auto& c : a.chunks) c.used = 0;  // the next proof on this stream runs after this one
+  } else {
+    a.release();
+    a.s = nullptr;
+  }
+}
+
+void arena_release_thread() {
+  Arena& a = t_arena;
+  if (a.active) return;
+  a.release();
+  a.s = nullptr;
+}
+
 int read_sync(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   StagedReads r(s);
   if (int rc = r.add(dst, src, bytes)) return rc;

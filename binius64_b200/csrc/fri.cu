@@ -220,7 +220,7 @@ int fold_codeword_impl(const binius_ntt* ntt, const void* d_codeword, uint32_t l
   // so steps chain through a stream-ordered intermediate buffer.
   void* tmp = nullptr;
   if (n_challenges > 4) {
-    BGPU_CUDA(cudaMallocAsync(&tmp, 16ull << (log_len - 4), s));
+    BGPU_CUDA(dev_alloc(&tmp, 16ull << (log_len - 4), s));
   }
   uint32_t done = 0, cur_len = log_len;
   const uint4* src = cw;
@@ -240,7 +240,7 @@ int fold_codeword_impl(const binius_ntt* ntt, const void* d_codeword, uint32_t l
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
-      if (tmp) cudaFreeAsync(tmp, s);
+      if (tmp) dev_free(tmp, s);
       return cuda_error(e, "fold_codeword_kernel");
     }
     count_launch();
@@ -248,7 +248,7 @@ int fold_codeword_impl(const binius_ntt* ntt, const void* d_codeword, uint32_t l
     cur_len -= step;
     done += step;
   }
-  if (tmp) BGPU_CUDA(cudaFreeAsync(tmp, s));
+  if (tmp) BGPU_CUDA(dev_free(tmp, s));
   return BINIUS_OK;
 }
 

@@ -355,7 +355,7 @@ class IntMulDevice {
  public:
   IntMulDevice(cudaStream_t s, Transcript& t) : s_(s), t_(t) {}
   ~IntMulDevice() {
-    for (void* p : ptrs_) cudaFreeAsync(p, s_);
+    for (void* p : ptrs_) dev_free(p, s_);
   }
 
   int run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* d_lo, const uint64_t* d_hi,
@@ -370,7 +370,7 @@ class IntMulDevice {
  private:
   template <class T>
   int alloc(T** p, size_t elems16) {
-    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(p), 16 * std::max<size_t>(elems16, 1), s_);
+    cudaError_t e = dev_alloc(reinterpret_cast<void**>(p), 16 * std::max<size_t>(elems16, 1), s_);
     if (e != cudaSuccess) return cuda_error(e, "intmul buffers");
     ptrs_.push_back(*p);
     return BINIUS_OK;
@@ -792,14 +792,14 @@ int intmul_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Trans
                            IntMulResult& res, cudaStream_t s) {
   const uint64_t n = cs->mul_ops.n_constraints;
   uint64_t* cols = nullptr;
-  BGPU_CUDA(cudaMallocAsync(&cols, 8 * 4 * n, s));
+  BGPU_CUDA(dev_alloc(&cols, 8 * 4 * n, s));
   int rc = eval_operands(cs->mul_ops, d_witness, cols, s);
   if (!rc) {
     // CSR slots are (a, b, hi, lo)
     IntMulDevice dev(s, t);
     rc = dev.run(cols, cols + n, cols + 3 * n, cols + 2 * n, log2_ceil(n), res);
   }
-  cudaFreeAsync(cols, s);
+  dev_free(cols, s);
   return rc;
 }
 

@@ -87,8 +87,8 @@ struct DevFri {
   DevFri(const binius_pcs& p, const binius_pcs_committed& c, cudaStream_t st, const uint4* chal)
       : P(p), C(c), s(st), next_commit(p.log_batch), d_chal(chal) {}
   ~DevFri() {
-    for (auto w : words) cudaFreeAsync(w, s);
-    for (auto t : trees) cudaFreeAsync(t, s);
+    for (auto w : words) dev_free(w, s);
+    for (auto t : trees) dev_free(t, s);
   }
 
   // FRIFoldProver::execute_fold_round (prover/prover/src/fri/fold.rs:117-175): on a commit round,
@@ -103,7 +103,7 @@ struct DevFri {
     uint32_t log_out;
     if (words.empty()) {
       log_out = P.rs_log_len();
-      BGPU_CUDA(cudaMallocAsync(&out, 16ull << log_out, s));
+      BGPU_CUDA(dev_alloc(&out, 16ull << log_out, s));
       words.push_back(out);
       word_log_len.push_back(log_out);
       if (int rc = fri_fold_interleaved_dev(C.d_codeword, log_out, P.log_batch, ch, out, s))
@@ -112,7 +112,7 @@ struct DevFri {
       const uint32_t log_prev = word_log_len.back();
       log_out = log_prev - n;
       const uint4* prev = words.back();
-      BGPU_CUDA(cudaMallocAsync(&out, 16ull << log_out, s));
+      BGPU_CUDA(dev_alloc(&out, 16ull << log_out, s));
       words.push_back(out);
       word_log_len.push_back(log_out);
       if (int rc = fri_fold_codeword_dev(P.ntt, prev, log_prev, ch, n, out, s)) return rc;
@@ -124,7 +124,7 @@ struct DevFri {
     const uint32_t log_coset = has_next ? next_arity : P.n_final();
     const uint32_t log_leaves = log_out - log_coset;
     uint8_t* nodes = nullptr;
-    BGPU_CUDA(cudaMallocAsync(&nodes, 32ull * ((2ull << log_leaves) - 1), s));
+    BGPU_CUDA(dev_alloc(&nodes, 32ull * ((2ull << log_leaves) - 1), s));
     trees.push_back(nodes);
     tree_log_leaves.push_back(log_leaves);
     if (int rc = merkle_commit(out, log_leaves, log_coset, nodes, s)) return rc;
@@ -201,8 +201,8 @@ struct DevFri {
     if (off == 0) return BINIUS_OK;
     GatherSegment* d_segs = nullptr;
     uint8_t* d_dst = nullptr;
-    BGPU_CUDA(cudaMallocAsync(&d_segs, segs.size() * sizeof(GatherSegment), s));
-    BGPU_CUDA(cudaMallocAsync(&d_dst, off, s));
+    BGPU_CUDA(dev_alloc(&d_segs, segs.size() * sizeof(GatherSegment), s));
+    BGPU_CUDA(dev_alloc(&d_dst, off, s));
     std::vector<uint8_t> h(off);
     int rc = BINIUS_OK;
     do {
@@ -212,8 +212,8 @@ struct DevFri {
       if ((rc = gather_segments(d_segs, (uint32_t)segs.size(), d_dst, s))) break;
       rc = read_sync(h.data(), d_dst, off, s);
     } while (0);
-    cudaFreeAsync(d_segs, s);
-    cudaFreeAsync(d_dst, s);
+    dev_free(d_segs, s);
+    dev_free(d_dst, s);
     if (rc) return rc;
     t.decommitment(h.data(), h.size());
     return BINIUS_OK;
@@ -235,13 +235,13 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
   const uint64_t N = 1ull << n;
   uint4 *a = nullptr, *b = nullptr, *eq_r = nullptr, *dev = nullptr;
   uint32_t* d_small = nullptr;  // 128 elements (ring switch)
-  BGPU_CUDA(cudaMallocAsync(&a, 16 * N, s));
-  BGPU_CUDA(cudaMallocAsync(&b, 16 * N, s));
-  BGPU_CUDA(cudaMallocAsync(&eq_r, 16 * 128, s));
-  BGPU_CUDA(cudaMallocAsync(&d_small, 16 * 128, s));
+  BGPU_CUDA(dev_alloc(&a, 16 * N, s));
+  BGPU_CUDA(dev_alloc(&b, 16 * N, s));
+  BGPU_CUDA(dev_alloc(&eq_r, 16 * 128, s));
+  BGPU_CUDA(dev_alloc(&d_small, 16 * 128, s));
   // BaseFold round state: sums (2 per round), the claim pair, challenges, r's byte table
   const uint64_t n_dev = 2ull * n + 2 + n + kMulTableEntries;
-  BGPU_CUDA(cudaMallocAsync(&dev, 16 * n_dev, s));
+  BGPU_CUDA(dev_alloc(&dev, 16 * n_dev, s));
   uint4* slots = dev;
   uint4* claim = dev + 2 * n;  // [0] running claim, [1] initial claim
   uint4* chal = claim + 2;
@@ -343,11 +343,11 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
       rc = fri.finish(t);
     } while (0);
   }
-  cudaFreeAsync(a, s);
-  cudaFreeAsync(b, s);
-  cudaFreeAsync(eq_r, s);
-  cudaFreeAsync(d_small, s);
-  cudaFreeAsync(dev, s);
+  dev_free(a, s);
+  dev_free(b, s);
+  dev_free(eq_r, s);
+  dev_free(d_small, s);
+  dev_free(dev, s);
   cudaError_t e = stream_wait(s);
   if (rc == BINIUS_OK && e != cudaSuccess) rc = cuda_error(e, "pcs prove");
   return rc;
@@ -405,18 +405,18 @@ int binius_pcs_commit(const binius_pcs* P, const void* d_witness, binius_pcs_com
   int rc = BINIUS_OK;
   do {
     // stream-ordered allocations from the (cached) device pool: no device-wide synchronisation
-    cudaError_t e = cudaMallocAsync(&c->d_codeword, 16ull << c->log_len, s);
-    if (e != cudaSuccess) { rc = cuda_error(e, "cudaMallocAsync(codeword)"); break; }
-    e = cudaMallocAsync(&c->d_nodes, 32ull * ((2ull << c->log_leaves) - 1), s);
-    if (e != cudaSuccess) { rc = cuda_error(e, "cudaMallocAsync(tree)"); break; }
+    cudaError_t e = dev_alloc(&c->d_codeword, 16ull << c->log_len, s);
+    if (e != cudaSuccess) { rc = cuda_error(e, "dev_alloc(codeword)"); break; }
+    e = dev_alloc(&c->d_nodes, 32ull * ((2ull << c->log_leaves) - 1), s);
+    if (e != cudaSuccess) { rc = cuda_error(e, "dev_alloc(tree)"); break; }
     if ((rc = binius_fri_commit_interleaved(P->ntt, d_witness, P->log_dim(), P->log_inv_rate,
                                             P->log_batch, c->d_codeword, c->d_nodes, c->root,
                                             stream)))
       break;
   } while (0);
   if (rc) {
-    if (c->d_codeword) cudaFreeAsync(c->d_codeword, s);
-    if (c->d_nodes) cudaFreeAsync(c->d_nodes, s);
+    if (c->d_codeword) dev_free(c->d_codeword, s);
+    if (c->d_nodes) dev_free(c->d_nodes, s);
     delete c;
     return rc;
   }
@@ -428,8 +428,8 @@ int binius_pcs_commit(const binius_pcs* P, const void* d_witness, binius_pcs_com
 // Releases the buffers in order on the commit stream, which must still exist.
 int binius_pcs_committed_destroy(binius_pcs_committed* c) {
   if (!c) return BINIUS_OK;
-  cudaFreeAsync(c->d_codeword, c->stream);
-  cudaFreeAsync(c->d_nodes, c->stream);
+  dev_free(c->d_codeword, c->stream);
+  dev_free(c->d_nodes, c->stream);
   delete c;
   return BINIUS_OK;
 }

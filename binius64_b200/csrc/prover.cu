@@ -144,6 +144,8 @@ int binius_prover_prove(const binius_prover* P, const void* d_witness,
   const uint64_t* words = static_cast<const uint64_t*>(d_witness);
   Transcript& t = transcript->t;
 
+  // every device buffer of the proof comes from one arena on s, released at the end
+  ArenaScope arena(s, false);
   typedef std::chrono::steady_clock Clock;
   auto t0 = Clock::now();
   auto lap = [&](int phase) {

@@ -99,8 +99,10 @@ void binius_queue::worker_loop() {
     std::vector<uint8_t> proof;
     const void* d_w = r->witness;
     void* owned = nullptr;
+    // the proof's device buffers come from this worker's arena, kept for its next proof
+    ArenaScope arena(s, true);
     if (!r->on_device) {
-      cudaError_t e = cudaMallocAsync(&owned, 8 * r->n_words, s);
+      cudaError_t e = dev_alloc(&owned, 8 * r->n_words, s);
       if (e == cudaSuccess)
         e = cudaMemcpyAsync(owned, r->witness, 8 * r->n_words, cudaMemcpyHostToDevice, s);
       if (e != cudaSuccess) rc = cuda_error(e, "queue witness upload");
@@ -114,7 +116,7 @@ void binius_queue::worker_loop() {
       binius_prover_phase_ms(r->prover, phases);
     }
     if (rc) err = binius_last_error();
-    if (owned) cudaFreeAsync(owned, s);
+    if (owned) dev_free(owned, s);
     stream_wait(s);
     {
       std::lock_guard<std::mutex> lock(mu);
@@ -130,6 +132,7 @@ void binius_queue::worker_loop() {
     cv_done.notify_all();
     cv_work.notify_all();
   }
+  arena_release_thread();
   cudaStreamDestroy(s);
 }
 

@@ -507,11 +507,11 @@ struct ShiftBuffers {
   std::vector<void*> ptrs;
   explicit ShiftBuffers(cudaStream_t st) : s(st) {}
   ~ShiftBuffers() {
-    for (void* p : ptrs) cudaFreeAsync(p, s);
+    for (void* p : ptrs) dev_free(p, s);
   }
   template <class T>
   int alloc(T** p, size_t bytes) {
-    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(p), bytes ? bytes : 16, s);
+    cudaError_t e = dev_alloc(reinterpret_cast<void**>(p), bytes ? bytes : 16, s);
     if (e != cudaSuccess) return cuda_error(e, "shift reduction buffers");
     ptrs.push_back(*p);
     return BINIUS_OK;

@@ -328,13 +328,13 @@ int eq_tensor(const uint4* h_point, uint32_t n, uint4* d_out, cudaStream_t s) {
   const uint32_t k = n / 2;
   uint4* tmp = nullptr;
   const uint64_t nlo = 1ull << k, nhi = 1ull << (n - k);
-  BGPU_CUDA(cudaMallocAsync(&tmp, 16 * (nlo + nhi), s));
+  BGPU_CUDA(dev_alloc(&tmp, 16 * (nlo + nhi), s));
   eq_small_kernel<<<grid_for(nlo, kThreads), kThreads, 0, s>>>(tmp, p, 0, k);
   eq_small_kernel<<<grid_for(nhi, kThreads), kThreads, 0, s>>>(tmp + nlo, p, k, n - k);
   eq_expand_kernel<<<grid_for(1ull << n, kThreads, 148 * 16), kThreads, 0, s>>>(d_out, tmp, tmp + nlo,
                                                                               k, 1ull << n);
   cudaError_t e = cudaGetLastError();
-  cudaFreeAsync(tmp, s);
+  dev_free(tmp, s);
   if (e != cudaSuccess) return cuda_error(e, "eq tensor kernels");
   count_launch(3);
   return BINIUS_OK;
@@ -354,7 +354,7 @@ int fold_1b_rows(const uint4* d_mat, const uint4* d_vec, uint64_t n, uint32_t* d
 int fold_b128_elems(const uint4* d_in, uint4* d_out, uint64_t n, const uint4* d_vec128,
                     cudaStream_t s) {
   uint4* tables = nullptr;
-  BGPU_CUDA(cudaMallocAsync(&tables, 16 * 16 * 256, s));
+  BGPU_CUDA(dev_alloc(&tables, 16 * 16 * 256, s));
   build_fold_tables_kernel<<<16, 256, 0, s>>>(d_vec128, tables);
   const size_t smem = 16 * 256 * sizeof(uint4);
   cudaError_t e = ensure_smem_limit(reinterpret_cast<const void*>(fold_elems_kernel), smem)
@@ -364,7 +364,7 @@ int fold_b128_elems(const uint4* d_in, uint4* d_out, uint64_t n, const uint4* d_
     fold_elems_kernel<<<grid_for(n, kThreads, 148 * 2), kThreads, smem, s>>>(d_in, d_out, n, tables);
     e = cudaGetLastError();
   }
-  cudaFreeAsync(tables, s);
+  dev_free(tables, s);
   if (e != cudaSuccess) return cuda_error(e, "fold_elems_kernel");
   count_launch(2);
   return BINIUS_OK;
@@ -398,7 +398,7 @@ int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[1
   if (size >= kMulTableMinSize) {
     // large rounds: the four products by r per thread go through r's byte table
     uint4* tab = nullptr;
-    BGPU_CUDA(cudaMallocAsync(&tab, 16 * kMulTableEntries, s));
+    BGPU_CUDA(dev_alloc(&tab, 16 * kMulTableEntries, s));
     int rc = build_mul_table(r, tab, s);
     if (!rc) {
       bivariate_fold_eval_kernel<true><<<grid, kThreads, 0, s>>>(d_a, d_b, size, rv, nullptr, tab,
@@ -407,7 +407,7 @@ int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[1
       if (e != cudaSuccess) rc = cuda_error(e, "bivariate_fold_eval_kernel");
       else count_launch();
     }
-    cudaFreeAsync(tab, s);
+    dev_free(tab, s);
     return rc;
   }
   bivariate_fold_eval_kernel<false><<<grid, kThreads, 0, s>>>(d_a, d_b, size, rv, nullptr, nullptr,

@@ -26,12 +26,12 @@ __global__ void transcript_message_kernel(TranscriptState* ts, uint8_t* tape,
 namespace bgpu {
 
 DeviceTranscript::~DeviceTranscript() {
-  if (mem_) cudaFreeAsync(mem_, s_);
+  if (mem_) dev_free(mem_, s_);
 }
 
 int DeviceTranscript::begin(const Transcript& t, cudaStream_t s) {
   s_ = s;
-  if (!mem_) BGPU_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&mem_), kStateBytes + kTapeCap, s));
+  if (!mem_) BGPU_CUDA(dev_alloc(reinterpret_cast<void**>(&mem_), kStateBytes + kTapeCap, s));
   TranscriptState st;
   t.save(st);
   st.tape_cap = kTapeCap;

@@ -279,6 +279,30 @@ int binius_queue_wait(binius_queue* queue, uint64_t ticket, void* h_proof, size_
                       size_t* len, double* h_times8);
 
 /* ------------------------------------------------------------------------------------------
+ * Wire formats around a prove call (load-prove serving).
+ * Replaces: ValuesData::{serialize, deserialize} (verifier/core/src/constraint_system.rs:939-963,
+ * version 1), Proof::{serialize, deserialize} (:1066-1098, version 1) and ValueVec::new_from_data
+ * (:803-823), as used by the reference's prover binary (prover/examples/src/bin/prover.rs:46-99).
+ * Encoders write at most `cap` bytes and always set *len; a too-small buffer returns BINIUS_E_ARG.
+ * Decoders reject another version with BINIUS_E_ARG ("InvalidConstruction: Witness::version",
+ * "... Proof::version") and truncated input with BINIUS_E_ARG ("NotEnoughBytes: ...").
+ * binius_value_vec_from_data requires n_public + n_non_public == committed_total_len
+ * ("ValueVecLenMismatch") and writes committed_total_len + n_scratch words, the scratch zeroed.
+ * The proof's challenger type for this library's transcript is "HasherChallenger<Sha256>".
+ * ------------------------------------------------------------------------------------------ */
+int binius_values_data_encode(const uint64_t* h_words, size_t n_words, void* h_out, size_t cap,
+                              size_t* len);
+int binius_values_data_decode(const void* h_bytes, size_t len, uint64_t* h_words, size_t cap,
+                              size_t* n_words);
+int binius_proof_encode(const void* h_transcript, size_t n_bytes, const char* challenger,
+                        void* h_out, size_t cap, size_t* len);
+int binius_proof_decode(const void* h_bytes, size_t len, void* h_transcript, size_t cap,
+                        size_t* n_bytes, char* h_challenger, size_t ch_cap);
+int binius_value_vec_from_data(const binius_cs* cs, const uint64_t* h_public, size_t n_public,
+                               const uint64_t* h_non_public, size_t n_non_public,
+                               uint64_t* h_out);
+
+/* ------------------------------------------------------------------------------------------
  * Integer multiplication reduction.
  * Replaces: build_intmul_witness + prove_intmul_reduction (prover/prover/src/prove.rs:374-391,
  * 432-470), intmul Witness (protocols/intmul/witness.rs:47-270) and IntMulProver::prove
