@@ -15,13 +15,18 @@
 // bivariate products on multiple pairs (bivariate_product_multi_mle.rs), the selector prover
 // (selector_mle.rs) and rerandomisation (rerand_mle.rs), with the Gruen eq factor
 // (gruen32.rs, mle_to_sumcheck.rs).  Kernels produce the per-claim round sums (y_1, y_inf) and
-// fold; the degree-2/3 coefficient algebra and the transcript run on the host between launches.
+// fold by the previous challenge; each round's degree-2/3 coefficient algebra over all claims and
+// the Fiat-Shamir step run in intmul_round_finish_kernel on the device transcript, so a batched
+// sumcheck of n rounds is one chain of launches with one read-back at its end.  The host sets each
+// sumcheck up (the eq points' alphas with one batched inversion, the powers of beta) and writes the
+// final evaluations.
 #include <string.h>
 
 #include <algorithm>
 #include <vector>
 
 #include "cs.h"
+#include "dev_transcript.cuh"
 #include "gf128.cuh"
 #include "gf_reduce.cuh"
 #include "internal.h"
@@ -104,10 +109,13 @@ __device__ __forceinline__ uint4 fold1(uint4 lo, uint4 hi, uint4 r) {
 // length L): out[8p..] += (sum eq[i] a1 b1, sum eq[i] (a0 + a1)(b0 + b1)) over i < L/2.  With
 // `fold`, both multilinears first shrink from 2L to L by r in place (fold_highest_var_inplace);
 // thread i owns positions i and i + L/2, so the fold and the round need one pass.  Grid: (chunks,
-// pairs).
+// pairs).  The fold's r is *r_ptr (a challenge in HBM); r_ptr == nullptr means no fold.
 __global__ void __launch_bounds__(kT)
     biv_round_kernel(uint4* __restrict__ set, uint64_t L, uint64_t stride,
-                     const uint4* __restrict__ eq, int fold, uint4 r, uint32_t* __restrict__ out) {
+                     const uint4* __restrict__ eq, const uint4* __restrict__ r_ptr,
+                     uint32_t* __restrict__ out) {
+  const bool fold = r_ptr != nullptr;
+  const uint4 r = fold ? *r_ptr : gf_zero();
   const uint32_t p = blockIdx.y;
   uint4* a = set + 2 * p * stride;
   uint4* b = a + stride;
@@ -143,7 +151,10 @@ __global__ void __launch_bounds__(kT)
 // optional fused fold.  Grid: (chunks, columns).
 __global__ void __launch_bounds__(kT)
     lin_round_kernel(uint4* __restrict__ set, uint64_t L, uint64_t stride,
-                     const uint4* __restrict__ eq, int fold, uint4 r, uint32_t* __restrict__ out) {
+                     const uint4* __restrict__ eq, const uint4* __restrict__ r_ptr,
+                     uint32_t* __restrict__ out) {
+  const bool fold = r_ptr != nullptr;
+  const uint4 r = fold ? *r_ptr : gf_zero();
   const uint32_t k = blockIdx.y;
   uint4* c = set + k * stride;
   const uint64_t h = L >> 1;
@@ -170,7 +181,9 @@ __global__ void __launch_bounds__(kT)
 __global__ void __launch_bounds__(kT)
     selector_round_kernel(const uint4* __restrict__ sel, uint4* __restrict__ cols, uint64_t L,
                           uint64_t stride, const uint4* __restrict__ eqs, uint64_t eq_stride,
-                          int fold, uint4 r, uint32_t* __restrict__ out) {
+                          const uint4* __restrict__ r_ptr, uint32_t* __restrict__ out) {
+  const bool fold = r_ptr != nullptr;
+  const uint4 r = fold ? *r_ptr : gf_zero();
   const uint32_t k = blockIdx.y;
   uint4* s = cols + k * stride;
   const uint4* eq = eqs + k * eq_stride;
@@ -198,7 +211,8 @@ __global__ void __launch_bounds__(kT)
 
 // In-place top-variable fold of `count` multilinears of length 2 * half.
 __global__ void fold_set_kernel(uint4* __restrict__ set, uint32_t count, uint64_t half,
-                                uint64_t stride, uint4 r) {
+                                uint64_t stride, const uint4* __restrict__ r_ptr) {
+  const uint4 r = *r_ptr;
   const uint64_t total = (uint64_t)count * half;
   for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total;
        t += (uint64_t)gridDim.x * blockDim.x) {
@@ -243,9 +257,88 @@ __global__ void __launch_bounds__(kT)
   block_xor_reduce<1>(r, out);
 }
 
-// ---------------------------------------------------------------- host side
+// One claim of a batched MLE-check round: the slots (uint4 index into the round's sums) of its
+// y_1 and, for a bivariate product (deg 2), y_inf; deg 1 is a linear claim (RoundEvals1).  group
+// selects the eq point (alphas, Gruen prefix) the claim follows.
+struct ImClaim {
+  uint16_t y1, yinf;
+  uint8_t deg, group;
+  uint16_t pad;
+};
+// The eq coordinate a group's MLE-check binds in one round and 1 / (1 + alpha).
+struct ImAlpha {
+  uint4 alpha, inv_one_plus_alpha;
+};
+constexpr int kImFinishThreads = 256;
+constexpr uint32_t kImMaxClaims = 256;
 
-typedef std::vector<hu128> Poly;
+// The Fiat-Shamir step of one round of a batched MLE-check (BatchSumcheckProver over decorated
+// MLE-check provers, batch.rs:41-135 + mle_to_sumcheck.rs + gruen32.rs), on the device.  Claim i:
+// prime_i = interpolate_eq(sum_i, y_1, [y_inf], alpha) (RoundEvals2 / RoundEvals1,
+// round_evals.rs:23-27, 80-87), all_i = round_coeffs_by_eq(prime_i, alpha) * prefix
+// (round_evals.rs:145-156); the round message is sum_i beta^i all_i without its top coefficient
+// (msg_coeffs elements).  Claims are spread over the block and block-reduced; warp 0 writes the
+// message and samples r; then every claim's sum becomes prime_i(r) and every group's prefix
+// takes the factor (1 + r + alpha).
+__global__ void __launch_bounds__(kImFinishThreads)
+    intmul_round_finish_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
+                               const uint4* __restrict__ slots, const ImClaim* __restrict__ claims,
+                               uint32_t n_claims, uint4* __restrict__ sums,
+                               uint4* __restrict__ prefix, const ImAlpha* __restrict__ alphas,
+                               uint32_t n_groups, const uint4* __restrict__ beta_pow,
+                               uint32_t msg_coeffs, uint4* __restrict__ r_out) {
+  __shared__ uint4 s_prime[kImMaxClaims][3];
+  __shared__ uint4 s_r;
+  uint4 acc[4] = {gf_zero(), gf_zero(), gf_zero(), gf_zero()};
+  for (uint32_t i = threadIdx.x; i < n_claims; i += blockDim.x) {
+    const ImClaim c = claims[i];
+    const ImAlpha a = alphas[c.group];
+    const uint4 y1 = slots[c.y1];
+    const uint4 y0 = gf_mul(gf_add(sums[i], gf_mul(y1, a.alpha)), a.inv_one_plus_alpha);
+    uint4 p0 = y0, p1, p2 = gf_zero();
+    if (c.deg == 2) {
+      const uint4 yinf = slots[c.yinf];
+      p1 = gf_add(gf_add(y1, y0), yinf);
+      p2 = yinf;
+    } else {
+      p1 = gf_add(y1, y0);
+    }
+    s_prime[i][0] = p0;
+    s_prime[i][1] = p1;
+    s_prime[i][2] = p2;
+    uint4 oma = a.alpha;
+    oma.x ^= 1u;
+    const uint4 sc = gf_mul(prefix[c.group], beta_pow[i]);
+    gf_add_into(acc[0], gf_mul(gf_mul(p0, oma), sc));
+    gf_add_into(acc[1], gf_mul(gf_add(gf_mul(p1, oma), p0), sc));
+    gf_add_into(acc[2], gf_mul(gf_add(gf_mul(p2, oma), p1), sc));
+    gf_add_into(acc[3], gf_mul(p2, sc));
+  }
+  block_xor_sum<4>(acc);
+  if (threadIdx.x < 32) {
+    DevTr st;
+    st.load(ts);
+    st.message_elems(tape, acc, msg_coeffs);
+    const uint4 r = st.sample_elem();
+    __syncwarp();
+    if (threadIdx.x == 0) {
+      *r_out = r;
+      st.store(ts);
+      s_r = r;
+    }
+  }
+  __syncthreads();
+  const uint4 r = s_r;
+  for (uint32_t i = threadIdx.x; i < n_claims; i += blockDim.x)
+    sums[i] = gf_add(s_prime[i][0], gf_mul(r, gf_add(s_prime[i][1], gf_mul(r, s_prime[i][2]))));
+  for (uint32_t g = threadIdx.x; g < n_groups; g += blockDim.x) {
+    uint4 f = gf_add(r, alphas[g].alpha);
+    f.x ^= 1u;
+    prefix[g] = gf_mul(prefix[g], f);
+  }
+}
+
+// ---------------------------------------------------------------- host side
 
 uint4 u4(hu128 v) {
   uint4 r;
@@ -285,39 +378,24 @@ void normalize_leaves(const std::vector<hu128>& biv, IntMulResult& res) {
   }
 }
 
-hu128 eval_poly(const Poly& c, hu128 x) {
-  hu128 acc = 0;
-  for (size_t i = c.size(); i-- > 0;) acc = host_gf_mul(acc, x) ^ c[i];
-  return acc;
-}
-// (1 + alpha)^-1 (invert_or_zero), memoised per thread: the claims of one prover share alpha.
-hu128 inv_one_plus(hu128 alpha) {
-  thread_local hu128 last_alpha = 0, last_inv = 1;
-  if (alpha != last_alpha) {
-    last_alpha = alpha;
-    last_inv = host_gf_inv(1 ^ alpha);
+// In place: v[i] <- 1 / v[i] for nonzero entries (zero stays zero, as invert_or_zero), with one
+// inversion for the whole vector (Montgomery's trick).
+void batch_inv(std::vector<hu128>& v) {
+  std::vector<hu128> pre(v.size());
+  hu128 acc = 1;
+  for (size_t i = 0; i < v.size(); i++) {
+    pre[i] = acc;
+    if (v[i]) acc = host_gf_mul(acc, v[i]);
   }
-  return last_inv;
-}
-// RoundEvals2 / RoundEvals1 ::interpolate_eq (round_evals.rs:23-27, 80-87).
-Poly interp2(hu128 sum, hu128 y1, hu128 yinf, hu128 alpha) {
-  const hu128 y0 = host_gf_mul(sum ^ host_gf_mul(y1, alpha), inv_one_plus(alpha));
-  return {y0, y1 ^ y0 ^ yinf, yinf};
-}
-Poly interp1(hu128 sum, hu128 y1, hu128 alpha) {
-  const hu128 y0 = host_gf_mul(sum ^ host_gf_mul(y1, alpha), inv_one_plus(alpha));
-  return {y0, y1 ^ y0};
-}
-// round_coeffs_by_eq (round_evals.rs:145-156) times `scale`.
-Poly by_eq(const Poly& prime, hu128 alpha, hu128 scale) {
-  Poly out(prime.size() + 1, 0);
-  for (size_t i = 0; i < prime.size(); i++) {
-    out[i] ^= host_gf_mul(prime[i], 1 ^ alpha);
-    out[i + 1] ^= prime[i];
+  hu128 inv = host_gf_inv(acc);
+  for (size_t i = v.size(); i-- > 0;) {
+    if (!v[i]) continue;
+    const hu128 x = v[i];
+    v[i] = host_gf_mul(inv, pre[i]);
+    inv = host_gf_mul(inv, x);
   }
-  for (auto& c : out) c = host_gf_mul(c, scale);
-  return out;
 }
+
 hu128 sample(Transcript& t) {
   uint8_t b[16];
   t.sample_elem(b);
@@ -326,31 +404,6 @@ hu128 sample(Transcript& t) {
 void write_elems(Transcript& t, const std::vector<hu128>& v) {
   if (!v.empty()) t.message(v.data(), 16 * v.size());
 }
-// Batched round polynomial sum_i beta^i c_i (rfold in batch.rs:76-78), truncated and written.
-void write_batched(Transcript& t, const std::vector<Poly>& all, hu128 beta) {
-  Poly acc;
-  for (size_t i = all.size(); i-- > 0;) {
-    for (auto& c : acc) c = host_gf_mul(c, beta);
-    if (acc.size() < all[i].size()) acc.resize(all[i].size(), 0);
-    for (size_t k = 0; k < all[i].size(); k++) acc[k] ^= all[i][k];
-  }
-  acc.pop_back();
-  write_elems(t, acc);
-}
-
-// The Gruen eq factor of an MLE-check: eq over point[0 .. n_rem - 1) on the device plus the
-// prefix product of eq_one_var over the folded coordinates.
-struct GruenState {
-  std::vector<hu128> point;
-  uint32_t n_rem;
-  hu128 prefix = 1;
-  hu128 alpha() const { return point[n_rem - 1]; }
-  void fold(hu128 r) {
-    prefix = host_gf_mul(prefix, 1 ^ r ^ alpha());
-    n_rem--;
-  }
-};
-
 class IntMulDevice {
  public:
   IntMulDevice(cudaStream_t s, Transcript& t) : s_(s), t_(t) {}
@@ -394,24 +447,105 @@ class IntMulDevice {
     for (uint32_t i = 0; i < m; i++) p[i] = u4(point[i]);
     return eq_tensor(p.data(), m, out, s_);
   }
-  int fold(uint4* set, uint32_t count, uint64_t half, hu128 r) {
+  int fold(uint4* set, uint32_t count, uint64_t half, const uint4* r_ptr) {
     if (half == 0) return BINIUS_OK;
-    fold_set_kernel<<<blocks_for((uint64_t)count * half), kT, 0, s_>>>(set, count, half, N_, u4(r));
+    fold_set_kernel<<<blocks_for((uint64_t)count * half), kT, 0, s_>>>(set, count, half, N_, r_ptr);
     return check("fold_set_kernel");
   }
-  // Fused round launches on multilinears of current length L (fold from 2L first when `fold`).
-  int biv_round(uint4* set, uint32_t pairs, uint64_t L, const uint4* eq, bool fold, hu128 r,
+  // Fused round launches on multilinears of current length L (fold from 2L first by *r_ptr when
+  // r_ptr is set).
+  int biv_round(uint4* set, uint32_t pairs, uint64_t L, const uint4* eq, const uint4* r_ptr,
                 uint32_t* out) {
     dim3 grid(blocks_for(L / 2, 148 * 2), pairs);
-    biv_round_kernel<<<grid, kT, 0, s_>>>(set, L, N_, eq, fold ? 1 : 0, u4(r), out);
+    biv_round_kernel<<<grid, kT, 0, s_>>>(set, L, N_, eq, r_ptr, out);
     return check("biv_round_kernel");
   }
-  int lin_round(uint4* set, uint32_t cols, uint64_t L, const uint4* eq, bool fold, hu128 r,
+  int lin_round(uint4* set, uint32_t cols, uint64_t L, const uint4* eq, const uint4* r_ptr,
                 uint32_t* out) {
     dim3 grid(blocks_for(L / 2, 148 * 2), cols);
-    lin_round_kernel<<<grid, kT, 0, s_>>>(set, L, N_, eq, fold ? 1 : 0, u4(r), out);
+    lin_round_kernel<<<grid, kT, 0, s_>>>(set, L, N_, eq, r_ptr, out);
     return check("lin_round_kernel");
   }
+  // A batched MLE-check whose rounds run on the device transcript: batch_begin uploads the claims,
+  // each eq point's per-round alpha and 1/(1 + alpha) (one batched inversion), the powers of
+  // beta and the initial sums; each round launches its evaluation kernels into batch_slots(t)
+  // (folding by batch_r(t)) and then batch_round; batch_read queues the copy-back of the
+  // challenges and the transcript, batch_end hands the transcript back to the host.
+  struct DevBatch {
+    uint32_t n = 0, n_claims = 0, n_groups = 0, msg = 3, per_round = 0;
+    ImClaim* claims = nullptr;
+    ImAlpha* alphas = nullptr;
+    uint4 *sums = nullptr, *prefix = nullptr, *beta = nullptr, *chal = nullptr, *slots = nullptr;
+    DeviceTranscript dt;
+  };
+  int batch_begin(DevBatch& b, const std::vector<ImClaim>& claims,
+                  const std::vector<const std::vector<hu128>*>& points,
+                  const std::vector<hu128>& sums, hu128 beta, uint32_t per_round) {
+    if (claims.empty() || claims.size() > kImMaxClaims || sums.size() != claims.size())
+      return set_error(BINIUS_E_ARG, "intmul batch: 1..256 claims with one sum each");
+    b.n = (uint32_t)points[0]->size();
+    b.n_claims = (uint32_t)claims.size();
+    b.n_groups = (uint32_t)points.size();
+    b.per_round = per_round;
+    b.msg = 2;
+    for (const auto& c : claims) b.msg = c.deg == 2 ? 3 : b.msg;
+    const size_t n_cl = (8 * claims.size() + 15) / 16, n_al = 2ull * b.n * b.n_groups;
+    const size_t host_elems = n_cl + b.n_claims + b.n_groups + n_al + b.n_claims;
+    const size_t total = host_elems + b.n + (size_t)b.n * per_round;
+    uint4* base = nullptr;
+    if (int rc = alloc(&base, total)) return rc;
+    std::vector<uint4> h(host_elems, make_uint4(0, 0, 0, 0));
+    memcpy(h.data(), claims.data(), 8 * claims.size());
+    uint4* hs = h.data() + n_cl;
+    for (uint32_t i = 0; i < b.n_claims; i++) hs[i] = u4(sums[i]);
+    uint4* hp = hs + b.n_claims;
+    for (uint32_t g = 0; g < b.n_groups; g++) hp[g] = u4(1);
+    uint4* ha = hp + b.n_groups;
+    std::vector<hu128> inv(b.n * b.n_groups);
+    for (uint32_t t = 0; t < b.n; t++)
+      for (uint32_t g = 0; g < b.n_groups; g++) {
+        if (points[g]->size() != b.n) return set_error(BINIUS_E_ARG, "intmul batch: point lengths");
+        inv[t * b.n_groups + g] = 1 ^ (*points[g])[b.n - 1 - t];
+      }
+    batch_inv(inv);
+    for (uint32_t t = 0; t < b.n; t++)
+      for (uint32_t g = 0; g < b.n_groups; g++) {
+        ha[2 * (t * b.n_groups + g)] = u4((*points[g])[b.n - 1 - t]);
+        ha[2 * (t * b.n_groups + g) + 1] = u4(inv[t * b.n_groups + g]);
+      }
+    uint4* hb = ha + n_al;
+    hu128 bp = 1;
+    for (uint32_t i = 0; i < b.n_claims; i++, bp = host_gf_mul(bp, beta)) hb[i] = u4(bp);
+    BGPU_CUDA(cudaMemcpyAsync(base, h.data(), 16 * host_elems, cudaMemcpyHostToDevice, s_));
+    b.claims = reinterpret_cast<ImClaim*>(base);
+    b.sums = base + n_cl;
+    b.prefix = b.sums + b.n_claims;
+    b.alphas = reinterpret_cast<ImAlpha*>(b.prefix + b.n_groups);
+    b.beta = b.prefix + b.n_groups + n_al;
+    b.chal = base + host_elems;
+    b.slots = b.chal + b.n;
+    BGPU_CUDA(cudaMemsetAsync(b.slots, 0, 16ull * b.n * per_round, s_));
+    return b.dt.begin(t_, s_);
+  }
+  static uint32_t* batch_slots(DevBatch& b, uint32_t t) {
+    return reinterpret_cast<uint32_t*>(b.slots + (size_t)t * b.per_round);
+  }
+  static const uint4* batch_r(const DevBatch& b, uint32_t t) {
+    return t ? b.chal + t - 1 : nullptr;
+  }
+  int batch_round(DevBatch& b, uint32_t t) {
+    intmul_round_finish_kernel<<<1, kImFinishThreads, 0, s_>>>(
+        b.dt.state(), b.dt.tape(), b.slots + (size_t)t * b.per_round, b.claims, b.n_claims,
+        b.sums, b.prefix, b.alphas + (size_t)t * b.n_groups, b.n_groups, b.beta, b.msg,
+        b.chal + t);
+    return check("intmul_round_finish_kernel");
+  }
+  int batch_read(DevBatch& b, StagedReads& rd, std::vector<hu128>& ch) {
+    ch.resize(b.n);
+    if (int rc = b.dt.read(rd, 16 * b.msg * b.n)) return rc;
+    return rd.add(ch.data(), b.chal, 16ull * b.n);
+  }
+  int batch_end(DevBatch& b) { return b.dt.finish(t_); }
   // eq levels of the given points over their first m' <= m coordinates (stride N_ per point).
   int eq_levels(const std::vector<const std::vector<hu128>*>& points, uint32_t m, uint4* out) {
     const uint32_t count = (uint32_t)points.size();
@@ -459,36 +593,24 @@ int IntMulDevice::layer(uint4* set, uint32_t pairs, std::vector<hu128>& point,
   if (n == 0) {
     if (int rc = read_first(set, 2 * pairs, N_, evals)) return rc;
   } else {
-    GruenState g{point, n};
     if (int rc = eq_levels({&point}, n - 1, eq_)) return rc;
-    uint32_t* acc = nullptr;
-    if (int rc = alloc(&acc, 2ull * pairs * n)) return rc;
-    BGPU_CUDA(cudaMemsetAsync(acc, 0, 32ull * pairs * n, s_));
-    std::vector<hu128> sums = claims, ch, last(4 * pairs);
-    std::vector<uint8_t> host(32ull * pairs);
-    hu128 r = 0;
+    std::vector<ImClaim> cl(pairs);
+    for (uint32_t p = 0; p < pairs; p++) cl[p] = ImClaim{(uint16_t)(2 * p), (uint16_t)(2 * p + 1), 2, 0, 0};
+    DevBatch b;
+    if (int rc = batch_begin(b, cl, {&point}, claims, beta, 2 * pairs)) return rc;
     for (uint32_t t = 0; t < n; t++) {
-      uint32_t* out = acc + 8ull * pairs * t;
-      if (int rc = biv_round(set, pairs, 1ull << (n - t), level(eq_, n - t - 1), t > 0, r, out))
+      if (int rc = biv_round(set, pairs, 1ull << (n - t), level(eq_, n - t - 1), batch_r(b, t),
+                             batch_slots(b, t)))
         return rc;
-      StagedReads rd(s_);
-      if (int rc = rd.add(host.data(), out, host.size())) return rc;
-      if (t + 1 == n)
-        if (int rc = copy_pairs(rd, set, 2 * pairs, last.data())) return rc;
-      if (int rc = rd.wait()) return rc;
-      const hu128 alpha = g.alpha();
-      std::vector<Poly> primes, all;
-      for (uint32_t p = 0; p < pairs; p++) {
-        primes.push_back(interp2(sums[p], h128(&host[32 * p]), h128(&host[32 * p + 16]), alpha));
-        all.push_back(by_eq(primes.back(), alpha, g.prefix));
-      }
-      write_batched(t_, all, beta);
-      r = sample(t_);
-      ch.push_back(r);
-      for (uint32_t p = 0; p < pairs; p++) sums[p] = eval_poly(primes[p], r);
-      g.fold(r);
+      if (int rc = batch_round(b, t)) return rc;
     }
-    evals = fold_pairs(last, r);
+    std::vector<hu128> ch, last(4 * pairs);
+    StagedReads rd(s_);
+    if (int rc = batch_read(b, rd, ch)) return rc;
+    if (int rc = copy_pairs(rd, set, 2 * pairs, last.data())) return rc;
+    if (int rc = rd.wait()) return rc;
+    if (int rc = batch_end(b)) return rc;
+    evals = fold_pairs(last, ch[n - 1]);
     point.assign(ch.rbegin(), ch.rend());
   }
   write_elems(t_, evals);
@@ -613,15 +735,24 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
   for (int d = 0; d < 6; d++)
     if (int rc = layer(b_layer(d + 1), 1u << d, pt, evals)) return rc;
 
-  // ---- phase 2: frobenius twist (common.rs:81-105)
-  std::vector<std::vector<hu128>> tw_points(64);
+  // ---- phase 2: frobenius twist (common.rs:81-105): x -> x^(2^(128 - i)); twist i is the
+  // square of twist i + 1, so the 64 twists of a value take 128 squarings in all
+  std::vector<std::vector<hu128>> tw_points(64, std::vector<hu128>(n_));
   std::vector<hu128> sel_sums(64);
-  for (int i = 0; i < 64; i++) {
-    for (hu128 c : pt) tw_points[i].push_back(sq_n(c, 128 - i));
-    sel_sums[i] = sq_n(evals[i], 128 - i);
+  {
+    std::vector<hu128> cur(pt);
+    for (auto& c : cur) c = sq_n(c, 65);  // i = 63: 2^(128 - 63)
+    for (int i = 63; i >= 0; i--) {
+      for (uint32_t j = 0; j < n_; j++) tw_points[i][j] = cur[j];
+      if (i > 0)
+        for (auto& c : cur) c = host_gf_mul(c, c);
+    }
+    for (int i = 0; i < 64; i++) sel_sums[i] = sq_n(evals[i], 128 - i);
   }
 
-  // ---- phase 3: selector prover on (a_root, bits of b) + bivariate c root prover
+  // ---- phase 3: selector prover on (a_root, bits of b) + bivariate c root prover, on the
+  // device transcript: claims 0..63 the selector (slots 2k, 2k + 1, eq point twist k), claim 64
+  // the c root pair (slots 128, 129, eq point point0)
   std::vector<hu128> p3, b_exp_evals;
   hu128 selector_eval, c_lo_root_eval, c_hi_root_eval;
   {
@@ -631,55 +762,40 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
     for (int i = 0; i < 64; i++) tw_ptrs.push_back(&tw_points[i]);
     if (int rc = eq_levels(tw_ptrs, n_ - 1, sel_eqs)) return rc;
     if (int rc = eq_levels({&point0}, n_ - 1, eq_)) return rc;
-    std::vector<GruenState> gs;
-    for (int i = 0; i < 64; i++) gs.push_back(GruenState{tw_points[i], n_});
-    GruenState gc{point0, n_};
     uint4* sel = acl_layer(0);
     uint4* croot = acl_layer(0) + N;
-    hu128 c_sum = c_eval;
     const hu128 beta = sample(t_);
-    uint32_t* acc3 = nullptr;
-    if (int rc = alloc(&acc3, 130ull * n_)) return rc;
-    BGPU_CUDA(cudaMemsetAsync(acc3, 0, 16ull * 130 * n_, s_));
-    std::vector<uint8_t> host(16 * 130);
-    std::vector<hu128> ch, last_cols(128), last_roots(6);
-    hu128 r = 0;
+    std::vector<ImClaim> cl;
+    for (int k = 0; k < 64; k++)
+      cl.push_back(ImClaim{(uint16_t)(2 * k), (uint16_t)(2 * k + 1), 2, (uint8_t)k, 0});
+    cl.push_back(ImClaim{128, 129, 2, 64, 0});
+    std::vector<const std::vector<hu128>*> pts = tw_ptrs;
+    pts.push_back(&point0);
+    std::vector<hu128> sums = sel_sums;
+    sums.push_back(c_eval);
+    DevBatch b;
+    if (int rc = batch_begin(b, cl, pts, sums, beta, 130)) return rc;
     for (uint32_t t = 0; t < n_; t++) {
       const uint64_t L = 1ull << (n_ - t);
-      uint32_t* out = acc3 + 4ull * 130 * t;
-      if (t > 0)
-        if (int rc = fold(sel, 1, L, r)) return rc;  // a_root, shared by the 64 claims
+      uint32_t* out = batch_slots(b, t);
+      const uint4* rp = batch_r(b, t);
+      if (rp)
+        if (int rc = fold(sel, 1, L, rp)) return rc;  // a_root, shared by the 64 claims
       dim3 grid(blocks_for(L / 2, 148 * 2), 64);
       selector_round_kernel<<<grid, kT, 0, s_>>>(sel, bcols, L, N, level(sel_eqs, n_ - t - 1), N,
-                                                 t > 0 ? 1 : 0, u4(r), out);
+                                                 rp, out);
       if (int rc = check("selector_round_kernel")) return rc;
-      if (int rc = biv_round(croot, 1, L, level(eq_, n_ - t - 1), t > 0, r, out + 4 * 128))
-        return rc;
-      StagedReads rd(s_);
-      if (int rc = rd.add(host.data(), out, host.size())) return rc;
-      if (t + 1 == n_) {
-        if (int rc = copy_pairs(rd, bcols, 64, last_cols.data())) return rc;
-        if (int rc = copy_pairs(rd, sel, 3, last_roots.data())) return rc;
-      }
-      if (int rc = rd.wait()) return rc;
-      std::vector<Poly> primes, all;
-      for (int i = 0; i < 64; i++) {
-        const hu128 a = gs[i].alpha();
-        primes.push_back(interp2(sel_sums[i], h128(&host[32 * i]), h128(&host[32 * i + 16]), a));
-        all.push_back(by_eq(primes.back(), a, gs[i].prefix));
-      }
-      primes.push_back(interp2(c_sum, h128(&host[2048]), h128(&host[2048 + 16]), gc.alpha()));
-      all.push_back(by_eq(primes.back(), gc.alpha(), gc.prefix));
-      write_batched(t_, all, beta);
-      r = sample(t_);
-      ch.push_back(r);
-      for (int i = 0; i < 64; i++) {
-        sel_sums[i] = eval_poly(primes[i], r);
-        gs[i].fold(r);
-      }
-      c_sum = eval_poly(primes[64], r);
-      gc.fold(r);
+      if (int rc = biv_round(croot, 1, L, level(eq_, n_ - t - 1), rp, out + 4 * 128)) return rc;
+      if (int rc = batch_round(b, t)) return rc;
     }
+    std::vector<hu128> ch, last_cols(128), last_roots(6);
+    StagedReads rd(s_);
+    if (int rc = batch_read(b, rd, ch)) return rc;
+    if (int rc = copy_pairs(rd, bcols, 64, last_cols.data())) return rc;
+    if (int rc = copy_pairs(rd, sel, 3, last_roots.data())) return rc;
+    if (int rc = rd.wait()) return rc;
+    if (int rc = batch_end(b)) return rc;
+    const hu128 r = ch[n_ - 1];
     const std::vector<hu128> colv = fold_pairs(last_cols, r), roots = fold_pairs(last_roots, r);
     std::vector<hu128> sel_evals = colv;
     sel_evals.push_back(roots[0]);
@@ -716,55 +832,39 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
     t_.message(cb, 16);
     if (int rc = eq_levels({&pt}, n_ - 1, eq_)) return rc;
     if (int rc = eq_levels({&p3}, n_ - 1, eq2_)) return rc;
-    GruenState gb{pt, n_}, gl{pt, n_}, gr{p3, n_};
-    std::vector<hu128> biv_sums = evals;
-    biv_sums.push_back(c_lo_0_eval);
-    hu128 lo_sum = c_lo_0_eval;
-    std::vector<hu128> b_sums = b_exp_evals;
+    // claims 0..96 the leaf pairs (slots 2p, 2p + 1, point pt), 97 the linear c_lo_0 claim (slot
+    // 194, point pt), 98..161 the rerandomised b columns (slots 195 + k, point p3)
     const hu128 beta = sample(t_);
-    constexpr size_t kSlots = 2 * 97 + 1 + 64;
-    uint32_t* acc5 = nullptr;
-    if (int rc = alloc(&acc5, kSlots * n_)) return rc;
-    BGPU_CUDA(cudaMemsetAsync(acc5, 0, 16 * kSlots * n_, s_));
-    std::vector<uint8_t> host(16 * kSlots);
-    std::vector<hu128> ch, last_leaves(2 * 194), last_lo(2), last_b(2 * 64);
-    hu128 r = 0;
+    std::vector<ImClaim> cl;
+    for (int p = 0; p < 97; p++)
+      cl.push_back(ImClaim{(uint16_t)(2 * p), (uint16_t)(2 * p + 1), 2, 0, 0});
+    cl.push_back(ImClaim{194, 0, 1, 0, 0});
+    for (int k = 0; k < 64; k++) cl.push_back(ImClaim{(uint16_t)(195 + k), 0, 1, 1, 0});
+    std::vector<hu128> sums = evals;
+    sums.push_back(c_lo_0_eval);
+    sums.push_back(c_lo_0_eval);
+    sums.insert(sums.end(), b_exp_evals.begin(), b_exp_evals.end());
+    constexpr uint32_t kSlots = 2 * 97 + 1 + 64;
+    DevBatch b;
+    if (int rc = batch_begin(b, cl, {&pt, &p3}, sums, beta, kSlots)) return rc;
     for (uint32_t t = 0; t < n_; t++) {
       const uint64_t L = 1ull << (n_ - t);
-      uint32_t* out = acc5 + 4 * kSlots * t;
-      const bool f = t > 0;
-      if (int rc = biv_round(leaves, 97, L, level(eq_, n_ - t - 1), f, r, out)) return rc;
-      if (int rc = lin_round(lo0, 1, L, level(eq_, n_ - t - 1), f, r, out + 4 * 194)) return rc;
-      if (int rc = lin_round(bcols, 64, L, level(eq2_, n_ - t - 1), f, r, out + 4 * 195)) return rc;
-      StagedReads rd(s_);
-      if (int rc = rd.add(host.data(), out, host.size())) return rc;
-      if (t + 1 == n_) {
-        if (int rc = copy_pairs(rd, leaves, 194, last_leaves.data())) return rc;
-        if (int rc = copy_pairs(rd, lo0, 1, last_lo.data())) return rc;
-        if (int rc = copy_pairs(rd, bcols, 64, last_b.data())) return rc;
-      }
-      if (int rc = rd.wait()) return rc;
-      std::vector<Poly> primes, all;
-      for (int p = 0; p < 97; p++) {
-        primes.push_back(interp2(biv_sums[p], h128(&host[32 * p]), h128(&host[32 * p + 16]), gb.alpha()));
-        all.push_back(by_eq(primes.back(), gb.alpha(), gb.prefix));
-      }
-      primes.push_back(interp1(lo_sum, h128(&host[16 * 194]), gl.alpha()));
-      all.push_back(by_eq(primes.back(), gl.alpha(), gl.prefix));
-      for (int k = 0; k < 64; k++) {
-        primes.push_back(interp1(b_sums[k], h128(&host[16 * (195 + k)]), gr.alpha()));
-        all.push_back(by_eq(primes.back(), gr.alpha(), gr.prefix));
-      }
-      write_batched(t_, all, beta);
-      r = sample(t_);
-      ch.push_back(r);
-      for (int p = 0; p < 97; p++) biv_sums[p] = eval_poly(primes[p], r);
-      lo_sum = eval_poly(primes[97], r);
-      for (int k = 0; k < 64; k++) b_sums[k] = eval_poly(primes[98 + k], r);
-      gb.fold(r);
-      gl.fold(r);
-      gr.fold(r);
+      uint32_t* out = batch_slots(b, t);
+      const uint4* rp = batch_r(b, t);
+      if (int rc = biv_round(leaves, 97, L, level(eq_, n_ - t - 1), rp, out)) return rc;
+      if (int rc = lin_round(lo0, 1, L, level(eq_, n_ - t - 1), rp, out + 4 * 194)) return rc;
+      if (int rc = lin_round(bcols, 64, L, level(eq2_, n_ - t - 1), rp, out + 4 * 195)) return rc;
+      if (int rc = batch_round(b, t)) return rc;
     }
+    std::vector<hu128> ch, last_leaves(2 * 194), last_lo(2), last_b(2 * 64);
+    StagedReads rd(s_);
+    if (int rc = batch_read(b, rd, ch)) return rc;
+    if (int rc = copy_pairs(rd, leaves, 194, last_leaves.data())) return rc;
+    if (int rc = copy_pairs(rd, lo0, 1, last_lo.data())) return rc;
+    if (int rc = copy_pairs(rd, bcols, 64, last_b.data())) return rc;
+    if (int rc = rd.wait()) return rc;
+    if (int rc = batch_end(b)) return rc;
+    const hu128 r = ch[n_ - 1];
     const std::vector<hu128> biv = fold_pairs(last_leaves, r), lo_ev = fold_pairs(last_lo, r),
                              b_ev = fold_pairs(last_b, r);
     write_elems(t_, biv);
