@@ -61,11 +61,13 @@ __device__ __forceinline__ void sha256_compress_1t(uint32_t* st, const uint32_t*
 }
 
 
-// The challenger held in registers by the thread that advances it.  The partial SHA-256 block
-// is kept as 16 big-endian words, zero past `len`, so absorbing a word is a shift/OR into the word
-// at a run-time position -- written as unrolled selects, which keeps every array in registers.
-// The stream is absorbed in 4-byte pieces (every message of the protocol is a whole number of
-// words); a piece may start at any byte offset.
+// The challenger held by the warp that advances it.  The partial SHA-256 block is kept as 16
+// big-endian words, the sample buffer as 8 little-endian words; absorbing a word is one store at
+// a run-time index (the arrays live in local memory, which the out-of-line compression reads
+// anyway), so the code stays small -- it runs once per launch and is fetched cold.  The stream is
+// absorbed in 4-byte pieces (every message of the protocol is a whole number of words); a piece
+// may start at any byte offset.  Words at or past `len` hold no meaning except that a partially
+// filled word is zero past its bytes.
 struct DevTr {
   uint32_t h[8], w[16], len;  // chaining value, partial block, bytes in it
   uint64_t total;             // bytes absorbed since the last reset
@@ -74,15 +76,12 @@ struct DevTr {
   uint32_t tape_len, tape_cap, error;
 
   __device__ __forceinline__ void load(const TranscriptState* g) {
-#pragma unroll
     for (int i = 0; i < 8; i++) h[i] = g->h[i];
-#pragma unroll
     for (int i = 0; i < 16; i++) w[i] = g->w[i];
     len = g->block_len & 63u;
     total = g->total;
     sampling = g->sampling;
     index = g->index;
-#pragma unroll
     for (int i = 0; i < 8; i++) buf[i] = g->buf[i];
     tape_len = g->tape_len;
     tape_cap = g->tape_cap;
@@ -90,73 +89,57 @@ struct DevTr {
   }
 
   __device__ __forceinline__ void store(TranscriptState* g) const {
-#pragma unroll
     for (int i = 0; i < 8; i++) g->h[i] = h[i];
-#pragma unroll
     for (int i = 0; i < 16; i++) g->w[i] = w[i];
     g->block_len = len;
     g->total = total;
     g->sampling = sampling;
     g->index = index;
-#pragma unroll
     for (int i = 0; i < 8; i++) g->buf[i] = buf[i];
     g->tape_len = tape_len;
     g->tape_cap = tape_cap;
     g->error = error;
   }
 
-  __device__ __forceinline__ void or_word(uint32_t k, uint32_t v) {
-#pragma unroll
-    for (uint32_t i = 0; i < 16; i++)
-      if (i == k) w[i] |= v;
-  }
-
-  __device__ __forceinline__ void compress_block() {
-    sha256_compress_1t(h, w);
-#pragma unroll
-    for (int i = 0; i < 16; i++) w[i] = 0;
-    len = 0;
-  }
-
   // Absorbs 4 stream bytes given as a little-endian word (first byte lowest).
-  __device__ __forceinline__ void absorb_word(uint32_t le) {
+  __device__ __noinline__ void absorb_word(uint32_t le) {
     const uint32_t be = bswap32(le);
     const uint32_t off = len & 3u;
     total += 4;
     if (off == 0) {
-      or_word(len >> 2, be);
+      w[len >> 2] = be;
       len += 4;
-      if (len == 64) compress_block();
+      if (len == 64) {
+        sha256_compress_1t(h, w);
+        len = 0;
+      }
     } else {
-      or_word(len >> 2, be >> (8 * off));
+      w[len >> 2] |= be >> (8 * off);
       len += 4 - off;
-      if (len == 64) compress_block();
-      or_word(len >> 2, be << (8 * (4 - off)));
+      if (len == 64) {
+        sha256_compress_1t(h, w);
+        len = 0;
+      }
+      w[len >> 2] = be << (8 * (4 - off));
       len += off;
     }
   }
 
   // Digest of the stream (FIPS 180-4 padding) as 8 big-endian words; the stream is unchanged.
-  __device__ __forceinline__ void digest(uint32_t d[8]) const {
+  __device__ __noinline__ void digest(uint32_t d[8]) const {
     uint32_t st[8], m[16];
-#pragma unroll
     for (int i = 0; i < 8; i++) st[i] = h[i];
-#pragma unroll
-    for (int i = 0; i < 16; i++) m[i] = w[i];
-    const uint32_t pad = 0x80u << (24 - 8 * (len & 3u));
-#pragma unroll
-    for (uint32_t i = 0; i < 16; i++)
-      if (i == (len >> 2)) m[i] |= pad;
+    const uint32_t full = len >> 2, part = len & 3u;
+    for (uint32_t i = 0; i < 16; i++) m[i] = (i < full || (i == full && part)) ? w[i] : 0u;
+    m[full] |= 0x80u << (24 - 8 * part);
     const uint64_t bits = total * 8;
     if (len + 9 > 64) {
       sha256_compress_1t(st, m);
-#pragma unroll
       for (int i = 0; i < 16; i++) m[i] = 0;
     }
     m[14] = (uint32_t)(bits >> 32);
     m[15] = (uint32_t)bits;
     sha256_compress_1t(st, m);
-#pragma unroll
     for (int i = 0; i < 8; i++) d[i] = st[i];
   }
 
@@ -203,29 +186,19 @@ struct DevTr {
   }
 
   // Refills the sample buffer from the digest of the stream, which restarts as that digest.
-  __device__ __forceinline__ void refill() {
+  __device__ __noinline__ void refill() {
     uint32_t d[8];
     digest(d);
     const uint32_t iv[8] = {0x6a09e667u, 0xbb67ae85u, 0x3c6ef372u, 0xa54ff53au,
                             0x510e527fu, 0x9b05688cu, 0x1f83d9abu, 0x5be0cd19u};
-#pragma unroll
     for (int i = 0; i < 8; i++) {
       h[i] = iv[i];
       w[i] = d[i];
-      w[8 + i] = 0;
       buf[i] = bswap32(d[i]);
     }
     len = 32;
     total = 32;
     index = 0;
-  }
-
-  __device__ __forceinline__ uint32_t buf_byte(uint32_t i) const {
-    uint32_t v = 0;
-#pragma unroll
-    for (uint32_t k = 0; k < 8; k++)
-      if (k == (i >> 2)) v = buf[k];
-    return (v >> (8 * (i & 3u))) & 255u;
   }
 
   __device__ __forceinline__ void begin_sampling() {
@@ -241,25 +214,19 @@ struct DevTr {
     for (uint32_t i = 0; i < (n + 3) / 4; i++) out[i] = 0;
     for (uint32_t i = 0; i < n; i++) {
       if (index == 32) refill();
-      out[i >> 2] |= buf_byte(index) << (8 * (i & 3u));
+      out[i >> 2] |= ((buf[index >> 2] >> (8 * (index & 3u))) & 255u) << (8 * (i & 3u));
       index++;
     }
   }
 
-  // A field element: 16 bytes read as a little-endian u128 (transcript.rs:398-407).  The common
-  // case (a word-aligned read within the buffer) is four register selects.
+  // A field element: 16 bytes read as a little-endian u128 (transcript.rs:398-407).
   __device__ __forceinline__ uint4 sample_elem() {
     begin_sampling();
     if (index == 32) refill();
     if ((index & 3u) == 0 && index + 16 <= 32) {
-      uint32_t o[4] = {0, 0, 0, 0};
-#pragma unroll
-      for (uint32_t k = 0; k < 8; k++)
-#pragma unroll
-        for (uint32_t j = 0; j < 4; j++)
-          if (k == (index >> 2) + j) o[j] = buf[k];
+      const uint32_t k = index >> 2;
       index += 16;
-      return make_uint4(o[0], o[1], o[2], o[3]);
+      return make_uint4(buf[k], buf[k + 1], buf[k + 2], buf[k + 3]);
     }
     uint32_t o[4];
     sample_words(o, 16);
