@@ -29,6 +29,7 @@
 
 #include "cs.h"
 #include "dev_transcript.cuh"
+#include "pdl.cuh"
 #include "gf128.cuh"
 #include "gf_reduce.cuh"
 #include "internal.h"
@@ -359,6 +360,8 @@ __global__ void __launch_bounds__(256, 2)
     and_mle_fold_eval_kernel(uint4* __restrict__ fa, uint4* __restrict__ fb, uint4* __restrict__ fc,
                              uint4* __restrict__ eq, uint64_t size, const uint4* __restrict__ r_ptr,
                              const uint4* __restrict__ tab, uint32_t* __restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
   const uint64_t h = size >> 1, q = size >> 2;
   u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
   uint4 s1r = gf_zero(), sinfr = gf_zero();  // small rounds: reduced sums
@@ -411,6 +414,8 @@ __global__ void __launch_bounds__(256)
                             const uint4* __restrict__ ys, const AndRoundConst* __restrict__ rc,
                             uint4* __restrict__ claim, uint4* __restrict__ r_out,
                             uint4* __restrict__ tab) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ uint4 r_sh;
   if (threadIdx.x < 32) {
     DevTr st;
@@ -444,6 +449,8 @@ __global__ void __launch_bounds__(kAndTailThreads)
                     uint4* __restrict__ eq, uint64_t len, uint32_t n_rounds,
                     const uint4* __restrict__ r_first, const AndRoundConst* __restrict__ rc,
                     uint4* __restrict__ claim, uint4* __restrict__ chal) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ uint4 r_sh;
   DevTr st;
   uint4 cl = gf_zero();
@@ -661,32 +668,29 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
       if (n_rem == log_n) {
         and_mle_eval_kernel<<<grid_for(size / 2, 256), 256, 0, s>>>(fa, fb, fc, eq, size / 2,
                                                                     acc);
+        e = cudaGetLastError();
       } else if (size * 2 >= kMulTableMinSize) {
-        and_mle_fold_eval_kernel<true><<<grid_for(size / 2, 256), 256, 0, s>>>(
-            fa, fb, fc, eq, size * 2, d_chal + k - 1, mul_tab, acc);
+        e = launch_pdl(and_mle_fold_eval_kernel<true>, grid_for(size / 2, 256), 256, 0, s, fa, fb,
+                       fc, eq, size * 2, d_chal + k - 1, mul_tab, acc);
       } else {
-        and_mle_fold_eval_kernel<false><<<grid_for(size / 2, 256), 256, 0, s>>>(
-            fa, fb, fc, eq, size * 2, d_chal + k - 1, nullptr, acc);
+        e = launch_pdl(and_mle_fold_eval_kernel<false>, grid_for(size / 2, 256), 256, 0, s, fa, fb,
+                       fc, eq, size * 2, d_chal + k - 1, (const uint4*)nullptr, acc);
       }
-      e = cudaGetLastError();
       if (e != cudaSuccess) { rc = cuda_error(e, "AND MLE-check round"); break; }
       // the next round folds by this round's challenge through a table when it is large
       const bool next_tab = n_rem > 1 && size >= kMulTableMinSize;
-      and_round_finish_kernel<<<1, 256, 0, s>>>(dt.state(), dt.tape(),
-                                                reinterpret_cast<const uint4*>(acc),
-                                                d_consts + k, d_claim, d_chal + k,
-                                                next_tab ? mul_tab : nullptr);
-      e = cudaGetLastError();
+      e = launch_pdl(and_round_finish_kernel, 1, 256, 0, s, dt.state(), dt.tape(),
+                     reinterpret_cast<const uint4*>(acc), (const AndRoundConst*)(d_consts + k),
+                     d_claim, d_chal + k, next_tab ? mul_tab : (uint4*)nullptr);
       if (e != cudaSuccess) { rc = cuda_error(e, "and_round_finish_kernel"); break; }
       count_launch(2);
     }
     if (rc) break;
     if (tail_n) {
       const uint32_t k0 = log_n - tail_n;
-      and_tail_kernel<<<1, kAndTailThreads, 0, s>>>(dt.state(), dt.tape(), fa, fb, fc, eq,
-                                                     2ull << tail_n, tail_n, d_chal + k0 - 1,
-                                                     d_consts + k0, d_claim, d_chal + k0);
-      e = cudaGetLastError();
+      e = launch_pdl(and_tail_kernel, 1, kAndTailThreads, 0, s, dt.state(), dt.tape(), fa, fb, fc,
+                     eq, 2ull << tail_n, tail_n, (const uint4*)(d_chal + k0 - 1),
+                     (const AndRoundConst*)(d_consts + k0), d_claim, d_chal + k0);
       if (e != cudaSuccess) { rc = cuda_error(e, "and_tail_kernel"); break; }
       count_launch();
     }

@@ -27,6 +27,7 @@
 
 #include "cs.h"
 #include "dev_transcript.cuh"
+#include "pdl.cuh"
 #include "gf128.cuh"
 #include "gf_reduce.cuh"
 #include "internal.h"
@@ -114,6 +115,8 @@ __global__ void __launch_bounds__(kT)
     biv_round_kernel(uint4* __restrict__ set, uint64_t L, uint64_t stride,
                      const uint4* __restrict__ eq, const uint4* __restrict__ r_ptr,
                      uint32_t* __restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
   const bool fold = r_ptr != nullptr;
   const uint4 r = fold ? *r_ptr : gf_zero();
   const uint32_t p = blockIdx.y;
@@ -153,6 +156,8 @@ __global__ void __launch_bounds__(kT)
     lin_round_kernel(uint4* __restrict__ set, uint64_t L, uint64_t stride,
                      const uint4* __restrict__ eq, const uint4* __restrict__ r_ptr,
                      uint32_t* __restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
   const bool fold = r_ptr != nullptr;
   const uint4 r = fold ? *r_ptr : gf_zero();
   const uint32_t k = blockIdx.y;
@@ -182,6 +187,8 @@ __global__ void __launch_bounds__(kT)
     selector_round_kernel(const uint4* __restrict__ sel, uint4* __restrict__ cols, uint64_t L,
                           uint64_t stride, const uint4* __restrict__ eqs, uint64_t eq_stride,
                           const uint4* __restrict__ r_ptr, uint32_t* __restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
   const bool fold = r_ptr != nullptr;
   const uint4 r = fold ? *r_ptr : gf_zero();
   const uint32_t k = blockIdx.y;
@@ -212,6 +219,8 @@ __global__ void __launch_bounds__(kT)
 // In-place top-variable fold of `count` multilinears of length 2 * half.
 __global__ void fold_set_kernel(uint4* __restrict__ set, uint32_t count, uint64_t half,
                                 uint64_t stride, const uint4* __restrict__ r_ptr) {
+  pdl_wait();
+  pdl_trigger();
   const uint4 r = *r_ptr;
   const uint64_t total = (uint64_t)count * half;
   for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total;
@@ -287,6 +296,8 @@ __global__ void __launch_bounds__(kImFinishThreads)
                                uint4* __restrict__ prefix, const ImAlpha* __restrict__ alphas,
                                uint32_t n_groups, const uint4* __restrict__ beta_pow,
                                uint32_t msg_coeffs, uint4* __restrict__ r_out) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ uint4 s_prime[kImMaxClaims][3];
   __shared__ uint4 s_r;
   uint4 acc[4] = {gf_zero(), gf_zero(), gf_zero(), gf_zero()};
@@ -449,7 +460,8 @@ class IntMulDevice {
   }
   int fold(uint4* set, uint32_t count, uint64_t half, const uint4* r_ptr) {
     if (half == 0) return BINIUS_OK;
-    fold_set_kernel<<<blocks_for((uint64_t)count * half), kT, 0, s_>>>(set, count, half, N_, r_ptr);
+    BGPU_CUDA(launch_pdl(fold_set_kernel, blocks_for((uint64_t)count * half), kT, 0, s_, set, count,
+                         half, N_, r_ptr));
     return check("fold_set_kernel");
   }
   // Fused round launches on multilinears of current length L (fold from 2L first by *r_ptr when
@@ -457,13 +469,13 @@ class IntMulDevice {
   int biv_round(uint4* set, uint32_t pairs, uint64_t L, const uint4* eq, const uint4* r_ptr,
                 uint32_t* out) {
     dim3 grid(blocks_for(L / 2, 148 * 2), pairs);
-    biv_round_kernel<<<grid, kT, 0, s_>>>(set, L, N_, eq, r_ptr, out);
+    BGPU_CUDA(launch_pdl(biv_round_kernel, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out));
     return check("biv_round_kernel");
   }
   int lin_round(uint4* set, uint32_t cols, uint64_t L, const uint4* eq, const uint4* r_ptr,
                 uint32_t* out) {
     dim3 grid(blocks_for(L / 2, 148 * 2), cols);
-    lin_round_kernel<<<grid, kT, 0, s_>>>(set, L, N_, eq, r_ptr, out);
+    BGPU_CUDA(launch_pdl(lin_round_kernel, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out));
     return check("lin_round_kernel");
   }
   // A batched MLE-check whose rounds run on the device transcript: batch_begin uploads the claims,
@@ -534,10 +546,11 @@ class IntMulDevice {
     return t ? b.chal + t - 1 : nullptr;
   }
   int batch_round(DevBatch& b, uint32_t t) {
-    intmul_round_finish_kernel<<<1, kImFinishThreads, 0, s_>>>(
-        b.dt.state(), b.dt.tape(), b.slots + (size_t)t * b.per_round, b.claims, b.n_claims,
-        b.sums, b.prefix, b.alphas + (size_t)t * b.n_groups, b.n_groups, b.beta, b.msg,
-        b.chal + t);
+    BGPU_CUDA(launch_pdl(intmul_round_finish_kernel, 1, kImFinishThreads, 0, s_, b.dt.state(),
+                         b.dt.tape(), (const uint4*)(b.slots + (size_t)t * b.per_round),
+                         (const ImClaim*)b.claims, b.n_claims, b.sums, b.prefix,
+                         (const ImAlpha*)(b.alphas + (size_t)t * b.n_groups), b.n_groups,
+                         (const uint4*)b.beta, b.msg, b.chal + t));
     return check("intmul_round_finish_kernel");
   }
   int batch_read(DevBatch& b, StagedReads& rd, std::vector<hu128>& ch) {
@@ -782,8 +795,8 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
       if (rp)
         if (int rc = fold(sel, 1, L, rp)) return rc;  // a_root, shared by the 64 claims
       dim3 grid(blocks_for(L / 2, 148 * 2), 64);
-      selector_round_kernel<<<grid, kT, 0, s_>>>(sel, bcols, L, N, level(sel_eqs, n_ - t - 1), N,
-                                                 rp, out);
+      BGPU_CUDA(launch_pdl(selector_round_kernel, grid, kT, 0, s_, (const uint4*)sel, bcols, L, N,
+                           level(sel_eqs, n_ - t - 1), N, rp, out));
       if (int rc = check("selector_round_kernel")) return rc;
       if (int rc = biv_round(croot, 1, L, level(eq_, n_ - t - 1), rp, out + 4 * 128)) return rc;
       if (int rc = batch_round(b, t)) return rc;

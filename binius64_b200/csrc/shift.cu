@@ -29,6 +29,7 @@
 
 #include "cs.h"
 #include "dev_transcript.cuh"
+#include "pdl.cuh"
 #include "gf128.cuh"
 #include "gf_reduce.cuh"
 #include "internal.h"
@@ -299,6 +300,8 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(256)
     dot2_kernel(const uint4* __restrict__ x, uint64_t off0, uint64_t off1,
                 const uint4* __restrict__ eq, uint64_t len, uint32_t* __restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
   u256 a0 = {0, 0, 0, 0}, a1 = {0, 0, 0, 0};
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < len;
        i += (uint64_t)gridDim.x * blockDim.x) {
@@ -331,6 +334,8 @@ __global__ void __launch_bounds__(256)
                               const uint4* __restrict__ init_lohi, uint4 z0, uint4 beta,
                               uint4* __restrict__ st3, uint4* __restrict__ r_out,
                               uint4* __restrict__ tab) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ uint4 r_sh;
   if (threadIdx.x < 32) {
     DevTr st;
@@ -387,6 +392,8 @@ __global__ void __launch_bounds__(kShiftTailThreads)
                       uint32_t n_rem0, uint32_t p, const uint4* __restrict__ r_first,
                       const ShiftRoundConst* __restrict__ rc, uint4 beta, uint4* __restrict__ run,
                       uint4* __restrict__ chal) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ uint4 r_sh;
   DevTr st;
   uint4 sum = gf_zero(), inout = gf_zero(), eqp = gf_zero();
@@ -693,9 +700,15 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
   std::vector<hu128> z(p);
   for (auto& v : z) v = sample(t);
   const hu128 beta = sample(t);
-  auto dot2 = [&](uint64_t off0, uint64_t off1, uint64_t len, uint4* out) -> int {
-    dot2_kernel<<<grid_for(len, 256, 148 * 2), 256, 0, s>>>(W, off0, off1, eq_pub, len,
-                                                            reinterpret_cast<uint32_t*>(out));
+  // in the round loop dot2 follows a kernel and is launched programmatically (PDL relaxes only
+  // kernel-to-kernel order); the first one follows a memset and is launched plainly
+  auto dot2 = [&](uint64_t off0, uint64_t off1, uint64_t len, uint4* out, bool pdl = true) -> int {
+    const unsigned grid = grid_for(len, 256, 148 * 2);
+    if (pdl)
+      BGPU_CUDA(launch_pdl(dot2_kernel, grid, 256, 0, s, (const uint4*)W, off0, off1,
+                           (const uint4*)eq_pub, len, reinterpret_cast<uint32_t*>(out)));
+    else
+      dot2_kernel<<<grid, 256, 0, s>>>(W, off0, off1, eq_pub, len, reinterpret_cast<uint32_t*>(out));
     SHIFT_TRY(launched("dot2_kernel"));
     return BINIUS_OK;
   };
@@ -704,7 +717,7 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
   uint4* run = dstate + 1;
   uint4* init_lohi = dstate + 4;
   BGPU_CUDA(cudaMemsetAsync(init_lohi, 0, 32, s));
-  SHIFT_TRY(dot2(0, 1ull << (gn - 1), 1ull << (gn - 1), init_lohi));
+  SHIFT_TRY(dot2(0, 1ull << (gn - 1), 1ull << (gn - 1), init_lohi, false));
   const uint4 z0 = u4(z[gn - 1]);
   std::vector<ShiftRoundConst> consts(log_words);
   {
@@ -754,17 +767,18 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
     }
     if (n_rem <= p) gn--;
     const bool next_tab = n_rem > 1 && half * 2 >= kMulTableMinSize;
-    shift_round_finish_kernel<<<1, 256, 0, s>>>(
-        dt.state(), dt.tape(), ys, rconst + k, n_rem == log_words ? init_lohi : nullptr, z0,
-        u4(beta), run, chal + 12 + k, next_tab ? tab : nullptr);
+    BGPU_CUDA(launch_pdl(shift_round_finish_kernel, 1, 256, 0, s, dt.state(), dt.tape(),
+                         (const uint4*)ys, (const ShiftRoundConst*)(rconst + k),
+                         n_rem == log_words ? (const uint4*)init_lohi : (const uint4*)nullptr, z0,
+                         u4(beta), run, chal + 12 + k, next_tab ? tab : (uint4*)nullptr));
     SHIFT_TRY(launched("shift_round_finish_kernel"));
   }
   if (tail_n) {
     const uint32_t k0 = log_words - tail_n;
     if (tail_n <= p) SHIFT_TRY(eq_tensor(to_u4(z).data(), tail_n - 1, eq_pub, s));
-    shift_tail_kernel<<<1, kShiftTailThreads, 0, s>>>(dt.state(), dt.tape(), W, M, eq_pub, tail_n,
-                                                      p, chal + 12 + k0 - 1, rconst + k0, u4(beta),
-                                                      run, chal + 12 + k0);
+    BGPU_CUDA(launch_pdl(shift_tail_kernel, 1, kShiftTailThreads, 0, s, dt.state(), dt.tape(), W,
+                         M, eq_pub, tail_n, p, (const uint4*)(chal + 12 + k0 - 1),
+                         (const ShiftRoundConst*)(rconst + k0), u4(beta), run, chal + 12 + k0));
     SHIFT_TRY(launched("shift_tail_kernel"));
   }
   {

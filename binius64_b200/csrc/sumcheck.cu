@@ -20,6 +20,7 @@
 #include <algorithm>
 
 #include "dev_transcript.cuh"
+#include "pdl.cuh"
 #include "gf128.cuh"
 #include "gf_reduce.cuh"
 #include "internal.h"
@@ -39,22 +40,32 @@ unsigned grid_for(uint64_t n, unsigned threads, unsigned max_blocks = 148 * 8) {
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, max_blocks));
 }
 
-// out[j] = prod_i (bit_i(j) ? r_i : 1 + r_i).  The n factors are multiplied as a balanced tree
-// (depth ceil(log2 n) instead of a chain of n dependent multiplies), out of line: these tensors are
-// small and on the protocol's critical path, so latency and code size matter, not throughput.
-__global__ void eq_small_kernel(uint4* __restrict__ out, Point32 p, uint32_t off, uint32_t n) {
+// out[j] = prod_i (bit_i(j) ? r_i : 1 + r_i) for n <= 16 coordinates.  Each block first builds
+// the eq tensors of the low k = min(n, 8) and the high n - k coordinates (at most 256 entries
+// each) in shared memory, then every output is one multiply lo[j mod 2^k] * hi[j >> k]: the
+// dependent chain is at most 8 multiplies + 1, where multiplying all n factors per output would be
+// n - 1.  These tensors are small and on the protocol's critical path, so latency matters.
+__global__ void __launch_bounds__(256)
+    eq_small_kernel(uint4* __restrict__ out, Point32 p, uint32_t off, uint32_t n) {
+  __shared__ uint4 s_lo[256], s_hi[256];
+  const uint32_t k = n < 8 ? n : 8, m = n - k;
+  const uint32_t n_lo = 1u << k, n_hi = 1u << m;
+  for (uint32_t t = threadIdx.x; t < n_lo + n_hi; t += blockDim.x) {
+    const bool lo = t < n_lo;
+    const uint32_t idx = lo ? t : t - n_lo, first = lo ? 0 : k, cnt = lo ? k : m;
+    uint4 acc = gf_one();
+    for (uint32_t i = 0; i < cnt; i++) {
+      uint4 f = p.r[off + first + i];
+      if (!((idx >> i) & 1)) f.x ^= 1u;
+      acc = gf_mul(acc, f);
+    }
+    (lo ? s_lo : s_hi)[idx] = acc;
+  }
+  __syncthreads();
   const uint64_t total = 1ull << n;
   for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < total;
-       j += (uint64_t)gridDim.x * blockDim.x) {
-    uint4 f[32];
-    for (uint32_t i = 0; i < n; i++) {
-      f[i] = p.r[off + i];
-      if (!((j >> i) & 1)) f[i].x ^= 1u;
-    }
-    for (uint32_t step = 1; step < n; step <<= 1)
-      for (uint32_t i = 0; i + step < n; i += 2 * step) f[i] = gf_mul_nl(f[i], f[i + step]);
-    out[j] = n ? f[0] : gf_one();
-  }
+       j += (uint64_t)gridDim.x * blockDim.x)
+    out[j] = gf_mul(s_lo[j & (n_lo - 1)], s_hi[j >> k]);
 }
 
 __global__ void eq_expand_kernel(uint4* __restrict__ out, const uint4* __restrict__ lo,
@@ -157,6 +168,8 @@ __global__ void __launch_bounds__(kThreads)
     bivariate_fold_eval_kernel(uint4* __restrict__ a, uint4* __restrict__ b, uint64_t size,
                                uint4 r_arg, const uint4* __restrict__ r_ptr,
                                const uint4* __restrict__ tab, uint32_t* __restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
   const uint64_t h = size >> 1, q = size >> 2;
   u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
   uint4 s1r = gf_zero(), sinfr = gf_zero();  // small rounds: reduced sums
@@ -199,6 +212,8 @@ __global__ void __launch_bounds__(256)
                                   const uint4* __restrict__ ys, const uint4* __restrict__ claim_init,
                                   uint4* __restrict__ claim, const uint8_t* __restrict__ commitment,
                                   uint4* __restrict__ r_out, uint4* __restrict__ tab) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ uint4 r_sh;
   if (threadIdx.x < 32) {
     DevTr st;
@@ -236,6 +251,8 @@ __global__ void __launch_bounds__(kTailThreads)
                           uint4* __restrict__ a, uint4* __restrict__ b, uint64_t len,
                           uint32_t n_rounds, const uint4* __restrict__ r_first,
                           uint4* __restrict__ claim, uint4* __restrict__ chal) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ uint4 r_sh;
   DevTr st;
   uint4 cl = gf_zero();
@@ -319,7 +336,7 @@ int eq_tensor(const uint4* h_point, uint32_t n, uint4* d_out, cudaStream_t s) {
   Point32 p;
   memset(&p, 0, sizeof(p));
   if (n) memcpy(p.r, h_point, 16 * (size_t)n);
-  if (n <= 12) {
+  if (n <= 16) {
     eq_small_kernel<<<grid_for(1ull << n, kThreads), kThreads, 0, s>>>(d_out, p, 0, n);
     BGPU_LAUNCH_CHECK("eq_small_kernel");
     count_launch();
@@ -421,15 +438,16 @@ int bivariate_fold_eval_dev(uint4* d_a, uint4* d_b, uint64_t size, const uint4* 
                             const uint4* d_tab, uint32_t* d_out8, cudaStream_t s) {
   if (size < 4) return set_error(BINIUS_E_ARG, "bivariate_fold_eval needs size >= 4");
   const unsigned grid = grid_for(size / 4, kThreads);
+  cudaError_t e;
   if (size >= kMulTableMinSize) {
     if (!d_tab) return set_error(BINIUS_E_ARG, "a large fold needs the challenge's table");
-    bivariate_fold_eval_kernel<true><<<grid, kThreads, 0, s>>>(d_a, d_b, size, gf_zero_host(),
-                                                               nullptr, d_tab, d_out8);
+    e = launch_pdl(bivariate_fold_eval_kernel<true>, grid, kThreads, 0, s, d_a, d_b, size,
+                   gf_zero_host(), (const uint4*)nullptr, d_tab, d_out8);
   } else {
-    bivariate_fold_eval_kernel<false><<<grid, kThreads, 0, s>>>(d_a, d_b, size, gf_zero_host(),
-                                                                d_r, nullptr, d_out8);
+    e = launch_pdl(bivariate_fold_eval_kernel<false>, grid, kThreads, 0, s, d_a, d_b, size,
+                   gf_zero_host(), d_r, (const uint4*)nullptr, d_out8);
   }
-  BGPU_LAUNCH_CHECK("bivariate_fold_eval_kernel");
+  if (e != cudaSuccess) return cuda_error(e, "bivariate_fold_eval_kernel");
   count_launch();
   return BINIUS_OK;
 }
@@ -437,9 +455,9 @@ int bivariate_fold_eval_dev(uint4* d_a, uint4* d_b, uint64_t size, const uint4* 
 int bivariate_round_finish(const DeviceTranscript& dt, const uint4* d_ys, const uint4* d_claim_init,
                            uint4* d_claim, const uint8_t* d_commitment, uint4* d_r_out,
                            uint4* d_tab, cudaStream_t s) {
-  bivariate_round_finish_kernel<<<1, 256, 0, s>>>(dt.state(), dt.tape(), d_ys, d_claim_init,
-                                                  d_claim, d_commitment, d_r_out, d_tab);
-  BGPU_LAUNCH_CHECK("bivariate_round_finish_kernel");
+  cudaError_t e = launch_pdl(bivariate_round_finish_kernel, 1, 256, 0, s, dt.state(), dt.tape(),
+                             d_ys, d_claim_init, d_claim, d_commitment, d_r_out, d_tab);
+  if (e != cudaSuccess) return cuda_error(e, "bivariate_round_finish_kernel");
   count_launch();
   return BINIUS_OK;
 }
@@ -450,9 +468,9 @@ int bivariate_tail(const DeviceTranscript& dt, uint4* d_a, uint4* d_b, uint64_t 
   if (n_rounds == 0) return BINIUS_OK;
   if ((len >> (n_rounds - (d_r_first ? 0 : 1))) < 2)
     return set_error(BINIUS_E_ARG, "bivariate tail: more rounds than variables");
-  bivariate_tail_kernel<<<1, kTailThreads, 0, s>>>(dt.state(), dt.tape(), d_a, d_b, len, n_rounds,
-                                                   d_r_first, d_claim, d_chal);
-  BGPU_LAUNCH_CHECK("bivariate_tail_kernel");
+  cudaError_t e = launch_pdl(bivariate_tail_kernel, 1, kTailThreads, 0, s, dt.state(), dt.tape(),
+                             d_a, d_b, len, n_rounds, d_r_first, d_claim, d_chal);
+  if (e != cudaSuccess) return cuda_error(e, "bivariate_tail_kernel");
   count_launch();
   return BINIUS_OK;
 }
