@@ -40,6 +40,9 @@ using namespace bgpu;
 namespace {
 
 constexpr int kT = 256;
+// Round kernels on multilinears of at most this many elements run few threads once per launch,
+// so they take the compact out-of-line multiply (their code is fetched cold).
+constexpr uint64_t kSmallRound = 1ull << 12;
 
 struct Pow64 {
   uint4 p[64];
@@ -111,6 +114,7 @@ __device__ __forceinline__ uint4 fold1(uint4 lo, uint4 hi, uint4 r) {
 // `fold`, both multilinears first shrink from 2L to L by r in place (fold_highest_var_inplace);
 // thread i owns positions i and i + L/2, so the fold and the round need one pass.  Grid: (chunks,
 // pairs).  The fold's r is *r_ptr (a challenge in HBM); r_ptr == nullptr means no fold.
+template <bool SMALL>
 __global__ void __launch_bounds__(kT)
     biv_round_kernel(uint4* __restrict__ set, uint64_t L, uint64_t stride,
                      const uint4* __restrict__ eq, const uint4* __restrict__ r_ptr,
@@ -124,14 +128,17 @@ __global__ void __launch_bounds__(kT)
   uint4* b = a + stride;
   const uint64_t h = L >> 1;
   u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
+  uint4 s1r = gf_zero(), sinfr = gf_zero();
+  // small rounds run once on few threads: one out-of-line multiply keeps the code compact
+  auto mul = [](uint4 x, uint4 y) { return SMALL ? gf_mul_nl(x, y) : gf_mul(x, y); };
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < h;
        i += (uint64_t)gridDim.x * blockDim.x) {
     uint4 a0, a1, b0, b1;
     if (fold) {
-      a0 = fold1(a[i], a[L + i], r);
-      a1 = fold1(a[h + i], a[L + h + i], r);
-      b0 = fold1(b[i], b[L + i], r);
-      b1 = fold1(b[h + i], b[L + h + i], r);
+      a0 = gf_add(a[i], mul(r, gf_add(a[L + i], a[i])));
+      a1 = gf_add(a[h + i], mul(r, gf_add(a[L + h + i], a[h + i])));
+      b0 = gf_add(b[i], mul(r, gf_add(b[L + i], b[i])));
+      b1 = gf_add(b[h + i], mul(r, gf_add(b[L + h + i], b[h + i])));
       a[i] = a0;
       a[h + i] = a1;
       b[i] = b0;
@@ -143,15 +150,21 @@ __global__ void __launch_bounds__(kT)
       b1 = b[h + i];
     }
     const uint4 e = eq[i];
-    xor_into(s1, clmul128(e, gf_mul(a1, b1)));
-    xor_into(sinf, clmul128(e, gf_mul(gf_add(a0, a1), gf_add(b0, b1))));
+    if constexpr (SMALL) {
+      gf_add_into(s1r, gf_mul_nl(e, gf_mul_nl(a1, b1)));
+      gf_add_into(sinfr, gf_mul_nl(e, gf_mul_nl(gf_add(a0, a1), gf_add(b0, b1))));
+    } else {
+      xor_into(s1, clmul128(e, gf_mul(a1, b1)));
+      xor_into(sinf, clmul128(e, gf_mul(gf_add(a0, a1), gf_add(b0, b1))));
+    }
   }
-  uint4 v[2] = {reduce256(s1), reduce256(sinf)};
+  uint4 v[2] = {SMALL ? s1r : reduce256(s1), SMALL ? sinfr : reduce256(sinf)};
   block_xor_reduce<2>(v, out + 8 * p);
 }
 
 // Column k of `set` (current length L): out[4k..] += sum eq[i] col_k[L/2 + i], with the same
 // optional fused fold.  Grid: (chunks, columns).
+template <bool SMALL>
 __global__ void __launch_bounds__(kT)
     lin_round_kernel(uint4* __restrict__ set, uint64_t L, uint64_t stride,
                      const uint4* __restrict__ eq, const uint4* __restrict__ r_ptr,
@@ -164,25 +177,31 @@ __global__ void __launch_bounds__(kT)
   uint4* c = set + k * stride;
   const uint64_t h = L >> 1;
   u256 s1 = {0, 0, 0, 0};
+  uint4 s1r = gf_zero();
+  auto mul = [](uint4 x, uint4 y) { return SMALL ? gf_mul_nl(x, y) : gf_mul(x, y); };
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < h;
        i += (uint64_t)gridDim.x * blockDim.x) {
     uint4 c1;
     if (fold) {
-      c[i] = fold1(c[i], c[L + i], r);
-      c1 = fold1(c[h + i], c[L + h + i], r);
+      c[i] = gf_add(c[i], mul(r, gf_add(c[L + i], c[i])));
+      c1 = gf_add(c[h + i], mul(r, gf_add(c[L + h + i], c[h + i])));
       c[h + i] = c1;
     } else {
       c1 = c[h + i];
     }
-    xor_into(s1, clmul128(eq[i], c1));
+    if constexpr (SMALL)
+      gf_add_into(s1r, gf_mul_nl(eq[i], c1));
+    else
+      xor_into(s1, clmul128(eq[i], c1));
   }
-  uint4 v[1] = {reduce256(s1)};
+  uint4 v[1] = {SMALL ? s1r : reduce256(s1)};
   block_xor_reduce<1>(v, out + 4 * k);
 }
 
 // Selector claim k with its own eq_k: out[8k..] += (sum eq_k[i] (s1 (sel1 + 1) + 1),
 // sum eq_k[i] (s0 + s1)(sel0 + sel1)); `sel` (shared by all claims) is folded beforehand, the
 // column s_k is folded here when `fold` is set.  Grid: (chunks, claims).
+template <bool SMALL>
 __global__ void __launch_bounds__(kT)
     selector_round_kernel(const uint4* __restrict__ sel, uint4* __restrict__ cols, uint64_t L,
                           uint64_t stride, const uint4* __restrict__ eqs, uint64_t eq_stride,
@@ -196,12 +215,14 @@ __global__ void __launch_bounds__(kT)
   const uint4* eq = eqs + k * eq_stride;
   const uint64_t h = L >> 1;
   u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
+  uint4 s1r = gf_zero(), sinfr = gf_zero();
+  auto mul = [](uint4 x, uint4 y) { return SMALL ? gf_mul_nl(x, y) : gf_mul(x, y); };
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < h;
        i += (uint64_t)gridDim.x * blockDim.x) {
     uint4 c0, c1;
     if (fold) {
-      c0 = fold1(s[i], s[L + i], r);
-      c1 = fold1(s[h + i], s[L + h + i], r);
+      c0 = gf_add(s[i], mul(r, gf_add(s[L + i], s[i])));
+      c1 = gf_add(s[h + i], mul(r, gf_add(s[L + h + i], s[h + i])));
       s[i] = c0;
       s[h + i] = c1;
     } else {
@@ -209,10 +230,17 @@ __global__ void __launch_bounds__(kT)
       c1 = s[h + i];
     }
     const uint4 e = eq[i], sel0 = sel[i], sel1 = sel[h + i];
-    xor_into(s1, clmul128(e, gf_add(gf_mul(c1, gf_add(sel1, gf_one())), gf_one())));
-    xor_into(sinf, clmul128(e, gf_mul(gf_add(c0, c1), gf_add(sel0, sel1))));
+    const uint4 x1 = gf_add(mul(c1, gf_add(sel1, gf_one())), gf_one());
+    const uint4 xi = mul(gf_add(c0, c1), gf_add(sel0, sel1));
+    if constexpr (SMALL) {
+      gf_add_into(s1r, gf_mul_nl(e, x1));
+      gf_add_into(sinfr, gf_mul_nl(e, xi));
+    } else {
+      xor_into(s1, clmul128(e, x1));
+      xor_into(sinf, clmul128(e, xi));
+    }
   }
-  uint4 v[2] = {reduce256(s1), reduce256(sinf)};
+  uint4 v[2] = {SMALL ? s1r : reduce256(s1), SMALL ? sinfr : reduce256(sinf)};
   block_xor_reduce<2>(v, out + 8 * k);
 }
 
@@ -305,7 +333,7 @@ __global__ void __launch_bounds__(kImFinishThreads)
     const ImClaim c = claims[i];
     const ImAlpha a = alphas[c.group];
     const uint4 y1 = slots[c.y1];
-    const uint4 y0 = gf_mul(gf_add(sums[i], gf_mul(y1, a.alpha)), a.inv_one_plus_alpha);
+    const uint4 y0 = gf_mul_nl(gf_add(sums[i], gf_mul_nl(y1, a.alpha)), a.inv_one_plus_alpha);
     uint4 p0 = y0, p1, p2 = gf_zero();
     if (c.deg == 2) {
       const uint4 yinf = slots[c.yinf];
@@ -319,11 +347,11 @@ __global__ void __launch_bounds__(kImFinishThreads)
     s_prime[i][2] = p2;
     uint4 oma = a.alpha;
     oma.x ^= 1u;
-    const uint4 sc = gf_mul(prefix[c.group], beta_pow[i]);
-    gf_add_into(acc[0], gf_mul(gf_mul(p0, oma), sc));
-    gf_add_into(acc[1], gf_mul(gf_add(gf_mul(p1, oma), p0), sc));
-    gf_add_into(acc[2], gf_mul(gf_add(gf_mul(p2, oma), p1), sc));
-    gf_add_into(acc[3], gf_mul(p2, sc));
+    const uint4 sc = gf_mul_nl(prefix[c.group], beta_pow[i]);
+    gf_add_into(acc[0], gf_mul_nl(gf_mul_nl(p0, oma), sc));
+    gf_add_into(acc[1], gf_mul_nl(gf_add(gf_mul_nl(p1, oma), p0), sc));
+    gf_add_into(acc[2], gf_mul_nl(gf_add(gf_mul_nl(p2, oma), p1), sc));
+    gf_add_into(acc[3], gf_mul_nl(p2, sc));
   }
   block_xor_sum<4>(acc);
   if (threadIdx.x < 32) {
@@ -341,11 +369,11 @@ __global__ void __launch_bounds__(kImFinishThreads)
   __syncthreads();
   const uint4 r = s_r;
   for (uint32_t i = threadIdx.x; i < n_claims; i += blockDim.x)
-    sums[i] = gf_add(s_prime[i][0], gf_mul(r, gf_add(s_prime[i][1], gf_mul(r, s_prime[i][2]))));
+    sums[i] = gf_add(s_prime[i][0], gf_mul_nl(r, gf_add(s_prime[i][1], gf_mul_nl(r, s_prime[i][2]))));
   for (uint32_t g = threadIdx.x; g < n_groups; g += blockDim.x) {
     uint4 f = gf_add(r, alphas[g].alpha);
     f.x ^= 1u;
-    prefix[g] = gf_mul(prefix[g], f);
+    prefix[g] = gf_mul_nl(prefix[g], f);
   }
 }
 
@@ -469,13 +497,19 @@ class IntMulDevice {
   int biv_round(uint4* set, uint32_t pairs, uint64_t L, const uint4* eq, const uint4* r_ptr,
                 uint32_t* out) {
     dim3 grid(blocks_for(L / 2, 148 * 2), pairs);
-    BGPU_CUDA(launch_pdl(biv_round_kernel, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out));
+    if (L <= kSmallRound)
+      BGPU_CUDA(launch_pdl(biv_round_kernel<true>, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out));
+    else
+      BGPU_CUDA(launch_pdl(biv_round_kernel<false>, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out));
     return check("biv_round_kernel");
   }
   int lin_round(uint4* set, uint32_t cols, uint64_t L, const uint4* eq, const uint4* r_ptr,
                 uint32_t* out) {
     dim3 grid(blocks_for(L / 2, 148 * 2), cols);
-    BGPU_CUDA(launch_pdl(lin_round_kernel, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out));
+    if (L <= kSmallRound)
+      BGPU_CUDA(launch_pdl(lin_round_kernel<true>, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out));
+    else
+      BGPU_CUDA(launch_pdl(lin_round_kernel<false>, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out));
     return check("lin_round_kernel");
   }
   // A batched MLE-check whose rounds run on the device transcript: batch_begin uploads the claims,
@@ -795,8 +829,12 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
       if (rp)
         if (int rc = fold(sel, 1, L, rp)) return rc;  // a_root, shared by the 64 claims
       dim3 grid(blocks_for(L / 2, 148 * 2), 64);
-      BGPU_CUDA(launch_pdl(selector_round_kernel, grid, kT, 0, s_, (const uint4*)sel, bcols, L, N,
-                           level(sel_eqs, n_ - t - 1), N, rp, out));
+      if (L <= kSmallRound)
+        BGPU_CUDA(launch_pdl(selector_round_kernel<true>, grid, kT, 0, s_, (const uint4*)sel, bcols,
+                             L, N, level(sel_eqs, n_ - t - 1), N, rp, out));
+      else
+        BGPU_CUDA(launch_pdl(selector_round_kernel<false>, grid, kT, 0, s_, (const uint4*)sel,
+                             bcols, L, N, level(sel_eqs, n_ - t - 1), N, rp, out));
       if (int rc = check("selector_round_kernel")) return rc;
       if (int rc = biv_round(croot, 1, L, level(eq_, n_ - t - 1), rp, out + 4 * 128)) return rc;
       if (int rc = batch_round(b, t)) return rc;
