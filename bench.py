@@ -467,7 +467,7 @@ def run_prove(args, rank, world, local):
                              "std::thread over all host cores); the Rust reference needs cargo"}
         batched = None
         if world == 1 and not args.no_batch:
-            batched, _ = batch_summary(torch, bg, local, 128, 16)
+            batched, _ = batch_summary(torch, bg, local, 256, 16)
         ph = {k: statistics.median(p[k] for p in phases) for k in phases[0]}
         line = {
             "metric": PROVE_METRIC, "value": ms, "unit": "ms", "n_gpus": world,

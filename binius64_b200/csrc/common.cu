@@ -272,10 +272,13 @@ int read_sync(void* dst, const void* src, size_t bytes, cudaStream_t s) {
 namespace {
 thread_local bool t_blocking_wait = false;
 thread_local cudaEvent_t t_wait_event = nullptr;
-constexpr double kPollMicros = 100.0;
+thread_local double t_poll_micros = 100.0;
 }  // namespace
 
-void set_blocking_waits(bool on) { t_blocking_wait = on; }
+void set_blocking_waits(bool on, double poll_micros) {
+  t_blocking_wait = on;
+  t_poll_micros = poll_micros;
+}
 
 cudaError_t stream_wait(cudaStream_t s) {
   if (!t_blocking_wait) return cudaStreamSynchronize(s);
@@ -290,8 +293,8 @@ cudaError_t stream_wait(cudaStream_t s) {
   for (;;) {
     e = cudaEventQuery(t_wait_event);
     if (e != cudaErrorNotReady) return e;
-    if (std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count() >
-        kPollMicros)
+    if (std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count() >=
+        t_poll_micros)
       return cudaEventSynchronize(t_wait_event);
     std::this_thread::yield();
   }

@@ -33,9 +33,10 @@ int cuda_error(cudaError_t e, const char* what);
   } while (0)
 
 // Waits for the work queued on s: cudaStreamSynchronize, or (threads that called
-// set_blocking_waits(true)) an event poll that yields the core, then a blocking-sync wait.
+// set_blocking_waits(true, us)) an event poll that yields the core for up to `us` microseconds,
+// then a blocking-sync wait.
 cudaError_t stream_wait(cudaStream_t s);
-void set_blocking_waits(bool on);
+void set_blocking_waits(bool on, double poll_micros = 100.0);
 
 // Device-to-host reads through a per-thread pinned staging buffer: add() queues copies on the
 // stream, wait() synchronises once and scatters them to their destinations.  Small reads from
