@@ -80,22 +80,27 @@ __device__ __forceinline__ uint64_t transpose8x8(uint64_t x) {
 //
 // A tile of 256 key-sorted terms is staged in shared memory as 32 chunks of 8.  For each chunk the
 // CTA first builds (a) its 64 bit-column bytes, byte j holding bit j of the chunk's 8 words (one
-// 8x8 bit transpose per thread), and (b) two 16-entry tables of XOR combinations of the chunk's
-// eq values (terms 0-3 and 4-7), a method-of-four-Russians split of the 0/1 x GF(2^128) product.
+// 8x8 bit transpose per thread, stored as one 8-byte word), and (b) two 16-entry tables of XOR
+// combinations of the chunk's eq values (terms 0-3 and 4-7; four entries per thread from the two
+// high eq values' sum), a method-of-four-Russians split of the 0/1 x GF(2^128) product.
 // Then each 64-thread group walks its 8 chunks with thread j owning bit position j: a chunk whose
 // 8 terms share one key costs one byte load and two table lookups; a chunk that straddles a key
 // boundary falls back to per-term masked XORs.  A group flushes its accumulators with atomicXor
 // when the key changes.
 constexpr uint32_t kChunk = 8, kChunks = kTile / kChunk;
+// Staged eq values and words sit at e + e / 8 (one pad slot per chunk), so that the four chunks a
+// warp reads at once fall in different shared-memory banks.
+__device__ __forceinline__ uint32_t pad8(uint32_t e) { return e + (e >> 3); }
+
 __global__ void __launch_bounds__(kTile)
     shift_g_kernel(const uint32_t* __restrict__ vi, const uint32_t* __restrict__ cidx,
                    const uint16_t* __restrict__ keys, uint64_t n,
                    const uint64_t* __restrict__ words, const uint4* __restrict__ eq_and,
                    const uint4* __restrict__ eq_mul, uint32_t* __restrict__ g_raw) {
-  __shared__ uint4 s_eq[kTile];
-  __shared__ uint64_t s_w[kTile];
+  __shared__ uint4 s_eq[kTile + kChunks];
+  __shared__ uint64_t s_w[kTile + kChunks];
   __shared__ uint32_t s_key[kTile];
-  __shared__ uint8_t s_col[kChunks][64];
+  __shared__ uint64_t s_col[kChunks][8];  // byte j of chunk c's row: bit j of its 8 words
   __shared__ uint4 s_tab[kChunks][2][16];
   const uint32_t tid = threadIdx.x, j = tid & 63, grp = tid >> 6;
   uint32_t cur = kNoKey;
@@ -134,27 +139,29 @@ __global__ void __launch_bounds__(kTile)
   for (uint64_t tile = tile0; tile < n_tiles; tile++) {
     __syncthreads();
     s_key[tid] = nk;
-    s_eq[tid] = ne;
-    s_w[tid] = nw;
+    s_eq[pad8(tid)] = ne;
+    s_w[pad8(tid)] = nw;
     fetch(tile + 1);
     __syncthreads();
     {  // bit columns: thread (chunk c, byte block b)
       const uint32_t c = tid >> 3, b = tid & 7;
       uint64_t x = 0;
 #pragma unroll
-      for (uint32_t i = 0; i < 8; i++) x |= ((s_w[c * 8 + i] >> (8 * b)) & 0xffull) << (8 * i);
-      x = transpose8x8(x);
-#pragma unroll
-      for (uint32_t k = 0; k < 8; k++) s_col[c][8 * b + k] = (uint8_t)(x >> (8 * k));
+      for (uint32_t i = 0; i < 8; i++) x |= ((s_w[c * 9 + i] >> (8 * b)) & 0xffull) << (8 * i);
+      s_col[c][b] = transpose8x8(x);
     }
-#pragma unroll
-    for (uint32_t q = 0; q < 4; q++) {  // tables: 1024 entries, 4 per thread
-      const uint32_t idx = tid * 4 + q, c = idx >> 5, h = (idx >> 4) & 1, nib = idx & 15;
-      uint4 v = gf_zero();
-#pragma unroll
-      for (uint32_t i = 0; i < 4; i++)
-        if ((nib >> i) & 1) gf_add_into(v, s_eq[c * 8 + 4 * h + i]);
-      s_tab[c][h][nib] = v;
+    {  // nibble tables: thread (chunk c, half h, quarter q) builds entries 4q .. 4q + 3
+      const uint32_t g = tid >> 2, c = g >> 1, h = g & 1, q = tid & 3;
+      const uint4* e = s_eq + c * 9 + 4 * h;
+      const uint4 e0 = e[0], e1 = e[1];
+      uint4 base = gf_zero();
+      if (q & 1) gf_add_into(base, e[2]);
+      if (q & 2) gf_add_into(base, e[3]);
+      uint4* t = s_tab[c][h] + 4 * q;
+      t[0] = base;
+      t[1] = gf_add(base, e0);
+      t[2] = gf_add(base, e1);
+      t[3] = gf_add(gf_add(base, e0), e1);
     }
     __syncthreads();
 #pragma unroll 2
@@ -164,7 +171,7 @@ __global__ void __launch_bounds__(kTile)
       if (k0 == k7) {
         switch_key(k0);
         if (k0 != kNoKey) {
-          const uint32_t byte = s_col[c][j];
+          const uint32_t byte = reinterpret_cast<const uint8_t*>(s_col[c])[j];
           gf_add_into(acc, s_tab[c][0][byte & 15]);
           gf_add_into(acc, s_tab[c][1][byte >> 4]);
         }
@@ -172,8 +179,8 @@ __global__ void __launch_bounds__(kTile)
         for (uint32_t i = 0; i < 8; i++) {
           const uint32_t e = e0 + i;
           switch_key(s_key[e]);
-          const uint32_t m = 0u - (uint32_t)((s_w[e] >> j) & 1);
-          const uint4 x = s_eq[e];
+          const uint32_t m = 0u - (uint32_t)((s_w[c * 9 + i] >> j) & 1);
+          const uint4 x = s_eq[c * 9 + i];
           acc.x ^= x.x & m;
           acc.y ^= x.y & m;
           acc.z ^= x.z & m;
