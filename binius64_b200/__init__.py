@@ -448,7 +448,8 @@ class DeviceConstraintSystem:
     """A constraint system parsed from the reference's v2 wire format and uploaded to the device
     (ConstraintSystem::deserialize + validate_and_prepare)."""
 
-    def __init__(self, cs_bytes: bytes, device: int | None = None):
+    def __init__(self, cs_bytes: bytes, device: int | None = None,
+                 key_collection: bytes | None = None):
         torch = _torch()
         self.device = torch.cuda.current_device() if device is None else int(device)
         self._h = ctypes.c_void_p()
@@ -458,10 +459,22 @@ class DeviceConstraintSystem:
         (self.n_const, self.n_inout, self.n_witness, self.n_internal, self.offset_inout,
          self.offset_witness, self.committed_total_len, self.n_scratch, self.n_and, self.n_mul,
          self.n_and_real, self.n_mul_real) = list(info)
+        if key_collection is not None:
+            self.load_key_collection(key_collection)
 
     @property
     def handle(self):
         return self._h
+
+    def key_collection(self) -> bytes:
+        """build_key_collection(cs) serialized (KeyCollection v1)."""
+        return _sized_bytes(lib().binius_cs_key_collection, self._h)
+
+    def load_key_collection(self, data: bytes) -> None:
+        """Rebuilds the shift reduction's term table from a serialized KeyCollection, as
+        Prover::setup_with_key_collection takes one; a collection that does not describe this
+        constraint system raises ArgumentError and leaves the table as it was."""
+        check(lib().binius_cs_load_key_collection(self._h, data, len(data)))
 
     def eval_operands(self, witness_words, which: int = 0, stream=None):
         torch = _torch()
@@ -479,6 +492,22 @@ class DeviceConstraintSystem:
             except Exception:
                 pass
             self._h = None
+
+
+def _sized_bytes(fn, *args) -> bytes:
+    """Calls a byte-writing entry point once to learn the length, then with a buffer that fits."""
+    n = ctypes.c_size_t(0)
+    if fn(*args, None, 0, ctypes.byref(n)) == 0:
+        return b""
+    buf = ctypes.create_string_buffer(max(n.value, 1))
+    check(fn(*args, buf, len(buf), ctypes.byref(n)))
+    return buf.raw[:n.value]
+
+
+def key_collection_from_cs_bytes(cs_bytes: bytes) -> bytes:
+    """build_key_collection + KeyCollection::serialize (prover/prover/src/protocols/shift/
+    key_collection.rs:238-312, 381-398) for a v2 constraint system, on the host alone."""
+    return _sized_bytes(lib().binius_key_collection_from_cs_bytes, cs_bytes, len(cs_bytes))
 
 
 def and_reduction_prove(cs: DeviceConstraintSystem, witness_words, transcript: ProverTranscript,
@@ -542,10 +571,16 @@ class Prover:
     """Prover::setup + Prover::prove (prover/prover/src/prove.rs:95-303) over a device constraint
     system, with the parameters Verifier::setup chooses (verifier/verifier/src/verify.rs:61-108)."""
 
-    def __init__(self, cs: DeviceConstraintSystem, log_inv_rate: int = 1):
+    def __init__(self, cs: DeviceConstraintSystem, log_inv_rate: int = 1,
+                 key_collection: bytes | None = None):
         self.cs = cs  # the native prover keeps a reference
         self._h = ctypes.c_void_p()
-        check(lib().binius_prover_setup(cs.handle, log_inv_rate, ctypes.byref(self._h)))
+        if key_collection is None:
+            check(lib().binius_prover_setup(cs.handle, log_inv_rate, ctypes.byref(self._h)))
+        else:  # Prover::setup_with_key_collection (prover/prover/src/prove.rs:89-115)
+            check(lib().binius_prover_setup_with_key_collection(
+                cs.handle, log_inv_rate, key_collection, len(key_collection),
+                ctypes.byref(self._h)))
         info = (ctypes.c_uint32 * 12)()
         check(lib().binius_prover_info(self._h, ctypes.addressof(info)))
         v = list(info)

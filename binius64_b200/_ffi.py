@@ -86,6 +86,12 @@ _SIGS = {
     "binius_proof_decode": (_int, [_vp, _c.c_size_t, _vp, _c.c_size_t, _c.POINTER(_c.c_size_t),
                                    _c.c_char_p, _c.c_size_t]),
     "binius_value_vec_from_data": (_int, [_vp, _vp, _c.c_size_t, _vp, _c.c_size_t, _vp]),
+    "binius_key_collection_from_cs_bytes": (_int, [_c.c_char_p, _c.c_size_t, _vp, _c.c_size_t,
+                                                   _c.POINTER(_c.c_size_t)]),
+    "binius_cs_key_collection": (_int, [_vp, _vp, _c.c_size_t, _c.POINTER(_c.c_size_t)]),
+    "binius_cs_load_key_collection": (_int, [_vp, _c.c_char_p, _c.c_size_t]),
+    "binius_prover_setup_with_key_collection": (_int, [_vp, _u32, _c.c_char_p, _c.c_size_t,
+                                                       _vp]),
     "binius_eval_operands": (_int, [_vp, _vp, _int, _vp, _vp]),
     "binius_and_reduction_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "binius_shift_reduction_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -172,20 +172,65 @@ int build_shift_terms(const HostOperands& and_h, const HostOperands& mul_h, Shif
   };
   visit(and_h, and_class, place);
   visit(mul_h, mul_class, place);
-  d.n = n;
-  const size_t m = n ? n : 1;
-  BGPU_CUDA(cudaMalloc(&d.vi, 4 * m));
-  BGPU_CUDA(cudaMalloc(&d.c, 4 * m));
-  BGPU_CUDA(cudaMalloc(&d.key, 2 * m));
-  BGPU_CUDA(cudaMemcpy(d.vi, vi.data(), 4 * m, cudaMemcpyHostToDevice));
-  BGPU_CUDA(cudaMemcpy(d.c, cc.data(), 4 * m, cudaMemcpyHostToDevice));
-  BGPU_CUDA(cudaMemcpy(d.key, key.data(), 2 * m, cudaMemcpyHostToDevice));
-  return BINIUS_OK;
+  return upload_shift_terms(vi, cc, key, n, d);
 }
 
 }  // namespace
 
 namespace bgpu {
+
+int upload_shift_terms(const std::vector<uint32_t>& vi, const std::vector<uint32_t>& c,
+                       const std::vector<uint16_t>& key, uint64_t n, ShiftTerms& out) {
+  const size_t m = n ? n : 1;
+  ShiftTerms d;
+  d.n = n;
+  cudaError_t e;
+  if ((e = cudaMalloc(&d.vi, 4 * m)) != cudaSuccess || (e = cudaMalloc(&d.c, 4 * m)) != cudaSuccess ||
+      (e = cudaMalloc(&d.key, 2 * m)) != cudaSuccess ||
+      (e = cudaMemcpy(d.vi, vi.data(), 4 * m, cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(d.c, c.data(), 4 * m, cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(d.key, key.data(), 2 * m, cudaMemcpyHostToDevice)) != cudaSuccess) {
+    cudaFree(d.vi);
+    cudaFree(d.c);
+    cudaFree(d.key);
+    return cuda_error(e, "shift term table");
+  }
+  cudaFree(out.vi);
+  cudaFree(out.c);
+  cudaFree(out.key);
+  out = d;
+  return BINIUS_OK;
+}
+
+// ConstraintSystem::deserialize + ValueVecLayout::validate + validate_and_prepare's padding, on
+// the host only (no device state).
+int parse_cs(const void* h_bytes, size_t len, binius_cs& cs) {
+  Reader r{static_cast<const uint8_t*>(h_bytes), len};
+  uint32_t version = r.u32();
+  BGPU_ARG(r.ok && version == 2, "ConstraintSystem::version must be 2");
+  uint32_t* fields[8] = {&cs.n_const,      &cs.n_inout,         &cs.n_witness,
+                         &cs.n_internal,   &cs.offset_inout,    &cs.offset_witness,
+                         &cs.committed_total_len, &cs.n_scratch};
+  for (auto f : fields) *f = r.u32();
+  uint32_t n_constants = r.u32();
+  BGPU_ARG(r.ok, "constraint system bytes truncated");
+  // ValueVecLayout::validate (constraint_system.rs:686-703)
+  BGPU_ARG(is_pow2(cs.committed_total_len), "ValueVecLenNotPowerOfTwo");
+  BGPU_ARG(is_pow2(cs.offset_witness), "PublicInputPowerOfTwo");
+  BGPU_ARG(cs.offset_witness >= 2, "PublicInputTooShort");
+  BGPU_ARG(n_constants == cs.n_const && n_constants <= (1u << 24),
+           "ConstraintSystem::constants length != n_const");
+  for (uint32_t i = 0; i < n_constants; i++) cs.constants.push_back(r.u64());
+  uint32_t n_and = r.u32();
+  if (int rc = parse_operands(r, n_and, 3, cs.committed_total_len, cs.h_and)) return rc;
+  uint32_t n_mul = r.u32();
+  if (int rc = parse_operands(r, n_mul, 4, cs.committed_total_len, cs.h_mul)) return rc;
+  cs.n_and_real = n_and;
+  cs.n_mul_real = n_mul;
+  pad_operands(cs.h_and, next_pow2_at_least(n_and, 8));
+  pad_operands(cs.h_mul, next_pow2_at_least(n_mul, 1));
+  return BINIUS_OK;
+}
 
 int eval_operands(const DevOperands& ops, const uint64_t* d_witness, uint64_t* d_out,
                   cudaStream_t s) {
@@ -206,40 +251,11 @@ extern "C" {
 int binius_cs_from_bytes(int device, const void* h_bytes, size_t len, binius_cs** out) {
   BGPU_ARG(out != nullptr && (h_bytes != nullptr || len == 0), "NULL argument");
   *out = nullptr;
-  Reader r{static_cast<const uint8_t*>(h_bytes), len};
-  uint32_t version = r.u32();
-  BGPU_ARG(r.ok && version == 2, "ConstraintSystem::version must be 2");
   if (int rc = configure_device_pool(device)) return rc;
   binius_cs* cs = new binius_cs();
   cs->device = device;
-  uint32_t* fields[8] = {&cs->n_const,      &cs->n_inout,         &cs->n_witness,
-                         &cs->n_internal,   &cs->offset_inout,    &cs->offset_witness,
-                         &cs->committed_total_len, &cs->n_scratch};
-  for (auto f : fields) *f = r.u32();
-  uint32_t n_constants = r.u32();
-  int rc = BINIUS_OK;
-  do {
-    if (!r.ok) { rc = set_error(BINIUS_E_ARG, "constraint system bytes truncated"); break; }
-    // ValueVecLayout::validate (constraint_system.rs:686-703)
-    if (!is_pow2(cs->committed_total_len)) {
-      rc = set_error(BINIUS_E_ARG, "ValueVecLenNotPowerOfTwo");
-      break;
-    }
-    if (!is_pow2(cs->offset_witness)) { rc = set_error(BINIUS_E_ARG, "PublicInputPowerOfTwo"); break; }
-    if (cs->offset_witness < 2) { rc = set_error(BINIUS_E_ARG, "PublicInputTooShort"); break; }
-    if (n_constants != cs->n_const || n_constants > (1u << 24)) {
-      rc = set_error(BINIUS_E_ARG, "ConstraintSystem::constants length != n_const");
-      break;
-    }
-    for (uint32_t i = 0; i < n_constants; i++) cs->constants.push_back(r.u64());
-    uint32_t n_and = r.u32();
-    if ((rc = parse_operands(r, n_and, 3, cs->committed_total_len, cs->h_and))) break;
-    uint32_t n_mul = r.u32();
-    if ((rc = parse_operands(r, n_mul, 4, cs->committed_total_len, cs->h_mul))) break;
-    cs->n_and_real = n_and;
-    cs->n_mul_real = n_mul;
-    pad_operands(cs->h_and, next_pow2_at_least(n_and, 8));
-    pad_operands(cs->h_mul, next_pow2_at_least(n_mul, 1));
+  int rc = parse_cs(h_bytes, len, *cs);
+  if (!rc) {
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(device);
@@ -247,7 +263,7 @@ int binius_cs_from_bytes(int device, const void* h_bytes, size_t len, binius_cs*
     if (!rc) rc = upload(cs->h_mul, cs->mul_ops);
     if (!rc) rc = build_shift_terms(cs->h_and, cs->h_mul, cs->shift_terms);
     cudaSetDevice(prev);
-  } while (0);
+  }
   if (rc) {
     binius_cs_destroy(cs);
     return rc;

@@ -37,6 +37,18 @@ struct ShiftTerms {
 constexpr uint32_t kShiftKeys = 512 * 8;
 constexpr uint32_t kShiftClasses = 7;
 
+}  // namespace bgpu
+struct binius_cs;
+namespace bgpu {
+// Parses and validates a v2 constraint system into cs's host fields and pads its operand lists
+// (no device state).
+int parse_cs(const void* h_bytes, size_t len, binius_cs& cs);
+
+// Uploads a term table (vi, c, key each of n entries, sorted by key) to the current device and
+// replaces `out`'s, freeing the old one; on failure `out` is unchanged.
+int upload_shift_terms(const std::vector<uint32_t>& vi, const std::vector<uint32_t>& c,
+                       const std::vector<uint16_t>& key, uint64_t n, ShiftTerms& out);
+
 // d_out[slot * n_constraints + i] = eval_operand of constraint i's operand `slot`.
 int eval_operands(const DevOperands& ops, const uint64_t* d_witness, uint64_t* d_out,
                   cudaStream_t s);

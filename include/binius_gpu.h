@@ -303,6 +303,29 @@ int binius_value_vec_from_data(const binius_cs* cs, const uint64_t* h_public, si
                                uint64_t* h_out);
 
 /* ------------------------------------------------------------------------------------------
+ * Shift-reduction KeyCollection (setup-time precomputation of the shift reduction's term index).
+ * Replaces: build_key_collection + KeyCollection::serialize (prover/prover/src/protocols/shift/
+ * key_collection.rs:238-312, 381-398, version 1), Prover::key_collection (prover/prover/src/
+ * prove.rs:120-122) and Prover::setup_with_key_collection (:89-115) with
+ * KeyCollection::deserialize (key_collection.rs:400-431).
+ * binius_key_collection_from_cs_bytes builds the collection of a v2 constraint system on the host
+ * alone (no device needed); binius_cs_key_collection builds it for an uploaded one.  Both write
+ * the reference's bytes exactly, at most `cap` of them, and always set *len.
+ * binius_cs_load_key_collection replaces the constraint system's device term table with the
+ * terms a serialized collection describes; it rejects another version ("InvalidConstruction:
+ * KeyCollection::version"), truncated or trailing bytes, and a collection that does not describe
+ * this constraint system's terms, with BINIUS_E_ARG and the table unchanged.  Not while a prove
+ * call on `cs` is in flight.
+ * binius_prover_setup_with_key_collection = binius_cs_load_key_collection + binius_prover_setup.
+ * ------------------------------------------------------------------------------------------ */
+int binius_key_collection_from_cs_bytes(const void* h_cs_bytes, size_t cs_len, void* h_out,
+                                        size_t cap, size_t* len);
+int binius_cs_key_collection(const binius_cs* cs, void* h_out, size_t cap, size_t* len);
+int binius_cs_load_key_collection(binius_cs* cs, const void* h_bytes, size_t len);
+int binius_prover_setup_with_key_collection(binius_cs* cs, uint32_t log_inv_rate,
+                                            const void* h_kc, size_t kc_len, binius_prover** out);
+
+/* ------------------------------------------------------------------------------------------
  * Integer multiplication reduction.
  * Replaces: build_intmul_witness + prove_intmul_reduction (prover/prover/src/prove.rs:374-391,
  * 432-470), intmul Witness (protocols/intmul/witness.rs:47-270) and IntMulProver::prove

@@ -575,3 +575,25 @@ def verify(public_words, log_words: int, log_public: int, and_csr, mul_csr, proo
     pr = np.frombuffer(proof, dtype=np.uint8).copy()
     return L.orc_verify(_p64(pub), log_words, log_public, pa, va, na, pm, vm, nm, log_inv_rate,
                         _p8(pr), len(proof))
+
+
+# ---- shift reduction KeyCollection (prover/prover/src/protocols/shift/key_collection.rs) ----
+
+def key_collection(and_csr, mul_csr, n_words: int) -> bytes:
+    """build_key_collection + serialize (v1) over the padded operand lists of a constraint system
+    with n_words committed words."""
+    L = lib()
+    if not getattr(L, "_kc_ready", False):
+        csr = [_u32pp, _u8p, ctypes.c_uint32]
+        L.orc_key_collection.argtypes = csr + csr + [ctypes.c_uint32, _u8p, ctypes.c_size_t,
+                                                     ctypes.POINTER(ctypes.c_size_t)]
+        L._kc_ready = True
+    ka, pa, va, na = _csr_args(and_csr)
+    km, pm, vm, nm = _csr_args(mul_csr)
+    n_terms = len(and_csr.value_index) + len(mul_csr.value_index)
+    cap = 16 + 8 * n_words + 16 * n_terms
+    out = np.zeros(cap, dtype=np.uint8)
+    n = ctypes.c_size_t(0)
+    rc = L.orc_key_collection(pa, va, na, pm, vm, nm, n_words, _p8(out), cap, ctypes.byref(n))
+    assert rc == 0
+    return out[: n.value].tobytes()
