@@ -59,6 +59,14 @@ def lib():
         L.orc_rs_encode_batch.restype = ctypes.c_int
         L.orc_merkle_commit.argtypes = [_u64p, ctypes.c_uint32, ctypes.c_uint32, _u8p]
         L.orc_merkle_commit.restype = ctypes.c_int
+        L.orc_vision4_permutation.argtypes = [_u64p]
+        L.orc_vision4_digest.argtypes = [_u8p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t),
+                                         ctypes.c_size_t, _u8p]
+        L.orc_vision4_compress.argtypes = [_u8p, _u8p]
+        L.orc_vision4_map.argtypes = [ctypes.c_int, _u64p, _u64p]
+        L.orc_vision4_constants.argtypes = [_u64p, _u64p]
+        L.orc_vision4_merkle_commit.argtypes = [_u64p, ctypes.c_uint32, ctypes.c_uint32, _u8p]
+        L.orc_vision4_merkle_commit.restype = ctypes.c_int
         L.orc_eq_ind_partial_eval.argtypes = [_u64p, ctypes.c_uint32, _u64p]
         L.orc_fri_fold_interleaved.argtypes = [_u64p, ctypes.c_uint32, ctypes.c_uint32, _u64p,
                                                _u64p]
@@ -230,6 +238,66 @@ def merkle_commit(elems_: np.ndarray, log_leaves: int, log_batch: int) -> np.nda
     assert e.shape[0] == 1 << (log_leaves + log_batch)
     nodes = np.zeros(((1 << (log_leaves + 1)) - 1) * 32, dtype=np.uint8)
     lib().orc_merkle_commit(_p64(e), log_leaves, log_batch, _p8(nodes))
+    return nodes.reshape(-1, 32)
+
+
+def _int_elems(vals) -> np.ndarray:
+    out = np.zeros(2 * len(vals), dtype=np.uint64)
+    for i, v in enumerate(vals):
+        out[2 * i] = v & (2**64 - 1)
+        out[2 * i + 1] = v >> 64
+    return out
+
+
+def _elems_int(arr) -> list:
+    a = np.asarray(arr, dtype=np.uint64).reshape(-1, 2)
+    return [int(lo) | (int(hi) << 64) for lo, hi in a]
+
+
+def vision4_permutation(state: list) -> list:
+    """Vision-4 permutation of a 4-element state (ints)."""
+    s = _int_elems(state)
+    lib().orc_vision4_permutation(_p64(s))
+    return _elems_int(s)
+
+
+def vision4_digest(data: bytes, splits=()) -> bytes:
+    """VisionHasherDigest over data, updated in pieces ending at each split offset."""
+    buf = np.frombuffer(bytes(data) or b"\0", dtype=np.uint8).copy()
+    sp = (ctypes.c_size_t * max(1, len(splits)))(*splits)
+    out = np.zeros(32, dtype=np.uint8)
+    lib().orc_vision4_digest(_p8(buf), len(data), sp, len(splits), _p8(out))
+    return out.tobytes()
+
+
+def vision4_compress(left: bytes, right: bytes) -> bytes:
+    buf = np.frombuffer(bytes(left) + bytes(right), dtype=np.uint8).copy()
+    out = np.zeros(32, dtype=np.uint8)
+    lib().orc_vision4_compress(_p8(buf), _p8(out))
+    return out.tobytes()
+
+
+def vision4_map(which: int, x: int) -> int:
+    """0 = L (linear part of B), 1 = L^-1, 2 = B, 3 = B^-1."""
+    a, o = _int_elems([x]), np.zeros(2, dtype=np.uint64)
+    lib().orc_vision4_map(which, _p64(a), _p64(o))
+    return _elems_int(o)[0]
+
+
+def vision4_constants():
+    """(17 x 4 round constants, B_INV_COEFFS[0]) as ints."""
+    rc, b0 = np.zeros(17 * 8, dtype=np.uint64), np.zeros(2, dtype=np.uint64)
+    lib().orc_vision4_constants(_p64(rc), _p64(b0))
+    e = _elems_int(rc)
+    return [e[4 * r:4 * r + 4] for r in range(17)], _elems_int(b0)[0]
+
+
+def vision4_merkle_commit(elems_: np.ndarray, log_leaves: int, log_batch: int) -> np.ndarray:
+    """All tree nodes with Vision-4 leaves and nodes, (2^(log_leaves+1) - 1, 32) uint8."""
+    e = np.ascontiguousarray(elems_, dtype=np.uint64)
+    assert e.shape[0] == 1 << (log_leaves + log_batch)
+    nodes = np.zeros(((1 << (log_leaves + 1)) - 1) * 32, dtype=np.uint8)
+    lib().orc_vision4_merkle_commit(_p64(e), log_leaves, log_batch, _p8(nodes))
     return nodes.reshape(-1, 32)
 
 

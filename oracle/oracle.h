@@ -65,6 +65,20 @@ int orc_rs_encode_batch(const uint64_t* twiddles, uint32_t log_domain, const uin
 int orc_merkle_commit(const uint64_t* elems, uint32_t log_leaves, uint32_t log_batch,
                       uint8_t* nodes_out);
 
+/* ---- Vision-4 hash (verifier/verifier/src/hash/vision_4) ----
+ * state: 4 elements (8 words); digest: incremental updates ending at each of splits[0..n_splits)
+ * then at len; compress: 64 input bytes (left || right) -> 32; map: 0 = L, 1 = L^-1, 2 = B,
+ * 3 = B^-1; constants: the 17 x 4 round constants and B_INV_COEFFS[0]; merkle_commit: as
+ * orc_merkle_commit with Vision-4 leaves (VisionHasherDigest) and nodes (VisionCompression). */
+void orc_vision4_permutation(uint64_t* state);
+void orc_vision4_digest(const uint8_t* data, size_t len, const size_t* splits, size_t n_splits,
+                        uint8_t* out);
+void orc_vision4_compress(const uint8_t* in64, uint8_t* out32);
+void orc_vision4_map(int which, const uint64_t* x, uint64_t* out);
+void orc_vision4_constants(uint64_t* rc, uint64_t* binv0);
+int orc_vision4_merkle_commit(const uint64_t* elems, uint32_t log_leaves, uint32_t log_batch,
+                              uint8_t* nodes_out);
+
 /* ---- FRI folds (prover/prover/src/fri/fold.rs:260-318; verifier/.../fri/fold.rs:20-130) ---- */
 void orc_eq_ind_partial_eval(const uint64_t* point, uint32_t n, uint64_t* out);
 int orc_fri_fold_interleaved(const uint64_t* codeword, uint32_t log_len, uint32_t log_batch,

@@ -51,6 +51,12 @@ void rs_encode(const u128* tw, const u128* msg, uint32_t log_dim, uint32_t log_i
                uint32_t log_batch, u128* out);
 void merkle_commit(const u128* elems, uint32_t log_leaves, uint32_t log_batch, uint8_t* nodes);
 void eq_ind_partial_eval(const u128* point, uint32_t n, u128* out);
+// Vision-4 (vision4.cpp)
+void vision4_permutation(u128 s[4]);
+void vision4_digest(const uint8_t* data, size_t len, uint8_t out[32]);
+void vision4_compress(const uint8_t left[32], const uint8_t right[32], uint8_t out[32]);
+void merkle_commit_vision4(const u128* elems, uint32_t log_leaves, uint32_t log_batch,
+                           uint8_t* nodes);
 void fold_interleaved(const u128* cw, uint32_t log_len, uint32_t log_batch, const u128* ch,
                       u128* out);
 u128 fold_chunk(const u128* tw, uint32_t log_len, size_t chunk_index, u128* vals, const u128* r,
