@@ -187,7 +187,15 @@ class MerkleCommitted:
 
 
 class BinaryMerkleTreeProver:
-    """SHA-256 leaves + Binius SHA-256 compression nodes (StdDigest / StdCompression)."""
+    """SHA-256 leaves + Binius SHA-256 compression nodes (StdDigest / StdCompression), or with
+    hash="vision4" VisionHasherDigest leaves + VisionCompression nodes (the `-c vision4` setup)."""
+
+    HASHES = ("sha256", "vision4")
+
+    def __init__(self, hash: str = "sha256"):
+        if hash not in self.HASHES:
+            raise ArgumentError(1, f"unknown Merkle hash {hash!r}")
+        self.hash = hash
 
     def commit(self, elements, batch_size: int, stream=None):
         n = _elems_of(elements)
@@ -197,10 +205,21 @@ class BinaryMerkleTreeProver:
         log_len = _log2_exact(n // batch_size, "leaf count")
         torch = _torch()
         nodes = torch.empty(((2 << log_len) - 1, 32), dtype=torch.uint8, device=elements.device)
-        check(lib().binius_merkle_commit(_ptr(elements), log_len, log_batch, _ptr(nodes),
-                                         _stream(stream)))
+        fn = lib().binius_merkle_commit if self.hash == "sha256" else \
+            lib().binius_merkle_commit_vision4
+        check(fn(_ptr(elements), log_len, log_batch, _ptr(nodes), _stream(stream)))
         committed = MerkleCommitted(log_len, nodes)
         return committed.root(), committed
+
+
+def vision4_permute(states, stream=None):
+    """The Vision-4 permutation of each 4-element state, in place: states is a device tensor of
+    n * 4 field elements (n * 64 bytes)."""
+    n = _elems_of(states)
+    if n % 4:
+        raise ArgumentError(1, "states: a multiple of 4 elements")
+    check(lib().binius_vision4_permute(_ptr(states), n // 4, _stream(stream)))
+    return states
 
 
 def n_test_queries(security_bits: int, log_inv_rate: int) -> int:
@@ -402,10 +421,20 @@ class PcsCommitted:
             self.handle = None
 
 
-class OneBitPCSProver:
-    """OneBitPCSProver (prover/prover/src/pcs.rs:30-169) with SHA-256 Merkle trees."""
+MERKLE_HASHES = {"sha256": 0, "vision4": 1}  # BINIUS_MERKLE_SHA256 / BINIUS_MERKLE_VISION4
 
-    def __init__(self, ntt: AdditiveNTT, fri_params: FRIParams):
+
+def _merkle_hash_id(name: str) -> int:
+    if name not in MERKLE_HASHES:
+        raise ArgumentError(1, f"unknown Merkle hash {name!r}")
+    return MERKLE_HASHES[name]
+
+
+class OneBitPCSProver:
+    """OneBitPCSProver (prover/prover/src/pcs.rs:30-169) with SHA-256 Merkle trees, or Vision-4
+    ones with merkle_hash="vision4"."""
+
+    def __init__(self, ntt: AdditiveNTT, fri_params: FRIParams, merkle_hash: str = "sha256"):
         self.ntt = ntt
         self.fri_params = fri_params
         self._h = ctypes.c_void_p()
@@ -414,6 +443,7 @@ class OneBitPCSProver:
                                       fri_params.log_batch_size, fri_params.rs_code.log_inv_rate,
                                       ar, len(fri_params.fold_arities), fri_params.n_test_queries,
                                       ctypes.byref(self._h)))
+        check(lib().binius_pcs_set_merkle_hash(self._h, _merkle_hash_id(merkle_hash)))
 
     def commit(self, packed_multilin, stream=None) -> PcsCommitted:
         if _elems_of(packed_multilin) != 1 << self.fri_params.log_msg_len():
@@ -572,15 +602,19 @@ class Prover:
     system, with the parameters Verifier::setup chooses (verifier/verifier/src/verify.rs:61-108)."""
 
     def __init__(self, cs: DeviceConstraintSystem, log_inv_rate: int = 1,
-                 key_collection: bytes | None = None):
+                 key_collection: bytes | None = None, merkle_hash: str = "sha256"):
         self.cs = cs  # the native prover keeps a reference
         self._h = ctypes.c_void_p()
+        hash_id = _merkle_hash_id(merkle_hash)
         if key_collection is None:
             check(lib().binius_prover_setup(cs.handle, log_inv_rate, ctypes.byref(self._h)))
         else:  # Prover::setup_with_key_collection (prover/prover/src/prove.rs:89-115)
             check(lib().binius_prover_setup_with_key_collection(
                 cs.handle, log_inv_rate, key_collection, len(key_collection),
                 ctypes.byref(self._h)))
+        # setup_sha256 / setup_vision4 (prover/examples/src/lib.rs:48-85)
+        self.merkle_hash = merkle_hash
+        check(lib().binius_prover_set_merkle_hash(self._h, hash_id))
         info = (ctypes.c_uint32 * 12)()
         check(lib().binius_prover_info(self._h, ctypes.addressof(info)))
         v = list(info)

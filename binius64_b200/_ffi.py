@@ -92,6 +92,10 @@ _SIGS = {
     "binius_cs_load_key_collection": (_int, [_vp, _c.c_char_p, _c.c_size_t]),
     "binius_prover_setup_with_key_collection": (_int, [_vp, _u32, _c.c_char_p, _c.c_size_t,
                                                        _vp]),
+    "binius_vision4_permute": (_int, [_vp, _u64, _vp]),
+    "binius_merkle_commit_vision4": (_int, [_vp, _u32, _u32, _vp, _vp]),
+    "binius_pcs_set_merkle_hash": (_int, [_vp, _u32]),
+    "binius_prover_set_merkle_hash": (_int, [_vp, _u32]),
     "binius_eval_operands": (_int, [_vp, _vp, _int, _vp, _vp]),
     "binius_and_reduction_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "binius_shift_reduction_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -280,6 +280,25 @@ int fri_fold_codeword_dev(const binius_ntt* ntt, const void* d_codeword, uint32_
 
 }  // namespace bgpu
 
+namespace bgpu {
+
+int fri_commit_interleaved(const binius_ntt* ntt, const void* d_msg, uint32_t log_dim,
+                           uint32_t log_inv_rate, uint32_t log_batch, uint32_t merkle_hash,
+                           void* d_codeword, void* d_nodes, void* h_root, cudaStream_t s) {
+  if (int rc = rs_encode_batch(ntt, d_msg, log_dim, log_inv_rate, log_batch, d_codeword, s))
+    return rc;
+  const uint32_t log_leaves = log_dim + log_inv_rate;
+  if (int rc = merkle_commit_with(merkle_hash, d_codeword, log_leaves, log_batch, d_nodes, s))
+    return rc;
+  if (h_root) {
+    const uint8_t* root = static_cast<const uint8_t*>(d_nodes) + 32 * ((2ull << log_leaves) - 2);
+    if (int rc = read_sync(h_root, root, 32, s)) return rc;
+  }
+  return BINIUS_OK;
+}
+
+}  // namespace bgpu
+
 extern "C" {
 
 int binius_fri_fold_interleaved(const void* d_codeword, uint32_t log_len, uint32_t log_batch,
@@ -374,15 +393,10 @@ int binius_fri_fold_codeword_noalloc(const binius_ntt* ntt, const void* d_codewo
 int binius_fri_commit_interleaved(const binius_ntt* ntt, const void* d_msg, uint32_t log_dim,
                                   uint32_t log_inv_rate, uint32_t log_batch, void* d_codeword,
                                   void* d_nodes, void* h_root, void* stream) {
-  cudaStream_t s = as_stream(stream);
-  if (int rc = bgpu::rs_encode_batch(ntt, d_msg, log_dim, log_inv_rate, log_batch, d_codeword, s))
+  if (int rc = bgpu::fri_commit_interleaved(ntt, d_msg, log_dim, log_inv_rate, log_batch,
+                                            bgpu::kMerkleSha256, d_codeword, d_nodes, h_root,
+                                            as_stream(stream)))
     return rc;
-  const uint32_t log_leaves = log_dim + log_inv_rate;
-  if (int rc = bgpu::merkle_commit(d_codeword, log_leaves, log_batch, d_nodes, s)) return rc;
-  if (h_root) {
-    const uint8_t* root = static_cast<const uint8_t*>(d_nodes) + 32 * ((2ull << log_leaves) - 2);
-    if (int rc = bgpu::read_sync(h_root, root, 32, s)) return rc;
-  }
   return clear_error();
 }
 

@@ -87,5 +87,18 @@ int rs_encode_batch(const binius_ntt* ntt, const void* d_msg, uint32_t log_dim,
                     cudaStream_t stream);
 int merkle_commit(const void* d_elems, uint32_t log_leaves, uint32_t log_batch, void* d_nodes,
                   cudaStream_t stream);
+int vision4_merkle_commit(const void* d_elems, uint32_t log_leaves, uint32_t log_batch,
+                          void* d_nodes, cudaStream_t stream);
+// The Merkle hash of a commitment scheme: SHA-256 (StdDigest + StdCompression) or Vision-4.
+enum MerkleHash : uint32_t { kMerkleSha256 = 0, kMerkleVision4 = 1 };
+inline int merkle_commit_with(uint32_t hash, const void* d_elems, uint32_t log_leaves,
+                              uint32_t log_batch, void* d_nodes, cudaStream_t stream) {
+  return hash == kMerkleVision4
+             ? vision4_merkle_commit(d_elems, log_leaves, log_batch, d_nodes, stream)
+             : merkle_commit(d_elems, log_leaves, log_batch, d_nodes, stream);
+}
+int fri_commit_interleaved(const binius_ntt* ntt, const void* d_msg, uint32_t log_dim,
+                           uint32_t log_inv_rate, uint32_t log_batch, uint32_t merkle_hash,
+                           void* d_codeword, void* d_nodes, void* h_root, cudaStream_t s);
 
 }  // namespace bgpu

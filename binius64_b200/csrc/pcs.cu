@@ -22,6 +22,7 @@ using namespace bgpu;
 struct binius_pcs {
   const binius_ntt* ntt;
   uint32_t log_msg, log_batch, log_inv_rate, n_queries;
+  uint32_t merkle_hash = bgpu::kMerkleSha256;
   std::vector<uint32_t> arities;
   uint32_t log_dim() const { return log_msg - log_batch; }
   uint32_t rs_log_len() const { return log_dim() + log_inv_rate; }
@@ -127,7 +128,8 @@ struct DevFri {
     BGPU_CUDA(dev_alloc(&nodes, 32ull * ((2ull << log_leaves) - 1), s));
     trees.push_back(nodes);
     tree_log_leaves.push_back(log_leaves);
-    if (int rc = merkle_commit(out, log_leaves, log_coset, nodes, s)) return rc;
+    if (int rc = merkle_commit_with(P.merkle_hash, out, log_leaves, log_coset, nodes, s))
+      return rc;
     *d_root = nodes + 32 * ((2ull << log_leaves) - 2);
     next_commit = has_next ? next_commit + next_arity : -1;
     *committed = true;
@@ -385,6 +387,13 @@ int binius_pcs_create(const binius_ntt* ntt, uint32_t log_msg, uint32_t log_batc
   return clear_error();
 }
 
+int binius_pcs_set_merkle_hash(binius_pcs* pcs, uint32_t merkle_hash) {
+  BGPU_ARG(pcs != nullptr, "NULL argument");
+  BGPU_ARG(merkle_hash <= bgpu::kMerkleVision4, "unknown Merkle hash");
+  pcs->merkle_hash = merkle_hash;
+  return clear_error();
+}
+
 int binius_pcs_destroy(binius_pcs* pcs) {
   delete pcs;
   return BINIUS_OK;
@@ -409,9 +418,9 @@ int binius_pcs_commit(const binius_pcs* P, const void* d_witness, binius_pcs_com
     if (e != cudaSuccess) { rc = cuda_error(e, "dev_alloc(codeword)"); break; }
     e = dev_alloc(&c->d_nodes, 32ull * ((2ull << c->log_leaves) - 1), s);
     if (e != cudaSuccess) { rc = cuda_error(e, "dev_alloc(tree)"); break; }
-    if ((rc = binius_fri_commit_interleaved(P->ntt, d_witness, P->log_dim(), P->log_inv_rate,
-                                            P->log_batch, c->d_codeword, c->d_nodes, c->root,
-                                            stream)))
+    if ((rc = fri_commit_interleaved(P->ntt, d_witness, P->log_dim(), P->log_inv_rate,
+                                     P->log_batch, P->merkle_hash, c->d_codeword, c->d_nodes,
+                                     c->root, s)))
       break;
   } while (0);
   if (rc) {

@@ -95,6 +95,11 @@ int binius_prover_setup(const binius_cs* cs, uint32_t log_inv_rate, binius_prove
   return clear_error();
 }
 
+int binius_prover_set_merkle_hash(binius_prover* P, uint32_t merkle_hash) {
+  BGPU_ARG(P != nullptr, "NULL argument");
+  return binius_pcs_set_merkle_hash(P->pcs, merkle_hash);
+}
+
 int binius_prover_destroy(binius_prover* P) {
   if (!P) return BINIUS_OK;
   binius_pcs_destroy(P->pcs);

@@ -94,6 +94,21 @@ int binius_merkle_branch(const void* d_nodes, uint32_t log_leaves, uint64_t inde
                          uint32_t layer_depth, void* h_branch, void* stream);
 
 /* ------------------------------------------------------------------------------------------
+ * Vision-4 hash (the `-c vision4` Merkle hash, prover/examples/src/lib.rs:67-85).
+ * binius_vision4_permute replaces the Vision-4 permutation over a batch of states
+ * (verifier/verifier/src/hash/vision_4/permutation.rs:104-123; the prover's batch_permutation,
+ * prover/prover/src/hash/vision_4/permutation.rs): d_states holds n states of 4 elements, permuted
+ * in place.
+ * binius_merkle_commit_vision4 is binius_merkle_commit with VisionHasherDigest leaves
+ * (verifier/verifier/src/hash/vision_4/digest.rs:37-136; prover/prover/src/hash/vision_4/
+ * digest.rs) and VisionCompression nodes (compression.rs:24-52; VisionParallelCompression,
+ * prover/prover/src/hash/vision_4/compression.rs:34-145); same layout and arguments.
+ * ------------------------------------------------------------------------------------------ */
+int binius_vision4_permute(void* d_states, uint64_t n, void* stream);
+int binius_merkle_commit_vision4(const void* d_elems, uint32_t log_leaves, uint32_t log_batch,
+                                 void* d_nodes, void* stream);
+
+/* ------------------------------------------------------------------------------------------
  * FRI folding.
  * binius_fri_fold_interleaved replaces fold_interleaved (prover/prover/src/fri/fold.rs:260-282):
  *   d_out[i] = <d_codeword[i*2^log_batch ..], eq_ind(h_challenges)>, 2^log_len outputs,
@@ -173,6 +188,13 @@ int binius_pcs_create(const binius_ntt* ntt, uint32_t log_msg, uint32_t log_batc
                       uint32_t log_inv_rate, const uint32_t* arities, uint32_t n_arities,
                       uint32_t n_queries, binius_pcs** out);
 int binius_pcs_destroy(binius_pcs* pcs);
+/* The Merkle hash of every commitment the PCS makes (the codeword and each FRI fold round):
+ * BINIUS_MERKLE_SHA256 (StdDigest + StdCompression, the default) or BINIUS_MERKLE_VISION4
+ * (VisionHasherDigest + VisionCompression, as Prover<_, VisionParallelCompression,
+ * VisionHasherDigest> of prover/examples/src/lib.rs:43-46). */
+#define BINIUS_MERKLE_SHA256 0u
+#define BINIUS_MERKLE_VISION4 1u
+int binius_pcs_set_merkle_hash(binius_pcs* pcs, uint32_t merkle_hash);
 /* RS encode + Merkle commit of d_witness (2^log_msg elements); the codeword and tree stay on the
  * device in *out; h_root receives the 32-byte commitment.  Synchronous.  The buffers come from
  * the device's stream-ordered pool on `stream` and are released on it by
@@ -239,6 +261,9 @@ typedef struct binius_prover binius_prover;
 
 int binius_prover_setup(const binius_cs* cs, uint32_t log_inv_rate, binius_prover** out);
 int binius_prover_destroy(binius_prover* prover);
+/* setup_vision4 (prover/examples/src/lib.rs:67-85) = binius_prover_setup +
+ * binius_prover_set_merkle_hash(prover, BINIUS_MERKLE_VISION4); not while a prove is in flight. */
+int binius_prover_set_merkle_hash(binius_prover* prover, uint32_t merkle_hash);
 int binius_prover_info(const binius_prover* prover, uint32_t* h_out12);
 int binius_prover_prove(const binius_prover* prover, const void* d_witness,
                         binius_transcript* transcript, void* stream);

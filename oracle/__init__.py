@@ -59,6 +59,7 @@ def lib():
         L.orc_rs_encode_batch.restype = ctypes.c_int
         L.orc_merkle_commit.argtypes = [_u64p, ctypes.c_uint32, ctypes.c_uint32, _u8p]
         L.orc_merkle_commit.restype = ctypes.c_int
+        L.orc_set_merkle_hash.argtypes = [ctypes.c_int]
         L.orc_vision4_permutation.argtypes = [_u64p]
         L.orc_vision4_digest.argtypes = [_u8p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t),
                                          ctypes.c_size_t, _u8p]
@@ -252,6 +253,24 @@ def _int_elems(vals) -> np.ndarray:
 def _elems_int(arr) -> list:
     a = np.asarray(arr, dtype=np.uint64).reshape(-1, 2)
     return [int(lo) | (int(hi) << 64) for lo, hi in a]
+
+
+class merkle_hash:
+    """Context manager selecting the oracle's Merkle hash ("sha256" or "vision4") for
+    merkle_commit, the PCS and prove / verify inside the block."""
+
+    KINDS = {"sha256": 0, "vision4": 1}
+
+    def __init__(self, name: str):
+        self.kind = self.KINDS[name]
+
+    def __enter__(self):
+        lib().orc_set_merkle_hash(self.kind)
+        return self
+
+    def __exit__(self, *exc):
+        lib().orc_set_merkle_hash(0)
+        return False
 
 
 def vision4_permutation(state: list) -> list:

@@ -114,7 +114,7 @@ void merkle_commit(const u128* elems, uint32_t log_leaves, uint32_t log_batch, u
   size_t batch = (size_t)1 << log_batch;
   parallel_for(n_leaves, [&](size_t lo, size_t hi) {
     for (size_t i = lo; i < hi; i++)
-      sha256((const uint8_t*)(elems + i * batch), batch * 16, nodes + 32 * i);
+      merkle_leaf_hash((const uint8_t*)(elems + i * batch), batch * 16, nodes + 32 * i);
   });
   size_t prev = 0, len = n_leaves;
   while (len > 1) {
@@ -122,8 +122,8 @@ void merkle_commit(const u128* elems, uint32_t log_leaves, uint32_t log_batch, u
     size_t half = len / 2;
     parallel_for(half, [&](size_t lo, size_t hi) {
       for (size_t i = lo; i < hi; i++)
-        compress_node(nodes + 32 * (prev + 2 * i), nodes + 32 * (prev + 2 * i + 1),
-                      nodes + 32 * (next + i));
+        merkle_node_hash(nodes + 32 * (prev + 2 * i), nodes + 32 * (prev + 2 * i + 1),
+                         nodes + 32 * (next + i));
     });
     prev = next;
     len = half;

@@ -71,6 +71,9 @@ int orc_merkle_commit(const uint64_t* elems, uint32_t log_leaves, uint32_t log_b
  * 3 = B^-1; constants: the 17 x 4 round constants and B_INV_COEFFS[0]; merkle_commit: as
  * orc_merkle_commit with Vision-4 leaves (VisionHasherDigest) and nodes (VisionCompression). */
 void orc_vision4_permutation(uint64_t* state);
+/* Selects the Merkle hash of orc_merkle_commit, the PCS and the whole prove / verify:
+ * 0 = SHA-256 (StdDigest + StdCompression, the default), 1 = Vision-4. */
+void orc_set_merkle_hash(int kind);
 void orc_vision4_digest(const uint8_t* data, size_t len, const size_t* splits, size_t n_splits,
                         uint8_t* out);
 void orc_vision4_compress(const uint8_t* in64, uint8_t* out32);

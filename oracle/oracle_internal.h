@@ -51,6 +51,12 @@ void rs_encode(const u128* tw, const u128* msg, uint32_t log_dim, uint32_t log_i
                uint32_t log_batch, u128* out);
 void merkle_commit(const u128* elems, uint32_t log_leaves, uint32_t log_batch, uint8_t* nodes);
 void eq_ind_partial_eval(const u128* point, uint32_t n, u128* out);
+// The Merkle hash of the tree code (merkle_commit, the PCS openings and their verification):
+// 0 = SHA-256 leaves + the Binius SHA-256 compression, 1 = Vision-4 leaves and compression.
+// Process-wide, set by orc_set_merkle_hash (the oracle serves one test at a time).
+extern int g_merkle_hash;
+void merkle_leaf_hash(const uint8_t* data, size_t len, uint8_t out[32]);
+void merkle_node_hash(const uint8_t left[32], const uint8_t right[32], uint8_t out[32]);
 // Vision-4 (vision4.cpp)
 void vision4_permutation(u128 s[4]);
 void vision4_digest(const uint8_t* data, size_t len, uint8_t out[32]);

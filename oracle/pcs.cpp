@@ -203,7 +203,7 @@ enum VerifyError {
 };
 
 static void leaf_digest(const u128* vals, size_t n, uint8_t out[32]) {
-  sha256((const uint8_t*)vals, 16 * n, out);
+  merkle_leaf_hash((const uint8_t*)vals, 16 * n, out);
 }
 
 static void fold_digests(std::vector<uint8_t> d, uint8_t root[32]) {
@@ -211,7 +211,7 @@ static void fold_digests(std::vector<uint8_t> d, uint8_t root[32]) {
   while (len > 1) {
     for (size_t i = 0; i < len / 2; i++) {
       uint8_t o[32];
-      compress_node(&d[64 * i], &d[64 * i + 32], o);
+      merkle_node_hash(&d[64 * i], &d[64 * i + 32], o);
       memcpy(&d[32 * i], o, 32);
     }
     len /= 2;
@@ -228,9 +228,9 @@ static bool verify_opening(Transcript& t, size_t index, const u128* vals, size_t
     uint8_t sib[32], o[32];
     if (!t.read_decommit(sib, 32)) return false;
     if ((index & 1) == 0)
-      compress_node(d, sib, o);
+      merkle_node_hash(d, sib, o);
     else
-      compress_node(sib, d, o);
+      merkle_node_hash(sib, d, o);
     memcpy(d, o, 32);
     index >>= 1;
   }

@@ -243,11 +243,29 @@ void merkle_commit_vision4(const u128* elems, uint32_t log_leaves, uint32_t log_
   }
 }
 
+int g_merkle_hash = 0;
+
+void merkle_leaf_hash(const uint8_t* data, size_t len, uint8_t out[32]) {
+  if (g_merkle_hash == 1)
+    vision4_digest(data, len, out);
+  else
+    sha256(data, len, out);
+}
+
+void merkle_node_hash(const uint8_t left[32], const uint8_t right[32], uint8_t out[32]) {
+  if (g_merkle_hash == 1)
+    vision4_compress(left, right, out);
+  else
+    compress_node(left, right, out);
+}
+
 }  // namespace orc
 
 using namespace orc;
 
 extern "C" {
+
+void orc_set_merkle_hash(int kind) { g_merkle_hash = kind; }
 
 void orc_vision4_permutation(uint64_t* state) {
   u128 s[4];
