@@ -44,6 +44,7 @@ LOG_INV_RATE = 1
 
 # prove workload
 LOG_WORDS = 20
+MERKLE_HASH = "sha256"  # or "vision4": the `-c vision4` setup, every commitment a Vision-4 tree
 
 # commit workload
 LOG_LEN = 20          # per-column codeword length 2^20
@@ -68,6 +69,7 @@ def prove_config(log_words):
         "log_inv_rate": LOG_INV_RATE, "security_bits": 96,
         "stand_in_for": "sha512 example circuit, 64 KiB message (2^20 words, 2^20 ANDs, 1 MUL)",
         "l2": "256 MiB buffer written between timed proofs (L2 flush)",
+        "merkle_hash": MERKLE_HASH,
         "seed": SEED,
     }
 
@@ -98,10 +100,14 @@ def parse_args():
                     help="prove workload: skip the batched-queue summary (profiling runs)")
     ap.add_argument("--log-words", type=int, default=None,
                     help="prove workload: log2 committed words (default 20)")
+    ap.add_argument("--merkle-hash", default="sha256", choices=["sha256", "vision4"],
+                    help="prove workload: Merkle hash of the commitments (default sha256; "
+                         "vision4 skips the batched summary)")
     ap.add_argument("--log-len", type=int, default=None,
                     help="commit workload: per-column codeword log length (default 20)")
     args = ap.parse_args()
-    global LOG_WORDS, LOG_LEN
+    global LOG_WORDS, LOG_LEN, MERKLE_HASH
+    MERKLE_HASH = args.merkle_hash
     if args.log_words is not None:
         assert 8 <= args.log_words <= 22
         LOG_WORDS = args.log_words
@@ -212,10 +218,11 @@ def cpu_prove_ms(circ, threads, reps=1):
     prep = circ.cs.prepared()
     orc.set_threads(threads)
     times = []
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        orc.prove(circ.witness, 1, prep.and_csr, prep.mul_csr, LOG_INV_RATE)
-        times.append(time.perf_counter() - t0)
+    with orc.merkle_hash(MERKLE_HASH):
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            orc.prove(circ.witness, 1, prep.and_csr, prep.mul_csr, LOG_INV_RATE)
+            times.append(time.perf_counter() - t0)
     orc.set_threads(1)
     return 1000.0 * statistics.mean(times)
 
@@ -397,7 +404,7 @@ def run_prove(args, rank, world, local):
     stream = torch.cuda.current_stream()
     circ = make_circuit(LOG_WORDS)
     dcs = bg.DeviceConstraintSystem(circ.cs.serialize(), device=local)
-    prover = bg.Prover(dcs, LOG_INV_RATE)
+    prover = bg.Prover(dcs, LOG_INV_RATE, merkle_hash=MERKLE_HASH)
     w = torch.from_numpy(circ.witness.view(np.int64)).to(f"cuda:{local}")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
@@ -466,7 +473,7 @@ def run_prove(args, rank, world, local):
                              "oracle (C++ restatement of the reference prover, PCLMULQDQ, "
                              "std::thread over all host cores); the Rust reference needs cargo"}
         batched = None
-        if world == 1 and not args.no_batch:
+        if world == 1 and not args.no_batch and MERKLE_HASH == "sha256":
             batched, _ = batch_summary(torch, bg, local, 256, 16)
         ph = {k: statistics.median(p[k] for p in phases) for k in phases[0]}
         line = {

@@ -321,12 +321,14 @@ __host__ __device__ __forceinline__ uint64_t layer_offset(uint32_t L, uint32_t k
   return (1ull << (L + 1)) - (1ull << (L + 1 - k));
 }
 
-constexpr uint32_t kV4Threads = 128;
-constexpr uint32_t kV4LeafFuse = 7;  // 2^7 leaves per CTA
-constexpr uint32_t kV4NodeFuse = 8;  // 2^8 inputs per CTA
+// 256 threads: two CTAs (2 x 66 KB of shared memory, 2 x 256 x <= 128 registers) and 16 warps per
+// SM; the permutation is a long dependent chain, so resident warps are what hides its latency.
+constexpr uint32_t kV4Threads = 256;
+constexpr uint32_t kV4LeafFuse = 8;  // 2^8 leaves per CTA
+constexpr uint32_t kV4NodeFuse = 9;  // 2^9 inputs per CTA
 constexpr size_t kV4Smem = kImageBytes + 2 * kV4Threads * 2 * 16;  // image + [2][threads][2] uint4
 
-__global__ void __launch_bounds__(kV4Threads) vision4_permute_kernel(const uint4* __restrict__ img,
+__global__ void __launch_bounds__(kV4Threads, 2) vision4_permute_kernel(const uint4* __restrict__ img,
                                                                      uint4* __restrict__ states,
                                                                      uint64_t n) {
   v4_load_image(img);
@@ -344,7 +346,7 @@ __device__ __forceinline__ uint4* v4_nodes_buf() { return v4_img + kImageBytes /
 
 // Hashes 2^fused leaves per CTA (VisionHasherDigest over each leaf's 2^log_batch elements) and
 // compresses `fused` layers above them in shared memory.
-__global__ void __launch_bounds__(kV4Threads)
+__global__ void __launch_bounds__(kV4Threads, 2)
     vision4_leaves_kernel(const uint4* __restrict__ img, const uint4* __restrict__ elems,
                           uint32_t log_batch, uint4* __restrict__ nodes, uint32_t L,
                           uint32_t fused) {
@@ -393,7 +395,7 @@ __global__ void __launch_bounds__(kV4Threads)
 }
 
 // Compresses `fused` layers starting at layer in_level; each CTA reduces 2^fused inputs.
-__global__ void __launch_bounds__(kV4Threads)
+__global__ void __launch_bounds__(kV4Threads, 2)
     vision4_nodes_kernel(const uint4* __restrict__ img, uint4* __restrict__ nodes, uint32_t L,
                          uint32_t in_level, uint32_t fused) {
   v4_load_image(img);
