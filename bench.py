@@ -227,6 +227,31 @@ def cpu_prove_ms(circ, threads, reps=1):
     return 1000.0 * statistics.mean(times)
 
 
+def vision4_kernels(torch, bg, device, stream):
+    """Kernel-level Vision-4 figures (CUDA events around one call after a warm-up call): the
+    permutation of 2^20 states, and the commit of the 2^20-word prove's codeword tree (2^16
+    leaves of 16 elements)."""
+    gen = torch.Generator(device=f"cuda:{device}").manual_seed(SEED)
+    states = torch.randint(-2**63, 2**63 - 1, (4 << 20, 2), dtype=torch.int64,
+                           device=f"cuda:{device}", generator=gen)
+    elems = torch.randint(-2**63, 2**63 - 1, (1 << 20, 2), dtype=torch.int64,
+                          device=f"cuda:{device}", generator=gen)
+    mp = bg.BinaryMerkleTreeProver("vision4")
+    out = {}
+    for name, fn in (("permute_2^20_states_ms", lambda: bg.vision4_permute(states)),
+                     ("commit_2^16_leaves_x16_ms", lambda: mp.commit(elems, 16))):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[name] = e0.elapsed_time(e1)
+    out["permutations_per_s"] = (1 << 20) / (out["permute_2^20_states_ms"] * 1e-3)
+    return out
+
+
 def bivariate_roofline(torch, bg, lib, device, stream, reps=20):
     """Live timing of binius_sumcheck_bivariate_fold_execute on 2^20-element operands (the first
     folded round of shift phase 2): algorithmic bytes = read a, b (2 x 16 MiB) + write the folded
@@ -472,6 +497,7 @@ def run_prove(args, rank, world, local):
                    "sample": f"2 whole proofs of the same 2^{LOG_WORDS}-word circuit on the "
                              "oracle (C++ restatement of the reference prover, PCLMULQDQ, "
                              "std::thread over all host cores); the Rust reference needs cargo"}
+        kernels = vision4_kernels(torch, bg, local, stream) if MERKLE_HASH == "vision4" else None
         batched = None
         if world == 1 and not args.no_batch and MERKLE_HASH == "sha256":
             batched, _ = batch_summary(torch, bg, local, 256, 16)
@@ -487,6 +513,7 @@ def run_prove(args, rank, world, local):
                            "max": max(per), "wall_per_proof": 1000.0 * wall / args.steps},
             "phase_ms_host": ph,
             "batched": batched,
+            "vision4_kernels": kernels,
             "proof_bytes": proof_len,
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(host_w.numel() * 8),
                     "d2h_bytes_per_step": proof_len},
