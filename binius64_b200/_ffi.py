@@ -93,6 +93,11 @@ _SIGS = {
     "binius_prover_setup_with_key_collection": (_int, [_vp, _u32, _c.c_char_p, _c.c_size_t,
                                                        _vp]),
     "binius_vision4_permute": (_int, [_vp, _u64, _vp]),
+    "binius_eval_form_create": (_int, [_c.c_char_p, _c.c_size_t, _u64, _vp]),
+    "binius_eval_form_info": (_int, [_vp, _vp]),
+    "binius_eval_form_evaluate": (_int, [_vp, _vp, _u32, _vp, _vp, _vp]),
+    "binius_eval_form_destroy": (_int, [_vp]),
+    "binius_values_transpose": (_int, [_vp, _u64, _u64, _vp, _vp]),
     "binius_merkle_commit_vision4": (_int, [_vp, _u32, _u32, _vp, _vp]),
     "binius_pcs_set_merkle_hash": (_int, [_vp, _u32]),
     "binius_prover_set_merkle_hash": (_int, [_vp, _u32]),

@@ -351,6 +351,35 @@ int binius_prover_setup_with_key_collection(binius_cs* cs, uint32_t log_inv_rate
                                             const void* h_kc, size_t kc_len, binius_prover** out);
 
 /* ------------------------------------------------------------------------------------------
+ * Witness evaluation (the frontend's evaluation form) on the device.
+ * Replaces: EvalForm::evaluate / Interpreter::run (verifier/frontend/src/compiler/eval_form/
+ * mod.rs:68-78, interpreter.rs:113-520) with the Word arithmetic of verifier/core/src/word.rs,
+ * over a batch of value vectors at once.
+ * binius_eval_form_create decodes the bytecode (builder.rs encoding) for value vectors of
+ * n_values words and level-schedules it; BINIUS_E_ARG for an unknown opcode, a register >=
+ * n_values, a truncated instruction, a shift amount >= 64 or a hint call (0x80: hint handlers
+ * are host code and are not run here).  binius_eval_form_info: out4 = instructions, levels,
+ * widest level, assertions.
+ * binius_eval_form_evaluate runs it over d_values, n_values * batch words laid out register-major
+ * (word r of instance i at d_values[r * batch + i]), in place and asynchronously on `stream`.
+ * d_fail_count[i] receives instance i's number of failed assertions and d_first_fail[i] its
+ * earliest failing assertion in program order as (instruction index << 32 | assertion id), or
+ * all ones.
+ * binius_values_transpose: d_dst[c * rows + r] = d_src[r * cols + c] for 64-bit words (between
+ * instance-major value vectors and the register-major batch).
+ * ------------------------------------------------------------------------------------------ */
+typedef struct binius_eval_form binius_eval_form;
+
+int binius_eval_form_create(const void* h_bytecode, size_t len, uint64_t n_values,
+                            binius_eval_form** out);
+int binius_eval_form_info(const binius_eval_form* ef, uint64_t* out4);
+int binius_eval_form_evaluate(const binius_eval_form* ef, void* d_values, uint32_t batch,
+                              uint32_t* d_fail_count, uint64_t* d_first_fail, void* stream);
+int binius_eval_form_destroy(binius_eval_form* ef);
+int binius_values_transpose(const void* d_src, uint64_t rows, uint64_t cols, void* d_dst,
+                            void* stream);
+
+/* ------------------------------------------------------------------------------------------
  * Integer multiplication reduction.
  * Replaces: build_intmul_witness + prove_intmul_reduction (prover/prover/src/prove.rs:374-391,
  * 432-470), intmul Witness (protocols/intmul/witness.rs:47-270) and IntMulProver::prove

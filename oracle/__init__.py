@@ -60,6 +60,10 @@ def lib():
         L.orc_merkle_commit.argtypes = [_u64p, ctypes.c_uint32, ctypes.c_uint32, _u8p]
         L.orc_merkle_commit.restype = ctypes.c_int
         L.orc_set_merkle_hash.argtypes = [ctypes.c_int]
+        L.orc_eval_form_run.argtypes = [_u8p, ctypes.c_size_t, _u64p, ctypes.c_size_t,
+                                        ctypes.POINTER(ctypes.c_uint32),
+                                        ctypes.POINTER(ctypes.c_uint32)]
+        L.orc_eval_form_run.restype = ctypes.c_int
         L.orc_vision4_permutation.argtypes = [_u64p]
         L.orc_vision4_digest.argtypes = [_u8p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t),
                                          ctypes.c_size_t, _u8p]
@@ -253,6 +257,17 @@ def _int_elems(vals) -> np.ndarray:
 def _elems_int(arr) -> list:
     a = np.asarray(arr, dtype=np.uint64).reshape(-1, 2)
     return [int(lo) | (int(hi) << 64) for lo, hi in a]
+
+
+def eval_form_run(code: bytes, values: np.ndarray):
+    """Interpreter::run over a copy of values (uint64); returns (rc, values, n_failures,
+    first_error_id)."""
+    v = np.ascontiguousarray(values, dtype=np.uint64).copy()
+    buf = np.frombuffer(bytes(code) or b"\0", dtype=np.uint8).copy()
+    nf, fe = ctypes.c_uint32(0), ctypes.c_uint32(0)
+    rc = lib().orc_eval_form_run(_p8(buf), len(code), _p64(v) if len(v) else None, len(v),
+                                 ctypes.byref(nf), ctypes.byref(fe))
+    return rc, v, nf.value, fe.value
 
 
 class merkle_hash:

@@ -82,6 +82,13 @@ void orc_vision4_constants(uint64_t* rc, uint64_t* binv0);
 int orc_vision4_merkle_commit(const uint64_t* elems, uint32_t log_leaves, uint32_t log_batch,
                               uint8_t* nodes_out);
 
+/* ---- Witness evaluation (verifier/frontend/src/compiler/eval_form/interpreter.rs) ----
+ * Runs the bytecode over values[0..n_values) in place.  Returns 0, or -1 unknown opcode, -2 hint
+ * call, -3 register out of range, -4 truncated instruction, -5 shift amount >= 64.
+ * n_failures / first_error_id: assertion failures and the id of the first one. */
+int orc_eval_form_run(const uint8_t* code, size_t len, uint64_t* values, size_t n_values,
+                      uint32_t* n_failures, uint32_t* first_error_id);
+
 /* ---- FRI folds (prover/prover/src/fri/fold.rs:260-318; verifier/.../fri/fold.rs:20-130) ---- */
 void orc_eq_ind_partial_eval(const uint64_t* point, uint32_t n, uint64_t* out);
 int orc_fri_fold_interleaved(const uint64_t* codeword, uint32_t log_len, uint32_t log_batch,
