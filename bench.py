@@ -19,6 +19,11 @@ proof (the bivariate product sumcheck fold + round, shift phase 2 and BaseFold) 
 --workload commit: the kernel-level FRI commit pipeline (RS encode of 16 interleaved columns of
 codeword length 2^20, SHA-256 Merkle commit, 3 FRI folds with commits) with the NTT pass roofline.
 
+--workload witness: witness generation on the device (the frontend's evaluation-form bytecode)
+for the same 2^20-word circuit, over a batch of instances with different witness inputs; value =
+ms per instance with the inputs resident, e2e with the inputs copied in and every generated
+witness copied out.
+
 --impl reference times the CPU restatement of the reference (oracle/, all host threads) on the
 same workload; the Rust reference cannot be built in this image (no cargo).
 """
@@ -53,6 +58,8 @@ FOLD_ARITY = 4
 N_FOLDS = 3
 
 PROVE_METRIC = "prove ms @2^20 words"
+WITNESS_METRIC = "witness generation ms per instance @2^20 words"
+WITNESS_BATCH = 32
 COMMIT_METRIC = "FRI commit ms: RS encode + SHA-256 Merkle + 3 FRI folds with commits"
 
 
@@ -92,7 +99,8 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="prove", choices=["prove", "commit", "batch", "serve"])
+    ap.add_argument("--workload", default="prove",
+                    choices=["prove", "commit", "batch", "serve", "witness"])
     ap.add_argument("--requests", type=int, default=256, help="batch / serve: proofs submitted")
     ap.add_argument("--workers", type=int, default=16, help="batch / serve: proving threads")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -718,6 +726,140 @@ def run_commit(args, rank, world, local):
         pg.destroy_process_group()
 
 
+# ----------------------------------------------------------------------------- witness workload
+
+def witness_setup(log_words):
+    from binius64_b200 import eval_form as ef
+    circ = make_circuit(log_words)
+    code, n_values, n_insn = ef.synthetic_program(circ, with_count=True)
+    return circ, code, n_values, n_insn, ef.synthetic_inputs(circ, n_values)
+
+
+def witness_config(log_words, n_values, n_insn, batch):
+    return {
+        "workload": f"witness generation: the evaluation-form program recomputing the internal "
+                    f"words of the 2^{log_words}-word synthetic circuit ({n_insn} instructions, "
+                    f"{n_values} registers) for {batch} instances with different witness inputs",
+        "log_words": log_words, "n_and": n_and_for(log_words), "n_mul": 1,
+        "instructions": n_insn, "registers": n_values, "batch": batch,
+        "l2": f"inputs larger than L2 ({n_values * batch * 8 >> 20} MiB of registers); no flush",
+        "seed": SEED,
+    }
+
+
+def cpu_witness_ms(code, v0, reps=1):
+    import oracle as orc
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        rc, _, _, _ = orc.eval_form_run(code, v0)
+        times.append(time.perf_counter() - t0)
+        assert rc == 0
+    return 1000.0 * statistics.mean(times)
+
+
+def run_witness(args, rank, world, local):
+    import torch
+    from binius64_b200 import eval_form as ef
+    from binius64_b200._ffi import lib
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    stream = torch.cuda.current_stream()
+    batch = WITNESS_BATCH
+    circ, code, n_values, _, v0 = witness_setup(LOG_WORDS)
+    prog = ef.EvalForm(code, n_values)
+    lay = circ.cs.layout
+    n_in, n_com = lay.committed_total_len - lay.n_internal, lay.committed_total_len
+    rng = np.random.default_rng(SEED + 7)
+    inputs = np.repeat(v0[None, :n_in], batch, axis=0)
+    inputs[1:, lay.offset_witness:n_in] = rng.integers(
+        0, 2**64, size=(batch - 1, n_in - lay.offset_witness), dtype=np.uint64, endpoint=False)
+    dev = f"cuda:{local}"
+    regs = torch.zeros(n_values * batch, dtype=torch.int64, device=dev)
+    host_in = torch.from_numpy(inputs.view(np.int64)).reshape(-1).pin_memory()
+    d_in = torch.empty_like(host_in, device=dev)
+    d_out = torch.empty(batch * n_com, dtype=torch.int64, device=dev)
+    host_out = torch.empty(batch * n_com, dtype=torch.int64).pin_memory()
+    d_in.copy_(host_in)
+    ef.transpose_words(d_in, batch, n_in, out=regs[: n_in * batch])
+    for _ in range(args.warmup):
+        fails, _ = prog.evaluate(regs, batch)
+    torch.cuda.synchronize()
+    assert int(fails.sum()) == 0
+    launches0 = lib().binius_launch_count()
+    if pg:
+        pg.barrier()
+    clk = sample_clocks_start(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        prog.evaluate(regs, batch)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sample_clocks_stop(clk)
+    launches = (lib().binius_launch_count() - launches0) / args.steps
+    step_ms = e0.elapsed_time(e1) / args.steps
+    if pg:
+        t = torch.tensor([step_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        step_ms = float(t.item())
+    ms = step_ms / (batch * world)  # whole-job ms per instance
+    # end to end: inputs in from pinned host memory, every witness out
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        d_in.copy_(host_in, non_blocking=True)
+        ef.transpose_words(d_in, batch, n_in, out=regs[: n_in * batch])
+        prog.evaluate(regs, batch)
+        ef.transpose_words(regs[: n_com * batch], n_com, batch, out=d_out)
+        host_out.copy_(d_out, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / (args.steps * batch)
+    out = host_out.numpy().view(np.uint64).reshape(batch, n_com)
+    assert np.array_equal(out[0], circ.witness), "instance 0 must regenerate the circuit witness"
+    line = None
+    if rank == 0:
+        peak, peak_kind = measured_peak_hbm()
+        bytes_step = 8 * prog.n_accesses * batch
+        achieved = bytes_step / (step_ms * 1e-3) / 1e9
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = {"value": cpu_witness_ms(code, v0), "unit": "ms", "cores": 1, "kind": "port",
+                   "sample": "one instance on the oracle's interpreter (a restatement of "
+                             "Interpreter::run, sequential like the reference's)"}
+        line = {
+            "metric": WITNESS_METRIC, "value": ms, "unit": "ms", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u64 words", "data": "synthetic (seeded witness inputs)",
+            "config": witness_config(LOG_WORDS, n_values, prog.n_insn, batch),
+            "levels": prog.n_levels,
+            "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(host_in.numel() * 8),
+                    "d2h_bytes_per_step": int(host_out.numel() * 8)},
+            "gpu_launches": int(round(launches)),
+            "roofline": {"bound": "hbm", "kernel": "eval_level_kernel (all levels of one step)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": None, "algorithmic_bytes_per_step": bytes_step,
+                         "note": "algorithmic bytes = 8 x register accesses x batch"},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if line:
+        print(json.dumps(line), flush=True)
+
+
 # ----------------------------------------------------------------------------- reference arm
 
 def reference_arm(args, rank):
@@ -735,6 +877,17 @@ def reference_arm(args, rank):
                 times.append(t)
         metric, config = PROVE_METRIC, prove_config(LOG_WORDS)
         sample = f"each step one whole proof of the 2^{LOG_WORDS}-word circuit"
+    elif args.workload == "witness":
+        circ, code, n_values, n_insn, v0 = witness_setup(LOG_WORDS)
+        times = []
+        for i in range(args.warmup + args.steps):
+            t = cpu_witness_ms(code, v0)
+            if i >= args.warmup:
+                times.append(t)
+        metric = WITNESS_METRIC
+        config = witness_config(LOG_WORDS, n_values, n_insn, WITNESS_BATCH)
+        sample = "each step one instance on the oracle's interpreter (sequential, one thread)"
+        threads = 1
     else:
         times = []
         for i in range(args.warmup + args.steps):
@@ -767,6 +920,8 @@ def main():
         run_prove(args, rank, world, local)
     elif args.workload in ("batch", "serve"):
         run_batch_workload(args, rank, world, local, serve=args.workload == "serve")
+    elif args.workload == "witness":
+        run_witness(args, rank, world, local)
     else:
         run_commit(args, rank, world, local)
 

@@ -39,7 +39,7 @@ static_assert(sizeof(EfInsn) == 24, "instruction layout");
 
 struct binius_eval_form {
   int device = 0;
-  uint64_t n_values = 0, n_insn = 0, n_asserts = 0, max_width = 0;
+  uint64_t n_values = 0, n_insn = 0, n_asserts = 0, max_width = 0, n_accesses = 0;
   std::vector<uint64_t> level_start;  // level k holds instructions [start[k], start[k+1])
   EfInsn* d_insn = nullptr;           // level order
   uint32_t* d_prog_index = nullptr;   // program position of each (for assertion order)
@@ -298,7 +298,7 @@ int binius_eval_form_create(const void* h_bytecode, size_t len, uint64_t n_value
   std::vector<uint32_t> side, src;
   std::vector<uint32_t> level;                               // per instruction
   std::vector<uint32_t> w_level(n_values, 0), r_level(n_values, 0);  // 0: initial value
-  uint64_t n_asserts = 0;
+  uint64_t n_asserts = 0, n_accesses = 0;
   while (d.pc < d.len) {
     EfInsn in;
     uint32_t dst[2], n_dst = 0;
@@ -314,6 +314,7 @@ int binius_eval_form_create(const void* h_bytecode, size_t len, uint64_t n_value
     for (uint32_t s : src) r_level[s] = std::max(r_level[s], lv);
     for (uint32_t i = 0; i < n_dst; i++) w_level[dst[i]] = lv;
     if (in.op >= 0x60 && in.op <= 0x65) n_asserts++;
+    n_accesses += src.size() + n_dst;
     prog.push_back(in);
     level.push_back(lv);
     BGPU_ARG(prog.size() < 0xffffffffull, "program too large");
@@ -337,6 +338,7 @@ int binius_eval_form_create(const void* h_bytecode, size_t len, uint64_t n_value
   ef->n_values = n_values;
   ef->n_insn = prog.size();
   ef->n_asserts = n_asserts;
+  ef->n_accesses = n_accesses;
   ef->level_start.assign(start.begin(), start.begin() + n_levels + 1);
   for (uint32_t k = 0; k < n_levels; k++)
     ef->max_width = std::max<uint64_t>(ef->max_width, start[k + 1] - start[k]);
@@ -360,13 +362,14 @@ int binius_eval_form_create(const void* h_bytecode, size_t len, uint64_t n_value
   return clear_error();
 }
 
-// out4: instructions, levels, widest level, assertions.
-int binius_eval_form_info(const binius_eval_form* ef, uint64_t* out4) {
-  BGPU_ARG(ef != nullptr && out4 != nullptr, "NULL argument");
-  out4[0] = ef->n_insn;
-  out4[1] = ef->level_start.empty() ? 0 : ef->level_start.size() - 1;
-  out4[2] = ef->max_width;
-  out4[3] = ef->n_asserts;
+// out5: instructions, levels, widest level, assertions, register accesses (sources + destinations).
+int binius_eval_form_info(const binius_eval_form* ef, uint64_t* out5) {
+  BGPU_ARG(ef != nullptr && out5 != nullptr, "NULL argument");
+  out5[0] = ef->n_insn;
+  out5[1] = ef->level_start.empty() ? 0 : ef->level_start.size() - 1;
+  out5[2] = ef->max_width;
+  out5[3] = ef->n_asserts;
+  out5[4] = ef->n_accesses;
   return clear_error();
 }
 

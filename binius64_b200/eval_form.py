@@ -151,9 +151,10 @@ def _emit_operand(bb, sc, terms) -> int:
     return out
 
 
-def synthetic_program(circ) -> tuple[bytes, int]:
+def synthetic_program(circ, with_count: bool = False):
     """(bytecode, n_values) recomputing every internal word of a synthetic_circuit from its
-    constants, public inputs and witness inputs; n_values = committed words + scratch."""
+    constants, public inputs and witness inputs; n_values = committed words + scratch.  With
+    with_count, (bytecode, n_values, number of instructions)."""
     cs = circ.cs
     lay = cs.layout
     total = lay.committed_total_len
@@ -181,6 +182,8 @@ def synthetic_program(circ) -> tuple[bytes, int]:
         a, b = terms(mul_csr, 4 * i), terms(mul_csr, 4 * i + 1)
         hi, lo = terms(mul_csr, 4 * i + 2)[0][0], terms(mul_csr, 4 * i + 3)[0][0]
         bb.imul(hi, lo, _emit_operand(bb, sc, a), _emit_operand(bb, sc, b))
+    if with_count:
+        return bb.finalize(), sc.next, bb.n_eval_insn
     return bb.finalize(), sc.next
 
 
@@ -202,10 +205,11 @@ class EvalForm:
         self._h = ctypes.c_void_p()
         check(lib().binius_eval_form_create(bytecode, len(bytecode), n_values,
                                             ctypes.byref(self._h)))
-        info = (ctypes.c_uint64 * 4)()
+        info = (ctypes.c_uint64 * 5)()
         check(lib().binius_eval_form_info(self._h, ctypes.addressof(info)))
         self.n_values = n_values
-        self.n_insn, self.n_levels, self.max_level_width, self.n_asserts = list(info)
+        (self.n_insn, self.n_levels, self.max_level_width, self.n_asserts,
+         self.n_accesses) = list(info)
 
     def evaluate(self, values, batch: int, stream=None):
         """values: device int64 tensor of n_values * batch words (register-major), updated in

@@ -358,8 +358,8 @@ int binius_prover_setup_with_key_collection(binius_cs* cs, uint32_t log_inv_rate
  * binius_eval_form_create decodes the bytecode (builder.rs encoding) for value vectors of
  * n_values words and level-schedules it; BINIUS_E_ARG for an unknown opcode, a register >=
  * n_values, a truncated instruction, a shift amount >= 64 or a hint call (0x80: hint handlers
- * are host code and are not run here).  binius_eval_form_info: out4 = instructions, levels,
- * widest level, assertions.
+ * are host code and are not run here).  binius_eval_form_info: out5 = instructions, levels,
+ * widest level, assertions, register accesses (sources + destinations over the program).
  * binius_eval_form_evaluate runs it over d_values, n_values * batch words laid out register-major
  * (word r of instance i at d_values[r * batch + i]), in place and asynchronously on `stream`.
  * d_fail_count[i] receives instance i's number of failed assertions and d_first_fail[i] its
@@ -372,7 +372,7 @@ typedef struct binius_eval_form binius_eval_form;
 
 int binius_eval_form_create(const void* h_bytecode, size_t len, uint64_t n_values,
                             binius_eval_form** out);
-int binius_eval_form_info(const binius_eval_form* ef, uint64_t* out4);
+int binius_eval_form_info(const binius_eval_form* ef, uint64_t* out5);
 int binius_eval_form_evaluate(const binius_eval_form* ef, void* d_values, uint32_t batch,
                               uint32_t* d_fail_count, uint64_t* d_first_fail, void* stream);
 int binius_eval_form_destroy(binius_eval_form* ef);
