@@ -133,6 +133,26 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(value: float, pg, device: str) -> float:
+    """The largest of every rank's value (replicas: the job ends when its slowest rank does);
+    the value itself with one rank (pg None).  device: where the collective's tensor lives
+    ("cuda:i" under NCCL, "cpu" under gloo)."""
+    if pg is None:
+        return value
+    import torch
+    pg.barrier()
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_ms_per_unit(slowest_ms: float, units_per_rank: int, world: int) -> float:
+    """Whole-job time per unit (proof, instance) for weak-scaled replicas: every rank processes
+    units_per_rank units in parallel, so the job does units_per_rank * world units in the
+    slowest rank's time."""
+    return slowest_ms / (units_per_rank * world)
+
+
 def fold_challenges(rng, n):
     return rng.integers(0, np.iinfo(np.uint64).max, size=(n, 2), dtype=np.uint64, endpoint=True)
 
@@ -466,13 +486,8 @@ def run_prove(args, rank, world, local):
     wall = time.perf_counter() - t_wall0
     clocks = sample_clocks_stop(clk)
     launches = (lib().binius_launch_count() - launches0) / args.steps
-    total_ms = sum(per)
-    if pg:
-        pg.barrier()
-        t = torch.tensor([total_ms], device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
-    ms = total_ms / (args.steps * world)  # whole-job ms per proof (replicas)
+    total_ms = max_over_ranks(sum(per), pg, f"cuda:{local}")
+    ms = whole_job_ms_per_unit(total_ms, args.steps, world)  # whole-job ms per proof
 
     # --- end to end: pinned host witness -> device, prove, proof bytes on the host
     host_w = torch.from_numpy(circ.witness.view(np.int64)).pin_memory()
@@ -651,12 +666,8 @@ def run_commit(args, rank, world, local):
     torch.cuda.synchronize()
     clocks = sample_clocks_stop(clk)
     launches = (lib().binius_launch_count() - launches0) / args.steps
-    ms = ev0.elapsed_time(ev1) / args.steps
-    if pg:
-        pg.barrier()
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item()) / world
+    ms = whole_job_ms_per_unit(
+        max_over_ranks(ev0.elapsed_time(ev1) / args.steps, pg, f"cuda:{local}"), 1, world)
 
     # dominant kernel: the NTT pass (ntt_pass_kernel launches over the codeword)
     reps = max(3, args.steps)
@@ -805,12 +816,8 @@ def run_witness(args, rank, world, local):
     torch.cuda.synchronize()
     clocks = sample_clocks_stop(clk)
     launches = (lib().binius_launch_count() - launches0) / args.steps
-    step_ms = e0.elapsed_time(e1) / args.steps
-    if pg:
-        t = torch.tensor([step_ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        step_ms = float(t.item())
-    ms = step_ms / (batch * world)  # whole-job ms per instance
+    step_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, pg, dev)
+    ms = whole_job_ms_per_unit(step_ms, batch, world)  # whole-job ms per instance
     # end to end: inputs in from pinned host memory, every witness out
     torch.cuda.synchronize()
     e0.record(stream)
