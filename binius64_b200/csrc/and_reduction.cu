@@ -181,7 +181,8 @@ struct PhiPowers {
 };
 
 constexpr int kUniThreads = 512;
-constexpr int kSlots = kUniThreads / 16;
+constexpr int kUniLanes = 8;  // lanes per word, 8 of the 64 points each
+constexpr int kSlots = kUniThreads / kUniLanes;
 constexpr size_t kUniSmem = sizeof(uint32_t) * 8 * 256 * 16 + 8 * 256 + 256 + 512 +
                             sizeof(uint4) * kSlots * 8;
 
@@ -190,11 +191,29 @@ __device__ __forceinline__ uint8_t gf8_mul(const uint8_t* s_log, const uint8_t* 
   return (a && b) ? s_exp[s_log[a] + s_log[b]] : 0;
 }
 
-__device__ __forceinline__ uint32_t word_ntt(const uint32_t* sT, uint64_t w, uint32_t kq) {
-  uint32_t acc = 0;
+// The word's extension values at points 8 kq .. 8 kq + 7: one 8-byte row per byte of the word.
+__device__ __forceinline__ uint2 word_ntt(const uint2* sT2, uint64_t w, uint32_t kq) {
+  uint2 acc = make_uint2(0u, 0u);
 #pragma unroll
-  for (int bi = 0; bi < 8; bi++) acc ^= sT[((bi << 8) | (uint32_t)((w >> (8 * bi)) & 255)) * 16 + kq];
+  for (int bi = 0; bi < 8; bi++) {
+    const uint2 t = sT2[((bi << 8) | (uint32_t)((w >> (8 * bi)) & 255)) * 8 + kq];
+    acc.x ^= t.x;
+    acc.y ^= t.y;
+  }
   return acc;
+}
+
+__device__ __forceinline__ uint32_t and_bytes(const uint8_t* s_log, const uint8_t* s_exp,
+                                              const uint8_t* mj, uint32_t A, uint32_t B,
+                                              uint32_t C) {
+  uint32_t v = 0;
+#pragma unroll
+  for (int l = 0; l < 4; l++) {
+    const uint32_t x = gf8_mul(s_log, s_exp, (A >> (8 * l)) & 255, (B >> (8 * l)) & 255) ^
+                       ((C >> (8 * l)) & 255);
+    v ^= (uint32_t)mj[x] << (8 * l);
+  }
+  return v;
 }
 
 __global__ void __launch_bounds__(kUniThreads, 1)
@@ -204,6 +223,7 @@ __global__ void __launch_bounds__(kUniThreads, 1)
                             uint32_t* __restrict__ out) {
   extern __shared__ uint4 smem4[];
   uint32_t* sT = reinterpret_cast<uint32_t*>(smem4);
+  const uint2* sT2 = reinterpret_cast<const uint2*>(sT);
   uint8_t* s_mul = reinterpret_cast<uint8_t*>(sT + 8 * 256 * 16);
   uint8_t* s_log = s_mul + 8 * 256;
   uint8_t* s_exp = s_log + 256;
@@ -212,35 +232,33 @@ __global__ void __launch_bounds__(kUniThreads, 1)
   for (uint32_t i = threadIdx.x; i < 8 * 256; i += blockDim.x) s_mul[i] = tab.mul_eq[i];
   for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) s_log[i] = tab.log[i];
   for (uint32_t i = threadIdx.x; i < 512; i += blockDim.x) s_exp[i] = tab.exp[i];
-  const uint32_t kq = threadIdx.x & 15, slot = threadIdx.x >> 4;
-  uint4 acc[4] = {gf_zero(), gf_zero(), gf_zero(), gf_zero()};
+  const uint32_t kq = threadIdx.x & (kUniLanes - 1), slot = threadIdx.x / kUniLanes;
+  uint4 acc[8];
+#pragma unroll
+  for (int l = 0; l < 8; l++) acc[l] = gf_zero();
   const uint64_t stride = (uint64_t)gridDim.x * kSlots;
   const uint64_t iters = (n_chunks + stride - 1) / stride;
   for (uint64_t it = 0; it < iters; it++) {
     const uint64_t chunk = it * stride + (uint64_t)blockIdx.x * kSlots + slot;
     const bool valid = chunk < n_chunks;
     __syncthreads();
-    if (valid && kq < 8) s_P[slot * 8 + kq] = gf_mul(eq_big[chunk], phi.p[kq]);
+    if (valid) s_P[slot * 8 + kq] = gf_mul(eq_big[chunk], phi.p[kq]);
     __syncthreads();
     if (valid) {
-      uint32_t v4 = 0;
+      uint32_t vlo = 0, vhi = 0;
 #pragma unroll 1
       for (int j = 0; j < 8; j++) {
         const uint64_t i = chunk * 8 + j;
-        const uint32_t A = word_ntt(sT, __ldg(wa + i), kq);
-        const uint32_t B = word_ntt(sT, __ldg(wb + i), kq);
-        const uint32_t Cv = word_ntt(sT, __ldg(wc + i), kq);
+        const uint2 A = word_ntt(sT2, __ldg(wa + i), kq);
+        const uint2 B = word_ntt(sT2, __ldg(wb + i), kq);
+        const uint2 Cv = word_ntt(sT2, __ldg(wc + i), kq);
         const uint8_t* mj = s_mul + (j << 8);
-#pragma unroll
-        for (int l = 0; l < 4; l++) {
-          const uint32_t x = gf8_mul(s_log, s_exp, (A >> (8 * l)) & 255, (B >> (8 * l)) & 255) ^
-                             ((Cv >> (8 * l)) & 255);
-          v4 ^= (uint32_t)mj[x] << (8 * l);
-        }
+        vlo ^= and_bytes(s_log, s_exp, mj, A.x, B.x, Cv.x);
+        vhi ^= and_bytes(s_log, s_exp, mj, A.y, B.y, Cv.y);
       }
 #pragma unroll
-      for (int l = 0; l < 4; l++) {
-        const uint32_t v = (v4 >> (8 * l)) & 255;
+      for (int l = 0; l < 8; l++) {
+        const uint32_t v = ((l < 4 ? vlo : vhi) >> (8 * (l & 3))) & 255;
 #pragma unroll
         for (int b = 0; b < 8; b++) {
           const uint32_t m = 0u - ((v >> b) & 1u);
@@ -257,7 +275,7 @@ __global__ void __launch_bounds__(kUniThreads, 1)
   __syncthreads();
   uint4* red = smem4;
 #pragma unroll
-  for (int l = 0; l < 4; l++) red[(4 * kq + l) * kSlots + slot] = acc[l];
+  for (int l = 0; l < 8; l++) red[(8 * kq + l) * kSlots + slot] = acc[l];
   __syncthreads();
   if (threadIdx.x < 64) {
     uint4 s = gf_zero();
