@@ -24,9 +24,10 @@ _u8p = ctypes.POINTER(ctypes.c_uint8)
 
 
 def build(force: bool = False) -> str:
-    """Compile ``liboracle.so`` with the committed Makefile."""
-    if force or not os.path.exists(_LIB_PATH):
-        subprocess.run(["make", "-C", _HERE, "-s"], check=True)
+    """Compile ``liboracle.so`` with the committed Makefile (make rebuilds it when a source is
+    newer; force rebuilds it regardless)."""
+    cmd = ["make", "-C", _HERE, "-s"] + (["-B"] if force else [])
+    subprocess.run(cmd, check=True)
     return _LIB_PATH
 
 
