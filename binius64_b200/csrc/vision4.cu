@@ -20,6 +20,8 @@
 //    x; the tables are stored as four 32-bit planes so a warp's lookups of one nibble position
 //    fall into 16 consecutive words of shared memory (no bank conflicts).
 // Six maps x 8 KiB of tables + the round constants stay in shared memory for the kernel's life.
+// Trees of up to 2^12 leaves (the FRI fold rounds') run one permutation over four lanes instead,
+// which shortens the chain of dependent permutations they are made of (see the lane kernels).
 #include <string.h>
 
 #include <mutex>
@@ -430,6 +432,138 @@ __global__ void __launch_bounds__(kV4Threads, 2)
   }
 }
 
+// ---- small trees: one permutation over four lanes
+//
+// A tree of few leaves cannot fill the GPU, so its time is the chain of dependent permutations
+// (a leaf's sponge, then one per layer) on single threads.  Here four consecutive lanes hold one
+// state, element e = lane & 3 each: every lane inverts its own element (four inversions instead
+// of Montgomery's one, but nothing of the sbox waits for another element) and applies B or B^-1;
+// the MDS combines the four elements by shuffles.  About half the instructions of one thread's
+// permutation sit on the chain.
+
+__device__ __forceinline__ uint4 shfl_xor_gf(uint4 v, int m) {
+  return make_uint4(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m),
+                    __shfl_xor_sync(0xffffffffu, v.z, m), __shfl_xor_sync(0xffffffffu, v.w, m));
+}
+
+__device__ __forceinline__ uint4 shfl_gf(uint4 v, int src) {
+  return make_uint4(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
+                    __shfl_sync(0xffffffffu, v.z, src), __shfl_sync(0xffffffffu, v.w, src));
+}
+
+// The permutation of the state held by this lane's group of four; returns element e.  Every lane
+// of the warp calls it together.
+static __device__ __noinline__ uint4 v4_permute_lane(uint4 x, uint32_t e) {
+  const uint32_t next = (threadIdx.x & 31u & ~3u) | ((e + 1) & 3u);
+  x = gf_add(x, v4_img[kRcOff + e]);
+#pragma unroll 1
+  for (uint32_t h = 0; h < 16; h++) {
+    const bool inverse = (h & 1) == 0;
+    x = gf_add(v4_map(inverse ? kMapLinv : kMapLfwd, v4_inv(x)),
+               v4_img[inverse ? kBinv0Off : kC0Off]);
+    // MDS: x_e += (x_0 + x_1 + x_2 + x_3) + 2 (x_e + x_{e+1 mod 4}), all from the old values
+    const uint4 s1 = gf_add(x, shfl_xor_gf(x, 1));
+    const uint4 sum = gf_add(s1, shfl_xor_gf(s1, 2));
+    const uint4 nx = shfl_gf(x, (int)next);
+    x = gf_add(gf_add(x, sum), mul_x(gf_add(x, nx)));
+    x = gf_add(x, v4_img[kRcOff + 4 * (h + 1) + e]);
+  }
+  return x;
+}
+
+constexpr uint32_t kLaneLeafFuse = 6;  // 2^6 leaves (256 lanes) per CTA
+constexpr uint32_t kLaneNodeFuse = 7;  // 2^7 inputs per CTA
+constexpr uint32_t kLaneMaxLog = 12;   // trees of up to 2^12 leaves take the four-lane kernels
+
+__global__ void __launch_bounds__(256)
+    vision4_leaves_lanes_kernel(const uint4* __restrict__ img, const uint4* __restrict__ elems,
+                                uint32_t log_batch, uint4* __restrict__ nodes, uint32_t L,
+                                uint32_t fused) {
+  v4_load_image(img);
+  uint4* buf = v4_nodes_buf();
+  const uint32_t e = threadIdx.x & 3, item = threadIdx.x >> 2, n0 = 1u << fused;
+  const bool valid = item < n0;  // lanes past the CTA's leaves compute along for the shuffles
+  const uint64_t leaf = (uint64_t)blockIdx.x * n0 + (valid ? item : 0);
+  const uint4* ep = elems + (leaf << log_batch);
+  uint4 x = gf_zero();
+  if (log_batch == 0) {
+    if (e == 0) x = ep[0];
+    if (e == 1) x = make_uint4(0x80u, 0u, 0u, 0x01000000u);
+    x = v4_permute_lane(x, e);
+  } else {
+    const uint32_t blocks = 1u << (log_batch - 1);
+#pragma unroll 1
+    for (uint32_t j = 0; j < blocks; j++) {
+      if (e < 2) x = ep[2 * j + e];
+      x = v4_permute_lane(x, e);
+    }
+    if (e == 0) x = make_uint4(0x80u, 0u, 0u, 0u);
+    if (e == 1) x = make_uint4(0u, 0u, 0u, 0x01000000u);
+    x = v4_permute_lane(x, e);
+  }
+  if (valid && e < 2) {
+    nodes[2 * leaf + e] = x;
+    buf[2 * item + e] = x;
+  }
+  for (uint32_t lvl = 1; lvl <= fused; lvl++) {
+    __syncthreads();
+    const uint32_t n = n0 >> lvl;
+    const uint32_t src = ((lvl - 1) & 1) * 2 * kV4Threads, dst = (lvl & 1) * 2 * kV4Threads;
+    const bool act = item < n;
+    const uint4 in = act ? buf[src + 4 * item + e] : gf_zero();
+    const uint4 y = v4_permute_lane(in, e);
+    if (act && e < 2) {
+      const uint4 o = gf_add(y, in);
+      buf[dst + 2 * item + e] = o;
+      nodes[2 * (layer_offset(L, lvl) + (uint64_t)blockIdx.x * n + item) + e] = o;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256)
+    vision4_nodes_lanes_kernel(const uint4* __restrict__ img, uint4* __restrict__ nodes,
+                               uint32_t L, uint32_t in_level, uint32_t fused) {
+  v4_load_image(img);
+  uint4* buf = v4_nodes_buf();
+  const uint32_t e = threadIdx.x & 3, item = threadIdx.x >> 2, n_in = 1u << fused;
+  const uint64_t in_off = layer_offset(L, in_level) + (uint64_t)blockIdx.x * n_in;
+  for (uint32_t lvl = 1; lvl <= fused; lvl++) {
+    const uint32_t n = n_in >> lvl;
+    const uint32_t src = ((lvl - 1) & 1) * 2 * kV4Threads, dst = (lvl & 1) * 2 * kV4Threads;
+    if (lvl > 1) __syncthreads();
+    const bool act = item < n;
+    uint4 in = gf_zero();
+    if (act) in = lvl == 1 ? nodes[2 * in_off + 4 * item + e] : buf[src + 4 * item + e];
+    const uint4 y = v4_permute_lane(in, e);
+    if (act && e < 2) {
+      const uint4 o = gf_add(y, in);
+      buf[dst + 2 * item + e] = o;
+      nodes[2 * (layer_offset(L, in_level + lvl) + (uint64_t)blockIdx.x * n + item) + e] = o;
+    }
+  }
+}
+
+int vision4_commit_lanes(const uint4* img, const uint4* elems, uint32_t L, uint32_t log_batch,
+                         uint4* nodes, cudaStream_t s) {
+  if (int rc = ensure_smem_limit((const void*)vision4_leaves_lanes_kernel, kV4Smem)) return rc;
+  if (int rc = ensure_smem_limit((const void*)vision4_nodes_lanes_kernel, kV4Smem)) return rc;
+  const uint32_t fused = L < kLaneLeafFuse ? L : kLaneLeafFuse;
+  const uint32_t threads = (4u << fused) < 32u ? 32u : (4u << fused);
+  vision4_leaves_lanes_kernel<<<1u << (L - fused), threads, kV4Smem, s>>>(img, elems, log_batch,
+                                                                        nodes, L, fused);
+  BGPU_LAUNCH_CHECK("vision4_leaves_lanes_kernel");
+  count_launch();
+  for (uint32_t level = fused; level < L;) {
+    const uint32_t f = (L - level) < kLaneNodeFuse ? (L - level) : kLaneNodeFuse;
+    const uint32_t t = (2u << f) < 32u ? 32u : (2u << f);
+    vision4_nodes_lanes_kernel<<<1u << (L - level - f), t, kV4Smem, s>>>(img, nodes, L, level, f);
+    BGPU_LAUNCH_CHECK("vision4_nodes_lanes_kernel");
+    count_launch();
+    level += f;
+  }
+  return BINIUS_OK;
+}
+
 }  // namespace
 
 namespace bgpu {
@@ -444,6 +578,8 @@ int vision4_merkle_commit(const void* d_elems, uint32_t log_leaves, uint32_t log
   if (int rc = ensure_smem_limit((const void*)vision4_nodes_kernel, kV4Smem)) return rc;
   const uint32_t L = log_leaves;
   uint4* nodes = static_cast<uint4*>(d_nodes);
+  if (L <= kLaneMaxLog)
+    return vision4_commit_lanes(img, static_cast<const uint4*>(d_elems), L, log_batch, nodes, s);
   const uint32_t fused = L < kV4LeafFuse ? L : kV4LeafFuse;
   const uint64_t grid = 1ull << (L - fused);
   BGPU_ARG(grid <= 0x7fffffffull, "too many leaves");
