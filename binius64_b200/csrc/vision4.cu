@@ -471,8 +471,10 @@ static __device__ __noinline__ uint4 v4_permute_lane(uint4 x, uint32_t e) {
   return x;
 }
 
-constexpr uint32_t kLaneLeafFuse = 6;  // 2^6 leaves (256 lanes) per CTA
-constexpr uint32_t kLaneNodeFuse = 7;  // 2^7 inputs per CTA
+// Small CTAs (16 leaves = 2 warps; 16 inputs = 1 warp): the trees are too small to fill the GPU,
+// so spreading them over many SMs leaves each chain a scheduler of its own.
+constexpr uint32_t kLaneLeafFuse = 4;  // 2^4 leaves (64 lanes) per CTA
+constexpr uint32_t kLaneNodeFuse = 4;  // 2^4 inputs per CTA
 constexpr uint32_t kLaneMaxLog = 12;   // trees of up to 2^12 leaves take the four-lane kernels
 
 __global__ void __launch_bounds__(256)
