@@ -150,16 +150,19 @@ __device__ __forceinline__ void st(uint64_t* v, uint32_t reg, uint32_t batch, ui
   v[(uint64_t)reg * batch + inst] = x;
 }
 
+// POW2: batch = 2^log_batch, so the (instruction, instance) split of a thread index is a shift
+// and a mask instead of a 64-bit division.
+template <bool POW2>
 __global__ void __launch_bounds__(256)
     eval_level_kernel(const EfInsn* __restrict__ insn, const uint32_t* __restrict__ prog_index,
                       const uint32_t* __restrict__ side, uint64_t lo, uint64_t n, uint32_t batch,
-                      uint64_t* __restrict__ v, uint32_t* __restrict__ fails,
+                      uint32_t log_batch, uint64_t* __restrict__ v, uint32_t* __restrict__ fails,
                       unsigned long long* __restrict__ first) {
   const uint64_t total = n * batch;
   for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total;
        t += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t k = lo + t / batch;
-    const uint32_t inst = (uint32_t)(t % batch);
+    const uint64_t k = lo + (POW2 ? (t >> log_batch) : t / batch);
+    const uint32_t inst = (uint32_t)(POW2 ? (t & (batch - 1)) : t % batch);
     const EfInsn in = insn[k];
     const uint32_t* r = in.r;
     switch (in.op) {
@@ -385,13 +388,21 @@ int binius_eval_form_evaluate(const binius_eval_form* ef, void* d_values, uint32
   BGPU_LAUNCH_CHECK("init_fail_kernel");
   count_launch();
   uint64_t* v = static_cast<uint64_t*>(d_values);
+  const bool pow2 = (batch & (batch - 1)) == 0;
+  uint32_t log_batch = 0;
+  while ((1u << log_batch) < batch) log_batch++;
   const size_t n_levels = ef->level_start.empty() ? 0 : ef->level_start.size() - 1;
   for (size_t k = 0; k < n_levels; k++) {
     const uint64_t lo = ef->level_start[k], n = ef->level_start[k + 1] - lo;
     if (n == 0) continue;
     const uint64_t threads = n * batch, blocks = (threads + 255) / 256;
-    eval_level_kernel<<<(unsigned)std::min<uint64_t>(blocks, 148ull * 64), 256, 0, s>>>(
-        ef->d_insn, ef->d_prog_index, ef->d_side, lo, n, batch, v, d_fail_count, first);
+    const unsigned grid = (unsigned)std::min<uint64_t>(blocks, 148ull * 64);
+    if (pow2)
+      eval_level_kernel<true><<<grid, 256, 0, s>>>(ef->d_insn, ef->d_prog_index, ef->d_side, lo,
+                                                    n, batch, log_batch, v, d_fail_count, first);
+    else
+      eval_level_kernel<false><<<grid, 256, 0, s>>>(ef->d_insn, ef->d_prog_index, ef->d_side, lo,
+                                                     n, batch, log_batch, v, d_fail_count, first);
     BGPU_LAUNCH_CHECK("eval_level_kernel");
     count_launch();
   }
