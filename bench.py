@@ -758,6 +758,34 @@ def witness_config(log_words, n_values, n_insn, batch):
     }
 
 
+DEEP_OPS = 1 << 17
+
+
+def deep_chain_figures(torch, ef, dev, stream, args):
+    """A deep program (chain_program: an add-rotate-xor chain of 2^17 instructions, levels a few
+    instructions wide) for 1, 32 and 1024 instances: CUDA events around one evaluation after a
+    warm-up one; the oracle's interpreter on one instance beside it."""
+    code, n_values = ef.chain_program(DEEP_OPS, seed=SEED)
+    prog = ef.EvalForm(code, n_values)
+    out = {"instructions": prog.n_insn, "levels": prog.n_levels}
+    for batch in (1, 32, 1024):
+        regs = torch.zeros(n_values * batch, dtype=torch.int64, device=dev)
+        regs[: 8 * batch] = 0x5A5A
+        prog.evaluate(regs, batch)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        prog.evaluate(regs, batch)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[f"ms_batch_{batch}"] = e0.elapsed_time(e1)
+    if not args.no_cpu_baseline:
+        v0 = np.zeros(n_values, dtype=np.uint64)
+        v0[:8] = 0x5A5A
+        out["oracle_ms_one_instance"] = cpu_witness_ms(code, v0)
+    return out
+
+
 def cpu_witness_ms(code, v0, reps=1):
     import oracle as orc
     times = []
@@ -832,6 +860,7 @@ def run_witness(args, rank, world, local):
     e2e_ms = e0.elapsed_time(e1) / (args.steps * batch)
     out = host_out.numpy().view(np.uint64).reshape(batch, n_com)
     assert np.array_equal(out[0], circ.witness), "instance 0 must regenerate the circuit witness"
+    deep = deep_chain_figures(torch, ef, dev, stream, args) if rank == 0 else None
     line = None
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
@@ -849,6 +878,7 @@ def run_witness(args, rank, world, local):
             "dtype": "u64 words", "data": "synthetic (seeded witness inputs)",
             "config": witness_config(LOG_WORDS, n_values, prog.n_insn, batch),
             "levels": prog.n_levels,
+            "deep_chain": deep,
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(host_in.numel() * 8),
                     "d2h_bytes_per_step": int(host_out.numel() * 8)},
             "gpu_launches": int(round(launches)),

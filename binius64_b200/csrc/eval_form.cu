@@ -15,6 +15,9 @@
 // while a chain of dependent instructions (a hash's rounds) needs one launch per link and a large
 // batch to fill the GPU.
 //
+// Runs of narrow levels (at most 64 instructions each) go to a kernel whose CTAs each take a group
+// of instances through all of them, separated by barriers instead of launches.
+//
 // Assertions count their failures per instance and keep the earliest failing assertion in
 // program order (its instruction index and id); the reference collects up to 100 messages.
 // Decoding rejects what the reference would panic on: an unknown opcode, a register outside the
@@ -44,6 +47,7 @@ struct binius_eval_form {
   EfInsn* d_insn = nullptr;           // level order
   uint32_t* d_prog_index = nullptr;   // program position of each (for assertion order)
   uint32_t* d_side = nullptr;         // bxor_multi source lists
+  uint64_t* d_level_start = nullptr;  // level_start on the device (for the segment kernel)
 };
 
 namespace {
@@ -150,8 +154,120 @@ __device__ __forceinline__ void st(uint64_t* v, uint32_t reg, uint32_t batch, ui
   v[(uint64_t)reg * batch + inst] = x;
 }
 
+// Executes instruction k (level order) for instance inst.
+__device__ __forceinline__ void exec_insn(const EfInsn* __restrict__ insn,
+                                          const uint32_t* __restrict__ prog_index,
+                                          const uint32_t* __restrict__ side, uint64_t k,
+                                          uint32_t batch, uint32_t inst, uint64_t* __restrict__ v,
+                                          uint32_t* __restrict__ fails,
+                                          unsigned long long* __restrict__ first) {
+  const EfInsn in = insn[k];
+  const uint32_t* r = in.r;
+  switch (in.op) {
+    case 0x01: st(v, r[0], batch, inst, ld(v, r[1], batch, inst) & ld(v, r[2], batch, inst)); break;
+    case 0x02: st(v, r[0], batch, inst, ld(v, r[1], batch, inst) | ld(v, r[2], batch, inst)); break;
+    case 0x03: st(v, r[0], batch, inst, ld(v, r[1], batch, inst) ^ ld(v, r[2], batch, inst)); break;
+    case 0x05: {
+      const bool c = (ld(v, r[1], batch, inst) >> 63) != 0;
+      st(v, r[0], batch, inst, ld(v, c ? r[2] : r[3], batch, inst));
+      break;
+    }
+    case 0x06: {
+      uint64_t x = 0;
+      for (uint32_t i = 0; i < r[2]; i++) x ^= ld(v, side[r[1] + i], batch, inst);
+      st(v, r[0], batch, inst, x);
+      break;
+    }
+    case 0x07:
+      st(v, r[0], batch, inst,
+         (ld(v, r[1], batch, inst) & ld(v, r[2], batch, inst)) ^ ld(v, r[3], batch, inst));
+      break;
+    case 0x10: st(v, r[0], batch, inst, ld(v, r[1], batch, inst) << in.imm); break;
+    case 0x11: st(v, r[0], batch, inst, ld(v, r[1], batch, inst) >> in.imm); break;
+    case 0x12:
+      st(v, r[0], batch, inst, (uint64_t)((int64_t)ld(v, r[1], batch, inst) >> in.imm));
+      break;
+    case 0x20: case 0x21: case 0x23: {
+      const uint64_t x = ld(v, r[2], batch, inst), y = ld(v, r[3], batch, inst);
+      const uint64_t c = in.op == 0x20 ? 0 : (ld(v, r[4], batch, inst) >> 63);
+      if (in.op == 0x23) {
+        const uint64_t diff = x - y - c;
+        st(v, r[0], batch, inst, diff);
+        st(v, r[1], batch, inst, (~x & y) | (~(x ^ y) & diff));
+      } else {
+        const uint64_t sum = x + y + c;
+        st(v, r[0], batch, inst, sum);
+        st(v, r[1], batch, inst, (x & y) | ((x ^ y) & ~sum));
+      }
+      break;
+    }
+    case 0x30: case 0x31: {
+      const uint64_t x = ld(v, r[2], batch, inst), y = ld(v, r[3], batch, inst);
+      const uint64_t lo64 = x * y;
+      uint64_t hi64 = __umul64hi(x, y);
+      if (in.op == 0x31)  // signed high half from the unsigned one
+        hi64 -= ((int64_t)x < 0 ? y : 0) + ((int64_t)y < 0 ? x : 0);
+      st(v, r[0], batch, inst, hi64);
+      st(v, r[1], batch, inst, lo64);
+      break;
+    }
+    case 0x40: {
+      const uint64_t x = ld(v, r[2], batch, inst), y = ld(v, r[3], batch, inst), s = x + y;
+      st(v, r[0], batch, inst, s & 0xFFFFFFFFull);
+      st(v, r[1], batch, inst, (x & y) | ((x ^ y) & ~s));
+      break;
+    }
+    case 0x41: {
+      const uint32_t x = (uint32_t)ld(v, r[1], batch, inst);
+      st(v, r[0], batch, inst, (uint64_t)__funnelshift_r(x, x, in.imm & 31));
+      break;
+    }
+    case 0x42: st(v, r[0], batch, inst, (ld(v, r[1], batch, inst) >> in.imm) & 0xFFFFFFFFull); break;
+    case 0x43: {
+      const uint64_t x = ld(v, r[1], batch, inst);
+      const uint32_t s = in.imm & 63;
+      st(v, r[0], batch, inst, s ? ((x >> s) | (x << (64 - s))) : x);
+      break;
+    }
+    case 0x50: case 0x51: {
+      const uint32_t nb = in.imm;
+      uint64_t mask = ~0ull;  // also mask_high(0): the reference's shift by 64 wraps to 0
+      if (nb < 64 && !(in.op == 0x51 && nb == 0))
+        mask = in.op == 0x50 ? ((1ull << nb) - 1) : ~((1ull << (64 - nb)) - 1);
+      st(v, r[0], batch, inst, ld(v, r[1], batch, inst) & mask);
+      break;
+    }
+    default: {  // assertions 0x60..0x65
+      bool bad;
+      if (in.op == 0x60) {
+        bad = ld(v, r[0], batch, inst) != ld(v, r[1], batch, inst);
+      } else if (in.op == 0x61) {
+        bad = (ld(v, r[0], batch, inst) >> 63) &&
+              ld(v, r[1], batch, inst) != ld(v, r[2], batch, inst);
+      } else {
+        const uint64_t x = ld(v, r[0], batch, inst);
+        bad = in.op == 0x62 ? x != 0 : in.op == 0x63 ? x == 0
+                                      : in.op == 0x64 ? (x >> 63) != 0 : (x >> 63) == 0;
+      }
+      if (bad) {
+        atomicAdd(fails + inst, 1u);
+        atomicMin(first + inst, ((unsigned long long)prog_index[k] << 32) | r[4]);
+      }
+      break;
+    }
+  }
+}
+
 // POW2: batch = 2^log_batch, so the (instruction, instance) split of a thread index is a shift
 // and a mask instead of a 64-bit division.
+template <bool POW2>
+__device__ __forceinline__ void split(uint64_t t, uint32_t batch, uint32_t log_batch,
+                                      uint64_t& k, uint32_t& inst) {
+  k = POW2 ? (t >> log_batch) : t / batch;
+  inst = (uint32_t)(POW2 ? (t & (batch - 1)) : t % batch);
+}
+
+// One wide level: (instruction, instance) pairs over the whole grid.
 template <bool POW2>
 __global__ void __launch_bounds__(256)
     eval_level_kernel(const EfInsn* __restrict__ insn, const uint32_t* __restrict__ prog_index,
@@ -161,103 +277,34 @@ __global__ void __launch_bounds__(256)
   const uint64_t total = n * batch;
   for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total;
        t += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t k = lo + (POW2 ? (t >> log_batch) : t / batch);
-    const uint32_t inst = (uint32_t)(POW2 ? (t & (batch - 1)) : t % batch);
-    const EfInsn in = insn[k];
-    const uint32_t* r = in.r;
-    switch (in.op) {
-      case 0x01: st(v, r[0], batch, inst, ld(v, r[1], batch, inst) & ld(v, r[2], batch, inst)); break;
-      case 0x02: st(v, r[0], batch, inst, ld(v, r[1], batch, inst) | ld(v, r[2], batch, inst)); break;
-      case 0x03: st(v, r[0], batch, inst, ld(v, r[1], batch, inst) ^ ld(v, r[2], batch, inst)); break;
-      case 0x05: {
-        const bool c = (ld(v, r[1], batch, inst) >> 63) != 0;
-        st(v, r[0], batch, inst, ld(v, c ? r[2] : r[3], batch, inst));
-        break;
-      }
-      case 0x06: {
-        uint64_t x = 0;
-        for (uint32_t i = 0; i < r[2]; i++) x ^= ld(v, side[r[1] + i], batch, inst);
-        st(v, r[0], batch, inst, x);
-        break;
-      }
-      case 0x07:
-        st(v, r[0], batch, inst,
-           (ld(v, r[1], batch, inst) & ld(v, r[2], batch, inst)) ^ ld(v, r[3], batch, inst));
-        break;
-      case 0x10: st(v, r[0], batch, inst, ld(v, r[1], batch, inst) << in.imm); break;
-      case 0x11: st(v, r[0], batch, inst, ld(v, r[1], batch, inst) >> in.imm); break;
-      case 0x12:
-        st(v, r[0], batch, inst, (uint64_t)((int64_t)ld(v, r[1], batch, inst) >> in.imm));
-        break;
-      case 0x20: case 0x21: case 0x23: {
-        const uint64_t x = ld(v, r[2], batch, inst), y = ld(v, r[3], batch, inst);
-        const uint64_t c = in.op == 0x20 ? 0 : (ld(v, r[4], batch, inst) >> 63);
-        if (in.op == 0x23) {
-          const uint64_t diff = x - y - c;
-          st(v, r[0], batch, inst, diff);
-          st(v, r[1], batch, inst, (~x & y) | (~(x ^ y) & diff));
-        } else {
-          const uint64_t sum = x + y + c;
-          st(v, r[0], batch, inst, sum);
-          st(v, r[1], batch, inst, (x & y) | ((x ^ y) & ~sum));
-        }
-        break;
-      }
-      case 0x30: case 0x31: {
-        const uint64_t x = ld(v, r[2], batch, inst), y = ld(v, r[3], batch, inst);
-        const uint64_t lo64 = x * y;
-        uint64_t hi64 = __umul64hi(x, y);
-        if (in.op == 0x31)  // signed high half from the unsigned one
-          hi64 -= ((int64_t)x < 0 ? y : 0) + ((int64_t)y < 0 ? x : 0);
-        st(v, r[0], batch, inst, hi64);
-        st(v, r[1], batch, inst, lo64);
-        break;
-      }
-      case 0x40: {
-        const uint64_t x = ld(v, r[2], batch, inst), y = ld(v, r[3], batch, inst), s = x + y;
-        st(v, r[0], batch, inst, s & 0xFFFFFFFFull);
-        st(v, r[1], batch, inst, (x & y) | ((x ^ y) & ~s));
-        break;
-      }
-      case 0x41: {
-        const uint32_t x = (uint32_t)ld(v, r[1], batch, inst);
-        st(v, r[0], batch, inst, (uint64_t)__funnelshift_r(x, x, in.imm & 31));
-        break;
-      }
-      case 0x42: st(v, r[0], batch, inst, (ld(v, r[1], batch, inst) >> in.imm) & 0xFFFFFFFFull); break;
-      case 0x43: {
-        const uint64_t x = ld(v, r[1], batch, inst);
-        const uint32_t s = in.imm & 63;
-        st(v, r[0], batch, inst, s ? ((x >> s) | (x << (64 - s))) : x);
-        break;
-      }
-      case 0x50: case 0x51: {
-        const uint32_t nb = in.imm;
-        uint64_t mask = ~0ull;  // also mask_high(0): the reference's shift by 64 wraps to 0
-        if (nb < 64 && !(in.op == 0x51 && nb == 0))
-          mask = in.op == 0x50 ? ((1ull << nb) - 1) : ~((1ull << (64 - nb)) - 1);
-        st(v, r[0], batch, inst, ld(v, r[1], batch, inst) & mask);
-        break;
-      }
-      default: {  // assertions 0x60..0x65
-        bool bad;
-        if (in.op == 0x60) {
-          bad = ld(v, r[0], batch, inst) != ld(v, r[1], batch, inst);
-        } else if (in.op == 0x61) {
-          bad = (ld(v, r[0], batch, inst) >> 63) &&
-                ld(v, r[1], batch, inst) != ld(v, r[2], batch, inst);
-        } else {
-          const uint64_t x = ld(v, r[0], batch, inst);
-          bad = in.op == 0x62 ? x != 0 : in.op == 0x63 ? x == 0
-                                        : in.op == 0x64 ? (x >> 63) != 0 : (x >> 63) == 0;
-        }
-        if (bad) {
-          atomicAdd(fails + inst, 1u);
-          atomicMin(first + inst, ((unsigned long long)prog_index[k] << 32) | r[4]);
-        }
-        break;
-      }
-    }
+    uint64_t k;
+    uint32_t inst;
+    split<POW2>(t, batch, log_batch, k, inst);
+    exec_insn(insn, prog_index, side, lo + k, batch, inst, v, fails, first);
+  }
+}
+
+// A run of narrow levels [k0, k1): each CTA takes kSegInstances instances through all of them,
+// a barrier between levels instead of a launch (a deep program, e.g. a hash's rounds, is a long
+// chain of levels a few instructions wide).  Instances never depend on one another, so the CTAs
+// run independently.  __syncthreads makes a level's global stores visible to the CTA.
+constexpr uint32_t kSegThreads = 1024;
+constexpr uint32_t kSegWidth = 64;      // levels of at most this many instructions are narrow
+constexpr uint32_t kSegInstances = 64;  // instances per CTA: <= 4096 items per level
+
+__global__ void __launch_bounds__(kSegThreads, 1)
+    eval_segment_kernel(const EfInsn* __restrict__ insn, const uint32_t* __restrict__ prog_index,
+                        const uint32_t* __restrict__ side, const uint64_t* __restrict__ level_start,
+                        uint32_t k0, uint32_t k1, uint32_t batch, uint64_t* __restrict__ v,
+                        uint32_t* __restrict__ fails, unsigned long long* __restrict__ first) {
+  const uint32_t i0 = blockIdx.x * kSegInstances;
+  const uint32_t g = batch - i0 < kSegInstances ? batch - i0 : kSegInstances;
+  for (uint32_t lv = k0; lv < k1; lv++) {
+    const uint64_t lo = level_start[lv];
+    const uint32_t total = (uint32_t)(level_start[lv + 1] - lo) * g;
+    for (uint32_t t = threadIdx.x; t < total; t += blockDim.x)
+      exec_insn(insn, prog_index, side, lo + t / g, batch, i0 + t % g, v, fails, first);
+    __syncthreads();
   }
 }
 
@@ -348,7 +395,10 @@ int binius_eval_form_create(const void* h_bytecode, size_t len, uint64_t n_value
   cudaGetDevice(&ef->device);
   const size_t m = prog.size() ? prog.size() : 1, ms = side.size() ? side.size() : 1;
   cudaError_t e;
-  if ((e = cudaMalloc(&ef->d_insn, sizeof(EfInsn) * m)) != cudaSuccess ||
+  if ((e = cudaMalloc(&ef->d_level_start, 8 * ef->level_start.size())) != cudaSuccess ||
+      (e = cudaMemcpy(ef->d_level_start, ef->level_start.data(), 8 * ef->level_start.size(),
+                      cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMalloc(&ef->d_insn, sizeof(EfInsn) * m)) != cudaSuccess ||
       (e = cudaMalloc(&ef->d_prog_index, 4 * m)) != cudaSuccess ||
       (e = cudaMalloc(&ef->d_side, 4 * ms)) != cudaSuccess ||
       (prog.size() &&
@@ -392,9 +442,24 @@ int binius_eval_form_evaluate(const binius_eval_form* ef, void* d_values, uint32
   uint32_t log_batch = 0;
   while ((1u << log_batch) < batch) log_batch++;
   const size_t n_levels = ef->level_start.empty() ? 0 : ef->level_start.size() - 1;
-  for (size_t k = 0; k < n_levels; k++) {
-    const uint64_t lo = ef->level_start[k], n = ef->level_start[k + 1] - lo;
-    if (n == 0) continue;
+  // Runs of narrow levels (at most kSegWidth instructions) go to the segment kernel; wider
+  // levels get a launch each.
+  const uint32_t seg_grid = (batch + kSegInstances - 1) / kSegInstances;
+  size_t k = 0;
+  while (k < n_levels) {
+    const uint64_t width = ef->level_start[k + 1] - ef->level_start[k];
+    if (width <= kSegWidth) {
+      size_t k1 = k + 1;
+      while (k1 < n_levels && ef->level_start[k1 + 1] - ef->level_start[k1] <= kSegWidth) k1++;
+      eval_segment_kernel<<<seg_grid, kSegThreads, 0, s>>>(
+          ef->d_insn, ef->d_prog_index, ef->d_side, ef->d_level_start, (uint32_t)k, (uint32_t)k1,
+          batch, v, d_fail_count, first);
+      BGPU_LAUNCH_CHECK("eval_segment_kernel");
+      count_launch();
+      k = k1;
+      continue;
+    }
+    const uint64_t lo = ef->level_start[k], n = width;
     const uint64_t threads = n * batch, blocks = (threads + 255) / 256;
     const unsigned grid = (unsigned)std::min<uint64_t>(blocks, 148ull * 64);
     if (pow2)
@@ -405,6 +470,7 @@ int binius_eval_form_evaluate(const binius_eval_form* ef, void* d_values, uint32
                                                      n, batch, log_batch, v, d_fail_count, first);
     BGPU_LAUNCH_CHECK("eval_level_kernel");
     count_launch();
+    k++;
   }
   return clear_error();
 }
@@ -414,6 +480,7 @@ int binius_eval_form_destroy(binius_eval_form* ef) {
   cudaFree(ef->d_insn);
   cudaFree(ef->d_prog_index);
   cudaFree(ef->d_side);
+  cudaFree(ef->d_level_start);
   delete ef;
   return BINIUS_OK;
 }

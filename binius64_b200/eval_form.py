@@ -187,6 +187,39 @@ def synthetic_program(circ, with_count: bool = False):
     return bb.finalize(), sc.next
 
 
+def chain_program(n_ops: int, seed: int = 0, first_free: int = 8) -> tuple[bytes, int]:
+    """(bytecode, n_values) of a deep program: an add-rotate-xor chain in the style of a hash's
+    rounds, each instruction writing a fresh register from the last few (registers 0..7 are its
+    inputs, fresh ones start at first_free, one or two per instruction), so the levels are a few
+    instructions wide and ~n_ops deep."""
+    rng = np.random.default_rng(seed)
+    bb = BytecodeBuilder()
+    live = list(range(8))
+    nxt = first_free
+    for _ in range(n_ops):
+        a, b, c = (live[-1 - int(rng.integers(0, 4))] for _ in range(3))
+        op = int(rng.integers(0, 5))
+        if op == 0:
+            bb.iadd_cout32(nxt, nxt + 1, a, b)
+            live += [nxt, nxt + 1]
+            nxt += 2
+            continue
+        if op == 1:
+            bb.rotr32(nxt, a, int(rng.integers(1, 32)))
+        elif op == 2:
+            bb.bxor(nxt, a, b)
+        elif op == 3:
+            bb.fax(nxt, a, b, c)
+        else:
+            bb.iadd_cout(nxt, nxt + 1, a, b)
+            live += [nxt, nxt + 1]
+            nxt += 2
+            continue
+        live.append(nxt)
+        nxt += 1
+    return bb.finalize(), nxt
+
+
 def synthetic_inputs(circ, n_values: int) -> np.ndarray:
     """The value vector before evaluation: constants, public and witness inputs set, internal
     words and scratch zero."""

@@ -2,7 +2,8 @@
 opcode (registers overwritten and read again, so the level schedule must keep the program's
 order), with their assertion counts and first failures, over batches of instances; the program
 that recomputes a synthetic circuit's witness, for instances with different inputs, followed by
-proofs of the generated witnesses identical to the oracle's; and the register-major transpose."""
+proofs of the generated witnesses identical to the oracle's; deep programs (runs of narrow levels
+in one CTA), alone and after wide levels; and the register-major transpose."""
 import numpy as np
 import pytest
 
@@ -122,3 +123,40 @@ def test_synthetic_witness_generation_then_prove(log_words, n_and, n_mul, seed, 
             assert proof == orc.prove(ref_vals[:1 << log_words], 1, prep.and_csr, prep.mul_csr, 1)
         finally:
             orc.set_threads(1)
+
+
+@pytest.mark.parametrize("n_ops,batch", [(3000, 1), (3000, 32), (3000, 100)])
+def test_deep_chain_vs_oracle(n_ops, batch):
+    """A deep program (levels a few instructions wide): runs of narrow levels in one CTA."""
+    code, n_values = ef.chain_program(n_ops, seed=n_ops + batch)
+    prog = ef.EvalForm(code, n_values)
+    assert prog.n_levels > n_ops // 4
+    rng = np.random.default_rng(batch)
+    inst = np.zeros((batch, n_values), dtype=np.uint64)
+    inst[:, :8] = rng.integers(0, 2**64, size=(batch, 8), dtype=np.uint64, endpoint=False)
+    d = torch.from_numpy(np.ascontiguousarray(inst.T).view(np.int64)).cuda().reshape(-1)
+    prog.evaluate(d, batch)
+    got = d.cpu().numpy().view(np.uint64).reshape(n_values, batch).T
+    for i in (0, batch // 2, batch - 1):
+        rc, ref, _, _ = orc.eval_form_run(code, inst[i])
+        assert rc == 0 and np.array_equal(got[i], ref), f"instance {i}"
+
+
+def test_wide_then_deep_program():
+    """Wide levels (the synthetic circuit's) and a deep chain after them in one program."""
+    circ = csm.synthetic_circuit(10, 300, 5, seed=9)
+    code, n_values = ef.synthetic_program(circ)
+    chain, total = ef.chain_program(500, seed=3, first_free=n_values)
+    full = code + chain
+    prog = ef.EvalForm(full, total)
+    v0 = np.zeros(total, dtype=np.uint64)
+    v0[:n_values] = ef.synthetic_inputs(circ, n_values)
+    batch = 3
+    inst = np.repeat(v0[None, :], batch, axis=0)
+    d = torch.from_numpy(np.ascontiguousarray(inst.T).view(np.int64)).cuda().reshape(-1)
+    prog.evaluate(d, batch)
+    got = d.cpu().numpy().view(np.uint64).reshape(total, batch).T
+    rc, ref, _, _ = orc.eval_form_run(full, v0)
+    assert rc == 0
+    assert np.array_equal(got[0], ref) and np.array_equal(got[2], ref)
+    assert np.array_equal(ref[:1 << 10], circ.witness)
