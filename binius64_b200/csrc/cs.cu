@@ -144,35 +144,131 @@ int upload(const HostOperands& h, DevOperands& d) {
 
 bool is_pow2(uint32_t v) { return v && !(v & (v - 1)); }
 
-// Counting sort of all operand terms by shift key (see ShiftTerms).
-int build_shift_terms(const HostOperands& and_h, const HostOperands& mul_h, ShiftTerms& d) {
-  static const uint8_t and_class[3] = {0, 1, 2};
-  static const uint8_t mul_class[4] = {3, 4, 6, 5};  // CSR slots (a, b, hi, lo)
-  std::vector<uint32_t> count(kShiftKeys + 1, 0);
-  auto key_of = [](uint32_t packed, uint32_t cls) {
-    return (uint32_t)(((packed >> 8) * 64 + (packed & 255)) * 8 + cls);
-  };
-  auto visit = [&](const HostOperands& h, const uint8_t* cls, auto&& fn) {
-    const uint32_t groups = (uint32_t)(h.offsets.size() - 1);
-    for (uint32_t g = 0; g < groups; g++)
-      for (uint32_t t = h.offsets[g]; t < h.offsets[g + 1]; t++)
-        fn(h.terms[t], g / h.k, key_of(h.terms[t].y, cls[g % h.k]));
-  };
-  visit(and_h, and_class, [&](uint2, uint32_t, uint32_t k) { count[k + 1]++; });
-  visit(mul_h, mul_class, [&](uint2, uint32_t, uint32_t k) { count[k + 1]++; });
-  for (uint32_t k = 0; k < kShiftKeys; k++) count[k + 1] += count[k];
-  const uint64_t n = count[kShiftKeys];
-  std::vector<uint32_t> vi(n ? n : 1), cc(n ? n : 1);
-  std::vector<uint16_t> key(n ? n : 1);
-  auto place = [&](uint2 term, uint32_t c, uint32_t k) {
-    const uint32_t pos = count[k]++;
-    vi[pos] = term.x;
+// The shift term table (ShiftTerms) built on the device: a counting sort of all operand terms by
+// shift key.  Groups (constraint, CSR slot) of both operations form one index space (AND groups
+// first); each CTA takes a contiguous range of it, counts its keys in shared memory, and -- after
+// one scan of the global counts -- reserves a range per key with one atomic and places its terms
+// there.  Terms of one key land in CTA order, in no fixed order within a CTA: every quantity the
+// shift reduction takes from the table is a XOR sum over a key's terms.
+constexpr uint32_t kSortThreads = 512;
+constexpr uint32_t kSortBlocks = 148 * 2;
+
+// Class of CSR slot `slot`: AND (a, b, c) -> 0, 1, 2; MUL slots (a, b, hi, lo) -> 3, 4, 6, 5.
+__device__ __forceinline__ uint32_t slot_class(uint32_t k, uint32_t slot) {
+  return k == 3 ? slot : (slot == 0 ? 3u : slot == 1 ? 4u : slot == 2 ? 6u : 5u);
+}
+
+template <class Fn>
+__device__ __forceinline__ void for_each_term(const DevOperands& A, const DevOperands& M,
+                                              uint64_t g0, uint64_t g1, Fn&& fn) {
+  const uint64_t ga = (uint64_t)A.n_constraints * A.k;
+  for (uint64_t g = g0 + threadIdx.x; g < g1; g += blockDim.x) {
+    const DevOperands& op = g < ga ? A : M;
+    const uint64_t gg = g < ga ? g : g - ga;
+    const uint32_t slot = (uint32_t)(gg % op.k), c = (uint32_t)(gg / op.k);
+    const uint32_t cls = slot_class(op.k, slot);
+    for (uint32_t t = op.offsets[gg]; t < op.offsets[gg + 1]; t++) {
+      const uint2 term = op.terms[t];
+      fn(term.x, c, ((term.y >> 8) * 64 + (term.y & 255)) * 8 + cls);
+    }
+  }
+}
+
+template <bool SCATTER>
+__global__ void __launch_bounds__(kSortThreads)
+    shift_terms_kernel(DevOperands A, DevOperands M, uint32_t* __restrict__ counts,
+                       uint32_t* __restrict__ vi, uint32_t* __restrict__ cc,
+                       uint16_t* __restrict__ keys) {
+  __shared__ uint32_t hist[kShiftKeys], base[kShiftKeys];
+  const uint64_t G = (uint64_t)A.n_constraints * A.k + (uint64_t)M.n_constraints * M.k;
+  const uint64_t per = (G + gridDim.x - 1) / gridDim.x;
+  const uint64_t g0 = blockIdx.x * per, g1 = g0 + per < G ? g0 + per : G;
+  for (uint32_t k = threadIdx.x; k < kShiftKeys; k += blockDim.x) hist[k] = 0;
+  __syncthreads();
+  if (g0 < g1) for_each_term(A, M, g0, g1, [&](uint32_t, uint32_t, uint32_t key) {
+    atomicAdd(&hist[key], 1u);
+  });
+  __syncthreads();
+  if (!SCATTER) {
+    for (uint32_t k = threadIdx.x; k < kShiftKeys; k += blockDim.x)
+      if (hist[k]) atomicAdd(&counts[k], hist[k]);
+    return;
+  }
+  // counts holds each key's next free position (an exclusive scan of the key totals)
+  for (uint32_t k = threadIdx.x; k < kShiftKeys; k += blockDim.x) {
+    base[k] = hist[k] ? atomicAdd(&counts[k], hist[k]) : 0u;
+    hist[k] = 0;
+  }
+  __syncthreads();
+  if (g0 < g1) for_each_term(A, M, g0, g1, [&](uint32_t v, uint32_t c, uint32_t key) {
+    const uint32_t pos = base[key] + atomicAdd(&hist[key], 1u);
+    vi[pos] = v;
     cc[pos] = c;
-    key[pos] = (uint16_t)k;
-  };
-  visit(and_h, and_class, place);
-  visit(mul_h, mul_class, place);
-  return upload_shift_terms(vi, cc, key, n, d);
+    keys[pos] = (uint16_t)key;
+  });
+}
+
+// counts[k] <- sum of counts[0..k) over the kShiftKeys keys, in one CTA of 1024 threads.
+__global__ void __launch_bounds__(1024) exclusive_scan_keys_kernel(uint32_t* counts) {
+  __shared__ uint32_t part[1024];
+  constexpr uint32_t per = kShiftKeys / 1024;
+  uint32_t v[per], sum = 0;
+  for (uint32_t i = 0; i < per; i++) {
+    v[i] = counts[threadIdx.x * per + i];
+    sum += v[i];
+  }
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  for (uint32_t off = 1; off < 1024; off <<= 1) {  // inclusive scan of the per-thread sums
+    const uint32_t x = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
+    __syncthreads();
+    part[threadIdx.x] += x;
+    __syncthreads();
+  }
+  uint32_t run = part[threadIdx.x] - sum;
+  for (uint32_t i = 0; i < per; i++) {
+    counts[threadIdx.x * per + i] = run;
+    run += v[i];
+  }
+}
+
+int build_shift_terms(const DevOperands& A, const DevOperands& M, ShiftTerms& d) {
+  const uint64_t n = A.n_terms + M.n_terms;
+  BGPU_ARG(n < 0xffffffffull, "too many operand terms");
+  const size_t m = n ? n : 1;
+  ShiftTerms t;
+  t.n = n;
+  uint32_t* counts = nullptr;
+  cudaStream_t s = nullptr;  // its own stream: set-up does not wait for other work on the device
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaMalloc(&t.vi, 4 * m)) != cudaSuccess || (e = cudaMalloc(&t.c, 4 * m)) != cudaSuccess ||
+      (e = cudaMalloc(&t.key, 2 * m)) != cudaSuccess ||
+      (e = cudaMalloc(&counts, 4 * kShiftKeys)) != cudaSuccess ||
+      (e = cudaMemsetAsync(counts, 0, 4 * kShiftKeys, s)) != cudaSuccess) {
+    cudaFree(t.vi);
+    cudaFree(t.c);
+    cudaFree(t.key);
+    cudaFree(counts);
+    if (s) cudaStreamDestroy(s);
+    return cuda_error(e, "shift term table");
+  }
+  shift_terms_kernel<false><<<kSortBlocks, kSortThreads, 0, s>>>(A, M, counts, t.vi, t.c, t.key);
+  exclusive_scan_keys_kernel<<<1, 1024, 0, s>>>(counts);
+  shift_terms_kernel<true><<<kSortBlocks, kSortThreads, 0, s>>>(A, M, counts, t.vi, t.c, t.key);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  cudaFree(counts);
+  if (e != cudaSuccess) {
+    cudaFree(t.vi);
+    cudaFree(t.c);
+    cudaFree(t.key);
+    return cuda_error(e, "shift term sort");
+  }
+  count_launch(3);
+  d = t;
+  return BINIUS_OK;
 }
 
 }  // namespace
@@ -261,7 +357,7 @@ int binius_cs_from_bytes(int device, const void* h_bytes, size_t len, binius_cs*
     cudaSetDevice(device);
     rc = upload(cs->h_and, cs->and_ops);
     if (!rc) rc = upload(cs->h_mul, cs->mul_ops);
-    if (!rc) rc = build_shift_terms(cs->h_and, cs->h_mul, cs->shift_terms);
+    if (!rc) rc = build_shift_terms(cs->and_ops, cs->mul_ops, cs->shift_terms);
     cudaSetDevice(prev);
   }
   if (rc) {
