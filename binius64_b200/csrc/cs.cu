@@ -189,23 +189,23 @@ __global__ void __launch_bounds__(kSortThreads)
     atomicAdd(&hist[key], 1u);
   });
   __syncthreads();
-  if (!SCATTER) {
+  if constexpr (!SCATTER) {
     for (uint32_t k = threadIdx.x; k < kShiftKeys; k += blockDim.x)
       if (hist[k]) atomicAdd(&counts[k], hist[k]);
-    return;
+  } else {
+    // counts holds each key's next free position (an exclusive scan of the key totals)
+    for (uint32_t k = threadIdx.x; k < kShiftKeys; k += blockDim.x) {
+      base[k] = hist[k] ? atomicAdd(&counts[k], hist[k]) : 0u;
+      hist[k] = 0;
+    }
+    __syncthreads();
+    if (g0 < g1) for_each_term(A, M, g0, g1, [&](uint32_t v, uint32_t c, uint32_t key) {
+      const uint32_t pos = base[key] + atomicAdd(&hist[key], 1u);
+      vi[pos] = v;
+      cc[pos] = c;
+      keys[pos] = (uint16_t)key;
+    });
   }
-  // counts holds each key's next free position (an exclusive scan of the key totals)
-  for (uint32_t k = threadIdx.x; k < kShiftKeys; k += blockDim.x) {
-    base[k] = hist[k] ? atomicAdd(&counts[k], hist[k]) : 0u;
-    hist[k] = 0;
-  }
-  __syncthreads();
-  if (g0 < g1) for_each_term(A, M, g0, g1, [&](uint32_t v, uint32_t c, uint32_t key) {
-    const uint32_t pos = base[key] + atomicAdd(&hist[key], 1u);
-    vi[pos] = v;
-    cc[pos] = c;
-    keys[pos] = (uint16_t)key;
-  });
 }
 
 // counts[k] <- sum of counts[0..k) over the kShiftKeys keys, in one CTA of 1024 threads.
