@@ -475,7 +475,10 @@ static __device__ __noinline__ uint4 v4_permute_lane(uint4 x, uint32_t e) {
 // so spreading them over many SMs leaves each chain a scheduler of its own.
 constexpr uint32_t kLaneLeafFuse = 4;  // 2^4 leaves (64 lanes) per CTA
 constexpr uint32_t kLaneNodeFuse = 4;  // 2^4 inputs per CTA
-constexpr uint32_t kLaneMaxLog = 12;   // trees of up to 2^12 leaves take the four-lane kernels
+// Trees of up to 2^12 leaves take the four-lane kernels.  Measured: 2^14 leaves on them took
+// 9.7 ms against 8.4 ms on the one-thread kernels (four inversions per sbox cost more than the
+// SMs the one-thread kernels leave idle).
+constexpr uint32_t kLaneMaxLog = 12;
 
 __global__ void __launch_bounds__(256)
     vision4_leaves_lanes_kernel(const uint4* __restrict__ img, const uint4* __restrict__ elems,

@@ -42,7 +42,7 @@ def test_permutation_known_answers_and_zeros():
 
 
 @pytest.mark.parametrize("log_leaves,log_batch", [
-    (0, 0), (0, 4), (1, 0), (3, 1), (7, 4), (8, 2), (9, 6), (10, 4), (12, 0), (14, 4),
+    (0, 0), (0, 4), (1, 0), (3, 1), (7, 4), (8, 2), (9, 6), (10, 4), (12, 0), (14, 4), (15, 0),
 ])
 def test_vision4_merkle_commit_vs_oracle(log_leaves, log_batch):
     r = np.random.default_rng(700 + 8 * log_leaves + log_batch)
