@@ -585,7 +585,8 @@ int vision4_merkle_commit(const void* d_elems, uint32_t log_leaves, uint32_t log
   uint4* nodes = static_cast<uint4*>(d_nodes);
   if (L <= kLaneMaxLog)
     return vision4_commit_lanes(img, static_cast<const uint4*>(d_elems), L, log_batch, nodes, s);
-  const uint32_t fused = L < kV4LeafFuse ? L : kV4LeafFuse;
+  // at least 2^8 CTAs: mid-size trees spread over every SM in smaller CTAs
+  const uint32_t fused = L - 8 < kV4LeafFuse ? L - 8 : kV4LeafFuse;
   const uint64_t grid = 1ull << (L - fused);
   BGPU_ARG(grid <= 0x7fffffffull, "too many leaves");
   vision4_leaves_kernel<<<(unsigned)grid, 1u << fused, kV4Smem, s>>>(
