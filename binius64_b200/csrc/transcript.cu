@@ -1,5 +1,8 @@
 // C ABI of the host-side Fiat-Shamir transcript (transcript.h), and the host side of device
 // transcript stretches (dev_transcript.cuh).
+#include <stdio.h>
+#include <stdlib.h>
+
 #include "dev_transcript.cuh"
 #include "internal.h"
 #include "transcript.h"
@@ -113,11 +116,20 @@ uint32_t binius_transcript_sample_bits(binius_transcript* t, uint32_t bits) {
 
 size_t binius_transcript_len(const binius_transcript* t) { return t ? t->t.tape().size() : 0; }
 
+// ProverTranscript::finalize (verifier/transcript/src/transcript.rs:245-284), including its proof
+// dump: with BINIUS_DUMP_PROOF set, the proof bytes are also written to the file it names.
 int binius_transcript_finalize(const binius_transcript* t, void* h_out, size_t cap, size_t* len) {
   BGPU_ARG(t != nullptr && len != nullptr, "NULL argument");
   *len = t->t.tape().size();
   BGPU_ARG(cap >= *len && (h_out != nullptr || *len == 0), "proof buffer too small");
   if (*len) memcpy(h_out, t->t.tape().data(), *len);
+  if (const char* path = getenv("BINIUS_DUMP_PROOF")) {
+    FILE* f = fopen(path, "wb");
+    BGPU_ARG(f != nullptr, "BINIUS_DUMP_PROOF: cannot create the proof dump file");
+    const size_t wrote = *len ? fwrite(t->t.tape().data(), 1, *len, f) : 0;
+    const int closed = fclose(f);
+    BGPU_ARG(wrote == *len && closed == 0, "BINIUS_DUMP_PROOF: cannot write the proof dump file");
+  }
   return clear_error();
 }
 

@@ -153,7 +153,9 @@ int binius_fri_commit_interleaved(const binius_ntt* ntt, const void* d_msg, uint
  * Replaces: ProverTranscript (verifier/transcript/src/transcript.rs:204-327), HasherChallenger
  * (verifier/transcript/src/fiat_shamir/hasher_challenger.rs:14-200), sample_bits_reader
  * (fiat_shamir/sampling.rs:34-50).  Host-side state; the proof is the tape of message() and
- * decommitment() bytes (ProverTranscript::finalize).
+ * decommitment() bytes (ProverTranscript::finalize).  As the reference's finalize does, with the
+ * environment variable BINIUS_DUMP_PROOF set binius_transcript_finalize also writes the proof
+ * bytes to the file it names (BINIUS_E_ARG if that fails).
  * ------------------------------------------------------------------------------------------ */
 typedef struct binius_transcript binius_transcript;
 
