@@ -292,19 +292,26 @@ constexpr uint32_t kSegThreads = 1024;
 constexpr uint32_t kSegWidth = 64;      // levels of at most this many instructions are narrow
 constexpr uint32_t kSegInstances = 64;  // instances per CTA: <= 4096 items per level
 
-__global__ void __launch_bounds__(kSegThreads, 1)
+// WARP: one warp per instance (small batches), the levels separated by __syncwarp, which orders
+// the warp's global stores before its next loads at a fraction of a CTA barrier's cost.
+template <bool WARP>
+__global__ void __launch_bounds__(WARP ? 32 : kSegThreads, 1)
     eval_segment_kernel(const EfInsn* __restrict__ insn, const uint32_t* __restrict__ prog_index,
                         const uint32_t* __restrict__ side, const uint64_t* __restrict__ level_start,
                         uint32_t k0, uint32_t k1, uint32_t batch, uint64_t* __restrict__ v,
                         uint32_t* __restrict__ fails, unsigned long long* __restrict__ first) {
-  const uint32_t i0 = blockIdx.x * kSegInstances;
-  const uint32_t g = batch - i0 < kSegInstances ? batch - i0 : kSegInstances;
+  constexpr uint32_t per = WARP ? 1 : kSegInstances;
+  const uint32_t i0 = blockIdx.x * per;
+  const uint32_t g = batch - i0 < per ? batch - i0 : per;
   for (uint32_t lv = k0; lv < k1; lv++) {
     const uint64_t lo = level_start[lv];
     const uint32_t total = (uint32_t)(level_start[lv + 1] - lo) * g;
     for (uint32_t t = threadIdx.x; t < total; t += blockDim.x)
       exec_insn(insn, prog_index, side, lo + t / g, batch, i0 + t % g, v, fails, first);
-    __syncthreads();
+    if (WARP)
+      __syncwarp();
+    else
+      __syncthreads();
   }
 }
 
@@ -444,16 +451,23 @@ int binius_eval_form_evaluate(const binius_eval_form* ef, void* d_values, uint32
   const size_t n_levels = ef->level_start.empty() ? 0 : ef->level_start.size() - 1;
   // Runs of narrow levels (at most kSegWidth instructions) go to the segment kernel; wider
   // levels get a launch each.
-  const uint32_t seg_grid = (batch + kSegInstances - 1) / kSegInstances;
+  // up to 32 instances: a warp each (on separate SMs); more: CTAs of 64 instances
+  const bool seg_warp = batch <= 32;
+  const uint32_t seg_grid = seg_warp ? batch : (batch + kSegInstances - 1) / kSegInstances;
   size_t k = 0;
   while (k < n_levels) {
     const uint64_t width = ef->level_start[k + 1] - ef->level_start[k];
     if (width <= kSegWidth) {
       size_t k1 = k + 1;
       while (k1 < n_levels && ef->level_start[k1 + 1] - ef->level_start[k1] <= kSegWidth) k1++;
-      eval_segment_kernel<<<seg_grid, kSegThreads, 0, s>>>(
-          ef->d_insn, ef->d_prog_index, ef->d_side, ef->d_level_start, (uint32_t)k, (uint32_t)k1,
-          batch, v, d_fail_count, first);
+      if (seg_warp)
+        eval_segment_kernel<true><<<seg_grid, 32, 0, s>>>(
+            ef->d_insn, ef->d_prog_index, ef->d_side, ef->d_level_start, (uint32_t)k,
+            (uint32_t)k1, batch, v, d_fail_count, first);
+      else
+        eval_segment_kernel<false><<<seg_grid, kSegThreads, 0, s>>>(
+            ef->d_insn, ef->d_prog_index, ef->d_side, ef->d_level_start, (uint32_t)k,
+            (uint32_t)k1, batch, v, d_fail_count, first);
       BGPU_LAUNCH_CHECK("eval_segment_kernel");
       count_launch();
       k = k1;
