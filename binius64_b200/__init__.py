@@ -524,11 +524,13 @@ class DeviceConstraintSystem:
             self._h = None
 
 
-def _sized_bytes(fn, *args) -> bytes:
-    """Calls a byte-writing entry point once to learn the length, then with a buffer that fits."""
+def _sized_bytes(fn, *args, guess: int = 0) -> bytes:
+    """Calls a byte-writing entry point with a buffer of `guess` bytes (an upper bound spares the
+    second call), or once to learn the length and again with a buffer that fits."""
     n = ctypes.c_size_t(0)
-    if fn(*args, None, 0, ctypes.byref(n)) == 0:
-        return b""
+    buf = ctypes.create_string_buffer(guess) if guess else None
+    if fn(*args, buf, guess, ctypes.byref(n)) == 0:
+        return buf.raw[:n.value] if buf is not None else b""
     buf = ctypes.create_string_buffer(max(n.value, 1))
     check(fn(*args, buf, len(buf), ctypes.byref(n)))
     return buf.raw[:n.value]
@@ -537,7 +539,12 @@ def _sized_bytes(fn, *args) -> bytes:
 def key_collection_from_cs_bytes(cs_bytes: bytes) -> bytes:
     """build_key_collection + KeyCollection::serialize (prover/prover/src/protocols/shift/
     key_collection.rs:238-312, 381-398) for a v2 constraint system, on the host alone."""
-    return _sized_bytes(lib().binius_key_collection_from_cs_bytes, cs_bytes, len(cs_bytes))
+    # bound: a term takes >= 9 bytes of the constraint system and <= 16 of the collection (a key
+    # of 11 and an index of 5); 8 bytes of key range per committed word (the u32 at byte 28)
+    words = int.from_bytes(cs_bytes[28:32], "little") if len(cs_bytes) >= 32 else 0
+    guess = 64 + 16 * (len(cs_bytes) // 9) + 8 * words
+    return _sized_bytes(lib().binius_key_collection_from_cs_bytes, cs_bytes, len(cs_bytes),
+                        guess=guess)
 
 
 def and_reduction_prove(cs: DeviceConstraintSystem, witness_words, transcript: ProverTranscript,
