@@ -17,7 +17,9 @@
 // a collection built for another constraint system is an argument error, not a wrong proof.
 #include <string.h>
 
+#include <algorithm>
 #include <memory>
+#include <thread>
 #include <vector>
 
 #include "cs.h"
@@ -41,93 +43,177 @@ inline uint64_t record(uint32_t constraint, uint32_t operand, uint32_t kid) {
   return (uint64_t)constraint | ((uint64_t)operand << 32) | ((uint64_t)kid << 34);
 }
 
-// Calls fn(word, record) for every operand term in the reference's traversal order.
-template <class Fn>
-void traverse(const binius_cs& cs, Fn&& fn) {
-  static const uint32_t mul_slot[4] = {0, 1, 3, 2};  // operands (a, b, lo, hi) in CSR slots
-  auto visit = [&](const HostOperands& h, uint32_t operation, uint32_t operand, uint32_t slot) {
-    const uint32_t n = (uint32_t)((h.offsets.size() - 1) / h.k);
-    for (uint32_t c = 0; c < n; c++) {
-      const uint32_t g = c * h.k + slot;
-      for (uint32_t t = h.offsets[g]; t < h.offsets[g + 1]; t++) {
-        const uint32_t packed = h.terms[t].y;  // variant << 8 | amount
-        const uint32_t kid = (operation << 9) | ((packed >> 8) << 6) | (packed & 255);
-        fn(h.terms[t].x, record(c, operand, kid));
+// The traversal as groups (pass, constraint): the passes are AND operands a, b, c then MUL
+// operands a, b, lo, hi, each over the constraints in order; group gi of the flat sequence.
+struct Passes {
+  const HostOperands* h[7];
+  uint32_t operation[7], operand[7], slot[7];
+  uint64_t first[8];  // first[p] = flat index of pass p's first group
+  explicit Passes(const binius_cs& cs) {
+    static const uint32_t mul_slot[4] = {0, 1, 3, 2};  // operands (a, b, lo, hi) in CSR slots
+    first[0] = 0;
+    for (uint32_t p = 0; p < 7; p++) {
+      const bool is_and = p < 3;
+      h[p] = is_and ? &cs.h_and : &cs.h_mul;
+      operation[p] = is_and ? 0 : 1;
+      operand[p] = is_and ? p : p - 3;
+      slot[p] = is_and ? p : mul_slot[p - 3];
+      first[p + 1] = first[p] + (h[p]->offsets.size() - 1) / h[p]->k;
+    }
+  }
+  uint64_t n_groups() const { return first[7]; }
+  // Calls fn(word, record) for every term of groups [g0, g1), in traversal order.
+  template <class Fn>
+  void visit(uint64_t g0, uint64_t g1, Fn&& fn) const {
+    for (uint32_t p = 0; p < 7; p++) {
+      const uint64_t lo = g0 > first[p] ? g0 : first[p], hi = g1 < first[p + 1] ? g1 : first[p + 1];
+      const HostOperands& H = *h[p];
+      for (uint64_t gi = lo; gi < hi; gi++) {
+        const uint32_t c = (uint32_t)(gi - first[p]), g = c * H.k + slot[p];
+        for (uint32_t t = H.offsets[g]; t < H.offsets[g + 1]; t++) {
+          const uint32_t packed = H.terms[t].y;  // variant << 8 | amount
+          const uint32_t kid = (operation[p] << 9) | ((packed >> 8) << 6) | (packed & 255);
+          fn(H.terms[t].x, record(c, operand[p], kid));
+        }
       }
     }
-  };
-  for (uint32_t a = 0; a < 3; a++) visit(cs.h_and, 0, a, a);
-  for (uint32_t a = 0; a < 4; a++) visit(cs.h_mul, 1, a, mul_slot[a]);
+  }
+};
+
+template <class Fn>
+void parallel(uint32_t T, Fn&& fn) {
+  std::vector<std::thread> th;
+  for (uint32_t j = 1; j < T; j++) th.emplace_back(fn, j);
+  fn(0u);
+  for (auto& x : th) x.join();
 }
 
+// The collection's bytes.  Threads split the traversal (a stable scatter of the records by word
+// through per-thread counts) and then the words (keys numbered per word; a word's constraint
+// indices start at its first record, so only the key ranges need the threads' key counts).
 int key_collection_bytes(const binius_cs& cs, std::vector<uint8_t>& out) {
   const uint32_t n_words = cs.committed_total_len;
   const size_t n = cs.h_and.terms.size() + cs.h_mul.terms.size();
-  // stable group by word: counts, then a scatter of records in traversal order
+  const Passes P(cs);
+  uint32_t T = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  while (T > 1 && (uint64_t)T * n_words > (1ull << 27)) T--;  // per-thread word counts
+  if (n < (1u << 16)) T = 1;
+  // stable group by word: per-thread counts over contiguous group ranges, then offsets
+  const uint64_t NG = P.n_groups();
+  std::vector<uint64_t> gcut(T + 1);
+  for (uint32_t j = 0; j <= T; j++) gcut[j] = NG * j / T;
+  std::vector<std::vector<uint32_t>> cnt(T, std::vector<uint32_t>(n_words, 0));
+  parallel(T, [&](uint32_t j) {
+    uint32_t* c = cnt[j].data();
+    P.visit(gcut[j], gcut[j + 1], [&](uint32_t w, uint64_t) { c[w]++; });
+  });
   std::vector<uint32_t> start((size_t)n_words + 1, 0);
-  for (const HostOperands* h : {&cs.h_and, &cs.h_mul})
-    for (const uint2& t : h->terms) start[t.x + 1]++;
+  parallel(T, [&](uint32_t j) {  // per word: total, kept in start[w + 1] for the scan below
+    const uint32_t w0 = (uint32_t)((uint64_t)n_words * j / T), w1 = (uint32_t)((uint64_t)n_words * (j + 1) / T);
+    for (uint32_t w = w0; w < w1; w++) {
+      uint32_t s = 0;
+      for (uint32_t q = 0; q < T; q++) s += cnt[q][w];
+      start[w + 1] = s;
+    }
+  });
   for (uint32_t w = 0; w < n_words; w++) start[w + 1] += start[w];
+  parallel(T, [&](uint32_t j) {  // thread q's first slot of word w: start[w] + counts of q' < q
+    const uint32_t w0 = (uint32_t)((uint64_t)n_words * j / T), w1 = (uint32_t)((uint64_t)n_words * (j + 1) / T);
+    for (uint32_t w = w0; w < w1; w++) {
+      uint32_t run = start[w];
+      for (uint32_t q = 0; q < T; q++) {
+        const uint32_t c = cnt[q][w];
+        cnt[q][w] = run;
+        run += c;
+      }
+    }
+  });
   std::unique_ptr<uint64_t[]> rec(new uint64_t[n ? n : 1]);
-  {
-    std::vector<uint32_t> fill(start.begin(), start.end() - 1);
-    traverse(cs, [&](uint32_t word, uint64_t r) { rec[fill[word]++] = r; });
+  parallel(T, [&](uint32_t j) {
+    uint32_t* fill = cnt[j].data();
+    P.visit(gcut[j], gcut[j + 1], [&](uint32_t w, uint64_t r) { rec[fill[w]++] = r; });
+  });
+  cnt.clear();
+  cnt.shrink_to_fit();
+  // per word range: keys in first-appearance order, constraint indices bucketed by (key, operand)
+  std::vector<uint32_t> wcut(T + 1);
+  for (uint32_t j = 0, w = 0; j <= T; j++) {  // balance the words by records
+    const uint64_t target = (uint64_t)n * j / T;
+    while (w < n_words && start[w] < target) w++;
+    wcut[j] = j == T ? n_words : w;
   }
-  std::unique_ptr<uint8_t[]> keys_b(new uint8_t[11 * (n ? n : 1)]);
   std::unique_ptr<uint8_t[]> cis_b(new uint8_t[5 * (n ? n : 1)]);
-  std::unique_ptr<uint8_t[]> ranges_b(new uint8_t[8ull * n_words + 1]);
-  uint8_t *kp = keys_b.get(), *cp = cis_b.get(), *rp = ranges_b.get();
-  std::vector<int32_t> local(kKidCount, -1);
-  std::vector<uint32_t> word_kids, key_fill;
-  std::vector<uint64_t> bucket;
-  uint32_t n_keys = 0, n_cis = 0;
-  for (uint32_t w = 0; w < n_words; w++) {
-    const uint64_t* r = rec.get() + start[w];
-    const uint32_t m = start[w + 1] - start[w];
-    word_kids.clear();
-    for (uint32_t q = 0; q < m; q++) {  // keys of the word in first-appearance order
-      const uint32_t kid = (uint32_t)(r[q] >> 34);
-      if (local[kid] < 0) {
-        local[kid] = (int32_t)word_kids.size();
-        word_kids.push_back(kid);
+  std::vector<std::vector<uint8_t>> keys_j(T);
+  std::vector<std::vector<uint32_t>> nk_j(T);  // keys per word of the range
+  parallel(T, [&](uint32_t j) {
+    std::vector<int32_t> local(kKidCount, -1);
+    std::vector<uint32_t> word_kids, key_fill;
+    std::vector<uint64_t> bucket;
+    std::vector<uint8_t>& kb = keys_j[j];
+    std::vector<uint32_t>& nkw = nk_j[j];
+    nkw.reserve(wcut[j + 1] - wcut[j]);
+    kb.reserve(11ull * (start[wcut[j + 1]] - start[wcut[j]]) / 2);
+    for (uint32_t w = wcut[j]; w < wcut[j + 1]; w++) {
+      const uint64_t* r = rec.get() + start[w];
+      const uint32_t m = start[w + 1] - start[w];
+      word_kids.clear();
+      for (uint32_t q = 0; q < m; q++) {
+        const uint32_t kid = (uint32_t)(r[q] >> 34);
+        if (local[kid] < 0) {
+          local[kid] = (int32_t)word_kids.size();
+          word_kids.push_back(kid);
+        }
       }
-    }
-    const uint32_t nk = (uint32_t)word_kids.size();
-    // bucket the word's records by (key, operand), stably
-    key_fill.assign(4 * nk + 1, 0);
-    for (uint32_t q = 0; q < m; q++)
-      key_fill[4 * local[r[q] >> 34] + ((r[q] >> 32) & 3) + 1]++;
-    for (uint32_t x = 0; x < 4 * nk; x++) key_fill[x + 1] += key_fill[x];
-    bucket.resize(m);
-    for (uint32_t q = 0; q < m; q++) bucket[key_fill[4 * local[r[q] >> 34] + ((r[q] >> 32) & 3)]++] = r[q];
-    rp = put_u32(rp, n_keys);
-    rp = put_u32(rp, n_keys + nk);
-    for (uint32_t k = 0, x = 0; k < nk; k++) {
-      const uint32_t kid = word_kids[k], end = key_fill[4 * k + 3];  // bucket ends after the fill
-      *kp++ = (uint8_t)(kid >> 9);  // Operation: BitwiseAnd = 0, IntegerMul = 1
-      *kp++ = (uint8_t)(kid & 255);
-      *kp++ = (uint8_t)((kid >> 8) & 1);
-      kp = put_u32(kp, n_cis + x);
-      for (; x < end; x++) {
-        *cp++ = (uint8_t)((bucket[x] >> 32) & 3);
-        cp = put_u32(cp, (uint32_t)bucket[x]);
+      const uint32_t nk = (uint32_t)word_kids.size();
+      key_fill.assign(4 * nk + 1, 0);
+      for (uint32_t q = 0; q < m; q++)
+        key_fill[4 * local[r[q] >> 34] + ((r[q] >> 32) & 3) + 1]++;
+      for (uint32_t x = 0; x < 4 * nk; x++) key_fill[x + 1] += key_fill[x];
+      bucket.resize(m);
+      for (uint32_t q = 0; q < m; q++)
+        bucket[key_fill[4 * local[r[q] >> 34] + ((r[q] >> 32) & 3)]++] = r[q];
+      uint8_t* cp = cis_b.get() + 5ull * start[w];
+      for (uint32_t k = 0, x = 0; k < nk; k++) {
+        const uint32_t kid = word_kids[k], end = key_fill[4 * k + 3];  // bucket ends after the fill
+        uint8_t key[11];
+        key[0] = (uint8_t)(kid >> 9);  // Operation: BitwiseAnd = 0, IntegerMul = 1
+        key[1] = (uint8_t)(kid & 255);
+        key[2] = (uint8_t)((kid >> 8) & 1);
+        put_u32(key + 3, start[w] + x);
+        for (; x < end; x++) {
+          *cp++ = (uint8_t)((bucket[x] >> 32) & 3);
+          cp = put_u32(cp, (uint32_t)bucket[x]);
+        }
+        put_u32(key + 7, start[w] + x);
+        kb.insert(kb.end(), key, key + 11);
       }
-      kp = put_u32(kp, n_cis + x);
+      nkw.push_back(nk);
+      for (uint32_t kid : word_kids) local[kid] = -1;
     }
-    n_keys += nk;
-    n_cis += m;
-    for (uint32_t kid : word_kids) local[kid] = -1;
-  }
-  const size_t kb = kp - keys_b.get(), rb = rp - ranges_b.get(), cb = cp - cis_b.get();
-  out.resize(16 + kb + rb + cb);
+  });
+  std::vector<uint64_t> kbase(T + 1, 0);
+  for (uint32_t j = 0; j < T; j++) kbase[j + 1] = kbase[j] + keys_j[j].size() / 11;
+  const uint64_t n_keys = kbase[T];
+  BGPU_ARG(n_keys <= 0xffffffffull, "too many keys");
+  const size_t key_off = 8, ranges_off = key_off + 11 * n_keys + 4, cis_off = ranges_off + 8ull * n_words + 4;
+  out.resize(cis_off + 5 * n);
   uint8_t* o = out.data();
-  o = put_u32(o, kKcVersion);
-  o = put_u32(o, n_keys);
-  memcpy(o, keys_b.get(), kb);
-  o = put_u32(o + kb, n_words);
-  memcpy(o, ranges_b.get(), rb);
-  o = put_u32(o + rb, n_cis);
-  memcpy(o, cis_b.get(), cb);
+  put_u32(o, kKcVersion);
+  put_u32(o + 4, (uint32_t)n_keys);
+  put_u32(o + ranges_off - 4, n_words);
+  put_u32(o + cis_off - 4, (uint32_t)n);
+  parallel(T, [&](uint32_t j) {
+    if (!keys_j[j].empty()) memcpy(o + key_off + 11 * kbase[j], keys_j[j].data(), keys_j[j].size());
+    uint32_t k = (uint32_t)kbase[j];
+    uint8_t* rp = o + ranges_off + 8ull * wcut[j];
+    for (uint32_t nk : nk_j[j]) {
+      rp = put_u32(rp, k);
+      rp = put_u32(rp, k + nk);
+      k += nk;
+    }
+    const uint64_t c0 = start[wcut[j]], c1 = start[wcut[j + 1]];
+    if (c1 > c0) memcpy(o + cis_off + 5 * c0, cis_b.get() + 5 * c0, 5 * (c1 - c0));
+  });
   return BINIUS_OK;
 }
 
