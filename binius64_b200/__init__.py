@@ -22,12 +22,12 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._ffi import ArgumentError, BiniusError, check, lib
+from ._ffi import ArgumentError, BiniusError, OutOfMemoryError, check, lib
 
 __all__ = [
     "AdditiveNTT", "ReedSolomonCode", "BinaryMerkleTreeProver", "MerkleCommitted", "FRIParams",
     "CommitOutput", "commit_interleaved", "fold_interleaved", "fold_codeword", "gf_mul_batch",
-    "to_device", "to_host", "ArgumentError", "BiniusError", "version",
+    "to_device", "to_host", "ArgumentError", "BiniusError", "OutOfMemoryError", "version",
 ]
 
 
@@ -638,6 +638,10 @@ class Prover:
                                         _stream(stream)))
         return t
 
+    def workspace_bytes(self) -> int:
+        """Device memory one proof takes (the queue's admission estimate)."""
+        return int(lib().binius_prover_workspace_bytes(self._h))
+
     def phase_ms(self) -> dict:
         """Host wall-clock milliseconds of the last prove's phases."""
         out = (ctypes.c_double * 5)()
@@ -773,6 +777,13 @@ class ProveQueue:
             check(lib().binius_queue_submit(self._h, prover._h, w.data_ptr(), 1, ctypes.byref(t)))
         self._keep[t.value] = (w, prover)
         return t.value
+
+    def stats(self) -> dict:
+        """The queue's device-memory accounting: budget, accounted bytes now and at their peak,
+        and the number of finished requests."""
+        out = (ctypes.c_uint64 * 4)()
+        check(lib().binius_queue_stats(self._h, out))
+        return {"budget": out[0], "in_use": out[1], "peak": out[2], "completed": out[3]}
 
     def done(self, ticket: int) -> bool:
         d = ctypes.c_int(0)

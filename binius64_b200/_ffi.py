@@ -35,6 +35,11 @@ class ArgumentError(BiniusError, ValueError):
     """Mirrors binius_prover::Error::ArgumentError (prover/prover/src/error.rs:9-24)."""
 
 
+class OutOfMemoryError(BiniusError, MemoryError):
+    """BINIUS_E_OOM: a device allocation was refused, or a proving queue refused a request that
+    needs more device memory than its budget."""
+
+
 _c = ctypes
 _vp = _c.c_void_p
 _u32 = _c.c_uint32
@@ -117,6 +122,8 @@ _SIGS = {
     "binius_queue_submit": (_int, [_vp, _vp, _vp, _int, _vp]),
     "binius_queue_poll": (_int, [_vp, _u64, _vp]),
     "binius_queue_wait": (_int, [_vp, _u64, _vp, _c.c_size_t, _vp, _vp]),
+    "binius_queue_stats": (_int, [_vp, _vp]),
+    "binius_debug_fail_allocs": (None, [_c.c_int64]),
     "binius_fri_n_test_queries": (_u32, [_u32, _u32]),
     "binius_fri_estimate_optimal_arity": (_u32, [_u32, _u32, _u32]),
     "binius_gf_mul_batch": (_int, [_vp, _vp, _vp, _u64, _vp]),
@@ -160,4 +167,6 @@ def check(rc: int) -> None:
         msg = lib().binius_last_error().decode(errors="replace")
         if rc == BINIUS_E_ARG:
             raise ArgumentError(rc, msg)
+        if rc == BINIUS_E_OOM:
+            raise OutOfMemoryError(rc, msg)
         raise BiniusError(rc, msg)

@@ -199,9 +199,23 @@ struct Arena {
 thread_local Arena t_arena;
 constexpr size_t kArenaChunk = 64ull << 20;
 
+// Host-side allocation-failure injection (binius_debug_fail_allocs): the number of device
+// allocations that still succeed before the next one is refused, or -1 when off.
+std::atomic<int64_t> g_allocs_before_failure{-1};
+
 }  // namespace
 
 cudaError_t dev_alloc_raw(void** p, size_t bytes, cudaStream_t s) {
+  int64_t left = g_allocs_before_failure.load(std::memory_order_relaxed);
+  while (left >= 0) {
+    if (g_allocs_before_failure.compare_exchange_weak(left, left - 1)) {
+      if (left == 0) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;  // as the pool reports an allocation it cannot serve
+      }
+      break;
+    }
+  }
   Arena& a = t_arena;
   if (!a.active || a.s != s) return cudaMallocAsync(p, bytes ? bytes : 16, s);
   const size_t need = (bytes + 255) & ~size_t(255);
@@ -256,6 +270,12 @@ void arena_release_thread() {
   if (a.active) return;
   a.release();
   a.s = nullptr;
+}
+
+uint64_t arena_held_bytes() {
+  uint64_t n = 0;
+  for (const auto& c : t_arena.chunks) n += c.size;
+  return n;
 }
 
 int read_sync(void* dst, const void* src, size_t bytes, cudaStream_t s) {
@@ -327,5 +347,9 @@ const char* binius_last_error(void) { return bgpu::g_last_error.c_str(); }
 const char* binius_version(void) { return "binius64_b200 0.1.0 (sm_100a)"; }
 
 uint64_t binius_launch_count(void) { return bgpu::g_launches.load(std::memory_order_relaxed); }
+
+void binius_debug_fail_allocs(int64_t n_before_failure) {
+  bgpu::g_allocs_before_failure.store(n_before_failure < 0 ? -1 : n_before_failure);
+}
 
 }  // extern "C"

@@ -204,52 +204,58 @@ int noalloc_scratch(void** out) {
   return BINIUS_OK;
 }
 
-// The fold behind binius_fri_fold_codeword; challenges from ch, or from device memory at dch.
-int fold_codeword_impl(const binius_ntt* ntt, const void* d_codeword, uint32_t log_len,
-                       const Challenges& ch, const uint4* dch, uint32_t n_challenges, void* d_out,
-                       cudaStream_t s) {
-  const uint4* cw = static_cast<const uint4*>(d_codeword);
+// The steps of a fold over n_challenges <= 8 rounds: at most 4 rounds per launch (one coset of
+// 16 values per thread in registers).  A fold over n challenges equals n successive
+// single-challenge folds of the whole codeword, so two steps chain through `tmp`
+// (2^(log_len - 4) elements, needed only when n_challenges > 4): codeword -> tmp -> out.
+// Challenges come from ch, or from device memory at dch.
+int fold_codeword_steps(const binius_ntt* ntt, const void* d_codeword, uint32_t log_len,
+                        const Challenges& ch, const uint4* dch, uint32_t n_challenges,
+                        void* d_out, uint4* tmp, cudaStream_t s) {
   const uint4* tw = static_cast<const uint4*>(ntt->d_twiddles);
   uint4* out = static_cast<uint4*>(d_out);
   if (n_challenges == 0) {
     BGPU_CUDA(cudaMemcpyAsync(d_out, d_codeword, 16ull << log_len, cudaMemcpyDeviceToDevice, s));
     return BINIUS_OK;
   }
-  // Rounds are applied in steps of at most 4 (one coset of 16 values per thread in registers);
-  // a fold over n challenges equals n successive single-challenge folds of the whole codeword,
-  // so steps chain through a stream-ordered intermediate buffer.
-  void* tmp = nullptr;
-  if (n_challenges > 4) {
-    BGPU_CUDA(dev_alloc(&tmp, 16ull << (log_len - 4), s));
-  }
   uint32_t done = 0, cur_len = log_len;
-  const uint4* src = cw;
+  const uint4* src = static_cast<const uint4*>(d_codeword);
   while (done < n_challenges) {
     uint32_t step = std::min<uint32_t>(4, n_challenges - done);
     Challenges sub;
     memset(&sub, 0, sizeof(sub));
     for (uint32_t i = 0; i < step; i++) sub.r[i] = ch.r[done + i];
     const uint4* dsub = dch ? dch + done : nullptr;
-    // n <= 8, so there are at most two steps: codeword -> tmp -> out.
-    uint4* dst = (done + step == n_challenges) ? out : static_cast<uint4*>(tmp);
+    // the first step writes all of tmp before the second reads it (same stream)
+    uint4* dst = (done + step == n_challenges) ? out : tmp;
     switch (step) {
       case 1: launch_fold_codeword<1>(src, cur_len, tw, sub, dsub, dst, s); break;
       case 2: launch_fold_codeword<2>(src, cur_len, tw, sub, dsub, dst, s); break;
       case 3: launch_fold_codeword<3>(src, cur_len, tw, sub, dsub, dst, s); break;
       default: launch_fold_codeword<4>(src, cur_len, tw, sub, dsub, dst, s); break;
     }
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) {
-      if (tmp) dev_free(tmp, s);
-      return cuda_error(e, "fold_codeword_kernel");
-    }
+    BGPU_LAUNCH_CHECK("fold_codeword_kernel");
     count_launch();
     src = dst;
     cur_len -= step;
     done += step;
   }
-  if (tmp) BGPU_CUDA(dev_free(tmp, s));
   return BINIUS_OK;
+}
+
+// The fold behind binius_fri_fold_codeword: the intermediate of a fold over more than 4
+// challenges is a stream-ordered allocation.
+int fold_codeword_impl(const binius_ntt* ntt, const void* d_codeword, uint32_t log_len,
+                       const Challenges& ch, const uint4* dch, uint32_t n_challenges, void* d_out,
+                       cudaStream_t s) {
+  uint4* tmp = nullptr;
+  if (n_challenges > 4) BGPU_CUDA(dev_alloc(&tmp, 16ull << (log_len - 4), s));
+  const int rc = fold_codeword_steps(ntt, d_codeword, log_len, ch, dch, n_challenges, d_out, tmp, s);
+  if (tmp) {
+    cudaError_t e = dev_free(tmp, s);
+    if (!rc && e != cudaSuccess) return cuda_error(e, "dev_free(fold intermediate)");
+  }
+  return rc;
 }
 
 }  // namespace
@@ -357,36 +363,10 @@ int binius_fri_fold_codeword_noalloc(const binius_ntt* ntt, const void* d_codewo
     if (int rc = noalloc_scratch(&p)) return rc;
     scratch = static_cast<uint4*>(p);
   }
-  cudaStream_t s = as_stream(stream);
-  const uint4* cw = static_cast<const uint4*>(d_codeword);
-  const uint4* tw = static_cast<const uint4*>(ntt->d_twiddles);
-  uint4* out = static_cast<uint4*>(d_out);
-  if (n_challenges == 0) {
-    BGPU_CUDA(cudaMemcpyAsync(d_out, d_codeword, 16ull << log_len, cudaMemcpyDeviceToDevice, s));
-    return clear_error();
-  }
-  uint32_t done = 0, cur_len = log_len;
-  const uint4* src = cw;
-  while (done < n_challenges) {
-    uint32_t step = std::min<uint32_t>(4, n_challenges - done);
-    Challenges sub;
-    memset(&sub, 0, sizeof(sub));
-    for (uint32_t i = 0; i < step; i++) sub.r[i] = ch.r[done + i];
-    // n <= 8: codeword -> scratch -> out.  The scratch is fully written by the first step before
-    // the second reads it (same stream), so it needs no clearing.
-    uint4* dst = (done + step == n_challenges) ? out : scratch;
-    switch (step) {
-      case 1: launch_fold_codeword<1>(src, cur_len, tw, sub, nullptr, dst, s); break;
-      case 2: launch_fold_codeword<2>(src, cur_len, tw, sub, nullptr, dst, s); break;
-      case 3: launch_fold_codeword<3>(src, cur_len, tw, sub, nullptr, dst, s); break;
-      default: launch_fold_codeword<4>(src, cur_len, tw, sub, nullptr, dst, s); break;
-    }
-    BGPU_LAUNCH_CHECK("fold_codeword_kernel");
-    count_launch();
-    src = dst;
-    cur_len -= step;
-    done += step;
-  }
+  // the same steps as binius_fri_fold_codeword, with the static scratch as the intermediate
+  if (int rc = fold_codeword_steps(ntt, d_codeword, log_len, ch, nullptr, n_challenges, d_out,
+                                   scratch, as_stream(stream)))
+    return rc;
   return clear_error();
 }
 

@@ -92,8 +92,13 @@ class ArenaScope {
 };
 
 // Returns the calling thread's kept arena chunks to the pool (a queue worker, before it destroys
-// its stream).
+// its stream, or when the memory it keeps stands in the way of the next request).
 void arena_release_thread();
+// Device bytes the calling thread's arena holds (its chunks, in use or kept).
+uint64_t arena_held_bytes();
+
+// Records that a proof of P took `bytes` of arena chunks from an empty arena (prover.cu).
+void prover_note_footprint(const binius_prover* P, uint64_t bytes);
 
 // Sets the dynamic shared memory limit of a kernel once per device (see common.cu).
 int ensure_smem_limit(const void* func, size_t bytes);

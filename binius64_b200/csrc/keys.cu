@@ -96,7 +96,9 @@ int key_collection_bytes(const binius_cs& cs, std::vector<uint8_t>& out) {
   const size_t n = cs.h_and.terms.size() + cs.h_mul.terms.size();
   const Passes P(cs);
   uint32_t T = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
-  while (T > 1 && (uint64_t)T * n_words > (1ull << 27)) T--;  // per-thread word counts
+  // per-thread word counts: T * n_words * 4 bytes of host memory, held to 128 MiB (8 threads up
+  // to 2^22 words; a 2^20-word system holds 32 MiB of counts)
+  while (T > 1 && (uint64_t)T * n_words > (1ull << 25)) T--;
   if (n < (1u << 16)) T = 1;
   // stable group by word: per-thread counts over contiguous group ranges, then offsets
   const uint64_t NG = P.n_groups();

@@ -10,6 +10,7 @@
 // log_dim + log_inv_rate layers.
 #include <string.h>
 
+#include <atomic>
 #include <chrono>
 #include <vector>
 
@@ -27,7 +28,18 @@ struct binius_prover {
   binius_pcs* pcs = nullptr;
   uint32_t log_inv_rate = 0, log_witness_elems = 0, log_batch = 0, n_queries = 0;
   std::vector<uint32_t> arities;
+  // largest device footprint (arena chunk bytes) a proof of this prover has taken from an empty
+  // arena; raises binius_prover_workspace_bytes when the static estimate is low
+  mutable std::atomic<uint64_t> footprint{0};
 };
+
+namespace bgpu {
+void prover_note_footprint(const binius_prover* P, uint64_t bytes) {
+  uint64_t cur = P->footprint.load(std::memory_order_relaxed);
+  while (bytes > cur && !P->footprint.compare_exchange_weak(cur, bytes)) {
+  }
+}
+}  // namespace bgpu
 
 namespace {
 
@@ -131,8 +143,11 @@ uint64_t binius_prover_workspace_bytes(const binius_prover* P) {
   const uint64_t n_mul = cs->mul_ops.n_constraints;
   const uint64_t code = 16ull << (P->log_witness_elems + P->log_inv_rate);
   // codeword + tree, AND columns / folds / eq, shift W / M / g parts, PCS fold buffers, IntMul
-  // trees; an upper bound of the stream-ordered allocations one proof holds at once
-  return 2 * code + 96 * n_and + 80 * words + 12288 * n_mul + (8ull << 20);
+  // trees: the stream-ordered allocations of one proof, which its arena never frees before the
+  // end, rounded up by one arena chunk; or, if larger, what a proof of this prover took
+  const uint64_t est = 2 * code + 96 * n_and + 80 * words + 12288 * n_mul + (72ull << 20);
+  const uint64_t seen = P->footprint.load(std::memory_order_relaxed);
+  return est > seen ? est : seen;
 }
 
 int binius_prover_phase_ms(const binius_prover* P, double* h_out5) {
@@ -151,6 +166,7 @@ int binius_prover_prove(const binius_prover* P, const void* d_witness,
 
   // every device buffer of the proof comes from one arena on s, released at the end
   ArenaScope arena(s, false);
+  const bool fresh_arena = arena_held_bytes() == 0;
   typedef std::chrono::steady_clock Clock;
   auto t0 = Clock::now();
   auto lap = [&](int phase) {
@@ -194,6 +210,7 @@ int binius_prover_prove(const binius_prover* P, const void* d_witness,
     lap(4);
   } while (0);
   binius_pcs_committed_destroy(committed);
+  if (!rc && fresh_arena) prover_note_footprint(P, arena_held_bytes());
   return rc ? rc : clear_error();
 }
 

@@ -2,10 +2,14 @@
 //
 // A queue owns `n_workers` host threads on one device, each with its own non-blocking CUDA
 // stream.  Requests (a prover, i.e. a constraint system with its parameters, and a witness) are
-// admitted in FIFO order while the sum of the admitted requests' workspace estimates
-// (binius_prover_workspace_bytes, plus the witness copy for host witnesses) stays within the
-// queue's HBM budget; an admitted request runs binius_prover_prove on its worker's stream with a
-// fresh transcript.  A proof is a chain of Fiat-Shamir rounds that synchronise with the host, so
+// admitted in FIFO order while the device memory the queue accounts for stays within its HBM
+// budget; an admitted request runs binius_prover_prove on its worker's stream with a fresh
+// transcript.  Accounted memory: every worker's arena (the chunks it keeps between proofs so that
+// the next proof allocates nothing) plus, for a running request, what its workspace estimate
+// (binius_prover_workspace_bytes, plus the witness copy for host witnesses) needs beyond the
+// chunks its worker already holds.  When the head request does not fit, idle workers give their
+// kept chunks back; a request whose estimate exceeds the whole budget is refused at submission
+// with BINIUS_E_OOM.  A proof is a chain of Fiat-Shamir rounds that synchronise with the host, so
 // requests proving at the same time fill each other's round trips with kernels, and the device
 // keeps every witness, codeword and tree resident until that request's proof is emitted.  Each
 // proof is exactly the proof of a lone call: no state is shared between requests.
@@ -13,6 +17,7 @@
 // The reference has no serving layer (its CLI proves one statement per process,
 // prover/examples/src/cli.rs:455-509); this is the batching / serving wrapper around
 // Prover::prove (prover/prover/src/prove.rs:124-303).
+#include <stdio.h>
 #include <string.h>
 
 #include <algorithm>
@@ -58,21 +63,24 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 
 struct binius_queue {
   int device = 0;
-  uint64_t budget = 0, in_use = 0;
+  // in_use: the accounted bytes (every worker's held chunks, plus each running request's
+  // reservation beyond them); peak: its maximum since creation
+  uint64_t budget = 0, in_use = 0, peak = 0;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<std::shared_ptr<Request>> pending;
   std::unordered_map<uint64_t, std::shared_ptr<Request>> requests;
   std::vector<std::thread> workers;
+  std::vector<cudaStream_t> streams;  // one per worker, created before the workers start
   bool stop = false;
   uint64_t next_ticket = 1;
   uint64_t completed = 0;
   uint32_t n_workers = 0;  // set before the workers start
 
-  void worker_loop();
+  void worker_loop(uint32_t w);
 };
 
-void binius_queue::worker_loop() {
+void binius_queue::worker_loop(uint32_t w) {
   cudaSetDevice(device);
   // Workers poll a finished-yet event for a short while before they sleep on it: most waits of a
   // proof end within the poll, and waking from a blocking sync costs more than the poll.  With
@@ -80,26 +88,50 @@ void binius_queue::worker_loop() {
   // (measured: 32 workers on 16 cores gave half the throughput of 16), so they sleep at once.
   set_blocking_waits(true, n_workers <= std::max(1u, std::thread::hardware_concurrency()) ? 100.0
                                                                                            : 0.0);
-  cudaStream_t s = nullptr;
-  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return;
+  cudaStream_t s = streams[w];
+  uint64_t held = 0;  // this worker's arena bytes, counted in in_use
   for (;;) {
     std::shared_ptr<Request> r;
+    uint64_t reserved = 0;
     {
       std::unique_lock<std::mutex> lock(mu);
-      // FIFO admission: the head request waits until its workspace fits in the budget (a lone
-      // request is always admitted, so an oversized one cannot stall the queue forever)
-      cv_work.wait(lock, [&] {
-        return stop || (!pending.empty() &&
-                        (in_use == 0 || in_use + pending.front()->bytes <= budget));
-      });
-      if (pending.empty()) {
-        if (stop) break;
-        continue;
+      bool give_back = false;
+      for (;;) {
+        if (pending.empty()) {
+          if (stop) break;
+        } else {
+          // FIFO admission: the head request runs here if the accounted memory with its
+          // reservation (the estimate, of which this worker's kept chunks already cover part)
+          // fits the budget.  Otherwise an idle worker that keeps chunks gives them back, so
+          // that the memory kept by idle workers cannot hold the head request off for good.
+          const uint64_t need = std::max(pending.front()->bytes, held);
+          if (in_use - held + need <= budget) {
+            r = pending.front();
+            pending.pop_front();
+            reserved = need;
+            in_use += need - held;
+            peak = std::max(peak, in_use);
+            r->started = Clock::now();
+            break;
+          }
+          if (held) {
+            give_back = true;
+            break;
+          }
+        }
+        cv_work.wait(lock);
       }
-      r = pending.front();
-      pending.pop_front();
-      in_use += r->bytes;
-      r->started = Clock::now();
+      if (!r && !give_back) break;  // stopped
+      if (give_back) {
+        in_use -= held;
+        held = 0;
+      }
+    }
+    if (!r) {  // give the kept chunks back to the pool and let the others re-check
+      arena_release_thread();
+      stream_wait(s);
+      cv_work.notify_all();
+      continue;
     }
     int rc = BINIUS_OK;
     std::string err;
@@ -125,9 +157,14 @@ void binius_queue::worker_loop() {
     if (rc) err = binius_last_error();
     if (owned) dev_free(owned, s);
     stream_wait(s);
+    const uint64_t held_now = arena_held_bytes();
+    // a proof that started from an empty arena measured the prover's real footprint
+    if (!rc && held == 0 && r->on_device) prover_note_footprint(r->prover, held_now);
     {
       std::lock_guard<std::mutex> lock(mu);
-      in_use -= r->bytes;
+      in_use = in_use - reserved + held_now;
+      held = held_now;
+      peak = std::max(peak, in_use);
       r->finished = Clock::now();
       r->status = rc;
       r->error = err;
@@ -140,7 +177,7 @@ void binius_queue::worker_loop() {
     cv_work.notify_all();
   }
   arena_release_thread();
-  cudaStreamDestroy(s);
+  stream_wait(s);
 }
 
 extern "C" {
@@ -177,7 +214,17 @@ int binius_queue_create(int device, uint32_t n_workers, uint64_t hbm_budget_byte
     cudaGetLastError();
   }
   q->n_workers = n_workers;
-  for (uint32_t i = 0; i < n_workers; i++) q->workers.emplace_back([q] { q->worker_loop(); });
+  for (uint32_t i = 0; i < n_workers; i++) {
+    cudaStream_t s = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      for (cudaStream_t t : q->streams) cudaStreamDestroy(t);
+      delete q;
+      return cuda_error(e, "queue worker stream");
+    }
+    q->streams.push_back(s);
+  }
+  for (uint32_t i = 0; i < n_workers; i++) q->workers.emplace_back([q, i] { q->worker_loop(i); });
   *out = q;
   return clear_error();
 }
@@ -198,6 +245,7 @@ int binius_queue_destroy(binius_queue* q) {
   q->cv_work.notify_all();
   q->cv_done.notify_all();
   for (auto& w : q->workers) w.join();
+  for (cudaStream_t s : q->streams) cudaStreamDestroy(s);
   delete q;
   return BINIUS_OK;
 }
@@ -214,6 +262,13 @@ int binius_queue_submit(binius_queue* q, const binius_prover* prover, const void
   {
     std::lock_guard<std::mutex> lock(q->mu);
     BGPU_ARG(!q->stop, "queue is shutting down");
+    if (r->bytes > q->budget) {
+      char buf[160];
+      snprintf(buf, sizeof(buf),
+               "request needs %llu bytes of device memory, more than the queue's budget of %llu",
+               (unsigned long long)r->bytes, (unsigned long long)q->budget);
+      return set_error(BINIUS_E_OOM, buf);
+    }
     r->ticket = q->next_ticket++;
     r->submitted = Clock::now();
     q->pending.push_back(r);
@@ -221,6 +276,16 @@ int binius_queue_submit(binius_queue* q, const binius_prover* prover, const void
     *ticket = r->ticket;
   }
   q->cv_work.notify_all();
+  return clear_error();
+}
+
+int binius_queue_stats(binius_queue* q, uint64_t* h_out4) {
+  BGPU_ARG(q && h_out4, "NULL argument");
+  std::lock_guard<std::mutex> lock(q->mu);
+  h_out4[0] = q->budget;
+  h_out4[1] = q->in_use;
+  h_out4[2] = q->peak;
+  h_out4[3] = q->completed;
   return clear_error();
 }
 

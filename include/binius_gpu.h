@@ -35,6 +35,11 @@ const char* binius_version(void);
 /* Cumulative number of CUDA kernels launched by this library in this process (no reference
  * counterpart: launch accounting for benchmarks and tests). */
 uint64_t binius_launch_count(void);
+/* Host-side failure injection for tests (no reference counterpart): after n_before_failure more
+ * device allocations of the prove path succeed, the next one is refused as the allocator refuses
+ * one (BINIUS_E_OOM from the call that made it); a negative value turns injection off.  No
+ * kernel is involved: the refusal happens on the host before anything is launched with it. */
+void binius_debug_fail_allocs(int64_t n_before_failure);
 
 /* ------------------------------------------------------------------------------------------
  * AdditiveNTT over a GenericPreExpanded domain context.
@@ -271,8 +276,9 @@ int binius_prover_prove(const binius_prover* prover, const void* d_witness,
                         binius_transcript* transcript, void* stream);
 /* committed_total_len of the prover's constraint system (the witness length in words). */
 uint64_t binius_prover_committed_words(const binius_prover* prover);
-/* Upper-bound estimate of the device memory one proof allocates while it runs (admission of
- * concurrent proofs); no reference counterpart. */
+/* Estimate of the device memory one proof allocates while it runs (admission of concurrent
+ * proofs): a static upper bound, or the largest footprint a proof of this prover has measured if
+ * that is larger; no reference counterpart. */
 uint64_t binius_prover_workspace_bytes(const binius_prover* prover);
 /* Host wall-clock milliseconds of the calling thread's last prove's phases (the spans of prove.rs:164-300):
  * witness commit, IntMul, BitAnd, shift reduction, PCS opening.  No counterpart in the reference
@@ -284,10 +290,15 @@ int binius_prover_phase_ms(const binius_prover* prover, double* h_out5);
  * call of Prover::prove, prover/prover/src/prove.rs:124-303, and per process in its CLI,
  * prover/examples/src/cli.rs:455-509).
  * A queue runs n_workers proving threads on `device`, each with its own CUDA stream, and admits
- * requests in FIFO order while the workspace estimates of the running requests fit in
- * hbm_budget_bytes (0 = 90% of the free device memory at creation).  submit: `witness` holds the
- * prover's committed_total_len words, on the device (witness_on_device = 1) or on the host; it
- * must stay valid until wait returns.  wait blocks until the request is done, copies its proof
+ * requests in FIFO order while the device memory it accounts for fits in hbm_budget_bytes (0 =
+ * 90% of the free device memory at creation): the chunks every worker keeps for its next proof,
+ * plus each running request's workspace estimate beyond its worker's chunks; idle workers give
+ * their chunks back when the head request does not fit.  submit: `witness` holds the prover's
+ * committed_total_len words, on the device (witness_on_device = 1) or on the host; it must stay
+ * valid until wait returns.  A request whose estimate (binius_prover_workspace_bytes, plus the
+ * witness copy for a host witness) exceeds the budget is refused with BINIUS_E_OOM.  A request
+ * whose proof fails (a refused allocation: BINIUS_E_OOM) reports the error from wait; the queue
+ * and its other requests carry on.  wait blocks until the request is done, copies its proof
  * (the finalized transcript of a fresh ProverTranscript) into h_proof and releases the ticket;
  * with a too-small buffer it sets *len, returns BINIUS_E_ARG and keeps the result.  h_times8
  * (optional): queued, proving and total milliseconds, then the proof's phase milliseconds
@@ -304,6 +315,8 @@ int binius_queue_submit(binius_queue* queue, const binius_prover* prover, const 
 int binius_queue_poll(binius_queue* queue, uint64_t ticket, int* done);
 int binius_queue_wait(binius_queue* queue, uint64_t ticket, void* h_proof, size_t cap,
                       size_t* len, double* h_times8);
+/* h_out4: budget, accounted bytes now, their peak since creation, finished requests. */
+int binius_queue_stats(binius_queue* queue, uint64_t* h_out4);
 
 /* ------------------------------------------------------------------------------------------
  * Wire formats around a prove call (load-prove serving).

@@ -2,21 +2,23 @@
 (verifier/core/test_data/{constraint_system_v2,witness_v1,proof_v1}.bin) as hex, with the contents
 its own tests assert (verifier/core/src/constraint_system.rs:1465-1500, 1579-1600, 1775-1800).
 
-Run in a container that has the reference tree at REFERENCE (default /root/reference); the GPU
-box and the tests read only the committed JSON.
+Usage: python tests/golden/make_format_fixtures.py <reference root>
+Run where the reference tree exists; the GPU box and the tests read only the committed JSON.
 """
 import json
 import os
 import sys
 
-REF = os.environ.get("REFERENCE", "/root/reference")
-DATA = os.path.join(REF, "verifier", "core", "test_data")
 
 
 def main():
+    if len(sys.argv) != 2:
+        print(__doc__)
+        return 2
+    data = os.path.join(sys.argv[1], "verifier", "core", "test_data")
     out = {}
     for name in ("constraint_system_v2", "witness_v1", "proof_v1"):
-        with open(os.path.join(DATA, name + ".bin"), "rb") as f:
+        with open(os.path.join(data, name + ".bin"), "rb") as f:
             out[name] = f.read().hex()
     out["expect"] = {
         "constraint_system_v2": {

@@ -7,14 +7,13 @@ Sources (read as text; nothing of the reference is executed):
       derivation in test_round_constants) and B_INV_COEFFS (the linearized polynomial of B^-1,
       checked against B^-1 o B = id in test_b_inverse_coeffs)
 
-Usage: python tests/golden/make_vision4_fixtures.py [reference root]
+Usage: python tests/golden/make_vision4_fixtures.py <reference root>
 """
 import json
 import os
 import re
 import sys
 
-ROOT = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 HEX = re.compile(r"Ghash::new\((0x[0-9a-fA-F]+)\)")
 
 
@@ -25,7 +24,10 @@ def block(text, start, end_pat=r"\n\];"):
 
 
 def main():
-    base = os.path.join(ROOT, "verifier/verifier/src/hash/vision_4")
+    if len(sys.argv) != 2:
+        print(__doc__)
+        return 2
+    base = os.path.join(sys.argv[1], "verifier/verifier/src/hash/vision_4")
     consts = open(os.path.join(base, "constants.rs")).read()
     perm = open(os.path.join(base, "permutation.rs")).read()
     round_constants = block(consts, "pub static ROUND_CONSTANTS")
