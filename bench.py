@@ -58,6 +58,7 @@ FOLD_ARITY = 4
 N_FOLDS = 3
 
 PROVE_METRIC = "prove ms @2^20 words"
+PUBLISHED_REFERENCE_MS = 128.58  # the reference README's sha512 64 KiB prove, hardware unstated
 WITNESS_METRIC = "witness generation ms per instance @2^20 words"
 WITNESS_BATCH = 32
 COMMIT_METRIC = "FRI commit ms: RS encode + SHA-256 Merkle + 3 FRI folds with commits"
@@ -106,6 +107,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true",
                     help="prove workload: skip the batched-queue summary (profiling runs)")
+    ap.add_argument("--no-matrix", action="store_true",
+                    help="prove workload: skip the kernel-level commit matrix summary")
     ap.add_argument("--log-words", type=int, default=None,
                     help="prove workload: log2 committed words (default 20)")
     ap.add_argument("--merkle-hash", default="sha256", choices=["sha256", "vision4"],
@@ -324,21 +327,26 @@ def bivariate_roofline(torch, bg, lib, device, stream, reps=20):
 BATCH_LOG_MIN, BATCH_LOG_MAX, BATCH_DISTINCT = 12, 20, 12
 
 
-def batch_statements(torch, bg, device, n_distinct=BATCH_DISTINCT):
-    """Distinct synthetic statements with log2(words) uniform in [12, 20] (log-uniform sizes),
-    AND chains over shifted operands plus 2^(log_words - 10) MUL constraints each."""
+SERVE_EXTRA_LOG_WORDS = [21, 22]  # the served mix adds statements beyond the batched range
+
+
+def mix_statement(torch, bg, device, lw, seed):
+    """A synthetic statement of 2^lw words: AND chains over shifted operands plus
+    2^(lw - 10) MUL constraints."""
     from binius64_b200 import constraint_system as csm
+    n_mul = max(1, 1 << (lw - 10))
+    sc = csm.synthetic_circuit(lw, n_and_for(lw) - 2 * n_mul, n_mul, seed=seed)
+    prover = bg.Prover(bg.DeviceConstraintSystem(sc.cs.serialize(), device=device), LOG_INV_RATE)
+    w = torch.from_numpy(sc.witness.view(np.int64)).to(f"cuda:{device}")
+    return (lw, prover, w)
+
+
+def batch_statements(torch, bg, device, n_distinct=BATCH_DISTINCT):
+    """Distinct synthetic statements with log2(words) uniform in [12, 20] (log-uniform sizes)."""
     rng = np.random.default_rng(SEED + 7)
     sizes = sorted(int(x) for x in rng.integers(BATCH_LOG_MIN, BATCH_LOG_MAX + 1, size=n_distinct))
-    out = []
-    for i, lw in enumerate(sizes):
-        n_mul = max(1, 1 << (lw - 10))
-        sc = csm.synthetic_circuit(lw, n_and_for(lw) - 2 * n_mul, n_mul, seed=SEED + 100 + i)
-        prover = bg.Prover(bg.DeviceConstraintSystem(sc.cs.serialize(), device=device),
-                           LOG_INV_RATE)
-        w = torch.from_numpy(sc.witness.view(np.int64)).to(f"cuda:{device}")
-        out.append((lw, prover, w))
-    return sizes, out
+    return sizes, [mix_statement(torch, bg, device, lw, SEED + 100 + i)
+                   for i, lw in enumerate(sizes)]
 
 
 def one_at_a_time(torch, stmts, order):
@@ -396,6 +404,43 @@ def batch_summary(torch, bg, device, n_requests, workers):
     }, (sizes, stmts, order, t_seq, lone)
 
 
+def serve_summary(torch, bg, device, batch_ctx, n_requests, workers):
+    """A Poisson request stream (seeded arrivals) over the batched mix plus statements of 2^21
+    and 2^22 words, at 70% of the queue's measured all-at-once capacity for this mix; latency
+    percentiles, throughput, the one-at-a-time rate of the same requests and bit identity with
+    the lone proofs."""
+    sizes, stmts, _, _, _ = batch_ctx
+    stmts = list(stmts)
+    for k, lw in enumerate(SERVE_EXTRA_LOG_WORDS):
+        stmts.append(mix_statement(torch, bg, device, lw, SEED + 300 + k))
+    sizes = [st[0] for st in stmts]
+    rng = np.random.default_rng(SEED + 17)
+    order = [int(x) for x in rng.integers(0, len(stmts), size=n_requests)]
+    for i in set(order):
+        stmts[i][1].prove(stmts[i][2])
+    t_seq, lone = one_at_a_time(torch, stmts, order)
+    t_cap, _, _, _ = run_queue(bg, stmts, order, workers)
+    rate = 0.7 * n_requests / t_cap
+    arrivals = np.cumsum(np.random.default_rng(SEED + 13).exponential(1.0 / rate,
+                                                                       size=n_requests)).tolist()
+    t_q, lat, prove, proofs = run_queue(bg, stmts, order, workers, arrivals)
+    identical = all(proofs[k] == lone[i] for k, i in enumerate(order))
+    by_size = {}
+    for k, i in enumerate(order):
+        by_size.setdefault(sizes[i], []).append(lat[k])
+    return {
+        "requests": n_requests, "workers": workers, "log_words": sizes,
+        "arrival_rate_per_s": rate, "capacity_proofs_per_s": n_requests / t_cap,
+        "proofs_per_s": n_requests / t_q,
+        "one_at_a_time_proofs_per_s": n_requests / t_seq,
+        "capacity_vs_one_at_a_time": t_seq / t_cap,
+        "latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99), "max": max(lat)},
+        "latency_ms_p99_by_log_words": {str(k): pct(v, 99) for k, v in sorted(by_size.items())},
+        "prove_ms_in_mix": {"p50": pct(prove, 50), "p99": pct(prove, 99)},
+        "bit_identical_to_lone_proofs": identical,
+    }
+
+
 def run_batch_workload(args, rank, world, local, serve=False):
     import torch
     import binius64_b200 as bg
@@ -422,19 +467,12 @@ def run_batch_workload(args, rank, world, local, serve=False):
         line.update({"value": summ["proofs_per_s"], "ms_per_step": 1000.0 / summ["proofs_per_s"],
                      "batch": summ})
     else:
-        rate = 0.7 * summ["proofs_per_s"]
-        rng = np.random.default_rng(SEED + 13)
-        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=args.requests)).tolist()
-        t_q, lat, prove, proofs = run_queue(bg, stmts, order, args.workers, arrivals)
-        identical = all(proofs[k] == lone[i] for k, i in enumerate(order))
-        line.update({"value": args.requests / t_q, "ms_per_step": 1000.0 * t_q / args.requests,
-                     "serve": {"arrival_rate_per_s": rate, "proofs_per_s": args.requests / t_q,
-                               "latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99),
-                                              "max": max(lat)},
-                               "prove_ms_in_mix": {"p50": pct(prove, 50), "p99": pct(prove, 99)},
-                               "one_at_a_time_proofs_per_s": args.requests / t_seq,
-                               "bit_identical_to_lone_proofs": identical},
-                     "batch": summ})
+        sv = serve_summary(torch, bg, local, (sizes, stmts, order, t_seq, lone), args.requests,
+                           args.workers)
+        line["config"]["log_words"] = sv["log_words"]
+        line["data"] = "synthetic statements, log2(words) in [12, 22], seeded"
+        line.update({"value": sv["proofs_per_s"], "ms_per_step": 1000.0 / sv["proofs_per_s"],
+                     "serve": sv, "batch": summ})
     line["gpu_launches"] = int(round((lib().binius_launch_count() - launches0) / args.requests))
     line["e2e"] = {"value": line["value"], "unit": "proofs/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}
@@ -533,9 +571,13 @@ def run_prove(args, rank, world, local):
                              "oracle (C++ restatement of the reference prover, PCLMULQDQ, "
                              "std::thread over all host cores); the Rust reference needs cargo"}
         kernels = vision4_kernels(torch, bg, local, stream) if MERKLE_HASH == "vision4" else None
-        batched = None
+        batched = served = matrix = None
         if world == 1 and not args.no_batch and MERKLE_HASH == "sha256":
-            batched, _ = batch_summary(torch, bg, local, 256, 16)
+            batched, ctx = batch_summary(torch, bg, local, 256, 16)
+            served = serve_summary(torch, bg, local, ctx, 256, 16)
+            del ctx
+        if world == 1 and not args.no_matrix and MERKLE_HASH == "sha256":
+            matrix = commit_matrix(torch, local, stream)
         ph = {k: statistics.median(p[k] for p in phases) for k in phases[0]}
         line = {
             "metric": PROVE_METRIC, "value": ms, "unit": "ms", "n_gpus": world,
@@ -549,6 +591,15 @@ def run_prove(args, rank, world, local):
             "phase_ms_host": ph,
             "setup": setup,
             "batched": batched,
+            "served": served,
+            "commit_matrix": matrix,
+            "vs_published_reference": {
+                "reference_ms": PUBLISHED_REFERENCE_MS,
+                "ratio_device": PUBLISHED_REFERENCE_MS / ms,
+                "ratio_e2e": PUBLISHED_REFERENCE_MS / e2e_ms,
+                "note": "the reference's own published prove time for the sha512 64 KiB "
+                        "example (README.md, hardware unstated) over this line's 2^20-word "
+                        "synthetic statement of the same shape: context, not a same-box ratio"},
             "vision4_kernels": kernels,
             "proof_bytes": proof_len,
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(host_w.numel() * 8),
@@ -575,55 +626,60 @@ def run_prove(args, rank, world, local):
 
 # ----------------------------------------------------------------------------- commit workload
 
-class GpuPipeline:
-    """Preallocated buffers; one step = encode + commit + 3 x (fold + commit) via the C ABI."""
+C2_POINTS = [(L, R, b) for L in (20, 22, 24) for R in (1, 2) for b in (0, 4, 6)]
 
-    def __init__(self, torch, device):
-        import binius64_b200 as bg
-        from binius64_b200._ffi import check, lib
-        self.torch, self.bg, self.L, self.check = torch, bg, lib(), check
-        self.device = device
-        log_dim = LOG_LEN - LOG_INV_RATE
-        self.log_dim = log_dim
-        basis = bg.standard_domain_rs_basis(LOG_LEN + LOG_BATCH, LOG_BATCH, device=device)
-        self.ntt = bg.AdditiveNTT(LOG_LEN, basis=basis, device=device)
-        gen = torch.Generator(device=f"cuda:{device}").manual_seed(SEED)
-        d = f"cuda:{device}"
-        self.msg = torch.randint(-2**63, 2**63 - 1, (1 << (log_dim + LOG_BATCH), 2),
-                                 dtype=torch.int64, device=d, generator=gen)
-        self.codeword = torch.empty((1 << (LOG_LEN + LOG_BATCH), 2), dtype=torch.int64, device=d)
-        self.nodes = [torch.empty(((2 << LOG_LEN) - 1, 32), dtype=torch.uint8, device=d)]
-        self.folded = []
-        cur = LOG_LEN
-        for i in range(N_FOLDS):
-            out_len = cur if i == 0 else cur - FOLD_ARITY
-            self.folded.append(torch.empty((1 << out_len, 2), dtype=torch.int64, device=d))
-            leaves = out_len - FOLD_ARITY
-            self.nodes.append(torch.empty(((2 << leaves) - 1, 32), dtype=torch.uint8, device=d))
-            cur = out_len
-        rng = np.random.default_rng(SEED)
-        self.ch = [fold_challenges(rng, LOG_BATCH)] + [fold_challenges(rng, FOLD_ARITY)
-                                                        for _ in range(N_FOLDS - 1)]
-        self.ch_ptrs = [c.ctypes.data_as(ctypes.c_void_p) for c in self.ch]
 
-    def step(self, stream):
-        L, chk = self.L, self.check
-        s = stream.cuda_stream
-        chk(L.binius_fri_commit_interleaved(self.ntt.handle, self.msg.data_ptr(), self.log_dim,
-                                            LOG_INV_RATE, LOG_BATCH, self.codeword.data_ptr(),
-                                            self.nodes[0].data_ptr(), None, s))
-        chk(L.binius_fri_fold_interleaved(self.codeword.data_ptr(), LOG_LEN, LOG_BATCH,
-                                          self.ch_ptrs[0], self.folded[0].data_ptr(), s))
-        chk(L.binius_merkle_commit(self.folded[0].data_ptr(), LOG_LEN - FOLD_ARITY, FOLD_ARITY,
-                                   self.nodes[1].data_ptr(), s))
-        cur = LOG_LEN
-        for i in range(1, N_FOLDS):
-            chk(L.binius_fri_fold_codeword(self.ntt.handle, self.folded[i - 1].data_ptr(), cur,
-                                           self.ch_ptrs[i], FOLD_ARITY, self.folded[i].data_ptr(),
-                                           s))
-            cur -= FOLD_ARITY
-            chk(L.binius_merkle_commit(self.folded[i].data_ptr(), cur - FOLD_ARITY, FOLD_ARITY,
-                                       self.nodes[i + 1].data_ptr(), s))
+def commit_point(torch, device, stream, L, R, b, warm=3, reps=3, flush=None):
+    """One point of the kernel-level FRI commit matrix: CUDA events around the encode, the
+    Merkle commit and the 3 fold rounds of each timed run (a 256 MiB buffer is written between
+    runs to flush L2).  Returns the point's figures."""
+    from binius64_b200.commit_phase import CommitPhase
+    ph = CommitPhase(L, R, b, seed=SEED + 1000 * L + 10 * R + b, device=device)
+    for _ in range(warm):
+        ph.run(stream)
+    torch.cuda.synchronize()
+    enc, mk, folds, step = [], [], [], []
+    for _ in range(reps):
+        if flush is not None:
+            flush.fill_(1)
+        marks = []
+        ph.run(stream, marks)
+        torch.cuda.synchronize()
+        t = [marks[0].elapsed_time(m) for m in marks[1:]]
+        enc.append(t[0])
+        mk.append(t[1] - t[0])
+        folds.append(t[-1] - t[1])
+        step.append(t[-1])
+    peak, _ = measured_peak_hbm()
+    e, m, f, st = (statistics.mean(x) for x in (enc, mk, folds, step))
+    out = {
+        "log_len": L, "log_inv_rate": R, "columns": 1 << b,
+        "codeword_bytes": 16 << (L + b),
+        "step_ms": st, "encode_ms": e, "merkle_ms": m, "folds_ms": f,
+        "encode_gbs": ph.encode_bytes() / (e * 1e-3) / 1e9,
+        "merkle_gbs": ph.merkle_bytes() / (m * 1e-3) / 1e9,
+        "encode_commit_gbs": ph.encode_commit_bytes() / ((e + m) * 1e-3) / 1e9,
+        "step_gbs": ph.algorithmic_bytes() / (st * 1e-3) / 1e9,
+        "ntt_gf_mults_per_s": ph.ntt_gf_mults() / (e * 1e-3),
+        "sha256_compressions_per_s": ph.merkle_compressions() / (m * 1e-3),
+    }
+    out["encode_commit_frac"] = out["encode_commit_gbs"] / peak
+    out["step_frac"] = out["step_gbs"] / peak
+    ph.release()
+    del ph
+    torch.cuda.empty_cache()
+    return out
+
+
+def commit_matrix(torch, device, stream, points=C2_POINTS, warm=3, reps=3):
+    """Every point of the C2 matrix, smallest first; peak HBM held: the largest point's buffers
+    (25.3 GiB at log_len 24, R=1, 64 columns)."""
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")
+    res = [commit_point(torch, device, stream, L, R, b, warm, reps, flush)
+           for (L, R, b) in sorted(points, key=lambda p: p[0] + p[2] - p[1])]
+    peak, kind = measured_peak_hbm()
+    return {"peak_gbs": peak, "peak_kind": kind, "warmup": warm, "reps": reps,
+            "l2": "256 MiB buffer written between timed runs", "points": res}
 
 
 def run_cpu_commit(threads):
@@ -653,6 +709,7 @@ def run_cpu_commit(threads):
 def run_commit(args, rank, world, local):
     import torch
     from binius64_b200._ffi import lib
+    from binius64_b200.commit_phase import CommitPhase
 
     torch.cuda.set_device(local)
     pg = None
@@ -662,9 +719,10 @@ def run_commit(args, rank, world, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
     stream = torch.cuda.current_stream()
-    pipe = GpuPipeline(torch, local)
+    pipe = CommitPhase(LOG_LEN, LOG_INV_RATE, LOG_BATCH, N_FOLDS, FOLD_ARITY, seed=SEED,
+                       device=local)
     for _ in range(args.warmup):
-        pipe.step(stream)
+        pipe.run(stream)
     torch.cuda.synchronize()
     launches0 = lib().binius_launch_count()
     if pg:
@@ -674,7 +732,7 @@ def run_commit(args, rank, world, local):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
-        pipe.step(stream)
+        pipe.run(stream)
     ev1.record(stream)
     torch.cuda.synchronize()
     clocks = sample_clocks_stop(clk)
@@ -701,23 +759,29 @@ def run_commit(args, rank, world, local):
     peak, peak_kind = measured_peak_hbm()
     mults_per_launch = (n_layers / n_passes) * (1 << (LOG_LEN + LOG_BATCH - 1))
 
-    host_msg = torch.empty_like(pipe.msg, device="cpu").pin_memory()
-    host_msg.copy_(pipe.msg.cpu())
-    host_out = torch.empty_like(pipe.folded[-1], device="cpu").pin_memory()
-    host_roots = torch.empty((len(pipe.nodes), 32), dtype=torch.uint8).pin_memory()
+    host_msg = torch.empty_like(pipe.message, device="cpu").pin_memory()
+    host_msg.copy_(pipe.message.cpu())
+    last = pipe.rounds[-1][3]
+    host_out = torch.empty_like(last, device="cpu").pin_memory()
+    trees = [pipe.nodes] + [r[4] for r in pipe.rounds]
+    host_roots = torch.empty((len(trees), 32), dtype=torch.uint8).pin_memory()
     h2d = host_msg.numel() * 8
     d2h = host_out.numel() * 8 + host_roots.numel()
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(args.steps):
-        pipe.msg.copy_(host_msg, non_blocking=True)
-        pipe.step(stream)
-        host_out.copy_(pipe.folded[-1], non_blocking=True)
-        for i, nd in enumerate(pipe.nodes):
+        pipe.message.copy_(host_msg, non_blocking=True)
+        pipe.run(stream)
+        host_out.copy_(last, non_blocking=True)
+        for i, nd in enumerate(trees):
             host_roots[i].copy_(nd[-1], non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.steps
+    pipe.release()
+    del pipe
+    torch.cuda.empty_cache()
+    matrix = commit_matrix(torch, local, stream) if (world == 1 and args.log_len is None) else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -741,6 +805,7 @@ def run_commit(args, rank, world, local):
                          "launch_ms": launch_ms, "algorithmic_bytes_per_launch": bytes_per_launch,
                          "gf_mults_per_launch": mults_per_launch,
                          "gf_mults_per_s": mults_per_launch / (launch_ms * 1e-3)},
+            "matrix": matrix,
             "cpu_baseline": cpu,
             "clocks": clocks,
         }

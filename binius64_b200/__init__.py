@@ -279,13 +279,20 @@ def standard_domain_rs_basis(log_code_len: int, log_batch: int, device=None) -> 
     """Basis of the RS code subspace chosen by Verifier::setup (verify.rs:85-97): row `log_batch` of
     the normalized subspace-polynomial evaluations of the standard domain of dim log_code_len
     (GenericOnTheFly::subspace)."""
-    big = AdditiveNTT(log_code_len, device=device)
-    n = log_code_len - log_batch
-    base = (1 << (log_code_len - 1 - log_batch)) - 1
-    idx = [base + (1 << k) for k in range(n - 1)]
-    tw = to_host(big.twiddles(copy=False)[idx]) if idx else np.zeros((0, 2), dtype=np.uint64)
-    del big
-    return [1] + [int(t[0]) | (int(t[1]) << 64) for t in tw]
+    return domain_subspace(log_code_len, log_code_len - log_batch)
+
+
+def domain_subspace(log_domain: int, dim: int, basis=None) -> list[int]:
+    """DomainContext::subspace(dim) (verifier/math/src/ntt/domain_context.rs:142-147) of the domain
+    of dimension log_domain over `basis` (default: BinarySubspace::with_dim, basis x^i), computed
+    on the host without the twiddle table."""
+    out = np.zeros((max(dim, 1), 2), dtype=np.uint64)
+    b = None
+    if basis is not None:
+        b = np.array([[int(v) & ((1 << 64) - 1), int(v) >> 64] for v in basis], dtype=np.uint64)
+    check(lib().binius_domain_subspace(None if b is None else b.ctypes.data, log_domain, dim,
+                                       out.ctypes.data))
+    return [int(t[0]) | (int(t[1]) << 64) for t in out[:dim]]
 
 
 @dataclass

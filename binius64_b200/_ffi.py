@@ -54,6 +54,7 @@ _SIGS = {
     "binius_ntt_create": (_int, [_int, _vp, _u32, _c.POINTER(_vp)]),
     "binius_ntt_destroy": (_int, [_vp]),
     "binius_ntt_log_domain": (_u32, [_vp]),
+    "binius_domain_subspace": (_int, [_vp, _u32, _u32, _vp]),
     "binius_ntt_twiddles": (_vp, [_vp]),
     "binius_ntt_forward": (_int, [_vp, _vp, _u32, _u32, _u32, _vp]),
     "binius_ntt_inverse": (_int, [_vp, _vp, _u32, _u32, _u32, _vp]),

@@ -299,6 +299,37 @@ def _random_term_arrays(rng, n, pool_lo, pool_hi, max_terms):
     return idx, variant, amount, counts
 
 
+def shifted_by(words: np.ndarray, variant: int, amounts: np.ndarray) -> np.ndarray:
+    """shifted() with a per-word shift amount (same variant for all words)."""
+    w = words.astype(np.uint64)
+    a = amounts.astype(np.uint64)
+    if variant == SLL:
+        return w << a
+    if variant == SLR:
+        return w >> a
+    if variant == SAR:
+        return (w.view(np.int64) >> a.astype(np.int64)).view(np.uint64)
+    if variant == ROTR:
+        rot = (w >> a) | (w << ((np.uint64(64) - a) & np.uint64(63)))
+        return np.where(a == 0, w, rot)
+    lo = (w & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+    hi = (w >> np.uint64(32)).astype(np.uint32)
+    s = (a & np.uint64(31)).astype(np.uint32)
+    if variant == SLL32:
+        lo2, hi2 = lo << s, hi << s
+    elif variant == SRL32:
+        lo2, hi2 = lo >> s, hi >> s
+    elif variant == SRA32:
+        si = s.astype(np.int32)
+        lo2 = (lo.view(np.int32) >> si).view(np.uint32)
+        hi2 = (hi.view(np.int32) >> si).view(np.uint32)
+    else:  # ROTR32
+        r = (np.uint32(32) - s) & np.uint32(31)
+        lo2 = np.where(s == 0, lo, (lo >> s) | (lo << r))
+        hi2 = np.where(s == 0, hi, (hi >> s) | (hi << r))
+    return (hi2.astype(np.uint64) << np.uint64(32)) | lo2.astype(np.uint64)
+
+
 def _eval_term_arrays(values, idx, variant, amount, counts):
     n, m = idx.shape
     acc = np.zeros(n, dtype=np.uint64)
@@ -308,13 +339,9 @@ def _eval_term_arrays(values, idx, variant, amount, counts):
         res = np.zeros(n, dtype=np.uint64)
         for v in range(8):
             for_v = (variant[:, j] == v) & active
-            if not for_v.any():
-                continue
-            amts = np.unique(amount[for_v, j])
-            for a in amts:
-                sel = for_v & (amount[:, j] == a)
-                res[sel] = shifted(w[sel], v, int(a))
-        acc ^= np.where(active, res, np.uint64(0))
+            if for_v.any():
+                res[for_v] = shifted_by(w[for_v], v, amount[for_v, j])
+        acc ^= res
     return acc
 
 

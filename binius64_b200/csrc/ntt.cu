@@ -227,14 +227,12 @@ int rs_encode_batch(const binius_ntt* ntt, const void* d_msg, uint32_t log_dim,
 
 }  // namespace bgpu
 
-extern "C" {
+namespace {
 
-int binius_ntt_create(int device, const void* h_basis, uint32_t log_domain, binius_ntt** out) {
-  BGPU_ARG(out != nullptr, "out is NULL");
-  *out = nullptr;
-  BGPU_ARG(log_domain >= 1 && log_domain <= 32, "log_domain must be in [1, 32]");
-  if (int rc = configure_device_pool(device)) return rc;
-  const uint32_t l = log_domain;
+// generate_evals_from_subspace (ntt/domain_context.rs:19-46): row i holds the normalized
+// subspace-polynomial evaluations [W_i(b_i), W_i(b_(i+1)), ...] / W_i(b_i) of the domain basis
+// (h_basis: l elements, or NULL for BinarySubspace::with_dim's basis x^i).
+int subspace_evals(const void* h_basis, uint32_t l, std::vector<std::vector<hu128>>& evals) {
   std::vector<hu128> basis(l);
   for (uint32_t i = 0; i < l; i++) {
     if (h_basis) {
@@ -244,8 +242,7 @@ int binius_ntt_create(int device, const void* h_basis, uint32_t log_domain, bini
       basis[i] = (hu128)1 << i;
     }
   }
-  // generate_evals_from_subspace (ntt/domain_context.rs:19-46).
-  std::vector<std::vector<hu128>> evals;
+  evals.clear();
   evals.push_back(basis);
   for (uint32_t i = 1; i < l; i++) {
     const auto& prev = evals[i - 1];
@@ -258,6 +255,37 @@ int binius_ntt_create(int device, const void* h_basis, uint32_t log_domain, bini
     hu128 inv = host_gf_inv(row[0]);
     for (auto& v : row) v = host_gf_mul(v, inv);
   }
+  return BINIUS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int binius_domain_subspace(const void* h_basis, uint32_t log_domain, uint32_t dim, void* h_out) {
+  BGPU_ARG(h_out != nullptr, "out is NULL");
+  BGPU_ARG(log_domain >= 1 && log_domain <= 64, "log_domain must be in [1, 64]");
+  BGPU_ARG(dim <= log_domain, "dim must be <= log_domain");
+  uint64_t* o = static_cast<uint64_t*>(h_out);
+  if (dim == 0) return clear_error();  // BinarySubspace::with_dim(0)
+  std::vector<std::vector<hu128>> evals;
+  if (int rc = subspace_evals(h_basis, log_domain, evals)) return rc;
+  const auto& row = evals[log_domain - dim];
+  for (uint32_t i = 0; i < dim; i++) {
+    o[2 * i] = (uint64_t)row[i];
+    o[2 * i + 1] = (uint64_t)(row[i] >> 64);
+  }
+  return clear_error();
+}
+
+int binius_ntt_create(int device, const void* h_basis, uint32_t log_domain, binius_ntt** out) {
+  BGPU_ARG(out != nullptr, "out is NULL");
+  *out = nullptr;
+  BGPU_ARG(log_domain >= 1 && log_domain <= 32, "log_domain must be in [1, 32]");
+  if (int rc = configure_device_pool(device)) return rc;
+  const uint32_t l = log_domain;
+  std::vector<std::vector<hu128>> evals;
+  if (int rc = subspace_evals(h_basis, l, evals)) return rc;
   std::vector<uint32_t> offsets(l);
   std::vector<uint64_t> packed;
   for (uint32_t i = 0; i < l; i++) {

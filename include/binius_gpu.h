@@ -54,6 +54,13 @@ typedef struct binius_ntt binius_ntt;
  * h_basis: log_domain field elements, or NULL for BinarySubspace::with_dim (basis x^i). */
 int binius_ntt_create(int device, const void* h_basis, uint32_t log_domain, binius_ntt** out);
 int binius_ntt_destroy(binius_ntt* ntt);
+/* DomainContext::subspace(dim) (ntt/domain_context.rs:142-147) of the domain a binius_ntt_create
+ * with the same h_basis / log_domain would build, computed on the host without building the
+ * twiddle table: h_out receives dim field elements (the subspace of dimension dim, as the
+ * normalized subspace-polynomial evaluations evals[log_domain - dim]).  The Reed-Solomon code of
+ * an interleaved commitment of 2^log_batch columns over the standard domain of dimension
+ * log_len + log_batch uses subspace(log_len) (verifier/verifier/src/verify.rs:85-97). */
+int binius_domain_subspace(const void* h_basis, uint32_t log_domain, uint32_t dim, void* h_out);
 /* log2 of the domain size (DomainContext::log_domain_size). */
 uint32_t binius_ntt_log_domain(const binius_ntt* ntt);
 /* Device pointer of the flat twiddle table (DomainContext::twiddle(layer, block) is entry
