@@ -284,7 +284,7 @@ def vision4_kernels(torch, bg, device, stream):
 
 
 def bivariate_roofline(torch, bg, lib, device, stream, reps=20):
-    """Live timing of binius_sumcheck_bivariate_fold_execute on 2^20-element operands (the first
+    """Live timing of binius_bivariate_fold_round_evals on 2^20-element operands (the first
     folded round of shift phase 2): algorithmic bytes = read a, b (2 x 16 MiB) + write the folded
     halves (2 x 8 MiB)."""
     log_len = 20
@@ -301,7 +301,7 @@ def bivariate_roofline(torch, bg, lib, device, stream, reps=20):
     for _ in range(3):
         a.copy_(a0)
         b.copy_(b0)
-        lib.binius_sumcheck_bivariate_fold_execute(a.data_ptr(), b.data_ptr(), log_len, r,
+        lib.binius_bivariate_fold_round_evals(a.data_ptr(), b.data_ptr(), log_len, r,
                                                    out.data_ptr(), s)
     torch.cuda.synchronize()
     tot = 0.0
@@ -310,7 +310,7 @@ def bivariate_roofline(torch, bg, lib, device, stream, reps=20):
         b.copy_(b0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        lib.binius_sumcheck_bivariate_fold_execute(a.data_ptr(), b.data_ptr(), log_len, r,
+        lib.binius_bivariate_fold_round_evals(a.data_ptr(), b.data_ptr(), log_len, r,
                                                    out.data_ptr(), s)
         e1.record(stream)
         torch.cuda.synchronize()

@@ -171,11 +171,14 @@ class MerkleCommitted:
     def root(self) -> bytes:
         return bytes(self.nodes[-1].cpu().numpy().tobytes())
 
-    def layer(self, layer_depth: int):
-        if layer_depth > self.log_len:
-            raise ArgumentError(1, "IncorrectLayerDepth")
-        start = self.nodes.shape[0] + 1 - (1 << (layer_depth + 1))
-        return self.nodes[start:start + (1 << layer_depth)]
+    def layer(self, layer_depth: int, stream=None) -> list[bytes]:
+        """MerkleTreeProver::layer (prover/prover/src/merkle_tree/mod.rs:50-55): the digests at
+        depth layer_depth (0 = the root), copied to the host."""
+        buf = (ctypes.c_uint8 * (32 << max(0, min(layer_depth, 40))))()
+        check(lib().binius_merkle_layer(_ptr(self.nodes), self.log_len, layer_depth,
+                                        ctypes.addressof(buf), _stream(stream)))
+        raw = bytes(buf)
+        return [raw[32 * i: 32 * (i + 1)] for i in range(1 << layer_depth)]
 
     def branch(self, index: int, layer_depth: int, stream=None) -> list[bytes]:
         n = self.log_len - layer_depth
@@ -350,6 +353,126 @@ def fold_codeword(ntt: AdditiveNTT, codeword, challenges, log_len: int, out=None
     check(lib().binius_fri_fold_codeword(ntt.handle, _ptr(codeword), log_len, buf, len(challenges),
                                          _ptr(out), _stream(stream)))
     return out
+
+
+# ------------------------------------------------------------------ round-by-round sumchecks
+
+def _elem_buf(v: int):
+    return (ctypes.c_uint8 * 16)(*int(v).to_bytes(16, "little"))
+
+
+def _elems_from(buf, n: int) -> list[int]:
+    raw = bytes(buf)
+    return [int.from_bytes(raw[16 * i:16 * (i + 1)], "little") for i in range(n)]
+
+
+class _SumcheckProver:
+    """The SumcheckProver trait (prover/prover/src/protocols/sumcheck/common.rs:29-101) over a
+    device prover: execute() -> the round's RoundCoeffs (lowest degree first), fold(challenge),
+    finish() -> the multilinears' evaluations.  The multilinears are device tensors folded in
+    place; they must stay alive and untouched until finish()."""
+
+    _kind = ""
+    _n_evals = 0
+
+    def __init__(self):
+        self._h = ctypes.c_void_p()
+        self._keep = ()
+
+    def n_vars(self) -> int:
+        return int(lib().binius_sumcheck_n_vars(self._h))
+
+    def execute(self) -> list[int]:
+        buf = (ctypes.c_uint8 * 48)()
+        n = ctypes.c_uint32(0)
+        check(getattr(lib(), f"binius_sumcheck_{self._kind}_execute")(self._h, buf,
+                                                                      ctypes.byref(n)))
+        return _elems_from(buf, n.value)
+
+    def fold(self, challenge: int) -> None:
+        check(getattr(lib(), f"binius_sumcheck_{self._kind}_fold")(self._h, _elem_buf(challenge)))
+
+    def finish(self) -> list[int]:
+        buf = (ctypes.c_uint8 * (16 * self._n_evals))()
+        check(getattr(lib(), f"binius_sumcheck_{self._kind}_finish")(self._h, buf))
+        return _elems_from(buf, self._n_evals)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().binius_sumcheck_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
+def _points_buf(point):
+    arr = np.array([[int(c) & (2**64 - 1), int(c) >> 64] for c in point] or [[0, 0]],
+                   dtype=np.uint64)
+    return arr
+
+
+class BivariateProductSumcheckProver(_SumcheckProver):
+    """BivariateProductSumcheckProver::new([a, b], sum)
+    (prover/prover/src/protocols/sumcheck/bivariate_product.rs:17-119)."""
+
+    _kind, _n_evals = "bivariate", 2
+
+    def __init__(self, a, b, sum: int, stream=None):
+        super().__init__()
+        n = _log2_exact(_elems_of(a), "multilinear length")
+        if _elems_of(b) != _elems_of(a):
+            raise ArgumentError(1, "MultilinearSizeMismatch")
+        check(lib().binius_sumcheck_bivariate_create(_ptr(a), _ptr(b), n, _elem_buf(sum),
+                                                     _stream(stream), ctypes.byref(self._h)))
+        self._keep = (a, b)
+
+
+class QuadraticMleCheckProver(_SumcheckProver):
+    """QuadraticMleCheckProver::new([a, b, c], a*b - c, a*b, eval_point, eval_claim)
+    (prover/prover/src/protocols/sumcheck/quadratic_mle.rs:21-229), the AND reduction's
+    MLE-check."""
+
+    _kind, _n_evals = "quadratic_mle", 3
+
+    def __init__(self, a, b, c, eval_point, eval_claim: int, stream=None):
+        super().__init__()
+        n = len(eval_point)
+        for m in (a, b, c):
+            if _elems_of(m) != 1 << n:
+                raise ArgumentError(1, "MultilinearSizeMismatch")
+        pts = _points_buf(eval_point)
+        check(lib().binius_sumcheck_quadratic_mle_create(
+            _ptr(a), _ptr(b), _ptr(c), n, pts.ctypes.data, _elem_buf(eval_claim), _stream(stream),
+            ctypes.byref(self._h)))
+        self._keep = (a, b, c)
+
+    def eval_point(self) -> list[int]:
+        buf = (ctypes.c_uint8 * (16 * max(1, self.n_vars())))()
+        check(lib().binius_sumcheck_quadratic_mle_eval_point(self._h, buf))
+        return _elems_from(buf, self.n_vars())
+
+
+class InOutCheckProver(_SumcheckProver):
+    """InOutCheckProver::new(witness, eval_point) (prover/prover/src/protocols/inout_check.rs:
+    19-221): eval_point has log_public coordinates, the public segment's."""
+
+    _kind, _n_evals = "inout", 1
+
+    def __init__(self, witness, eval_point, stream=None):
+        super().__init__()
+        n = _log2_exact(_elems_of(witness), "witness length")
+        pts = _points_buf(eval_point)
+        check(lib().binius_sumcheck_inout_create(_ptr(witness), n, pts.ctypes.data,
+                                                 len(eval_point), _stream(stream),
+                                                 ctypes.byref(self._h)))
+        self._keep = (witness,)
+
+    def eval_point(self) -> list[int]:
+        buf = (ctypes.c_uint8 * (16 * max(1, self.n_vars())))()
+        check(lib().binius_sumcheck_inout_eval_point(self._h, buf))
+        return _elems_from(buf, self.n_vars())
 
 
 def gf_mul_batch(a, b, out=None, stream=None):
@@ -629,11 +752,31 @@ class Prover:
         # setup_sha256 / setup_vision4 (prover/examples/src/lib.rs:48-85)
         self.merkle_hash = merkle_hash
         check(lib().binius_prover_set_merkle_hash(self._h, hash_id))
+        self._load_info()
+
+    def _load_info(self):
         info = (ctypes.c_uint32 * 12)()
         check(lib().binius_prover_info(self._h, ctypes.addressof(info)))
         v = list(info)
         self.log_witness_elems, self.log_batch, self.log_inv_rate, self.n_queries = v[:4]
         self.fold_arities = v[5:5 + v[4]]
+
+    def prove_host(self, words, transcript: ProverTranscript | None = None, stream=None) -> bytes:
+        """Prover::prove over a host witness (committed_total_len uint64 words) through
+        binius_prove: the witness is copied in and the finalized proof bytes come back."""
+        w = np.ascontiguousarray(words, dtype=np.uint64)
+        n = ctypes.c_size_t(0)
+        cap = 1 << 20
+        t = transcript.handle if transcript is not None else None
+        while True:
+            buf = (ctypes.c_uint8 * cap)()
+            rc = lib().binius_prove(self._h, w.ctypes.data, len(w), t, buf, cap, ctypes.byref(n),
+                                    _stream(stream))
+            if rc == 1 and n.value > cap and t is None:  # too small: prove again with room
+                cap = n.value
+                continue
+            check(rc)
+            return bytes(buf)[: n.value]
 
     def prove(self, witness_words, transcript: ProverTranscript | None = None,
               stream=None) -> ProverTranscript:
@@ -663,6 +806,32 @@ class Prover:
             except Exception:
                 pass
             self._h = None
+
+
+class _OwnedConstraintSystem:
+    """The constraint system a prover from setup() owns: its witness length and device."""
+
+    def __init__(self, committed_total_len: int, device: int):
+        self.committed_total_len = committed_total_len
+        self.device = device
+
+
+def setup(cs_bytes: bytes, log_inv_rate: int = 1, key_collection: bytes | None = None,
+          device: int | None = None) -> Prover:
+    """binius_setup: ConstraintSystem::deserialize then Prover::setup (or
+    setup_with_key_collection) in one call (prover/prover/src/prove.rs:81-121); the prover owns
+    its constraint system."""
+    torch = _torch()
+    dev = torch.cuda.current_device() if device is None else int(device)
+    p = Prover.__new__(Prover)
+    p._h = ctypes.c_void_p()
+    kc = key_collection
+    check(lib().binius_setup(dev, cs_bytes, len(cs_bytes), log_inv_rate, kc,
+                             len(kc) if kc else 0, ctypes.byref(p._h)))
+    p.cs = _OwnedConstraintSystem(int(lib().binius_prover_committed_words(p._h)), dev)
+    p.merkle_hash = "sha256"
+    p._load_info()
+    return p
 
 
 # ---------------------------------------------------------------------------------------- formats

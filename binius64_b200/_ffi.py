@@ -61,6 +61,7 @@ _SIGS = {
     "binius_rs_encode_batch": (_int, [_vp, _vp, _u32, _u32, _u32, _vp, _vp]),
     "binius_merkle_commit": (_int, [_vp, _u32, _u32, _vp, _vp]),
     "binius_merkle_branch": (_int, [_vp, _u32, _u64, _u32, _vp, _vp]),
+    "binius_merkle_layer": (_int, [_vp, _u32, _u32, _vp, _vp]),
     "binius_fri_fold_interleaved": (_int, [_vp, _u32, _u32, _vp, _vp, _vp]),
     "binius_fri_fold_codeword": (_int, [_vp, _vp, _u32, _vp, _u32, _vp, _vp]),
     "binius_fri_fold_codeword_noalloc": (_int, [_vp, _vp, _u32, _vp, _u32, _vp, _vp]),
@@ -112,6 +113,10 @@ _SIGS = {
     "binius_shift_reduction_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "binius_intmul_reduction_prove": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "binius_prover_setup": (_int, [_vp, _u32, _vp]),
+    "binius_setup": (_int, [_int, _c.c_char_p, _c.c_size_t, _u32, _c.c_char_p, _c.c_size_t,
+                            _vp]),
+    "binius_prove": (_int, [_vp, _vp, _c.c_size_t, _vp, _vp, _c.c_size_t,
+                            _c.POINTER(_c.c_size_t), _vp]),
     "binius_prover_destroy": (_int, [_vp]),
     "binius_prover_info": (_int, [_vp, _vp]),
     "binius_prover_prove": (_int, [_vp, _vp, _vp, _vp]),
@@ -128,8 +133,24 @@ _SIGS = {
     "binius_fri_n_test_queries": (_u32, [_u32, _u32]),
     "binius_fri_estimate_optimal_arity": (_u32, [_u32, _u32, _u32]),
     "binius_gf_mul_batch": (_int, [_vp, _vp, _vp, _u64, _vp]),
-    "binius_sumcheck_bivariate_execute": (_int, [_vp, _vp, _u32, _vp, _vp]),
-    "binius_sumcheck_bivariate_fold_execute": (_int, [_vp, _vp, _u32, _vp, _vp, _vp]),
+    "binius_bivariate_round_evals": (_int, [_vp, _vp, _u32, _vp, _vp]),
+    "binius_bivariate_fold_round_evals": (_int, [_vp, _vp, _u32, _vp, _vp, _vp]),
+    "binius_sumcheck_bivariate_create": (_int, [_vp, _vp, _u32, _vp, _vp, _vp]),
+    "binius_sumcheck_bivariate_execute": (_int, [_vp, _vp, _vp]),
+    "binius_sumcheck_bivariate_fold": (_int, [_vp, _vp]),
+    "binius_sumcheck_bivariate_finish": (_int, [_vp, _vp]),
+    "binius_sumcheck_quadratic_mle_create": (_int, [_vp, _vp, _vp, _u32, _vp, _vp, _vp, _vp]),
+    "binius_sumcheck_quadratic_mle_execute": (_int, [_vp, _vp, _vp]),
+    "binius_sumcheck_quadratic_mle_fold": (_int, [_vp, _vp]),
+    "binius_sumcheck_quadratic_mle_finish": (_int, [_vp, _vp]),
+    "binius_sumcheck_quadratic_mle_eval_point": (_int, [_vp, _vp]),
+    "binius_sumcheck_inout_create": (_int, [_vp, _u32, _vp, _u32, _vp, _vp]),
+    "binius_sumcheck_inout_execute": (_int, [_vp, _vp, _vp]),
+    "binius_sumcheck_inout_fold": (_int, [_vp, _vp]),
+    "binius_sumcheck_inout_finish": (_int, [_vp, _vp]),
+    "binius_sumcheck_inout_eval_point": (_int, [_vp, _vp]),
+    "binius_sumcheck_n_vars": (_u32, [_vp]),
+    "binius_sumcheck_destroy": (_int, [_vp]),
 }
 
 _lib = None

@@ -572,6 +572,15 @@ namespace bgpu {
 void lagrange_phi(uint32_t dim, hu128 x, hu128* out) { lagrange_b128(dim, x, out); }
 hu128 phi_elem(uint32_t b) { return and_constants().phi[b & 255]; }
 
+int and_mle_eval(const uint4* d_a, const uint4* d_b, const uint4* d_c, const uint4* d_eq,
+                 uint64_t half, uint32_t* d_out8, cudaStream_t s) {
+  BGPU_CUDA(cudaMemsetAsync(d_out8, 0, 32, s));
+  and_mle_eval_kernel<<<grid_for(half, 256), 256, 0, s>>>(d_a, d_b, d_c, d_eq, half, d_out8);
+  BGPU_LAUNCH_CHECK("and_mle_eval_kernel");
+  count_launch();
+  return BINIUS_OK;
+}
+
 int fold_words64(const uint64_t* d_words, uint64_t n, const hu128* vec64, uint4* d_out,
                  cudaStream_t s) {
   if (n == 0) return BINIUS_OK;

@@ -68,6 +68,10 @@ constexpr uint64_t kMulTableMinSize = 1ull << 15;
 // (BinarySubspace::<AESTowerField8b>::with_dim(dim).isomorphic(), lagrange_evals).
 void lagrange_phi(uint32_t dim, hu128 x, hu128* out);
 hu128 phi_elem(uint32_t b);
+// d_out8 = (y_1, y_inf) of the AND reduction's MLE-check round on columns a, b, c of length
+// 2 * half with eq of length half: y_1 = sum eq (a_1 b_1 + c_1), y_inf = sum eq a_inf b_inf.
+int and_mle_eval(const uint4* d_a, const uint4* d_b, const uint4* d_c, const uint4* d_eq,
+                 uint64_t half, uint32_t* d_out8, cudaStream_t s);
 // d_out[i] = sum over set bits t of d_words[i] of vec64[t] (fold_words, prover/prover/src/
 // fold_word.rs:77-96).
 int fold_words64(const uint64_t* d_words, uint64_t n, const hu128* vec64, uint4* d_out,

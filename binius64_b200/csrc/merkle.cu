@@ -178,4 +178,18 @@ int binius_merkle_branch(const void* d_nodes, uint32_t log_leaves, uint64_t inde
   return clear_error();
 }
 
+int binius_merkle_layer(const void* d_nodes, uint32_t log_leaves, uint32_t layer_depth,
+                        void* h_out, void* stream) {
+  BGPU_ARG(d_nodes != nullptr && h_out != nullptr, "nodes / out is NULL");
+  BGPU_ARG(log_leaves <= 40, "log_leaves too large");
+  BGPU_ARG(layer_depth <= log_leaves, "IncorrectLayerDepth");
+  // BinaryMerkleTree::layer: the 2^depth digests that end 2^depth - 1 digests before the end
+  const uint64_t total = (2ull << log_leaves) - 1;
+  const uint64_t start = total + 1 - (2ull << layer_depth);
+  if (int rc = read_sync(h_out, static_cast<const uint8_t*>(d_nodes) + 32 * start,
+                         32ull << layer_depth, as_stream(stream)))
+    return rc;
+  return clear_error();
+}
+
 }  // extern "C"

@@ -24,6 +24,7 @@ using namespace bgpu;
 
 struct binius_prover {
   const binius_cs* cs = nullptr;
+  binius_cs* owned_cs = nullptr;  // binius_setup: the constraint system lives with the prover
   binius_ntt* ntt = nullptr;
   binius_pcs* pcs = nullptr;
   uint32_t log_inv_rate = 0, log_witness_elems = 0, log_batch = 0, n_queries = 0;
@@ -116,8 +117,27 @@ int binius_prover_destroy(binius_prover* P) {
   if (!P) return BINIUS_OK;
   binius_pcs_destroy(P->pcs);
   binius_ntt_destroy(P->ntt);
+  binius_cs_destroy(P->owned_cs);
   delete P;
   return BINIUS_OK;
+}
+
+int binius_setup(int device, const void* h_cs_bytes, size_t cs_len, uint32_t log_inv_rate,
+                 const void* h_kc, size_t kc_len, binius_prover** out) {
+  BGPU_ARG(h_cs_bytes && out, "NULL argument");
+  *out = nullptr;
+  binius_cs* cs = nullptr;
+  if (int rc = binius_cs_from_bytes(device, h_cs_bytes, cs_len, &cs)) return rc;
+  binius_prover* P = nullptr;
+  int rc = h_kc ? binius_prover_setup_with_key_collection(cs, log_inv_rate, h_kc, kc_len, &P)
+                : binius_prover_setup(cs, log_inv_rate, &P);
+  if (rc) {
+    binius_cs_destroy(cs);
+    return rc;
+  }
+  P->owned_cs = cs;
+  *out = P;
+  return clear_error();
 }
 
 int binius_prover_info(const binius_prover* P, uint32_t* h_out12) {
@@ -211,6 +231,42 @@ int binius_prover_prove(const binius_prover* P, const void* d_witness,
   } while (0);
   binius_pcs_committed_destroy(committed);
   if (!rc && fresh_arena) prover_note_footprint(P, arena_held_bytes());
+  return rc ? rc : clear_error();
+}
+
+int binius_prove(const binius_prover* P, const uint64_t* h_words, size_t n_words,
+                 binius_transcript* transcript, void* h_proof, size_t cap, size_t* len,
+                 void* stream) {
+  BGPU_ARG(P && h_words && len, "NULL argument");
+  *len = 0;
+  BGPU_ARG(n_words == P->cs->committed_total_len,
+           "witness length != the constraint system's committed_total_len");
+  int prev = 0;
+  BGPU_CUDA(cudaGetDevice(&prev));
+  if (prev != P->cs->device) BGPU_CUDA(cudaSetDevice(P->cs->device));
+  cudaStream_t s = as_stream(stream);
+  binius_transcript fresh;
+  binius_transcript* t = transcript ? transcript : &fresh;
+  int rc = BINIUS_OK;
+  {
+    // the witness copy and every buffer of the proof come from one arena, released at the end
+    ArenaScope arena(s, false);
+    void* d_w = nullptr;
+    cudaError_t e = dev_alloc(&d_w, 8 * n_words, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_w, h_words, 8 * n_words, cudaMemcpyHostToDevice, s);
+    rc = e != cudaSuccess ? cuda_error(e, "witness upload")
+                          : binius_prover_prove(P, d_w, t, stream);
+    if (!rc) {
+      *len = t->t.tape().size();
+      if (cap < *len || (!h_proof && *len))
+        rc = set_error(BINIUS_E_ARG, "proof buffer too small (len set)");
+      else if (*len)
+        memcpy(h_proof, t->t.tape().data(), *len);
+    }
+    stream_wait(s);
+  }
+  if (prev != P->cs->device) cudaSetDevice(prev);
   return rc ? rc : clear_error();
 }
 

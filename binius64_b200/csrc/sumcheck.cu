@@ -487,8 +487,8 @@ int gather_segments(const GatherSegment* d_segs, uint32_t n, uint8_t* d_dst, cud
 
 extern "C" {
 
-int binius_sumcheck_bivariate_execute(const void* d_a, const void* d_b, uint32_t log_len,
-                                      void* d_out2, void* stream) {
+int binius_bivariate_round_evals(const void* d_a, const void* d_b, uint32_t log_len,
+                                 void* d_out2, void* stream) {
   BGPU_ARG(d_a && d_b && d_out2, "NULL argument");
   BGPU_ARG(log_len >= 1 && log_len <= 40, "log_len must be in [1, 40]");
   return bivariate_eval(static_cast<const uint4*>(d_a), static_cast<const uint4*>(d_b),
@@ -497,8 +497,8 @@ int binius_sumcheck_bivariate_execute(const void* d_a, const void* d_b, uint32_t
              : clear_error();
 }
 
-int binius_sumcheck_bivariate_fold_execute(void* d_a, void* d_b, uint32_t log_len,
-                                           const void* h_r, void* d_out2, void* stream) {
+int binius_bivariate_fold_round_evals(void* d_a, void* d_b, uint32_t log_len, const void* h_r,
+                                      void* d_out2, void* stream) {
   BGPU_ARG(d_a && d_b && d_out2 && h_r, "NULL argument");
   BGPU_ARG(log_len >= 2 && log_len <= 40, "log_len must be in [2, 40]");
   return bivariate_fold_eval(static_cast<uint4*>(d_a), static_cast<uint4*>(d_b), 1ull << log_len,

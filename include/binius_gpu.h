@@ -105,6 +105,14 @@ int binius_merkle_commit(const void* d_elems, uint32_t log_leaves, uint32_t log_
 int binius_merkle_branch(const void* d_nodes, uint32_t log_leaves, uint64_t index,
                          uint32_t layer_depth, void* h_branch, void* stream);
 
+/* Copies the 2^layer_depth digests of the tree's layer at depth layer_depth (0 = the root,
+ * log_leaves = the leaf digests) into h_out (32 << layer_depth bytes): MerkleTreeProver::layer
+ * (prover/prover/src/merkle_tree/mod.rs:50-55), BinaryMerkleTree::layer
+ * (binary_merkle_tree.rs:142-150); BINIUS_E_ARG "IncorrectLayerDepth" when layer_depth >
+ * log_leaves.  Synchronous. */
+int binius_merkle_layer(const void* d_nodes, uint32_t log_leaves, uint32_t layer_depth,
+                        void* h_out, void* stream);
+
 /* ------------------------------------------------------------------------------------------
  * Vision-4 hash (the `-c vision4` Merkle hash, prover/examples/src/lib.rs:67-85).
  * binius_vision4_permute replaces the Vision-4 permutation over a batch of states
@@ -281,6 +289,21 @@ int binius_prover_set_merkle_hash(binius_prover* prover, uint32_t merkle_hash);
 int binius_prover_info(const binius_prover* prover, uint32_t* h_out12);
 int binius_prover_prove(const binius_prover* prover, const void* d_witness,
                         binius_transcript* transcript, void* stream);
+/* Prover set-up from wire bytes in one call: ConstraintSystem::deserialize (constraint_system.rs:
+ * 615-650) on `device`, then Prover::setup, or Prover::setup_with_key_collection when h_kc (a
+ * serialized KeyCollection v1, key_collection.rs:400-431) is given (prove.rs:81-121).  The prover
+ * owns the constraint system and releases it in binius_prover_destroy. */
+int binius_setup(int device, const void* h_cs_bytes, size_t cs_len, uint32_t log_inv_rate,
+                 const void* h_kc, size_t kc_len, binius_prover** out);
+/* Prover::prove (prove.rs:124-303) over a witness in host memory, returning the proof bytes
+ * (ProverTranscript::finalize, verifier/transcript/src/transcript.rs:245-284): h_words holds the
+ * ValueVec's committed_total_len words; the proof is appended to `transcript` (NULL = a fresh
+ * ProverTranscript of the default challenger) and its whole tape copied to h_proof.  *len is
+ * always set; a too-small buffer returns BINIUS_E_ARG.  Synchronous on `stream`; the witness copy
+ * and every buffer of the proof are released before it returns. */
+int binius_prove(const binius_prover* prover, const uint64_t* h_words, size_t n_words,
+                 binius_transcript* transcript, void* h_proof, size_t cap, size_t* len,
+                 void* stream);
 /* committed_total_len of the prover's constraint system (the witness length in words). */
 uint64_t binius_prover_committed_words(const binius_prover* prover);
 /* Estimate of the device memory one proof allocates while it runs (admission of concurrent
@@ -439,18 +462,62 @@ uint32_t binius_fri_estimate_optimal_arity(uint32_t log_block_length, uint32_t d
                                            uint32_t field_size);
 
 /* ------------------------------------------------------------------------------------------
- * Bivariate product sumcheck rounds (BivariateProductSumcheckProver::execute / fold,
- * prover/prover/src/protocols/sumcheck/bivariate_product.rs:43-95; fold_highest_var_inplace,
- * verifier/math/src/multilinear/fold.rs:14-29).  d_a, d_b: 2^log_len elements each.
- * execute: d_out2 = (y_1, y_inf) = (sum a_hi b_hi, sum (a_lo + a_hi)(b_lo + b_hi)).
- * fold_execute: folds the top variable of both by h_r in place (a[i] += r (a[i + half] - a[i]))
- * and writes the next round's (y_1, y_inf) on the 2^(log_len-1) folded values.  d_out2 stays on
- * the device; both are asynchronous on `stream`.
+ * Round-by-round sumcheck provers: the SumcheckProver trait (prover/prover/src/protocols/
+ * sumcheck/common.rs:29-101) -- n_vars, execute() -> RoundCoeffs, fold(challenge), finish() ->
+ * multilinear evaluations -- and MleCheckProver::eval_point (common.rs:88-101), for
+ *   BivariateProductSumcheckProver::new([a, b], sum) (sumcheck/bivariate_product.rs:17-119);
+ *   QuadraticMleCheckProver::new([a, b, c], a*b - c, a*b, eval_point, eval_claim)
+ *     (sumcheck/quadratic_mle.rs:21-229; the AND reduction's composition, prove.rs:89-121);
+ *   InOutCheckProver::new(witness, eval_point) (protocols/inout_check.rs:19-221), the public
+ *     segment being the witness's first 2^log_public values.
+ * The multilinears (2^n_vars elements each, d_* device buffers) are folded in place by fold
+ * (fold_highest_var_inplace), so they must stay valid and untouched until finish; the prover
+ * keeps its own eq expansion.  execute writes the round polynomial's coefficients, lowest degree
+ * first, to h_coeffs (3 elements for the degree-2 provers, 2 for InOut) and their count to
+ * *n_coeffs; finish writes the multilinears' values at the challenge point (2 for the bivariate,
+ * 3 for the quadratic MLE-check, 1 for InOut).  Out-of-order calls return BINIUS_E_ARG with
+ * "ExpectedFold" / "ExpectedExecute" (sumcheck/error.rs).  All calls synchronize `stream`.
  * ------------------------------------------------------------------------------------------ */
-int binius_sumcheck_bivariate_execute(const void* d_a, const void* d_b, uint32_t log_len,
+typedef struct binius_sumcheck binius_sumcheck;
+
+int binius_sumcheck_bivariate_create(void* d_a, void* d_b, uint32_t log_len, const void* h_sum,
+                                     void* stream, binius_sumcheck** out);
+int binius_sumcheck_bivariate_execute(binius_sumcheck* prover, void* h_coeffs,
+                                      uint32_t* n_coeffs);
+int binius_sumcheck_bivariate_fold(binius_sumcheck* prover, const void* h_challenge);
+int binius_sumcheck_bivariate_finish(binius_sumcheck* prover, void* h_evals2);
+
+int binius_sumcheck_quadratic_mle_create(void* d_a, void* d_b, void* d_c, uint32_t n_vars,
+                                         const void* h_eval_point, const void* h_eval_claim,
+                                         void* stream, binius_sumcheck** out);
+int binius_sumcheck_quadratic_mle_execute(binius_sumcheck* prover, void* h_coeffs,
+                                          uint32_t* n_coeffs);
+int binius_sumcheck_quadratic_mle_fold(binius_sumcheck* prover, const void* h_challenge);
+int binius_sumcheck_quadratic_mle_finish(binius_sumcheck* prover, void* h_evals3);
+int binius_sumcheck_quadratic_mle_eval_point(const binius_sumcheck* prover, void* h_out);
+
+int binius_sumcheck_inout_create(void* d_witness, uint32_t log_len, const void* h_eval_point,
+                                 uint32_t log_public, void* stream, binius_sumcheck** out);
+int binius_sumcheck_inout_execute(binius_sumcheck* prover, void* h_coeffs, uint32_t* n_coeffs);
+int binius_sumcheck_inout_fold(binius_sumcheck* prover, const void* h_challenge);
+int binius_sumcheck_inout_finish(binius_sumcheck* prover, void* h_eval);
+int binius_sumcheck_inout_eval_point(const binius_sumcheck* prover, void* h_out);
+
+/* SumcheckProver::n_vars, and the release of any of the three. */
+uint32_t binius_sumcheck_n_vars(const binius_sumcheck* prover);
+int binius_sumcheck_destroy(binius_sumcheck* prover);
+
+/* The bivariate product round's device kernels on their own (the prove path's fused form of
+ * BivariateProductSumcheckProver::execute / fold, bivariate_product.rs:43-95;
+ * fold_highest_var_inplace, verifier/math/src/multilinear/fold.rs:14-29).  d_a, d_b: 2^log_len
+ * elements each.  round_evals: d_out2 = (y_1, y_inf) = (sum a_hi b_hi, sum (a_lo + a_hi)(b_lo +
+ * b_hi)).  fold_round_evals: folds the top variable of both by h_r in place (a[i] += r (a[i + half]
+ * - a[i])) and writes the next round's (y_1, y_inf) on the 2^(log_len-1) folded values.  d_out2
+ * stays on the device; both are asynchronous on `stream`. */
+int binius_bivariate_round_evals(const void* d_a, const void* d_b, uint32_t log_len, void* d_out2,
+                                 void* stream);
+int binius_bivariate_fold_round_evals(void* d_a, void* d_b, uint32_t log_len, const void* h_r,
                                       void* d_out2, void* stream);
-int binius_sumcheck_bivariate_fold_execute(void* d_a, void* d_b, uint32_t log_len,
-                                           const void* h_r, void* d_out2, void* stream);
 
 /* Elementwise GF(2^128) products d_out[i] = d_a[i] * d_b[i] (kernel-level check of the field
  * multiplier; BinaryField128bGhash::mul, verifier/field/src/ghash.rs:188-194). */

@@ -110,6 +110,12 @@ def lib():
         L.orc_and_reduction_prove.restype = ctypes.c_int
         L.orc_and_reduction_verify.argtypes = [ctypes.c_uint32, _u8p, ctypes.c_size_t, _u64p, _u64p]
         L.orc_and_reduction_verify.restype = ctypes.c_int
+        L.orc_bivariate_rounds.argtypes = [_u64p, _u64p, ctypes.c_uint32, _u64p, _u64p, _u64p,
+                                           _u64p]
+        L.orc_quadratic_mle_rounds.argtypes = [_u64p, _u64p, _u64p, ctypes.c_uint32, _u64p,
+                                               _u64p, _u64p, _u64p, _u64p]
+        L.orc_inout_rounds.argtypes = [_u64p, ctypes.c_uint32, _u64p, ctypes.c_uint32, _u64p,
+                                       _u64p, _u64p]
         _lib = L
     return _lib
 
@@ -700,3 +706,44 @@ def key_collection(and_csr, mul_csr, n_words: int) -> bytes:
     rc = L.orc_key_collection(pa, va, na, pm, vm, nm, n_words, _p8(out), cap, ctypes.byref(n))
     assert rc == 0
     return out[: n.value].tobytes()
+
+
+# ---------------------------------------------------------------- round-by-round sumchecks
+
+def bivariate_rounds(a, b, claimed_sum: int, challenges):
+    """BivariateProductSumcheckProver (sumcheck/bivariate_product.rs:17-119) over the given
+    challenges: (per-round coefficients (n, 3, 2), final evaluations (2, 2))."""
+    n = len(challenges)
+    a, b = np.ascontiguousarray(a), np.ascontiguousarray(b)
+    ch = np.ascontiguousarray(challenges, dtype=np.uint64).reshape(-1, 2)
+    s = from_int(claimed_sum)
+    co, ev = elems(3 * n), elems(2)
+    lib().orc_bivariate_rounds(_p64(a), _p64(b), n, _p64(s), _p64(ch), _p64(co), _p64(ev))
+    return co.reshape(n, 3, 2), ev
+
+
+def quadratic_mle_rounds(a, b, c, point, claim: int, challenges):
+    """QuadraticMleCheckProver with composition a*b - c (sumcheck/quadratic_mle.rs:21-229)."""
+    n = len(challenges)
+    cols = [np.ascontiguousarray(x) for x in (a, b, c)]
+    pt = np.ascontiguousarray(point, dtype=np.uint64).reshape(-1, 2)
+    ch = np.ascontiguousarray(challenges, dtype=np.uint64).reshape(-1, 2)
+    cl = from_int(claim)
+    co, ev = elems(3 * n), elems(3)
+    lib().orc_quadratic_mle_rounds(_p64(cols[0]), _p64(cols[1]), _p64(cols[2]), n, _p64(pt),
+                                   _p64(cl), _p64(ch), _p64(co), _p64(ev))
+    return co.reshape(n, 3, 2), ev
+
+
+def inout_rounds(w, point, challenges):
+    """InOutCheckProver (protocols/inout_check.rs:19-221): witness of 2^n values, point of m
+    coordinates (the public segment's)."""
+    n = len(challenges)
+    w = np.ascontiguousarray(w)
+    pt = np.ascontiguousarray(point, dtype=np.uint64).reshape(-1, 2)
+    m = pt.shape[0]
+    ch = np.ascontiguousarray(challenges, dtype=np.uint64).reshape(-1, 2)
+    co, ev = elems(2 * n), elems(1)
+    lib().orc_inout_rounds(_p64(w), n, _p64(pt if m else elems(1)), m, _p64(ch), _p64(co),
+                           _p64(ev))
+    return co.reshape(n, 2, 2), ev

@@ -178,6 +178,19 @@ int orc_verify(const uint64_t* public_words, uint32_t log_words, uint32_t log_pu
 /* Number of worker threads the oracle may use (1 = scalar). */
 void orc_set_threads(int n);
 
+/* ---- Round-by-round sumcheck provers over given challenges (sumcheck.cpp):
+ * BivariateProductSumcheckProver (bivariate_product.rs:17-119), QuadraticMleCheckProver with
+ * composition a*b - c (quadratic_mle.rs:21-229), InOutCheckProver (inout_check.rs:19-221).
+ * coeffs_out: each round's RoundCoeffs (3 or 2 elements); evals_out: finish(). */
+int orc_bivariate_rounds(const uint64_t* a, const uint64_t* b, uint32_t n, const uint64_t* sum,
+                         const uint64_t* challenges, uint64_t* coeffs_out, uint64_t* evals_out);
+int orc_quadratic_mle_rounds(const uint64_t* a, const uint64_t* b, const uint64_t* c, uint32_t n,
+                             const uint64_t* point, const uint64_t* claim,
+                             const uint64_t* challenges, uint64_t* coeffs_out,
+                             uint64_t* evals_out);
+int orc_inout_rounds(const uint64_t* w, uint32_t n, const uint64_t* point, uint32_t m,
+                     const uint64_t* challenges, uint64_t* coeffs_out, uint64_t* eval_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -110,6 +110,12 @@ def test_merkle_commit_vs_oracle(log_leaves, log_batch):
     ref = orc.merkle_commit(elems, log_leaves, log_batch)
     assert np.array_equal(committed.nodes.cpu().numpy(), ref)
     assert root == bytes(ref[-1])
+    # MerkleTreeProver::layer at every depth: the flat node slice of that layer
+    for depth in range(log_leaves + 1):
+        start = (2 << log_leaves) - (2 << depth)
+        assert committed.layer(depth) == [bytes(x) for x in ref[start:start + (1 << depth)]]
+    with pytest.raises(bg.ArgumentError, match="IncorrectLayerDepth"):
+        committed.layer(log_leaves + 1)
     if log_leaves >= 3:
         idx = (1 << log_leaves) - 3
         br = committed.branch(idx, 1)

@@ -71,3 +71,25 @@ def test_prover_is_reusable_and_deterministic():
     assert a == b
     with pytest.raises(bg.ArgumentError):
         prover.prove(w[:-1])
+
+
+@pytest.mark.parametrize("with_key_collection", [False, True])
+def test_setup_and_prove_from_host_buffers(with_key_collection):
+    """binius_setup (ConstraintSystem bytes -> prover) and binius_prove (host witness words ->
+    proof bytes): the same bytes as the device-witness path and the oracle."""
+    sc = csm.synthetic_circuit(12, 1800, 9, seed=77, log_public=2)
+    prep = sc.cs.prepared()
+    ref = orc.prove(sc.witness, 2, prep.and_csr, prep.mul_csr, 1)
+    cs_bytes = sc.cs.serialize()
+    kc = bg.key_collection_from_cs_bytes(cs_bytes) if with_key_collection else None
+    p = bg.setup(cs_bytes, 1, key_collection=kc)
+    assert p.cs.committed_total_len == len(sc.witness)
+    assert p.prove_host(sc.witness) == ref
+    assert p.prove_host(sc.witness) == ref  # the prover is reusable
+    with pytest.raises(bg.ArgumentError):
+        p.prove_host(sc.witness[:-1])
+    # appended to a caller's transcript: the tape is the caller's bytes followed by the proof
+    t = bg.ProverTranscript()
+    t.message(b"\x01" * 16)
+    out = p.prove_host(sc.witness, transcript=t)
+    assert out[:16] == b"\x01" * 16 and len(out) == 16 + len(ref)
