@@ -110,6 +110,8 @@ def lib():
         L.orc_and_reduction_prove.restype = ctypes.c_int
         L.orc_and_reduction_verify.argtypes = [ctypes.c_uint32, _u8p, ctypes.c_size_t, _u64p, _u64p]
         L.orc_and_reduction_verify.restype = ctypes.c_int
+        L.orc_and_word_ntt.argtypes = [ctypes.c_uint64, _u8p]
+        L.orc_shift_h_parts.argtypes = [_u64p, _u64p, _u64p]
         L.orc_bivariate_rounds.argtypes = [_u64p, _u64p, ctypes.c_uint32, _u64p, _u64p, _u64p,
                                            _u64p]
         L.orc_quadratic_mle_rounds.argtypes = [_u64p, _u64p, _u64p, ctypes.c_uint32, _u64p,
@@ -747,3 +749,19 @@ def inout_rounds(w, point, challenges):
     lib().orc_inout_rounds(_p64(w), n, _p64(pt if m else elems(1)), m, _p64(ch), _p64(co),
                            _p64(ev))
     return co.reshape(n, 2, 2), ev
+
+
+def and_word_ntt(w: int) -> list[int]:
+    """The AND univariate round's extension evaluations of one 64-bit word (64 GF(2^8) bytes at
+    the points 64..127)."""
+    out = np.zeros(64, dtype=np.uint8)
+    lib().orc_and_word_ntt(int(w), _p8(out))
+    return [int(x) for x in out]
+
+
+def shift_h_parts(r_zhat: int):
+    """build_h_parts at r_zhat: ((8, 4096, 2) h multilinears, (64, 2) Lagrange evaluations)."""
+    z = from_int(r_zhat)
+    h, lt = elems(8 * 4096), elems(64)
+    lib().orc_shift_h_parts(_p64(z), _p64(h), _p64(lt))
+    return h.reshape(8, 4096, 2), lt

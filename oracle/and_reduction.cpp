@@ -293,6 +293,13 @@ void orc_and_univariate_round(const uint64_t* a, const uint64_t* b, const uint64
   univariate_round(a, b, c, log_n, (const u128*)big, (u128*)msg_out);
 }
 
+// The univariate round's per-word extension evaluations (NTTLookup::ntt, ntt_lookup.rs:91-164):
+// out[k] = the word's interpolant over {0..63} in GF(2^8) at the point 64 + k.
+void orc_and_word_ntt(uint64_t w, uint8_t out[64]) {
+  static const WordNtt ntt;
+  ntt.eval(w, out);
+}
+
 // Words folded at z: out[i] = sum_t bit_t(w[i]) L_t(z) over {phi(t) : t < 64}.
 void orc_and_fold_words(const uint64_t* w, size_t n, const uint64_t* z, uint64_t* out) {
   u128 lag[64];

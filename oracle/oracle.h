@@ -191,6 +191,11 @@ int orc_quadratic_mle_rounds(const uint64_t* a, const uint64_t* b, const uint64_
 int orc_inout_rounds(const uint64_t* w, uint32_t n, const uint64_t* point, uint32_t m,
                      const uint64_t* challenges, uint64_t* coeffs_out, uint64_t* eval_out);
 
+/* The AND univariate round's per-word lookup NTT (ntt_lookup.rs:91-164) and the shift
+ * reduction's h multilinears with their Lagrange basis (monster.rs:34-104). */
+void orc_and_word_ntt(uint64_t w, uint8_t out[64]);
+void orc_shift_h_parts(const uint64_t* r_zhat, uint64_t* h_out, uint64_t* l_tilde_out);
+
 #ifdef __cplusplus
 }
 #endif

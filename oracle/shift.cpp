@@ -425,6 +425,17 @@ void make_data(const uint64_t* evals, uint32_t n_evals, const uint64_t* rz, cons
 // lo).  Operator data: AND evals (a, b, c), MUL evals (a, b, lo, hi), each with its r_zhat' and
 // r_x'.  out_point: 6 + log_words elements (r_j ++ r_y); out3: witness eval, the phase-1 initial
 // sum and the verifier's batched claim.
+// build_h_parts (monster.rs:34-104) at r_zhat: h_out holds 8 x 4096 elements (variant-major,
+// index s * 64 + j); l_tilde_out the 64 Lagrange evaluations it is built from.
+void orc_shift_h_parts(const uint64_t* r_zhat, uint64_t* h_out, uint64_t* l_tilde_out) {
+  std::vector<u128> h;
+  build_h_parts(load(r_zhat), h);
+  for (size_t i = 0; i < h.size(); i++) store(h_out + 2 * i, h[i]);
+  u128 L[64];
+  l_tilde64(load(r_zhat), L);
+  for (int i = 0; i < 64; i++) store(l_tilde_out + 2 * i, L[i]);
+}
+
 int orc_shift_prove(const uint64_t* words, uint32_t log_words, uint32_t log_public,
                     const uint32_t* const* and_csr, const uint8_t* and_var, uint32_t n_and,
                     const uint32_t* const* mul_csr, const uint8_t* mul_var, uint32_t n_mul,
