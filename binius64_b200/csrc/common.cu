@@ -278,6 +278,24 @@ uint64_t arena_held_bytes() {
   return n;
 }
 
+namespace {
+struct PinnedSmall {
+  uint8_t* buf = nullptr;
+  ~PinnedSmall() {
+    if (buf) cudaFreeHost(buf);
+  }
+};
+thread_local PinnedSmall t_early;
+}  // namespace
+
+int early_read_buffer(uint8_t** out) {
+  if (!t_early.buf)
+    BGPU_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&t_early.buf), kEarlyReadBytes,
+                            cudaHostAllocDefault));
+  *out = t_early.buf;
+  return BINIUS_OK;
+}
+
 int read_sync(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   StagedReads r(s);
   if (int rc = r.add(dst, src, bytes)) return rc;

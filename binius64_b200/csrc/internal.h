@@ -64,6 +64,11 @@ class StagedReads {
 // One staged read: copy, synchronise, return.
 int read_sync(void* dst, const void* src, size_t bytes, cudaStream_t s);
 
+// A small pinned buffer of the calling thread, apart from the StagedReads stage: a copy queued
+// into it before a later synchronising read (of any kind) has landed once that read returns.
+constexpr size_t kEarlyReadBytes = 4096;
+int early_read_buffer(uint8_t** out);
+
 // Stream-ordered device allocations of the prove path.  Inside an ArenaScope on the calling
 // thread (same stream), dev_alloc bump-allocates from a few large chunks the scope took from the
 // stream-ordered pool and dev_free of such a buffer does nothing: the scope releases (or, for a

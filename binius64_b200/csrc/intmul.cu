@@ -666,29 +666,13 @@ int IntMulDevice::layer(uint4* set, uint32_t pairs, std::vector<hu128>& point,
   return BINIUS_OK;
 }
 
-int IntMulDevice::run_single(uint4* acl, uint4* btree, uint4* bcols, uint4* lo0,
-                             const uint64_t* d_a, const uint64_t* d_b, const uint64_t* d_lo,
-                             IntMulResult& res) {
-  constexpr int kAcl = 3 * 127 + 2, kB = 127;
-  bit_columns_kernel<<<1, kT, 0, s_>>>(d_b, 1, 0, 64, bcols, 1);
-  bit_columns_kernel<<<1, kT, 0, s_>>>(d_a, 1, 0, 1, acl + 3 * 127, 1);
-  bit_columns_kernel<<<1, kT, 0, s_>>>(d_b, 1, 0, 1, acl + 3 * 127 + 1, 1);
-  bit_columns_kernel<<<1, kT, 0, s_>>>(d_lo, 1, 0, 1, lo0, 1);
-  if (int rc = check("bit_columns_kernel", 4)) return rc;
-  // c_root = c_lo_root * c_hi_root (acl nodes 1 and 2), through the dot kernel with eq = [1]
-  if (int rc = eq_single({}, 0, eq_)) return rc;
-  BGPU_CUDA(cudaMemsetAsync(acc_, 0, 16, s_));
-  dot_kernel<<<1, kT, 0, s_>>>(acl + 1, acl + 2, eq_, 1, acc_);
-  if (int rc = check("dot_kernel")) return rc;
-  std::vector<hu128> hacl(kAcl), hb(kB), hcols(64);
-  hu128 c_root = 0, lo_bit = 0;
-  StagedReads rd(s_);
-  if (int rc = rd.add(hacl.data(), acl, 16 * kAcl)) return rc;
-  if (int rc = rd.add(hb.data(), btree, 16 * kB)) return rc;
-  if (int rc = rd.add(hcols.data(), bcols, 16 * 64)) return rc;
-  if (int rc = rd.add(&c_root, acc_, 16)) return rc;
-  if (int rc = rd.add(&lo_bit, lo0, 16)) return rc;
-  if (int rc = rd.wait()) return rc;
+// The transcript of a one-statement IntMul (n_vars = 0: every sumcheck has zero rounds, so the
+// messages are the tree values themselves) from the host copies of its trees: hacl the a / c_lo /
+// c_hi tree (layer k at 3 (2^k - 1), 3 * 2^k values) with a_0 and b_0 after layer 6, hb the b
+// tree (layer k at 2^k - 1), hcols the 64 bit columns of b, c_root = c_lo root * c_hi root, lo_bit
+// bit 0 of c_lo (prove.rs:91-194 with the phase structure of run).
+void emit_single(Transcript& t_, const std::vector<hu128>& hacl, const std::vector<hu128>& hb,
+                 const std::vector<hu128>& hcols, hu128 c_root, hu128 lo_bit, IntMulResult& res) {
   auto acl_layer = [&](int k) { return hacl.begin() + 3 * ((1 << k) - 1); };
   auto b_layer = [&](int k) { return hb.begin() + ((1 << k) - 1); };
   write_elems(t_, {hb[0], c_root});
@@ -714,6 +698,32 @@ int IntMulDevice::run_single(uint4* acl, uint4* btree, uint4* bcols, uint4* lo0,
   res = IntMulResult();
   normalize_leaves(biv, res);
   res.b_evals = hcols;
+}
+
+int IntMulDevice::run_single(uint4* acl, uint4* btree, uint4* bcols, uint4* lo0,
+                             const uint64_t* d_a, const uint64_t* d_b, const uint64_t* d_lo,
+                             IntMulResult& res) {
+  constexpr int kAcl = 3 * 127 + 2, kB = 127;
+  bit_columns_kernel<<<1, kT, 0, s_>>>(d_b, 1, 0, 64, bcols, 1);
+  bit_columns_kernel<<<1, kT, 0, s_>>>(d_a, 1, 0, 1, acl + 3 * 127, 1);
+  bit_columns_kernel<<<1, kT, 0, s_>>>(d_b, 1, 0, 1, acl + 3 * 127 + 1, 1);
+  bit_columns_kernel<<<1, kT, 0, s_>>>(d_lo, 1, 0, 1, lo0, 1);
+  if (int rc = check("bit_columns_kernel", 4)) return rc;
+  // c_root = c_lo_root * c_hi_root (acl nodes 1 and 2), through the dot kernel with eq = [1]
+  if (int rc = eq_single({}, 0, eq_)) return rc;
+  BGPU_CUDA(cudaMemsetAsync(acc_, 0, 16, s_));
+  dot_kernel<<<1, kT, 0, s_>>>(acl + 1, acl + 2, eq_, 1, acc_);
+  if (int rc = check("dot_kernel")) return rc;
+  std::vector<hu128> hacl(kAcl), hb(kB), hcols(64);
+  hu128 c_root = 0, lo_bit = 0;
+  StagedReads rd(s_);
+  if (int rc = rd.add(hacl.data(), acl, 16 * kAcl)) return rc;
+  if (int rc = rd.add(hb.data(), btree, 16 * kB)) return rc;
+  if (int rc = rd.add(hcols.data(), bcols, 16 * 64)) return rc;
+  if (int rc = rd.add(&c_root, acc_, 16)) return rc;
+  if (int rc = rd.add(&lo_bit, lo0, 16)) return rc;
+  if (int rc = rd.wait()) return rc;
+  emit_single(t_, hacl, hb, hcols, c_root, lo_bit, res);
   return BINIUS_OK;
 }
 
@@ -938,6 +948,40 @@ uint32_t log2_ceil(uint64_t n) {
 }  // namespace
 
 namespace bgpu {
+
+// One MUL constraint (padded count 1): the trees of run's witness stage are 64-leaf exponent
+// trees of four words, a few hundred products, so they are formed here from the operand words
+// (read back with the commit's root by the prove entry) and the proof needs no device round
+// trip for this phase.  Same values as const_leaves_kernel / var_leaves_kernel /
+// tree_layer_kernel / bit_columns_kernel at n = 1.
+int intmul_single_from_words(uint64_t a, uint64_t b, uint64_t lo, uint64_t hi, Transcript& t,
+                             IntMulResult& res) {
+  const hu128 g = ((hu128)0x494ef99794d5244fULL << 64) | (hu128)0x9152df59d87a9186ULL;
+  std::vector<hu128> hacl(3 * 127 + 2), hb(127), hcols(64);
+  auto leaves = [](uint64_t e, hu128 base, hu128* out) {  // bit_i(e) ? base^(2^i) : 1
+    for (int i = 0; i < 64; i++, base = host_gf_mul(base, base)) out[i] = ((e >> i) & 1) ? base : 1;
+  };
+  hu128* l6 = hacl.data() + 3 * 63;
+  leaves(a, g, l6);
+  leaves(lo, g, l6 + 64);
+  leaves(hi, sq_n(g, 64), l6 + 128);
+  for (int k = 5; k >= 0; k--) {  // parent[q] = child[2q] child[2q + 1]
+    const hu128* child = hacl.data() + 3 * ((2 << k) - 1);
+    hu128* parent = hacl.data() + 3 * ((1 << k) - 1);
+    for (int q = 0; q < (3 << k); q++) parent[q] = host_gf_mul(child[2 * q], child[2 * q + 1]);
+  }
+  hacl[3 * 127] = a & 1;
+  hacl[3 * 127 + 1] = b & 1;
+  leaves(b, hacl[0], hb.data() + 63);
+  for (int k = 5; k >= 0; k--) {
+    const hu128* child = hb.data() + ((2 << k) - 1);
+    hu128* parent = hb.data() + ((1 << k) - 1);
+    for (int q = 0; q < (1 << k); q++) parent[q] = host_gf_mul(child[2 * q], child[2 * q + 1]);
+  }
+  for (int i = 0; i < 64; i++) hcols[i] = (b >> i) & 1;
+  emit_single(t, hacl, hb, hcols, host_gf_mul(hacl[1], hacl[2]), lo & 1, res);
+  return BINIUS_OK;
+}
 
 int intmul_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcript& t,
                            IntMulResult& res, cudaStream_t s) {

@@ -194,6 +194,17 @@ int binius_prover_prove(const binius_prover* P, const void* d_witness,
     t_phase_ms[phase] = std::chrono::duration<double, std::milli>(now - t0).count();
     t0 = now;
   };
+  // One MUL constraint: its four operand words ride back with the commitment's root (same
+  // synchronisation), and the IntMul reduction then needs no device work.
+  const bool single_mul = cs->mul_ops.n_constraints == 1;
+  uint8_t* mul_words = nullptr;
+  if (single_mul) {
+    uint64_t* d_cols = nullptr;
+    if (int rc = early_read_buffer(&mul_words)) return rc;
+    BGPU_CUDA(dev_alloc(&d_cols, 32, s));
+    if (int rc = eval_operands(cs->mul_ops, words, d_cols, s)) return rc;
+    BGPU_CUDA(cudaMemcpyAsync(mul_words, d_cols, 32, cudaMemcpyDeviceToHost, s));
+  }
   // [phase] Witness Commit
   binius_pcs_committed* committed = nullptr;
   uint8_t root[32];
@@ -204,7 +215,14 @@ int binius_prover_prove(const binius_prover* P, const void* d_witness,
   do {
     // [phase] IntMul Reduction
     IntMulResult im;
-    if ((rc = intmul_reduction_prove(cs, words, t, im, s))) break;
+    if (single_mul) {
+      uint64_t w[4];  // CSR slots a, b, hi, lo
+      memcpy(w, mul_words, 32);
+      rc = intmul_single_from_words(w[0], w[1], w[3], w[2], t, im);
+    } else {
+      rc = intmul_reduction_prove(cs, words, t, im, s);
+    }
+    if (rc) break;
     lap(1);
     // [phase] BitAnd Reduction
     AndResult ao;

@@ -32,6 +32,10 @@ struct IntMulResult {
 
 int intmul_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcript& t,
                            IntMulResult& res, cudaStream_t s);
+// The same reduction for a constraint system with one MUL constraint, from its operand words
+// (a, b, lo, hi): no device work.
+int intmul_single_from_words(uint64_t a, uint64_t b, uint64_t lo, uint64_t hi, Transcript& t,
+                             IntMulResult& res);
 
 // OperatorData (prover/prover/src/protocols/shift/prove.rs:20-33): operand evaluations at the
 // oblong point (r_zhat', r_x').  AND: (a, b, c); MUL: (a, b, lo, hi).
