@@ -123,6 +123,9 @@ _SIGS = {
     "binius_prover_phase_ms": (_int, [_vp, _vp]),
     "binius_prover_committed_words": (_u64, [_vp]),
     "binius_prover_workspace_bytes": (_u64, [_vp]),
+    "binius_prover_get_tuning": (_int, [_vp, _vp]),
+    "binius_prover_set_tuning": (_int, [_vp, _vp]),
+    "binius_prover_autotune": (_int, [_vp, _vp, _u32, _vp, _vp]),
     "binius_queue_create": (_int, [_int, _u32, _u64, _vp]),
     "binius_queue_destroy": (_int, [_vp]),
     "binius_queue_submit": (_int, [_vp, _vp, _vp, _int, _vp]),

@@ -702,10 +702,10 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
     if (e != cudaSuccess) { rc = cuda_error(e, "round constants"); break; }
     DeviceTranscript dt;
     if ((rc = dt.begin(t, s))) break;
-    // rounds whose fold starts from at most kTailMaxLen elements run in the single-CTA tail
+    // rounds whose fold starts from at most tail_max_len() elements run in the single-CTA tail
     uint32_t tail_n = 0;  // n_rem of the first tail round (0: no tail)
     for (uint32_t n_rem = log_n - 1; n_rem > 0; n_rem--)
-      if ((2ull << n_rem) <= kTailMaxLen) {
+      if ((2ull << n_rem) <= tail_max_len()) {
         tail_n = n_rem;
         break;
       }

@@ -272,6 +272,14 @@ void arena_release_thread() {
   a.s = nullptr;
 }
 
+namespace {
+thread_local Tuning t_tuning;
+}  // namespace
+
+const Tuning& tuning() { return t_tuning; }
+TuningScope::TuningScope(const Tuning& t) : saved_(t_tuning) { t_tuning = t; }
+TuningScope::~TuningScope() { t_tuning = saved_; }
+
 uint64_t arena_held_bytes() {
   uint64_t n = 0;
   for (const auto& c : t_arena.chunks) n += c.size;

@@ -105,6 +105,28 @@ uint64_t arena_held_bytes();
 // Records that a proof of P took `bytes` of arena chunks from an empty arena (prover.cu).
 void prover_note_footprint(const binius_prover* P, uint64_t bytes);
 
+// Launch-shape choices of the prove path that change no result, only speed (exact arithmetic: any
+// choice gives identical bytes).  A prover carries its own (binius_prover_autotune measures them
+// per statement shape); standalone entry points use the defaults.
+struct Tuning {
+  uint32_t tail_log = 11;          // sumcheck rounds on <= 2^tail_log elements: single-CTA tail
+  uint32_t ntt_pass_layers = 8;    // NTT layers fused per shared-memory pass (<= 8)
+  uint32_t merkle_leaf_fuse = 8;   // Merkle leaf CTA: 2^fuse leaves, as many layers above them
+  uint32_t merkle_node_fuse = 9;   // Merkle node CTA: 2^fuse inputs (<= 9)
+};
+// The calling thread's current choices (a prove sets its prover's for its duration).
+const Tuning& tuning();
+class TuningScope {
+ public:
+  explicit TuningScope(const Tuning& t);
+  ~TuningScope();
+  TuningScope(const TuningScope&) = delete;
+  TuningScope& operator=(const TuningScope&) = delete;
+
+ private:
+  Tuning saved_;
+};
+
 // Sets the dynamic shared memory limit of a kernel once per device (see common.cu).
 int ensure_smem_limit(const void* func, size_t bytes);
 

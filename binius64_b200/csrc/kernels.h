@@ -78,8 +78,8 @@ int bivariate_tail(const DeviceTranscript& dt, uint4* d_a, uint4* d_b, uint64_t 
                    uint32_t n_rounds, const uint4* d_r_first, uint4* d_claim, uint4* d_chal,
                    cudaStream_t s);
 // Sumcheck rounds whose arrays have at most this many elements before the fold run in the
-// single-CTA tail kernels.
-constexpr uint64_t kTailMaxLen = 1ull << 11;
+// single-CTA tail kernels (the calling thread's Tuning::tail_log; 2^11 by default).
+inline uint64_t tail_max_len() { return 1ull << tuning().tail_log; }
 int gather_segments(const GatherSegment* d_segs, uint32_t n, uint8_t* d_dst, cudaStream_t s);
 // d_tab (16 * 256 elements) = the byte table of multiplication by r (gf_mul_table).
 int build_mul_table(const uint8_t r[16], uint4* d_tab, cudaStream_t s);

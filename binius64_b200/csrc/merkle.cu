@@ -21,8 +21,8 @@ using namespace bgpu;
 
 namespace {
 
-constexpr uint32_t kLeafFuse = 8;  // leaves per CTA = 2^8
-constexpr uint32_t kNodeFuse = 9;  // inputs per CTA = 2^9
+constexpr uint32_t kLeafFuse = 8;  // at most 2^8 leaves per CTA (Tuning::merkle_leaf_fuse)
+constexpr uint32_t kNodeFuse = 9;  // at most 2^9 inputs per CTA (Tuning::merkle_node_fuse)
 
 __host__ __device__ __forceinline__ uint64_t layer_offset(uint32_t L, uint32_t k) {
   return (1ull << (L + 1)) - (1ull << (L + 1 - k));
@@ -134,7 +134,9 @@ int merkle_commit(const void* d_elems, uint32_t log_leaves, uint32_t log_batch, 
   const uint32_t L = log_leaves;
   const NodeIV iv = node_iv();
   uint4* nodes = static_cast<uint4*>(d_nodes);
-  uint32_t fused = std::min(L, kLeafFuse);
+  const uint32_t leaf_fuse = std::max(5u, std::min(kLeafFuse, tuning().merkle_leaf_fuse));
+  const uint32_t node_fuse = std::max(5u, std::min(kNodeFuse, tuning().merkle_node_fuse));
+  uint32_t fused = std::min(L, leaf_fuse);
   uint64_t grid = 1ull << (L - fused);
   BGPU_ARG(grid <= 0x7fffffffull, "too many leaves");
   merkle_leaves_kernel<<<(unsigned)grid, 1u << fused, 0, stream>>>(
@@ -143,7 +145,7 @@ int merkle_commit(const void* d_elems, uint32_t log_leaves, uint32_t log_batch, 
   count_launch();
   uint32_t level = fused;
   while (level < L) {
-    uint32_t f = std::min(L - level, kNodeFuse);
+    uint32_t f = std::min(L - level, node_fuse);
     uint64_t g = 1ull << (L - level - f);
     merkle_nodes_kernel<<<(unsigned)g, 1u << (f - 1), 0, stream>>>(nodes, L, level, f, iv);
     BGPU_LAUNCH_CHECK("merkle_nodes_kernel");

@@ -134,7 +134,8 @@ std::vector<NttPass> plan_passes(uint32_t log_d, uint32_t skip_early, uint32_t s
     }
     return passes;
   }
-  uint32_t n_passes = (n_layers + kMaxPassLayers - 1) / kMaxPassLayers;
+  const uint32_t max_layers = std::max(1u, std::min(kMaxPassLayers, tuning().ntt_pass_layers));
+  uint32_t n_passes = (n_layers + max_layers - 1) / max_layers;
   uint32_t base = n_layers / n_passes, extra = n_layers % n_passes;
   uint32_t l0 = skip_early;
   for (uint32_t i = 0; i < n_passes; i++) {

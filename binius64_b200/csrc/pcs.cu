@@ -300,7 +300,7 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
       if ((rc = dt.begin(t, s))) break;
       uint32_t tape_bytes = 0;
       // the rounds after the last FRI commit inside the loop whose fold starts from at most
-      // kTailMaxLen elements run in the single-CTA tail
+      // tail_max_len() elements run in the single-CTA tail
       uint32_t tail0 = 1;
       {
         uint32_t c = P->log_batch;
@@ -309,7 +309,7 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
           c += a_i;
           if (c < n) tail0 = std::max(tail0, c + 1);
         }
-        while (tail0 < n && (N >> (tail0 - 1)) > kTailMaxLen) tail0++;
+        while (tail0 < n && (N >> (tail0 - 1)) > tail_max_len()) tail0++;
       }
       for (uint32_t round = 0; round < tail0 && round < n && rc == BINIUS_OK; round++) {
         const uint64_t size = N >> round;

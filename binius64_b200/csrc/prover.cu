@@ -10,8 +10,10 @@
 // log_dim + log_inv_rate layers.
 #include <string.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <mutex>
 #include <vector>
 
 #include "cs.h"
@@ -32,7 +34,67 @@ struct binius_prover {
   // largest device footprint (arena chunk bytes) a proof of this prover has taken from an empty
   // arena; raises binius_prover_workspace_bytes when the static estimate is low
   mutable std::atomic<uint64_t> footprint{0};
+  // launch-shape choices of its proofs (binius_prover_autotune); not changed while proving
+  Tuning tuning;
+  uint32_t merkle_hash = 0;
 };
+
+namespace {
+
+// Statement shape -> the choices binius_prover_autotune measured for it, so that provers set up
+// later for the same shape start from them.
+struct ShapeKey {
+  uint64_t words, n_and, n_mul;
+  uint32_t log_inv_rate, merkle_hash;
+  bool operator==(const ShapeKey& o) const {
+    return words == o.words && n_and == o.n_and && n_mul == o.n_mul &&
+           log_inv_rate == o.log_inv_rate && merkle_hash == o.merkle_hash;
+  }
+};
+std::mutex g_tuned_mu;
+std::vector<std::pair<ShapeKey, Tuning>> g_tuned;
+
+ShapeKey shape_of(const binius_prover* P) {
+  return ShapeKey{P->cs->committed_total_len, P->cs->and_ops.n_constraints,
+                  P->cs->mul_ops.n_constraints, P->log_inv_rate, P->merkle_hash};
+}
+
+// The choices measured for P's shape, if any.
+void load_tuned(binius_prover* P) {
+  std::lock_guard<std::mutex> lock(g_tuned_mu);
+  const ShapeKey k = shape_of(P);
+  for (const auto& e : g_tuned)
+    if (e.first == k) {
+      P->tuning = e.second;
+      return;
+    }
+}
+
+void store_tuned(const binius_prover* P) {
+  std::lock_guard<std::mutex> lock(g_tuned_mu);
+  const ShapeKey k = shape_of(P);
+  for (auto& e : g_tuned)
+    if (e.first == k) {
+      e.second = P->tuning;
+      return;
+    }
+  g_tuned.emplace_back(k, P->tuning);
+}
+
+bool valid_tuning(const Tuning& t) {
+  return t.tail_log >= 8 && t.tail_log <= 12 && t.ntt_pass_layers >= 4 &&
+         t.ntt_pass_layers <= 8 && t.merkle_leaf_fuse >= 5 && t.merkle_leaf_fuse <= 8 &&
+         t.merkle_node_fuse >= 5 && t.merkle_node_fuse <= 9;
+}
+
+void tuning_out(const Tuning& t, uint32_t* out4) {
+  out4[0] = t.tail_log;
+  out4[1] = t.ntt_pass_layers;
+  out4[2] = t.merkle_leaf_fuse;
+  out4[3] = t.merkle_node_fuse;
+}
+
+}  // namespace
 
 namespace bgpu {
 void prover_note_footprint(const binius_prover* P, uint64_t bytes) {
@@ -104,13 +166,38 @@ int binius_prover_setup(const binius_cs* cs, uint32_t log_inv_rate, binius_prove
     binius_prover_destroy(P);
     return rc;
   }
+  load_tuned(P);
   *out = P;
   return clear_error();
 }
 
 int binius_prover_set_merkle_hash(binius_prover* P, uint32_t merkle_hash) {
   BGPU_ARG(P != nullptr, "NULL argument");
-  return binius_pcs_set_merkle_hash(P->pcs, merkle_hash);
+  if (int rc = binius_pcs_set_merkle_hash(P->pcs, merkle_hash)) return rc;
+  P->merkle_hash = merkle_hash;
+  P->tuning = Tuning();
+  load_tuned(P);
+  return clear_error();
+}
+
+int binius_prover_get_tuning(const binius_prover* P, uint32_t* h_out4) {
+  BGPU_ARG(P && h_out4, "NULL argument");
+  tuning_out(P->tuning, h_out4);
+  return clear_error();
+}
+
+int binius_prover_set_tuning(binius_prover* P, const uint32_t* h_in4) {
+  BGPU_ARG(P && h_in4, "NULL argument");
+  Tuning t;
+  t.tail_log = h_in4[0];
+  t.ntt_pass_layers = h_in4[1];
+  t.merkle_leaf_fuse = h_in4[2];
+  t.merkle_node_fuse = h_in4[3];
+  BGPU_ARG(valid_tuning(t),
+           "tuning out of range: tail_log 8..12, ntt_pass_layers 4..8, merkle_leaf_fuse 5..8, "
+           "merkle_node_fuse 5..9");
+  P->tuning = t;
+  return clear_error();
 }
 
 int binius_prover_destroy(binius_prover* P) {
@@ -186,6 +273,7 @@ int binius_prover_prove(const binius_prover* P, const void* d_witness,
 
   // every device buffer of the proof comes from one arena on s, released at the end
   ArenaScope arena(s, false);
+  TuningScope tuned(P->tuning);
   const bool fresh_arena = arena_held_bytes() == 0;
   typedef std::chrono::steady_clock Clock;
   auto t0 = Clock::now();
@@ -250,6 +338,84 @@ int binius_prover_prove(const binius_prover* P, const void* d_witness,
   binius_pcs_committed_destroy(committed);
   if (!rc && fresh_arena) prover_note_footprint(P, arena_held_bytes());
   return rc ? rc : clear_error();
+}
+
+// Coordinate search over the launch-shape choices: each knob in turn takes every value in its range
+// with the others at their best so far; a candidate's score is the median CUDA-event time of
+// `reps` proofs (after one warm-up proof), the whole proof on the stream as the bench times it.
+// Every candidate's proof must equal the proof under the starting choices byte for byte (the
+// choices change no arithmetic); a difference is reported as an error and the starting choices
+// are kept.
+int binius_prover_autotune(binius_prover* P, const void* d_witness, uint32_t reps, void* stream,
+                           uint32_t* h_out4) {
+  BGPU_ARG(P && d_witness, "NULL argument");
+  reps = std::max(1u, std::min(reps, 64u));
+  cudaStream_t s = as_stream(stream);
+  const Tuning start = P->tuning;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  BGPU_CUDA(cudaEventCreate(&e0));
+  cudaError_t ce = cudaEventCreate(&e1);
+  if (ce != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return cuda_error(ce, "cudaEventCreate");
+  }
+  std::vector<uint8_t> ref;
+  auto score = [&](const Tuning& t, double* ms) -> int {
+    P->tuning = t;
+    std::vector<float> times;
+    for (uint32_t r = 0; r <= reps; r++) {
+      binius_transcript tr;
+      BGPU_CUDA(cudaEventRecord(e0, s));
+      if (int rc = binius_prover_prove(P, d_witness, &tr, stream)) return rc;
+      BGPU_CUDA(cudaEventRecord(e1, s));
+      BGPU_CUDA(cudaEventSynchronize(e1));
+      float t_ms = 0;
+      BGPU_CUDA(cudaEventElapsedTime(&t_ms, e0, e1));
+      if (r > 0) times.push_back(t_ms);
+      const std::vector<uint8_t>& tape = tr.t.tape();
+      if (ref.empty()) ref = tape;
+      else if (tape != ref)
+        return set_error(BINIUS_E_CUDA, "autotune: a launch shape changed the proof bytes");
+    }
+    std::sort(times.begin(), times.end());
+    *ms = times[times.size() / 2];
+    return BINIUS_OK;
+  };
+  int rc = BINIUS_OK;
+  Tuning best = start;
+  double best_ms = 0;
+  rc = score(best, &best_ms);
+  struct Knob {
+    uint32_t Tuning::*field;
+    uint32_t lo, hi;
+  };
+  const Knob knobs[4] = {{&Tuning::tail_log, 8, 12},
+                         {&Tuning::ntt_pass_layers, 6, 8},
+                         {&Tuning::merkle_leaf_fuse, 6, 8},
+                         {&Tuning::merkle_node_fuse, 7, 9}};
+  for (const Knob& k : knobs) {
+    for (uint32_t v = k.lo; v <= k.hi && !rc; v++) {
+      if (best.*(k.field) == v) continue;
+      Tuning cand = best;
+      cand.*(k.field) = v;
+      double ms = 0;
+      rc = score(cand, &ms);
+      if (!rc && ms < best_ms) {
+        best = cand;
+        best_ms = ms;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) {
+    P->tuning = start;
+    return rc;
+  }
+  P->tuning = best;
+  store_tuned(P);
+  if (h_out4) tuning_out(best, h_out4);
+  return clear_error();
 }
 
 int binius_prove(const binius_prover* P, const uint64_t* h_words, size_t n_words,

@@ -657,9 +657,9 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
   SHIFT_TRY(launched("dot2_kernel"));
   DeviceTranscript dt;
   SHIFT_TRY(dt.begin(t, s));
-  // rounds whose fold starts from at most kTailMaxLen elements run in the single-CTA tail
+  // rounds whose fold starts from at most tail_max_len() elements run in the single-CTA tail
   int tail0 = 1;
-  while (((uint64_t)kFlat >> (tail0 - 1)) > kTailMaxLen) tail0++;
+  while (((uint64_t)kFlat >> (tail0 - 1)) > tail_max_len()) tail0++;
   for (int round = 0; round < tail0; round++) {
     const uint64_t size = (uint64_t)kFlat >> round;  // before this round's fold
     uint32_t* ys = reinterpret_cast<uint32_t*>(slots + 2 * round);
@@ -774,10 +774,10 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
     BGPU_CUDA(cudaMemcpyAsync(run, init3, sizeof(init3), cudaMemcpyHostToDevice, s));
   }
   SHIFT_TRY(dt.begin(t, s));
-  // rounds whose fold starts from at most kTailMaxLen elements run in the single-CTA tail
+  // rounds whose fold starts from at most tail_max_len() elements run in the single-CTA tail
   uint32_t tail_n = 0;  // n_rem of the first tail round (0: no tail)
   for (uint32_t n_rem = log_words - 1; n_rem > 0; n_rem--)
-    if ((2ull << n_rem) <= kTailMaxLen) {
+    if ((2ull << n_rem) <= tail_max_len()) {
       tail_n = n_rem;
       break;
     }

@@ -93,3 +93,29 @@ def test_setup_and_prove_from_host_buffers(with_key_collection):
     t.message(b"\x01" * 16)
     out = p.prove_host(sc.witness, transcript=t)
     assert out[:16] == b"\x01" * 16 and len(out) == 16 + len(ref)
+
+
+def test_launch_shapes_change_no_bytes_and_autotune():
+    """Every launch-shape choice gives the oracle's proof (exact arithmetic); the autotuner picks
+    one in range, keeps the bytes and hands it to provers of the same shape set up later."""
+    sc = csm.synthetic_circuit(14, 12000, 3, seed=91, log_public=2)
+    prep = sc.cs.prepared()
+    ref = orc.prove(sc.witness, 2, prep.and_csr, prep.mul_csr, 1)
+    p = bg.Prover(bg.DeviceConstraintSystem(sc.cs.serialize()), 1)
+    w = torch.from_numpy(sc.witness.view(np.int64)).cuda()
+    assert p.tuning() == {"tail_log": 11, "ntt_pass_layers": 8, "merkle_leaf_fuse": 8,
+                          "merkle_node_fuse": 9}
+    for kw in ({"tail_log": 8}, {"tail_log": 12}, {"ntt_pass_layers": 4}, {"ntt_pass_layers": 6},
+               {"merkle_leaf_fuse": 5}, {"merkle_node_fuse": 5}, {"merkle_node_fuse": 7}):
+        p.set_tuning(**kw)
+        assert p.prove(w).finalize() == ref, kw
+        p.set_tuning(tail_log=11, ntt_pass_layers=8, merkle_leaf_fuse=8, merkle_node_fuse=9)
+    with pytest.raises(bg.ArgumentError):
+        p.set_tuning(tail_log=20)
+    best = p.autotune(w, reps=1)
+    assert 8 <= best["tail_log"] <= 12 and 6 <= best["ntt_pass_layers"] <= 8
+    assert p.tuning() == best
+    assert p.prove(w).finalize() == ref
+    p2 = bg.Prover(bg.DeviceConstraintSystem(sc.cs.serialize()), 1)
+    assert p2.tuning() == best
+    assert p2.prove(w).finalize() == ref

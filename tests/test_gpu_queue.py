@@ -64,7 +64,7 @@ def test_queue_with_tight_budget_serialises(statements):
 def test_queue_refuses_a_request_over_its_budget(statements):
     # the refusal is the host's: nothing is launched for it, and the queue keeps serving
     small, large = statements[0], statements[-1]
-    budget = small[1].workspace_bytes() + 8 * small[0].cs.committed_total_len
+    budget = small[1].workspace_bytes() + 8 * len(small[0].witness)
     assert large[1].workspace_bytes() > budget
     q = bg.ProveQueue(n_workers=2, hbm_budget_bytes=budget)
     with pytest.raises(bg.OutOfMemoryError):
