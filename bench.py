@@ -163,6 +163,8 @@ def fold_challenges(rng, n):
 # ----------------------------------------------------------------------------- clocks / peaks
 
 def sample_clocks_start(device):
+    """Starts nvidia-smi sampling every 50 ms and waits (up to 3 s) for its first sample, so
+    that the region measured next is covered from its start."""
     try:
         f = tempfile.NamedTemporaryFile(prefix="clocks_", suffix=".csv", delete=False)
         p = subprocess.Popen(
@@ -170,8 +172,11 @@ def sample_clocks_start(device):
              "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-             "--format=csv,noheader,nounits", "-lms", "100"],
+             "--format=csv,noheader,nounits", "-lms", "50"],
             stdout=f, stderr=subprocess.DEVNULL)
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 3.0 and os.path.getsize(f.name) == 0:
+            time.sleep(0.02)
         return p, f.name
     except (OSError, FileNotFoundError):
         return None, None
@@ -391,6 +396,7 @@ def batch_summary(torch, bg, device, n_requests, workers):
     for i in set(order):  # warm-up of every shape
         stmts[i][1].prove(stmts[i][2])
     t_seq, lone = one_at_a_time(torch, stmts, order)
+    run_queue(bg, stmts, order[:64], workers)  # warm: the workers' arenas and the pool grow once
     t_q, lat, prove, proofs = run_queue(bg, stmts, order, workers)
     identical = all(proofs[k] == lone[i] for k, i in enumerate(order))
     return {
@@ -419,6 +425,7 @@ def serve_summary(torch, bg, device, batch_ctx, n_requests, workers):
     for i in set(order):
         stmts[i][1].prove(stmts[i][2])
     t_seq, lone = one_at_a_time(torch, stmts, order)
+    run_queue(bg, stmts, order[:64], workers)  # warm: the workers' arenas and the pool grow once
     t_cap, _, _, _ = run_queue(bg, stmts, order, workers)
     rate = 0.7 * n_requests / t_cap
     arrivals = np.cumsum(np.random.default_rng(SEED + 13).exponential(1.0 / rate,

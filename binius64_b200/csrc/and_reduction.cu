@@ -353,60 +353,11 @@ __device__ __forceinline__ void reduce2_atomic(uint4 v0, uint4 v1, uint32_t* dst
   }
 }
 
-// Per-round constants of the MLE-check: the eq coordinate alpha the round binds and
-// 1 / (1 + alpha), both known before the loop starts.
-struct AndRoundConst {
-  uint4 alpha, inv_one_plus_alpha;
-};
-
-// Where a round's Fiat-Shamir step goes: the device transcript, the round's constants, the running
-// claim, the challenge's slot, the byte table to build for the next fold (or null) and the
-// round's CTA ticket.  ts == null: the kernel only evaluates.
-struct AndFinish {
-  TranscriptState* ts;
-  uint8_t* tape;
-  const AndRoundConst* rc;
-  uint4* claim;
-  uint4* r_out;
-  uint4* tab;
-  uint32_t* ticket;
-};
-
-// The Fiat-Shamir step of one MLE-check round, on the device: the round's sums (y_1, y_inf) ->
-// the round polynomial by RoundEvals2::interpolate_eq (prover/prover/src/protocols/sumcheck/
-// round_evals.rs:80-86) -> the truncated proof (c_1, c_2) (mlecheck::RoundProof::truncate) ->
-// the challenge r -> the next claim c_0 + c_1 r + c_2 r^2.  Warp 0 runs the chain; with a
-// table pointer the whole block then builds r's byte table for the next fold.  Every thread of
-// the block calls it.
-__device__ __noinline__ void and_round_finish(const AndFinish& f, const uint4* __restrict__ ys) {
-  __shared__ uint4 r_sh;
-  if (threadIdx.x < 32) {
-    DevTr st;
-    st.load(f.ts);
-    const uint4 y1 = __ldcg(ys), yinf = __ldcg(ys + 1);
-    const AndRoundConst rc = *f.rc;
-    const uint4 y0 =
-        gf_mul_warp(gf_add(*f.claim, gf_mul_warp(y1, rc.alpha)), rc.inv_one_plus_alpha);
-    const uint4 c0 = y0, c2 = yinf, c1 = gf_add(gf_add(y1, c0), c2);
-    const uint4 msg[2] = {c1, c2};
-    st.message_elems(f.tape, msg, 2);
-    const uint4 r = st.sample_elem();
-    *f.r_out = r;
-    *f.claim = gf_add(c0, gf_mul_warp(r, gf_add(c1, gf_mul_warp(c2, r))));
-    st.store(f.ts);
-    r_sh = r;
-  }
-  if (f.tab) {
-    __syncthreads();
-    dt_build_mul_table(r_sh, f.tab);
-  }
-}
-
 // Round evaluation without a fold: columns of length 2*half, eq of length half.
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256)
     and_mle_eval_kernel(const uint4* __restrict__ fa, const uint4* __restrict__ fb,
                         const uint4* __restrict__ fc, const uint4* __restrict__ eq, uint64_t half,
-                        uint32_t* __restrict__ out, AndFinish fin) {
+                        uint32_t* __restrict__ out) {
   u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < half;
        i += (uint64_t)gridDim.x * blockDim.x) {
@@ -416,8 +367,6 @@ __global__ void __launch_bounds__(256, 2)
     xor_into(sinf, clmul128(e, gf_mul(gf_add(a0, a1), gf_add(b0, b1))));
   }
   reduce2_atomic(reduce256(s1), reduce256(sinf), out);
-  if (fin.ts && last_cta_of_grid(fin.ticket))
-    and_round_finish(fin, reinterpret_cast<const uint4*>(out));
 }
 
 // Fold the three columns (length size) by the previous round's challenge *r_ptr, truncate eq
@@ -428,8 +377,7 @@ template <bool TAB>
 __global__ void __launch_bounds__(256, 2)
     and_mle_fold_eval_kernel(uint4* __restrict__ fa, uint4* __restrict__ fb, uint4* __restrict__ fc,
                              uint4* __restrict__ eq, uint64_t size, const uint4* __restrict__ r_ptr,
-                             const uint4* __restrict__ tab, uint32_t* __restrict__ out,
-                             AndFinish fin) {
+                             const uint4* __restrict__ tab, uint32_t* __restrict__ out) {
   pdl_wait();
   pdl_trigger();
   const uint64_t h = size >> 1, q = size >> 2;
@@ -466,16 +414,51 @@ __global__ void __launch_bounds__(256, 2)
     reduce2_atomic(reduce256(s1), reduce256(sinf), out);
   else
     reduce2_atomic(s1r, sinfr, out);
-  // the last CTA runs the round's Fiat-Shamir step; the fold above read the table it replaces
-  // only in CTAs that have all finished
-  if (fin.ts && last_cta_of_grid(fin.ticket))
-    and_round_finish(fin, reinterpret_cast<const uint4*>(out));
 }
 
+// Per-round constants of the MLE-check: the eq coordinate alpha the round binds and
+// 1 / (1 + alpha), both known before the loop starts.
+struct AndRoundConst {
+  uint4 alpha, inv_one_plus_alpha;
+};
+
+// The Fiat-Shamir step of one MLE-check round, on the device: the round's sums (y_1, y_inf) ->
+// the round polynomial by RoundEvals2::interpolate_eq (prover/prover/src/protocols/sumcheck/
+// round_evals.rs:80-86) -> the truncated proof (c_1, c_2) (mlecheck::RoundProof::truncate) ->
+// the challenge r -> the next claim c_0 + c_1 r + c_2 r^2.  Warp 0 runs the chain; with a
+// table pointer the whole block then builds r's byte table for the next fold.
+__global__ void __launch_bounds__(256)
+    and_round_finish_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
+                            const uint4* __restrict__ ys, const AndRoundConst* __restrict__ rc,
+                            uint4* __restrict__ claim, uint4* __restrict__ r_out,
+                            uint4* __restrict__ tab) {
+  pdl_wait();
+  pdl_trigger();
+  __shared__ uint4 r_sh;
+  if (threadIdx.x < 32) {
+    DevTr st;
+    st.load(ts);
+    const uint4 y1 = ys[0], yinf = ys[1];
+    const uint4 y0 =
+        gf_mul_warp(gf_add(*claim, gf_mul_warp(y1, rc->alpha)), rc->inv_one_plus_alpha);
+    const uint4 c0 = y0, c2 = yinf, c1 = gf_add(gf_add(y1, c0), c2);
+    const uint4 msg[2] = {c1, c2};
+    st.message_elems(tape, msg, 2);
+    const uint4 r = st.sample_elem();
+    *r_out = r;
+    *claim = gf_add(c0, gf_mul_warp(r, gf_add(c1, gf_mul_warp(c2, r))));
+    st.store(ts);
+    r_sh = r;
+  }
+  if (tab) {
+    __syncthreads();
+    dt_build_mul_table(r_sh, tab);
+  }
+}
 
 // The small last rounds of the MLE-check in one CTA (see bivariate_tail_kernel): per round fold
 // the three columns (length len -> len/2) by the previous challenge, truncate eq (len/2 -> len/4),
-// evaluate (y_1, y_inf) and let warp 0 run and_round_finish's Fiat-Shamir step with
+// evaluate (y_1, y_inf) and let warp 0 run and_round_finish_kernel's Fiat-Shamir step with
 // the round's constants rc[k].
 constexpr int kAndTailThreads = 512;
 __global__ void __launch_bounds__(kAndTailThreads)
@@ -592,8 +575,7 @@ hu128 phi_elem(uint32_t b) { return and_constants().phi[b & 255]; }
 int and_mle_eval(const uint4* d_a, const uint4* d_b, const uint4* d_c, const uint4* d_eq,
                  uint64_t half, uint32_t* d_out8, cudaStream_t s) {
   BGPU_CUDA(cudaMemsetAsync(d_out8, 0, 32, s));
-  and_mle_eval_kernel<<<grid_for(half, 256), 256, 0, s>>>(d_a, d_b, d_c, d_eq, half, d_out8,
-                                                          AndFinish{});
+  and_mle_eval_kernel<<<grid_for(half, 256), 256, 0, s>>>(d_a, d_b, d_c, d_eq, half, d_out8);
   BGPU_LAUNCH_CHECK("and_mle_eval_kernel");
   count_launch();
   return BINIUS_OK;
@@ -629,10 +611,8 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
   BGPU_CUDA(dev_alloc(&eq_big, 16 * n_chunks, s));
   BGPU_CUDA(dev_alloc(&fcols, 16 * 3 * N, s));
   BGPU_CUDA(dev_alloc(&eq, 16 * (N / 2), s));
-  // 64 univariate slots, then one (y_1, y_inf) slot pair per MLE-check round, then one CTA
-  // ticket per round; zeroed once
-  const size_t acc_bytes = 16 * (64 + 2 * (log_n + 1)) + 4 * (log_n + 1);
-  BGPU_CUDA(dev_alloc(&d_acc, acc_bytes, s));
+  // 64 univariate slots, then one (y_1, y_inf) slot pair per MLE-check round, zeroed once
+  BGPU_CUDA(dev_alloc(&d_acc, 16 * (64 + 2 * (log_n + 1)), s));
   uint4* mul_tab = nullptr;
   BGPU_CUDA(dev_alloc(&mul_tab, 16 * kMulTableEntries, s));
   // round constants (2 per round), the claim slot pair, the challenges
@@ -648,8 +628,7 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
     // univariate round
     PhiPowers pw;
     for (int i = 0; i < 8; i++) pw.p[i] = to_uint4(C.phi[1u << i]);
-    cudaError_t e = cudaMemsetAsync(d_acc, 0, acc_bytes, s);
-    uint32_t* tickets = d_acc + 4 * (64 + 2 * (log_n + 1));
+    cudaError_t e = cudaMemsetAsync(d_acc, 0, 16 * (64 + 2 * (log_n + 1)), s);
     if (e != cudaSuccess) { rc = cuda_error(e, "memset"); break; }
     univariate_round_kernel<<<148, kUniThreads, kUniSmem, s>>>(words, words + N, words + 2 * N,
                                                               eq_big, n_chunks, tab, pw, d_acc);
@@ -713,24 +692,25 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
       const uint32_t k = log_n - n_rem;
       uint32_t* acc = d_acc + 4 * (64 + 2 * k);
       const uint64_t size = 1ull << n_rem;
-      // the round's evaluation kernel runs its Fiat-Shamir step in its last CTA; the next round
-      // folds by this round's challenge through a table when it is large
-      const bool next_tab = n_rem > 1 && size >= kMulTableMinSize;
-      const AndFinish fin = {dt.state(), dt.tape(), d_consts + k, d_claim, d_chal + k,
-                             next_tab ? mul_tab : (uint4*)nullptr, tickets + k};
       if (n_rem == log_n) {
         and_mle_eval_kernel<<<grid_for(size / 2, 256), 256, 0, s>>>(fa, fb, fc, eq, size / 2,
-                                                                    acc, fin);
+                                                                    acc);
         e = cudaGetLastError();
       } else if (size * 2 >= kMulTableMinSize) {
         e = launch_pdl(and_mle_fold_eval_kernel<true>, grid_for(size / 2, 256), 256, 0, s, fa, fb,
-                       fc, eq, size * 2, d_chal + k - 1, mul_tab, acc, fin);
+                       fc, eq, size * 2, d_chal + k - 1, mul_tab, acc);
       } else {
         e = launch_pdl(and_mle_fold_eval_kernel<false>, grid_for(size / 2, 256), 256, 0, s, fa, fb,
-                       fc, eq, size * 2, d_chal + k - 1, (const uint4*)nullptr, acc, fin);
+                       fc, eq, size * 2, d_chal + k - 1, (const uint4*)nullptr, acc);
       }
       if (e != cudaSuccess) { rc = cuda_error(e, "AND MLE-check round"); break; }
-      count_launch(1);
+      // the next round folds by this round's challenge through a table when it is large
+      const bool next_tab = n_rem > 1 && size >= kMulTableMinSize;
+      e = launch_pdl(and_round_finish_kernel, 1, 256, 0, s, dt.state(), dt.tape(),
+                     reinterpret_cast<const uint4*>(acc), (const AndRoundConst*)(d_consts + k),
+                     d_claim, d_chal + k, next_tab ? mul_tab : (uint4*)nullptr);
+      if (e != cudaSuccess) { rc = cuda_error(e, "and_round_finish_kernel"); break; }
+      count_launch(2);
     }
     if (rc) break;
     if (tail_n) {

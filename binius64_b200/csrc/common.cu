@@ -13,6 +13,7 @@
 #endif
 
 #include "internal.h"
+#include "pdl.cuh"
 
 namespace bgpu {
 
@@ -274,7 +275,11 @@ void arena_release_thread() {
 
 namespace {
 thread_local Tuning t_tuning;
+thread_local bool t_pdl = true;
 }  // namespace
+
+bool pdl_enabled() { return t_pdl; }
+void set_pdl_enabled(bool on) { t_pdl = on; }
 
 const Tuning& tuning() { return t_tuning; }
 TuningScope::TuningScope(const Tuning& t) : saved_(t_tuning) { t_tuning = t; }

@@ -70,23 +70,4 @@ __device__ __forceinline__ void block_xor_sum(uint4 (&v)[NV]) {
   __syncthreads();
 }
 
-// True in every thread of the CTA that arrives last among the grid's CTAs.  Each CTA's atomics
-// into a round's sums are issued by its thread 0 (block_xor_reduce, and the reductions built like
-// it) before that thread's fence and ticket, so the last CTA, after its own fence, reads every
-// contribution (through L2: __ldcg).  `ticket` is zeroed before the launch; no CTA waits for
-// another, the last one merely continues with the round's Fiat-Shamir step.
-__device__ __forceinline__ bool last_cta_of_grid(uint32_t* ticket) {
-  __shared__ uint32_t s_last;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    const uint32_t n = gridDim.x * gridDim.y * gridDim.z;
-    s_last = atomicAdd(ticket, 1u) == n - 1 ? 1u : 0u;
-  }
-  __syncthreads();
-  const bool last = s_last != 0;
-  if (last) __threadfence();
-  return last;
-}
-
 }  // namespace bgpu

@@ -16,8 +16,7 @@
 // (selector_mle.rs) and rerandomisation (rerand_mle.rs), with the Gruen eq factor
 // (gruen32.rs, mle_to_sumcheck.rs).  Kernels produce the per-claim round sums (y_1, y_inf) and
 // fold by the previous challenge; each round's degree-2/3 coefficient algebra over all claims and
-// the Fiat-Shamir step run in im_round_finish (the last CTA of the round's last evaluation kernel)
-// on the device transcript, so a batched
+// the Fiat-Shamir step run in intmul_round_finish_kernel on the device transcript, so a batched
 // sumcheck of n rounds is one chain of launches with one read-back at its end.  The host sets each
 // sumcheck up (the eq points' alphas with one batched inversion, the powers of beta) and writes the
 // final evaluations.
@@ -106,107 +105,6 @@ __global__ void bit_columns_kernel(const uint64_t* __restrict__ e, uint64_t n, u
 
 // ---------------------------------------------------------------- sumcheck kernels
 
-// One claim of a batched MLE-check round: the slots (uint4 index into the round's sums) of its
-// y_1 and, for a bivariate product (deg 2), y_inf; deg 1 is a linear claim (RoundEvals1).  group
-// selects the eq point (alphas, Gruen prefix) the claim follows.
-struct ImClaim {
-  uint16_t y1, yinf;
-  uint8_t deg, group;
-  uint16_t pad;
-};
-// The eq coordinate a group's MLE-check binds in one round and 1 / (1 + alpha).
-struct ImAlpha {
-  uint4 alpha, inv_one_plus_alpha;
-};
-constexpr int kImFinishThreads = 256;
-constexpr uint32_t kImMaxClaims = 256;
-
-// Where a batched round's Fiat-Shamir step goes (run by the last CTA of the round's last
-// evaluation kernel, after the round's other evaluation kernels have completed): the device
-// transcript, the round's sums (slots), the claims, the running sums and Gruen prefixes, the
-// round's alphas, the powers of beta, the message length, the challenge's slot and the round's
-// CTA ticket.  ts == null: the kernel only evaluates.
-struct ImFinish {
-  TranscriptState* ts;
-  uint8_t* tape;
-  const uint4* slots;
-  const ImClaim* claims;
-  uint32_t n_claims;
-  uint4* sums;
-  uint4* prefix;
-  const ImAlpha* alphas;
-  uint32_t n_groups;
-  const uint4* beta_pow;
-  uint32_t msg_coeffs;
-  uint4* r_out;
-  uint32_t* ticket;
-};
-
-// The Fiat-Shamir step of one round of a batched MLE-check (BatchSumcheckProver over decorated
-// MLE-check provers, batch.rs:41-135 + mle_to_sumcheck.rs + gruen32.rs), on the device.  Claim i:
-// prime_i = interpolate_eq(sum_i, y_1, [y_inf], alpha) (RoundEvals2 / RoundEvals1,
-// round_evals.rs:23-27, 80-87), all_i = round_coeffs_by_eq(prime_i, alpha) * prefix
-// (round_evals.rs:145-156); the round message is sum_i beta^i all_i without its top coefficient
-// (msg_coeffs elements).  Claims are spread over the block and block-reduced; warp 0 writes the
-// message and samples r; then every claim's sum becomes prime_i(r) and every group's prefix
-// takes the factor (1 + r + alpha).
-// Every thread of the (kImFinishThreads-thread) block calls it; the round's sums are read through
-// L2 (the round's CTAs added them atomically).
-__device__ __noinline__ void im_round_finish(const ImFinish& f) {
-  __shared__ uint4 s_prime[kImMaxClaims][3];
-  __shared__ uint4 s_r;
-  uint4 acc[4] = {gf_zero(), gf_zero(), gf_zero(), gf_zero()};
-  for (uint32_t i = threadIdx.x; i < f.n_claims; i += blockDim.x) {
-    const ImClaim c = f.claims[i];
-    const ImAlpha a = f.alphas[c.group];
-    const uint4 y1 = __ldcg(f.slots + c.y1);
-    const uint4 y0 = gf_mul_nl(gf_add(f.sums[i], gf_mul_nl(y1, a.alpha)), a.inv_one_plus_alpha);
-    uint4 p0 = y0, p1, p2 = gf_zero();
-    if (c.deg == 2) {
-      const uint4 yinf = __ldcg(f.slots + c.yinf);
-      p1 = gf_add(gf_add(y1, y0), yinf);
-      p2 = yinf;
-    } else {
-      p1 = gf_add(y1, y0);
-    }
-    s_prime[i][0] = p0;
-    s_prime[i][1] = p1;
-    s_prime[i][2] = p2;
-    uint4 oma = a.alpha;
-    oma.x ^= 1u;
-    const uint4 sc = gf_mul_nl(f.prefix[c.group], f.beta_pow[i]);
-    gf_add_into(acc[0], gf_mul_nl(gf_mul_nl(p0, oma), sc));
-    gf_add_into(acc[1], gf_mul_nl(gf_add(gf_mul_nl(p1, oma), p0), sc));
-    gf_add_into(acc[2], gf_mul_nl(gf_add(gf_mul_nl(p2, oma), p1), sc));
-    gf_add_into(acc[3], gf_mul_nl(p2, sc));
-  }
-  block_xor_sum<4>(acc);
-  if (threadIdx.x < 32) {
-    DevTr st;
-    st.load(f.ts);
-    st.message_elems(f.tape, acc, f.msg_coeffs);
-    const uint4 r = st.sample_elem();
-    __syncwarp();
-    if (threadIdx.x == 0) {
-      *f.r_out = r;
-      st.store(f.ts);
-      s_r = r;
-    }
-  }
-  __syncthreads();
-  const uint4 r = s_r;
-  for (uint32_t i = threadIdx.x; i < f.n_claims; i += blockDim.x)
-    f.sums[i] = gf_add(s_prime[i][0], gf_mul_nl(r, gf_add(s_prime[i][1], gf_mul_nl(r, s_prime[i][2]))));
-  for (uint32_t g = threadIdx.x; g < f.n_groups; g += blockDim.x) {
-    uint4 fac = gf_add(r, f.alphas[g].alpha);
-    fac.x ^= 1u;
-    f.prefix[g] = gf_mul_nl(f.prefix[g], fac);
-  }
-}
-
-
-
-
 __device__ __forceinline__ uint4 fold1(uint4 lo, uint4 hi, uint4 r) {
   return gf_add(lo, gf_mul(r, gf_add(hi, lo)));
 }
@@ -220,7 +118,7 @@ template <bool SMALL>
 __global__ void __launch_bounds__(kT)
     biv_round_kernel(uint4* __restrict__ set, uint64_t L, uint64_t stride,
                      const uint4* __restrict__ eq, const uint4* __restrict__ r_ptr,
-                     uint32_t* __restrict__ out, ImFinish fin) {
+                     uint32_t* __restrict__ out) {
   pdl_wait();
   pdl_trigger();
   const bool fold = r_ptr != nullptr;
@@ -262,7 +160,6 @@ __global__ void __launch_bounds__(kT)
   }
   uint4 v[2] = {SMALL ? s1r : reduce256(s1), SMALL ? sinfr : reduce256(sinf)};
   block_xor_reduce<2>(v, out + 8 * p);
-  if (fin.ts && last_cta_of_grid(fin.ticket)) im_round_finish(fin);
 }
 
 // Column k of `set` (current length L): out[4k..] += sum eq[i] col_k[L/2 + i], with the same
@@ -271,7 +168,7 @@ template <bool SMALL>
 __global__ void __launch_bounds__(kT)
     lin_round_kernel(uint4* __restrict__ set, uint64_t L, uint64_t stride,
                      const uint4* __restrict__ eq, const uint4* __restrict__ r_ptr,
-                     uint32_t* __restrict__ out, ImFinish fin) {
+                     uint32_t* __restrict__ out) {
   pdl_wait();
   pdl_trigger();
   const bool fold = r_ptr != nullptr;
@@ -299,7 +196,6 @@ __global__ void __launch_bounds__(kT)
   }
   uint4 v[1] = {SMALL ? s1r : reduce256(s1)};
   block_xor_reduce<1>(v, out + 4 * k);
-  if (fin.ts && last_cta_of_grid(fin.ticket)) im_round_finish(fin);
 }
 
 // Selector claim k with its own eq_k: out[8k..] += (sum eq_k[i] (s1 (sel1 + 1) + 1),
@@ -398,6 +294,88 @@ __global__ void __launch_bounds__(kT)
   block_xor_reduce<1>(r, out);
 }
 
+// One claim of a batched MLE-check round: the slots (uint4 index into the round's sums) of its
+// y_1 and, for a bivariate product (deg 2), y_inf; deg 1 is a linear claim (RoundEvals1).  group
+// selects the eq point (alphas, Gruen prefix) the claim follows.
+struct ImClaim {
+  uint16_t y1, yinf;
+  uint8_t deg, group;
+  uint16_t pad;
+};
+// The eq coordinate a group's MLE-check binds in one round and 1 / (1 + alpha).
+struct ImAlpha {
+  uint4 alpha, inv_one_plus_alpha;
+};
+constexpr int kImFinishThreads = 256;
+constexpr uint32_t kImMaxClaims = 256;
+
+// The Fiat-Shamir step of one round of a batched MLE-check (BatchSumcheckProver over decorated
+// MLE-check provers, batch.rs:41-135 + mle_to_sumcheck.rs + gruen32.rs), on the device.  Claim i:
+// prime_i = interpolate_eq(sum_i, y_1, [y_inf], alpha) (RoundEvals2 / RoundEvals1,
+// round_evals.rs:23-27, 80-87), all_i = round_coeffs_by_eq(prime_i, alpha) * prefix
+// (round_evals.rs:145-156); the round message is sum_i beta^i all_i without its top coefficient
+// (msg_coeffs elements).  Claims are spread over the block and block-reduced; warp 0 writes the
+// message and samples r; then every claim's sum becomes prime_i(r) and every group's prefix
+// takes the factor (1 + r + alpha).
+__global__ void __launch_bounds__(kImFinishThreads)
+    intmul_round_finish_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
+                               const uint4* __restrict__ slots, const ImClaim* __restrict__ claims,
+                               uint32_t n_claims, uint4* __restrict__ sums,
+                               uint4* __restrict__ prefix, const ImAlpha* __restrict__ alphas,
+                               uint32_t n_groups, const uint4* __restrict__ beta_pow,
+                               uint32_t msg_coeffs, uint4* __restrict__ r_out) {
+  pdl_wait();
+  pdl_trigger();
+  __shared__ uint4 s_prime[kImMaxClaims][3];
+  __shared__ uint4 s_r;
+  uint4 acc[4] = {gf_zero(), gf_zero(), gf_zero(), gf_zero()};
+  for (uint32_t i = threadIdx.x; i < n_claims; i += blockDim.x) {
+    const ImClaim c = claims[i];
+    const ImAlpha a = alphas[c.group];
+    const uint4 y1 = slots[c.y1];
+    const uint4 y0 = gf_mul_nl(gf_add(sums[i], gf_mul_nl(y1, a.alpha)), a.inv_one_plus_alpha);
+    uint4 p0 = y0, p1, p2 = gf_zero();
+    if (c.deg == 2) {
+      const uint4 yinf = slots[c.yinf];
+      p1 = gf_add(gf_add(y1, y0), yinf);
+      p2 = yinf;
+    } else {
+      p1 = gf_add(y1, y0);
+    }
+    s_prime[i][0] = p0;
+    s_prime[i][1] = p1;
+    s_prime[i][2] = p2;
+    uint4 oma = a.alpha;
+    oma.x ^= 1u;
+    const uint4 sc = gf_mul_nl(prefix[c.group], beta_pow[i]);
+    gf_add_into(acc[0], gf_mul_nl(gf_mul_nl(p0, oma), sc));
+    gf_add_into(acc[1], gf_mul_nl(gf_add(gf_mul_nl(p1, oma), p0), sc));
+    gf_add_into(acc[2], gf_mul_nl(gf_add(gf_mul_nl(p2, oma), p1), sc));
+    gf_add_into(acc[3], gf_mul_nl(p2, sc));
+  }
+  block_xor_sum<4>(acc);
+  if (threadIdx.x < 32) {
+    DevTr st;
+    st.load(ts);
+    st.message_elems(tape, acc, msg_coeffs);
+    const uint4 r = st.sample_elem();
+    __syncwarp();
+    if (threadIdx.x == 0) {
+      *r_out = r;
+      st.store(ts);
+      s_r = r;
+    }
+  }
+  __syncthreads();
+  const uint4 r = s_r;
+  for (uint32_t i = threadIdx.x; i < n_claims; i += blockDim.x)
+    sums[i] = gf_add(s_prime[i][0], gf_mul_nl(r, gf_add(s_prime[i][1], gf_mul_nl(r, s_prime[i][2]))));
+  for (uint32_t g = threadIdx.x; g < n_groups; g += blockDim.x) {
+    uint4 f = gf_add(r, alphas[g].alpha);
+    f.x ^= 1u;
+    prefix[g] = gf_mul_nl(prefix[g], f);
+  }
+}
 
 // ---------------------------------------------------------------- host side
 
@@ -516,41 +494,34 @@ class IntMulDevice {
   }
   // Fused round launches on multilinears of current length L (fold from 2L first by *r_ptr when
   // r_ptr is set).
-  // With fin set, the launch is the round's last and its last CTA runs the round's Fiat-Shamir
-  // step (batch_finish).
   int biv_round(uint4* set, uint32_t pairs, uint64_t L, const uint4* eq, const uint4* r_ptr,
-                uint32_t* out, const ImFinish& fin = ImFinish{}) {
+                uint32_t* out) {
     dim3 grid(blocks_for(L / 2, 148 * 2), pairs);
     if (L <= kSmallRound)
-      BGPU_CUDA(launch_pdl(biv_round_kernel<true>, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out,
-                           fin));
+      BGPU_CUDA(launch_pdl(biv_round_kernel<true>, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out));
     else
-      BGPU_CUDA(launch_pdl(biv_round_kernel<false>, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out,
-                           fin));
+      BGPU_CUDA(launch_pdl(biv_round_kernel<false>, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out));
     return check("biv_round_kernel");
   }
   int lin_round(uint4* set, uint32_t cols, uint64_t L, const uint4* eq, const uint4* r_ptr,
-                uint32_t* out, const ImFinish& fin = ImFinish{}) {
+                uint32_t* out) {
     dim3 grid(blocks_for(L / 2, 148 * 2), cols);
     if (L <= kSmallRound)
-      BGPU_CUDA(launch_pdl(lin_round_kernel<true>, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out,
-                           fin));
+      BGPU_CUDA(launch_pdl(lin_round_kernel<true>, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out));
     else
-      BGPU_CUDA(launch_pdl(lin_round_kernel<false>, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out,
-                           fin));
+      BGPU_CUDA(launch_pdl(lin_round_kernel<false>, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out));
     return check("lin_round_kernel");
   }
   // A batched MLE-check whose rounds run on the device transcript: batch_begin uploads the claims,
   // each eq point's per-round alpha and 1/(1 + alpha) (one batched inversion), the powers of
   // beta and the initial sums; each round launches its evaluation kernels into batch_slots(t)
-  // (folding by batch_r(t)), the last of them with batch_finish(t); batch_read queues the copy-back of the
+  // (folding by batch_r(t)) and then batch_round; batch_read queues the copy-back of the
   // challenges and the transcript, batch_end hands the transcript back to the host.
   struct DevBatch {
     uint32_t n = 0, n_claims = 0, n_groups = 0, msg = 3, per_round = 0;
     ImClaim* claims = nullptr;
     ImAlpha* alphas = nullptr;
     uint4 *sums = nullptr, *prefix = nullptr, *beta = nullptr, *chal = nullptr, *slots = nullptr;
-    uint32_t* tickets = nullptr;  // one CTA ticket per round
     DeviceTranscript dt;
   };
   int batch_begin(DevBatch& b, const std::vector<ImClaim>& claims,
@@ -566,7 +537,7 @@ class IntMulDevice {
     for (const auto& c : claims) b.msg = c.deg == 2 ? 3 : b.msg;
     const size_t n_cl = (8 * claims.size() + 15) / 16, n_al = 2ull * b.n * b.n_groups;
     const size_t host_elems = n_cl + b.n_claims + b.n_groups + n_al + b.n_claims;
-    const size_t total = host_elems + b.n + (size_t)b.n * per_round + (b.n + 3) / 4;
+    const size_t total = host_elems + b.n + (size_t)b.n * per_round;
     uint4* base = nullptr;
     if (int rc = alloc(&base, total)) return rc;
     std::vector<uint4> h(host_elems, make_uint4(0, 0, 0, 0));
@@ -599,8 +570,7 @@ class IntMulDevice {
     b.beta = b.prefix + b.n_groups + n_al;
     b.chal = base + host_elems;
     b.slots = b.chal + b.n;
-    b.tickets = reinterpret_cast<uint32_t*>(b.slots + (size_t)b.n * per_round);
-    BGPU_CUDA(cudaMemsetAsync(b.slots, 0, 16ull * b.n * per_round + 4ull * b.n, s_));
+    BGPU_CUDA(cudaMemsetAsync(b.slots, 0, 16ull * b.n * per_round, s_));
     return b.dt.begin(t_, s_);
   }
   static uint32_t* batch_slots(DevBatch& b, uint32_t t) {
@@ -609,21 +579,13 @@ class IntMulDevice {
   static const uint4* batch_r(const DevBatch& b, uint32_t t) {
     return t ? b.chal + t - 1 : nullptr;
   }
-  // The Fiat-Shamir step of round t, for the round's last evaluation launch.
-  static ImFinish batch_finish(DevBatch& b, uint32_t t) {
-    return ImFinish{b.dt.state(),
-                    b.dt.tape(),
-                    b.slots + (size_t)t * b.per_round,
-                    b.claims,
-                    b.n_claims,
-                    b.sums,
-                    b.prefix,
-                    b.alphas + (size_t)t * b.n_groups,
-                    b.n_groups,
-                    b.beta,
-                    b.msg,
-                    b.chal + t,
-                    b.tickets + t};
+  int batch_round(DevBatch& b, uint32_t t) {
+    BGPU_CUDA(launch_pdl(intmul_round_finish_kernel, 1, kImFinishThreads, 0, s_, b.dt.state(),
+                         b.dt.tape(), (const uint4*)(b.slots + (size_t)t * b.per_round),
+                         (const ImClaim*)b.claims, b.n_claims, b.sums, b.prefix,
+                         (const ImAlpha*)(b.alphas + (size_t)t * b.n_groups), b.n_groups,
+                         (const uint4*)b.beta, b.msg, b.chal + t));
+    return check("intmul_round_finish_kernel");
   }
   int batch_read(DevBatch& b, StagedReads& rd, std::vector<hu128>& ch) {
     ch.resize(b.n);
@@ -685,8 +647,9 @@ int IntMulDevice::layer(uint4* set, uint32_t pairs, std::vector<hu128>& point,
     if (int rc = batch_begin(b, cl, {&point}, claims, beta, 2 * pairs)) return rc;
     for (uint32_t t = 0; t < n; t++) {
       if (int rc = biv_round(set, pairs, 1ull << (n - t), level(eq_, n - t - 1), batch_r(b, t),
-                             batch_slots(b, t), batch_finish(b, t)))
+                             batch_slots(b, t)))
         return rc;
+      if (int rc = batch_round(b, t)) return rc;
     }
     std::vector<hu128> ch, last(4 * pairs);
     StagedReads rd(s_);
@@ -883,9 +846,8 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
         BGPU_CUDA(launch_pdl(selector_round_kernel<false>, grid, kT, 0, s_, (const uint4*)sel,
                              bcols, L, N, level(sel_eqs, n_ - t - 1), N, rp, out));
       if (int rc = check("selector_round_kernel")) return rc;
-      if (int rc = biv_round(croot, 1, L, level(eq_, n_ - t - 1), rp, out + 4 * 128,
-                             batch_finish(b, t)))
-        return rc;
+      if (int rc = biv_round(croot, 1, L, level(eq_, n_ - t - 1), rp, out + 4 * 128)) return rc;
+      if (int rc = batch_round(b, t)) return rc;
     }
     std::vector<hu128> ch, last_cols(128), last_roots(6);
     StagedReads rd(s_);
@@ -952,9 +914,8 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
       const uint4* rp = batch_r(b, t);
       if (int rc = biv_round(leaves, 97, L, level(eq_, n_ - t - 1), rp, out)) return rc;
       if (int rc = lin_round(lo0, 1, L, level(eq_, n_ - t - 1), rp, out + 4 * 194)) return rc;
-      if (int rc = lin_round(bcols, 64, L, level(eq2_, n_ - t - 1), rp, out + 4 * 195,
-                             batch_finish(b, t)))
-        return rc;
+      if (int rc = lin_round(bcols, 64, L, level(eq2_, n_ - t - 1), rp, out + 4 * 195)) return rc;
+      if (int rc = batch_round(b, t)) return rc;
     }
     std::vector<hu128> ch, last_leaves(2 * 194), last_lo(2), last_b(2 * 64);
     StagedReads rd(s_);

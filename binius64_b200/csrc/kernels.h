@@ -41,28 +41,6 @@ int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[1
 int bivariate_fold_eval_dev(uint4* d_a, uint4* d_b, uint64_t size, const uint4* d_r,
                             const uint4* d_tab, uint32_t* d_out8, cudaStream_t s);
 class DeviceTranscript;
-// A plain bivariate product round's Fiat-Shamir step run by the last CTA of the round's
-// evaluation kernel (see bivariate_round_finish for what it does; no commitment is written):
-// the device transcript, the claim (claim_init when set, the first round), the challenge's slot,
-// the byte table to build for the next fold (or null), and the round's CTA ticket (zeroed before
-// the launch).
-struct BivFinish {
-  void* ts;
-  uint8_t* tape;
-  const uint4* claim_init;
-  uint4* claim;
-  uint4* r_out;
-  uint4* tab;
-  uint32_t* ticket;
-};
-BivFinish bivariate_finish_args(const DeviceTranscript& dt, const uint4* d_claim_init,
-                                uint4* d_claim, uint4* d_r_out, uint4* d_tab, uint32_t* d_ticket);
-// bivariate_eval / bivariate_fold_eval_dev whose last CTA runs the round's Fiat-Shamir step.
-int bivariate_eval_finish(const uint4* d_a, const uint4* d_b, uint64_t half, uint32_t* d_out8,
-                          const BivFinish& fin, cudaStream_t s);
-int bivariate_fold_eval_finish(uint4* d_a, uint4* d_b, uint64_t size, const uint4* d_r,
-                               const uint4* d_tab, uint32_t* d_out8, const BivFinish& fin,
-                               cudaStream_t s);
 // The device Fiat-Shamir step of a plain bivariate product round: reads (y_1, y_inf) at d_ys
 // and the claim (d_claim_init if set, else d_claim), writes the message (c_0, c_1) and then the
 // 32 bytes at d_commitment if set, samples r into d_r_out, updates d_claim and, with d_tab,

@@ -95,9 +95,6 @@ struct DevFri {
   // FRIFoldProver::execute_fold_round (prover/prover/src/fri/fold.rs:117-175): on a commit round,
   // folds by the challenges received since the last commit (device memory) and commits the new
   // codeword; *d_root is then the device address of the new tree's root.
-  // Whether execute() commits in the current round.
-  bool commits_now() const { return next_commit >= 0 && (int64_t)curr_round == next_commit; }
-
   int execute(bool* committed, const uint8_t** d_root) {
     *committed = false;
     if (next_commit < 0 || (int64_t)curr_round != next_commit) return BINIUS_OK;
@@ -244,15 +241,13 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
   BGPU_CUDA(dev_alloc(&b, 16 * N, s));
   BGPU_CUDA(dev_alloc(&eq_r, 16 * 128, s));
   BGPU_CUDA(dev_alloc(&d_small, 16 * 128, s));
-  // BaseFold round state: sums (2 per round), the claim pair, challenges, r's byte table, one
-  // CTA ticket per round (for rounds whose evaluation kernel runs the Fiat-Shamir step itself)
-  const uint64_t n_dev = 2ull * n + 2 + n + kMulTableEntries + (n + 3) / 4;
+  // BaseFold round state: sums (2 per round), the claim pair, challenges, r's byte table
+  const uint64_t n_dev = 2ull * n + 2 + n + kMulTableEntries;
   BGPU_CUDA(dev_alloc(&dev, 16 * n_dev, s));
   uint4* slots = dev;
   uint4* claim = dev + 2 * n;  // [0] running claim, [1] initial claim
   uint4* chal = claim + 2;
   uint4* tab = chal + n;
-  uint32_t* tickets = reinterpret_cast<uint32_t*>(tab + kMulTableEntries);
   int rc = BINIUS_OK;
   {
     DevFri fri(*P, *C, s, chal);
@@ -287,7 +282,6 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
       e = cudaMemcpyAsync(claim + 1, &sum, 16, cudaMemcpyHostToDevice, s);
       if (e != cudaSuccess) { rc = cuda_error(e, "claim upload"); break; }
       e = cudaMemsetAsync(slots, 0, 32ull * n, s);
-      if (e == cudaSuccess) e = cudaMemsetAsync(tickets, 0, 4ull * n, s);
       if (e != cudaSuccess) { rc = cuda_error(e, "round sums"); break; }
       // rs_eq_ind = fold_b128_elems_inplace(suffix_tensor, eq(r'')) in place in b
       if ((rc = fold_b128_elems(b, b, N, eq_r, s))) break;
@@ -314,27 +308,17 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
       for (uint32_t round = 0; round < tail0 && round < n && rc == BINIUS_OK; round++) {
         const uint64_t size = N >> round;
         uint32_t* ys = reinterpret_cast<uint32_t*>(slots + 2 * round);
-        const bool next_tab = round + 1 < n && size >= kMulTableMinSize;
-        // a round without a FRI commit runs its Fiat-Shamir step in its evaluation kernel's last
-        // CTA; a commit round folds and commits between the sums and the message
-        const bool commits = fri.commits_now();
-        const BivFinish fin =
-            commits ? BivFinish{}
-                    : bivariate_finish_args(dt, round == 0 ? claim + 1 : nullptr, claim,
-                                            chal + round, next_tab ? tab : nullptr,
-                                            tickets + round);
         if (round == 0)
-          rc = bivariate_eval_finish(a, b, size / 2, ys, fin, s);
+          rc = bivariate_eval(a, b, size / 2, ys, s);
         else
-          rc = bivariate_fold_eval_finish(a, b, size * 2, chal + round - 1,
-                                          size * 2 >= kMulTableMinSize ? tab : nullptr, ys, fin,
-                                          s);
+          rc = bivariate_fold_eval_dev(a, b, size * 2, chal + round - 1,
+                                       size * 2 >= kMulTableMinSize ? tab : nullptr, ys, s);
         if (rc) break;
         bool committed = false;
         const uint8_t* d_root = nullptr;
         if ((rc = fri.execute(&committed, &d_root))) break;
-        if (commits &&
-            (rc = bivariate_round_finish(dt, slots + 2 * round, round == 0 ? claim + 1 : nullptr,
+        const bool next_tab = round + 1 < n && size >= kMulTableMinSize;
+        if ((rc = bivariate_round_finish(dt, slots + 2 * round, round == 0 ? claim + 1 : nullptr,
                                          claim, committed ? d_root : nullptr, chal + round,
                                          next_tab ? tab : nullptr, s)))
           break;

@@ -17,6 +17,12 @@ __device__ __forceinline__ void pdl_trigger() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// Whether the calling thread's launch_pdl calls use programmatic dependent launch (default on).
+// A dependent grid scheduled early holds its CTAs' SM slots while it waits; a thread that
+// proves beside others on the same GPU (a proving-queue worker) may launch plainly instead.
+bool pdl_enabled();
+void set_pdl_enabled(bool on);
+
 template <typename... KArgs, typename... Args>
 cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
                        cudaStream_t s, Args... args) {
@@ -29,7 +35,7 @@ cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t s
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
 }
 

@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "pdl.cuh"
 #include "transcript.h"
 
 using namespace bgpu;
@@ -89,6 +90,7 @@ void binius_queue::worker_loop(uint32_t w) {
   set_blocking_waits(true, n_workers <= std::max(1u, std::thread::hardware_concurrency()) ? 100.0
                                                                                            : 0.0);
   cudaStream_t s = streams[w];
+  set_pdl_enabled(true);
   uint64_t held = 0;  // this worker's arena bytes, counted in in_use
   for (;;) {
     std::shared_ptr<Request> r;

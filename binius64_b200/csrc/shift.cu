@@ -303,6 +303,23 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// out[0] += <x[off0 ..], eq>, out[1] += <x[off1 ..], eq> over len elements.
+__global__ void __launch_bounds__(256)
+    dot2_kernel(const uint4* __restrict__ x, uint64_t off0, uint64_t off1,
+                const uint4* __restrict__ eq, uint64_t len, uint32_t* __restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
+  u256 a0 = {0, 0, 0, 0}, a1 = {0, 0, 0, 0};
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < len;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint4 e = eq[i];
+    xor_into(a0, clmul128(x[off0 + i], e));
+    xor_into(a1, clmul128(x[off1 + i], e));
+  }
+  uint4 v[2] = {reduce256(a0), reduce256(a1)};
+  block_xor_reduce<2>(v, out);
+}
+
 // Per-round constants of the phase-2 batch, known before the loop: the in/out check's current
 // eq coordinate zc = z[gn - 1] and 1 / (1 + zc) (used when the round is past the public
 // segment's extra variables), the coordinate alpha_dec the Gruen eq prefix absorbs (0 while the
@@ -312,42 +329,29 @@ struct ShiftRoundConst {
   uint32_t early, pad[3];
 };
 
-// Where a phase-2 round's Fiat-Shamir step goes (run by the last CTA of the round's in/out dot
-// product kernel): the device transcript, the round's sums ys = (y_1, y_inf) of the bivariate
-// product (W, M) and (lo, hi) of the in/out check's dot products, the round's constants, the
-// first round's in/out (lo, hi) when set, z0, beta, the three running values, the challenge's
-// slot, the next fold's byte table (or null) and the round's CTA ticket.  ts == null: the kernel
-// only evaluates.
-struct ShiftFinish {
-  TranscriptState* ts;
-  uint8_t* tape;
-  const uint4* ys;
-  const ShiftRoundConst* rc;
-  const uint4* init_lohi;
-  uint4 z0, beta;
-  uint4* st3;
-  uint4* r_out;
-  uint4* tab;
-  uint32_t* ticket;
-};
-
-// The Fiat-Shamir step of one phase-2 round on the device.  st3 = (shift claim, in/out claim,
-// Gruen eq prefix).  The batch message is the shift round's (s_0, s_1) plus beta times the in/out
-// check's Gruen-scaled (d_0, d_1) (MleToSumCheckDecorator + batch_prove); then r is sampled and
-// the three running values advance.  When init_lohi is set (the first round) the in/out claim is
-// first set to lo + (hi - lo) z0 from it.  Every thread of the block calls it.
-__device__ __noinline__ void shift_round_finish(const ShiftFinish& f) {
+// The Fiat-Shamir step of one phase-2 round on the device.  ys = (y_1, y_inf) of the bivariate
+// product (r_j_witness, M) and (lo, hi) of the in/out check's dot products; st3 = (shift claim,
+// in/out claim, Gruen eq prefix).  The batch message is the shift round's (s_0, s_1) plus beta
+// times the in/out check's Gruen-scaled (d_0, d_1) (MleToSumCheckDecorator + batch_prove); then r
+// is sampled and the three running values advance.  When init_lohi is set (the first round) the
+// in/out claim is first set to lo + (hi - lo) z0 from it.
+__global__ void __launch_bounds__(256)
+    shift_round_finish_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
+                              const uint4* __restrict__ ys, const ShiftRoundConst* __restrict__ rc,
+                              const uint4* __restrict__ init_lohi, uint4 z0, uint4 beta,
+                              uint4* __restrict__ st3, uint4* __restrict__ r_out,
+                              uint4* __restrict__ tab) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ uint4 r_sh;
   if (threadIdx.x < 32) {
     DevTr st;
-    st.load(f.ts);
-    const ShiftRoundConst c = *f.rc;
-    uint4* st3 = f.st3;
+    st.load(ts);
+    const ShiftRoundConst c = *rc;
     uint4 inout = st3[1];
-    if (f.init_lohi)
-      inout = gf_add(f.init_lohi[0], gf_mul_warp(gf_add(f.init_lohi[1], f.init_lohi[0]), f.z0));
-    const uint4 y1 = __ldcg(f.ys), yinf = __ldcg(f.ys + 1), lo = __ldcg(f.ys + 2),
-                hi = __ldcg(f.ys + 3);
+    if (init_lohi)
+      inout = gf_add(init_lohi[0], gf_mul_warp(gf_add(init_lohi[1], init_lohi[0]), z0));
+    const uint4 y1 = ys[0], yinf = ys[1], lo = ys[2], hi = ys[3];
     const uint4 s0 = gf_add(st3[0], y1), s2 = yinf, s1 = gf_add(gf_add(y1, s0), s2);
     uint4 iy0, iy1;
     if (c.early) {
@@ -363,49 +367,28 @@ __device__ __noinline__ void shift_round_finish(const ShiftFinish& f) {
     const uint4 eqp = st3[2];
     const uint4 d0 = gf_mul_warp(gf_mul_warp(q0, one_a), eqp);
     const uint4 d1 = gf_mul_warp(gf_add(gf_mul_warp(q1, one_a), q0), eqp);
-    const uint4 msg[2] = {gf_add(s0, gf_mul_warp(f.beta, d0)),
-                          gf_add(s1, gf_mul_warp(f.beta, d1))};
-    st.message_elems(f.tape, msg, 2);
+    const uint4 msg[2] = {gf_add(s0, gf_mul_warp(beta, d0)), gf_add(s1, gf_mul_warp(beta, d1))};
+    st.message_elems(tape, msg, 2);
     const uint4 r = st.sample_elem();
-    *f.r_out = r;
+    *r_out = r;
     st3[0] = gf_add(s0, gf_mul_warp(r, gf_add(s1, gf_mul_warp(s2, r))));
     st3[1] = gf_add(q0, gf_mul_warp(q1, r));
-    uint4 fr = gf_add(r, c.alpha_dec);
-    fr.x ^= 1u;
-    st3[2] = gf_mul_warp(eqp, fr);
-    st.store(f.ts);
+    uint4 f = gf_add(r, c.alpha_dec);
+    f.x ^= 1u;
+    st3[2] = gf_mul_warp(eqp, f);
+    st.store(ts);
     r_sh = r;
   }
-  if (f.tab) {
+  if (tab) {
     __syncthreads();
-    dt_build_mul_table(r_sh, f.tab);
+    dt_build_mul_table(r_sh, tab);
   }
-}
-
-// out[0] += <x[off0 ..], eq>, out[1] += <x[off1 ..], eq> over len elements; with fin.ts set, the
-// last CTA then runs the phase-2 round's Fiat-Shamir step.
-__global__ void __launch_bounds__(256, 2)
-    dot2_kernel(const uint4* __restrict__ x, uint64_t off0, uint64_t off1,
-                const uint4* __restrict__ eq, uint64_t len, uint32_t* __restrict__ out,
-                ShiftFinish fin) {
-  pdl_wait();
-  pdl_trigger();
-  u256 a0 = {0, 0, 0, 0}, a1 = {0, 0, 0, 0};
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < len;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint4 e = eq[i];
-    xor_into(a0, clmul128(x[off0 + i], e));
-    xor_into(a1, clmul128(x[off1 + i], e));
-  }
-  uint4 v[2] = {reduce256(a0), reduce256(a1)};
-  block_xor_reduce<2>(v, out);
-  if (fin.ts && last_cta_of_grid(fin.ticket)) shift_round_finish(fin);
 }
 
 // The small last rounds of phase 2 in one CTA (see bivariate_tail_kernel).  Round n_rem folds
 // (W, M) from 2^(n_rem+1) to 2^n_rem elements by the previous challenge, evaluates the product
 // round, takes the in/out check's two dot products with eq_pub and lets warp 0 run
-// shift_round_finish's Fiat-Shamir step.  eq_pub holds eq(z[0 .. m)) with m = p - 1 while
+// shift_round_finish_kernel's Fiat-Shamir step.  eq_pub holds eq(z[0 .. m)) with m = p - 1 while
 // rounds are early (p < n_rem), then m = n_rem - 1: summing the two halves of eq(z[0 .. m))
 // gives eq(z[0 .. m - 1)), so later rounds shrink it in place.  On entry eq_pub is right for
 // the first round.
@@ -644,16 +627,11 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
   SHIFT_TRY(B.alloc(&tab, 16 * kMulTableEntries));
   SHIFT_TRY(B.alloc(&rconst, sizeof(ShiftRoundConst) * log_words));
   BGPU_CUDA(cudaMemsetAsync(slots, 0, 16 * n_slots, s));
-  // one CTA ticket per round whose evaluation kernel runs the round's Fiat-Shamir step itself
-  uint32_t* tickets;
-  SHIFT_TRY(B.alloc(&tickets, 4 * (12 + (uint64_t)log_words)));
-  BGPU_CUDA(cudaMemsetAsync(tickets, 0, 4 * (12 + (uint64_t)log_words), s));
   uint4* slots2 = slots + 24;
 
   // the provers' claims: sum_v <g_v, h_v> (phase_1.rs:96-101)
   BGPU_CUDA(cudaMemsetAsync(acc + 8, 0, 32, s));
-  dot2_kernel<<<grid_for(kFlat, 256, 148), 256, 0, s>>>(g, 0, 0, h, kFlat, acc + 8,
-                                                        ShiftFinish{});
+  dot2_kernel<<<grid_for(kFlat, 256, 148), 256, 0, s>>>(g, 0, 0, h, kFlat, acc + 8);
   SHIFT_TRY(launched("dot2_kernel"));
   DeviceTranscript dt;
   SHIFT_TRY(dt.begin(t, s));
@@ -663,19 +641,17 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
   for (int round = 0; round < tail0; round++) {
     const uint64_t size = (uint64_t)kFlat >> round;  // before this round's fold
     uint32_t* ys = reinterpret_cast<uint32_t*>(slots + 2 * round);
-    // the next round folds arrays of `size` elements; the round's evaluation kernel runs its
-    // Fiat-Shamir step in its last CTA
-    const bool next_tab = round < 11 && size >= kMulTableMinSize;
-    const BivFinish fin = bivariate_finish_args(
-        dt, round == 0 ? reinterpret_cast<const uint4*>(acc + 8) : nullptr, dstate, chal + round,
-        next_tab ? tab : nullptr, tickets + round);
     if (round == 0) {
-      SHIFT_TRY(bivariate_eval_finish(g, h, size / 2, ys, fin, s));
+      SHIFT_TRY(bivariate_eval(g, h, size / 2, ys, s));
     } else {
-      SHIFT_TRY(bivariate_fold_eval_finish(g, h, size * 2, chal + round - 1,
-                                           size * 2 >= kMulTableMinSize ? tab : nullptr, ys, fin,
-                                           s));
+      SHIFT_TRY(bivariate_fold_eval_dev(g, h, size * 2, chal + round - 1,
+                                        size * 2 >= kMulTableMinSize ? tab : nullptr, ys, s));
     }
+    // the next round folds arrays of `size` elements
+    const bool next_tab = round < 11 && size >= kMulTableMinSize;
+    SHIFT_TRY(bivariate_round_finish(dt, slots + 2 * round,
+                                     round == 0 ? reinterpret_cast<const uint4*>(acc + 8) : nullptr,
+                                     dstate, nullptr, chal + round, next_tab ? tab : nullptr, s));
   }
   SHIFT_TRY(bivariate_tail(dt, g, h, (uint64_t)kFlat >> (tail0 - 1), 12 - tail0, chal + tail0 - 1,
                            dstate, chal + tail0, s));
@@ -733,15 +709,13 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
   const hu128 beta = sample(t);
   // in the round loop dot2 follows a kernel and is launched programmatically (PDL relaxes only
   // kernel-to-kernel order); the first one follows a memset and is launched plainly
-  auto dot2 = [&](uint64_t off0, uint64_t off1, uint64_t len, uint4* out, bool pdl = true,
-                  const ShiftFinish& fin = ShiftFinish{}) -> int {
+  auto dot2 = [&](uint64_t off0, uint64_t off1, uint64_t len, uint4* out, bool pdl = true) -> int {
     const unsigned grid = grid_for(len, 256, 148 * 2);
     if (pdl)
       BGPU_CUDA(launch_pdl(dot2_kernel, grid, 256, 0, s, (const uint4*)W, off0, off1,
-                           (const uint4*)eq_pub, len, reinterpret_cast<uint32_t*>(out), fin));
+                           (const uint4*)eq_pub, len, reinterpret_cast<uint32_t*>(out)));
     else
-      dot2_kernel<<<grid, 256, 0, s>>>(W, off0, off1, eq_pub, len, reinterpret_cast<uint32_t*>(out),
-                                       fin);
+      dot2_kernel<<<grid, 256, 0, s>>>(W, off0, off1, eq_pub, len, reinterpret_cast<uint32_t*>(out));
     SHIFT_TRY(launched("dot2_kernel"));
     return BINIUS_OK;
   };
@@ -792,19 +766,19 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
                                         half * 4 >= kMulTableMinSize ? tab : nullptr,
                                         reinterpret_cast<uint32_t*>(ys), s));
     }
-    // the in/out dot products' kernel runs the round's Fiat-Shamir step in its last CTA
-    const bool next_tab = n_rem > 1 && half * 2 >= kMulTableMinSize;
-    const ShiftFinish fin = {dt.state(), dt.tape(), ys, rconst + k,
-                             n_rem == log_words ? (const uint4*)init_lohi : (const uint4*)nullptr,
-                             z0, u4(beta), run, chal + 12 + k, next_tab ? tab : (uint4*)nullptr,
-                             tickets + 12 + k};
     if (p < n_rem) {
-      SHIFT_TRY(dot2(half, half + (1ull << (gn - 1)), 1ull << (gn - 1), ys + 2, true, fin));
+      SHIFT_TRY(dot2(half, half + (1ull << (gn - 1)), 1ull << (gn - 1), ys + 2));
     } else {
       SHIFT_TRY(eq_tensor(to_u4(z).data(), n_rem - 1, eq_pub, s));
-      SHIFT_TRY(dot2(half, half, half, ys + 2, true, fin));
+      SHIFT_TRY(dot2(half, half, half, ys + 2));
     }
     if (n_rem <= p) gn--;
+    const bool next_tab = n_rem > 1 && half * 2 >= kMulTableMinSize;
+    BGPU_CUDA(launch_pdl(shift_round_finish_kernel, 1, 256, 0, s, dt.state(), dt.tape(),
+                         (const uint4*)ys, (const ShiftRoundConst*)(rconst + k),
+                         n_rem == log_words ? (const uint4*)init_lohi : (const uint4*)nullptr, z0,
+                         u4(beta), run, chal + 12 + k, next_tab ? tab : (uint4*)nullptr));
+    SHIFT_TRY(launched("shift_round_finish_kernel"));
   }
   if (tail_n) {
     const uint32_t k0 = log_words - tail_n;

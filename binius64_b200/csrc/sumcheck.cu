@@ -143,49 +143,10 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// The Fiat-Shamir step of a plain bivariate product round (BivariateProductSumcheckProver,
-// bivariate_product.rs:43-95, through the prover's round-proof truncation) on the device: the
-// sums (y_1, y_inf) and the claim give c_0 = claim + y_1, c_2 = y_inf, c_1 = y_1 + c_0 + c_2; the
-// message is (c_0, c_1), then optionally a 32-byte commitment (a Merkle root the device just
-// built), then the challenge r is sampled and the claim becomes c_0 + c_1 r + c_2 r^2.  The claim
-// is read from claim_init when that is set (the first round).  With a table pointer the block
-// then builds r's byte table for the next fold.  Every thread of the block calls it; the sums are
-// read through L2 (the round's other CTAs added them atomically).
-__device__ __noinline__ void bivariate_round_finish_dev(const BivFinish& f,
-                                                        const uint4* __restrict__ ys,
-                                                        const uint8_t* __restrict__ commitment) {
-  __shared__ uint4 r_sh;
-  if (threadIdx.x < 32) {
-    TranscriptState* ts = static_cast<TranscriptState*>(f.ts);
-    DevTr st;
-    st.load(ts);
-    const uint4 y1 = __ldcg(ys), yinf = __ldcg(ys + 1);
-    const uint4 c0 = gf_add(f.claim_init ? *f.claim_init : *f.claim, y1), c2 = yinf;
-    const uint4 c1 = gf_add(gf_add(y1, c0), c2);
-    const uint4 msg[2] = {c0, c1};
-    st.message_elems(f.tape, msg, 2);
-    if (commitment) {
-      uint32_t root[8];
-      for (int i = 0; i < 8; i++) root[i] = reinterpret_cast<const uint32_t*>(commitment)[i];
-      st.message_words(f.tape, root, 8);
-    }
-    const uint4 r = st.sample_elem();
-    *f.r_out = r;
-    *f.claim = gf_add(c0, gf_mul_warp(r, gf_add(c1, gf_mul_warp(c2, r))));
-    st.store(ts);
-    r_sh = r;
-  }
-  if (f.tab) {
-    __syncthreads();
-    dt_build_mul_table(r_sh, f.tab);
-  }
-}
-
-// Round evaluation on (a, b) of length 2*half, no fold; with fin.ts set, the last CTA then runs
-// the round's Fiat-Shamir step.
+// Round evaluation on (a, b) of length 2*half, no fold.
 __global__ void __launch_bounds__(kThreads)
     bivariate_eval_kernel(const uint4* __restrict__ a, const uint4* __restrict__ b, uint64_t half,
-                          uint32_t* __restrict__ out, BivFinish fin) {
+                          uint32_t* __restrict__ out) {
   u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < half;
        i += (uint64_t)gridDim.x * blockDim.x) {
@@ -195,8 +156,6 @@ __global__ void __launch_bounds__(kThreads)
   }
   uint4 v[2] = {reduce256(s1), reduce256(sinf)};
   block_xor_reduce<2>(v, out);
-  if (fin.ts && last_cta_of_grid(fin.ticket))
-    bivariate_round_finish_dev(fin, reinterpret_cast<const uint4*>(out), nullptr);
 }
 
 // Folds (a, b) of length `size` by r in place (a[i] = a[i] + r (a[i + size/2] - a[i])) and
@@ -205,11 +164,10 @@ __global__ void __launch_bounds__(kThreads)
 // through the byte table of r (gf_mul_table); otherwise r is r_arg, or *r_ptr when that is set
 // (a challenge the device transcript sampled).
 template <bool TAB>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads)
     bivariate_fold_eval_kernel(uint4* __restrict__ a, uint4* __restrict__ b, uint64_t size,
                                uint4 r_arg, const uint4* __restrict__ r_ptr,
-                               const uint4* __restrict__ tab, uint32_t* __restrict__ out,
-                               BivFinish fin) {
+                               const uint4* __restrict__ tab, uint32_t* __restrict__ out) {
   pdl_wait();
   pdl_trigger();
   const uint64_t h = size >> 1, q = size >> 2;
@@ -240,25 +198,51 @@ __global__ void __launch_bounds__(kThreads, 2)
   }
   uint4 v[2] = {TAB ? reduce256(s1) : s1r, TAB ? reduce256(sinf) : sinfr};
   block_xor_reduce<2>(v, out);
-  // the last CTA runs the round's Fiat-Shamir step; the table it rebuilds was read by CTAs that
-  // have all finished
-  if (fin.ts && last_cta_of_grid(fin.ticket))
-    bivariate_round_finish_dev(fin, reinterpret_cast<const uint4*>(out), nullptr);
 }
 
-// bivariate_round_finish_dev as its own launch, for rounds with a commitment between the sums and
-// the message (a FRI commit round of BaseFold).
+// The Fiat-Shamir step of a plain bivariate product round (BivariateProductSumcheckProver,
+// bivariate_product.rs:43-95, through the prover's round-proof truncation) on the device: the
+// sums (y_1, y_inf) and the claim give c_0 = claim + y_1, c_2 = y_inf, c_1 = y_1 + c_0 + c_2; the
+// message is (c_0, c_1), then optionally a 32-byte commitment (a Merkle root the device just
+// built), then the challenge r is sampled and the claim becomes c_0 + c_1 r + c_2 r^2.  The claim
+// is read from claim_init when that is set (the first round).  With a table pointer the block
+// then builds r's byte table for the next fold.
 __global__ void __launch_bounds__(256)
-    bivariate_round_finish_kernel(BivFinish f, const uint4* __restrict__ ys,
-                                  const uint8_t* __restrict__ commitment) {
+    bivariate_round_finish_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
+                                  const uint4* __restrict__ ys, const uint4* __restrict__ claim_init,
+                                  uint4* __restrict__ claim, const uint8_t* __restrict__ commitment,
+                                  uint4* __restrict__ r_out, uint4* __restrict__ tab) {
   pdl_wait();
   pdl_trigger();
-  bivariate_round_finish_dev(f, ys, commitment);
+  __shared__ uint4 r_sh;
+  if (threadIdx.x < 32) {
+    DevTr st;
+    st.load(ts);
+    const uint4 y1 = ys[0], yinf = ys[1];
+    const uint4 c0 = gf_add(claim_init ? *claim_init : *claim, y1), c2 = yinf;
+    const uint4 c1 = gf_add(gf_add(y1, c0), c2);
+    const uint4 msg[2] = {c0, c1};
+    st.message_elems(tape, msg, 2);
+    if (commitment) {
+      uint32_t root[8];
+      for (int i = 0; i < 8; i++) root[i] = reinterpret_cast<const uint32_t*>(commitment)[i];
+      st.message_words(tape, root, 8);
+    }
+    const uint4 r = st.sample_elem();
+    *r_out = r;
+    *claim = gf_add(c0, gf_mul_warp(r, gf_add(c1, gf_mul_warp(c2, r))));
+    st.store(ts);
+    r_sh = r;
+  }
+  if (tab) {
+    __syncthreads();
+    dt_build_mul_table(r_sh, tab);
+  }
 }
 
 // The small last rounds of a plain bivariate product sumcheck in one CTA: per round, fold (a, b)
 // by the previous challenge (r_first for the first round when set), evaluate (y_1, y_inf) on the
-// folded arrays, and let warp 0 run the Fiat-Shamir step of bivariate_round_finish_dev with
+// folded arrays, and let warp 0 run the Fiat-Shamir step of bivariate_round_finish_kernel with
 // the transcript held in its registers.  The rounds of a sumcheck below a few thousand elements
 // are latency chains; run as one launch, the loop body stays in the instruction cache and no
 // launch gap separates the rounds.  len is the arrays' length before the first fold.
@@ -406,23 +390,7 @@ int fold_b128_elems(const uint4* d_in, uint4* d_out, uint64_t n, const uint4* d_
 int bivariate_eval(const uint4* d_a, const uint4* d_b, uint64_t half, uint32_t* d_out8,
                    cudaStream_t s) {
   BGPU_CUDA(cudaMemsetAsync(d_out8, 0, 32, s));
-  bivariate_eval_kernel<<<grid_for(half, kThreads), kThreads, 0, s>>>(d_a, d_b, half, d_out8,
-                                                                      BivFinish{});
-  BGPU_LAUNCH_CHECK("bivariate_eval_kernel");
-  count_launch();
-  return BINIUS_OK;
-}
-
-BivFinish bivariate_finish_args(const DeviceTranscript& dt, const uint4* d_claim_init,
-                                uint4* d_claim, uint4* d_r_out, uint4* d_tab, uint32_t* d_ticket) {
-  return BivFinish{dt.state(), dt.tape(), d_claim_init, d_claim, d_r_out, d_tab, d_ticket};
-}
-
-int bivariate_eval_finish(const uint4* d_a, const uint4* d_b, uint64_t half, uint32_t* d_out8,
-                          const BivFinish& fin, cudaStream_t s) {
-  BGPU_CUDA(cudaMemsetAsync(d_out8, 0, 32, s));
-  bivariate_eval_kernel<<<grid_for(half, kThreads), kThreads, 0, s>>>(d_a, d_b, half, d_out8,
-                                                                      fin);
+  bivariate_eval_kernel<<<grid_for(half, kThreads), kThreads, 0, s>>>(d_a, d_b, half, d_out8);
   BGPU_LAUNCH_CHECK("bivariate_eval_kernel");
   count_launch();
   return BINIUS_OK;
@@ -451,7 +419,7 @@ int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[1
     int rc = build_mul_table(r, tab, s);
     if (!rc) {
       bivariate_fold_eval_kernel<true><<<grid, kThreads, 0, s>>>(d_a, d_b, size, rv, nullptr, tab,
-                                                                 d_out8, BivFinish{});
+                                                                 d_out8);
       cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) rc = cuda_error(e, "bivariate_fold_eval_kernel");
       else count_launch();
@@ -460,41 +428,35 @@ int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[1
     return rc;
   }
   bivariate_fold_eval_kernel<false><<<grid, kThreads, 0, s>>>(d_a, d_b, size, rv, nullptr, nullptr,
-                                                              d_out8, BivFinish{});
+                                                              d_out8);
   BGPU_LAUNCH_CHECK("bivariate_fold_eval_kernel");
-  count_launch();
-  return BINIUS_OK;
-}
-
-int bivariate_fold_eval_finish(uint4* d_a, uint4* d_b, uint64_t size, const uint4* d_r,
-                               const uint4* d_tab, uint32_t* d_out8, const BivFinish& fin,
-                               cudaStream_t s) {
-  if (size < 4) return set_error(BINIUS_E_ARG, "bivariate_fold_eval needs size >= 4");
-  const unsigned grid = grid_for(size / 4, kThreads);
-  cudaError_t e;
-  if (size >= kMulTableMinSize) {
-    if (!d_tab) return set_error(BINIUS_E_ARG, "a large fold needs the challenge's table");
-    e = launch_pdl(bivariate_fold_eval_kernel<true>, grid, kThreads, 0, s, d_a, d_b, size,
-                   gf_zero_host(), (const uint4*)nullptr, d_tab, d_out8, fin);
-  } else {
-    e = launch_pdl(bivariate_fold_eval_kernel<false>, grid, kThreads, 0, s, d_a, d_b, size,
-                   gf_zero_host(), d_r, (const uint4*)nullptr, d_out8, fin);
-  }
-  if (e != cudaSuccess) return cuda_error(e, "bivariate_fold_eval_kernel");
   count_launch();
   return BINIUS_OK;
 }
 
 int bivariate_fold_eval_dev(uint4* d_a, uint4* d_b, uint64_t size, const uint4* d_r,
                             const uint4* d_tab, uint32_t* d_out8, cudaStream_t s) {
-  return bivariate_fold_eval_finish(d_a, d_b, size, d_r, d_tab, d_out8, BivFinish{}, s);
+  if (size < 4) return set_error(BINIUS_E_ARG, "bivariate_fold_eval needs size >= 4");
+  const unsigned grid = grid_for(size / 4, kThreads);
+  cudaError_t e;
+  if (size >= kMulTableMinSize) {
+    if (!d_tab) return set_error(BINIUS_E_ARG, "a large fold needs the challenge's table");
+    e = launch_pdl(bivariate_fold_eval_kernel<true>, grid, kThreads, 0, s, d_a, d_b, size,
+                   gf_zero_host(), (const uint4*)nullptr, d_tab, d_out8);
+  } else {
+    e = launch_pdl(bivariate_fold_eval_kernel<false>, grid, kThreads, 0, s, d_a, d_b, size,
+                   gf_zero_host(), d_r, (const uint4*)nullptr, d_out8);
+  }
+  if (e != cudaSuccess) return cuda_error(e, "bivariate_fold_eval_kernel");
+  count_launch();
+  return BINIUS_OK;
 }
 
 int bivariate_round_finish(const DeviceTranscript& dt, const uint4* d_ys, const uint4* d_claim_init,
                            uint4* d_claim, const uint8_t* d_commitment, uint4* d_r_out,
                            uint4* d_tab, cudaStream_t s) {
-  const BivFinish f{dt.state(), dt.tape(), d_claim_init, d_claim, d_r_out, d_tab, nullptr};
-  cudaError_t e = launch_pdl(bivariate_round_finish_kernel, 1, 256, 0, s, f, d_ys, d_commitment);
+  cudaError_t e = launch_pdl(bivariate_round_finish_kernel, 1, 256, 0, s, dt.state(), dt.tape(),
+                             d_ys, d_claim_init, d_claim, d_commitment, d_r_out, d_tab);
   if (e != cudaSuccess) return cuda_error(e, "bivariate_round_finish_kernel");
   count_launch();
   return BINIUS_OK;
