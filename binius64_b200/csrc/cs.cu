@@ -232,7 +232,75 @@ __global__ void __launch_bounds__(1024) exclusive_scan_keys_kernel(uint32_t* cou
   }
 }
 
-int build_shift_terms(const DevOperands& A, const DevOperands& M, ShiftTerms& d) {
+__global__ void word_count_kernel(const uint32_t* __restrict__ vi, uint64_t n,
+                                  uint32_t* __restrict__ counts) {
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n;
+       t += (uint64_t)gridDim.x * blockDim.x)
+    atomicAdd(&counts[vi[t]], 1u);
+}
+
+// cursor[w] starts at word w's first slot; each term takes the next one (the order of a word's
+// terms is immaterial: the monster sums them in GF(2^128)).
+__global__ void word_scatter_kernel(const uint32_t* __restrict__ vi, const uint32_t* __restrict__ c,
+                                    const uint16_t* __restrict__ key, uint64_t n,
+                                    uint32_t* __restrict__ cursor, uint32_t* __restrict__ w_c,
+                                    uint16_t* __restrict__ w_key) {
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t pos = atomicAdd(&cursor[vi[t]], 1u);
+    w_c[pos] = c[t];
+    w_key[pos] = key[t];
+  }
+}
+
+// Groups the key-sorted terms by word (a counting sort: per-word counts on the device, their
+// exclusive scan on the host, a scatter), for the monster multilinear's per-word sums.
+int build_word_order(ShiftTerms& t, uint32_t n_words) {
+  const size_t m = t.n ? t.n : 1;
+  uint32_t* cursor = nullptr;
+  cudaStream_t s = nullptr;
+  cudaError_t e;
+  std::vector<uint32_t> h((size_t)n_words + 1, 0);
+  const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((t.n + 255) / 256, 148 * 16));
+  do {
+    if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) != cudaSuccess) break;
+    if ((e = cudaMalloc(&t.w_off, 4 * ((size_t)n_words + 1))) != cudaSuccess) break;
+    if ((e = cudaMalloc(&t.w_c, 4 * m)) != cudaSuccess) break;
+    if ((e = cudaMalloc(&t.w_key, 2 * m)) != cudaSuccess) break;
+    if ((e = cudaMalloc(&cursor, 4 * ((size_t)n_words + 1))) != cudaSuccess) break;
+    if ((e = cudaMemsetAsync(cursor, 0, 4 * (size_t)n_words, s)) != cudaSuccess) break;
+    if (t.n) word_count_kernel<<<blocks, 256, 0, s>>>(t.vi, t.n, cursor);
+    if ((e = cudaGetLastError()) != cudaSuccess) break;
+    if ((e = cudaMemcpyAsync(h.data(), cursor, 4 * (size_t)n_words, cudaMemcpyDeviceToHost, s)) !=
+        cudaSuccess)
+      break;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) break;
+    uint32_t run = 0;
+    for (uint32_t w = 0; w <= n_words; w++) {
+      const uint32_t c = w < n_words ? h[w] : 0;
+      h[w] = run;
+      run += c;
+    }
+    if ((e = cudaMemcpyAsync(t.w_off, h.data(), 4 * h.size(), cudaMemcpyHostToDevice, s)) !=
+        cudaSuccess)
+      break;
+    if ((e = cudaMemcpyAsync(cursor, t.w_off, 4 * (size_t)n_words, cudaMemcpyDeviceToDevice, s)) !=
+        cudaSuccess)
+      break;
+    if (t.n) word_scatter_kernel<<<blocks, 256, 0, s>>>(t.vi, t.c, t.key, t.n, cursor, t.w_c, t.w_key);
+    if ((e = cudaGetLastError()) != cudaSuccess) break;
+    e = cudaStreamSynchronize(s);
+  } while (0);
+  if (s) cudaStreamDestroy(s);
+  cudaFree(cursor);
+  if (e != cudaSuccess) return cuda_error(e, "shift term word order");
+  t.n_words = n_words;
+  count_launch(t.n ? 2 : 0);
+  return BINIUS_OK;
+}
+
+int build_shift_terms(const DevOperands& A, const DevOperands& M, uint32_t n_words,
+                      ShiftTerms& d) {
   const uint64_t n = A.n_terms + M.n_terms;
   BGPU_ARG(n < 0xffffffffull, "too many operand terms");
   const size_t m = n ? n : 1;
@@ -267,6 +335,10 @@ int build_shift_terms(const DevOperands& A, const DevOperands& M, ShiftTerms& d)
     return cuda_error(e, "shift term sort");
   }
   count_launch(3);
+  if (int rc = build_word_order(t, n_words)) {
+    free_shift_terms(t);
+    return rc;
+  }
   d = t;
   return BINIUS_OK;
 }
@@ -275,8 +347,19 @@ int build_shift_terms(const DevOperands& A, const DevOperands& M, ShiftTerms& d)
 
 namespace bgpu {
 
+void free_shift_terms(ShiftTerms& t) {
+  cudaFree(t.vi);
+  cudaFree(t.c);
+  cudaFree(t.key);
+  cudaFree(t.w_off);
+  cudaFree(t.w_c);
+  cudaFree(t.w_key);
+  t = ShiftTerms();
+}
+
 int upload_shift_terms(const std::vector<uint32_t>& vi, const std::vector<uint32_t>& c,
-                       const std::vector<uint16_t>& key, uint64_t n, ShiftTerms& out) {
+                       const std::vector<uint16_t>& key, uint64_t n, uint32_t n_words,
+                       ShiftTerms& out) {
   const size_t m = n ? n : 1;
   ShiftTerms d;
   d.n = n;
@@ -292,8 +375,11 @@ int upload_shift_terms(const std::vector<uint32_t>& vi, const std::vector<uint32
     return cuda_error(e, "shift term table");
   }
   cudaFree(out.vi);
-  cudaFree(out.c);
-  cudaFree(out.key);
+  if (int rc = build_word_order(d, n_words)) {
+    free_shift_terms(d);
+    return rc;
+  }
+  free_shift_terms(out);
   out = d;
   return BINIUS_OK;
 }
@@ -357,7 +443,8 @@ int binius_cs_from_bytes(int device, const void* h_bytes, size_t len, binius_cs*
     cudaSetDevice(device);
     rc = upload(cs->h_and, cs->and_ops);
     if (!rc) rc = upload(cs->h_mul, cs->mul_ops);
-    if (!rc) rc = build_shift_terms(cs->and_ops, cs->mul_ops, cs->shift_terms);
+    if (!rc)
+      rc = build_shift_terms(cs->and_ops, cs->mul_ops, cs->committed_total_len, cs->shift_terms);
     cudaSetDevice(prev);
   }
   if (rc) {
@@ -374,9 +461,7 @@ int binius_cs_destroy(binius_cs* cs) {
   cudaFree(cs->and_ops.terms);
   cudaFree(cs->mul_ops.offsets);
   cudaFree(cs->mul_ops.terms);
-  cudaFree(cs->shift_terms.vi);
-  cudaFree(cs->shift_terms.c);
-  cudaFree(cs->shift_terms.key);
+  free_shift_terms(cs->shift_terms);
   delete cs;
   return BINIUS_OK;
 }

@@ -33,7 +33,14 @@ struct ShiftTerms {
   uint32_t* vi = nullptr;   // value index
   uint32_t* c = nullptr;    // constraint index within its operation
   uint16_t* key = nullptr;
+  // the same terms grouped by word: word w's terms are [w_off[w], w_off[w + 1]) of w_c / w_key
+  uint32_t n_words = 0;
+  uint32_t* w_off = nullptr;
+  uint32_t* w_c = nullptr;
+  uint16_t* w_key = nullptr;
 };
+// Frees the device arrays of a term table.
+void free_shift_terms(ShiftTerms& t);
 constexpr uint32_t kShiftKeys = 512 * 8;
 constexpr uint32_t kShiftClasses = 7;
 
@@ -47,7 +54,8 @@ int parse_cs(const void* h_bytes, size_t len, binius_cs& cs);
 // Uploads a term table (vi, c, key each of n entries, sorted by key) to the current device and
 // replaces `out`'s, freeing the old one; on failure `out` is unchanged.
 int upload_shift_terms(const std::vector<uint32_t>& vi, const std::vector<uint32_t>& c,
-                       const std::vector<uint16_t>& key, uint64_t n, ShiftTerms& out);
+                       const std::vector<uint16_t>& key, uint64_t n, uint32_t n_words,
+                       ShiftTerms& out);
 
 // d_out[slot * n_constraints + i] = eval_operand of constraint i's operand `slot`.
 int eval_operands(const DevOperands& ops, const uint64_t* d_witness, uint64_t* d_out,

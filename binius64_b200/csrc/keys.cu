@@ -312,7 +312,8 @@ int load_key_collection(binius_cs& cs, const uint8_t* kc, size_t len) {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(cs.device);
-  const int rc = upload_shift_terms(svi, scc, skey, n_cis, cs.shift_terms);
+  const int rc = upload_shift_terms(svi, scc, skey, n_cis, cs.committed_total_len,
+                                  cs.shift_terms);
   cudaSetDevice(prev);
   return rc;
 }

@@ -289,17 +289,24 @@ __global__ void shift_scalars_kernel(ClassPowers pw, Lag64 eq_rs, const uint4* _
   T[key] = gf_mul(gf_mul(pw.p[cls], hop), eq_rs.l[s]);
 }
 
-// M[vi] += T[key] * eq[c] for every term.
+// M[w] = sum over word w's terms of T[key] * eq[c] (build_monster_multilinear, monster.rs:138-219):
+// one thread per word over the word-ordered term table, the products accumulated unreduced and
+// reduced once, every M[w] written once (no atomics, no clearing).
 __global__ void __launch_bounds__(256)
-    shift_monster_kernel(const uint32_t* __restrict__ vi, const uint32_t* __restrict__ cidx,
-                         const uint16_t* __restrict__ keys, uint64_t n,
+    shift_monster_kernel(const uint32_t* __restrict__ off, const uint32_t* __restrict__ cidx,
+                         const uint16_t* __restrict__ keys, uint32_t n_words,
                          const uint4* __restrict__ eq_and, const uint4* __restrict__ eq_mul,
-                         const uint4* __restrict__ T, uint32_t* __restrict__ M) {
-  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n;
-       t += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t k = keys[t];
-    const uint4 e = __ldg(eq_of_class(k, eq_and, eq_mul) + cidx[t]);
-    atomic_xor_gf(M + 4 * (uint64_t)vi[t], gf_mul(__ldg(T + k), e));
+                         const uint4* __restrict__ T, uint4* __restrict__ M) {
+  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < n_words;
+       w += (uint64_t)gridDim.x * blockDim.x) {
+    u256 acc = {0, 0, 0, 0};
+    const uint32_t t1 = off[w + 1];
+    for (uint32_t t = off[w]; t < t1; t++) {
+      const uint32_t k = keys[t];
+      const uint4 e = __ldg(eq_of_class(k, eq_and, eq_mul) + cidx[t]);
+      xor_into(acc, clmul128(__ldg(T + k), e));
+    }
+    M[w] = reduce256(acc);
   }
 }
 
@@ -694,12 +701,10 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
   for (int i = 0; i < 64; i++) ers.l[i] = u4(eq_rs[i]);
   shift_scalars_kernel<<<kShiftKeys / 256, 256, 0, s>>>(pw, ers, h_ops, same_z ? 0 : 8, T);
   SHIFT_TRY(launched("shift_scalars_kernel"));
-  BGPU_CUDA(cudaMemsetAsync(M, 0, 16ull * n_words, s));
-  if (terms.n) {
-    shift_monster_kernel<<<grid_for(terms.n, 256, 148 * 16), 256, 0, s>>>(
-        terms.vi, terms.c, terms.key, terms.n, eq_and, eq_mul, T, reinterpret_cast<uint32_t*>(M));
-    SHIFT_TRY(launched("shift_monster_kernel"));
-  }
+  if (terms.n_words != n_words) return set_error(BINIUS_E_ARG, "shift term table of another size");
+  shift_monster_kernel<<<grid_for(n_words, 256, 148 * 16), 256, 0, s>>>(
+      terms.w_off, terms.w_c, terms.w_key, n_words, eq_and, eq_mul, T, M);
+  SHIFT_TRY(launched("shift_monster_kernel"));
 
   // in/out check point (InOutCheckProver::new) and the batching coefficient; the public
   // evaluation is taken on the device by the first round's finish kernel
