@@ -374,7 +374,6 @@ int upload_shift_terms(const std::vector<uint32_t>& vi, const std::vector<uint32
     cudaFree(d.key);
     return cuda_error(e, "shift term table");
   }
-  cudaFree(out.vi);
   if (int rc = build_word_order(d, n_words)) {
     free_shift_terms(d);
     return rc;
