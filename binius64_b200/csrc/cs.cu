@@ -254,13 +254,14 @@ __global__ void word_scatter_kernel(const uint32_t* __restrict__ vi, const uint3
 }
 
 // Groups the key-sorted terms by word (a counting sort: per-word counts on the device, their
-// exclusive scan on the host, a scatter), for the monster multilinear's per-word sums.
+// exclusive scan on the host, a scatter), for the monster multilinear's per-word sums, and
+// records the word each kMonsterChunk-term chunk of that order starts in.
 int build_word_order(ShiftTerms& t, uint32_t n_words) {
   const size_t m = t.n ? t.n : 1;
   uint32_t* cursor = nullptr;
   cudaStream_t s = nullptr;
   cudaError_t e;
-  std::vector<uint32_t> h((size_t)n_words + 1, 0);
+  std::vector<uint32_t> h((size_t)n_words + 1, 0), chunk_word;
   const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((t.n + 255) / 256, 148 * 16));
   do {
     if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) != cudaSuccess) break;
@@ -281,6 +282,16 @@ int build_word_order(ShiftTerms& t, uint32_t n_words) {
       h[w] = run;
       run += c;
     }
+    const uint64_t n_chunks = (t.n + kMonsterChunk - 1) / kMonsterChunk;
+    chunk_word.assign(n_chunks ? n_chunks : 1, 0);
+    for (uint32_t w = 0; w < n_words; w++)  // chunks that start inside word w's terms
+      for (uint64_t j = ((uint64_t)h[w] + kMonsterChunk - 1) / kMonsterChunk;
+           j * kMonsterChunk < h[w + 1]; j++)
+        chunk_word[j] = w;
+    if ((e = cudaMalloc(&t.w_chunk, 4 * chunk_word.size())) != cudaSuccess) break;
+    if ((e = cudaMemcpyAsync(t.w_chunk, chunk_word.data(), 4 * chunk_word.size(),
+                             cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      break;
     if ((e = cudaMemcpyAsync(t.w_off, h.data(), 4 * h.size(), cudaMemcpyHostToDevice, s)) !=
         cudaSuccess)
       break;
@@ -354,6 +365,7 @@ void free_shift_terms(ShiftTerms& t) {
   cudaFree(t.w_off);
   cudaFree(t.w_c);
   cudaFree(t.w_key);
+  cudaFree(t.w_chunk);
   t = ShiftTerms();
 }
 

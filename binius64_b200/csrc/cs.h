@@ -33,14 +33,18 @@ struct ShiftTerms {
   uint32_t* vi = nullptr;   // value index
   uint32_t* c = nullptr;    // constraint index within its operation
   uint16_t* key = nullptr;
-  // the same terms grouped by word: word w's terms are [w_off[w], w_off[w + 1]) of w_c / w_key
+  // the same terms grouped by word: word w's terms are [w_off[w], w_off[w + 1]) of w_c / w_key;
+  // w_chunk[j] is the word that holds term j * kMonsterChunk of that order
   uint32_t n_words = 0;
   uint32_t* w_off = nullptr;
   uint32_t* w_c = nullptr;
   uint16_t* w_key = nullptr;
+  uint32_t* w_chunk = nullptr;
 };
 // Frees the device arrays of a term table.
 void free_shift_terms(ShiftTerms& t);
+// Terms one thread of the monster multilinear takes, consecutive in word order.
+constexpr uint32_t kMonsterChunk = 8;
 constexpr uint32_t kShiftKeys = 512 * 8;
 constexpr uint32_t kShiftClasses = 7;
 

@@ -289,24 +289,47 @@ __global__ void shift_scalars_kernel(ClassPowers pw, Lag64 eq_rs, const uint4* _
   T[key] = gf_mul(gf_mul(pw.p[cls], hop), eq_rs.l[s]);
 }
 
-// M[w] = sum over word w's terms of T[key] * eq[c] (build_monster_multilinear, monster.rs:138-219):
-// one thread per word over the word-ordered term table, the products accumulated unreduced and
-// reduced once, every M[w] written once (no atomics, no clearing).
+// M[w] = sum over word w's terms of T[key] * eq[c] (build_monster_multilinear, monster.rs:138-219).
+// Each thread takes kMonsterChunk consecutive terms of the word-ordered table, so every thread does
+// the same number of multiplies whatever the words' term counts.  Products are accumulated
+// unreduced while the word stays the same and reduced once per (thread, word); a word whose terms
+// all lie in the thread's chunk is stored, one split across chunks is XORed in atomically (M is
+// cleared first, which also covers words with no terms).
 __global__ void __launch_bounds__(256)
-    shift_monster_kernel(const uint32_t* __restrict__ off, const uint32_t* __restrict__ cidx,
-                         const uint16_t* __restrict__ keys, uint32_t n_words,
-                         const uint4* __restrict__ eq_and, const uint4* __restrict__ eq_mul,
-                         const uint4* __restrict__ T, uint4* __restrict__ M) {
-  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < n_words;
-       w += (uint64_t)gridDim.x * blockDim.x) {
+    shift_monster_kernel(const uint32_t* __restrict__ off, const uint32_t* __restrict__ chunk_word,
+                         const uint32_t* __restrict__ cidx, const uint16_t* __restrict__ keys,
+                         uint64_t n, const uint4* __restrict__ eq_and,
+                         const uint4* __restrict__ eq_mul, const uint4* __restrict__ T,
+                         uint4* __restrict__ M) {
+  const uint64_t n_chunks = (n + kMonsterChunk - 1) / kMonsterChunk;
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n_chunks;
+       j += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t t0 = j * kMonsterChunk, t1 = min(t0 + kMonsterChunk, n);
+    uint32_t w = chunk_word[j];
+    uint64_t lo = off[w], hi = off[w + 1];  // word w's terms
     u256 acc = {0, 0, 0, 0};
-    const uint32_t t1 = off[w + 1];
-    for (uint32_t t = off[w]; t < t1; t++) {
+    auto flush = [&]() {
+      const uint4 v = reduce256(acc);
+      if (lo >= t0 && hi <= t1)
+        M[w] = v;
+      else
+        atomic_xor_gf(reinterpret_cast<uint32_t*>(M + w), v);
+    };
+    for (uint64_t t = t0; t < t1; t++) {
+      if (t == hi) {  // word w ends here; the next word with terms starts at t (t < n)
+        flush();
+        acc = {0, 0, 0, 0};
+        do {
+          w++;
+          lo = hi;
+          hi = off[w + 1];
+        } while (hi == lo);
+      }
       const uint32_t k = keys[t];
       const uint4 e = __ldg(eq_of_class(k, eq_and, eq_mul) + cidx[t]);
       xor_into(acc, clmul128(__ldg(T + k), e));
     }
-    M[w] = reduce256(acc);
+    flush();
   }
 }
 
@@ -702,9 +725,13 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
   shift_scalars_kernel<<<kShiftKeys / 256, 256, 0, s>>>(pw, ers, h_ops, same_z ? 0 : 8, T);
   SHIFT_TRY(launched("shift_scalars_kernel"));
   if (terms.n_words != n_words) return set_error(BINIUS_E_ARG, "shift term table of another size");
-  shift_monster_kernel<<<grid_for(n_words, 256, 148 * 16), 256, 0, s>>>(
-      terms.w_off, terms.w_c, terms.w_key, n_words, eq_and, eq_mul, T, M);
-  SHIFT_TRY(launched("shift_monster_kernel"));
+  BGPU_CUDA(cudaMemsetAsync(M, 0, 16ull * n_words, s));
+  if (terms.n) {
+    const uint64_t n_chunks = (terms.n + kMonsterChunk - 1) / kMonsterChunk;
+    shift_monster_kernel<<<grid_for(n_chunks, 256, 148 * 32), 256, 0, s>>>(
+        terms.w_off, terms.w_chunk, terms.w_c, terms.w_key, terms.n, eq_and, eq_mul, T, M);
+    SHIFT_TRY(launched("shift_monster_kernel"));
+  }
 
   // in/out check point (InOutCheckProver::new) and the batching coefficient; the public
   // evaluation is taken on the device by the first round's finish kernel
