@@ -470,7 +470,7 @@ __global__ void __launch_bounds__(kAndTailThreads)
   pdl_wait();
   pdl_trigger();
   __shared__ uint4 r_sh;
-  DevTr st;
+  DevTrLoop st;
   uint4 cl = gf_zero();
   if (threadIdx.x < 32) {
     st.load(ts);

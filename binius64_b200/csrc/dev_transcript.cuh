@@ -21,19 +21,21 @@
 
 namespace bgpu {
 
-// Code run once by a single thread is fetched cold: straight-line code costs an instruction-cache
-// miss every few instructions, which for fully unrolled SHA-256 rounds and inlined GF(2^128)
-// multiplies comes to tens of microseconds per launch.  The scalar protocol steps therefore call
-// one out-of-line copy of each: the multiply (gf_mul_nl) and the compression
-// (sha256_compress_compact).
+// The scalar protocol steps run on one warp, where every dependent instruction waits out its full
+// latency.  Measured on a B200, one warp: the multiply below 0.38 us (the 16 partial products
+// combined by shuffle butterflies instead: 0.45 us; nine clmul32 on one thread: 0.63 us); a
+// SHA-256 compression fully unrolled on registers 1.5 us, a compact loop 2.2 us.  A Fiat-Shamir
+// step of its own launch (two compressions, two multiplies) costs 7.3 us with the unrolled
+// compression against 8.5 us with the compact one, so the one-shot finish launches use the
+// unrolled form (DevTr); the tail loops, whose warp 0 alternates between a step and the round's
+// folds, ran slower with it and keep the compact loop (DevTrLoop).
 __device__ __forceinline__ uint4 gf_mul_1t(uint4 a, uint4 b) { return gf_mul_nl(a, b); }
 
 // A product on the critical path of a Fiat-Shamir step, computed by a whole warp: every lane
 // passes the same a and b; lane l < 16 forms the 32x32 carry-less product of word l/4 of a and
-// word l%4 of b, the 16 products are XOR-combined into the eight words of the 256-bit product by
-// shuffle reductions, and every lane returns the reduced product.  One multiply's latency is
-// then one clmul32 plus the shuffles instead of nine dependent clmul32 on one thread; one
-// out-of-line copy keeps the launch's cold instruction fetch small.
+// word l%4 of b, each of the eight words of the 256-bit product is the XOR of the partial-product
+// halves that land on it (one warp reduction, REDUX, per word), and every lane returns the
+// reduced product.  One out-of-line copy keeps the code of the launches that call it small.
 static __device__ __noinline__ uint4 gf_mul_warp(uint4 a, uint4 b) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t i = (lane >> 2) & 3, j = lane & 3;
@@ -43,12 +45,8 @@ static __device__ __noinline__ uint4 gf_mul_warp(uint4 a, uint4 b) {
   const uint32_t lo = (uint32_t)p, hi = (uint32_t)(p >> 32), k = i + j;
   uint32_t w[8];
 #pragma unroll
-  for (uint32_t q = 0; q < 8; q++) {
-    uint32_t v = (k == q ? lo : 0u) ^ (k + 1 == q ? hi : 0u);
-#pragma unroll
-    for (int m = 16; m >= 1; m >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, m);
-    w[q] = v;
-  }
+  for (uint32_t q = 0; q < 8; q++)
+    w[q] = __reduce_xor_sync(0xffffffffu, (k == q ? lo : 0u) ^ (k + 1 == q ? hi : 0u));
   u256 r;
   r.p0 = ((uint64_t)w[1] << 32) | w[0];
   r.p1 = ((uint64_t)w[3] << 32) | w[2];
@@ -56,24 +54,46 @@ static __device__ __noinline__ uint4 gf_mul_warp(uint4 a, uint4 b) {
   r.p3 = ((uint64_t)w[7] << 32) | w[6];
   return reduce256(r);
 }
-__device__ __forceinline__ void sha256_compress_1t(uint32_t* st, const uint32_t* blk) {
-  sha256_compress_compact(st, blk);
+
+// One compression of blk into st, both held in local memory by the caller: copied to registers,
+// compressed by the fully unrolled sha256_compress (round constants as immediates) and written
+// back.  One out-of-line copy serves every call site.
+static __device__ __noinline__ void sha256_compress_1t(uint32_t* st, const uint32_t* blk) {
+  uint32_t s[8], w[16];
+#pragma unroll
+  for (int i = 0; i < 8; i++) s[i] = st[i];
+#pragma unroll
+  for (int i = 0; i < 16; i++) w[i] = blk[i];
+  sha256_compress(s, w);
+#pragma unroll
+  for (int i = 0; i < 8; i++) st[i] = s[i];
 }
 
+// Which compression a DevTrT runs: kUnrolled in the one-shot Fiat-Shamir launches, kCompact in the
+// tail loops (see sha256_compress_compact).
+enum class ShaForm { kUnrolled, kCompact };
 
 // The challenger held by the warp that advances it.  The partial SHA-256 block is kept as 16
 // big-endian words, the sample buffer as 8 little-endian words; absorbing a word is one store at
-// a run-time index (the arrays live in local memory, which the out-of-line compression reads
-// anyway), so the code stays small -- it runs once per launch and is fetched cold.  The stream is
+// a run-time index (the arrays live in local memory, which the out-of-line compression copies to
+// registers), so the code around the compression stays small.  The stream is
 // absorbed in 4-byte pieces (every message of the protocol is a whole number of words); a piece
 // may start at any byte offset.  Words at or past `len` hold no meaning except that a partially
 // filled word is zero past its bytes.
-struct DevTr {
+template <ShaForm kForm>
+struct DevTrT {
   uint32_t h[8], w[16], len;  // chaining value, partial block, bytes in it
   uint64_t total;             // bytes absorbed since the last reset
   uint32_t sampling, index;   // mode and bytes of buf consumed
   uint32_t buf[8];            // sample buffer, little-endian words
   uint32_t tape_len, tape_cap, error;
+
+  static __device__ __forceinline__ void compress(uint32_t* st, const uint32_t* blk) {
+    if (kForm == ShaForm::kUnrolled)
+      sha256_compress_1t(st, blk);
+    else
+      sha256_compress_compact(st, blk);
+  }
 
   __device__ __forceinline__ void load(const TranscriptState* g) {
     for (int i = 0; i < 8; i++) h[i] = g->h[i];
@@ -110,14 +130,14 @@ struct DevTr {
       w[len >> 2] = be;
       len += 4;
       if (len == 64) {
-        sha256_compress_1t(h, w);
+        compress(h, w);
         len = 0;
       }
     } else {
       w[len >> 2] |= be >> (8 * off);
       len += 4 - off;
       if (len == 64) {
-        sha256_compress_1t(h, w);
+        compress(h, w);
         len = 0;
       }
       w[len >> 2] = be << (8 * (4 - off));
@@ -134,12 +154,12 @@ struct DevTr {
     m[full] |= 0x80u << (24 - 8 * part);
     const uint64_t bits = total * 8;
     if (len + 9 > 64) {
-      sha256_compress_1t(st, m);
+      compress(st, m);
       for (int i = 0; i < 16; i++) m[i] = 0;
     }
     m[14] = (uint32_t)(bits >> 32);
     m[15] = (uint32_t)bits;
-    sha256_compress_1t(st, m);
+    compress(st, m);
     for (int i = 0; i < 8; i++) d[i] = st[i];
   }
 
@@ -240,6 +260,9 @@ struct DevTr {
     return bits >= 32 ? v : v & ((1u << bits) - 1);
   }
 };
+
+using DevTr = DevTrT<ShaForm::kUnrolled>;
+using DevTrLoop = DevTrT<ShaForm::kCompact>;
 
 // r's byte table for gf_mul_table, built by the calling block (any size) from r.
 __device__ __forceinline__ void dt_build_mul_table(uint4 r, uint4* __restrict__ tab) {

@@ -11,11 +11,12 @@ __device__ __forceinline__ void atomic_xor_gf(uint32_t* dst, uint4 v) {
   if (v.w) atomicXor(dst + 3, v.w);
 }
 
-__device__ __forceinline__ uint4 shfl_xor_gf(uint4 v, int lane_mask) {
-  v.x = __shfl_xor_sync(0xffffffffu, v.x, lane_mask);
-  v.y = __shfl_xor_sync(0xffffffffu, v.y, lane_mask);
-  v.z = __shfl_xor_sync(0xffffffffu, v.z, lane_mask);
-  v.w = __shfl_xor_sync(0xffffffffu, v.w, lane_mask);
+// The XOR of v over the 32 lanes of the (converged) warp, in every lane: one REDUX per word.
+__device__ __forceinline__ uint4 warp_xor_gf(uint4 v) {
+  v.x = __reduce_xor_sync(0xffffffffu, v.x);
+  v.y = __reduce_xor_sync(0xffffffffu, v.y);
+  v.z = __reduce_xor_sync(0xffffffffu, v.z);
+  v.w = __reduce_xor_sync(0xffffffffu, v.w);
   return v;
 }
 
@@ -27,8 +28,7 @@ __device__ __forceinline__ void block_xor_reduce(uint4 (&v)[NV], uint32_t* dst) 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int q = 0; q < NV; q++) {
-#pragma unroll
-    for (int m = 16; m >= 1; m >>= 1) gf_add_into(v[q], shfl_xor_gf(v[q], m));
+    v[q] = warp_xor_gf(v[q]);
     if (lane == 0) red[q][warp] = v[q];
   }
   __syncthreads();
@@ -36,9 +36,7 @@ __device__ __forceinline__ void block_xor_reduce(uint4 (&v)[NV], uint32_t* dst) 
     const int nwarps = (blockDim.x + 31) >> 5;
 #pragma unroll
     for (int q = 0; q < NV; q++) {
-      uint4 x = lane < nwarps ? red[q][lane] : gf_zero();
-#pragma unroll
-      for (int m = 16; m >= 1; m >>= 1) gf_add_into(x, shfl_xor_gf(x, m));
+      const uint4 x = warp_xor_gf(lane < nwarps ? red[q][lane] : gf_zero());
       if (lane == 0) atomic_xor_gf(dst + 4 * q, x);
     }
   }
@@ -52,8 +50,7 @@ __device__ __forceinline__ void block_xor_sum(uint4 (&v)[NV]) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int q = 0; q < NV; q++) {
-#pragma unroll
-    for (int m = 16; m >= 1; m >>= 1) gf_add_into(v[q], shfl_xor_gf(v[q], m));
+    v[q] = warp_xor_gf(v[q]);
     if (lane == 0) red[q][warp] = v[q];
   }
   __syncthreads();
@@ -61,9 +58,7 @@ __device__ __forceinline__ void block_xor_sum(uint4 (&v)[NV]) {
     const int nwarps = (blockDim.x + 31) >> 5;
 #pragma unroll
     for (int q = 0; q < NV; q++) {
-      uint4 x = lane < nwarps ? red[q][lane] : gf_zero();
-#pragma unroll
-      for (int m = 16; m >= 1; m >>= 1) gf_add_into(x, shfl_xor_gf(x, m));
+      const uint4 x = warp_xor_gf(lane < nwarps ? red[q][lane] : gf_zero());
       v[q] = x;
     }
   }

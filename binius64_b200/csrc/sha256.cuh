@@ -72,8 +72,9 @@ __device__ __forceinline__ void sha256_compress(uint32_t s[8], uint32_t w[16]) {
 }
 
 // The same compression as one small out-of-line copy (a four-round body run 16 times), for the
-// device transcript's single-warp steps, which run once per launch: there the fully unrolled form
-// costs more in cold instruction fetch than in arithmetic.
+// device transcript's single-warp steps inside the sumcheck tail loops: there one warp alternates
+// between the compression and the rest of the round's code, and the fully unrolled form (30 KiB
+// of instructions) measured slower than this 2 KiB loop.
 static __device__ __noinline__ void sha256_compress_compact(uint32_t* st, const uint32_t* blk) {
   // win[0..16) = W[t .. t + 16) for the round t about to run; each pass extends the schedule by
   // four words (win[16..20)), runs rounds t .. t + 3 and slides the window, so every index is

@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(kShiftTailThreads)
   pdl_wait();
   pdl_trigger();
   __shared__ uint4 r_sh;
-  DevTr st;
+  DevTrLoop st;
   uint4 sum = gf_zero(), inout = gf_zero(), eqp = gf_zero();
   if (threadIdx.x < 32) {
     st.load(ts);
