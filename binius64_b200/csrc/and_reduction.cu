@@ -593,34 +593,69 @@ int fold_words64(const uint64_t* d_words, uint64_t n, const hu128* vec64, uint4*
 }
 
 // d_witness: committed_total_len words; writes the AND reduction's transcript messages.
-int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcript& t,
-                        AndResult& res, cudaStream_t s) {
+void and_prep_free(AndPrep& p, cudaStream_t s) {
+  dev_free(p.words, s);
+  dev_free(p.eq_big, s);
+  dev_free(p.fcols, s);
+  dev_free(p.eq, s);
+  dev_free(p.d_acc, s);
+  dev_free(p.mul_tab, s);
+  dev_free(p.dev, s);
+  p = AndPrep();
+}
+
+int and_reduction_begin(const binius_cs* cs, const uint64_t* d_witness, AndPrep& p,
+                        cudaStream_t s) {
   const uint64_t N = cs->and_ops.n_constraints;
   uint32_t log_n = 0;
   while ((1ull << log_n) < N) log_n++;
   if (log_n < 3) return set_error(BINIUS_E_ARG, "AND reduction needs at least 8 constraints");
-  const uint64_t n_chunks = N >> 3;
-  DevAndTables tab;
-  if (int rc = device_tables(tab)) return rc;
-  const AndConstants& C = and_constants();
+  p = AndPrep();
+  cudaError_t e;
+  if ((e = dev_alloc(&p.words, 8 * 3 * N, s)) != cudaSuccess ||
+      (e = dev_alloc(&p.eq_big, 16 * (N >> 3), s)) != cudaSuccess ||
+      (e = dev_alloc(&p.fcols, 16 * 3 * N, s)) != cudaSuccess ||
+      (e = dev_alloc(&p.eq, 16 * (N / 2), s)) != cudaSuccess ||
+      // 64 univariate slots, then one (y_1, y_inf) slot pair per MLE-check round, zeroed once
+      (e = dev_alloc(&p.d_acc, 16 * (64 + 2 * (log_n + 1)), s)) != cudaSuccess ||
+      (e = dev_alloc(&p.mul_tab, 16 * kMulTableEntries, s)) != cudaSuccess ||
+      // round constants (2 per round), the claim slot pair, the challenges
+      (e = dev_alloc(&p.dev, 16 * (2 * (log_n + 1) + log_n), s)) != cudaSuccess) {
+    and_prep_free(p, s);
+    return cuda_error(e, "AND reduction buffers");
+  }
+  if (int rc = eval_operands(cs->and_ops, d_witness, p.words, s)) {
+    and_prep_free(p, s);
+    return rc;
+  }
+  return BINIUS_OK;
+}
 
-  uint64_t* words = nullptr;
-  uint4 *eq_big = nullptr, *fcols = nullptr, *eq = nullptr;
-  uint32_t* d_acc = nullptr;
-  BGPU_CUDA(dev_alloc(&words, 8 * 3 * N, s));
-  BGPU_CUDA(dev_alloc(&eq_big, 16 * n_chunks, s));
-  BGPU_CUDA(dev_alloc(&fcols, 16 * 3 * N, s));
-  BGPU_CUDA(dev_alloc(&eq, 16 * (N / 2), s));
-  // 64 univariate slots, then one (y_1, y_inf) slot pair per MLE-check round, zeroed once
-  BGPU_CUDA(dev_alloc(&d_acc, 16 * (64 + 2 * (log_n + 1)), s));
-  uint4* mul_tab = nullptr;
-  BGPU_CUDA(dev_alloc(&mul_tab, 16 * kMulTableEntries, s));
-  // round constants (2 per round), the claim slot pair, the challenges
-  uint4* dev = nullptr;
-  BGPU_CUDA(dev_alloc(&dev, 16 * (2 * (log_n + 1) + log_n), s));
-  int rc = BINIUS_OK;
+int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcript& t,
+                        AndResult& res, cudaStream_t s) {
+  AndPrep p;
+  if (int rc = and_reduction_begin(cs, d_witness, p, s)) return rc;
+  return and_reduction_finish(cs, p, t, res, s);
+}
+
+int and_reduction_finish(const binius_cs* cs, AndPrep& p, Transcript& t, AndResult& res,
+                         cudaStream_t s) {
+  const uint64_t N = cs->and_ops.n_constraints;
+  uint32_t log_n = 0;
+  while ((1ull << log_n) < N) log_n++;
+  const uint64_t n_chunks = N >> 3;
+  const AndConstants& C = and_constants();
+  uint64_t* const words = p.words;
+  uint4* const eq_big = p.eq_big;
+  uint4* const fcols = p.fcols;
+  uint4* const eq = p.eq;
+  uint32_t* const d_acc = p.d_acc;
+  uint4* const mul_tab = p.mul_tab;
+  uint4* const dev = p.dev;
+  DevAndTables tab;
+  int rc = device_tables(tab);
   do {
-    if ((rc = eval_operands(cs->and_ops, d_witness, words, s))) break;
+    if (rc) break;
     // big-field zerocheck challenges
     std::vector<uint8_t> big(16 * (log_n - 3));
     for (uint32_t i = 0; i < log_n - 3; i++) t.sample_elem(big.data() + 16 * i);
@@ -743,13 +778,7 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
     res.c_eval = from_bytes16(ev + 32);
     res.eval_point.assign(challenges.rbegin(), challenges.rend());
   } while (0);
-  dev_free(words, s);
-  dev_free(eq_big, s);
-  dev_free(fcols, s);
-  dev_free(eq, s);
-  dev_free(d_acc, s);
-  dev_free(mul_tab, s);
-  dev_free(dev, s);
+  and_prep_free(p, s);
   return rc;
 }
 

@@ -351,6 +351,34 @@ cudaError_t stream_wait(cudaStream_t s) {
   }
 }
 
+namespace {
+thread_local cudaEvent_t t_mark_event = nullptr;
+}  // namespace
+
+cudaError_t stream_mark(cudaStream_t s) {
+  if (!t_mark_event) {
+    cudaError_t e = cudaEventCreateWithFlags(&t_mark_event,
+                                             cudaEventBlockingSync | cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaEventRecord(t_mark_event, s);
+}
+
+cudaError_t mark_wait() {
+  if (!t_mark_event) return cudaErrorInvalidResourceHandle;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    const cudaError_t e = cudaEventQuery(t_mark_event);
+    if (e != cudaErrorNotReady) return e;
+    if (t_blocking_wait) {
+      if (std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0)
+              .count() >= t_poll_micros)
+        return cudaEventSynchronize(t_mark_event);
+      std::this_thread::yield();
+    }
+  }
+}
+
 // The stream-ordered allocator of `device` keeps freed blocks cached (release threshold = max)
 // instead of returning them to the driver at every synchronisation: a proof synchronises once per
 // sumcheck round and reallocates its scratch per phase.  The attribute belongs to this process's

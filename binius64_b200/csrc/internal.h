@@ -36,6 +36,10 @@ int cuda_error(cudaError_t e, const char* what);
 // set_blocking_waits(true, us)) an event poll that yields the core for up to `us` microseconds,
 // then a blocking-sync wait.
 cudaError_t stream_wait(cudaStream_t s);
+// A point on s that the calling thread waits for later with mark_wait (one outstanding mark per
+// thread), while the work queued on s after it runs on; mark_wait waits as stream_wait does.
+cudaError_t stream_mark(cudaStream_t s);
+cudaError_t mark_wait();
 void set_blocking_waits(bool on, double poll_micros = 100.0);
 
 // Device-to-host reads through a per-thread pinned staging buffer: add() queues copies on the

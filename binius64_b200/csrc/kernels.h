@@ -13,15 +13,6 @@ struct Point32 {
   uint4 r[32];
 };
 
-// One contiguous copy of a gather: `bytes` (a multiple of 16, 16-byte aligned) from src to
-// dst + dst_off.
-struct GatherSegment {
-  const uint8_t* src;
-  uint64_t dst_off;
-  uint32_t bytes;
-  uint32_t pad;
-};
-
 // eq_ind_partial_eval of a host point with n <= 32 coordinates into d_out (2^n elements).
 int eq_tensor(const uint4* h_point, uint32_t n, uint4* d_out, cudaStream_t s);
 // d_out512 (128 elements) = fold_1b_rows_for_b128(mat, vec) over n rows.
@@ -58,7 +49,6 @@ int bivariate_tail(const DeviceTranscript& dt, uint4* d_a, uint4* d_b, uint64_t 
 // Sumcheck rounds whose arrays have at most this many elements before the fold run in the
 // single-CTA tail kernels (the calling thread's Tuning::tail_log; 2^11 by default).
 inline uint64_t tail_max_len() { return 1ull << tuning().tail_log; }
-int gather_segments(const GatherSegment* d_segs, uint32_t n, uint8_t* d_dst, cudaStream_t s);
 // d_tab (16 * 256 elements) = the byte table of multiplication by r (gf_mul_table).
 int build_mul_table(const uint8_t r[16], uint4* d_tab, cudaStream_t s);
 // Folds of at least this many elements multiply by the fold challenge through its byte table.
@@ -104,5 +94,12 @@ inline int merkle_commit_with(uint32_t hash, const void* d_elems, uint32_t log_l
 int fri_commit_interleaved(const binius_ntt* ntt, const void* d_msg, uint32_t log_dim,
                            uint32_t log_inv_rate, uint32_t log_batch, uint32_t merkle_hash,
                            void* d_codeword, void* d_nodes, void* h_root, cudaStream_t s);
+// binius_pcs_commit without the root's read-back: queues the encode and the Merkle commit on s;
+// the root is at pcs_committed_root(*out) on the device once they ran, and the caller hands
+// the host copy to pcs_committed_set_root before anything reads the committed root.
+int pcs_commit_enqueue(const binius_pcs* P, const void* d_witness, binius_pcs_committed** out,
+                       cudaStream_t s);
+const uint8_t* pcs_committed_root(const binius_pcs_committed* c);
+void pcs_committed_set_root(binius_pcs_committed* c, const uint8_t* h_root);
 
 }  // namespace bgpu

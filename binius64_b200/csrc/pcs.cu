@@ -6,7 +6,7 @@
 // suffix, the ring-switch row fold, the ring-switch equality indicator, the BaseFold rounds
 // (bivariate product sumcheck, protocols/basefold.rs:130-166) interleaved with FRI folds and
 // Merkle commits of the folded codewords (fri/fold.rs:117-175), and the FRI query openings
-// (fri/fold.rs:221-244, fri/query.rs:51-134) gathered into one buffer by a single kernel.
+// (fri/fold.rs:221-244, fri/query.rs:51-134) gathered on the device into one buffer.
 #include <string.h>
 
 #include <algorithm>
@@ -69,7 +69,53 @@ u128h to_u128(const uint8_t b[16]) {
 }
 void from_u128(u128h v, uint8_t b[16]) { memcpy(b, &v, 16); }
 
-uint64_t layer_off(uint32_t L, uint32_t j) { return (1ull << (L + 1)) - (1ull << (L + 1 - j)); }
+__host__ __device__ inline uint64_t layer_off(uint32_t L, uint32_t j) {
+  return (1ull << (L + 1)) - (1ull << (L + 1 - j));
+}
+
+// One opened oracle of a FRI query (FRIQueryProver::prove_at_index, fri/query.rs:51-110): the
+// query index is shifted right by `shift` first (the previous fold's arity), then the coset of
+// 2^log_coset elements at that index of `data` and the Merkle branch of `nodes` (a tree of 2^L
+// leaves whose layers are stored leaves-first) from the leaf up to layer `depth` are opened.
+struct QueryLevel {
+  const uint8_t* data;
+  const uint8_t* nodes;
+  uint32_t shift, log_coset, L, depth;
+};
+constexpr uint32_t kMaxQueryLevels = 16;
+struct QueryLayout {
+  QueryLevel lv[kMaxQueryLevels];
+  uint32_t n_levels;
+  uint64_t per_query;  // bytes one query opens
+};
+
+// The openings of every query, one warp per query: query q's bytes go to dst[q * per_query ..) in
+// the order the proof carries them (per level the coset values, then the branch siblings from
+// the leaf layer up), so the host appends the buffer as it is.
+__global__ void fri_query_gather_kernel(QueryLayout lay, const uint64_t* __restrict__ idx,
+                                        uint32_t n_queries, uint8_t* __restrict__ dst) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (q >= n_queries) return;
+  uint4* out = reinterpret_cast<uint4*>(dst + q * lay.per_query);
+  uint64_t index = idx[q];
+  for (uint32_t l = 0; l < lay.n_levels; l++) {
+    const QueryLevel v = lay.lv[l];
+    index >>= v.shift;
+    const uint32_t n_coset = 1u << v.log_coset;  // 16-byte elements
+    const uint4* coset = reinterpret_cast<const uint4*>(v.data) + (index << v.log_coset);
+    for (uint32_t i = lane; i < n_coset; i += 32) out[i] = coset[i];
+    out += n_coset;
+    const uint32_t n_sib = v.L - v.depth;
+    const uint4* nodes = reinterpret_cast<const uint4*>(v.nodes);
+    for (uint32_t i = lane; i < 2 * n_sib; i += 32) {
+      const uint32_t j = i >> 1;
+      const uint64_t node = layer_off(v.L, j) | ((index >> j) ^ 1);
+      out[i] = nodes[2 * node + (i & 1)];
+    }
+    out += 2 * n_sib;
+  }
+}
 
 // Device-side FRIFoldProver state.
 struct DevFri {
@@ -141,37 +187,23 @@ struct DevFri {
     curr_round++;
   }
 
-  void add_branch(std::vector<GatherSegment>& segs, uint64_t& off, const uint8_t* nodes,
-                  uint32_t L, uint64_t index, uint32_t depth) {
-    for (uint32_t j = 0; j < L - depth; j++) {
-      const uint64_t node = layer_off(L, j) | ((index >> j) ^ 1);
-      segs.push_back({nodes + 32 * node, off, 32, 0});
-      off += 32;
-    }
-  }
-
   // FRIFoldProver::finish_proof (fri/fold.rs:221-244) with FRIQueryProver (fri/query.rs:51-110).
   // The terminal codeword and the optimal Merkle layers are decommitments (tape only, unseen by
   // the challenger), so the query indices can be sampled first and every opened byte -- terminal
-  // codeword, layers, then per query the coset values and branches -- gathered in one pass and
-  // read back once, then appended in the reference's order.
+  // codeword, layers, then per query the coset values and branches -- gathered on the device into
+  // one buffer (bulk copies, then fri_query_gather_kernel from the uploaded indices) and read back
+  // once, then appended in the reference's order.
   int finish(Transcript& t) {
-    std::vector<GatherSegment> segs;
+    const auto depths = P.optimal_depths();
+    uint8_t* d_dst = nullptr;
+    uint64_t* d_idx = nullptr;
+    std::vector<std::pair<const uint8_t*, uint64_t>> bulk;
     uint64_t off = 0;
-    auto add_bulk = [&](const uint8_t* src, uint64_t bytes) {
-      for (uint64_t done = 0; done < bytes;) {  // segments of at most 1 MiB
-        const uint64_t n = bytes - done < (1ull << 20) ? bytes - done : (1ull << 20);
-        segs.push_back({src + done, off, (uint32_t)n, 0});
-        off += n;
-        done += n;
-      }
-    };
     {
       const uint8_t* term = static_cast<const uint8_t*>(words.empty() ? C.d_codeword : words.back());
       const uint32_t log_term = words.empty() ? C.log_len : word_log_len.back();
-      add_bulk(term, 16ull << log_term);
+      bulk.push_back({term, 16ull << log_term});
     }
-    const auto depths = P.optimal_depths();
     {
       std::vector<const uint8_t*> tr{static_cast<const uint8_t*>(C.d_nodes)};
       std::vector<uint32_t> tl{C.log_leaves};
@@ -181,40 +213,59 @@ struct DevFri {
       }
       for (size_t i = 0; i < tr.size() && i < depths.size(); i++) {
         const uint32_t d = depths[i], L = tl[i];
-        add_bulk(tr[i] + 32 * ((2ull << L) - 1 + 1 - (2ull << d)), 32ull << d);
+        bulk.push_back({tr[i] + 32 * ((2ull << L) - 1 + 1 - (2ull << d)), 32ull << d});
       }
     }
-    const uint8_t* cw = static_cast<const uint8_t*>(C.d_codeword);
-    for (uint32_t q = 0; q < P.n_queries; q++) {
-      uint64_t index = t.sample_bits(P.rs_log_len());
-      segs.push_back({cw + (index << P.log_batch) * 16, off, 16u << P.log_batch, 0});
-      off += 16u << P.log_batch;
-      add_branch(segs, off, static_cast<const uint8_t*>(C.d_nodes), C.log_leaves, index,
-                 depths[0]);
-      for (size_t i = 0; i < words.size() && i < P.arities.size() && i + 1 < depths.size(); i++) {
-        const uint32_t a = P.arities[i];
-        index >>= a;
-        const uint8_t* w = reinterpret_cast<const uint8_t*>(words[i]);
-        segs.push_back({w + (index << a) * 16, off, 16u << a, 0});
-        off += 16u << a;
-        add_branch(segs, off, trees[i], tree_log_leaves[i], index, depths[i + 1]);
-      }
+    for (const auto& b : bulk) off += b.second;
+    QueryLayout lay;
+    memset(&lay, 0, sizeof(lay));
+    lay.lv[0] = {static_cast<const uint8_t*>(C.d_codeword), static_cast<const uint8_t*>(C.d_nodes),
+                 0, P.log_batch, C.log_leaves, depths[0]};
+    lay.n_levels = 1;
+    for (size_t i = 0; i < words.size() && i < P.arities.size() && i + 1 < depths.size(); i++) {
+      if (lay.n_levels == kMaxQueryLevels) return set_error(BINIUS_E_ARG, "fri: too many folds");
+      lay.lv[lay.n_levels++] = {reinterpret_cast<const uint8_t*>(words[i]), trees[i],
+                                P.arities[i], P.arities[i], tree_log_leaves[i], depths[i + 1]};
     }
-    if (off == 0) return BINIUS_OK;
-    GatherSegment* d_segs = nullptr;
-    uint8_t* d_dst = nullptr;
-    BGPU_CUDA(dev_alloc(&d_segs, segs.size() * sizeof(GatherSegment), s));
-    BGPU_CUDA(dev_alloc(&d_dst, off, s));
-    std::vector<uint8_t> h(off);
+    lay.per_query = 0;
+    for (uint32_t l = 0; l < lay.n_levels; l++)
+      lay.per_query += (16ull << lay.lv[l].log_coset) + 32ull * (lay.lv[l].L - lay.lv[l].depth);
+    std::vector<uint64_t> idx(P.n_queries);
+    for (uint32_t q = 0; q < P.n_queries; q++) idx[q] = t.sample_bits(P.rs_log_len());
+    const uint64_t total = off + lay.per_query * P.n_queries;
+    if (total == 0) return BINIUS_OK;
+    BGPU_CUDA(dev_alloc(&d_dst, total, s));
+    std::vector<uint8_t> h(total);
     int rc = BINIUS_OK;
     do {
-      cudaError_t e = cudaMemcpyAsync(d_segs, segs.data(), segs.size() * sizeof(GatherSegment),
-                                      cudaMemcpyHostToDevice, s);
-      if (e != cudaSuccess) { rc = cuda_error(e, "upload query segments"); break; }
-      if ((rc = gather_segments(d_segs, (uint32_t)segs.size(), d_dst, s))) break;
-      rc = read_sync(h.data(), d_dst, off, s);
+      cudaError_t e = cudaSuccess;
+      uint64_t o = 0;
+      for (const auto& b : bulk) {
+        if (b.second)
+          e = cudaMemcpyAsync(d_dst + o, b.first, b.second, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) break;
+        o += b.second;
+      }
+      if (e != cudaSuccess) { rc = cuda_error(e, "fri decommitment copy"); break; }
+      if (P.n_queries) {
+        if ((e = dev_alloc(&d_idx, 8ull * P.n_queries, s)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(d_idx, idx.data(), 8ull * P.n_queries, cudaMemcpyHostToDevice,
+                                 s)) != cudaSuccess) {
+          rc = cuda_error(e, "fri query indices");
+          break;
+        }
+        const unsigned per_block = 4;  // warps (queries) per CTA
+        fri_query_gather_kernel<<<(P.n_queries + per_block - 1) / per_block, 32 * per_block, 0,
+                                  s>>>(lay, d_idx, P.n_queries, d_dst + off);
+        if ((e = cudaGetLastError()) != cudaSuccess) {
+          rc = cuda_error(e, "fri_query_gather_kernel");
+          break;
+        }
+        count_launch();
+      }
+      rc = read_sync(h.data(), d_dst, total, s);
     } while (0);
-    dev_free(d_segs, s);
+    dev_free(d_idx, s);
     dev_free(d_dst, s);
     if (rc) return rc;
     t.decommitment(h.data(), h.size());
@@ -222,12 +273,19 @@ struct DevFri {
   }
 };
 
-// TensorAlgebra<B1, B128>::transpose of the 128 x 128 bit matrix whose row k is s[k].
+// TensorAlgebra<B1, B128>::transpose of the 128 x 128 bit matrix whose row k is s[k]: out[j] bit
+// k = in[k] bit j.  Block swaps of halving size (64, 32, .., 1): at size j, row k < k + j (bit j
+// of k clear) trades its columns c + j for row k + j's columns c (bit j of c clear).
 void transpose128(const u128h in[128], u128h out[128]) {
-  for (int j = 0; j < 128; j++) {
-    u128h v = 0;
-    for (int k = 0; k < 128; k++) v |= (u128h)((in[k] >> j) & 1) << k;
-    out[j] = v;
+  for (int k = 0; k < 128; k++) out[k] = in[k];
+  u128h m = ~(u128h)0 >> 64;  // columns with bit j clear, j = 64
+  for (int j = 64; j >= 1; j >>= 1, m ^= m << j) {
+    for (int k = 0; k < 128; k++) {
+      if (k & j) continue;
+      const u128h t = ((out[k] >> j) ^ out[k + j]) & m;
+      out[k + j] ^= t;
+      out[k] ^= t << j;
+    }
   }
 }
 
@@ -256,6 +314,9 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
       if ((rc = eq_tensor(reinterpret_cast<const uint4*>(h_point + 16 * 7), n, b, s))) break;
       // s_hat_v = fold_1b_rows_for_b128(witness, suffix_tensor)
       if ((rc = fold_1b_rows(static_cast<const uint4*>(d_witness), b, N, d_small, s))) break;
+      // the BaseFold message copy needs no challenge: queued before the host round trip
+      cudaError_t e = cudaMemcpyAsync(a, d_witness, 16 * N, cudaMemcpyDeviceToDevice, s);
+      if (e != cudaSuccess) { rc = cuda_error(e, "copy witness"); break; }
       uint8_t s_hat_v[128 * 16];
       if ((rc = read_sync(s_hat_v, d_small, sizeof(s_hat_v), s))) break;
       t.message(s_hat_v, sizeof(s_hat_v));
@@ -275,7 +336,7 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
           h_eq[k] ^= hi;
         }
       }
-      cudaError_t e = cudaMemcpyAsync(eq_r, h_eq, sizeof(h_eq), cudaMemcpyHostToDevice, s);
+      e = cudaMemcpyAsync(eq_r, h_eq, sizeof(h_eq), cudaMemcpyHostToDevice, s);
       if (e != cudaSuccess) { rc = cuda_error(e, "eq(r'') upload"); break; }
       u128h sum = 0;
       for (int j = 0; j < 128; j++) sum ^= host_gf_mul(u[j], h_eq[j]);
@@ -285,8 +346,6 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
       if (e != cudaSuccess) { rc = cuda_error(e, "round sums"); break; }
       // rs_eq_ind = fold_b128_elems_inplace(suffix_tensor, eq(r'')) in place in b
       if ((rc = fold_b128_elems(b, b, N, eq_r, s))) break;
-      e = cudaMemcpyAsync(a, d_witness, 16 * N, cudaMemcpyDeviceToDevice, s);
-      if (e != cudaSuccess) { rc = cuda_error(e, "copy witness"); break; }
 
       // BaseFold rounds on the device transcript: the round's sums, the FRI fold and commit on a
       // commit round, then the finish kernel (message, root, challenge, next table)
@@ -404,6 +463,33 @@ int binius_pcs_commit(const binius_pcs* P, const void* d_witness, binius_pcs_com
   BGPU_ARG(P != nullptr && d_witness != nullptr && out != nullptr, "NULL argument");
   *out = nullptr;
   cudaStream_t s = as_stream(stream);
+  binius_pcs_committed* c = nullptr;
+  if (int rc = pcs_commit_enqueue(P, d_witness, &c, s)) return rc;
+  const uint8_t* d_root = pcs_committed_root(c);
+  if (int rc = read_sync(c->root, d_root, 32, s)) {
+    binius_pcs_committed_destroy(c);
+    return rc;
+  }
+  if (h_root) memcpy(h_root, c->root, 32);
+  *out = c;
+  return clear_error();
+}
+
+}  // extern "C"
+
+namespace bgpu {
+
+const uint8_t* pcs_committed_root(const binius_pcs_committed* c) {
+  return static_cast<const uint8_t*>(c->d_nodes) + 32 * ((2ull << c->log_leaves) - 2);
+}
+
+void pcs_committed_set_root(binius_pcs_committed* c, const uint8_t* h_root) {
+  memcpy(c->root, h_root, 32);
+}
+
+int pcs_commit_enqueue(const binius_pcs* P, const void* d_witness, binius_pcs_committed** out,
+                       cudaStream_t s) {
+  *out = nullptr;
   binius_pcs_committed* c = new binius_pcs_committed();
   BGPU_CUDA(cudaGetDevice(&c->device));
   c->log_len = P->log_len();
@@ -420,7 +506,7 @@ int binius_pcs_commit(const binius_pcs* P, const void* d_witness, binius_pcs_com
     if (e != cudaSuccess) { rc = cuda_error(e, "dev_alloc(tree)"); break; }
     if ((rc = fri_commit_interleaved(P->ntt, d_witness, P->log_dim(), P->log_inv_rate,
                                      P->log_batch, P->merkle_hash, c->d_codeword, c->d_nodes,
-                                     c->root, s)))
+                                     nullptr, s)))
       break;
   } while (0);
   if (rc) {
@@ -429,10 +515,13 @@ int binius_pcs_commit(const binius_pcs* P, const void* d_witness, binius_pcs_com
     delete c;
     return rc;
   }
-  if (h_root) memcpy(h_root, c->root, 32);
   *out = c;
-  return clear_error();
+  return BINIUS_OK;
 }
+
+}  // namespace bgpu
+
+extern "C" {
 
 // Releases the buffers in order on the commit stream, which must still exist.
 int binius_pcs_committed_destroy(binius_pcs_committed* c) {

@@ -282,30 +282,39 @@ int binius_prover_prove(const binius_prover* P, const void* d_witness,
     t_phase_ms[phase] = std::chrono::duration<double, std::milli>(now - t0).count();
     t0 = now;
   };
-  // One MUL constraint: its four operand words ride back with the commitment's root (same
-  // synchronisation), and the IntMul reduction then needs no device work.
+  // The opening host round trip: the commitment's root -- and, with one MUL constraint, that
+  // constraint's four operand words, after which the IntMul reduction needs no device work --
+  // ride back through the pinned early buffer while the device goes on with the AND reduction's
+  // operand evaluation, queued behind the commit (it needs no challenge).
   const bool single_mul = cs->mul_ops.n_constraints == 1;
-  uint8_t* mul_words = nullptr;
+  uint8_t* early = nullptr;
+  if (int rc = early_read_buffer(&early)) return rc;
   if (single_mul) {
     uint64_t* d_cols = nullptr;
-    if (int rc = early_read_buffer(&mul_words)) return rc;
     BGPU_CUDA(dev_alloc(&d_cols, 32, s));
     if (int rc = eval_operands(cs->mul_ops, words, d_cols, s)) return rc;
-    BGPU_CUDA(cudaMemcpyAsync(mul_words, d_cols, 32, cudaMemcpyDeviceToHost, s));
+    BGPU_CUDA(cudaMemcpyAsync(early, d_cols, 32, cudaMemcpyDeviceToHost, s));
   }
   // [phase] Witness Commit
   binius_pcs_committed* committed = nullptr;
-  uint8_t root[32];
-  int rc = binius_pcs_commit(P->pcs, d_witness, &committed, root, stream);
+  int rc = pcs_commit_enqueue(P->pcs, d_witness, &committed, s);
   if (rc) return rc;
-  t.message(root, 32);
-  lap(0);
+  AndPrep ap;
   do {
+    cudaError_t e = cudaMemcpyAsync(early + 32, pcs_committed_root(committed), 32,
+                                    cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = stream_mark(s);
+    if (e != cudaSuccess) { rc = cuda_error(e, "commitment root read"); break; }
+    if ((rc = and_reduction_begin(cs, words, ap, s))) break;
+    if ((e = mark_wait()) != cudaSuccess) { rc = cuda_error(e, "commitment root read"); break; }
+    pcs_committed_set_root(committed, early + 32);
+    t.message(early + 32, 32);
+    lap(0);
     // [phase] IntMul Reduction
     IntMulResult im;
     if (single_mul) {
       uint64_t w[4];  // CSR slots a, b, hi, lo
-      memcpy(w, mul_words, 32);
+      memcpy(w, early, 32);
       rc = intmul_single_from_words(w[0], w[1], w[3], w[2], t, im);
     } else {
       rc = intmul_reduction_prove(cs, words, t, im, s);
@@ -314,7 +323,7 @@ int binius_prover_prove(const binius_prover* P, const void* d_witness,
     lap(1);
     // [phase] BitAnd Reduction
     AndResult ao;
-    if ((rc = and_reduction_prove(cs, words, t, ao, s))) break;
+    if ((rc = and_reduction_finish(cs, ap, t, ao, s))) break;
     lap(2);
     // OperatorData of both operations at the AND reduction's r_zhat'
     ShiftOperatorData band, bmul;
@@ -335,6 +344,7 @@ int binius_prover_prove(const binius_prover* P, const void* d_witness,
     rc = binius_pcs_prove(P->pcs, committed, d_witness, sh.point.data(), transcript, stream);
     lap(4);
   } while (0);
+  if (ap.words) and_prep_free(ap, s);  // a failure before the AND reduction ran
   binius_pcs_committed_destroy(committed);
   if (!rc && fresh_arena) prover_note_footprint(P, arena_held_bytes());
   return rc ? rc : clear_error();

@@ -22,6 +22,19 @@ struct AndResult {
 // d_witness: committed_total_len words; writes the AND reduction's transcript messages.
 int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcript& t,
                         AndResult& res, cudaStream_t s);
+// The same in two steps: and_reduction_begin queues what needs no challenge (the device buffers
+// and the operand evaluation), so a caller can queue it before a host round trip;
+// and_reduction_finish runs the rest and releases the buffers (also on error).
+struct AndPrep {
+  uint64_t* words = nullptr;
+  uint4 *eq_big = nullptr, *fcols = nullptr, *eq = nullptr, *mul_tab = nullptr, *dev = nullptr;
+  uint32_t* d_acc = nullptr;
+};
+int and_reduction_begin(const binius_cs* cs, const uint64_t* d_witness, AndPrep& p,
+                        cudaStream_t s);
+int and_reduction_finish(const binius_cs* cs, AndPrep& p, Transcript& t, AndResult& res,
+                         cudaStream_t s);
+void and_prep_free(AndPrep& p, cudaStream_t s);
 
 // IntMulOutput (verifier/verifier/src/protocols/intmul/common.rs:6-13): bit-column evaluations
 // of a, b, c_lo and c_hi at eval_point.

@@ -317,15 +317,6 @@ __global__ void build_mul_table_kernel(uint4 r, uint4* __restrict__ tab) {
   tab[idx] = acc;
 }
 
-__global__ void gather_segments_kernel(const GatherSegment* __restrict__ segs, uint32_t n,
-                                       uint8_t* __restrict__ dst) {
-  for (uint32_t s = blockIdx.x; s < n; s += gridDim.x) {
-    const GatherSegment g = segs[s];
-    const uint4* src = reinterpret_cast<const uint4*>(g.src);
-    uint4* d = reinterpret_cast<uint4*>(dst + g.dst_off);
-    for (uint32_t i = threadIdx.x; i < g.bytes / 16; i += blockDim.x) d[i] = src[i];
-  }
-}
 
 }  // namespace
 
@@ -475,13 +466,6 @@ int bivariate_tail(const DeviceTranscript& dt, uint4* d_a, uint4* d_b, uint64_t 
   return BINIUS_OK;
 }
 
-int gather_segments(const GatherSegment* d_segs, uint32_t n, uint8_t* d_dst, cudaStream_t s) {
-  if (n == 0) return BINIUS_OK;
-  gather_segments_kernel<<<std::min<uint32_t>(n, 148 * 16), 64, 0, s>>>(d_segs, n, d_dst);
-  BGPU_LAUNCH_CHECK("gather_segments_kernel");
-  count_launch();
-  return BINIUS_OK;
-}
 
 }  // namespace bgpu
 
