@@ -43,6 +43,9 @@ constexpr int kT = 256;
 // Round kernels on multilinears of at most this many elements run few threads once per launch,
 // so they take the compact out-of-line multiply (their code is fetched cold).
 constexpr uint64_t kSmallRound = 1ull << 12;
+// (pair, position) items of the layer rounds that run in intmul_layer_tail_kernel: a quarter of
+// the other sumchecks' tail length (a layer item folds two multilinears at two positions).
+inline uint64_t tail_items() { return tail_max_len() >> 2; }
 
 struct Pow64 {
   uint4 p[64];
@@ -377,6 +380,95 @@ __global__ void __launch_bounds__(kImFinishThreads)
   }
 }
 
+// The small last rounds of one GKR layer's batched MLE-check (IntMulDevice::layer: `pairs`
+// bivariate product claims, one eq point, messages of three coefficients) in one CTA, from round
+// t0 on: per round every multilinear of the set folds 2L -> L by the previous challenge (r_first
+// for round t0 when t0 > 0), the products are summed with their eq weights, and warp 0 runs the
+// batch's Fiat-Shamir step with the transcript in its registers.  The step is the one of
+// intmul_round_finish_kernel rewritten for a single group: the message is linear in the round's
+// sums, so with Y1 = sum_p beta^p y_1,p and Yinf = sum_p beta^p y_inf,p (one block sum per
+// round) and the running G = sum_p beta^p sum_p, T0 = (G + alpha Y1) / (1 + alpha),
+// T1 = Y1 + T0 + Yinf, T2 = Yinf, the message is prefix ((1 + alpha) T0, (1 + alpha) T1 + T0,
+// (1 + alpha) T2 + T1), and after r the batch keeps G = T0 + r T1 + r^2 T2 and
+// prefix (1 + r + alpha).  Thread items are (pair, index) with the index fastest; item i of pair
+// p folds positions i and L/2 + i of both multilinears and evaluates that pair of positions.
+constexpr int kImTailThreads = 512;
+__global__ void __launch_bounds__(kImTailThreads)
+    intmul_layer_tail_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
+                             uint4* __restrict__ set, uint32_t pairs, uint64_t stride,
+                             uint32_t n, uint32_t t0, const uint4* __restrict__ eq_base,
+                             const uint4* __restrict__ sums, const uint4* __restrict__ prefix,
+                             const ImAlpha* __restrict__ alphas,
+                             const uint4* __restrict__ beta_pow, uint4* __restrict__ chal) {
+  pdl_wait();
+  pdl_trigger();
+  __shared__ uint4 r_sh;
+  DevTrLoop st;
+  uint4 G = gf_zero(), pf = gf_zero();
+  {
+    uint4 v[1] = {gf_zero()};
+    for (uint32_t p = threadIdx.x; p < pairs; p += blockDim.x)
+      gf_add_into(v[0], gf_mul_nl(beta_pow[p], sums[p]));
+    block_xor_sum<1>(v);
+    if (threadIdx.x < 32) {
+      G = v[0];
+      pf = prefix[0];
+      st.load(ts);
+      if (t0 > 0) r_sh = chal[t0 - 1];
+    }
+    __syncthreads();
+  }
+  for (uint32_t t = t0; t < n; t++) {
+    const bool fold = t > 0;
+    const uint4 r = r_sh;
+    const uint64_t L = 1ull << (n - t), h = L >> 1;
+    const uint4* eq = eq_base + ((1ull << (n - t - 1)) - 1);
+    uint4 v[2] = {gf_zero(), gf_zero()};
+    for (uint64_t it = threadIdx.x; it < (uint64_t)pairs * h; it += blockDim.x) {
+      const uint32_t p = (uint32_t)(it / h);
+      const uint64_t i = it - (uint64_t)p * h;
+      uint4* a = set + 2 * (uint64_t)p * stride;
+      uint4* b = a + stride;
+      uint4 a0 = a[i], a1 = a[h + i], b0 = b[i], b1 = b[h + i];
+      if (fold) {
+        a0 = gf_add(a0, gf_mul_nl(r, gf_add(a[L + i], a0)));
+        a1 = gf_add(a1, gf_mul_nl(r, gf_add(a[L + h + i], a1)));
+        b0 = gf_add(b0, gf_mul_nl(r, gf_add(b[L + i], b0)));
+        b1 = gf_add(b1, gf_mul_nl(r, gf_add(b[L + h + i], b1)));
+        a[i] = a0;
+        a[h + i] = a1;
+        b[i] = b0;
+        b[h + i] = b1;
+      }
+      const uint4 w = gf_mul_nl(eq[i], beta_pow[p]);
+      gf_add_into(v[0], gf_mul_nl(w, gf_mul_nl(a1, b1)));
+      gf_add_into(v[1], gf_mul_nl(w, gf_mul_nl(gf_add(a0, a1), gf_add(b0, b1))));
+    }
+    block_xor_sum<2>(v);
+    if (threadIdx.x < 32) {
+      const ImAlpha al = alphas[t];
+      const uint4 y1 = v[0], yinf = v[1];
+      const uint4 T0 = gf_mul_warp(gf_add(G, gf_mul_warp(al.alpha, y1)), al.inv_one_plus_alpha);
+      const uint4 T1 = gf_add(gf_add(y1, T0), yinf), T2 = yinf;
+      uint4 oma = al.alpha;
+      oma.x ^= 1u;
+      const uint4 m[3] = {gf_mul_warp(pf, gf_mul_warp(oma, T0)),
+                          gf_mul_warp(pf, gf_add(gf_mul_warp(oma, T1), T0)),
+                          gf_mul_warp(pf, gf_add(gf_mul_warp(oma, T2), T1))};
+      st.message_elems(tape, m, 3);
+      const uint4 rr = st.sample_elem();
+      chal[t] = rr;
+      G = gf_add(T0, gf_mul_warp(rr, gf_add(T1, gf_mul_warp(rr, T2))));
+      uint4 f = gf_add(rr, al.alpha);
+      f.x ^= 1u;
+      pf = gf_mul_warp(pf, f);
+      r_sh = rr;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) st.store(ts);
+}
+
 // ---------------------------------------------------------------- host side
 
 uint4 u4(hu128 v) {
@@ -645,11 +737,21 @@ int IntMulDevice::layer(uint4* set, uint32_t pairs, std::vector<hu128>& point,
     for (uint32_t p = 0; p < pairs; p++) cl[p] = ImClaim{(uint16_t)(2 * p), (uint16_t)(2 * p + 1), 2, 0, 0};
     DevBatch b;
     if (int rc = batch_begin(b, cl, {&point}, claims, beta, 2 * pairs)) return rc;
-    for (uint32_t t = 0; t < n; t++) {
+    // rounds of at most tail_items() (pair, position) items run in one intmul_layer_tail_kernel
+    uint32_t t0 = 0;
+    while (t0 < n && ((uint64_t)pairs << (n - t0 - 1)) > tail_items()) t0++;
+    for (uint32_t t = 0; t < t0; t++) {
       if (int rc = biv_round(set, pairs, 1ull << (n - t), level(eq_, n - t - 1), batch_r(b, t),
                              batch_slots(b, t)))
         return rc;
       if (int rc = batch_round(b, t)) return rc;
+    }
+    if (t0 < n) {
+      BGPU_CUDA(launch_pdl(intmul_layer_tail_kernel, 1, kImTailThreads, 0, s_, b.dt.state(),
+                           b.dt.tape(), set, pairs, N_, n, t0, (const uint4*)eq_,
+                           (const uint4*)b.sums, (const uint4*)b.prefix,
+                           (const ImAlpha*)b.alphas, (const uint4*)b.beta, b.chal));
+      if (int rc = check("intmul_layer_tail_kernel")) return rc;
     }
     std::vector<hu128> ch, last(4 * pairs);
     StagedReads rd(s_);
