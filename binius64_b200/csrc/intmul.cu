@@ -273,12 +273,21 @@ __global__ void eq_levels_kernel(const uint4* __restrict__ points, uint32_t coun
     const uint64_t k = t / per, rr = t - k * per;
     const uint32_t lvl = 63 - __clzll(rr + 1);
     const uint64_t i = rr + 1 - (1ull << lvl);
-    uint4 acc = gf_one();
-    for (uint32_t j = 0; j < lvl; j++) {
+    // four interleaved partial products: the dependent chain is ~lvl / 4 multiplies, not lvl
+    auto factor = [&](uint32_t j) {
       const uint4 p = points[k * m + j];
-      acc = gf_mul(acc, ((i >> j) & 1) ? p : gf_add(p, gf_one()));
+      return ((i >> j) & 1) ? p : gf_add(p, gf_one());
+    };
+    uint4 a0 = gf_one(), a1 = gf_one(), a2 = gf_one(), a3 = gf_one();
+    uint32_t j = 0;
+    for (; j + 4 <= lvl; j += 4) {
+      a0 = gf_mul(a0, factor(j));
+      a1 = gf_mul(a1, factor(j + 1));
+      a2 = gf_mul(a2, factor(j + 2));
+      a3 = gf_mul(a3, factor(j + 3));
     }
-    out[k * stride + rr] = acc;
+    for (; j < lvl; j++) a0 = gf_mul(a0, factor(j));
+    out[k * stride + rr] = gf_mul(gf_mul(a0, a1), gf_mul(a2, a3));
   }
 }
 

@@ -42,9 +42,30 @@ unsigned grid_for(uint64_t n, unsigned threads, unsigned max_blocks = 148 * 8) {
 
 // out[j] = prod_i (bit_i(j) ? r_i : 1 + r_i) for n <= 16 coordinates.  Each block first builds
 // the eq tensors of the low k = min(n, 8) and the high n - k coordinates (at most 256 entries
-// each) in shared memory, then every output is one multiply lo[j mod 2^k] * hi[j >> k]: the
-// dependent chain is at most 8 multiplies + 1, where multiplying all n factors per output would be
-// n - 1.  These tensors are small and on the protocol's critical path, so latency matters.
+// each) in shared memory, then every output is one multiply lo[j mod 2^k] * hi[j >> k].  A table
+// entry multiplies its at most 8 factors as a balanced tree (depth 3, not a chain of 7).  These
+// tensors are small and on the protocol's critical path, so latency matters: the tables depend
+// only on the point (a kernel argument), so under programmatic dependent launch they are built
+// while the previous kernel still runs, and only the writes wait for it.
+__device__ __forceinline__ uint4 eq_factor(const Point32& p, uint32_t c, uint32_t idx,
+                                           uint32_t bit) {
+  uint4 f = p.r[c];
+  if (!((idx >> bit) & 1)) f.x ^= 1u;
+  return f;
+}
+__device__ __forceinline__ uint4 eq_entry(const Point32& p, uint32_t first, uint32_t cnt,
+                                          uint32_t idx) {
+  uint4 f[8];
+#pragma unroll
+  for (uint32_t i = 0; i < 8; i++) f[i] = i < cnt ? eq_factor(p, first + i, idx, i) : gf_one();
+#pragma unroll
+  for (uint32_t w = 1; w < 8; w <<= 1)
+#pragma unroll
+    for (uint32_t i = 0; i < 8; i += 2 * w)
+      if (i + w < cnt) f[i] = gf_mul(f[i], f[i + w]);
+  return f[0];
+}
+
 __global__ void __launch_bounds__(256)
     eq_small_kernel(uint4* __restrict__ out, Point32 p, uint32_t off, uint32_t n) {
   __shared__ uint4 s_lo[256], s_hi[256];
@@ -52,15 +73,11 @@ __global__ void __launch_bounds__(256)
   const uint32_t n_lo = 1u << k, n_hi = 1u << m;
   for (uint32_t t = threadIdx.x; t < n_lo + n_hi; t += blockDim.x) {
     const bool lo = t < n_lo;
-    const uint32_t idx = lo ? t : t - n_lo, first = lo ? 0 : k, cnt = lo ? k : m;
-    uint4 acc = gf_one();
-    for (uint32_t i = 0; i < cnt; i++) {
-      uint4 f = p.r[off + first + i];
-      if (!((idx >> i) & 1)) f.x ^= 1u;
-      acc = gf_mul(acc, f);
-    }
-    (lo ? s_lo : s_hi)[idx] = acc;
+    const uint32_t idx = lo ? t : t - n_lo;
+    (lo ? s_lo : s_hi)[idx] = lo ? eq_entry(p, off, k, idx) : eq_entry(p, off + k, m, idx);
   }
+  pdl_wait();
+  pdl_trigger();
   __syncthreads();
   const uint64_t total = 1ull << n;
   for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < total;
@@ -70,6 +87,8 @@ __global__ void __launch_bounds__(256)
 
 __global__ void eq_expand_kernel(uint4* __restrict__ out, const uint4* __restrict__ lo,
                                  const uint4* __restrict__ hi, uint32_t k, uint64_t total) {
+  pdl_wait();
+  pdl_trigger();
   const uint64_t mask = (1ull << k) - 1;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
        i += (uint64_t)gridDim.x * blockDim.x)
@@ -328,8 +347,8 @@ int eq_tensor(const uint4* h_point, uint32_t n, uint4* d_out, cudaStream_t s) {
   memset(&p, 0, sizeof(p));
   if (n) memcpy(p.r, h_point, 16 * (size_t)n);
   if (n <= 16) {
-    eq_small_kernel<<<grid_for(1ull << n, kThreads), kThreads, 0, s>>>(d_out, p, 0, n);
-    BGPU_LAUNCH_CHECK("eq_small_kernel");
+    BGPU_CUDA(launch_pdl(eq_small_kernel, grid_for(1ull << n, kThreads), kThreads, 0, s, d_out, p,
+                         0u, n));
     count_launch();
     return BINIUS_OK;
   }
@@ -337,11 +356,14 @@ int eq_tensor(const uint4* h_point, uint32_t n, uint4* d_out, cudaStream_t s) {
   uint4* tmp = nullptr;
   const uint64_t nlo = 1ull << k, nhi = 1ull << (n - k);
   BGPU_CUDA(dev_alloc(&tmp, 16 * (nlo + nhi), s));
-  eq_small_kernel<<<grid_for(nlo, kThreads), kThreads, 0, s>>>(tmp, p, 0, k);
-  eq_small_kernel<<<grid_for(nhi, kThreads), kThreads, 0, s>>>(tmp + nlo, p, k, n - k);
-  eq_expand_kernel<<<grid_for(1ull << n, kThreads, 148 * 16), kThreads, 0, s>>>(d_out, tmp, tmp + nlo,
-                                                                              k, 1ull << n);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e =
+      launch_pdl(eq_small_kernel, grid_for(nlo, kThreads), kThreads, 0, s, tmp, p, 0u, k);
+  if (e == cudaSuccess)
+    e = launch_pdl(eq_small_kernel, grid_for(nhi, kThreads), kThreads, 0, s, tmp + nlo, p, k,
+                   n - k);
+  if (e == cudaSuccess)
+    e = launch_pdl(eq_expand_kernel, grid_for(1ull << n, kThreads, 148 * 16), kThreads, 0, s,
+                   d_out, (const uint4*)tmp, (const uint4*)(tmp + nlo), k, 1ull << n);
   dev_free(tmp, s);
   if (e != cudaSuccess) return cuda_error(e, "eq tensor kernels");
   count_launch(3);
