@@ -788,24 +788,25 @@ class Prover:
                                         _stream(stream)))
         return t
 
-    TUNING_KEYS = ("tail_log", "ntt_pass_layers", "merkle_leaf_fuse", "merkle_node_fuse")
+    TUNING_KEYS = ("tail_log", "ntt_pass_layers", "merkle_leaf_fuse", "merkle_node_fuse",
+                   "ntt_tile_bits")
 
     def tuning(self) -> dict:
         """The prover's launch-shape choices (binius_prover_get_tuning)."""
-        out = (ctypes.c_uint32 * 4)()
+        out = (ctypes.c_uint32 * len(self.TUNING_KEYS))()
         check(lib().binius_prover_get_tuning(self._h, out))
         return dict(zip(self.TUNING_KEYS, list(out)))
 
     def set_tuning(self, **kw) -> None:
         t = self.tuning()
         t.update(kw)
-        buf = (ctypes.c_uint32 * 4)(*[t[k] for k in self.TUNING_KEYS])
+        buf = (ctypes.c_uint32 * len(self.TUNING_KEYS))(*[t[k] for k in self.TUNING_KEYS])
         check(lib().binius_prover_set_tuning(self._h, buf))
 
     def autotune(self, witness_words, reps: int = 3, stream=None) -> dict:
         """binius_prover_autotune: measures the launch-shape choices for this statement shape on
         the device witness, keeps the fastest (proof bytes unchanged) and returns them."""
-        out = (ctypes.c_uint32 * 4)()
+        out = (ctypes.c_uint32 * len(self.TUNING_KEYS))()
         check(lib().binius_prover_autotune(self._h, witness_words.data_ptr(), reps,
                                            _stream(stream), out))
         return dict(zip(self.TUNING_KEYS, list(out)))

@@ -117,6 +117,7 @@ struct Tuning {
   uint32_t ntt_pass_layers = 8;    // NTT layers fused per shared-memory pass (<= 8)
   uint32_t merkle_leaf_fuse = 8;   // Merkle leaf CTA: 2^fuse leaves, as many layers above them
   uint32_t merkle_node_fuse = 9;   // Merkle node CTA: 2^fuse inputs (<= 9)
+  uint32_t ntt_tile_bits = 12;     // NTT shared-memory tile: 2^bits elements (9..12)
 };
 // The calling thread's current choices (a prove sets its prover's for its duration).
 const Tuning& tuning();

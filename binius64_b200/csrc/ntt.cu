@@ -22,7 +22,7 @@ using namespace bgpu;
 namespace {
 
 constexpr int kNttThreads = 256;
-constexpr uint32_t kTileBits = 12;  // 4096 elements = 64 KiB of shared memory per tile
+constexpr uint32_t kTileBits = 12;  // the largest tile: 4096 elements = 64 KiB of shared memory
 constexpr uint32_t kMaxPassLayers = 8;
 
 struct NttPass {
@@ -125,23 +125,27 @@ __global__ void __launch_bounds__(kNttThreads)
 
 std::vector<NttPass> plan_passes(uint32_t log_d, uint32_t skip_early, uint32_t skip_late,
                                  bool rs, uint32_t rs_bits) {
+  // tiles of 2^tile_bits elements: fewer, larger tiles fuse more work per CTA; more, smaller ones
+  // spread a small transform evenly over the 148 SMs (a 2^20 codeword is 256 tiles of 2^12)
+  const uint32_t tile_bits = std::max(9u, std::min(kTileBits, tuning().ntt_tile_bits));
   std::vector<NttPass> passes;
   uint32_t n_layers = log_d - skip_late - skip_early;
   if (n_layers == 0) {
     if (rs) {
       uint32_t s = log_d - skip_early;
-      passes.push_back({log_d, skip_early, 0, std::min(kTileBits, s), rs_bits});
+      passes.push_back({log_d, skip_early, 0, std::min(tile_bits, s), rs_bits});
     }
     return passes;
   }
-  const uint32_t max_layers = std::max(1u, std::min(kMaxPassLayers, tuning().ntt_pass_layers));
+  const uint32_t max_layers =
+      std::max(1u, std::min({kMaxPassLayers, tuning().ntt_pass_layers, tile_bits}));
   uint32_t n_passes = (n_layers + max_layers - 1) / max_layers;
   uint32_t base = n_layers / n_passes, extra = n_layers % n_passes;
   uint32_t l0 = skip_early;
   for (uint32_t i = 0; i < n_passes; i++) {
     uint32_t k = base + (i < extra ? 1 : 0);
     uint32_t s = log_d - l0 - k;
-    uint32_t c = std::min(kTileBits - k, s);
+    uint32_t c = std::min(tile_bits - k, s);
     passes.push_back({log_d, l0, k, c, i == 0 ? rs_bits : 0u});
     l0 += k;
   }

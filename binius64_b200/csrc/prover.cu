@@ -84,14 +84,16 @@ void store_tuned(const binius_prover* P) {
 bool valid_tuning(const Tuning& t) {
   return t.tail_log >= 8 && t.tail_log <= 12 && t.ntt_pass_layers >= 4 &&
          t.ntt_pass_layers <= 8 && t.merkle_leaf_fuse >= 5 && t.merkle_leaf_fuse <= 8 &&
-         t.merkle_node_fuse >= 5 && t.merkle_node_fuse <= 9;
+         t.merkle_node_fuse >= 5 && t.merkle_node_fuse <= 9 && t.ntt_tile_bits >= 9 &&
+         t.ntt_tile_bits <= 12;
 }
 
-void tuning_out(const Tuning& t, uint32_t* out4) {
-  out4[0] = t.tail_log;
-  out4[1] = t.ntt_pass_layers;
-  out4[2] = t.merkle_leaf_fuse;
-  out4[3] = t.merkle_node_fuse;
+void tuning_out(const Tuning& t, uint32_t* out5) {
+  out5[0] = t.tail_log;
+  out5[1] = t.ntt_pass_layers;
+  out5[2] = t.merkle_leaf_fuse;
+  out5[3] = t.merkle_node_fuse;
+  out5[4] = t.ntt_tile_bits;
 }
 
 }  // namespace
@@ -180,22 +182,23 @@ int binius_prover_set_merkle_hash(binius_prover* P, uint32_t merkle_hash) {
   return clear_error();
 }
 
-int binius_prover_get_tuning(const binius_prover* P, uint32_t* h_out4) {
-  BGPU_ARG(P && h_out4, "NULL argument");
-  tuning_out(P->tuning, h_out4);
+int binius_prover_get_tuning(const binius_prover* P, uint32_t* h_out5) {
+  BGPU_ARG(P && h_out5, "NULL argument");
+  tuning_out(P->tuning, h_out5);
   return clear_error();
 }
 
-int binius_prover_set_tuning(binius_prover* P, const uint32_t* h_in4) {
-  BGPU_ARG(P && h_in4, "NULL argument");
+int binius_prover_set_tuning(binius_prover* P, const uint32_t* h_in5) {
+  BGPU_ARG(P && h_in5, "NULL argument");
   Tuning t;
-  t.tail_log = h_in4[0];
-  t.ntt_pass_layers = h_in4[1];
-  t.merkle_leaf_fuse = h_in4[2];
-  t.merkle_node_fuse = h_in4[3];
+  t.tail_log = h_in5[0];
+  t.ntt_pass_layers = h_in5[1];
+  t.merkle_leaf_fuse = h_in5[2];
+  t.merkle_node_fuse = h_in5[3];
+  t.ntt_tile_bits = h_in5[4];
   BGPU_ARG(valid_tuning(t),
            "tuning out of range: tail_log 8..12, ntt_pass_layers 4..8, merkle_leaf_fuse 5..8, "
-           "merkle_node_fuse 5..9");
+           "merkle_node_fuse 5..9, ntt_tile_bits 9..12");
   P->tuning = t;
   return clear_error();
 }
@@ -357,7 +360,7 @@ int binius_prover_prove(const binius_prover* P, const void* d_witness,
 // choices change no arithmetic); a difference is reported as an error and the starting choices
 // are kept.
 int binius_prover_autotune(binius_prover* P, const void* d_witness, uint32_t reps, void* stream,
-                           uint32_t* h_out4) {
+                           uint32_t* h_out5) {
   BGPU_ARG(P && d_witness, "NULL argument");
   reps = std::max(1u, std::min(reps, 64u));
   cudaStream_t s = as_stream(stream);
@@ -399,7 +402,8 @@ int binius_prover_autotune(binius_prover* P, const void* d_witness, uint32_t rep
     uint32_t Tuning::*field;
     uint32_t lo, hi;
   };
-  const Knob knobs[4] = {{&Tuning::tail_log, 8, 12},
+  const Knob knobs[5] = {{&Tuning::tail_log, 8, 12},
+                         {&Tuning::ntt_tile_bits, 10, 12},
                          {&Tuning::ntt_pass_layers, 6, 8},
                          {&Tuning::merkle_leaf_fuse, 6, 8},
                          {&Tuning::merkle_node_fuse, 7, 9}};
@@ -424,7 +428,7 @@ int binius_prover_autotune(binius_prover* P, const void* d_witness, uint32_t rep
   }
   P->tuning = best;
   store_tuned(P);
-  if (h_out4) tuning_out(best, h_out4);
+  if (h_out5) tuning_out(best, h_out5);
   return clear_error();
 }
 

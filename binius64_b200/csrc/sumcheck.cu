@@ -43,7 +43,8 @@ unsigned grid_for(uint64_t n, unsigned threads, unsigned max_blocks = 148 * 8) {
 // out[j] = prod_i (bit_i(j) ? r_i : 1 + r_i) for n <= 16 coordinates.  Each block first builds
 // the eq tensors of the low k = min(n, 8) and the high n - k coordinates (at most 256 entries
 // each) in shared memory, then every output is one multiply lo[j mod 2^k] * hi[j >> k].  A table
-// entry multiplies its at most 8 factors as a balanced tree (depth 3, not a chain of 7).  These
+// entry multiplies its at most 8 factors as a balanced tree (depth 3, not a chain of 7) with the
+// out-of-line multiply (the inlined one made the launch's cold code 7x longer).  These
 // tensors are small and on the protocol's critical path, so latency matters: the tables depend
 // only on the point (a kernel argument), so under programmatic dependent launch they are built
 // while the previous kernel still runs, and only the writes wait for it.
@@ -62,7 +63,7 @@ __device__ __forceinline__ uint4 eq_entry(const Point32& p, uint32_t first, uint
   for (uint32_t w = 1; w < 8; w <<= 1)
 #pragma unroll
     for (uint32_t i = 0; i < 8; i += 2 * w)
-      if (i + w < cnt) f[i] = gf_mul(f[i], f[i + w]);
+      if (i + w < cnt) f[i] = gf_mul_nl(f[i], f[i + w]);
   return f[0];
 }
 

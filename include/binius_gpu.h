@@ -305,24 +305,25 @@ int binius_prove(const binius_prover* prover, const uint64_t* h_words, size_t n_
                  binius_transcript* transcript, void* h_proof, size_t cap, size_t* len,
                  void* stream);
 /* Launch-shape choices of a prover's proofs, none of which changes a result (the arithmetic is
- * exact): h4 = {tail_log: sumcheck rounds on at most 2^tail_log elements run in one single-CTA
+ * exact): h5 = {tail_log: sumcheck rounds on at most 2^tail_log elements run in one single-CTA
  * kernel (8..12, default 11); ntt_pass_layers: NTT layers fused per shared-memory pass (4..8,
  * default 8); merkle_leaf_fuse: a Merkle leaf CTA hashes 2^k leaves and compresses k layers above
- * them (5..8, default 8); merkle_node_fuse: a node CTA reduces 2^k inputs (5..9, default 9)}.
+ * them (5..8, default 8); merkle_node_fuse: a node CTA reduces 2^k inputs (5..9, default 9);
+ * ntt_tile_bits: an NTT pass works on tiles of 2^k elements (9..12, default 12)}.
  * No reference counterpart (the reference's rayon code has no launch shapes).  Not while a prove
  * on the prover is in flight.
  * binius_prover_autotune measures them for the prover's statement shape: coordinate search over
- * the ranges above (tail_log 8..12, ntt 6..8, leaf 6..8, node 7..9), each candidate scored by the
- * median CUDA-event time of `reps` whole proofs of d_witness on `stream` after a warm-up proof,
- * every candidate's proof checked byte for byte against the first one (BINIUS_E_CUDA if one
- * differs; the prover keeps its choices).  The winner is kept by the prover, written to h_out4
- * when set, and cached for the process: provers set up later for the same shape (words, AND and
- * MUL counts, log_inv_rate, Merkle hash) start from it.  Synchronous; runs 14 x (reps + 1)
- * proofs at most. */
-int binius_prover_get_tuning(const binius_prover* prover, uint32_t* h_out4);
-int binius_prover_set_tuning(binius_prover* prover, const uint32_t* h_in4);
+ * the ranges above (tail_log 8..12, tile 10..12, ntt 6..8, leaf 6..8, node 7..9), each candidate
+ * scored by the median CUDA-event time of `reps` whole proofs of d_witness on `stream` after a
+ * warm-up proof, every candidate's proof checked byte for byte against the first one
+ * (BINIUS_E_CUDA if one differs; the prover keeps its choices).  The winner is kept by the
+ * prover, written to h_out5 when set, and cached for the process: provers set up later for the
+ * same shape (words, AND and MUL counts, log_inv_rate, Merkle hash) start from it.  Synchronous;
+ * runs 17 x (reps + 1) proofs at most. */
+int binius_prover_get_tuning(const binius_prover* prover, uint32_t* h_out5);
+int binius_prover_set_tuning(binius_prover* prover, const uint32_t* h_in5);
 int binius_prover_autotune(binius_prover* prover, const void* d_witness, uint32_t reps,
-                           void* stream, uint32_t* h_out4);
+                           void* stream, uint32_t* h_out5);
 /* committed_total_len of the prover's constraint system (the witness length in words). */
 uint64_t binius_prover_committed_words(const binius_prover* prover);
 /* Estimate of the device memory one proof allocates while it runs (admission of concurrent

@@ -103,15 +103,20 @@ def test_launch_shapes_change_no_bytes_and_autotune():
     ref = orc.prove(sc.witness, 2, prep.and_csr, prep.mul_csr, 1)
     p = bg.Prover(bg.DeviceConstraintSystem(sc.cs.serialize()), 1)
     w = torch.from_numpy(sc.witness.view(np.int64)).cuda()
-    assert p.tuning() == {"tail_log": 11, "ntt_pass_layers": 8, "merkle_leaf_fuse": 8,
-                          "merkle_node_fuse": 9}
+    default = {"tail_log": 11, "ntt_pass_layers": 8, "merkle_leaf_fuse": 8,
+               "merkle_node_fuse": 9, "ntt_tile_bits": 12}
+    assert p.tuning() == default
     for kw in ({"tail_log": 8}, {"tail_log": 12}, {"ntt_pass_layers": 4}, {"ntt_pass_layers": 6},
-               {"merkle_leaf_fuse": 5}, {"merkle_node_fuse": 5}, {"merkle_node_fuse": 7}):
+               {"merkle_leaf_fuse": 5}, {"merkle_node_fuse": 5}, {"merkle_node_fuse": 7},
+               {"ntt_tile_bits": 9}, {"ntt_tile_bits": 10, "ntt_pass_layers": 8},
+               {"ntt_tile_bits": 11, "ntt_pass_layers": 5}):
         p.set_tuning(**kw)
         assert p.prove(w).finalize() == ref, kw
-        p.set_tuning(tail_log=11, ntt_pass_layers=8, merkle_leaf_fuse=8, merkle_node_fuse=9)
+        p.set_tuning(**default)
     with pytest.raises(bg.ArgumentError):
         p.set_tuning(tail_log=20)
+    with pytest.raises(bg.ArgumentError):
+        p.set_tuning(ntt_tile_bits=8)
     best = p.autotune(w, reps=1)
     assert 8 <= best["tail_log"] <= 12 and 6 <= best["ntt_pass_layers"] <= 8
     assert p.tuning() == best
