@@ -470,7 +470,7 @@ __global__ void __launch_bounds__(kAndTailThreads)
   pdl_wait();
   pdl_trigger();
   __shared__ uint4 r_sh;
-  DevTrLoop st;
+  DevTr st;
   uint4 cl = gf_zero();
   if (threadIdx.x < 32) {
     st.load(ts);
@@ -483,9 +483,9 @@ __global__ void __launch_bounds__(kAndTailThreads)
     const uint64_t h = len >> 1, q = len >> 2;
     for (uint64_t j = threadIdx.x; j < h; j += blockDim.x) {
       const uint4 a0 = fa[j], b0 = fb[j], c0 = fc[j];
-      fa[j] = gf_add(a0, gf_mul(r, gf_add(fa[h + j], a0)));
-      fb[j] = gf_add(b0, gf_mul(r, gf_add(fb[h + j], b0)));
-      fc[j] = gf_add(c0, gf_mul(r, gf_add(fc[h + j], c0)));
+      fa[j] = gf_add(a0, gf_mul_nl(r, gf_add(fa[h + j], a0)));
+      fb[j] = gf_add(b0, gf_mul_nl(r, gf_add(fb[h + j], b0)));
+      fc[j] = gf_add(c0, gf_mul_nl(r, gf_add(fc[h + j], c0)));
     }
     for (uint64_t j = threadIdx.x; j < q; j += blockDim.x) eq[j] = gf_add(eq[j], eq[q + j]);
     len = h;
@@ -494,8 +494,8 @@ __global__ void __launch_bounds__(kAndTailThreads)
     for (uint64_t j = threadIdx.x; j < q; j += blockDim.x) {
       const uint4 e = eq[j];
       const uint4 a0 = fa[j], a1 = fa[q + j], b0 = fb[j], b1 = fb[q + j], c1 = fc[q + j];
-      gf_add_into(v[0], gf_mul(e, gf_add(gf_mul(a1, b1), c1)));
-      gf_add_into(v[1], gf_mul(e, gf_mul(gf_add(a0, a1), gf_add(b0, b1))));
+      gf_add_into(v[0], gf_mul_nl(e, gf_add(gf_mul_nl(a1, b1), c1)));
+      gf_add_into(v[1], gf_mul_nl(e, gf_mul_nl(gf_add(a0, a1), gf_add(b0, b1))));
     }
     block_xor_sum<2>(v);
     if (threadIdx.x < 32) {

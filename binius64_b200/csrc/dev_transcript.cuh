@@ -24,11 +24,14 @@ namespace bgpu {
 // The scalar protocol steps run on one warp, where every dependent instruction waits out its full
 // latency.  Measured on a B200, one warp: the multiply below 0.38 us (the 16 partial products
 // combined by shuffle butterflies instead: 0.45 us; nine clmul32 on one thread: 0.63 us); a
-// SHA-256 compression fully unrolled on registers 1.5 us, a compact loop 2.2 us.  A Fiat-Shamir
-// step of its own launch (two compressions, two multiplies) costs 7.3 us with the unrolled
-// compression against 8.5 us with the compact one, so the one-shot finish launches use the
-// unrolled form (DevTr); the tail loops, whose warp 0 alternates between a step and the round's
-// folds, ran slower with it and keep the compact loop (DevTrLoop).
+// SHA-256 compression fully unrolled on registers 1.5 us, a compact loop (four- or sixteen-round
+// body, round constants loaded) 2.2 us.  A Fiat-Shamir step of its own launch (two compressions,
+// two multiplies) costs 7.3 us with the unrolled compression against 8.5 us with the loop, so the
+// transcript uses the unrolled one everywhere; the tail loops, whose warp 0 alternates between a
+// step and the round's folds, also keep their folds on the out-of-line multiply (gf_mul_nl) so
+// that the loop's code stays within the instruction cache (measured: the three tails with inlined
+// folds and the unrolled compression took 120 us longer per 2^20 proof than with the compact loop;
+// with out-of-line folds the unrolled compression is ~30 us faster than the loop).
 __device__ __forceinline__ uint4 gf_mul_1t(uint4 a, uint4 b) { return gf_mul_nl(a, b); }
 
 // A product on the critical path of a Fiat-Shamir step, computed by a whole warp: every lane
@@ -69,10 +72,6 @@ static __device__ __noinline__ void sha256_compress_1t(uint32_t* st, const uint3
   for (int i = 0; i < 8; i++) st[i] = s[i];
 }
 
-// Which compression a DevTrT runs: kUnrolled in the one-shot Fiat-Shamir launches, kCompact in the
-// tail loops (see sha256_compress_compact).
-enum class ShaForm { kUnrolled, kCompact };
-
 // The challenger held by the warp that advances it.  The partial SHA-256 block is kept as 16
 // big-endian words, the sample buffer as 8 little-endian words; absorbing a word is one store at
 // a run-time index (the arrays live in local memory, which the out-of-line compression copies to
@@ -80,8 +79,7 @@ enum class ShaForm { kUnrolled, kCompact };
 // absorbed in 4-byte pieces (every message of the protocol is a whole number of words); a piece
 // may start at any byte offset.  Words at or past `len` hold no meaning except that a partially
 // filled word is zero past its bytes.
-template <ShaForm kForm>
-struct DevTrT {
+struct DevTr {
   uint32_t h[8], w[16], len;  // chaining value, partial block, bytes in it
   uint64_t total;             // bytes absorbed since the last reset
   uint32_t sampling, index;   // mode and bytes of buf consumed
@@ -89,10 +87,7 @@ struct DevTrT {
   uint32_t tape_len, tape_cap, error;
 
   static __device__ __forceinline__ void compress(uint32_t* st, const uint32_t* blk) {
-    if (kForm == ShaForm::kUnrolled)
-      sha256_compress_1t(st, blk);
-    else
-      sha256_compress_compact(st, blk);
+    sha256_compress_1t(st, blk);
   }
 
   __device__ __forceinline__ void load(const TranscriptState* g) {
@@ -260,9 +255,6 @@ struct DevTrT {
     return bits >= 32 ? v : v & ((1u << bits) - 1);
   }
 };
-
-using DevTr = DevTrT<ShaForm::kUnrolled>;
-using DevTrLoop = DevTrT<ShaForm::kCompact>;
 
 // r's byte table for gf_mul_table, built by the calling block (any size) from r.
 __device__ __forceinline__ void dt_build_mul_table(uint4 r, uint4* __restrict__ tab) {

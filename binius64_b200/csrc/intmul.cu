@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(kImTailThreads)
   pdl_wait();
   pdl_trigger();
   __shared__ uint4 r_sh;
-  DevTrLoop st;
+  DevTr st;
   uint4 G = gf_zero(), pf = gf_zero();
   {
     uint4 v[1] = {gf_zero()};

@@ -71,56 +71,6 @@ __device__ __forceinline__ void sha256_compress(uint32_t s[8], uint32_t w[16]) {
   s[7] += h;
 }
 
-// The same compression as one small out-of-line copy (a four-round body run 16 times), for the
-// device transcript's single-warp steps inside the sumcheck tail loops: there one warp alternates
-// between the compression and the rest of the round's code, and the fully unrolled form (30 KiB
-// of instructions) measured slower than this 2 KiB loop.
-static __device__ __noinline__ void sha256_compress_compact(uint32_t* st, const uint32_t* blk) {
-  // win[0..16) = W[t .. t + 16) for the round t about to run; each pass extends the schedule by
-  // four words (win[16..20)), runs rounds t .. t + 3 and slides the window, so every index is
-  // static while the body stays four rounds long.
-  uint32_t win[20];
-#pragma unroll
-  for (int i = 0; i < 16; i++) win[i] = blk[i];
-  uint32_t a = st[0], b = st[1], c = st[2], d = st[3], e = st[4], f = st[5], g = st[6], h = st[7];
-#pragma unroll 1
-  for (int t = 0; t < 64; t += 4) {
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const uint32_t w15 = win[j + 1], w2 = win[j + 14];
-      const uint32_t s0 = rotr32(w15, 7) ^ rotr32(w15, 18) ^ (w15 >> 3);
-      const uint32_t s1 = rotr32(w2, 17) ^ rotr32(w2, 19) ^ (w2 >> 10);
-      win[16 + j] = win[j] + s0 + win[j + 9] + s1;
-    }
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const uint32_t S1 = rotr32(e, 6) ^ rotr32(e, 11) ^ rotr32(e, 25);
-      const uint32_t ch = (e & f) ^ (~e & g);
-      const uint32_t t1 = h + S1 + ch + kSha256K[t + j] + win[j];
-      const uint32_t S0 = rotr32(a, 2) ^ rotr32(a, 13) ^ rotr32(a, 22);
-      const uint32_t mj = (a & b) ^ (a & c) ^ (b & c);
-      h = g;
-      g = f;
-      f = e;
-      e = d + t1;
-      d = c;
-      c = b;
-      b = a;
-      a = t1 + S0 + mj;
-    }
-#pragma unroll
-    for (int i = 0; i < 16; i++) win[i] = win[i + 4];
-  }
-  st[0] += a;
-  st[1] += b;
-  st[2] += c;
-  st[3] += d;
-  st[4] += e;
-  st[5] += f;
-  st[6] += g;
-  st[7] += h;
-}
-
 __device__ __forceinline__ void sha256_init(uint32_t s[8]) {
   s[0] = 0x6a09e667u;
   s[1] = 0xbb67ae85u;

@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(kShiftTailThreads)
   pdl_wait();
   pdl_trigger();
   __shared__ uint4 r_sh;
-  DevTrLoop st;
+  DevTr st;
   uint4 sum = gf_zero(), inout = gf_zero(), eqp = gf_zero();
   if (threadIdx.x < 32) {
     st.load(ts);
@@ -447,8 +447,8 @@ __global__ void __launch_bounds__(kShiftTailThreads)
     const uint64_t h = 1ull << n_rem, half = h >> 1;
     for (uint64_t j = threadIdx.x; j < h; j += blockDim.x) {
       const uint4 w0 = W[j], m0 = M[j];
-      W[j] = gf_add(w0, gf_mul(r, gf_add(W[h + j], w0)));
-      M[j] = gf_add(m0, gf_mul(r, gf_add(M[h + j], m0)));
+      W[j] = gf_add(w0, gf_mul_nl(r, gf_add(W[h + j], w0)));
+      M[j] = gf_add(m0, gf_mul_nl(r, gf_add(M[h + j], m0)));
     }
     const bool early = p < n_rem;
     if (k > 0 && n_rem < p)
@@ -458,14 +458,14 @@ __global__ void __launch_bounds__(kShiftTailThreads)
     uint4 v[4] = {gf_zero(), gf_zero(), gf_zero(), gf_zero()};
     for (uint64_t j = threadIdx.x; j < half; j += blockDim.x) {
       const uint4 w0 = W[j], w1 = W[half + j], m0 = M[j], m1 = M[half + j];
-      gf_add_into(v[0], gf_mul(w1, m1));
-      gf_add_into(v[1], gf_mul(gf_add(w0, w1), gf_add(m0, m1)));
+      gf_add_into(v[0], gf_mul_nl(w1, m1));
+      gf_add_into(v[1], gf_mul_nl(gf_add(w0, w1), gf_add(m0, m1)));
     }
     const uint64_t E = early ? 1ull << (p - 1) : half;
     for (uint64_t i = threadIdx.x; i < E; i += blockDim.x) {
       const uint4 e = eq_pub[i];
-      gf_add_into(v[2], gf_mul(W[half + i], e));
-      if (early) gf_add_into(v[3], gf_mul(W[half + E + i], e));
+      gf_add_into(v[2], gf_mul_nl(W[half + i], e));
+      if (early) gf_add_into(v[3], gf_mul_nl(W[half + E + i], e));
     }
     block_xor_sum<4>(v);
     if (threadIdx.x < 32) {

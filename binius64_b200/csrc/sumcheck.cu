@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(kTailThreads)
   pdl_wait();
   pdl_trigger();
   __shared__ uint4 r_sh;
-  DevTrLoop st;
+  DevTr st;
   uint4 cl = gf_zero();
   if (threadIdx.x < 32) {
     st.load(ts);
@@ -288,8 +288,8 @@ __global__ void __launch_bounds__(kTailThreads)
       const uint64_t h = len >> 1;
       for (uint64_t j = threadIdx.x; j < h; j += blockDim.x) {
         const uint4 a0 = a[j], b0 = b[j];
-        a[j] = gf_add(a0, gf_mul(r, gf_add(a[h + j], a0)));
-        b[j] = gf_add(b0, gf_mul(r, gf_add(b[h + j], b0)));
+        a[j] = gf_add(a0, gf_mul_nl(r, gf_add(a[h + j], a0)));
+        b[j] = gf_add(b0, gf_mul_nl(r, gf_add(b[h + j], b0)));
       }
       len = h;
       __syncthreads();
@@ -298,8 +298,8 @@ __global__ void __launch_bounds__(kTailThreads)
     uint4 v[2] = {gf_zero(), gf_zero()};
     for (uint64_t j = threadIdx.x; j < h; j += blockDim.x) {
       const uint4 a0 = a[j], a1 = a[h + j], b0 = b[j], b1 = b[h + j];
-      gf_add_into(v[0], gf_mul(a1, b1));
-      gf_add_into(v[1], gf_mul(gf_add(a0, a1), gf_add(b0, b1)));
+      gf_add_into(v[0], gf_mul_nl(a1, b1));
+      gf_add_into(v[1], gf_mul_nl(gf_add(a0, a1), gf_add(b0, b1)));
     }
     block_xor_sum<2>(v);
     if (threadIdx.x < 32) {
