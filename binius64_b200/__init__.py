@@ -738,6 +738,8 @@ class Prover:
     """Prover::setup + Prover::prove (prover/prover/src/prove.rs:95-303) over a device constraint
     system, with the parameters Verifier::setup chooses (verifier/verifier/src/verify.rs:61-108)."""
 
+    _proof_buf = None  # prove_host's output buffer, kept between calls
+
     def __init__(self, cs: DeviceConstraintSystem, log_inv_rate: int = 1,
                  key_collection: bytes | None = None, merkle_hash: str = "sha256"):
         self.cs = cs  # the native prover keeps a reference
@@ -766,17 +768,20 @@ class Prover:
         binius_prove: the witness is copied in and the finalized proof bytes come back."""
         w = np.ascontiguousarray(words, dtype=np.uint64)
         n = ctypes.c_size_t(0)
-        cap = 1 << 20
         t = transcript.handle if transcript is not None else None
         while True:
-            buf = (ctypes.c_uint8 * cap)()
+            # the proof buffer is kept by the prover (sized by the largest proof so far)
+            buf = self._proof_buf
+            if buf is None:
+                buf = self._proof_buf = (ctypes.c_uint8 * (1 << 20))()
+            cap = len(buf)
             rc = lib().binius_prove(self._h, w.ctypes.data, len(w), t, buf, cap, ctypes.byref(n),
                                     _stream(stream))
             if rc == 1 and n.value > cap and t is None:  # too small: prove again with room
-                cap = n.value
+                self._proof_buf = (ctypes.c_uint8 * n.value)()
                 continue
             check(rc)
-            return bytes(buf)[: n.value]
+            return ctypes.string_at(buf, n.value)
 
     def prove(self, witness_words, transcript: ProverTranscript | None = None,
               stream=None) -> ProverTranscript:
