@@ -107,6 +107,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true",
                     help="prove workload: skip the batched-queue summary (profiling runs)")
+    ap.add_argument("--tuning", default="",
+                    help="launch shapes to set instead of autotuning, e.g. "
+                         "'tail_log=10,ntt_tile_bits=10' (implies --no-autotune)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="prove workload: time the default launch shapes")
     ap.add_argument("--no-matrix", action="store_true",
@@ -527,7 +530,12 @@ def run_prove(args, rank, world, local):
     # the autotuner picks this statement shape's launch shapes (tail size, NTT layers per pass,
     # Merkle fusion; the proof bytes are unchanged) before anything is timed
     tuning = None
-    if not args.no_autotune:
+    if args.tuning:
+        prover.set_tuning(**{k: int(v) for k, v in
+                             (kv.split("=") for kv in args.tuning.split(",") if kv)})
+        tuning = prover.tuning()
+        assert prover.prove(w).finalize() == proof, "proof differs under the given launch shapes"
+    elif not args.no_autotune:
         t_at = time.perf_counter()
         tuning = prover.autotune(w, reps=3)
         tuning["autotune_s"] = time.perf_counter() - t_at
