@@ -478,6 +478,111 @@ __global__ void __launch_bounds__(kImTailThreads)
   if (threadIdx.x == 0) st.store(ts);
 }
 
+// The small last rounds of the leaf batch (IntMulDevice phase 5) in one CTA, from round t0 on,
+// with intmul_layer_tail_kernel's single-group step per group: claims 0..96 are the bivariate
+// leaf pairs and 97 the linear c_lo_0 column, all on eq point 0 (eq_base); claims 98..161 are
+// the 64 linear b columns on eq point 1 (eq2_base).  Per round every multilinear folds 2L -> L
+// by the previous challenge and the group sums Y1_0, Yinf_0, Y1_1 (beta^claim and eq weighted)
+// feed the step; deg-1 claims have no y_inf.  Items are (multilinear group m, index i) with the
+// index fastest: m < 97 a leaf pair, m = 97 the c_lo_0 column, m > 97 b column m - 98.
+constexpr uint32_t kLeafPairs = 97, kLeafCols = 64;
+__global__ void __launch_bounds__(kImTailThreads)
+    intmul_leaf_tail_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
+                            uint4* __restrict__ leaves, uint4* __restrict__ lo0,
+                            uint4* __restrict__ bcols, uint64_t stride, uint32_t n, uint32_t t0,
+                            const uint4* __restrict__ eq_base, const uint4* __restrict__ eq2_base,
+                            const uint4* __restrict__ sums, const uint4* __restrict__ prefix,
+                            const ImAlpha* __restrict__ alphas,
+                            const uint4* __restrict__ beta_pow, uint4* __restrict__ chal) {
+  pdl_wait();
+  pdl_trigger();
+  constexpr uint32_t kClaims0 = kLeafPairs + 1, kClaims = kClaims0 + kLeafCols;
+  __shared__ uint4 r_sh;
+  DevTr st;
+  uint4 G[2] = {gf_zero(), gf_zero()}, pf[2] = {gf_zero(), gf_zero()};
+  {
+    uint4 v[2] = {gf_zero(), gf_zero()};
+    for (uint32_t i = threadIdx.x; i < kClaims; i += blockDim.x)
+      gf_add_into(v[i < kClaims0 ? 0 : 1], gf_mul_nl(beta_pow[i], sums[i]));
+    block_xor_sum<2>(v);
+    if (threadIdx.x < 32) {
+      G[0] = v[0];
+      G[1] = v[1];
+      pf[0] = prefix[0];
+      pf[1] = prefix[1];
+      st.load(ts);
+      if (t0 > 0) r_sh = chal[t0 - 1];
+    }
+    __syncthreads();
+  }
+  auto fold2 = [](uint4* col, uint64_t i, uint64_t L, uint64_t h, uint4 r, bool fold,
+                  uint4& x0, uint4& x1) {
+    x0 = col[i];
+    x1 = col[h + i];
+    if (fold) {
+      x0 = gf_add(x0, gf_mul_nl(r, gf_add(col[L + i], x0)));
+      x1 = gf_add(x1, gf_mul_nl(r, gf_add(col[L + h + i], x1)));
+      col[i] = x0;
+      col[h + i] = x1;
+    }
+  };
+  for (uint32_t t = t0; t < n; t++) {
+    const bool fold = t > 0;
+    const uint4 r = r_sh;
+    const uint64_t L = 1ull << (n - t), h = L >> 1;
+    const uint64_t lvl = (1ull << (n - t - 1)) - 1;
+    uint4 v[3] = {gf_zero(), gf_zero(), gf_zero()};  // Y1_0, Yinf_0, Y1_1
+    for (uint64_t it = threadIdx.x; it < (uint64_t)kClaims * h; it += blockDim.x) {
+      const uint32_t m = (uint32_t)(it / h);
+      const uint64_t i = it - (uint64_t)m * h;
+      if (m < kLeafPairs) {
+        uint4 a0, a1, b0, b1;
+        fold2(leaves + 2 * (uint64_t)m * stride, i, L, h, r, fold, a0, a1);
+        fold2(leaves + (2 * (uint64_t)m + 1) * stride, i, L, h, r, fold, b0, b1);
+        const uint4 w = gf_mul_nl(eq_base[lvl + i], beta_pow[m]);
+        gf_add_into(v[0], gf_mul_nl(w, gf_mul_nl(a1, b1)));
+        gf_add_into(v[1], gf_mul_nl(w, gf_mul_nl(gf_add(a0, a1), gf_add(b0, b1))));
+      } else {
+        const bool g0 = m == kLeafPairs;
+        uint4* col = g0 ? lo0 : bcols + (uint64_t)(m - kClaims0) * stride;
+        uint4 c0, c1;
+        fold2(col, i, L, h, r, fold, c0, c1);
+        const uint4 w = gf_mul_nl(g0 ? eq_base[lvl + i] : eq2_base[lvl + i], beta_pow[m]);
+        gf_add_into(v[g0 ? 0 : 2], gf_mul_nl(w, c1));
+      }
+    }
+    block_xor_sum<3>(v);
+    if (threadIdx.x < 32) {
+      uint4 m3[3] = {gf_zero(), gf_zero(), gf_zero()};
+      uint4 T[2][3];
+      for (int g = 0; g < 2; g++) {
+        const ImAlpha al = alphas[2 * t + g];
+        const uint4 y1 = g == 0 ? v[0] : v[2], yinf = g == 0 ? v[1] : gf_zero();
+        T[g][0] = gf_mul_warp(gf_add(G[g], gf_mul_warp(al.alpha, y1)), al.inv_one_plus_alpha);
+        T[g][1] = gf_add(gf_add(y1, T[g][0]), yinf);
+        T[g][2] = yinf;
+        uint4 oma = al.alpha;
+        oma.x ^= 1u;
+        gf_add_into(m3[0], gf_mul_warp(pf[g], gf_mul_warp(oma, T[g][0])));
+        gf_add_into(m3[1], gf_mul_warp(pf[g], gf_add(gf_mul_warp(oma, T[g][1]), T[g][0])));
+        gf_add_into(m3[2], gf_mul_warp(pf[g], gf_add(gf_mul_warp(oma, T[g][2]), T[g][1])));
+      }
+      st.message_elems(tape, m3, 3);
+      const uint4 rr = st.sample_elem();
+      chal[t] = rr;
+      for (int g = 0; g < 2; g++) {
+        G[g] = gf_add(T[g][0], gf_mul_warp(rr, gf_add(T[g][1], gf_mul_warp(rr, T[g][2]))));
+        uint4 f = gf_add(rr, alphas[2 * t + g].alpha);
+        f.x ^= 1u;
+        pf[g] = gf_mul_warp(pf[g], f);
+      }
+      r_sh = rr;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) st.store(ts);
+}
+
 // ---------------------------------------------------------------- host side
 
 uint4 u4(hu128 v) {
@@ -1019,7 +1124,11 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
     constexpr uint32_t kSlots = 2 * 97 + 1 + 64;
     DevBatch b;
     if (int rc = batch_begin(b, cl, {&pt, &p3}, sums, beta, kSlots)) return rc;
-    for (uint32_t t = 0; t < n_; t++) {
+    // rounds of at most tail_items() (multilinear group, position) items: intmul_leaf_tail_kernel
+    uint32_t t0 = 0;
+    while (t0 < n_ && ((uint64_t)(kLeafPairs + 1 + kLeafCols) << (n_ - t0 - 1)) > tail_items())
+      t0++;
+    for (uint32_t t = 0; t < t0; t++) {
       const uint64_t L = 1ull << (n_ - t);
       uint32_t* out = batch_slots(b, t);
       const uint4* rp = batch_r(b, t);
@@ -1027,6 +1136,13 @@ int IntMulDevice::run(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
       if (int rc = lin_round(lo0, 1, L, level(eq_, n_ - t - 1), rp, out + 4 * 194)) return rc;
       if (int rc = lin_round(bcols, 64, L, level(eq2_, n_ - t - 1), rp, out + 4 * 195)) return rc;
       if (int rc = batch_round(b, t)) return rc;
+    }
+    if (t0 < n_) {
+      BGPU_CUDA(launch_pdl(intmul_leaf_tail_kernel, 1, kImTailThreads, 0, s_, b.dt.state(),
+                           b.dt.tape(), leaves, lo0, bcols, N_, n_, t0, (const uint4*)eq_,
+                           (const uint4*)eq2_, (const uint4*)b.sums, (const uint4*)b.prefix,
+                           (const ImAlpha*)b.alphas, (const uint4*)b.beta, b.chal));
+      if (int rc = check("intmul_leaf_tail_kernel")) return rc;
     }
     std::vector<hu128> ch, last_leaves(2 * 194), last_lo(2), last_b(2 * 64);
     StagedReads rd(s_);
