@@ -13,6 +13,7 @@
 #include <mutex>
 
 #include "gf128.cuh"
+#include "gf_reduce.cuh"
 #include "internal.h"
 #include "kernels.h"
 
@@ -104,42 +105,54 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// The same fold with compact code for launches of less than one wave: a kernel whose threads
-// each run it once fetches its instructions cold, so the unrolled variant's ~30 inlined
-// multiplies cost more in instruction fetch than in arithmetic.  Here the rounds and butterflies
-// are loops and the multiply is one out-of-line copy (gf_mul_nl).
+// The same fold for launches of less than one wave, where one thread per chunk leaves the SMs
+// nearly empty and each thread's 2 (2^N - 1) dependent multiplies are the launch's latency.  Here
+// a chunk takes P = 2^(N-1) consecutive lanes: in a round of 2^size values, lane q < 2^(size-1)
+// holds values 2q and 2q + 1, runs butterfly q and keeps its output, which lanes 2q' and 2q' + 1
+// hand to lane q' by shuffles for the next round.  The chain is N rounds of two multiplies.
 template <int N>
 __global__ void __launch_bounds__(256)
-    fold_codeword_compact_kernel(const uint4* __restrict__ cw, uint32_t log_len,
-                                 const uint4* __restrict__ tw, Challenges ch,
-                                 const uint4* __restrict__ dch, uint4* __restrict__ out) {
-  constexpr uint32_t n = N;
-  const uint64_t n_chunks = 1ull << (log_len - n);
-  for (uint64_t ci = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; ci < n_chunks;
-       ci += (uint64_t)gridDim.x * blockDim.x) {
-    uint4 v[1 << N];
-#pragma unroll 1
-    for (uint32_t j = 0; j < (1u << n); j++) v[j] = __ldg(cw + (ci << n) + j);
+    fold_codeword_lanes_kernel(const uint4* __restrict__ cw, uint32_t log_len,
+                               const uint4* __restrict__ tw, Challenges ch,
+                               const uint4* __restrict__ dch, uint4* __restrict__ out) {
+  constexpr uint32_t P = 1u << (N - 1);
+  const uint64_t n_chunks = 1ull << (log_len - N);
+  const uint32_t q = threadIdx.x & (P - 1);
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x / P;
+  // every lane of a warp runs the same number of iterations (blockDim.x is a multiple of 32)
+  const uint64_t first = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / P;
+  const uint64_t warp_first = (blockIdx.x * (uint64_t)blockDim.x + (threadIdx.x & ~31u)) / P;
+  for (uint64_t base = warp_first; base < n_chunks; base += stride) {
+    const uint64_t ci = base + (first - warp_first);
+    const bool live = ci < n_chunks;
+    uint4 u = gf_zero(), w = gf_zero();
+    if (live) {
+      u = __ldg(cw + (ci << N) + 2 * q);
+      w = __ldg(cw + (ci << N) + 2 * q + 1);
+    }
     uint32_t cur = log_len;
-#pragma unroll 1
-    for (uint32_t kk = 0; kk < n; kk++) {
-      const uint32_t size = n - kk;
-      const uint4 r = dch ? dch[kk] : ch.r[kk];
-      const uint64_t layer_base = (1ull << (cur - 1)) - 1;
-#pragma unroll 1
-      for (uint32_t off = 0; off < (1u << (size - 1)); off++) {
-        uint4 u = v[off << 1], w = v[(off << 1) | 1];
-        const uint64_t index = (ci << (size - 1)) | (uint64_t)off;
+#pragma unroll
+    for (int kk = 0; kk < N; kk++) {
+      const int size = N - kk;
+      if (kk > 0) {  // gather this round's pair from the previous round's outputs
+        const uint32_t src = 2 * q < (1u << size) ? 2 * q : 0u;
+        const uint4 a = shfl_gf(u, src, P), b = shfl_gf(u, src + 1 < P ? src + 1 : 0u, P);
+        w = b;
+        u = a;
+      }
+      if (live && q < (1u << (size - 1))) {
+        const uint4 r = dch ? dch[kk] : ch.r[kk];
+        const uint64_t layer_base = (1ull << (cur - 1)) - 1;
+        const uint64_t index = (ci << (size - 1)) | (uint64_t)q;
         const uint4 t = __ldg(tw + layer_base + index);
         gf_add_into(w, u);
-        gf_add_into(u, gf_mul_nl(w, t));
+        gf_add_into(u, gf_mul(w, t));
         gf_add_into(w, u);
-        gf_add_into(u, gf_mul_nl(w, r));
-        v[off] = u;
+        gf_add_into(u, gf_mul(w, r));
       }
       cur--;
     }
-    out[ci] = v[0];
+    if (live && q == 0) out[ci] = u;
   }
 }
 
@@ -159,7 +172,7 @@ int load_challenges(const void* h, uint32_t n, Challenges& ch) {
 }
 
 // Launches of fewer chunks than this (under one wave of 256-thread blocks on 148 SMs) take the
-// compact kernel.
+// lane-parallel kernel.
 constexpr uint64_t kCompactFoldChunks = 148ull * 256;
 
 template <int N>
@@ -167,8 +180,8 @@ void launch_fold_codeword(const uint4* cw, uint32_t log_len, const uint4* tw, co
                           const uint4* dch, uint4* out, cudaStream_t s) {
   uint64_t n_chunks = 1ull << (log_len - N);
   if (n_chunks < kCompactFoldChunks)
-    fold_codeword_compact_kernel<N><<<grid_for(n_chunks, 256), 256, 0, s>>>(cw, log_len, tw, ch,
-                                                                            dch, out);
+    fold_codeword_lanes_kernel<N><<<grid_for(n_chunks << (N - 1), 256), 256, 0, s>>>(
+        cw, log_len, tw, ch, dch, out);
   else
     fold_codeword_kernel<N><<<grid_for(n_chunks, 256), 256, 0, s>>>(cw, log_len, tw, ch, dch, out);
 }

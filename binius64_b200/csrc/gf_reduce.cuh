@@ -11,6 +11,15 @@ __device__ __forceinline__ void atomic_xor_gf(uint32_t* dst, uint4 v) {
   if (v.w) atomicXor(dst + 3, v.w);
 }
 
+// v from lane src of the caller's width-lane segment of the (converged) warp.
+__device__ __forceinline__ uint4 shfl_gf(uint4 v, uint32_t src, int width) {
+  v.x = __shfl_sync(0xffffffffu, v.x, (int)src, width);
+  v.y = __shfl_sync(0xffffffffu, v.y, (int)src, width);
+  v.z = __shfl_sync(0xffffffffu, v.z, (int)src, width);
+  v.w = __shfl_sync(0xffffffffu, v.w, (int)src, width);
+  return v;
+}
+
 // The XOR of v over the 32 lanes of the (converged) warp, in every lane: one REDUX per word.
 __device__ __forceinline__ uint4 warp_xor_gf(uint4 v) {
   v.x = __reduce_xor_sync(0xffffffffu, v.x);
