@@ -416,6 +416,48 @@ __global__ void __launch_bounds__(256, 2)
     reduce2_atomic(s1r, sinfr, out);
 }
 
+// The small rounds of and_mle_fold_eval_kernel (no byte table) on eight lanes per position j:
+// lanes 0..5 fold column k / 2 at j (k even) or q + j (k odd) by r, lane 6 truncates eq at j,
+// the folded values and eq are shared by shuffles and lanes 0 and 1 form the two products.
+// Three dependent multiplies per lane instead of ten on one thread.
+__global__ void __launch_bounds__(256)
+    and_mle_fold_eval_lanes_kernel(uint4* __restrict__ fa, uint4* __restrict__ fb,
+                                   uint4* __restrict__ fc, uint4* __restrict__ eq, uint64_t size,
+                                   const uint4* __restrict__ r_ptr, uint32_t* __restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
+  const uint64_t h = size >> 1, q = size >> 2;
+  const uint4 r = *r_ptr;
+  const uint32_t k = threadIdx.x & 7;
+  uint4 s1 = gf_zero(), sinf = gf_zero();
+  const uint64_t all = (uint64_t)gridDim.x * blockDim.x;
+  // warp-uniform sweeps: every lane of a warp runs the same iterations (shuffles below)
+  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + (threadIdx.x & ~31u); base < 8 * q;
+       base += all) {
+    const uint64_t j = (base + (threadIdx.x & 31)) >> 3;
+    const bool live = j < q;
+    uint4 f = gf_zero();
+    if (live && k < 6) {
+      uint4* col = k < 2 ? fa : k < 4 ? fb : fc;
+      const uint64_t pos = j + ((k & 1) ? q : 0);
+      const uint4 lo = col[pos];
+      f = gf_add(lo, gf_mul_nl(r, gf_add(col[h + pos], lo)));
+      col[pos] = f;
+    } else if (live && k == 6) {
+      f = gf_add(eq[j], eq[q + j]);
+      eq[j] = f;
+    }
+    // (qualified: this file's own shfl_gf is the xor-butterfly one)
+    const uint4 a0 = bgpu::shfl_gf(f, 0, 8), a1 = bgpu::shfl_gf(f, 1, 8);
+    const uint4 b0 = bgpu::shfl_gf(f, 2, 8), b1 = bgpu::shfl_gf(f, 3, 8);
+    const uint4 c1 = bgpu::shfl_gf(f, 5, 8), e = bgpu::shfl_gf(f, 6, 8);
+    if (live && k == 0) gf_add_into(s1, gf_mul_nl(e, gf_add(gf_mul_nl(a1, b1), c1)));
+    if (live && k == 1)
+      gf_add_into(sinf, gf_mul_nl(e, gf_mul_nl(gf_add(a0, a1), gf_add(b0, b1))));
+  }
+  reduce2_atomic(s1, sinf, out);
+}
+
 // Per-round constants of the MLE-check: the eq coordinate alpha the round binds and
 // 1 / (1 + alpha), both known before the loop starts.
 struct AndRoundConst {
@@ -735,8 +777,8 @@ int and_reduction_finish(const binius_cs* cs, AndPrep& p, Transcript& t, AndResu
         e = launch_pdl(and_mle_fold_eval_kernel<true>, grid_for(size / 2, 256), 256, 0, s, fa, fb,
                        fc, eq, size * 2, d_chal + k - 1, mul_tab, acc);
       } else {
-        e = launch_pdl(and_mle_fold_eval_kernel<false>, grid_for(size / 2, 256), 256, 0, s, fa, fb,
-                       fc, eq, size * 2, d_chal + k - 1, (const uint4*)nullptr, acc);
+        e = launch_pdl(and_mle_fold_eval_lanes_kernel, grid_for(4 * size, 256), 256, 0, s, fa,
+                       fb, fc, eq, size * 2, (const uint4*)(d_chal + k - 1), acc);
       }
       if (e != cudaSuccess) { rc = cuda_error(e, "AND MLE-check round"); break; }
       // the next round folds by this round's challenge through a table when it is large

@@ -220,6 +220,43 @@ __global__ void __launch_bounds__(kThreads)
   block_xor_reduce<2>(v, out);
 }
 
+// The small rounds of bivariate_fold_eval_kernel (no byte table) on four lanes per position j:
+// lane k folds one of a[j], a[q + j], b[j], b[q + j] by r, the four folded values are shared by
+// shuffles, and lanes 0 and 1 form the two products.  One multiply then one product per lane,
+// where one thread per position ran six dependent out-of-line multiplies: these rounds are
+// latency chains on few CTAs.
+__global__ void __launch_bounds__(kThreads)
+    bivariate_fold_eval_lanes_kernel(uint4* __restrict__ a, uint4* __restrict__ b, uint64_t size,
+                                     uint4 r_arg, const uint4* __restrict__ r_ptr,
+                                     uint32_t* __restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
+  const uint64_t h = size >> 1, q = size >> 2;
+  const uint4 r = r_ptr ? *r_ptr : r_arg;
+  const uint32_t k = threadIdx.x & 3;
+  uint4 v[2] = {gf_zero(), gf_zero()};
+  const uint64_t all = (uint64_t)gridDim.x * blockDim.x;
+  // warp-uniform sweeps: every lane of a warp runs the same iterations (shuffles below)
+  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + (threadIdx.x & ~31u); base < 4 * q;
+       base += all) {
+    const uint64_t j = (base + (threadIdx.x & 31)) >> 2;
+    const bool live = j < q;
+    uint4 f = gf_zero();
+    if (live) {
+      uint4* col = k < 2 ? a : b;
+      const uint64_t pos = j + ((k & 1) ? q : 0);
+      const uint4 lo = col[pos];
+      f = gf_add(lo, gf_mul_nl(r, gf_add(col[h + pos], lo)));
+      col[pos] = f;
+    }
+    const uint4 fa0 = shfl_gf(f, 0, 4), fa1 = shfl_gf(f, 1, 4), fb0 = shfl_gf(f, 2, 4),
+                fb1 = shfl_gf(f, 3, 4);
+    if (live && k == 0) gf_add_into(v[0], gf_mul_nl(fa1, fb1));
+    if (live && k == 1) gf_add_into(v[1], gf_mul_nl(gf_add(fa0, fa1), gf_add(fb0, fb1)));
+  }
+  block_xor_reduce<2>(v, out);
+}
+
 // The Fiat-Shamir step of a plain bivariate product round (BivariateProductSumcheckProver,
 // bivariate_product.rs:43-95, through the prover's round-proof truncation) on the device: the
 // sums (y_1, y_inf) and the claim give c_0 = claim + y_1, c_2 = y_inf, c_1 = y_1 + c_0 + c_2; the
@@ -441,9 +478,9 @@ int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[1
     dev_free(tab, s);
     return rc;
   }
-  bivariate_fold_eval_kernel<false><<<grid, kThreads, 0, s>>>(d_a, d_b, size, rv, nullptr, nullptr,
-                                                              d_out8);
-  BGPU_LAUNCH_CHECK("bivariate_fold_eval_kernel");
+  bivariate_fold_eval_lanes_kernel<<<grid_for(size, kThreads), kThreads, 0, s>>>(
+      d_a, d_b, size, rv, nullptr, d_out8);
+  BGPU_LAUNCH_CHECK("bivariate_fold_eval_lanes_kernel");
   count_launch();
   return BINIUS_OK;
 }
@@ -458,8 +495,8 @@ int bivariate_fold_eval_dev(uint4* d_a, uint4* d_b, uint64_t size, const uint4* 
     e = launch_pdl(bivariate_fold_eval_kernel<true>, grid, kThreads, 0, s, d_a, d_b, size,
                    gf_zero_host(), (const uint4*)nullptr, d_tab, d_out8);
   } else {
-    e = launch_pdl(bivariate_fold_eval_kernel<false>, grid, kThreads, 0, s, d_a, d_b, size,
-                   gf_zero_host(), d_r, (const uint4*)nullptr, d_out8);
+    e = launch_pdl(bivariate_fold_eval_lanes_kernel, grid_for(size, kThreads), kThreads, 0, s,
+                   d_a, d_b, size, gf_zero_host(), d_r, d_out8);
   }
   if (e != cudaSuccess) return cuda_error(e, "bivariate_fold_eval_kernel");
   count_launch();
