@@ -165,6 +165,48 @@ __global__ void __launch_bounds__(kT)
   block_xor_reduce<2>(v, out + 8 * p);
 }
 
+// The small rounds of biv_round_kernel (L <= kSmallRound) on four lanes per position i: lane k
+// folds a or b (k < 2) at i or L/2 + i (k odd), the folded values meet by shuffles and lanes 0
+// and 1 form the two eq-weighted products: three dependent multiplies per lane instead of eight
+// on one thread.  Grid: (chunks of four-lane groups, pairs).
+__global__ void __launch_bounds__(kT)
+    biv_round_lanes_kernel(uint4* __restrict__ set, uint64_t L, uint64_t stride,
+                           const uint4* __restrict__ eq, const uint4* __restrict__ r_ptr,
+                           uint32_t* __restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
+  const bool fold = r_ptr != nullptr;
+  const uint4 r = fold ? *r_ptr : gf_zero();
+  const uint32_t p = blockIdx.y, k = threadIdx.x & 3;
+  uint4* a = set + 2 * p * stride;
+  uint4* b = a + stride;
+  const uint64_t h = L >> 1;
+  uint4 v[2] = {gf_zero(), gf_zero()};
+  const uint64_t all = (uint64_t)gridDim.x * blockDim.x;
+  // warp-uniform sweeps: every lane of a warp runs the same iterations (shuffles below)
+  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + (threadIdx.x & ~31u); base < 4 * h;
+       base += all) {
+    const uint64_t i = (base + (threadIdx.x & 31)) >> 2;
+    const bool live = i < h;
+    uint4 f = gf_zero();
+    if (live) {
+      uint4* col = k < 2 ? a : b;
+      const uint64_t pos = i + ((k & 1) ? h : 0);
+      f = col[pos];
+      if (fold) {
+        f = gf_add(f, gf_mul_nl(r, gf_add(col[L + pos], f)));
+        col[pos] = f;
+      }
+    }
+    const uint4 a0 = shfl_gf(f, 0, 4), a1 = shfl_gf(f, 1, 4), b0 = shfl_gf(f, 2, 4),
+                b1 = shfl_gf(f, 3, 4);
+    if (live && k == 0) gf_add_into(v[0], gf_mul_nl(eq[i], gf_mul_nl(a1, b1)));
+    if (live && k == 1)
+      gf_add_into(v[1], gf_mul_nl(eq[i], gf_mul_nl(gf_add(a0, a1), gf_add(b0, b1))));
+  }
+  block_xor_reduce<2>(v, out + 8 * p);
+}
+
 // Column k of `set` (current length L): out[4k..] += sum eq[i] col_k[L/2 + i], with the same
 // optional fused fold.  Grid: (chunks, columns).
 template <bool SMALL>
@@ -704,7 +746,8 @@ class IntMulDevice {
                 uint32_t* out) {
     dim3 grid(blocks_for(L / 2, 148 * 2), pairs);
     if (L <= kSmallRound)
-      BGPU_CUDA(launch_pdl(biv_round_kernel<true>, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out));
+      BGPU_CUDA(launch_pdl(biv_round_lanes_kernel, dim3(blocks_for(2 * L, 148 * 2), pairs), kT, 0,
+                           s_, set, L, N_, eq, r_ptr, out));
     else
       BGPU_CUDA(launch_pdl(biv_round_kernel<false>, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out));
     return check("biv_round_kernel");
