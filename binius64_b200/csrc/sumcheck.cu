@@ -42,40 +42,30 @@ unsigned grid_for(uint64_t n, unsigned threads, unsigned max_blocks = 148 * 8) {
 
 // out[j] = prod_i (bit_i(j) ? r_i : 1 + r_i) for n <= 16 coordinates.  Each block first builds
 // the eq tensors of the low k = min(n, 8) and the high n - k coordinates (at most 256 entries
-// each) in shared memory, then every output is one multiply lo[j mod 2^k] * hi[j >> k].  A table
-// entry multiplies its at most 8 factors as a balanced tree (depth 3, not a chain of 7) with the
-// out-of-line multiply (the inlined one made the launch's cold code 7x longer).  These
+// each) in shared memory, then every output is one multiply lo[j mod 2^k] * hi[j >> k].  The
+// tables are built by doubling (8 steps of one multiply per thread; a balanced product tree per
+// entry on one thread, its multiplies sequential calls, cost ~20 us more per 2^20 proof).  These
 // tensors are small and on the protocol's critical path, so latency matters: the tables depend
 // only on the point (a kernel argument), so under programmatic dependent launch they are built
 // while the previous kernel still runs, and only the writes wait for it.
-__device__ __forceinline__ uint4 eq_factor(const Point32& p, uint32_t c, uint32_t idx,
-                                           uint32_t bit) {
-  uint4 f = p.r[c];
-  if (!((idx >> bit) & 1)) f.x ^= 1u;
-  return f;
-}
-__device__ __forceinline__ uint4 eq_entry(const Point32& p, uint32_t first, uint32_t cnt,
-                                          uint32_t idx) {
-  uint4 f[8];
-#pragma unroll
-  for (uint32_t i = 0; i < 8; i++) f[i] = i < cnt ? eq_factor(p, first + i, idx, i) : gf_one();
-#pragma unroll
-  for (uint32_t w = 1; w < 8; w <<= 1)
-#pragma unroll
-    for (uint32_t i = 0; i < 8; i += 2 * w)
-      if (i + w < cnt) f[i] = gf_mul_nl(f[i], f[i + w]);
-  return f[0];
-}
-
 __global__ void __launch_bounds__(256)
     eq_small_kernel(uint4* __restrict__ out, Point32 p, uint32_t off, uint32_t n) {
   __shared__ uint4 s_lo[256], s_hi[256];
   const uint32_t k = n < 8 ? n : 8, m = n - k;
-  const uint32_t n_lo = 1u << k, n_hi = 1u << m;
-  for (uint32_t t = threadIdx.x; t < n_lo + n_hi; t += blockDim.x) {
-    const bool lo = t < n_lo;
-    const uint32_t idx = lo ? t : t - n_lo;
-    (lo ? s_lo : s_hi)[idx] = lo ? eq_entry(p, off, k, idx) : eq_entry(p, off + k, m, idx);
+  const uint32_t n_lo = 1u << k;
+  // threads 0..127 build the low table, 128..255 the high one, by doubling: after step i a
+  // table holds eq of its first i + 1 coordinates (entry t: factor 1 + r_i, t + 2^i: r_i)
+  const bool lo_side = threadIdx.x < 128;
+  const uint32_t t = threadIdx.x & 127, cnt = lo_side ? k : m, first = lo_side ? off : off + k;
+  uint4* tab = lo_side ? s_lo : s_hi;
+  if (t == 0) tab[0] = gf_one();
+  for (uint32_t i = 0; i < 8; i++) {
+    __syncthreads();
+    if (i < cnt && t < (1u << i)) {
+      const uint4 x = tab[t], y = gf_mul(x, p.r[first + i]);
+      tab[t + (1u << i)] = y;
+      tab[t] = gf_add(x, y);
+    }
   }
   pdl_wait();
   pdl_trigger();
