@@ -369,23 +369,19 @@ __global__ void __launch_bounds__(256)
   reduce2_atomic(reduce256(s1), reduce256(sinf), out);
 }
 
-// Fold the three columns (length size) by the previous round's challenge *r_ptr, truncate eq
-// (length size/2 -> size/4) and evaluate the next round.  Thread j owns folded positions j,
-// j + size/4 and eq position j.  With TAB the six products by r go through r's byte table
-// (gf_mul_table), which the previous round's finish kernel built.
-template <bool TAB>
+// Fold the three columns (length size) by the previous round's challenge, truncate eq (length
+// size/2 -> size/4) and evaluate the next round.  Thread j owns folded positions j, j + size/4
+// and eq position j.  The six products by r go through r's byte table (gf_mul_table), which the
+// previous round's finish kernel built; rounds below kMulTableMinSize elements, which have no
+// table, run in and_mle_fold_eval_lanes_kernel.
 __global__ void __launch_bounds__(256, 2)
     and_mle_fold_eval_kernel(uint4* __restrict__ fa, uint4* __restrict__ fb, uint4* __restrict__ fc,
-                             uint4* __restrict__ eq, uint64_t size, const uint4* __restrict__ r_ptr,
-                             const uint4* __restrict__ tab, uint32_t* __restrict__ out) {
+                             uint4* __restrict__ eq, uint64_t size, const uint4* __restrict__ tab,
+                             uint32_t* __restrict__ out) {
   pdl_wait();
   pdl_trigger();
   const uint64_t h = size >> 1, q = size >> 2;
   u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
-  uint4 s1r = gf_zero(), sinfr = gf_zero();  // small rounds: reduced sums
-  const uint4 r = TAB ? gf_zero() : *r_ptr;
-  // small rounds (no table) run on few threads once: out-of-line multiplies keep the code compact
-  auto mul_r = [&](uint4 x) { return TAB ? gf_mul_table(tab, x) : gf_mul_nl(r, x); };
   for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < q;
        j += (uint64_t)gridDim.x * blockDim.x) {
     uint4 f[3][2];
@@ -394,26 +390,17 @@ __global__ void __launch_bounds__(256, 2)
     for (int c = 0; c < 3; c++) {
       uint4* col = cols[c];
       const uint4 lo0 = col[j], hi0 = col[h + j], lo1 = col[q + j], hi1 = col[h + q + j];
-      f[c][0] = gf_add(lo0, mul_r(gf_add(hi0, lo0)));
-      f[c][1] = gf_add(lo1, mul_r(gf_add(hi1, lo1)));
+      f[c][0] = gf_add(lo0, gf_mul_table(tab, gf_add(hi0, lo0)));
+      f[c][1] = gf_add(lo1, gf_mul_table(tab, gf_add(hi1, lo1)));
       col[j] = f[c][0];
       col[q + j] = f[c][1];
     }
     const uint4 e = gf_add(eq[j], eq[q + j]);
     eq[j] = e;
-    if constexpr (TAB) {
-      xor_into(s1, clmul128(e, gf_add(gf_mul(f[0][1], f[1][1]), f[2][1])));
-      xor_into(sinf, clmul128(e, gf_mul(gf_add(f[0][0], f[0][1]), gf_add(f[1][0], f[1][1]))));
-    } else {
-      gf_add_into(s1r, gf_mul_nl(e, gf_add(gf_mul_nl(f[0][1], f[1][1]), f[2][1])));
-      gf_add_into(sinfr, gf_mul_nl(e, gf_mul_nl(gf_add(f[0][0], f[0][1]),
-                                                gf_add(f[1][0], f[1][1]))));
-    }
+    xor_into(s1, clmul128(e, gf_add(gf_mul(f[0][1], f[1][1]), f[2][1])));
+    xor_into(sinf, clmul128(e, gf_mul(gf_add(f[0][0], f[0][1]), gf_add(f[1][0], f[1][1]))));
   }
-  if constexpr (TAB)
-    reduce2_atomic(reduce256(s1), reduce256(sinf), out);
-  else
-    reduce2_atomic(s1r, sinfr, out);
+  reduce2_atomic(reduce256(s1), reduce256(sinf), out);
 }
 
 // The small rounds of and_mle_fold_eval_kernel (no byte table) on eight lanes per position j:
@@ -774,8 +761,8 @@ int and_reduction_finish(const binius_cs* cs, AndPrep& p, Transcript& t, AndResu
                                                                     acc);
         e = cudaGetLastError();
       } else if (size * 2 >= kMulTableMinSize) {
-        e = launch_pdl(and_mle_fold_eval_kernel<true>, grid_for(size / 2, 256), 256, 0, s, fa, fb,
-                       fc, eq, size * 2, d_chal + k - 1, mul_tab, acc);
+        e = launch_pdl(and_mle_fold_eval_kernel, grid_for(size / 2, 256), 256, 0, s, fa, fb, fc,
+                       eq, size * 2, (const uint4*)mul_tab, acc);
       } else {
         e = launch_pdl(and_mle_fold_eval_lanes_kernel, grid_for(4 * size, 256), 256, 0, s, fa,
                        fb, fc, eq, size * 2, (const uint4*)(d_chal + k - 1), acc);

@@ -116,8 +116,8 @@ __device__ __forceinline__ uint4 fold1(uint4 lo, uint4 hi, uint4 r) {
 // length L): out[8p..] += (sum eq[i] a1 b1, sum eq[i] (a0 + a1)(b0 + b1)) over i < L/2.  With
 // `fold`, both multilinears first shrink from 2L to L by r in place (fold_highest_var_inplace);
 // thread i owns positions i and i + L/2, so the fold and the round need one pass.  Grid: (chunks,
-// pairs).  The fold's r is *r_ptr (a challenge in HBM); r_ptr == nullptr means no fold.
-template <bool SMALL>
+// pairs).  The fold's r is *r_ptr (a challenge in HBM); r_ptr == nullptr means no fold.  Rounds of
+// at most kSmallRound elements run in biv_round_lanes_kernel.
 __global__ void __launch_bounds__(kT)
     biv_round_kernel(uint4* __restrict__ set, uint64_t L, uint64_t stride,
                      const uint4* __restrict__ eq, const uint4* __restrict__ r_ptr,
@@ -131,17 +131,14 @@ __global__ void __launch_bounds__(kT)
   uint4* b = a + stride;
   const uint64_t h = L >> 1;
   u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
-  uint4 s1r = gf_zero(), sinfr = gf_zero();
-  // small rounds run once on few threads: one out-of-line multiply keeps the code compact
-  auto mul = [](uint4 x, uint4 y) { return SMALL ? gf_mul_nl(x, y) : gf_mul(x, y); };
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < h;
        i += (uint64_t)gridDim.x * blockDim.x) {
     uint4 a0, a1, b0, b1;
     if (fold) {
-      a0 = gf_add(a[i], mul(r, gf_add(a[L + i], a[i])));
-      a1 = gf_add(a[h + i], mul(r, gf_add(a[L + h + i], a[h + i])));
-      b0 = gf_add(b[i], mul(r, gf_add(b[L + i], b[i])));
-      b1 = gf_add(b[h + i], mul(r, gf_add(b[L + h + i], b[h + i])));
+      a0 = gf_add(a[i], gf_mul(r, gf_add(a[L + i], a[i])));
+      a1 = gf_add(a[h + i], gf_mul(r, gf_add(a[L + h + i], a[h + i])));
+      b0 = gf_add(b[i], gf_mul(r, gf_add(b[L + i], b[i])));
+      b1 = gf_add(b[h + i], gf_mul(r, gf_add(b[L + h + i], b[h + i])));
       a[i] = a0;
       a[h + i] = a1;
       b[i] = b0;
@@ -153,15 +150,10 @@ __global__ void __launch_bounds__(kT)
       b1 = b[h + i];
     }
     const uint4 e = eq[i];
-    if constexpr (SMALL) {
-      gf_add_into(s1r, gf_mul_nl(e, gf_mul_nl(a1, b1)));
-      gf_add_into(sinfr, gf_mul_nl(e, gf_mul_nl(gf_add(a0, a1), gf_add(b0, b1))));
-    } else {
-      xor_into(s1, clmul128(e, gf_mul(a1, b1)));
-      xor_into(sinf, clmul128(e, gf_mul(gf_add(a0, a1), gf_add(b0, b1))));
-    }
+    xor_into(s1, clmul128(e, gf_mul(a1, b1)));
+    xor_into(sinf, clmul128(e, gf_mul(gf_add(a0, a1), gf_add(b0, b1))));
   }
-  uint4 v[2] = {SMALL ? s1r : reduce256(s1), SMALL ? sinfr : reduce256(sinf)};
+  uint4 v[2] = {reduce256(s1), reduce256(sinf)};
   block_xor_reduce<2>(v, out + 8 * p);
 }
 
@@ -749,7 +741,7 @@ class IntMulDevice {
       BGPU_CUDA(launch_pdl(biv_round_lanes_kernel, dim3(blocks_for(2 * L, 148 * 2), pairs), kT, 0,
                            s_, set, L, N_, eq, r_ptr, out));
     else
-      BGPU_CUDA(launch_pdl(biv_round_kernel<false>, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out));
+      BGPU_CUDA(launch_pdl(biv_round_kernel, grid, kT, 0, s_, set, L, N_, eq, r_ptr, out));
     return check("biv_round_kernel");
   }
   int lin_round(uint4* set, uint32_t cols, uint64_t L, const uint4* eq, const uint4* r_ptr,

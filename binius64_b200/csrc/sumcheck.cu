@@ -170,43 +170,32 @@ __global__ void __launch_bounds__(kThreads)
 
 // Folds (a, b) of length `size` by r in place (a[i] = a[i] + r (a[i + size/2] - a[i])) and
 // evaluates the next round on the folded length-size/2 arrays.  Thread j owns folded positions j
-// and j + size/4, so no two threads touch the same element.  With TAB the four products by r go
-// through the byte table of r (gf_mul_table); otherwise r is r_arg, or *r_ptr when that is set
-// (a challenge the device transcript sampled).
-template <bool TAB>
+// and j + size/4, so no two threads touch the same element.  The four products by r go through
+// the byte table of r (gf_mul_table); the rounds below kMulTableMinSize elements, which have no
+// table, run in bivariate_fold_eval_lanes_kernel.
 __global__ void __launch_bounds__(kThreads)
     bivariate_fold_eval_kernel(uint4* __restrict__ a, uint4* __restrict__ b, uint64_t size,
-                               uint4 r_arg, const uint4* __restrict__ r_ptr,
                                const uint4* __restrict__ tab, uint32_t* __restrict__ out) {
   pdl_wait();
   pdl_trigger();
   const uint64_t h = size >> 1, q = size >> 2;
   u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
-  uint4 s1r = gf_zero(), sinfr = gf_zero();  // small rounds: reduced sums
-  const uint4 r = TAB || !r_ptr ? r_arg : *r_ptr;
-  // small rounds (no table) run on few threads once: out-of-line multiplies keep the code compact
-  auto mul_r = [&](uint4 x) { return TAB ? gf_mul_table(tab, x) : gf_mul_nl(r, x); };
   for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < q;
        j += (uint64_t)gridDim.x * blockDim.x) {
-    uint4 a_lo = a[j], a_hi = a[h + j], a_lo2 = a[q + j], a_hi2 = a[h + q + j];
-    uint4 b_lo = b[j], b_hi = b[h + j], b_lo2 = b[q + j], b_hi2 = b[h + q + j];
-    uint4 fa0 = gf_add(a_lo, mul_r(gf_add(a_hi, a_lo)));
-    uint4 fa1 = gf_add(a_lo2, mul_r(gf_add(a_hi2, a_lo2)));
-    uint4 fb0 = gf_add(b_lo, mul_r(gf_add(b_hi, b_lo)));
-    uint4 fb1 = gf_add(b_lo2, mul_r(gf_add(b_hi2, b_lo2)));
+    const uint4 a_lo = a[j], a_hi = a[h + j], a_lo2 = a[q + j], a_hi2 = a[h + q + j];
+    const uint4 b_lo = b[j], b_hi = b[h + j], b_lo2 = b[q + j], b_hi2 = b[h + q + j];
+    const uint4 fa0 = gf_add(a_lo, gf_mul_table(tab, gf_add(a_hi, a_lo)));
+    const uint4 fa1 = gf_add(a_lo2, gf_mul_table(tab, gf_add(a_hi2, a_lo2)));
+    const uint4 fb0 = gf_add(b_lo, gf_mul_table(tab, gf_add(b_hi, b_lo)));
+    const uint4 fb1 = gf_add(b_lo2, gf_mul_table(tab, gf_add(b_hi2, b_lo2)));
     a[j] = fa0;
     a[q + j] = fa1;
     b[j] = fb0;
     b[q + j] = fb1;
-    if constexpr (TAB) {
-      xor_into(s1, clmul128(fa1, fb1));
-      xor_into(sinf, clmul128(gf_add(fa0, fa1), gf_add(fb0, fb1)));
-    } else {
-      gf_add_into(s1r, gf_mul_nl(fa1, fb1));
-      gf_add_into(sinfr, gf_mul_nl(gf_add(fa0, fa1), gf_add(fb0, fb1)));
-    }
+    xor_into(s1, clmul128(fa1, fb1));
+    xor_into(sinf, clmul128(gf_add(fa0, fa1), gf_add(fb0, fb1)));
   }
-  uint4 v[2] = {TAB ? reduce256(s1) : s1r, TAB ? reduce256(sinf) : sinfr};
+  uint4 v[2] = {reduce256(s1), reduce256(sinf)};
   block_xor_reduce<2>(v, out);
 }
 
@@ -459,8 +448,7 @@ int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[1
     BGPU_CUDA(dev_alloc(&tab, 16 * kMulTableEntries, s));
     int rc = build_mul_table(r, tab, s);
     if (!rc) {
-      bivariate_fold_eval_kernel<true><<<grid, kThreads, 0, s>>>(d_a, d_b, size, rv, nullptr, tab,
-                                                                 d_out8);
+      bivariate_fold_eval_kernel<<<grid, kThreads, 0, s>>>(d_a, d_b, size, tab, d_out8);
       cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) rc = cuda_error(e, "bivariate_fold_eval_kernel");
       else count_launch();
@@ -482,8 +470,8 @@ int bivariate_fold_eval_dev(uint4* d_a, uint4* d_b, uint64_t size, const uint4* 
   cudaError_t e;
   if (size >= kMulTableMinSize) {
     if (!d_tab) return set_error(BINIUS_E_ARG, "a large fold needs the challenge's table");
-    e = launch_pdl(bivariate_fold_eval_kernel<true>, grid, kThreads, 0, s, d_a, d_b, size,
-                   gf_zero_host(), (const uint4*)nullptr, d_tab, d_out8);
+    e = launch_pdl(bivariate_fold_eval_kernel, grid, kThreads, 0, s, d_a, d_b, size,
+                   (const uint4*)d_tab, d_out8);
   } else {
     e = launch_pdl(bivariate_fold_eval_lanes_kernel, grid_for(size, kThreads), kThreads, 0, s,
                    d_a, d_b, size, gf_zero_host(), d_r, d_out8);
