@@ -11,9 +11,9 @@ FRIFoldProver::execute_fold_round, prover/prover/src/fri/fold.rs:117-175):
 * later rounds fold `arity` codeword variables (fold_codeword, fold.rs:297-318).
 
 Every kernel runs through the C ABI on one stream; nothing is allocated per run.  The counters
-(`algorithmic_bytes`, `gf_mults`, `sha256_compressions`) are the per-run work of the survey's
-roofline formulas: message read, codeword written and read once by the leaf hashing, tree
-written, each fold reading its input and writing its output and tree.
+(`algorithmic_bytes`, `gf_mults`, `sha256_compressions`) are the per-run work that the roofline
+figures divide: message read, codeword written and read once by the leaf hashing, tree written,
+each fold reading its input and writing its output and tree.
 """
 from __future__ import annotations
 
