@@ -189,7 +189,19 @@ struct DevTr {
     tape_words(tape, v, n);
     if (n) {
       to_observer();
-      for (uint32_t i = 0; i < n; i++) absorb_word(v[i]);
+      if ((len & 3u) == 0) {  // word-aligned stream (every message of the protocol): inline
+        for (uint32_t i = 0; i < n; i++) {
+          w[len >> 2] = bswap32(v[i]);
+          len += 4;
+          if (len == 64) {
+            compress(h, w);
+            len = 0;
+          }
+        }
+        total += 4ull * n;
+      } else {
+        for (uint32_t i = 0; i < n; i++) absorb_word(v[i]);
+      }
     }
   }
   __device__ __forceinline__ void message_elems(uint8_t* tape, const uint4* e, uint32_t n) {
