@@ -37,7 +37,7 @@ __device__ __forceinline__ uint4 gf_mul_1t(uint4 a, uint4 b) { return gf_mul_nl(
 // A product on the critical path of a Fiat-Shamir step, computed by a whole warp: every lane
 // passes the same a and b; lane l < 16 forms the 32x32 carry-less product of word l/4 of a and
 // word l%4 of b, each of the eight words of the 256-bit product is the XOR of the partial-product
-// halves that land on it (one warp reduction, REDUX, per word), and every lane returns the
+// halves that land on it (one warp reduction, __reduce_xor_sync, per word), and every lane returns the
 // reduced product.  One out-of-line copy keeps the code of the launches that call it small.
 static __device__ __noinline__ uint4 gf_mul_warp(uint4 a, uint4 b) {
   const uint32_t lane = threadIdx.x & 31;

@@ -20,7 +20,7 @@ __device__ __forceinline__ uint4 shfl_gf(uint4 v, uint32_t src, int width) {
   return v;
 }
 
-// The XOR of v over the 32 lanes of the (converged) warp, in every lane: one REDUX per word.
+// The XOR of v over the 32 lanes of the (converged) warp, in every lane: one warp reduction (__reduce_xor_sync) per word.
 __device__ __forceinline__ uint4 warp_xor_gf(uint4 v) {
   v.x = __reduce_xor_sync(0xffffffffu, v.x);
   v.y = __reduce_xor_sync(0xffffffffu, v.y);

@@ -7,7 +7,7 @@
 // B200 mapping: one thread hashes one leaf (its 2^log_batch elements are read as 128-bit loads);
 // the CTA's 256 leaf digests stay in shared memory and the next 8 tree layers are compressed there
 // before anything but the layer outputs touches HBM.  Upper layers run in CTAs that fuse 9 layers
-// (512 inputs -> 1).  SHA-256 is pure integer work (funnel-shift rotates, LOP3, IADD3).
+// (512 inputs -> 1).  SHA-256 is pure integer work (funnel-shift rotates, three-input logic ops, adds).
 #include <string.h>
 
 #include <algorithm>
