@@ -370,40 +370,58 @@ __global__ void __launch_bounds__(256)
 }
 
 // Fold the three columns (length size) by the previous round's challenge, truncate eq (length
-// size/2 -> size/4) and evaluate the next round.  Thread j owns folded positions j, j + size/4
-// and eq position j.  The six products by r go through r's byte table (gf_mul_table), which the
-// previous round's finish kernel built; rounds below kMulTableMinSize elements, which have no
-// table, run in and_mle_fold_eval_lanes_kernel.
-__global__ void __launch_bounds__(256, 2)
+// size/2 -> size/4) and evaluate the next round.  Each folded position j < size/4 belongs to a
+// pair of adjacent lanes: the odd lane folds a, b, c at j and truncates eq there, the even lane
+// folds them at j + size/4, and each forms one of the two products (the even lane y_1's
+// e (a1 b1 + c1), the odd lane y_inf's e (a0 + a1)(b0 + b1)); shuffles bring a1, b1 to the odd
+// lane and e to the even one.  The six products by r (read from r_ptr) go through r's nibble
+// tables, which each block builds in shared memory.
+__global__ void __launch_bounds__(256)
     and_mle_fold_eval_kernel(uint4* __restrict__ fa, uint4* __restrict__ fb, uint4* __restrict__ fc,
-                             uint4* __restrict__ eq, uint64_t size, const uint4* __restrict__ tab,
+                             uint4* __restrict__ eq, uint64_t size, const uint4* __restrict__ r_ptr,
                              uint32_t* __restrict__ out) {
+  __shared__ NibbleTable tab;
+  __shared__ uint4 basis[128];
   pdl_wait();
   pdl_trigger();
+  nibble_table_build(tab, basis, *r_ptr);
   const uint64_t h = size >> 1, q = size >> 2;
-  u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
-  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < q;
-       j += (uint64_t)gridDim.x * blockDim.x) {
-    uint4 f[3][2];
-    uint4* cols[3] = {fa, fb, fc};
+  const uint32_t odd = threadIdx.x & 1;
+  u256 acc = {0, 0, 0, 0};
+  const uint64_t all = (uint64_t)gridDim.x * blockDim.x;
+  // warp-uniform sweeps: every lane of a warp runs the same iterations (shuffles below)
+  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + (threadIdx.x & ~31u); base < 2 * q;
+       base += all) {
+    const uint64_t j = (base + (threadIdx.x & 31)) >> 1;
+    const bool live = j < q;
+    uint4 f[3] = {gf_zero(), gf_zero(), gf_zero()}, e = gf_zero();
+    if (live) {
+      const uint64_t pos = odd ? j : q + j;
+      uint4* cols[3] = {fa, fb, fc};
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-      uint4* col = cols[c];
-      const uint4 lo0 = col[j], hi0 = col[h + j], lo1 = col[q + j], hi1 = col[h + q + j];
-      f[c][0] = gf_add(lo0, gf_mul_table(tab, gf_add(hi0, lo0)));
-      f[c][1] = gf_add(lo1, gf_mul_table(tab, gf_add(hi1, lo1)));
-      col[j] = f[c][0];
-      col[q + j] = f[c][1];
+      for (int c = 0; c < 3; c++) {
+        uint4* col = cols[c];
+        const uint4 lo = col[pos], hi = col[h + pos];
+        f[c] = gf_add(lo, gf_mul_nibble(tab, gf_add(hi, lo)));
+        col[pos] = f[c];
+      }
+      if (odd) {
+        e = gf_add(eq[j], eq[q + j]);
+        eq[j] = e;
+      }
     }
-    const uint4 e = gf_add(eq[j], eq[q + j]);
-    eq[j] = e;
-    xor_into(s1, clmul128(e, gf_add(gf_mul(f[0][1], f[1][1]), f[2][1])));
-    xor_into(sinf, clmul128(e, gf_mul(gf_add(f[0][0], f[0][1]), gf_add(f[1][0], f[1][1]))));
+    // (qualified: this file's own shfl_gf is the xor-butterfly one)
+    const uint4 pa = bgpu::shfl_gf(f[0], 0, 2), pb = bgpu::shfl_gf(f[1], 0, 2);
+    e = bgpu::shfl_gf(e, 1, 2);
+    // one product chain per lane, selected without divergence (zero on dead lanes)
+    const uint4 x = odd ? gf_add(f[0], pa) : f[0], y = odd ? gf_add(f[1], pb) : f[1];
+    xor_into(acc, clmul128(e, gf_add(gf_mul(x, y), odd ? gf_zero() : f[2])));
   }
-  reduce2_atomic(reduce256(s1), reduce256(sinf), out);
+  const uint4 v = reduce256(acc);
+  reduce2_atomic(odd ? gf_zero() : v, odd ? v : gf_zero(), out);
 }
 
-// The small rounds of and_mle_fold_eval_kernel (no byte table) on eight lanes per position j:
+// The small rounds of and_mle_fold_eval_kernel (no nibble tables) on eight lanes per position j:
 // lanes 0..5 fold column k / 2 at j (k even) or q + j (k odd) by r, lane 6 truncates eq at j,
 // the folded values and eq are shared by shuffles and lanes 0 and 1 form the two products.
 // Three dependent multiplies per lane instead of ten on one thread.
@@ -454,17 +472,14 @@ struct AndRoundConst {
 // The Fiat-Shamir step of one MLE-check round, on the device: the round's sums (y_1, y_inf) ->
 // the round polynomial by RoundEvals2::interpolate_eq (prover/prover/src/protocols/sumcheck/
 // round_evals.rs:80-86) -> the truncated proof (c_1, c_2) (mlecheck::RoundProof::truncate) ->
-// the challenge r -> the next claim c_0 + c_1 r + c_2 r^2.  Warp 0 runs the chain; with a
-// table pointer the whole block then builds r's byte table for the next fold.
-__global__ void __launch_bounds__(256)
+// the challenge r -> the next claim c_0 + c_1 r + c_2 r^2.  One warp runs the chain.
+__global__ void __launch_bounds__(32)
     and_round_finish_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
                             const uint4* __restrict__ ys, const AndRoundConst* __restrict__ rc,
-                            uint4* __restrict__ claim, uint4* __restrict__ r_out,
-                            uint4* __restrict__ tab) {
+                            uint4* __restrict__ claim, uint4* __restrict__ r_out) {
   pdl_wait();
   pdl_trigger();
-  __shared__ uint4 r_sh;
-  if (threadIdx.x < 32) {
+  {
     DevTr st;
     st.load(ts);
     const uint4 y1 = ys[0], yinf = ys[1];
@@ -477,11 +492,6 @@ __global__ void __launch_bounds__(256)
     *r_out = r;
     *claim = gf_add(c0, gf_mul_warp(r, gf_add(c1, gf_mul_warp(c2, r))));
     st.store(ts);
-    r_sh = r;
-  }
-  if (tab) {
-    __syncthreads();
-    dt_build_mul_table(r_sh, tab);
   }
 }
 
@@ -628,7 +638,6 @@ void and_prep_free(AndPrep& p, cudaStream_t s) {
   dev_free(p.fcols, s);
   dev_free(p.eq, s);
   dev_free(p.d_acc, s);
-  dev_free(p.mul_tab, s);
   dev_free(p.dev, s);
   p = AndPrep();
 }
@@ -647,7 +656,6 @@ int and_reduction_begin(const binius_cs* cs, const uint64_t* d_witness, AndPrep&
       (e = dev_alloc(&p.eq, 16 * (N / 2), s)) != cudaSuccess ||
       // 64 univariate slots, then one (y_1, y_inf) slot pair per MLE-check round, zeroed once
       (e = dev_alloc(&p.d_acc, 16 * (64 + 2 * (log_n + 1)), s)) != cudaSuccess ||
-      (e = dev_alloc(&p.mul_tab, 16 * kMulTableEntries, s)) != cudaSuccess ||
       // round constants (2 per round), the claim slot pair, the challenges
       (e = dev_alloc(&p.dev, 16 * (2 * (log_n + 1) + log_n), s)) != cudaSuccess) {
     and_prep_free(p, s);
@@ -679,7 +687,6 @@ int and_reduction_finish(const binius_cs* cs, AndPrep& p, Transcript& t, AndResu
   uint4* const fcols = p.fcols;
   uint4* const eq = p.eq;
   uint32_t* const d_acc = p.d_acc;
-  uint4* const mul_tab = p.mul_tab;
   uint4* const dev = p.dev;
   DevAndTables tab;
   int rc = device_tables(tab);
@@ -761,18 +768,17 @@ int and_reduction_finish(const binius_cs* cs, AndPrep& p, Transcript& t, AndResu
                                                                     acc);
         e = cudaGetLastError();
       } else if (size * 2 >= kMulTableMinSize) {
-        e = launch_pdl(and_mle_fold_eval_kernel, grid_for(size / 2, 256), 256, 0, s, fa, fb, fc,
-                       eq, size * 2, (const uint4*)mul_tab, acc);
+        // two lanes per folded position (size of them)
+        e = launch_pdl(and_mle_fold_eval_kernel, grid_for(size, 256), 256, 0, s, fa, fb, fc,
+                       eq, size * 2, (const uint4*)(d_chal + k - 1), acc);
       } else {
         e = launch_pdl(and_mle_fold_eval_lanes_kernel, grid_for(4 * size, 256), 256, 0, s, fa,
                        fb, fc, eq, size * 2, (const uint4*)(d_chal + k - 1), acc);
       }
       if (e != cudaSuccess) { rc = cuda_error(e, "AND MLE-check round"); break; }
-      // the next round folds by this round's challenge through a table when it is large
-      const bool next_tab = n_rem > 1 && size >= kMulTableMinSize;
-      e = launch_pdl(and_round_finish_kernel, 1, 256, 0, s, dt.state(), dt.tape(),
+      e = launch_pdl(and_round_finish_kernel, 1, 32, 0, s, dt.state(), dt.tape(),
                      reinterpret_cast<const uint4*>(acc), (const AndRoundConst*)(d_consts + k),
-                     d_claim, d_chal + k, next_tab ? mul_tab : (uint4*)nullptr);
+                     d_claim, d_chal + k);
       if (e != cudaSuccess) { rc = cuda_error(e, "and_round_finish_kernel"); break; }
       count_launch(2);
     }

@@ -268,21 +268,6 @@ struct DevTr {
   }
 };
 
-// r's byte table for gf_mul_table, built by the calling block (any size) from r.
-__device__ __forceinline__ void dt_build_mul_table(uint4 r, uint4* __restrict__ tab) {
-  for (uint32_t v = threadIdx.x; v < 256; v += blockDim.x) {
-    uint4 base = r;
-    for (uint32_t j = 0; j < 16; j++) {
-      uint4 acc = gf_zero();
-#pragma unroll
-      for (int k = 0; k < 8; k++) {
-        if ((v >> k) & 1u) gf_add_into(acc, base);
-        base = gf_mul_x(base);
-      }
-      tab[j * 256 + v] = acc;
-    }
-  }
-}
 
 // Host side of one device stretch.  begin() hands the host transcript's state to the device;
 // kernels advance state() and write to tape(); read() queues the copy-back of the state and of

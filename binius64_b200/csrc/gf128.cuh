@@ -111,27 +111,64 @@ __device__ __forceinline__ bool gf_is_zero(uint4 a) { return (a.x | a.y | a.z | 
 __device__ __forceinline__ uint4 gf_zero() { return make_uint4(0u, 0u, 0u, 0u); }
 __device__ __forceinline__ uint4 gf_one() { return make_uint4(1u, 0u, 0u, 0u); }
 
-// Multiplication by a fixed element r through a byte table (the fold challenge of a sumcheck
-// round multiplies every element by the same r): tab[j * 256 + v] = r * (v x^(8j)), so
-// r * x = XOR over the 16 bytes x_j of x of tab[j * 256 + x_j] -- 16 cached loads and XORs, no
-// reduction.  The 64 KiB table is read through the read-only data cache.
-constexpr int kMulTableEntries = 16 * 256;
+// Multiplication by a fixed element r (the fold challenge of a sumcheck round multiplies every
+// element by the same r) through nibble tables in shared memory, which each block builds for
+// itself from r: entry (p, v) = r * (v x^(4p)) for the 32 nibble positions p and v < 16, so
+// r * x = XOR over the nibbles x_p of x of entry (p, x_p) -- 32 lookups, no reduction.  An entry
+// is kept as two 8-byte halves in separate arrays: one 16-entry table of 8-byte words spans the
+// 32 banks exactly once, so the scattered lookups of a warp cost two conflict-free wavefronts
+// each (16-byte entries put two entries on every bank group).  8 KiB per block.
+struct NibbleTable {
+  uint2 lo[32][16];
+  uint2 hi[32][16];
+};
 
-__device__ __forceinline__ uint4 gf_mul_x(uint4 a) {
-  const uint32_t carry = a.w >> 31;
-  uint4 r = make_uint4(a.x << 1, (a.y << 1) | (a.x >> 31), (a.z << 1) | (a.y >> 31),
-                       (a.w << 1) | (a.z >> 31));
-  r.x ^= carry * 0x87u;  // x^128 = x^7 + x^2 + x + 1
-  return r;
+// x^k * r for k < 128: r shifted left by k as a 256-bit value, reduced.
+__device__ __forceinline__ uint4 gf_mul_xk(uint4 r, uint32_t k) {
+  const uint64_t r0 = lo64(r), r1 = hi64(r);
+  const uint32_t s = k & 63;
+  const uint64_t a = r0 << s;
+  const uint64_t b = s ? (r1 << s) | (r0 >> (64 - s)) : r1;
+  const uint64_t c = s ? r1 >> (64 - s) : 0;
+  u256 u;
+  if (k < 64) {
+    u.p0 = a; u.p1 = b; u.p2 = c; u.p3 = 0;
+  } else {
+    u.p0 = 0; u.p1 = a; u.p2 = b; u.p3 = c;
+  }
+  return reduce256(u);
 }
 
-__device__ __forceinline__ uint4 gf_mul_table(const uint4* __restrict__ tab, uint4 x) {
-  uint4 acc = gf_zero();
+// Builds r's nibble tables with the calling block (any block size >= 1; ends with a barrier, so
+// every thread of the block must call it).  `basis` is 128 elements of scratch shared memory.
+__device__ __forceinline__ void nibble_table_build(NibbleTable& t, uint4* basis, uint4 r) {
+  for (uint32_t k = threadIdx.x; k < 128; k += blockDim.x) basis[k] = gf_mul_xk(r, k);
+  __syncthreads();
+  for (uint32_t e = threadIdx.x; e < 32 * 16; e += blockDim.x) {
+    const uint32_t p = e >> 4, v = e & 15;
+    uint4 acc = gf_zero();
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+      if ((v >> i) & 1u) gf_add_into(acc, basis[4 * p + i]);
+    t.lo[p][v] = make_uint2(acc.x, acc.y);
+    t.hi[p][v] = make_uint2(acc.z, acc.w);
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ uint4 gf_mul_nibble(const NibbleTable& t, uint4 x) {
+  uint2 lo = make_uint2(0u, 0u), hi = make_uint2(0u, 0u);
   const uint32_t w[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
-  for (int j = 0; j < 16; j++)
-    gf_add_into(acc, __ldg(tab + j * 256 + ((w[j >> 2] >> (8 * (j & 3))) & 255u)));
-  return acc;
+  for (int p = 0; p < 32; p++) {
+    const uint32_t v = (w[p >> 3] >> (4 * (p & 7))) & 15u;
+    const uint2 l = t.lo[p][v], h = t.hi[p][v];
+    lo.x ^= l.x;
+    lo.y ^= l.y;
+    hi.x ^= h.x;
+    hi.y ^= h.y;
+  }
+  return make_uint4(lo.x, lo.y, hi.x, hi.y);
 }
 
 }  // namespace bgpu

@@ -27,18 +27,16 @@ int bivariate_eval(const uint4* d_a, const uint4* d_b, uint64_t half, uint32_t* 
 // Fold (a, b) of length size by r, then (y_1, y_inf) of the next round.
 int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[16],
                         uint32_t* d_out8, cudaStream_t s);
-// As bivariate_fold_eval with the challenge in device memory (d_r) and no clearing of d_out8:
-// folds of at least kMulTableMinSize elements read r's byte table d_tab, built beforehand.
+// As bivariate_fold_eval with the challenge in device memory (d_r) and no clearing of d_out8.
 int bivariate_fold_eval_dev(uint4* d_a, uint4* d_b, uint64_t size, const uint4* d_r,
-                            const uint4* d_tab, uint32_t* d_out8, cudaStream_t s);
+                            uint32_t* d_out8, cudaStream_t s);
 class DeviceTranscript;
 // The device Fiat-Shamir step of a plain bivariate product round: reads (y_1, y_inf) at d_ys
 // and the claim (d_claim_init if set, else d_claim), writes the message (c_0, c_1) and then the
-// 32 bytes at d_commitment if set, samples r into d_r_out, updates d_claim and, with d_tab,
-// builds r's byte table.
+// 32 bytes at d_commitment if set, samples r into d_r_out and updates d_claim.
 int bivariate_round_finish(const DeviceTranscript& dt, const uint4* d_ys, const uint4* d_claim_init,
                            uint4* d_claim, const uint8_t* d_commitment, uint4* d_r_out,
-                           uint4* d_tab, cudaStream_t s);
+                           cudaStream_t s);
 // The last n_rounds rounds of a plain bivariate product sumcheck in one launch (one CTA): each
 // round folds (a, b) -- of length len before the first fold -- by the previous challenge
 // (d_r_first for the first round, when set) and runs the Fiat-Shamir step of
@@ -49,9 +47,9 @@ int bivariate_tail(const DeviceTranscript& dt, uint4* d_a, uint4* d_b, uint64_t 
 // Sumcheck rounds whose arrays have at most this many elements before the fold run in the
 // single-CTA tail kernels (the calling thread's Tuning::tail_log; 2^11 by default).
 inline uint64_t tail_max_len() { return 1ull << tuning().tail_log; }
-// d_tab (16 * 256 elements) = the byte table of multiplication by r (gf_mul_table).
-int build_mul_table(const uint8_t r[16], uint4* d_tab, cudaStream_t s);
-// Folds of at least this many elements multiply by the fold challenge through its byte table.
+// Folds of at least this many elements multiply by the fold challenge through its nibble tables
+// (gf_mul_nibble, built by every block in shared memory); smaller ones spread each position
+// over lanes and use the integer multiply.
 constexpr uint64_t kMulTableMinSize = 1ull << 15;
 
 // Lagrange basis of the subspace {phi(t) : t < 2^dim} at x, phi the AES-to-GHASH embedding

@@ -299,13 +299,12 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
   BGPU_CUDA(dev_alloc(&b, 16 * N, s));
   BGPU_CUDA(dev_alloc(&eq_r, 16 * 128, s));
   BGPU_CUDA(dev_alloc(&d_small, 16 * 128, s));
-  // BaseFold round state: sums (2 per round), the claim pair, challenges, r's byte table
-  const uint64_t n_dev = 2ull * n + 2 + n + kMulTableEntries;
+  // BaseFold round state: sums (2 per round), the claim pair, challenges
+  const uint64_t n_dev = 2ull * n + 2 + n;
   BGPU_CUDA(dev_alloc(&dev, 16 * n_dev, s));
   uint4* slots = dev;
   uint4* claim = dev + 2 * n;  // [0] running claim, [1] initial claim
   uint4* chal = claim + 2;
-  uint4* tab = chal + n;
   int rc = BINIUS_OK;
   {
     DevFri fri(*P, *C, s, chal);
@@ -370,16 +369,13 @@ int pcs_prove_impl(const binius_pcs* P, const binius_pcs_committed* C, const voi
         if (round == 0)
           rc = bivariate_eval(a, b, size / 2, ys, s);
         else
-          rc = bivariate_fold_eval_dev(a, b, size * 2, chal + round - 1,
-                                       size * 2 >= kMulTableMinSize ? tab : nullptr, ys, s);
+          rc = bivariate_fold_eval_dev(a, b, size * 2, chal + round - 1, ys, s);
         if (rc) break;
         bool committed = false;
         const uint8_t* d_root = nullptr;
         if ((rc = fri.execute(&committed, &d_root))) break;
-        const bool next_tab = round + 1 < n && size >= kMulTableMinSize;
         if ((rc = bivariate_round_finish(dt, slots + 2 * round, round == 0 ? claim + 1 : nullptr,
-                                         claim, committed ? d_root : nullptr, chal + round,
-                                         next_tab ? tab : nullptr, s)))
+                                         claim, committed ? d_root : nullptr, chal + round, s)))
           break;
         tape_bytes += committed ? 64 : 32;
         fri.receive();

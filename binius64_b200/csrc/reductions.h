@@ -27,7 +27,7 @@ int and_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transcri
 // and_reduction_finish runs the rest and releases the buffers (also on error).
 struct AndPrep {
   uint64_t* words = nullptr;
-  uint4 *eq_big = nullptr, *fcols = nullptr, *eq = nullptr, *mul_tab = nullptr, *dev = nullptr;
+  uint4 *eq_big = nullptr, *fcols = nullptr, *eq = nullptr, *dev = nullptr;
   uint32_t* d_acc = nullptr;
 };
 int and_reduction_begin(const binius_cs* cs, const uint64_t* d_witness, AndPrep& p,

@@ -101,7 +101,9 @@ __global__ void __launch_bounds__(kTile)
   __shared__ uint64_t s_w[kTile + kChunks];
   __shared__ uint32_t s_key[kTile];
   __shared__ uint64_t s_col[kChunks][8];  // byte j of chunk c's row: bit j of its 8 words
-  __shared__ uint4 s_tab[kChunks][2][16];
+  // nibble tables as 8-byte halves: a 16-entry table of 8-byte words spans the 32 banks once, so
+  // the random lookups of a half-warp never conflict (16-byte entries: ~1.7x the wavefronts)
+  __shared__ uint2 s_tlo[kChunks][2][16], s_thi[kChunks][2][16];
   const uint32_t tid = threadIdx.x, j = tid & 63, grp = tid >> 6;
   uint32_t cur = kNoKey;
   uint4 acc = gf_zero();
@@ -157,11 +159,12 @@ __global__ void __launch_bounds__(kTile)
       uint4 base = gf_zero();
       if (q & 1) gf_add_into(base, e[2]);
       if (q & 2) gf_add_into(base, e[3]);
-      uint4* t = s_tab[c][h] + 4 * q;
-      t[0] = base;
-      t[1] = gf_add(base, e0);
-      t[2] = gf_add(base, e1);
-      t[3] = gf_add(gf_add(base, e0), e1);
+      const uint4 v[4] = {base, gf_add(base, e0), gf_add(base, e1), gf_add(gf_add(base, e0), e1)};
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        s_tlo[c][h][4 * q + i] = make_uint2(v[i].x, v[i].y);
+        s_thi[c][h][4 * q + i] = make_uint2(v[i].z, v[i].w);
+      }
     }
     __syncthreads();
 #pragma unroll 2
@@ -172,8 +175,12 @@ __global__ void __launch_bounds__(kTile)
         switch_key(k0);
         if (k0 != kNoKey) {
           const uint32_t byte = reinterpret_cast<const uint8_t*>(s_col[c])[j];
-          gf_add_into(acc, s_tab[c][0][byte & 15]);
-          gf_add_into(acc, s_tab[c][1][byte >> 4]);
+          const uint2 l0 = s_tlo[c][0][byte & 15], h0 = s_thi[c][0][byte & 15];
+          const uint2 l1 = s_tlo[c][1][byte >> 4], h1 = s_thi[c][1][byte >> 4];
+          acc.x ^= l0.x ^ l1.x;
+          acc.y ^= l0.y ^ l1.y;
+          acc.z ^= h0.x ^ h1.x;
+          acc.w ^= h0.y ^ h1.y;
         }
       } else {
         for (uint32_t i = 0; i < 8; i++) {
@@ -364,17 +371,15 @@ struct ShiftRoundConst {
 // in/out claim, Gruen eq prefix).  The batch message is the shift round's (s_0, s_1) plus beta
 // times the in/out check's Gruen-scaled (d_0, d_1) (MleToSumCheckDecorator + batch_prove); then r
 // is sampled and the three running values advance.  When init_lohi is set (the first round) the
-// in/out claim is first set to lo + (hi - lo) z0 from it.
-__global__ void __launch_bounds__(256)
+// in/out claim is first set to lo + (hi - lo) z0 from it.  One warp runs the step.
+__global__ void __launch_bounds__(32)
     shift_round_finish_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
                               const uint4* __restrict__ ys, const ShiftRoundConst* __restrict__ rc,
                               const uint4* __restrict__ init_lohi, uint4 z0, uint4 beta,
-                              uint4* __restrict__ st3, uint4* __restrict__ r_out,
-                              uint4* __restrict__ tab) {
+                              uint4* __restrict__ st3, uint4* __restrict__ r_out) {
   pdl_wait();
   pdl_trigger();
-  __shared__ uint4 r_sh;
-  if (threadIdx.x < 32) {
+  {
     DevTr st;
     st.load(ts);
     const ShiftRoundConst c = *rc;
@@ -407,11 +412,6 @@ __global__ void __launch_bounds__(256)
     f.x ^= 1u;
     st3[2] = gf_mul_warp(eqp, f);
     st.store(ts);
-    r_sh = r;
-  }
-  if (tab) {
-    __syncthreads();
-    dt_build_mul_table(r_sh, tab);
   }
 }
 
@@ -647,14 +647,13 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
 
   // device round state: phase-1 sum slots (12 x 2), phase-2 slots (log_words x 4); dstate = the
   // phase-1 claim, the phase-2 running values (shift claim, in/out claim, eq prefix) and the
-  // in/out check's first (lo, hi); challenges (12 + log_words); the last challenge's byte table
-  uint4 *slots, *dstate, *chal, *tab;
+  // in/out check's first (lo, hi); challenges (12 + log_words)
+  uint4 *slots, *dstate, *chal;
   ShiftRoundConst* rconst;
   const uint64_t n_slots = 2 * 12 + 4 * (uint64_t)log_words;
   SHIFT_TRY(B.alloc(&slots, 16 * n_slots));
   SHIFT_TRY(B.alloc(&dstate, 16 * 6));
   SHIFT_TRY(B.alloc(&chal, 16 * (12 + (uint64_t)log_words)));
-  SHIFT_TRY(B.alloc(&tab, 16 * kMulTableEntries));
   SHIFT_TRY(B.alloc(&rconst, sizeof(ShiftRoundConst) * log_words));
   BGPU_CUDA(cudaMemsetAsync(slots, 0, 16 * n_slots, s));
   uint4* slots2 = slots + 24;
@@ -674,14 +673,11 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
     if (round == 0) {
       SHIFT_TRY(bivariate_eval(g, h, size / 2, ys, s));
     } else {
-      SHIFT_TRY(bivariate_fold_eval_dev(g, h, size * 2, chal + round - 1,
-                                        size * 2 >= kMulTableMinSize ? tab : nullptr, ys, s));
+      SHIFT_TRY(bivariate_fold_eval_dev(g, h, size * 2, chal + round - 1, ys, s));
     }
-    // the next round folds arrays of `size` elements
-    const bool next_tab = round < 11 && size >= kMulTableMinSize;
     SHIFT_TRY(bivariate_round_finish(dt, slots + 2 * round,
                                      round == 0 ? reinterpret_cast<const uint4*>(acc + 8) : nullptr,
-                                     dstate, nullptr, chal + round, next_tab ? tab : nullptr, s));
+                                     dstate, nullptr, chal + round, s));
   }
   SHIFT_TRY(bivariate_tail(dt, g, h, (uint64_t)kFlat >> (tail0 - 1), 12 - tail0, chal + tail0 - 1,
                            dstate, chal + tail0, s));
@@ -795,7 +791,6 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
       SHIFT_TRY(bivariate_eval(W, M, half, reinterpret_cast<uint32_t*>(ys), s));
     } else {
       SHIFT_TRY(bivariate_fold_eval_dev(W, M, half * 4, chal + 12 + k - 1,
-                                        half * 4 >= kMulTableMinSize ? tab : nullptr,
                                         reinterpret_cast<uint32_t*>(ys), s));
     }
     if (p < n_rem) {
@@ -805,11 +800,10 @@ int shift_reduction_prove(const binius_cs* cs, const uint64_t* d_witness, Transc
       SHIFT_TRY(dot2(half, half, half, ys + 2));
     }
     if (n_rem <= p) gn--;
-    const bool next_tab = n_rem > 1 && half * 2 >= kMulTableMinSize;
-    BGPU_CUDA(launch_pdl(shift_round_finish_kernel, 1, 256, 0, s, dt.state(), dt.tape(),
+    BGPU_CUDA(launch_pdl(shift_round_finish_kernel, 1, 32, 0, s, dt.state(), dt.tape(),
                          (const uint4*)ys, (const ShiftRoundConst*)(rconst + k),
                          n_rem == log_words ? (const uint4*)init_lohi : (const uint4*)nullptr, z0,
-                         u4(beta), run, chal + 12 + k, next_tab ? tab : (uint4*)nullptr));
+                         u4(beta), run, chal + 12 + k));
     SHIFT_TRY(launched("shift_round_finish_kernel"));
   }
   if (tail_n) {

@@ -169,37 +169,49 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // Folds (a, b) of length `size` by r in place (a[i] = a[i] + r (a[i + size/2] - a[i])) and
-// evaluates the next round on the folded length-size/2 arrays.  Thread j owns folded positions j
-// and j + size/4, so no two threads touch the same element.  The four products by r go through
-// the byte table of r (gf_mul_table); the rounds below kMulTableMinSize elements, which have no
-// table, run in bivariate_fold_eval_lanes_kernel.
+// evaluates the next round on the folded length-size/2 arrays.  Each folded position j < size/4
+// belongs to a pair of adjacent lanes: the odd lane folds a and b at j, the even lane at
+// j + size/4, and each forms one of the two products (the even lane y_1's fa1 fb1, the odd lane
+// y_inf's after a shuffle brings fa1, fb1 over).  The products by r go through r's nibble tables,
+// which each block builds in shared memory from r (read from r_ptr, else r_arg).
 __global__ void __launch_bounds__(kThreads)
     bivariate_fold_eval_kernel(uint4* __restrict__ a, uint4* __restrict__ b, uint64_t size,
-                               const uint4* __restrict__ tab, uint32_t* __restrict__ out) {
+                               uint4 r_arg, const uint4* __restrict__ r_ptr,
+                               uint32_t* __restrict__ out) {
+  __shared__ NibbleTable tab;
+  __shared__ uint4 basis[128];
   pdl_wait();
   pdl_trigger();
+  nibble_table_build(tab, basis, r_ptr ? *r_ptr : r_arg);
   const uint64_t h = size >> 1, q = size >> 2;
-  u256 s1 = {0, 0, 0, 0}, sinf = {0, 0, 0, 0};
-  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < q;
-       j += (uint64_t)gridDim.x * blockDim.x) {
-    const uint4 a_lo = a[j], a_hi = a[h + j], a_lo2 = a[q + j], a_hi2 = a[h + q + j];
-    const uint4 b_lo = b[j], b_hi = b[h + j], b_lo2 = b[q + j], b_hi2 = b[h + q + j];
-    const uint4 fa0 = gf_add(a_lo, gf_mul_table(tab, gf_add(a_hi, a_lo)));
-    const uint4 fa1 = gf_add(a_lo2, gf_mul_table(tab, gf_add(a_hi2, a_lo2)));
-    const uint4 fb0 = gf_add(b_lo, gf_mul_table(tab, gf_add(b_hi, b_lo)));
-    const uint4 fb1 = gf_add(b_lo2, gf_mul_table(tab, gf_add(b_hi2, b_lo2)));
-    a[j] = fa0;
-    a[q + j] = fa1;
-    b[j] = fb0;
-    b[q + j] = fb1;
-    xor_into(s1, clmul128(fa1, fb1));
-    xor_into(sinf, clmul128(gf_add(fa0, fa1), gf_add(fb0, fb1)));
+  const uint32_t odd = threadIdx.x & 1;
+  u256 acc = {0, 0, 0, 0};
+  const uint64_t all = (uint64_t)gridDim.x * blockDim.x;
+  // warp-uniform sweeps: every lane of a warp runs the same iterations (shuffles below)
+  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + (threadIdx.x & ~31u); base < 2 * q;
+       base += all) {
+    const uint64_t j = (base + (threadIdx.x & 31)) >> 1;
+    const bool live = j < q;
+    uint4 fa = gf_zero(), fb = gf_zero();
+    if (live) {
+      const uint64_t pos = odd ? j : q + j;
+      const uint4 a_lo = a[pos], a_hi = a[h + pos], b_lo = b[pos], b_hi = b[h + pos];
+      fa = gf_add(a_lo, gf_mul_nibble(tab, gf_add(a_hi, a_lo)));
+      fb = gf_add(b_lo, gf_mul_nibble(tab, gf_add(b_hi, b_lo)));
+      a[pos] = fa;
+      b[pos] = fb;
+    }
+    // the odd lane takes its even partner's (fa1, fb1)
+    const uint4 pa = shfl_gf(fa, 0, 2), pb = shfl_gf(fb, 0, 2);
+    // one product per lane, selected without divergence (fa, fb are zero on dead lanes)
+    xor_into(acc, clmul128(odd ? gf_add(fa, pa) : fa, odd ? gf_add(fb, pb) : fb));
   }
-  uint4 v[2] = {reduce256(s1), reduce256(sinf)};
+  const uint4 s = reduce256(acc);
+  uint4 v[2] = {odd ? gf_zero() : s, odd ? s : gf_zero()};
   block_xor_reduce<2>(v, out);
 }
 
-// The small rounds of bivariate_fold_eval_kernel (no byte table) on four lanes per position j:
+// The small rounds of bivariate_fold_eval_kernel (no nibble tables) on four lanes per position j:
 // lane k folds one of a[j], a[q + j], b[j], b[q + j] by r, the four folded values are shared by
 // shuffles, and lanes 0 and 1 form the two products.  One multiply then one product per lane,
 // where one thread per position ran six dependent out-of-line multiplies: these rounds are
@@ -241,17 +253,15 @@ __global__ void __launch_bounds__(kThreads)
 // sums (y_1, y_inf) and the claim give c_0 = claim + y_1, c_2 = y_inf, c_1 = y_1 + c_0 + c_2; the
 // message is (c_0, c_1), then optionally a 32-byte commitment (a Merkle root the device just
 // built), then the challenge r is sampled and the claim becomes c_0 + c_1 r + c_2 r^2.  The claim
-// is read from claim_init when that is set (the first round).  With a table pointer the block
-// then builds r's byte table for the next fold.
-__global__ void __launch_bounds__(256)
+// is read from claim_init when that is set (the first round).  One warp runs the step.
+__global__ void __launch_bounds__(32)
     bivariate_round_finish_kernel(TranscriptState* __restrict__ ts, uint8_t* __restrict__ tape,
                                   const uint4* __restrict__ ys, const uint4* __restrict__ claim_init,
                                   uint4* __restrict__ claim, const uint8_t* __restrict__ commitment,
-                                  uint4* __restrict__ r_out, uint4* __restrict__ tab) {
+                                  uint4* __restrict__ r_out) {
   pdl_wait();
   pdl_trigger();
-  __shared__ uint4 r_sh;
-  if (threadIdx.x < 32) {
+  {
     DevTr st;
     st.load(ts);
     const uint4 y1 = ys[0], yinf = ys[1];
@@ -268,11 +278,6 @@ __global__ void __launch_bounds__(256)
     *r_out = r;
     *claim = gf_add(c0, gf_mul_warp(r, gf_add(c1, gf_mul_warp(c2, r))));
     st.store(ts);
-    r_sh = r;
-  }
-  if (tab) {
-    __syncthreads();
-    dt_build_mul_table(r_sh, tab);
   }
 }
 
@@ -334,23 +339,6 @@ __global__ void __launch_bounds__(kTailThreads)
     st.store(ts);
     *claim = cl;
   }
-}
-
-// tab[j * 256 + v] = r * (v x^(8j)): the byte table of gf_mul_table, one entry per thread from
-// r x^(8j) by repeated multiplication by x.
-__global__ void build_mul_table_kernel(uint4 r, uint4* __restrict__ tab) {
-  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (uint32_t)kMulTableEntries) return;
-  const uint32_t j = idx >> 8, v = idx & 255u;
-  uint4 base = r;
-  for (uint32_t k = 0; k < 8 * j; k++) base = gf_mul_x(base);
-  uint4 acc = gf_zero();
-#pragma unroll
-  for (int k = 0; k < 8; k++) {
-    if ((v >> k) & 1u) gf_add_into(acc, base);
-    base = gf_mul_x(base);
-  }
-  tab[idx] = acc;
 }
 
 
@@ -426,35 +414,18 @@ int bivariate_eval(const uint4* d_a, const uint4* d_b, uint64_t half, uint32_t* 
   return BINIUS_OK;
 }
 
-int build_mul_table(const uint8_t r[16], uint4* d_tab, cudaStream_t s) {
-  uint4 rv;
-  memcpy(&rv, r, 16);
-  build_mul_table_kernel<<<kMulTableEntries / 256, 256, 0, s>>>(rv, d_tab);
-  BGPU_LAUNCH_CHECK("build_mul_table_kernel");
-  count_launch();
-  return BINIUS_OK;
-}
-
 int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[16],
                         uint32_t* d_out8, cudaStream_t s) {
   if (size < 4) return set_error(BINIUS_E_ARG, "bivariate_fold_eval needs size >= 4");
   uint4 rv;
   memcpy(&rv, r, 16);
   BGPU_CUDA(cudaMemsetAsync(d_out8, 0, 32, s));
-  const unsigned grid = grid_for(size / 4, kThreads);
+  const unsigned grid = grid_for(size / 2, kThreads);  // two lanes per folded position
   if (size >= kMulTableMinSize) {
-    // large rounds: the four products by r per thread go through r's byte table
-    uint4* tab = nullptr;
-    BGPU_CUDA(dev_alloc(&tab, 16 * kMulTableEntries, s));
-    int rc = build_mul_table(r, tab, s);
-    if (!rc) {
-      bivariate_fold_eval_kernel<<<grid, kThreads, 0, s>>>(d_a, d_b, size, tab, d_out8);
-      cudaError_t e = cudaGetLastError();
-      if (e != cudaSuccess) rc = cuda_error(e, "bivariate_fold_eval_kernel");
-      else count_launch();
-    }
-    dev_free(tab, s);
-    return rc;
+    bivariate_fold_eval_kernel<<<grid, kThreads, 0, s>>>(d_a, d_b, size, rv, nullptr, d_out8);
+    BGPU_LAUNCH_CHECK("bivariate_fold_eval_kernel");
+    count_launch();
+    return BINIUS_OK;
   }
   bivariate_fold_eval_lanes_kernel<<<grid_for(size, kThreads), kThreads, 0, s>>>(
       d_a, d_b, size, rv, nullptr, d_out8);
@@ -464,14 +435,13 @@ int bivariate_fold_eval(uint4* d_a, uint4* d_b, uint64_t size, const uint8_t r[1
 }
 
 int bivariate_fold_eval_dev(uint4* d_a, uint4* d_b, uint64_t size, const uint4* d_r,
-                            const uint4* d_tab, uint32_t* d_out8, cudaStream_t s) {
+                            uint32_t* d_out8, cudaStream_t s) {
   if (size < 4) return set_error(BINIUS_E_ARG, "bivariate_fold_eval needs size >= 4");
-  const unsigned grid = grid_for(size / 4, kThreads);
+  const unsigned grid = grid_for(size / 2, kThreads);  // two lanes per folded position
   cudaError_t e;
   if (size >= kMulTableMinSize) {
-    if (!d_tab) return set_error(BINIUS_E_ARG, "a large fold needs the challenge's table");
     e = launch_pdl(bivariate_fold_eval_kernel, grid, kThreads, 0, s, d_a, d_b, size,
-                   (const uint4*)d_tab, d_out8);
+                   gf_zero_host(), d_r, d_out8);
   } else {
     e = launch_pdl(bivariate_fold_eval_lanes_kernel, grid_for(size, kThreads), kThreads, 0, s,
                    d_a, d_b, size, gf_zero_host(), d_r, d_out8);
@@ -483,9 +453,9 @@ int bivariate_fold_eval_dev(uint4* d_a, uint4* d_b, uint64_t size, const uint4* 
 
 int bivariate_round_finish(const DeviceTranscript& dt, const uint4* d_ys, const uint4* d_claim_init,
                            uint4* d_claim, const uint8_t* d_commitment, uint4* d_r_out,
-                           uint4* d_tab, cudaStream_t s) {
-  cudaError_t e = launch_pdl(bivariate_round_finish_kernel, 1, 256, 0, s, dt.state(), dt.tape(),
-                             d_ys, d_claim_init, d_claim, d_commitment, d_r_out, d_tab);
+                           cudaStream_t s) {
+  cudaError_t e = launch_pdl(bivariate_round_finish_kernel, 1, 32, 0, s, dt.state(), dt.tape(),
+                             d_ys, d_claim_init, d_claim, d_commitment, d_r_out);
   if (e != cudaSuccess) return cuda_error(e, "bivariate_round_finish_kernel");
   count_launch();
   return BINIUS_OK;
