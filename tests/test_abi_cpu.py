@@ -18,6 +18,18 @@ def test_library_loads_and_exports_all_declared_symbols():
     assert set(declared) <= set(_ffi._SIGS), set(declared) - set(_ffi._SIGS)
 
 
+def test_rust_binding_declares_every_entry():
+    """The Rust `extern "C"` block a reference maintainer adds declares every
+    entry point of the header, so the binding is complete as written."""
+    import os
+    import re
+    with open(os.path.join(_ffi.ROOT, "INTEGRATION.md")) as f:
+        text = f.read()
+    rust = set(re.findall(r"pub fn (binius_[a-z0-9_]+)\(", text))
+    missing = sorted(set(_ffi.declared_functions()) - rust)
+    assert not missing, f"declared in the header, not in the Rust binding: {missing}"
+
+
 def test_version():
     assert b"sm_100a" in _ffi.lib().binius_version()
 
