@@ -8,6 +8,10 @@
   build_h_parts, evaluated directly at r_j ++ r_s, equal the verifier's succinct evaluate_h_op
   (verifier/verifier/src/protocols/shift/monster.rs:31-99 with shift_ind.rs's partial_eval_sigmas,
   partial_eval_sigmas_transpose, partial_eval_phi), restated below in Python.
+* verifier/verifier/src/protocols/shift/monster.rs:263-323 (test_evaluate_h_op_hypercube_vertices):
+  at the hypercube vertices, with the challenge on a domain point, every h_op value is the
+  indicator of its integer shift relation -- for the restated evaluate_h_op and for the oracle's
+  build_h_parts on every vertex.
 * prover/prover/src/fri/fold.rs:334-369 (test_fri_compatible_ntt_domains) with the shrunk cases of
   prover/prover/proptest-regressions/fri/fold.txt (log_dim = 0 with arity 0 and 1) first, then
   the property's whole range (log_dim < 8, arity < 4): over the domain of
@@ -20,7 +24,14 @@ import pytest
 
 import oracle as orc
 
-gm = orc.gf_mul
+
+def gm(a, b):
+    """GHASH product; products by 0 or 1 (the hypercube vertices below) without a library call."""
+    if a <= 1:
+        return b if a else 0
+    if b <= 1:
+        return a if b else 0
+    return orc.gf_mul(a, b)
 
 
 # ---------------------------------------------------------------- NTT lookup KAT
@@ -166,6 +177,45 @@ def test_h_op_consistency(case):
     point = orc.from_ints(r_j + r_s)
     direct = [orc.to_int(orc.mle_eval(np.ascontiguousarray(h[v]), point)) for v in range(8)]
     assert succinct == direct
+
+
+def h_op_indicators(i, j, s):
+    """The integer relations a shift variant's h multilinear indicates at a hypercube vertex:
+    bit i of the shifted word comes from bit j of the input shifted by s (sll, srl, sra, rotr on
+    64 bits, then the same on each 32-bit half)."""
+    i_hi, i_lo, j_hi, j_lo, s_lo = i // 32, i % 32, j // 32, j % 32, s % 32
+    return [j + s == i, i + s == j, min(i + s, 63) == j, (i + s) % 64 == j,
+            i_hi == j_hi and j_lo + s_lo == i_lo, i_hi == j_hi and i_lo + s_lo == j_lo,
+            i_hi == j_hi and min(i_lo + s_lo, 31) == j_lo,
+            i_hi == j_hi and (i_lo + s_lo) % 32 == j_lo]
+
+
+def test_h_op_hypercube_vertices():
+    """verifier/verifier/src/protocols/shift/monster.rs:263-323
+    (test_evaluate_h_op_hypercube_vertices): with the challenge at the i-th point of the
+    64-point domain (so the Lagrange evaluations are the indicator of i) and r_j, r_s at the
+    hypercube vertices of j and s (index_to_hypercube_point: bit k of the index is coordinate k),
+    each of the eight h_op values is 1 exactly when the integer shift relation holds.  Checked on
+    1024 random (i, j, s) (the reference test's count) for the restated succinct evaluate_h_op,
+    and on every (j, s) of each i for the oracle's build_h_parts, whose domain point i is phi(i),
+    the AES byte i embedded in GHASH (the reference test's domain is the GHASH subspace of the
+    integers 0..63; the indicator form of the Lagrange evaluations is what both rely on)."""
+    phi = orc.aes_to_ghash_table()
+    rng = np.random.default_rng(0)
+    for _ in range(1024):
+        i, j, s = (int(x) for x in rng.integers(0, 64, size=3))
+        lt = [1 if t == i else 0 for t in range(64)]
+        r_j = [(j >> k) & 1 for k in range(6)]
+        r_s = [(s >> k) & 1 for k in range(6)]
+        assert evaluate_h_op(lt, r_j, r_s) == [int(b) for b in h_op_indicators(i, j, s)], (i, j, s)
+    for i in range(64):
+        h, lt = orc.shift_h_parts(phi[i])
+        assert [orc.to_int(x) for x in lt] == [1 if t == i else 0 for t in range(64)], i
+        want = np.zeros((8, 4096, 2), dtype=np.uint64)  # h[v][s * 64 + j], (lo, hi) words
+        for s in range(64):
+            for j in range(64):
+                want[:, s * 64 + j, 0] = h_op_indicators(i, j, s)
+        assert np.array_equal(h, want), i
 
 
 # ---------------------------------------------------------------- FRI fold / encode commutation
