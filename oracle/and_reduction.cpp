@@ -123,25 +123,47 @@ static void eq_aes(const uint8_t* r, uint32_t n, uint8_t* out) {
 static const uint8_t kSmallChallenges[3] = {0x2, 0x4, 0x10};  // config.rs:33-37
 
 // Evaluations of each 64-bit word's interpolant at the 64 points 64..127: val[k] = sum over set
-// bits t of M[k][t].
+// bits t of M[k][t], M[k][t] the Lagrange basis polynomial of domain point t at 64 + k.  The map is
+// linear in the word's bits, so it is tabulated per byte of the word (the byte-chunked lookup of
+// and_reduction/ntt_lookup.rs:91-164): tab[p][v] holds the 64 values of the word whose byte p is
+// v and whose other bytes are zero, and a word's values are the XOR of its eight byte rows.
 struct WordNtt {
-  uint8_t M[64][64];
+  uint64_t tab[8][256][8];  // 64 output bytes per row, as eight 8-byte words
   WordNtt() {
+    uint8_t M[64][64];
     for (int k = 0; k < 64; k++) lagrange_aes(6, (uint8_t)(64 + k), M[k]);
+    for (int p = 0; p < 8; p++)
+      for (int v = 0; v < 256; v++) {
+        uint8_t row[64] = {0};
+        for (int bit = 0; bit < 8; bit++)
+          if ((v >> bit) & 1)
+            for (int k = 0; k < 64; k++) row[k] ^= M[k][8 * p + bit];
+        memcpy(tab[p][v], row, 64);
+      }
   }
   void eval(uint64_t w, uint8_t out[64]) const {
-    for (int k = 0; k < 64; k++) {
-      uint8_t acc = 0;
-      for (int t = 0; t < 64; t++)
-        if ((w >> t) & 1) acc ^= M[k][t];
-      out[k] = acc;
+    uint64_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int p = 0; p < 8; p++) {
+      const uint64_t* r = tab[p][(w >> (8 * p)) & 0xff];
+      for (int q = 0; q < 8; q++) acc[q] ^= r[q];
     }
+    memcpy(out, acc, 64);
+  }
+};
+
+// The AES-field product as a 256 x 256 table (the same values as aes_mul).
+struct AesMulTable {
+  uint8_t t[256][256];
+  AesMulTable() {
+    for (int a = 0; a < 256; a++)
+      for (int b = 0; b < 256; b++) t[a][b] = aes_mul((uint8_t)a, (uint8_t)b);
   }
 };
 
 void univariate_round(const uint64_t* a, const uint64_t* b, const uint64_t* c, uint32_t log_n,
                       const u128* big, u128 msg[64]) {
   static const WordNtt ntt;
+  static const AesMulTable mul;
   uint8_t eq_small[8];
   eq_aes(kSmallChallenges, 3, eq_small);
   size_t n_chunks = (size_t)1 << (log_n - 3);
@@ -159,8 +181,8 @@ void univariate_round(const uint64_t* a, const uint64_t* b, const uint64_t* c, u
         ntt.eval(a[i], va);
         ntt.eval(b[i], vb);
         ntt.eval(c[i], vc);
-        for (int k = 0; k < 64; k++)
-          summed[k] ^= aes_mul((uint8_t)(aes_mul(va[k], vb[k]) ^ vc[k]), eq_small[j]);
+        const uint8_t* by_eq = mul.t[eq_small[j]];
+        for (int k = 0; k < 64; k++) summed[k] ^= by_eq[mul.t[va[k]][vb[k]] ^ vc[k]];
       }
       for (int k = 0; k < 64; k++) acc[k] ^= gf_mul(eq_big[ch], phi(summed[k]));
     }
@@ -214,12 +236,19 @@ AndOutput and_reduction_prove(const uint64_t* a, const uint64_t* b, const uint64
     std::vector<u128> eq(half);
     eq_ind_partial_eval(point.data(), n_rem - 1, eq.data());
     u128 y1 = 0, yinf = 0;
-    for (size_t i = 0; i < half; i++) {
-      u128 a1 = fa[half + i], b1 = fb[half + i], c1 = fc[half + i];
-      u128 ai = fa[i] ^ a1, bi = fb[i] ^ b1;
-      y1 ^= gf_mul(eq[i], gf_mul(a1, b1) ^ c1);
-      yinf ^= gf_mul(eq[i], gf_mul(ai, bi));
-    }
+    std::mutex m;
+    parallel_for(half, [&](size_t lo, size_t hi) {  // XOR sums: any split gives the same value
+      u128 s1 = 0, sinf = 0;
+      for (size_t i = lo; i < hi; i++) {
+        u128 a1 = fa[half + i], b1 = fb[half + i], c1 = fc[half + i];
+        u128 ai = fa[i] ^ a1, bi = fb[i] ^ b1;
+        s1 ^= gf_mul(eq[i], gf_mul(a1, b1) ^ c1);
+        sinf ^= gf_mul(eq[i], gf_mul(ai, bi));
+      }
+      std::lock_guard<std::mutex> g(m);
+      y1 ^= s1;
+      yinf ^= sinf;
+    });
     const u128 alpha = point[n_rem - 1];
     // RoundEvals2::interpolate_eq: y0 = (sum - y1 alpha) / (1 - alpha)
     const u128 y0 = gf_mul(sum ^ gf_mul(y1, alpha), gf_inv(1 ^ alpha));
@@ -229,11 +258,13 @@ AndOutput and_reduction_prove(const uint64_t* a, const uint64_t* b, const uint64
     const u128 r = t.sample();
     challenges.push_back(r);
     sum = c0 ^ gf_mul(c1, r) ^ gf_mul(c2, gf_mul(r, r));
-    for (size_t i = 0; i < half; i++) {
-      fa[i] ^= gf_mul(r, fa[half + i] ^ fa[i]);
-      fb[i] ^= gf_mul(r, fb[half + i] ^ fb[i]);
-      fc[i] ^= gf_mul(r, fc[half + i] ^ fc[i]);
-    }
+    parallel_for(half, [&](size_t lo, size_t hi) {
+      for (size_t i = lo; i < hi; i++) {
+        fa[i] ^= gf_mul(r, fa[half + i] ^ fa[i]);
+        fb[i] ^= gf_mul(r, fb[half + i] ^ fb[i]);
+        fc[i] ^= gf_mul(r, fc[half + i] ^ fc[i]);
+      }
+    });
   }
   u128 evals[3] = {fa[0], fb[0], fc[0]};
   t.message_elems(evals, 3);

@@ -12,6 +12,7 @@
 //                fri/fold.rs:132-278, fri/verify.rs:40-320, merkle_tree/scheme.rs:85-180
 #include <string.h>
 
+#include <mutex>
 #include <vector>
 
 #include "oracle.h"
@@ -104,20 +105,27 @@ struct FriFolder {
 // ---------------------------------------------------------------- ring switching helpers
 
 // fold_1b_rows_for_b128 (ring_switch.rs:197-265): out[k] = sum_i bit_k(mat[i]) * vec[i].
+// Rows split over the threads; the partial sums are XORs, combined in any order.
 static void fold_1b_rows(const u128* mat, const u128* vec, size_t n, u128 out[128]) {
   for (int k = 0; k < 128; k++) out[k] = 0;
-  for (size_t i = 0; i < n; i++) {
-    u128 m = mat[i];
-    for (int k = 0; k < 128; k++)
-      if ((m >> k) & 1) out[k] ^= vec[i];
-  }
+  std::mutex mu;
+  parallel_for(n, [&](size_t lo, size_t hi) {
+    u128 part[128] = {0};
+    for (size_t i = lo; i < hi; i++) {
+      const u128 v = vec[i];
+      for (uint64_t w = (uint64_t)mat[i]; w; w &= w - 1) part[__builtin_ctzll(w)] ^= v;
+      for (uint64_t w = (uint64_t)(mat[i] >> 64); w; w &= w - 1) part[64 + __builtin_ctzll(w)] ^= v;
+    }
+    std::lock_guard<std::mutex> g(mu);
+    for (int k = 0; k < 128; k++) out[k] ^= part[k];
+  });
 }
 
 // fold_b128_elems_inplace (ring_switch.rs:130-171): x -> sum_k bit_k(x) * vec[k].
 static u128 fold_elem(u128 x, const u128 vec[128]) {
   u128 acc = 0;
-  for (int k = 0; k < 128; k++)
-    if ((x >> k) & 1) acc ^= vec[k];
+  for (uint64_t w = (uint64_t)x; w; w &= w - 1) acc ^= vec[__builtin_ctzll(w)];
+  for (uint64_t w = (uint64_t)(x >> 64); w; w &= w - 1) acc ^= vec[64 + __builtin_ctzll(w)];
   return acc;
 }
 
@@ -155,17 +163,26 @@ void pcs_prove(const FriParams& p, const u128* tw, const u128* codeword, const T
   eq_ind_partial_eval(r_dp, 7, eq_r);
   u128 sum = inner(s_hat_u, eq_r, 128);
   std::vector<u128> a(witness, witness + N), b(N);
-  for (size_t i = 0; i < N; i++) b[i] = fold_elem(suffix_tensor[i], eq_r);
+  parallel_for(N, [&](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; i++) b[i] = fold_elem(suffix_tensor[i], eq_r);
+  });
 
   // BaseFoldProver::prove: bivariate product sumcheck interleaved with FRI folding.
   FriFolder fri(p, tw, codeword, tree);
   for (uint32_t round = 0; round < n; round++) {
     size_t half = a.size() / 2;
     u128 y1 = 0, yinf = 0;
-    for (size_t i = 0; i < half; i++) {
-      y1 ^= gf_mul(a[half + i], b[half + i]);
-      yinf ^= gf_mul(a[i] ^ a[half + i], b[i] ^ b[half + i]);
-    }
+    std::mutex mu;
+    parallel_for(half, [&](size_t lo, size_t hi) {  // XOR sums: any split gives the same value
+      u128 s1 = 0, sinf = 0;
+      for (size_t i = lo; i < hi; i++) {
+        s1 ^= gf_mul(a[half + i], b[half + i]);
+        sinf ^= gf_mul(a[i] ^ a[half + i], b[i] ^ b[half + i]);
+      }
+      std::lock_guard<std::mutex> g(mu);
+      y1 ^= s1;
+      yinf ^= sinf;
+    });
     u128 c0 = sum ^ y1, c2 = yinf, c1 = y1 ^ c0 ^ c2;
     uint8_t root[32];
     bool committed = fri.execute_fold_round(root);
@@ -173,10 +190,12 @@ void pcs_prove(const FriParams& p, const u128* tw, const u128* codeword, const T
     t.message_elems(coeffs, 2);
     if (committed) t.message(root, 32);
     u128 r = t.sample();
-    for (size_t i = 0; i < half; i++) {
-      a[i] ^= gf_mul(r, a[half + i] ^ a[i]);
-      b[i] ^= gf_mul(r, b[half + i] ^ b[i]);
-    }
+    parallel_for(half, [&](size_t lo, size_t hi) {
+      for (size_t i = lo; i < hi; i++) {
+        a[i] ^= gf_mul(r, a[half + i] ^ a[i]);
+        b[i] ^= gf_mul(r, b[half + i] ^ b[i]);
+      }
+    });
     a.resize(half);
     b.resize(half);
     sum = c0 ^ gf_mul(c1, r) ^ gf_mul(c2, gf_mul(r, r));

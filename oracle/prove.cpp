@@ -60,14 +60,16 @@ Setup setup(uint32_t log_words, uint32_t log_inv_rate) {
 // eval_operand over every constraint of a CSR list; out is slot-major (out[slot * n + i]).
 std::vector<uint64_t> eval_ops(const uint64_t* words, const Ops& o) {
   std::vector<uint64_t> out((size_t)o.k * o.n, 0);
-  for (uint32_t c = 0; c < o.n; c++)
-    for (uint32_t sl = 0; sl < o.k; sl++) {
-      const uint32_t g = c * o.k + sl;
-      uint64_t acc = 0;
-      for (uint32_t e = o.off[g]; e < o.off[g + 1]; e++)
-        acc ^= shifted_word(words[o.vi[e]], o.var[e], o.amt[e]);
-      out[(size_t)sl * o.n + c] = acc;
-    }
+  parallel_for(o.n, [&](size_t c_lo, size_t c_hi) {  // constraints are independent
+    for (size_t c = c_lo; c < c_hi; c++)
+      for (uint32_t sl = 0; sl < o.k; sl++) {
+        const uint32_t g = (uint32_t)c * o.k + sl;
+        uint64_t acc = 0;
+        for (uint32_t e = o.off[g]; e < o.off[g + 1]; e++)
+          acc ^= shifted_word(words[o.vi[e]], o.var[e], o.amt[e]);
+        out[(size_t)sl * o.n + c] = acc;
+      }
+  });
   return out;
 }
 

@@ -14,6 +14,7 @@
 //   claim relation               verifier/verifier/src/protocols/shift/verify.rs:74-130
 #include <string.h>
 
+#include <mutex>
 #include <vector>
 
 #include "oracle.h"
@@ -91,15 +92,28 @@ u128 inner(const u128* a, const u128* b, size_t n) {
   return acc;
 }
 
-// One round of the bivariate product on (a, b) (halves lo | hi): y1, yinf.
+// One round of the bivariate product on (a, b) (halves lo | hi): y1, yinf.  The sums are XORs,
+// so the threads' partial sums combine to the same values in any order.
 void biv_round(const std::vector<u128>& a, const std::vector<u128>& b, size_t off, size_t len,
                u128& y1, u128& yinf) {
   const size_t half = len / 2;
-  for (size_t i = 0; i < half; i++) {
-    const u128 a0 = a[off + i], a1 = a[off + half + i], b0 = b[off + i], b1 = b[off + half + i];
-    y1 ^= gf_mul(a1, b1);
-    yinf ^= gf_mul(a0 ^ a1, b0 ^ b1);
-  }
+  std::mutex m;
+  parallel_for(half, [&](size_t lo, size_t hi) {
+    u128 s1 = 0, sinf = 0;
+    for (size_t i = lo; i < hi; i++) {
+      const u128 a0 = a[off + i], a1 = a[off + half + i], b0 = b[off + i], b1 = b[off + half + i];
+      s1 ^= gf_mul(a1, b1);
+      sinf ^= gf_mul(a0 ^ a1, b0 ^ b1);
+    }
+    std::lock_guard<std::mutex> g(m);
+    y1 ^= s1;
+    yinf ^= sinf;
+  });
+}
+
+// out[i] ^= v for each set bit i of w.
+inline void xor_at_bits(u128* out, uint64_t w, u128 v) {
+  for (; w; w &= w - 1) out[__builtin_ctzll(w)] ^= v;
 }
 
 void fold_top(std::vector<u128>& a, size_t off, size_t len, u128 r, std::vector<u128>& out) {
@@ -134,18 +148,22 @@ ShiftResult shift_prove(const uint64_t* words, uint32_t log_words, uint32_t log_
 
   // ---- phase 1: g parts
   std::vector<u128> g(8 * 4096, 0);
+  std::mutex g_mu;
   auto add_terms = [&](const Ops& ops, const OpData& d) {
-    for (uint32_t c = 0; c < ops.n; c++)
-      for (uint32_t sl = 0; sl < ops.k; sl++) {
-        const uint32_t grp = c * ops.k + sl;
-        const u128 weight = gf_mul(d.lpow[ops.slot_to_operand[sl]], d.eq[c]);
-        for (uint32_t e = ops.off[grp]; e < ops.off[grp + 1]; e++) {
-          const uint64_t w = words[ops.vi[e]];
-          u128* row = g.data() + ops.var[e] * 4096 + ops.amt[e] * 64;
-          for (int j = 0; j < 64; j++)
-            if ((w >> j) & 1) row[j] ^= weight;
+    // constraints split over the threads, each into its own copy of g, XORed together at the end
+    parallel_for(ops.n, [&](size_t c_lo, size_t c_hi) {
+      std::vector<u128> part(8 * 4096, 0);
+      for (size_t c = c_lo; c < c_hi; c++)
+        for (uint32_t sl = 0; sl < ops.k; sl++) {
+          const uint32_t grp = (uint32_t)c * ops.k + sl;
+          const u128 weight = gf_mul(d.lpow[ops.slot_to_operand[sl]], d.eq[c]);
+          for (uint32_t e = ops.off[grp]; e < ops.off[grp + 1]; e++)
+            xor_at_bits(part.data() + ops.var[e] * 4096 + ops.amt[e] * 64, words[ops.vi[e]],
+                        weight);
         }
-      }
+      std::lock_guard<std::mutex> lk(g_mu);
+      for (size_t i = 0; i < part.size(); i++) g[i] ^= part[i];
+    });
   };
   add_terms(and_ops, band);
   add_terms(mul_ops, bmul);
@@ -183,12 +201,13 @@ ShiftResult shift_prove(const uint64_t* words, uint32_t log_words, uint32_t log_
   u128 eq_rj[64];
   eq_ind_partial_eval(r_j.data(), 6, eq_rj);
   std::vector<u128> W(N);
-  for (size_t i = 0; i < N; i++) {
-    u128 acc = 0;
-    for (int j = 0; j < 64; j++)
-      if ((words[i] >> j) & 1) acc ^= eq_rj[j];
-    W[i] = acc;
-  }
+  parallel_for(N, [&](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; i++) {
+      u128 acc = 0;
+      for (uint64_t w = words[i]; w; w &= w - 1) acc ^= eq_rj[__builtin_ctzll(w)];
+      W[i] = acc;
+    }
+  });
   std::vector<u128> rjs(r_j);
   rjs.insert(rjs.end(), r_s.begin(), r_s.end());
   std::vector<u128> eq_rjs(4096);
@@ -202,14 +221,25 @@ ShiftResult shift_prove(const uint64_t* words, uint32_t log_words, uint32_t log_
     for (int v = 0; v < 8; v++) h_ops[kind][v] = inner(hk.data() + v * 4096, eq_rjs.data(), 4096);
   }
   std::vector<u128> M(N, 0);
+  std::mutex m_mu;
   auto add_monster = [&](const Ops& ops, const OpData& d, int kind) {
-    for (uint32_t c = 0; c < ops.n; c++)
-      for (uint32_t sl = 0; sl < ops.k; sl++) {
-        const uint32_t grp = c * ops.k + sl;
-        const u128 weight = gf_mul(d.lpow[ops.slot_to_operand[sl]], d.eq[c]);
-        for (uint32_t e = ops.off[grp]; e < ops.off[grp + 1]; e++)
-          M[ops.vi[e]] ^= gf_mul(weight, gf_mul(h_ops[kind][ops.var[e]], eq_rs[ops.amt[e]]));
-      }
+    // h_op(variant) * eq(r_s, amount) once per (variant, amount); constraints split over the
+    // threads, each into its own copy of M, XORed together at the end
+    std::vector<u128> hs(8 * 64);
+    for (int v = 0; v < 8; v++)
+      for (int a = 0; a < 64; a++) hs[v * 64 + a] = gf_mul(h_ops[kind][v], eq_rs[a]);
+    parallel_for(ops.n, [&](size_t c_lo, size_t c_hi) {
+      std::vector<u128> part(N, 0);
+      for (size_t c = c_lo; c < c_hi; c++)
+        for (uint32_t sl = 0; sl < ops.k; sl++) {
+          const uint32_t grp = (uint32_t)c * ops.k + sl;
+          const u128 weight = gf_mul(d.lpow[ops.slot_to_operand[sl]], d.eq[c]);
+          for (uint32_t e = ops.off[grp]; e < ops.off[grp + 1]; e++)
+            part[ops.vi[e]] ^= gf_mul(weight, hs[ops.var[e] * 64 + ops.amt[e]]);
+        }
+      std::lock_guard<std::mutex> lk(m_mu);
+      for (size_t i = 0; i < N; i++) M[i] ^= part[i];
+    });
   };
   add_monster(and_ops, band, 0);
   add_monster(mul_ops, bmul, 1);
@@ -266,10 +296,12 @@ ShiftResult shift_prove(const uint64_t* words, uint32_t log_words, uint32_t log_
     ch2.push_back(r);
     shift_sum = s0 ^ gf_mul(s1, r) ^ gf_mul(s2, gf_mul(r, r));
     inout_eval = q0 ^ gf_mul(q1, r);
-    for (size_t i = 0; i < half; i++) {
-      W[i] ^= gf_mul(r, W[half + i] ^ W[i]);
-      M[i] ^= gf_mul(r, M[half + i] ^ M[i]);
-    }
+    parallel_for(half, [&](size_t lo, size_t hi) {
+      for (size_t i = lo; i < hi; i++) {
+        W[i] ^= gf_mul(r, W[half + i] ^ W[i]);
+        M[i] ^= gf_mul(r, M[half + i] ^ M[i]);
+      }
+    });
     W.resize(half);
     M.resize(half);
     if (n_rem <= p) gruen_n--;
