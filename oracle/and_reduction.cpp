@@ -193,12 +193,20 @@ void univariate_round(const uint64_t* a, const uint64_t* b, const uint64_t* c, u
 }
 
 // Folds each word into sum_t bit_t(w) L_t(z) over the domain {phi(t) : t < 64}.
+// The sum is linear in the word's bits, so it is tabulated per byte: tab[p][v] = sum over the set
+// bits b of v of lag[8p + b], and a word's sum is the XOR of its eight byte entries.
 void fold_words(const uint64_t* w, size_t n, const u128 lag[64], u128* out) {
+  std::vector<u128> tab(8 * 256);
+  for (int p = 0; p < 8; p++) {
+    u128* tp = tab.data() + 256 * p;
+    tp[0] = 0;
+    for (int v = 1; v < 256; v++) tp[v] = tp[v & (v - 1)] ^ lag[8 * p + __builtin_ctz(v)];
+  }
   parallel_for(n, [&](size_t lo, size_t hi) {
     for (size_t i = lo; i < hi; i++) {
+      const uint64_t x = w[i];
       u128 acc = 0;
-      for (int t = 0; t < 64; t++)
-        if ((w[i] >> t) & 1) acc ^= lag[t];
+      for (int p = 0; p < 8; p++) acc ^= tab[256 * p + ((x >> (8 * p)) & 0xff)];
       out[i] = acc;
     }
   });

@@ -136,11 +136,17 @@ void eq_ind_partial_eval(const u128* point, uint32_t n, u128* out) {
   out[0] = 1;
   size_t len = 1;
   for (uint32_t i = 0; i < n; i++) {
-    for (size_t j = 0; j < len; j++) {
-      u128 prod = gf_mul(out[j], point[i]);
-      out[j] ^= prod;
-      out[len + j] = prod;
-    }
+    auto expand = [&](size_t lo, size_t hi) {
+      for (size_t j = lo; j < hi; j++) {
+        u128 prod = gf_mul(out[j], point[i]);
+        out[j] ^= prod;
+        out[len + j] = prod;
+      }
+    };
+    if (len >= ((size_t)1 << 14))
+      parallel_for(len, expand);  // entries of one level are independent
+    else
+      expand(0, len);
     len <<= 1;
   }
 }
