@@ -224,11 +224,12 @@ ShiftResult shift_prove(const uint64_t* words, uint32_t log_words, uint32_t log_
   std::mutex m_mu;
   auto add_monster = [&](const Ops& ops, const OpData& d, int kind) {
     // h_op(variant) * eq(r_s, amount) once per (variant, amount); constraints split over the
-    // threads, each into its own copy of M, XORed together at the end
+    // threads, each into its own copy of M, XORed together at the end (the copies are held to
+    // 1 GiB in all; beyond that one thread adds every term)
     std::vector<u128> hs(8 * 64);
     for (int v = 0; v < 8; v++)
       for (int a = 0; a < 64; a++) hs[v * 64 + a] = gf_mul(h_ops[kind][v], eq_rs[a]);
-    parallel_for(ops.n, [&](size_t c_lo, size_t c_hi) {
+    auto run = [&](size_t c_lo, size_t c_hi) {
       std::vector<u128> part(N, 0);
       for (size_t c = c_lo; c < c_hi; c++)
         for (uint32_t sl = 0; sl < ops.k; sl++) {
@@ -239,7 +240,11 @@ ShiftResult shift_prove(const uint64_t* words, uint32_t log_words, uint32_t log_
         }
       std::lock_guard<std::mutex> lk(m_mu);
       for (size_t i = 0; i < N; i++) M[i] ^= part[i];
-    });
+    };
+    if ((uint64_t)N * sizeof(u128) * (uint64_t)num_threads() <= (1ull << 30))
+      parallel_for(ops.n, run);
+    else
+      run(0, ops.n);
   };
   add_monster(and_ops, band, 0);
   add_monster(mul_ops, bmul, 1);
