@@ -68,6 +68,41 @@ def test_argument_errors_without_gpu():
                                          ctypes.c_void_p(16), None) == _ffi.BINIUS_E_ARG
 
 
+def test_boundary_entries_reject_bad_arguments_without_gpu():
+    """The MerkleTreeProver::layer, SumcheckProver, set-up and host-buffer prove entries check
+    their arguments before touching the device (the pointers below are never dereferenced)."""
+    L = _ffi.lib()
+    E = _ffi.BINIUS_E_ARG
+    fake = ctypes.c_void_p(256)
+    # MerkleTreeProver::layer: NULL buffers; a layer below the leaves is IncorrectLayerDepth
+    assert L.binius_merkle_layer(None, 4, 2, fake, None) == E
+    assert L.binius_merkle_layer(fake, 4, 5, fake, None) == E
+    assert b"IncorrectLayerDepth" in L.binius_last_error()
+    out = ctypes.c_void_p()
+    assert L.binius_sumcheck_bivariate_create(None, fake, 4, fake, None, ctypes.byref(out)) == E
+    assert L.binius_sumcheck_quadratic_mle_create(fake, fake, fake, 34, fake, fake, None,
+                                                  ctypes.byref(out)) == E
+    assert L.binius_sumcheck_quadratic_mle_create(fake, fake, fake, 3, None, fake, None,
+                                                  ctypes.byref(out)) == E
+    # InOutCheckProver::new asserts eval_point.len() <= witness.log_len()
+    assert L.binius_sumcheck_inout_create(fake, 3, fake, 4, None, ctypes.byref(out)) == E
+    assert out.value is None
+    # round calls on a NULL prover
+    buf = (ctypes.c_uint8 * 64)()
+    n = ctypes.c_uint32()
+    for name in ("bivariate", "quadratic_mle", "inout"):
+        assert getattr(L, f"binius_sumcheck_{name}_execute")(None, buf, ctypes.byref(n)) == E
+        assert getattr(L, f"binius_sumcheck_{name}_fold")(None, buf) == E
+        assert getattr(L, f"binius_sumcheck_{name}_finish")(None, buf) == E
+    assert L.binius_sumcheck_destroy(None) == _ffi.BINIUS_OK
+    assert L.binius_sumcheck_n_vars(None) == 0
+    # one-call set-up and the host-buffer prove
+    assert L.binius_setup(0, None, 0, 1, None, 0, ctypes.byref(out)) == E
+    ln = ctypes.c_size_t(7)
+    assert L.binius_prove(None, fake, 16, None, fake, 16, ctypes.byref(ln), None) == E
+    assert ln.value == 7  # rejected before *len is written
+
+
 def test_check_maps_argument_error():
     L = _ffi.lib()
     rc = L.binius_merkle_commit(None, 3, 0, None, None)
