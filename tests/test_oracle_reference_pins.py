@@ -12,6 +12,9 @@
   at the hypercube vertices, with the challenge on a domain point, every h_op value is the
   indicator of its integer shift relation -- for the restated evaluate_h_op and for the oracle's
   build_h_parts on every vertex.
+* verifier/verifier/src/and_reduction/univariate/univariate_poly.rs:151-182
+  (univariate_po2_sanity_check): Lagrange evaluation over the embedded AES subspace agrees with
+  the embedded monomial form, which pins the embedding and the 64-point Lagrange basis together.
 * prover/prover/src/fri/fold.rs:334-369 (test_fri_compatible_ntt_domains) with the shrunk cases of
   prover/prover/proptest-regressions/fri/fold.txt (log_dim = 0 with arity 0 and 1) first, then
   the property's whole range (log_dim < 8, arity < 4): over the domain of
@@ -216,6 +219,37 @@ def test_h_op_hypercube_vertices():
             for j in range(64):
                 want[:, s * 64 + j, 0] = h_op_indicators(i, j, s)
         assert np.array_equal(h, want), i
+
+
+def test_univariate_po2_sanity_check():
+    """verifier/verifier/src/and_reduction/univariate/univariate_poly.rs:151-182
+    (univariate_po2_sanity_check): a polynomial of degree < 64 with AES-field coefficients, given
+    by its values on the 6-dimensional AES subspace (the integers 0..63), evaluated at a GHASH
+    challenge by Lagrange interpolation over the embedded domain equals the polynomial with
+    embedded coefficients evaluated there.  The oracle's Lagrange evaluations over
+    {phi(t) : t < 64} (the ones build_h_parts and the AND reduction use) stand in for
+    GenericPo2UnivariatePoly::evaluate_at_challenge."""
+    phi = orc.aes_to_ghash_table()
+    rng = np.random.default_rng(5)
+    for _ in range(4):
+        coeffs = [int(x) for x in rng.integers(0, 256, size=64)]
+        values = []
+        for t in range(64):
+            acc, x = 0, 1
+            for c in coeffs:
+                acc ^= orc.aes_mul(c, x)
+                x = orc.aes_mul(x, t)
+            values.append(acc)
+        z = int.from_bytes(rng.bytes(16), "little")
+        _, lt = orc.shift_h_parts(z)
+        lhs = 0
+        for t in range(64):
+            lhs ^= gm(phi[values[t]], orc.to_int(lt[t]))
+        rhs, zp = 0, 1
+        for c in coeffs:
+            rhs ^= gm(phi[c], zp)
+            zp = gm(zp, z)
+        assert lhs == rhs
 
 
 # ---------------------------------------------------------------- FRI fold / encode commutation
