@@ -16,7 +16,7 @@
 // The univariate message is the interpolation of each 64-bit word (bit t = value at the domain
 // point t of the 6-dimensional subspace of GF(2^8) with basis 1, 2, .., 32) evaluated at the 64
 // points 64..127; any exact method gives the same field values, so the oracle evaluates the
-// Lagrange basis directly.
+// Lagrange basis directly, tabulated per byte of the word.
 #include <string.h>
 
 #include <mutex>
