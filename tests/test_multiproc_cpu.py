@@ -52,3 +52,15 @@ def test_single_rank_is_identity():
     import bench
     assert bench.max_over_ranks(3.5, None, "cpu") == 3.5
     assert bench.whole_job_ms_per_unit(40.0, 10, 1) == 4.0
+
+
+def test_roofline_traffic_comes_from_committed_profiles():
+    """The bench's roofline lines read `traffic` (DRAM bytes per launch) from the committed ncu
+    summaries of the kernels they time; both summaries carry the figure."""
+    import bench
+    fold = bench.profiled_traffic("bivariate_fold_eval_kernel_log20.md")
+    ntt = bench.profiled_traffic("ntt_pass_kernel_log20_b4.md")
+    assert isinstance(fold, int) and isinstance(ntt, int)
+    # the fold reads its two 2^20-element operands (32 MiB) once: traffic near the read bytes
+    assert 32 << 20 <= fold <= 48 << 20
+    assert ntt > 0
