@@ -1,6 +1,7 @@
 """The multi-GPU plumbing of bench.py on CPU: ranks as gloo processes (world size 2), each with its
 own timing; every rank must see the slowest rank's time, and the whole-job figure divides it over
-all ranks' units (replicas: weak scaling, no data-path collective)."""
+all ranks' units (replicas: weak scaling, no data-path collective).  Also the bench helper that
+reads the roofline's DRAM traffic from the committed ncu summaries."""
 import os
 import socket
 
