@@ -41,6 +41,24 @@ def test_prove_verify_round_trip(log_words, n_and, n_mul, log_public, seed):
     assert orc.prove(sc.witness, log_public, prep.and_csr, prep.mul_csr) == proof
 
 
+def test_proof_bytes_do_not_depend_on_host_threads():
+    """The oracle splits its sums and folds over the host threads (the bench's CPU baseline uses
+    every core, the GPU tests eight); every split must give the same proof bytes.  2^16 words so
+    that the large eq tensor levels and the per-thread partial sums all take their threaded
+    branches."""
+    sc, prep = _circuit(16, 60000, 70, 11, 2)
+    proofs = []
+    try:
+        for threads in (1, 3, 8):
+            orc.set_threads(threads)
+            proofs.append(orc.prove(sc.witness, 2, prep.and_csr, prep.mul_csr))
+    finally:
+        orc.set_threads(1)
+    assert proofs[0] == proofs[1] == proofs[2]
+    pub = sc.witness[:4]
+    assert orc.verify(pub, 16, 2, prep.and_csr, prep.mul_csr, proofs[0]) == 0
+
+
 def test_verify_rejects_tampering_and_wrong_public_input():
     sc, prep = _circuit(9, 100, 3, 4)
     proof = orc.prove(sc.witness, 1, prep.and_csr, prep.mul_csr)
